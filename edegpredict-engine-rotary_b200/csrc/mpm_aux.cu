@@ -1,0 +1,740 @@
+// mpm_aux.cu -- re-binning (counting sort by 4^3-cell bin), scans, upload and
+// download conversions, the reference-layout AoS export, FP64 metric
+// reductions, tool rasterisation and the seeded workpiece generator.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "mpm_device.cuh"
+#include "mpm_internal.h"
+
+namespace mpmb {
+
+namespace {
+
+constexpr int kT = 256;
+
+inline int nblk(int64_t n, int t = kT) {
+    int64_t b = (n + t - 1) / t;
+    if (b < 1) b = 1;
+    if (b > (1 << 20)) b = (1 << 20);
+    return (int)b;
+}
+
+template <typename R> __device__ __forceinline__ R ld_user(const void* p, int elem, int64_t i) {
+    return elem == 8 ? (R)((const double*)p)[i] : (R)((const float*)p)[i];
+}
+__device__ __forceinline__ double ld_userd(const void* p, int elem, int64_t i) {
+    return elem == 8 ? ((const double*)p)[i] : (double)((const float*)p)[i];
+}
+__device__ __forceinline__ void st_user(void* p, int elem, int64_t i, double v) {
+    if (elem == 8) ((double*)p)[i] = v; else ((float*)p)[i] = (float)v;
+}
+
+template <typename R> __device__ __forceinline__ int find_inst(const Inst<R>* insts, int n_inst, int64_t pi) {
+    int lo = 0, hi = n_inst - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (insts[mid].pbase <= pi) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ scan
+
+// Three-phase exclusive scan: per-CTA scan of 1024 elements with block sums,
+// a single-CTA scan of the block sums, then the offsets are added.
+__global__ void k_scan_local(const int32_t* in, int32_t* out, int32_t* sums, int64_t n) {
+    __shared__ int32_t s[1024];
+    const int64_t base = (int64_t)blockIdx.x * 1024;
+    const int t = threadIdx.x;  // 512 threads, 2 elements each
+    int64_t i0 = base + 2 * t, i1 = i0 + 1;
+    int32_t a = i0 < n ? in[i0] : 0, b = i1 < n ? in[i1] : 0;
+    s[2 * t] = a;
+    s[2 * t + 1] = b;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {  // Hillis-Steele on the 1024 values
+        int32_t x0 = 0, x1 = 0;
+        int j0 = 2 * t, j1 = 2 * t + 1;
+        if (j0 >= off) x0 = s[j0 - off];
+        if (j1 >= off) x1 = s[j1 - off];
+        __syncthreads();
+        s[j0] += x0;
+        s[j1] += x1;
+        __syncthreads();
+    }
+    if (i0 < n) out[i0] = s[2 * t] - a;
+    if (i1 < n) out[i1] = s[2 * t + 1] - b;
+    if (t == 511) sums[blockIdx.x] = s[1023];
+}
+
+__global__ void k_scan_sums(int32_t* sums, int nb) {
+    __shared__ int32_t carry;
+    __shared__ int32_t s[1024];
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < nb; base += 1024) {
+        const int t = threadIdx.x;
+        int32_t v = (base + t < nb) ? sums[base + t] : 0;
+        s[t] = v;
+        __syncthreads();
+        for (int off = 1; off < 1024; off <<= 1) {
+            int32_t x = t >= off ? s[t - off] : 0;
+            __syncthreads();
+            s[t] += x;
+            __syncthreads();
+        }
+        if (base + t < nb) sums[base + t] = carry + s[t] - v;
+        __syncthreads();
+        if (t == 1023) carry += s[1023];
+        __syncthreads();
+    }
+}
+
+__global__ void k_scan_add(int32_t* out, const int32_t* sums, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += sums[i / 1024];
+}
+
+int64_t scan_tmp_size(int64_t n) { return (n + 1023) / 1024 + 1; }
+
+void exclusive_scan(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t st) {
+    if (n <= 0) return;
+    const int nb = (int)((n + 1023) / 1024);
+    k_scan_local<<<nb, 512, 0, st>>>(in, out, tmp, n);
+    k_scan_sums<<<1, 1024, 0, st>>>(tmp, nb);
+    k_scan_add<<<(int)((n + 255) / 256), 256, 0, st>>>(out, tmp, n);
+    launch_counter() += 3;
+}
+
+__global__ void k_fill_i32(int32_t* p, int32_t v, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+void fill_i32(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
+    if (n > 0) {
+        k_fill_i32<<<nblk(n), kT, 0, st>>>(p, v, n);
+        ++launch_counter();
+    }
+}
+
+// ------------------------------------------------------------------ work list
+
+__global__ void k_work_flags(const int32_t* count, const int32_t* key_bin, const int32_t* key_inst, int64_t nkeys,
+                             int32_t* flag) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nkeys) flag[k] = (key_bin[k] >= 0 && count[k] > 0) ? 1 : 0;
+}
+
+__global__ void k_work_emit(const int32_t* count, const int32_t* offset, const int32_t* key_inst,
+                            const int32_t* key_bin, const int64_t* inst_pbase, const int32_t* flag,
+                            const int32_t* flag_scan, int64_t nkeys, Work* work, int* n_work) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nkeys && flag[k]) {
+        const int i = key_inst[k];
+        Work w;
+        w.inst = i;
+        w.bin = key_bin[k];
+        w.start = (int)(offset[k] - inst_pbase[i]);
+        w.count = count[k];
+        work[flag_scan[k]] = w;
+    }
+    if (k == nkeys - 1) *n_work = flag_scan[k] + flag[k];
+}
+
+void build_work(const int32_t* count, const int32_t* offset, const int32_t* key_inst, const int32_t* key_bin,
+                const int64_t* inst_pbase, int64_t nkeys, int32_t* flag, int32_t* flag_scan, int32_t* tmp, Work* work,
+                int* n_work, cudaStream_t st) {
+    k_work_flags<<<nblk(nkeys), kT, 0, st>>>(count, key_bin, key_inst, nkeys, flag);
+    exclusive_scan(flag, flag_scan, nkeys, tmp, st);
+    k_work_emit<<<nblk(nkeys), kT, 0, st>>>(count, offset, key_inst, key_bin, inst_pbase, flag, flag_scan, nkeys,
+                                            work, n_work);
+    launch_counter() += 2;
+}
+
+// ------------------------------------------------------------------ re-bin
+
+// New key of every particle: the bin of its stencil base node, or the
+// instance's sentinel key when INACTIVE; rank = order of arrival in the key.
+template <typename R>
+__global__ void k_bin_count(const Inst<R>* insts, int n_inst, PState<R> ps, const int32_t* key_base, bool initial,
+                            const double* pos_scratch, int32_t* key, int32_t* rank, int32_t* count, int32_t* newbin,
+                            int64_t np) {
+    const int64_t pi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pi >= np) return;
+    const int ii = find_inst(insts, n_inst, pi);
+    const Inst<R>& P = insts[ii];
+    if (pi >= P.pbase + P.np) return;  // unused slot of the instance
+    const bool fresh = initial && P.fresh;
+    int b[3];
+    if (fresh) {
+        for (int a = 0; a < 3; ++a) b[a] = (int)floor(pos_scratch[3 * pi + a] - 0.5);
+    } else {
+        const int bn = ps.bin[pi];
+        const int ob[3] = {bn % P.nbx, (bn / P.nbx) % P.nby, bn / (P.nbx * P.nby)};
+        const V4<R> a0 = ps.A[0][pi];
+        const R xl[3] = {a0.x, a0.y, a0.z};
+        for (int a = 0; a < 3; ++a) b[a] = ob[a] * kBin + (int)floor(xl[a] - R(0.5));
+    }
+    const int nb[3] = {P.nbx, P.nby, P.nbz};
+    int B[3];
+    for (int a = 0; a < 3; ++a) {
+        int q = b[a] >= 0 ? b[a] / kBin : -1;
+        B[a] = q < 0 ? 0 : (q >= nb[a] ? nb[a] - 1 : q);
+    }
+    const int bin = B[0] + P.nbx * (B[1] + P.nby * B[2]);
+    const int nbins = P.nbx * P.nby * P.nbz;
+    const int32_t kk = key_base[ii] + ((ps.status[pi] == ST_INACTIVE) ? nbins : bin);
+    key[pi] = kk;
+    newbin[pi] = bin;
+    rank[pi] = atomicAdd(&count[kk], 1);
+}
+
+template <typename R>
+__global__ void k_bin_scatter(PState<R> src, PState<R> dst, const Inst<R>* insts, int n_inst, const int32_t* key,
+                              const int32_t* rank, const int32_t* offset, const int32_t* newbin, bool initial,
+                              const double* pos_scratch, bool has_K, int64_t np) {
+    const int64_t pi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pi >= np) return;
+    const int ii = find_inst(insts, n_inst, pi);
+    const Inst<R>& P = insts[ii];
+    if (pi >= P.pbase + P.np) return;
+    const bool fresh = initial && P.fresh;
+    const int64_t d = offset[key[pi]] + rank[pi];
+    const int nbn = newbin[pi];
+    const int nbv[3] = {nbn % P.nbx, (nbn / P.nbx) % P.nby, nbn / (P.nbx * P.nby)};
+    V4<R> a0 = src.A[0][pi];
+    if (fresh) {
+        a0.x = (R)(pos_scratch[3 * pi + 0] - (double)(nbv[0] * kBin));
+        a0.y = (R)(pos_scratch[3 * pi + 1] - (double)(nbv[1] * kBin));
+        a0.z = (R)(pos_scratch[3 * pi + 2] - (double)(nbv[2] * kBin));
+    } else {
+        const int ob = src.bin[pi];
+        const int obv[3] = {ob % P.nbx, (ob / P.nbx) % P.nby, ob / (P.nbx * P.nby)};
+        if (ob != nbn) {
+            a0.x += (R)((obv[0] - nbv[0]) * kBin);
+            a0.y += (R)((obv[1] - nbv[1]) * kBin);
+            a0.z += (R)((obv[2] - nbv[2]) * kBin);
+        }
+    }
+    dst.A[0][d] = a0;
+#pragma unroll
+    for (int q = 1; q < 6; ++q) dst.A[q][d] = src.A[q][pi];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) dst.B[q][d] = src.B[q][pi];
+    dst.S[0][d] = src.S[0][pi];
+    dst.S[1][d] = src.S[1][pi];
+    if (has_K) {
+        dst.K[0][d] = src.K[0][pi];
+        dst.K[1][d] = src.K[1][pi];
+    }
+    dst.sres[d] = src.sres[pi];
+    dst.status[d] = src.status[pi];
+    dst.id[d] = src.id[pi];
+    dst.orig[d] = src.orig[pi];
+    dst.bin[d] = nbn;
+}
+
+// Unused slots of each instance are counted into the instance's last key so
+// that the global scan keeps every instance at its own slot range.
+template <typename R>
+__global__ void k_pad_counts(const Inst<R>* insts, int n_inst, const int32_t* key_base, int32_t* count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_inst) return;
+    count[key_base[i] + insts[i].nbins + 1] = (int32_t)(insts[i].pcap - insts[i].np);
+}
+
+template <typename R>
+void launch_pad_counts(const Inst<R>* insts, int n_inst, const int32_t* key_base, int32_t* count, cudaStream_t st) {
+    k_pad_counts<R><<<(n_inst + 127) / 128, 128, 0, st>>>(insts, n_inst, key_base, count);
+    ++launch_counter();
+}
+template void launch_pad_counts<float>(const Inst<float>*, int, const int32_t*, int32_t*, cudaStream_t);
+template void launch_pad_counts<double>(const Inst<double>*, int, const int32_t*, int32_t*, cudaStream_t);
+
+// ------------------------------------------------------------------ raster
+
+// rasterizeToolKernel (reference src/MPMSolver.cu:444-473): each tool sample
+// marks the 2x2x2 nodes from round((x - min)/dx).
+__global__ void k_raster(const double* sx, const double* sy, const double* sz, int ns, double px, double py,
+                         double pz, double ox, double oy, double oz, double inv_dx, int nx, int ny, int nz,
+                         uint8_t* mask) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ns) return;
+    const int gx = (int)round(((px + sx[t]) - ox) * inv_dx);
+    const int gy = (int)round(((py + sy[t]) - oy) * inv_dx);
+    const int gz = (int)round(((pz + sz[t]) - oz) * inv_dx);
+    for (int a = 0; a < 2; ++a) {
+        const int cx = gx + a;
+        if (cx < 0 || cx >= nx) continue;
+        for (int b = 0; b < 2; ++b) {
+            const int cy = gy + b;
+            if (cy < 0 || cy >= ny) continue;
+            for (int c = 0; c < 2; ++c) {
+                const int cz = gz + c;
+                if (cz < 0 || cz >= nz) continue;
+                mask[cx + (int64_t)nx * (cy + (int64_t)ny * cz)] = 1;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ upload
+
+template <typename R>
+__global__ void k_import(DevSoA in, int64_t n, double ox, double oy, double oz, double inv_dx, double Tamb, PState<R> ps,
+                         int64_t pbase, double* pos_scratch) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int e = in.elem;
+    const int64_t d = pbase + i;
+    const double x = ld_userd(in.x, e, i), y = ld_userd(in.y, e, i), z = ld_userd(in.z, e, i);
+    pos_scratch[3 * d + 0] = (x - ox) * inv_dx;
+    pos_scratch[3 * d + 1] = (y - oy) * inv_dx;
+    pos_scratch[3 * d + 2] = (z - oz) * inv_dx;
+    const R eps = in.eps ? ld_user<R>(in.eps, e, i) : R(0);
+    R H[9], Hp[9], C[9];
+    for (int q = 0; q < 9; ++q) {
+        const double id = (q % 4 == 0) ? 1.0 : 0.0;
+        H[q] = in.F ? (R)(ld_userd(in.F, e, 9 * i + q) - id) : R(0);
+        Hp[q] = in.Fp ? (R)(ld_userd(in.Fp, e, 9 * i + q) - id) : R(0);
+        C[q] = in.C ? ld_user<R>(in.C, e, 9 * i + q) : R(0);
+    }
+    const R dT = in.T ? (R)(ld_userd(in.T, e, i) - Tamb) : R(0);
+    const R D = in.D ? ld_user<R>(in.D, e, i) : R(0);
+    ps.A[0][d] = mk4<R>(R(0), R(0), R(0), eps);
+    ps.A[1][d] = mk4<R>(H[0], H[1], H[2], H[3]);
+    ps.A[2][d] = mk4<R>(H[4], H[5], H[6], H[7]);
+    ps.A[3][d] = mk4<R>(H[8], Hp[8], dT, D);
+    ps.A[4][d] = mk4<R>(Hp[0], Hp[1], Hp[2], Hp[3]);
+    ps.A[5][d] = mk4<R>(Hp[4], Hp[5], Hp[6], Hp[7]);
+    const R vx = in.vx ? ld_user<R>(in.vx, e, i) : R(0), vy = in.vy ? ld_user<R>(in.vy, e, i) : R(0),
+            vz = in.vz ? ld_user<R>(in.vz, e, i) : R(0);
+    const R ed = in.edot ? ld_user<R>(in.edot, e, i) : R(0);
+    ps.B[0][d] = mk4<R>(vx, vy, vz, ed);
+    ps.B[1][d] = mk4<R>(C[0], C[1], C[2], C[3]);
+    ps.B[2][d] = mk4<R>(C[4], C[5], C[6], C[7]);
+    ps.B[3][d] = mk4<R>(C[8], R(0), R(0), R(0));
+    R s[6] = {0, 0, 0, 0, 0, 0}, k[6] = {0, 0, 0, 0, 0, 0};
+    for (int q = 0; q < 6; ++q) {
+        if (in.stress) s[q] = ld_user<R>(in.stress, e, 6 * i + q);
+        if (in.bs) k[q] = ld_user<R>(in.bs, e, 6 * i + q);
+    }
+    ps.S[0][d] = mk4<R>(s[0], s[1], s[2], s[3]);
+    ps.S[1][d] = mk4<R>(s[4], s[5], R(0), R(0));
+    if (ps.K[0]) {
+        ps.K[0][d] = mk4<R>(k[0], k[1], k[2], k[3]);
+        ps.K[1][d] = mk4<R>(k[4], k[5], R(0), R(0));
+    }
+    ps.sres[d] = in.sres ? ld_user<R>(in.sres, e, i) : R(0);
+    ps.status[d] = in.status ? (uint8_t)in.status[i] : (uint8_t)ST_ACTIVE;
+    ps.id[d] = in.id ? in.id[i] : (int32_t)i;
+    ps.orig[d] = (int32_t)i;
+    ps.bin[d] = 0;
+}
+
+// ------------------------------------------------------------------ generator
+
+// Seeded box workpiece: candidate (cell, k) gets Philox4x32-10 uniforms keyed
+// by (seed_lo, seed_hi) with counter (cell index in the box, k, instance, 0).
+// keep = not inside the tool at t=0 (phi > 0 when a tool is given).
+template <typename R>
+__global__ void k_gen_flags(Inst<R> P, int c0x, int c0y, int c0z, int wx, int wy, int wz, int ppc, uint32_t s0,
+                            uint32_t s1, uint32_t inst, int tool_check, int32_t* flag, int64_t ncand) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncand) return;
+    int keep = 1;
+    if (tool_check) {
+        const int64_t cell = c / ppc;
+        const int k = (int)(c % ppc);
+        const int ix = (int)(cell % wx), iy = (int)((cell / wx) % wy), iz = (int)(cell / ((int64_t)wx * wy));
+        float u[4];
+        philox_u4(s0, s1, (uint32_t)cell, (uint32_t)k, inst, 0u, u);
+        const double x = P.ox + ((double)(c0x + ix) + (double)u[0]) * P.dx;
+        const double z = P.oz + ((double)(c0z + iz) + (double)u[2]) * P.dx;
+        (void)iy;
+        double nrm[3];
+        if (tool_sdf(P, x, z, P.tool_p0[0], P.tool_p0[2], nrm) <= 0.0) keep = 0;
+    }
+    flag[c] = keep;
+}
+
+template <typename R>
+__global__ void k_gen_write(Inst<R> P, int c0x, int c0y, int c0z, int wx, int wy, int wz, int ppc, uint32_t s0,
+                            uint32_t s1, uint32_t inst, int fixed_layers, R dT0, const int32_t* flag,
+                            const int32_t* idx, PState<R> ps, int64_t pbase, double* pos_scratch, int64_t ncand) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncand || !flag[c]) return;
+    const int64_t cell = c / ppc;
+    const int k = (int)(c % ppc);
+    const int ix = (int)(cell % wx), iy = (int)((cell / wx) % wy), iz = (int)(cell / ((int64_t)wx * wy));
+    float u[4];
+    philox_u4(s0, s1, (uint32_t)cell, (uint32_t)k, inst, 0u, u);
+    const int64_t i = idx[c];
+    const int64_t d = pbase + i;
+    pos_scratch[3 * d + 0] = (double)(c0x + ix) + (double)u[0];
+    pos_scratch[3 * d + 1] = (double)(c0y + iy) + (double)u[1];
+    pos_scratch[3 * d + 2] = (double)(c0z + iz) + (double)u[2];
+    ps.A[0][d] = mk4<R>(R(0), R(0), R(0), R(0));
+    ps.A[1][d] = mk4<R>(R(0), R(0), R(0), R(0));
+    ps.A[2][d] = mk4<R>(R(0), R(0), R(0), R(0));
+    ps.A[3][d] = mk4<R>(R(0), R(0), dT0, R(0));
+    ps.A[4][d] = mk4<R>(R(0), R(0), R(0), R(0));
+    ps.A[5][d] = mk4<R>(R(0), R(0), R(0), R(0));
+    for (int q = 0; q < 4; ++q) ps.B[q][d] = mk4<R>(R(0), R(0), R(0), R(0));
+    ps.S[0][d] = mk4<R>(R(0), R(0), R(0), R(0));
+    ps.S[1][d] = mk4<R>(R(0), R(0), R(0), R(0));
+    if (ps.K[0]) {
+        ps.K[0][d] = mk4<R>(R(0), R(0), R(0), R(0));
+        ps.K[1][d] = mk4<R>(R(0), R(0), R(0), R(0));
+    }
+    ps.sres[d] = R(0);
+    ps.status[d] = (iz < fixed_layers) ? (uint8_t)ST_FIXED : (uint8_t)ST_ACTIVE;
+    ps.id[d] = (int32_t)i;
+    ps.orig[d] = (int32_t)i;
+    ps.bin[d] = 0;
+    (void)wz;
+    (void)P;
+}
+
+// ------------------------------------------------------------------ download
+
+template <typename R>
+__device__ __forceinline__ void world_pos(const Inst<R>& P, int bin, const V4<R>& a0, double out[3]) {
+    const int bx = bin % P.nbx, by = (bin / P.nbx) % P.nby, bz = bin / (P.nbx * P.nby);
+    out[0] = P.ox + ((double)(bx * kBin) + (double)a0.x) * P.dx;
+    out[1] = P.oy + ((double)(by * kBin) + (double)a0.y) * P.dx;
+    out[2] = P.oz + ((double)(bz * kBin) + (double)a0.z) * P.dx;
+}
+
+template <typename R>
+__global__ void k_export(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64_t n, double Tamb, DevSoAOut o) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const Inst<R>& P = *inst;
+    const int64_t pi = pbase + s;
+    const int64_t i = ps.orig[pi];
+    const int e = o.elem;
+    const V4<R> a0 = ps.A[0][pi], a1 = ps.A[1][pi], a2 = ps.A[2][pi], a3 = ps.A[3][pi], a4 = ps.A[4][pi],
+                a5 = ps.A[5][pi];
+    const V4<R> b0 = ps.B[0][pi], b1 = ps.B[1][pi], b2 = ps.B[2][pi], b3 = ps.B[3][pi];
+    double xw[3];
+    world_pos(P, ps.bin[pi], a0, xw);
+    if (o.x) st_user(o.x, e, i, xw[0]);
+    if (o.y) st_user(o.y, e, i, xw[1]);
+    if (o.z) st_user(o.z, e, i, xw[2]);
+    if (o.vx) st_user(o.vx, e, i, (double)b0.x);
+    if (o.vy) st_user(o.vy, e, i, (double)b0.y);
+    if (o.vz) st_user(o.vz, e, i, (double)b0.z);
+    if (o.edot) st_user(o.edot, e, i, (double)b0.w);
+    const R H[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
+    const R Hp[9] = {a4.x, a4.y, a4.z, a4.w, a5.x, a5.y, a5.z, a5.w, a3.y};
+    const R C[9] = {b1.x, b1.y, b1.z, b1.w, b2.x, b2.y, b2.z, b2.w, b3.x};
+    for (int q = 0; q < 9; ++q) {
+        const double id = (q % 4 == 0) ? 1.0 : 0.0;
+        if (o.F) st_user(o.F, e, 9 * i + q, (double)H[q] + id);
+        if (o.Fp) st_user(o.Fp, e, 9 * i + q, (double)Hp[q] + id);
+        if (o.C) st_user(o.C, e, 9 * i + q, (double)C[q]);
+    }
+    const V4<R> s0 = ps.S[0][pi], s1 = ps.S[1][pi];
+    const R sv[6] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y};
+    for (int q = 0; q < 6; ++q) {
+        if (o.stress) st_user(o.stress, e, 6 * i + q, (double)sv[q]);
+    }
+    if (o.bs) {
+        R kv[6] = {0, 0, 0, 0, 0, 0};
+        if (ps.K[0]) {
+            const V4<R> k0 = ps.K[0][pi], k1 = ps.K[1][pi];
+            kv[0] = k0.x; kv[1] = k0.y; kv[2] = k0.z; kv[3] = k0.w; kv[4] = k1.x; kv[5] = k1.y;
+        }
+        for (int q = 0; q < 6; ++q) st_user(o.bs, e, 6 * i + q, (double)kv[q]);
+    }
+    if (o.eps) st_user(o.eps, e, i, (double)a0.w);
+    if (o.T) st_user(o.T, e, i, Tamb + (double)a3.z);
+    if (o.D) st_user(o.D, e, i, (double)a3.w);
+    if (o.sres) st_user(o.sres, e, i, (double)ps.sres[pi]);
+    if (o.status) o.status[i] = ps.status[pi];
+    if (o.id) o.id[i] = ps.id[pi];
+}
+
+// MPMParticle, include/Types.h:199-266 (504 bytes): the byte layout that the
+// reference's ContactSolver, CFD coupling and exporters read.
+struct AosParticle {
+    double x, y, z, vx, vy, vz, fx, fy, fz, ext_fx, ext_fy, ext_fz;
+    double density, pressure, volume, mass, temperature;
+    double F[9], F_p[9], C[9];
+    double stress_xx, stress_yy, stress_zz, stress_xy, stress_xz, stress_yz;
+    double backstress_xx, backstress_yy, backstress_zz, backstress_xy, backstress_xz, backstress_yz;
+    double plasticStrain, strainRate, damage, residualStress;
+    int32_t id, status, cellHash, lodZone, lastUpdateStep;
+    uint8_t asbCounter;
+};
+static_assert(sizeof(AosParticle) == 504, "MPMParticle layout is 504 bytes");
+
+template <typename R>
+__global__ void k_export_aos(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64_t n, double Tamb, double rho,
+                             AosParticle* out) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const Inst<R>& P = *inst;
+    const int64_t pi = pbase + s;
+    AosParticle q;
+    const V4<R> a0 = ps.A[0][pi], a1 = ps.A[1][pi], a2 = ps.A[2][pi], a3 = ps.A[3][pi], a4 = ps.A[4][pi],
+                a5 = ps.A[5][pi];
+    const V4<R> b0 = ps.B[0][pi], b1 = ps.B[1][pi], b2 = ps.B[2][pi], b3 = ps.B[3][pi];
+    double xw[3];
+    world_pos(P, ps.bin[pi], a0, xw);
+    q.x = xw[0]; q.y = xw[1]; q.z = xw[2];
+    q.vx = b0.x; q.vy = b0.y; q.vz = b0.z;
+    q.fx = q.fy = q.fz = 0.0;
+    q.ext_fx = q.ext_fy = q.ext_fz = 0.0;
+    q.density = rho;
+    q.pressure = 0.0;
+    q.volume = (double)P.pvol;
+    q.mass = (double)P.pmass;
+    q.temperature = Tamb + (double)a3.z;
+    const R H[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
+    const R Hp[9] = {a4.x, a4.y, a4.z, a4.w, a5.x, a5.y, a5.z, a5.w, a3.y};
+    const R C[9] = {b1.x, b1.y, b1.z, b1.w, b2.x, b2.y, b2.z, b2.w, b3.x};
+    for (int k = 0; k < 9; ++k) {
+        const double id = (k % 4 == 0) ? 1.0 : 0.0;
+        q.F[k] = (double)H[k] + id;
+        q.F_p[k] = (double)Hp[k] + id;
+        q.C[k] = (double)C[k];
+    }
+    const V4<R> s0 = ps.S[0][pi], s1 = ps.S[1][pi];
+    q.stress_xx = s0.x; q.stress_yy = s0.y; q.stress_zz = s0.z; q.stress_xy = s0.w; q.stress_xz = s1.x; q.stress_yz = s1.y;
+    q.backstress_xx = q.backstress_yy = q.backstress_zz = q.backstress_xy = q.backstress_xz = q.backstress_yz = 0.0;
+    if (ps.K[0]) {
+        const V4<R> k0 = ps.K[0][pi], k1 = ps.K[1][pi];
+        q.backstress_xx = k0.x; q.backstress_yy = k0.y; q.backstress_zz = k0.z;
+        q.backstress_xy = k0.w; q.backstress_xz = k1.x; q.backstress_yz = k1.y;
+    }
+    q.plasticStrain = a0.w;
+    q.strainRate = b0.w;
+    q.damage = a3.w;
+    q.residualStress = ps.sres[pi];
+    q.id = ps.id[pi];
+    q.status = ps.status[pi];
+    q.cellHash = 0;
+    q.lodZone = 0;
+    q.lastUpdateStep = 0;
+    q.asbCounter = 0;
+    out[ps.orig[pi]] = q;
+}
+
+// ------------------------------------------------------------------ metrics
+
+// Per-CTA FP64 partials (slots below), then a single-CTA final pass:
+//  0 mass 1-3 momentum 4 kinetic 5 elastic 6 thermal 7 max dT 8 max vm 9 max eps
+//  10 sum eps 11 ref max stress 12 ref max T 13 ref kinetic 14 ref internal
+//  15 n active 16 n chip 17 n fixed 18 n inactive 19-21 bmin 22-24 bmax
+template <typename R>
+__global__ void k_stats(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64_t n, double mu, double K, double rho,
+                        double cp, double Tamb, double* partial) {
+    __shared__ double sh[kStatSlots][kT / 32];
+    const Inst<R>& P = *inst;
+    double acc[kStatSlots];
+    for (int q = 0; q < kStatSlots; ++q) acc[q] = 0.0;
+    acc[7] = -INFINITY; acc[8] = 0.0; acc[9] = -INFINITY; acc[11] = 0.0; acc[12] = 0.0;
+    for (int q = 19; q < 22; ++q) acc[q] = INFINITY;
+    for (int q = 22; q < 25; ++q) acc[q] = -INFINITY;
+    const double m = (double)P.pmass, V = (double)P.pvol;
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pi = pbase + s;
+        const int st = ps.status[pi];
+        if (st == ST_INACTIVE) { acc[18] += 1.0; continue; }
+        if (st == ST_ACTIVE) acc[15] += 1.0;
+        else if (st == ST_CHIP) acc[16] += 1.0;
+        else if (st == ST_FIXED) acc[17] += 1.0;
+        const V4<R> a0 = ps.A[0][pi], a3 = ps.A[3][pi], b0 = ps.B[0][pi], s0 = ps.S[0][pi], s1 = ps.S[1][pi];
+        const double sxx = s0.x, syy = s0.y, szz = s0.z, sxy = s0.w, sxz = s1.x, syz = s1.y;
+        const double tr = sxx + syy + szz;
+        const double dx_ = sxx - tr / 3.0, dy_ = syy - tr / 3.0, dz_ = szz - tr / 3.0;
+        const double vm = sqrt(1.5 * (dx_ * dx_ + dy_ * dy_ + dz_ * dz_ + 2.0 * (sxy * sxy + sxz * sxz + syz * syz)));
+        const double vx = b0.x, vy = b0.y, vz = b0.z;
+        const double v2 = vx * vx + vy * vy + vz * vz;
+        const double dT = a3.z, eps = a0.w;
+        acc[0] += m;
+        acc[1] += m * vx; acc[2] += m * vy; acc[3] += m * vz;
+        acc[4] += 0.5 * m * v2;
+        const double pr = tr / 3.0;
+        acc[5] += V * (vm * vm / (6.0 * mu) + pr * pr / (2.0 * K));
+        acc[6] += rho * V * cp * dT;
+        acc[7] = fmax(acc[7], dT);
+        acc[8] = fmax(acc[8], vm);
+        acc[9] = fmax(acc[9], eps);
+        acc[10] += eps;
+        if (st == ST_ACTIVE || st == ST_CHIP) {
+            acc[11] = fmax(acc[11], vm);
+            acc[12] = fmax(acc[12], Tamb + dT);
+            acc[13] += 0.5 * m * v2;
+            acc[14] += (vm * vm * m) / (6.0 * 80e9) + V * eps * vm;
+            double xw[3];
+            world_pos(P, ps.bin[pi], a0, xw);
+            for (int q = 0; q < 3; ++q) {
+                acc[19 + q] = fmin(acc[19 + q], xw[q]);
+                acc[22 + q] = fmax(acc[22 + q], xw[q]);
+            }
+        }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int q = 0; q < kStatSlots; ++q) {
+        double v = acc[q];
+        const bool isMin = (q >= 19 && q < 22);
+        const bool isMax = (q == 7 || q == 8 || q == 9 || q == 11 || q == 12 || (q >= 22 && q < 25));
+        for (int o = 16; o > 0; o >>= 1) {
+            const double u = __shfl_down_sync(0xffffffffu, v, o);
+            v = isMin ? fmin(v, u) : (isMax ? fmax(v, u) : v + u);
+        }
+        if (lane == 0) sh[q][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kStatSlots) {
+        const int q = threadIdx.x;
+        const bool isMin = (q >= 19 && q < 22);
+        const bool isMax = (q == 7 || q == 8 || q == 9 || q == 11 || q == 12 || (q >= 22 && q < 25));
+        double v = sh[q][0];
+        for (int w = 1; w < kT / 32; ++w) v = isMin ? fmin(v, sh[q][w]) : (isMax ? fmax(v, sh[q][w]) : v + sh[q][w]);
+        partial[(int64_t)blockIdx.x * kStatSlots + q] = v;
+    }
+}
+
+__global__ void k_stats_final(const double* partial, int nb, double* out) {
+    const int q = threadIdx.x;
+    if (q >= kStatSlots) return;
+    const bool isMin = (q >= 19 && q < 22);
+    const bool isMax = (q == 7 || q == 8 || q == 9 || q == 11 || q == 12 || (q >= 22 && q < 25));
+    double v = partial[q];
+    for (int b = 1; b < nb; ++b) {
+        const double u = partial[(int64_t)b * kStatSlots + q];
+        v = isMin ? fmin(v, u) : (isMax ? fmax(v, u) : v + u);
+    }
+    out[q] = v;
+}
+
+template <typename R>
+__global__ void k_set_temps(PState<R> ps, int64_t pbase, int64_t n, const double* T, int64_t count, double Tamb) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int64_t pi = pbase + s;
+    const int64_t o = ps.orig[pi];
+    if (o < count) {
+        V4<R> a3 = ps.A[3][pi];
+        a3.z = (R)(T[o] - Tamb);
+        ps.A[3][pi] = a3;
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+
+int64_t& launch_counter() {
+    static int64_t c = 0;
+    return c;
+}
+
+template <typename R>
+void launch_bin_count(const Inst<R>* insts, int n_inst, const PState<R>& ps, const int32_t* key_base, bool initial,
+                      const double* pos_scratch, int32_t* key, int32_t* rank, int32_t* count, int32_t* newbin,
+                      int64_t np, cudaStream_t st) {
+    if (np <= 0) return;
+    k_bin_count<R><<<(int)((np + kT - 1) / kT), kT, 0, st>>>(insts, n_inst, ps, key_base, initial, pos_scratch, key,
+                                                             rank, count, newbin, np);
+    ++launch_counter();
+}
+
+template <typename R>
+void launch_bin_scatter(const PState<R>& src, const PState<R>& dst, const Inst<R>* insts, int n_inst,
+                        const int32_t* key, const int32_t* rank, const int32_t* offset, const int32_t* newbin,
+                        bool initial, const double* pos_scratch, bool has_K, int64_t np, cudaStream_t st) {
+    if (np <= 0) return;
+    k_bin_scatter<R><<<(int)((np + kT - 1) / kT), kT, 0, st>>>(src, dst, insts, n_inst, key, rank, offset, newbin,
+                                                               initial, pos_scratch, has_K, np);
+    ++launch_counter();
+}
+
+void launch_raster(const double* sx, const double* sy, const double* sz, int ns, double px, double py, double pz,
+                   double ox, double oy, double oz, double dx, int nx, int ny, int nz, uint8_t* mask, cudaStream_t st) {
+    if (ns <= 0) return;
+    k_raster<<<(ns + kT - 1) / kT, kT, 0, st>>>(sx, sy, sz, ns, px, py, pz, ox, oy, oz, 1.0 / dx, nx, ny, nz, mask);
+    ++launch_counter();
+}
+
+template <typename R>
+void launch_import(const DevSoA& in, int64_t n, double ox, double oy, double oz, double dx, double Tamb,
+                   const PState<R>& ps, int64_t pbase, double* pos_scratch, cudaStream_t st) {
+    if (n <= 0) return;
+    k_import<R><<<(int)((n + kT - 1) / kT), kT, 0, st>>>(in, n, ox, oy, oz, 1.0 / dx, Tamb, ps, pbase, pos_scratch);
+    ++launch_counter();
+}
+
+template <typename R>
+void launch_gen(const Inst<R>& P, const int32_t c0[3], const int32_t c1[3], int ppc, uint64_t seed, uint32_t inst,
+                int fixed_layers, double dT0, int tool_check, int32_t* flag, int32_t* idx, int32_t* scan_tmp,
+                const PState<R>& ps, int64_t pbase, double* pos_scratch, cudaStream_t st) {
+    const int wx = c1[0] - c0[0], wy = c1[1] - c0[1], wz = c1[2] - c0[2];
+    const int64_t ncand = (int64_t)wx * wy * wz * ppc;
+    if (ncand <= 0) return;
+    const uint32_t s0 = (uint32_t)(seed & 0xffffffffu), s1 = (uint32_t)(seed >> 32);
+    const int nb = (int)((ncand + kT - 1) / kT);
+    k_gen_flags<R><<<nb, kT, 0, st>>>(P, c0[0], c0[1], c0[2], wx, wy, wz, ppc, s0, s1, inst, tool_check, flag, ncand);
+    exclusive_scan(flag, idx, ncand, scan_tmp, st);
+    k_gen_write<R><<<nb, kT, 0, st>>>(P, c0[0], c0[1], c0[2], wx, wy, wz, ppc, s0, s1, inst, fixed_layers, (R)dT0,
+                                      flag, idx, ps, pbase, pos_scratch, ncand);
+    launch_counter() += 2;
+}
+
+template <typename R>
+void launch_export(const Inst<R>* inst_dev, const PState<R>& ps, int64_t pbase, int64_t n, double Tamb,
+                   const DevSoAOut& out, cudaStream_t st) {
+    if (n <= 0) return;
+    k_export<R><<<(int)((n + kT - 1) / kT), kT, 0, st>>>(inst_dev, ps, pbase, n, Tamb, out);
+    ++launch_counter();
+}
+
+template <typename R>
+void launch_export_aos(const Inst<R>* inst_dev, const PState<R>& ps, int64_t pbase, int64_t n, double Tamb,
+                       double rho, void* out, cudaStream_t st) {
+    if (n <= 0) return;
+    k_export_aos<R><<<(int)((n + kT - 1) / kT), kT, 0, st>>>(inst_dev, ps, pbase, n, Tamb, rho, (AosParticle*)out);
+    ++launch_counter();
+}
+
+template <typename R>
+void launch_stats(const Inst<R>* inst_dev, const PState<R>& ps, int64_t pbase, int64_t n, double mu, double K,
+                  double rho, double cp, double Tamb, double* partial, int nblocks, double* out, cudaStream_t st) {
+    k_stats<R><<<nblocks, kT, 0, st>>>(inst_dev, ps, pbase, n, mu, K, rho, cp, Tamb, partial);
+    k_stats_final<<<1, kStatSlots, 0, st>>>(partial, nblocks, out);
+    launch_counter() += 2;
+}
+
+template <typename R>
+void launch_set_temps(const PState<R>& ps, int64_t pbase, int64_t n, const double* T, int64_t count, double Tamb,
+                      cudaStream_t st) {
+    if (n <= 0) return;
+    k_set_temps<R><<<(int)((n + kT - 1) / kT), kT, 0, st>>>(ps, pbase, n, T, count, Tamb);
+    ++launch_counter();
+}
+
+#define MPMB_INST(R)                                                                                                  \
+    template void launch_bin_count<R>(const Inst<R>*, int, const PState<R>&, const int32_t*, bool, const double*,   \
+                                      int32_t*, int32_t*, int32_t*, int32_t*, int64_t, cudaStream_t);               \
+    template void launch_bin_scatter<R>(const PState<R>&, const PState<R>&, const Inst<R>*, int, const int32_t*,    \
+                                        const int32_t*, const int32_t*, const int32_t*, bool, const double*, bool,  \
+                                        int64_t, cudaStream_t);                                                      \
+    template void launch_import<R>(const DevSoA&, int64_t, double, double, double, double, double, const PState<R>&, \
+                                   int64_t, double*, cudaStream_t);                                                  \
+    template void launch_gen<R>(const Inst<R>&, const int32_t*, const int32_t*, int, uint64_t, uint32_t, int, double, \
+                                int, int32_t*, int32_t*, int32_t*, const PState<R>&, int64_t, double*, cudaStream_t); \
+    template void launch_export<R>(const Inst<R>*, const PState<R>&, int64_t, int64_t, double, const DevSoAOut&,     \
+                                   cudaStream_t);                                                                    \
+    template void launch_export_aos<R>(const Inst<R>*, const PState<R>&, int64_t, int64_t, double, double, void*,    \
+                                       cudaStream_t);                                                                \
+    template void launch_stats<R>(const Inst<R>*, const PState<R>&, int64_t, int64_t, double, double, double, double, \
+                                  double, double*, int, double*, cudaStream_t);                                      \
+    template void launch_set_temps<R>(const PState<R>&, int64_t, int64_t, const double*, int64_t, double, cudaStream_t);
+
+MPMB_INST(float)
+MPMB_INST(double)
+
+}  // namespace mpmb

@@ -1,0 +1,195 @@
+// mpm_device.cuh -- device-side types and helpers of the B200 MPM step.
+//
+// Layout in HBM (per handle; a batch concatenates instances):
+//   particles, SoA of 16-byte (FP32) or 32-byte (FP64) vectors, one vector
+//   array per group of four scalars, so every particle load is one coalesced
+//   128-bit access per group:
+//     A0 = (xi_x, xi_y, xi_z, eps_p)   xi: position in cells relative to the
+//                                       origin of the particle's 4^3-cell bin
+//     A1 = (H0..H3) A2 = (H4..H7)      H  = F - I   (row-major)
+//     A3 = (H8, Hp8, dT, D)            Hp = F_p - I, dT = T - T_amb, D damage
+//     A4 = (Hp0..Hp3) A5 = (Hp4..Hp7)
+//     B0 = (vx, vy, vz, edot) B1 = (C0..C3) B2 = (C4..C7) B3 = (C8, 0, 0, 0)
+//     S0 = (sxx, syy, szz, sxy) S1 = (sxz, syz, 0, 0)
+//     K0/K1 backstress (same packing as S; only with H_kin > 0)
+//     sres (scalar), status (u8), id (i32)
+//   Storing F - I and F_p - I keeps FP32 relative precision on small strains;
+//   block-local positions keep ~5e-7-cell resolution for the per-step move.
+//   grid: per node one vector (m, p_x, p_y, p_z), row-major (x fastest); p
+//   already contains the internal and external force impulse f*dt.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mpmb {
+
+constexpr int kBin = 4;          // bin edge in cells (particles binned by their stencil base node)
+constexpr int kTile = 6;         // tile edge in nodes (bin + 2 for the quadratic stencil)
+constexpr int kTileNodes = kTile * kTile * kTile;
+// padded shared-memory plane: node (x,y,z) -> x + 8y + 68z; a warp of 32 distinct
+// bin cells (4x4x2) then maps to 32 distinct banks
+constexpr int kSY = 8, kSZ = 68, kPlane = 392;
+
+enum : uint8_t { ST_ACTIVE = 0, ST_INACTIVE = 1, ST_CHIP = 2, ST_BOUNDARY = 3, ST_FIXED = 4 };
+enum : int { TOOL_NONE = 0, TOOL_RASTER = 1, TOOL_SDF_STICKY = 2, TOOL_SDF_SLIP = 3 };
+enum : int { ERR_NUMERIC = 1, ERR_TIMEOUT = 2, ERR_NEWTON = 4 };
+
+struct alignas(32) D4 { double x, y, z, w; };
+
+template <typename R> struct V4T;
+template <> struct V4T<float> { using T = float4; };
+template <> struct V4T<double> { using T = D4; };
+template <typename R> using V4 = typename V4T<R>::T;
+
+template <typename R> __host__ __device__ inline V4<R> mk4(R a, R b, R c, R d) {
+    V4<R> v;
+    v.x = a; v.y = b; v.z = c; v.w = d;
+    return v;
+}
+
+// Particle state of a handle (or of a whole batch), device pointers.
+template <typename R> struct PState {
+    V4<R>* A[6];
+    V4<R>* B[4];
+    V4<R>* S[2];
+    V4<R>* K[2];
+    R* sres;
+    uint8_t* status;
+    int32_t* id;
+    int32_t* bin;       // bin (block) index the particle is filed under, written by the re-bin
+    int32_t* orig;      // position of the particle in upload order
+};
+
+// Per-instance constants, built on the host.  Lives in a device array (the
+// tensor maps must be 64-byte aligned in global memory).
+template <typename R> struct alignas(128) Inst {
+    CUtensorMap tmap[2];           // TMA descriptors of grid buffers 0 and 1
+    V4<R>* grid[2];
+    uint8_t* tool_mask;            // raster mode: 1 where a tool sample marked the node
+    int nx, ny, nz;
+    int nbx, nby, nbz;
+    int64_t nn;
+    double dx, ox, oy, oz;
+    double dt, t0;                 // step size and time at the first step of the current call
+    int64_t step0;                 // step counter at the first step of the current call
+    // material (R copies for the hot path)
+    R mu, lam, pmass, pvol;
+    R A, B, n, C, m, edot0, Hkin;
+    R D1, D2, D3, D4c, D5, Dth;
+    R Tspan;                       // max(Tm - Tamb, 1)
+    R dTmax;                       // Tm - Tamb (temperature cap as a rise)
+    R heat;                        // beta / max(rho_phys cp, 1e-12)
+    R apic;                        // apic_dinv_factor, applied as factor/dx
+    R decay, deps_cap, dT_cap;
+    double fix_thick, fix_damp, grav, mthr;
+    int lod, plast;
+    double lod_r1, lod_r2;
+    int chip_every;
+    int newton_maxit;
+    double newton_tol;
+    // tool
+    int tool_mode, tool_shape;
+    double tool_p0[3], tool_v[3], tool_t0;
+    double tool_r, tool_rake, tool_clear, tool_tip_dz;
+    // external force for one step (radius 0: none)
+    double ext_c[3], ext_r, ext_f[3];
+    int64_t pbase;                 // first particle slot of this instance in the batch arrays
+    int64_t np;                    // live particles of this instance, at [pbase, pbase + np)
+    int64_t pcap;                  // particle slots of this instance
+    int fresh;                     // positions still in the upload scratch (not yet binned)
+    int nbins;                     // nbx * nby * nbz
+};
+
+// One unit of work: the particles of one bin of one instance.
+struct Work {
+    int inst;
+    int bin;
+    int start;     // relative to the instance's pbase
+    int count;
+};
+
+struct StepArgs {
+    int k;              // step index within the current call (G2P part: step k; P2G part: step k+1 when fused)
+    int write_out;      // G2P: store v, C, edot (final step of a call, or split schedule)
+    int sigma_all;      // P2G: store stress for every ACTIVE particle (last P2G of a call)
+    int use_ext;        // P2G: apply the one-step external force
+    int p2g_step;       // step index of the P2G part
+};
+
+// ------------------------------------------------------------------ weights
+
+// Quadratic B-spline weights on one axis, restating getWeightsAndGradients
+// (reference src/MPMSolver.cu:20-34) in cell units: base = floor(xi - 0.5),
+// d = xi - base in [0.5, 1.5); dw is d/dxi (divide by dx for a gradient).
+template <typename R> __device__ __forceinline__ int bspline(R xi, R w[3], R dw[3]) {
+    R fb = floor(xi - R(0.5));
+    R d = xi - fb;
+    R a = R(1.5) - d, b = d - R(1), c = d - R(0.5);
+    w[0] = R(0.5) * a * a;
+    w[1] = R(0.75) - b * b;
+    w[2] = R(0.5) * c * c;
+    dw[0] = -a;
+    dw[1] = R(-2) * b;
+    dw[2] = c;
+    return (int)fb;
+}
+
+__device__ __forceinline__ int tidx(int x, int y, int z) { return x + kSY * y + kSZ * z; }
+
+// ------------------------------------------------------------------ tool SDF
+
+// Analytic rigid-tool SDF and outward normal (an extension of this build; the
+// reference boundary is the rasterised tool, src/MPMSolver.cu:444-492).
+// Cylinder with axis along y, or a rounded wedge extruded along y (sharp core
+// wedge with apex at the edge-circle centre, offset by the edge radius).
+template <typename I>
+__device__ inline double tool_sdf(const I& P, double x, double z, double pr0, double pr2, double nrm[3]) {
+    double qx = x - pr0, qz = z - pr2;
+    nrm[1] = 0.0;
+    if (P.tool_shape == 0) {
+        double r = sqrt(qx * qx + qz * qz);
+        if (r > 0.0) { nrm[0] = qx / r; nrm[2] = qz / r; } else { nrm[0] = 0.0; nrm[2] = 1.0; }
+        return r - P.tool_r;
+    }
+    double sg = sin(P.tool_rake), cg = cos(P.tool_rake), sa = sin(P.tool_clear), ca = cos(P.tool_clear);
+    double t1x = -sg, t1z = cg, n1x = cg, n1z = sg;
+    double t2x = -ca, t2z = sa, n2x = -sa, n2z = -ca;
+    double d1 = n1x * qx + n1z * qz, d2 = n2x * qx + n2z * qz, core;
+    if (d1 <= 0.0 && d2 <= 0.0) {
+        if (d1 >= d2) { core = d1; nrm[0] = n1x; nrm[2] = n1z; } else { core = d2; nrm[0] = n2x; nrm[2] = n2z; }
+    } else {
+        double s1 = fmax(qx * t1x + qz * t1z, 0.0), s2 = fmax(qx * t2x + qz * t2z, 0.0);
+        double e1x = qx - s1 * t1x, e1z = qz - s1 * t1z, e2x = qx - s2 * t2x, e2z = qz - s2 * t2z;
+        double l1 = sqrt(e1x * e1x + e1z * e1z), l2 = sqrt(e2x * e2x + e2z * e2z);
+        if (l1 <= l2) {
+            core = l1;
+            if (l1 > 0) { nrm[0] = e1x / l1; nrm[2] = e1z / l1; } else { nrm[0] = n1x; nrm[2] = n1z; }
+        } else {
+            core = l2;
+            if (l2 > 0) { nrm[0] = e2x / l2; nrm[2] = e2z / l2; } else { nrm[0] = n2x; nrm[2] = n2z; }
+        }
+    }
+    return core - P.tool_r;
+}
+
+// ------------------------------------------------------------------ Philox
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), 24-bit uniforms in [0,1).
+__host__ __device__ inline void philox_u4(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1, uint32_t c2,
+                                          uint32_t c3, float out[4]) {
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0, hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+    out[0] = (float)(c0 >> 8) * (1.0f / 16777216.0f);
+    out[1] = (float)(c1 >> 8) * (1.0f / 16777216.0f);
+    out[2] = (float)(c2 >> 8) * (1.0f / 16777216.0f);
+    out[3] = (float)(c3 >> 8) * (1.0f / 16777216.0f);
+}
+
+}  // namespace mpmb

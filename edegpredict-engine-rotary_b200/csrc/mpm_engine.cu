@@ -1,0 +1,900 @@
+// mpm_engine.cu -- host engine: device memory, TMA descriptors, the step
+// schedule, re-binning, upload/download and metrics.  One engine holds one or
+// more workpiece instances (the plain C ABI uses one).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "mpm_engine.h"
+
+namespace mpmb {
+
+namespace {
+
+typedef CUresult (*PFN_encodeTiled_t)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                      const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                      CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+PFN_encodeTiled_t encode_fn() {
+    static PFN_encodeTiled_t fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_encodeTiled_t)p;
+    }
+    return fn;
+}
+
+inline size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+#define CK(call)                                                                                     \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess) {                                                                     \
+            err = std::string(#call) + ": " + cudaGetErrorString(e_);                                \
+            return e_ == cudaErrorMemoryAllocation ? MPM_OOM : MPM_CUDA_ERROR;                       \
+        }                                                                                            \
+    } while (0)
+
+}  // namespace
+
+mpm_status check_params(const mpm_params* p, std::string* err) {
+    auto bad = [&](const char* m) {
+        *err = m;
+        return MPM_INVALID_ARG;
+    };
+    if (!p) return bad("params is NULL");
+    if (p->abi_version != MPM_ABI_VERSION) return bad("params.abi_version does not match MPM_ABI_VERSION");
+    if (p->precision != MPM_PREC_F32 && p->precision != MPM_PREC_F64) return bad("precision must be F32 or F64");
+    if (p->nx < 8 || p->ny < 8 || p->nz < 8) return bad("grid needs at least 8 nodes per axis");
+    if ((int64_t)p->nx * p->ny * p->nz > (int64_t)1 << 31) return bad("grid larger than 2^31 nodes");
+    if (!(p->dx > 0.0) || !std::isfinite(p->dx)) return bad("dx must be positive");
+    if (!(p->particle_mass > 0.0) || !(p->particle_volume > 0.0)) return bad("particle mass and volume must be positive");
+    if (!(p->E > 0.0) || !(p->nu > -1.0 && p->nu < 0.5)) return bad("E > 0 and -1 < nu < 0.5 required");
+    if (!(p->D_th > 0.0)) return bad("D_th must be positive");
+    if (p->plasticity != MPM_PLAST_EXPLICIT && p->plasticity != MPM_PLAST_NEWTON) return bad("plasticity mode");
+    if (p->schedule != MPM_SCHED_FUSED && p->schedule != MPM_SCHED_SPLIT) return bad("schedule");
+    if (p->threads_per_block < 0 || p->threads_per_block > 256 || (p->threads_per_block % 32) != 0)
+        return bad("threads_per_block must be 0 or a multiple of 32 up to 256");
+    return MPM_OK;
+}
+
+template <typename R>
+class Engine final : public EngineBase {
+   public:
+    std::vector<InstHost> I;
+    cudaStream_t st = nullptr;
+    bool own_st = false;
+    int64_t cap_total = 0, nn_total = 0, nkeys = 0;
+    void* pbuf[2] = {nullptr, nullptr};
+    PState<R> ps[2];
+    int cur = 0;
+    bool has_K = false;
+    V4<R>* gpool[2] = {nullptr, nullptr};
+    uint8_t* mask_pool = nullptr;
+    Inst<R>* d_inst = nullptr;
+    std::vector<Inst<R>> h_inst;
+    int32_t *d_key_base = nullptr, *d_key_inst = nullptr, *d_key_bin = nullptr;
+    int64_t* d_inst_pbase = nullptr;
+    int32_t *d_key = nullptr, *d_rank = nullptr, *d_newbin = nullptr, *d_count = nullptr, *d_offset = nullptr;
+    int32_t *d_flag = nullptr, *d_flag_scan = nullptr, *d_scan_tmp = nullptr;
+    double* d_pos = nullptr;
+    Work* d_work = nullptr;
+    int* d_nwork = nullptr;
+    int max_work = 0;
+    int* d_err = nullptr;
+    unsigned long long* d_ctr = nullptr;
+    double *d_stat_part = nullptr, *d_stat_out = nullptr;
+    int stat_blocks = 0;
+    void* d_stage = nullptr;
+    size_t stage_bytes = 0;
+    int32_t* d_gen = nullptr;
+    size_t gen_bytes = 0;
+    bool binned = false;
+    int64_t since_sort = 0, n_sorts = 0;
+    int64_t launch_base = 0;
+    int sort_every = 16, threads = 128;
+    int rbuf = 0;
+
+    ~Engine() override {
+        if (st) cudaStreamSynchronize(st);
+        void* ptrs[] = {pbuf[0], pbuf[1], gpool[0], gpool[1], mask_pool, d_inst, d_key_base, d_key_inst, d_key_bin,
+                        d_inst_pbase, d_key, d_rank, d_newbin, d_count, d_offset, d_flag, d_flag_scan, d_scan_tmp,
+                        d_pos, d_work, d_nwork, d_err, d_ctr, d_stat_part, d_stat_out, d_stage, d_gen};
+        for (void* p : ptrs)
+            if (p) cudaFree(p);
+        for (auto& x : I)
+            if (x.d_samples) cudaFree(x.d_samples);
+        if (own_st && st) cudaStreamDestroy(st);
+    }
+
+    int n_inst() const override { return (int)I.size(); }
+    const InstHost& inst(int i) const override { return I[i]; }
+    cudaStream_t stream() const override { return st; }
+    int64_t launches() const override { return launch_counter() - launch_base; }
+
+    // ---------------------------------------------------------------- setup
+
+    mpm_status init(const mpm_params* params, const int64_t* caps, int n, cudaStream_t stream_in) {
+        launch_base = launch_counter();
+        I.resize(n);
+        for (int i = 0; i < n; ++i) {
+            mpm_status s = check_params(&params[i], &err);
+            if (s != MPM_OK) return s;
+            if (params[i].precision != params[0].precision) {
+                err = "all instances of an engine share one precision";
+                return MPM_INVALID_ARG;
+            }
+            if (caps[i] < 0 || caps[i] > ((int64_t)1 << 31) - 1) {
+                err = "capacity out of range";
+                return MPM_INVALID_ARG;
+            }
+            I[i].p = params[i];
+            I[i].cap = caps[i];
+            I[i].tool = mpm_tool_desc{};
+            I[i].tool.mode = MPM_TOOL_NONE;
+            if (params[i].H_kin > 0.0) has_K = true;
+        }
+        sort_every = params[0].sort_every > 0 ? params[0].sort_every : 16;
+        threads = params[0].threads_per_block > 0 ? params[0].threads_per_block : 128;
+        if (stream_in) {
+            st = stream_in;
+        } else {
+            CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            own_st = true;
+        }
+        // layout of instances
+        int64_t pb = 0, go = 0, kb = 0;
+        std::vector<int32_t> key_base(n), key_inst, key_bin;
+        std::vector<int64_t> inst_pbase(n);
+        for (int i = 0; i < n; ++i) {
+            InstHost& x = I[i];
+            x.pbase = pb;
+            pb += x.cap;
+            x.nn = (int64_t)x.p.nx * x.p.ny * x.p.nz;
+            x.grid_off = go;
+            go += x.nn;
+            x.nbx = (x.p.nx + kBin - 1) / kBin;
+            x.nby = (x.p.ny + kBin - 1) / kBin;
+            x.nbz = (x.p.nz + kBin - 1) / kBin;
+            const int nbins = x.nbx * x.nby * x.nbz;
+            key_base[i] = (int32_t)kb;
+            for (int b = 0; b < nbins + 2; ++b) {
+                key_inst.push_back(i);
+                key_bin.push_back(b < nbins ? b : -1);
+            }
+            kb += nbins + 2;
+            inst_pbase[i] = x.pbase;
+            max_work += nbins;
+        }
+        if (kb > ((int64_t)1 << 31) - 1 || pb > ((int64_t)1 << 31) - 1) {
+            err = "too many bins or particles for one engine";
+            return MPM_CAPACITY;
+        }
+        cap_total = pb;
+        nn_total = go;
+        nkeys = kb;
+        // particle buffers
+        const int64_t cp = std::max<int64_t>(cap_total, 1);
+        const size_t v4 = sizeof(V4<R>);
+        size_t need = 0;
+        need += 6 * al256(v4 * cp) + 4 * al256(v4 * cp) + 2 * al256(v4 * cp) + (has_K ? 2 * al256(v4 * cp) : 0);
+        need += al256(sizeof(R) * cp) + al256(cp) + 3 * al256(4 * cp);
+        for (int b = 0; b < 2; ++b) {
+            CK(cudaMalloc(&pbuf[b], need));
+            char* q = (char*)pbuf[b];
+            auto take = [&](size_t bytes) {
+                void* r = q;
+                q += al256(bytes);
+                return r;
+            };
+            PState<R>& s = ps[b];
+            for (int k = 0; k < 6; ++k) s.A[k] = (V4<R>*)take(v4 * cp);
+            for (int k = 0; k < 4; ++k) s.B[k] = (V4<R>*)take(v4 * cp);
+            for (int k = 0; k < 2; ++k) s.S[k] = (V4<R>*)take(v4 * cp);
+            for (int k = 0; k < 2; ++k) s.K[k] = has_K ? (V4<R>*)take(v4 * cp) : nullptr;
+            s.sres = (R*)take(sizeof(R) * cp);
+            s.status = (uint8_t*)take(cp);
+            s.id = (int32_t*)take(4 * cp);
+            s.bin = (int32_t*)take(4 * cp);
+            s.orig = (int32_t*)take(4 * cp);
+        }
+        // grids, tool masks
+        for (int b = 0; b < 2; ++b) {
+            CK(cudaMalloc(&gpool[b], sizeof(V4<R>) * std::max<int64_t>(nn_total, 1)));
+            CK(cudaMemsetAsync(gpool[b], 0, sizeof(V4<R>) * nn_total, st));
+        }
+        CK(cudaMalloc(&mask_pool, std::max<int64_t>(nn_total, 1)));
+        CK(cudaMemsetAsync(mask_pool, 0, nn_total, st));
+        // sort scratch
+        CK(cudaMalloc(&d_key, 4 * cp));
+        CK(cudaMalloc(&d_rank, 4 * cp));
+        CK(cudaMalloc(&d_newbin, 4 * cp));
+        CK(cudaMalloc(&d_pos, 3 * sizeof(double) * cp));
+        CK(cudaMalloc(&d_count, 4 * (nkeys + 1)));
+        CK(cudaMalloc(&d_offset, 4 * (nkeys + 1)));
+        CK(cudaMalloc(&d_flag, 4 * (nkeys + 1)));
+        CK(cudaMalloc(&d_flag_scan, 4 * (nkeys + 1)));
+        CK(cudaMalloc(&d_scan_tmp, 4 * std::max<int64_t>(scan_tmp_size(nkeys + 1), scan_tmp_size(cp))));
+        CK(cudaMalloc(&d_key_base, 4 * n));
+        CK(cudaMalloc(&d_key_inst, 4 * nkeys));
+        CK(cudaMalloc(&d_key_bin, 4 * nkeys));
+        CK(cudaMalloc(&d_inst_pbase, 8 * n));
+        CK(cudaMemcpyAsync(d_key_base, key_base.data(), 4 * n, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_key_inst, key_inst.data(), 4 * nkeys, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_key_bin, key_bin.data(), 4 * nkeys, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_inst_pbase, inst_pbase.data(), 8 * n, cudaMemcpyHostToDevice, st));
+        CK(cudaMalloc(&d_work, sizeof(Work) * std::max(max_work, 1)));
+        CK(cudaMalloc(&d_nwork, sizeof(int)));
+        CK(cudaMemsetAsync(d_nwork, 0, sizeof(int), st));
+        CK(cudaMalloc(&d_err, sizeof(int)));
+        CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+        CK(cudaMalloc(&d_ctr, 4 * sizeof(unsigned long long)));
+        CK(cudaMemsetAsync(d_ctr, 0, 4 * sizeof(unsigned long long), st));
+        stat_blocks = 592;
+        CK(cudaMalloc(&d_stat_part, sizeof(double) * kStatSlots * stat_blocks));
+        CK(cudaMalloc(&d_stat_out, sizeof(double) * kStatSlots));
+        // instance table with TMA descriptors
+        h_inst.resize(n);
+        CK(cudaMalloc(&d_inst, sizeof(Inst<R>) * n));
+        for (int i = 0; i < n; ++i) {
+            mpm_status s = build_inst(i);
+            if (s != MPM_OK) return s;
+        }
+        CK(cudaMemcpyAsync(d_inst, h_inst.data(), sizeof(Inst<R>) * n, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        return MPM_OK;
+    }
+
+    mpm_status build_inst(int i) {
+        InstHost& x = I[i];
+        const mpm_params& p = x.p;
+        Inst<R>& d = h_inst[i];
+        std::memset((void*)&d, 0, sizeof(d));
+        PFN_encodeTiled_t enc = encode_fn();
+        if (!enc) {
+            err = "cuTensorMapEncodeTiled is not available from the driver";
+            return MPM_CUDA_ERROR;
+        }
+        const size_t es = sizeof(R);
+        for (int b = 0; b < 2; ++b) {
+            d.grid[b] = gpool[b] + x.grid_off;
+            cuuint64_t dims[4] = {4, (cuuint64_t)p.nx, (cuuint64_t)p.ny, (cuuint64_t)p.nz};
+            cuuint64_t strides[3] = {4 * es, 4 * es * (cuuint64_t)p.nx, 4 * es * (cuuint64_t)p.nx * p.ny};
+            cuuint32_t box[4] = {4, (cuuint32_t)kTile, (cuuint32_t)kTile, (cuuint32_t)kTile};
+            cuuint32_t estr[4] = {1, 1, 1, 1};
+            CUresult r = enc(&d.tmap[b], es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
+                             (void*)d.grid[b], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) {
+                err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
+                return MPM_CUDA_ERROR;
+            }
+        }
+        d.tool_mask = mask_pool + x.grid_off;
+        d.nx = p.nx; d.ny = p.ny; d.nz = p.nz;
+        d.nbx = x.nbx; d.nby = x.nby; d.nbz = x.nbz;
+        d.nbins = x.nbx * x.nby * x.nbz;
+        d.nn = x.nn;
+        d.dx = p.dx; d.ox = p.origin[0]; d.oy = p.origin[1]; d.oz = p.origin[2];
+        d.dt = x.dt; d.t0 = x.time; d.step0 = x.step;
+        const double mu = p.E / (2.0 * (1.0 + p.nu));
+        const double lam = p.E * p.nu / ((1.0 + p.nu) * (1.0 - 2.0 * p.nu));
+        d.mu = (R)mu; d.lam = (R)lam;
+        d.pmass = (R)p.particle_mass; d.pvol = (R)p.particle_volume;
+        d.A = (R)p.jc_A; d.B = (R)p.jc_B; d.n = (R)p.jc_n; d.C = (R)p.jc_C; d.m = (R)p.jc_m;
+        d.edot0 = (R)std::max(p.edot0, 1e-12);
+        d.Hkin = (R)p.H_kin;
+        d.D1 = (R)p.D1; d.D2 = (R)p.D2; d.D3 = (R)p.D3; d.D4c = (R)p.D4; d.D5 = (R)p.D5; d.Dth = (R)p.D_th;
+        d.Tspan = (R)std::max(p.Tm - p.Tamb, 1.0);
+        d.dTmax = (R)(p.Tm - p.Tamb);
+        d.heat = (R)(p.beta / std::max(p.rho_phys * p.cp, 1e-12));
+        d.apic = (R)p.apic_dinv_factor;
+        d.decay = (R)p.apic_decay;
+        d.deps_cap = (R)p.deps_cap;
+        d.dT_cap = (R)p.dT_cap;
+        d.fix_thick = p.fixture_thickness; d.fix_damp = p.fixture_damping;
+        d.grav = p.gravity_z; d.mthr = p.mass_threshold;
+        d.lod = p.lod_enabled; d.plast = p.plasticity;
+        d.lod_r1 = p.lod_active_r; d.lod_r2 = p.lod_near_r;
+        d.chip_every = p.chip_every;
+        d.newton_maxit = p.newton_maxit > 0 ? p.newton_maxit : 60;
+        d.newton_tol = p.newton_tol > 0 ? p.newton_tol : 1e-12;
+        const mpm_tool_desc& t = x.tool;
+        d.tool_mode = t.mode; d.tool_shape = t.shape;
+        for (int a = 0; a < 3; ++a) { d.tool_p0[a] = t.position[a]; d.tool_v[a] = t.velocity[a]; }
+        d.tool_t0 = tool_t0_[i];
+        d.tool_r = t.radius; d.tool_rake = t.rake; d.tool_clear = t.clearance; d.tool_tip_dz = t.tip_dz;
+        for (int a = 0; a < 3; ++a) { d.ext_c[a] = x.ext_c[a]; d.ext_f[a] = x.ext_f[a]; }
+        d.ext_r = x.ext_pending ? x.ext_r : 0.0;
+        d.pbase = x.pbase; d.np = x.np; d.pcap = x.cap;
+        d.fresh = fresh_[i];
+        return MPM_OK;
+    }
+    std::vector<double> tool_t0_;
+    std::vector<int> fresh_;
+
+    mpm_status push_insts() {
+        for (int i = 0; i < (int)I.size(); ++i) {
+            mpm_status s = refresh_inst(i);
+            if (s != MPM_OK) return s;
+        }
+        CK(cudaMemcpyAsync(d_inst, h_inst.data(), sizeof(Inst<R>) * I.size(), cudaMemcpyHostToDevice, st));
+        return MPM_OK;
+    }
+    // update the mutable fields without re-encoding the tensor maps
+    mpm_status refresh_inst(int i) {
+        CUtensorMap t0 = h_inst[i].tmap[0], t1 = h_inst[i].tmap[1];
+        mpm_status s = build_inst_noenc(i);
+        h_inst[i].tmap[0] = t0;
+        h_inst[i].tmap[1] = t1;
+        return s;
+    }
+    mpm_status build_inst_noenc(int i) {
+        // same as build_inst but keep descriptors (they only depend on the grid)
+        CUtensorMap keep[2] = {h_inst[i].tmap[0], h_inst[i].tmap[1]};
+        InstHost& x = I[i];
+        const mpm_params& p = x.p;
+        Inst<R>& d = h_inst[i];
+        V4<R>* g0 = d.grid[0];
+        V4<R>* g1 = d.grid[1];
+        std::memset((void*)&d, 0, sizeof(d));
+        d.tmap[0] = keep[0];
+        d.tmap[1] = keep[1];
+        d.grid[0] = g0;
+        d.grid[1] = g1;
+        d.tool_mask = mask_pool + x.grid_off;
+        d.nx = p.nx; d.ny = p.ny; d.nz = p.nz;
+        d.nbx = x.nbx; d.nby = x.nby; d.nbz = x.nbz;
+        d.nbins = x.nbx * x.nby * x.nbz;
+        d.nn = x.nn;
+        d.dx = p.dx; d.ox = p.origin[0]; d.oy = p.origin[1]; d.oz = p.origin[2];
+        d.dt = x.dt; d.t0 = x.time; d.step0 = x.step;
+        const double mu = p.E / (2.0 * (1.0 + p.nu));
+        const double lam = p.E * p.nu / ((1.0 + p.nu) * (1.0 - 2.0 * p.nu));
+        d.mu = (R)mu; d.lam = (R)lam;
+        d.pmass = (R)p.particle_mass; d.pvol = (R)p.particle_volume;
+        d.A = (R)p.jc_A; d.B = (R)p.jc_B; d.n = (R)p.jc_n; d.C = (R)p.jc_C; d.m = (R)p.jc_m;
+        d.edot0 = (R)std::max(p.edot0, 1e-12);
+        d.Hkin = (R)p.H_kin;
+        d.D1 = (R)p.D1; d.D2 = (R)p.D2; d.D3 = (R)p.D3; d.D4c = (R)p.D4; d.D5 = (R)p.D5; d.Dth = (R)p.D_th;
+        d.Tspan = (R)std::max(p.Tm - p.Tamb, 1.0);
+        d.dTmax = (R)(p.Tm - p.Tamb);
+        d.heat = (R)(p.beta / std::max(p.rho_phys * p.cp, 1e-12));
+        d.apic = (R)p.apic_dinv_factor;
+        d.decay = (R)p.apic_decay;
+        d.deps_cap = (R)p.deps_cap;
+        d.dT_cap = (R)p.dT_cap;
+        d.fix_thick = p.fixture_thickness; d.fix_damp = p.fixture_damping;
+        d.grav = p.gravity_z; d.mthr = p.mass_threshold;
+        d.lod = p.lod_enabled; d.plast = p.plasticity;
+        d.lod_r1 = p.lod_active_r; d.lod_r2 = p.lod_near_r;
+        d.chip_every = p.chip_every;
+        d.newton_maxit = p.newton_maxit > 0 ? p.newton_maxit : 60;
+        d.newton_tol = p.newton_tol > 0 ? p.newton_tol : 1e-12;
+        const mpm_tool_desc& t = x.tool;
+        d.tool_mode = t.mode; d.tool_shape = t.shape;
+        for (int a = 0; a < 3; ++a) { d.tool_p0[a] = t.position[a]; d.tool_v[a] = t.velocity[a]; }
+        d.tool_t0 = tool_t0_[i];
+        d.tool_r = t.radius; d.tool_rake = t.rake; d.tool_clear = t.clearance; d.tool_tip_dz = t.tip_dz;
+        for (int a = 0; a < 3; ++a) { d.ext_c[a] = x.ext_c[a]; d.ext_f[a] = x.ext_f[a]; }
+        d.ext_r = x.ext_pending ? x.ext_r : 0.0;
+        d.pbase = x.pbase; d.np = x.np; d.pcap = x.cap;
+        d.fresh = fresh_[i];
+        return MPM_OK;
+    }
+
+    // ---------------------------------------------------------------- binning
+
+    mpm_status rebin() {
+        CK(cudaMemsetAsync(d_count, 0, 4 * (nkeys + 1), st));
+        launch_pad_counts<R>(d_inst, (int)I.size(), d_key_base, d_count, st);
+        launch_bin_count<R>(d_inst, (int)I.size(), ps[cur], d_key_base, true, d_pos, d_key, d_rank, d_count, d_newbin,
+                            cap_total, st);
+        exclusive_scan(d_count, d_offset, nkeys, d_scan_tmp, st);
+        launch_bin_scatter<R>(ps[cur], ps[cur ^ 1], d_inst, (int)I.size(), d_key, d_rank, d_offset, d_newbin, true,
+                              d_pos, has_K, cap_total, st);
+        build_work(d_count, d_offset, d_key_inst, d_key_bin, d_inst_pbase, nkeys, d_flag, d_flag_scan, d_scan_tmp,
+                   d_work, d_nwork, st);
+        cur ^= 1;
+        since_sort = 0;
+        ++n_sorts;
+        binned = true;
+        bool any_fresh = false;
+        for (auto& f : fresh_) { any_fresh |= (f != 0); f = 0; }
+        if (any_fresh) return push_insts();
+        return MPM_OK;
+    }
+
+    mpm_status ensure_binned() {
+        bool any_fresh = false;
+        for (auto f : fresh_) any_fresh |= (f != 0);
+        if (!binned || any_fresh) return rebin();
+        return MPM_OK;
+    }
+
+    // ---------------------------------------------------------------- particles in
+
+    mpm_status init_box(int i, const int32_t c0[3], const int32_t c1[3], int32_t ppc, uint64_t seed, uint32_t instance,
+                        int32_t fixed_layers, double T0, const mpm_tool_desc* tool) override {
+        InstHost& x = I[i];
+        for (int a = 0; a < 3; ++a)
+            if (c1[a] <= c0[a] || c0[a] < 0) {
+                err = "empty or negative cell box";
+                return MPM_INVALID_ARG;
+            }
+        if (ppc <= 0) {
+            err = "ppc must be positive";
+            return MPM_INVALID_ARG;
+        }
+        const int64_t ncand = (int64_t)(c1[0] - c0[0]) * (c1[1] - c0[1]) * (c1[2] - c0[2]) * ppc;
+        if (ncand > x.cap) {
+            err = "box holds more candidates than the instance capacity";
+            return MPM_CAPACITY;
+        }
+        x.time = 0.0;
+        x.step = 0;
+        if (tool) {
+            mpm_status s = set_tool(i, tool);
+            if (s != MPM_OK) return s;
+        }
+        const size_t need = 4 * (size_t)(2 * ncand + 2);
+        if (gen_bytes < need) {
+            if (d_gen) cudaFree(d_gen);
+            d_gen = nullptr;
+            CK(cudaMalloc(&d_gen, need));
+            gen_bytes = need;
+        }
+        int32_t* flag = d_gen;
+        int32_t* idx = d_gen + ncand + 1;
+        int32_t* tmp = nullptr;
+        CK(cudaMalloc(&tmp, 4 * scan_tmp_size(ncand)));
+        Inst<R> P = h_inst[i];
+        const int tool_check = (tool && tool->mode != MPM_TOOL_NONE) ? 1 : 0;
+        launch_gen<R>(P, c0, c1, ppc, seed, instance, fixed_layers, T0 - x.p.Tamb, tool_check, flag, idx, tmp, ps[cur],
+                      x.pbase, d_pos, st);
+        int32_t lastf = 0, lasti = 0;
+        CK(cudaMemcpyAsync(&lastf, flag + ncand - 1, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&lasti, idx + ncand - 1, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        cudaFree(tmp);
+        x.np = (int64_t)lasti + lastf;
+        fresh_[i] = 1;
+        CK(cudaGetLastError());
+        mpm_status s = push_insts();
+        if (s != MPM_OK) return s;
+        return rebin();
+    }
+
+    static size_t fbytes(const void* p, int elem, int64_t n, int per) { return p ? al256((size_t)elem * n * per) : 0; }
+
+    mpm_status upload(int i, const mpm_particles_soa* h, int64_t n) override {
+        InstHost& x = I[i];
+        if (!h || (h->elem != 4 && h->elem != 8)) {
+            err = "particles.elem must be 4 or 8";
+            return MPM_INVALID_ARG;
+        }
+        if (n < 0 || n > x.cap) {
+            err = "particle count exceeds the capacity";
+            return MPM_CAPACITY;
+        }
+        if (n > 0 && (!h->x || !h->y || !h->z)) {
+            err = "positions are required";
+            return MPM_INVALID_ARG;
+        }
+        const int e = h->elem;
+        struct F { const void* src; size_t per; const void** dst; };
+        DevSoA d{};
+        d.elem = e;
+        F fs[] = {{h->x, 1, &d.x}, {h->y, 1, &d.y}, {h->z, 1, &d.z}, {h->vx, 1, &d.vx}, {h->vy, 1, &d.vy},
+                  {h->vz, 1, &d.vz}, {h->F, 9, &d.F}, {h->Fp, 9, &d.Fp}, {h->C, 9, &d.C}, {h->stress, 6, &d.stress},
+                  {h->backstress, 6, &d.bs}, {h->plastic_strain, 1, &d.eps}, {h->strain_rate, 1, &d.edot},
+                  {h->temperature, 1, &d.T}, {h->damage, 1, &d.D}, {h->residual_stress, 1, &d.sres}};
+        size_t need = 0;
+        for (auto& f : fs) need += fbytes(f.src, e, n, (int)f.per);
+        need += (h->status ? al256(4 * n) : 0) + (h->id ? al256(4 * n) : 0);
+        if (stage_bytes < need) {
+            if (d_stage) cudaFree(d_stage);
+            d_stage = nullptr;
+            CK(cudaMalloc(&d_stage, need));
+            stage_bytes = need;
+        }
+        char* q = (char*)d_stage;
+        for (auto& f : fs) {
+            if (!f.src) { *f.dst = nullptr; continue; }
+            const size_t b = (size_t)e * n * f.per;
+            CK(cudaMemcpyAsync(q, f.src, b, cudaMemcpyHostToDevice, st));
+            *f.dst = q;
+            q += al256(b);
+        }
+        d.status = nullptr;
+        d.id = nullptr;
+        if (h->status) {
+            CK(cudaMemcpyAsync(q, h->status, 4 * n, cudaMemcpyHostToDevice, st));
+            d.status = (const int32_t*)q;
+            q += al256(4 * n);
+        }
+        if (h->id) {
+            CK(cudaMemcpyAsync(q, h->id, 4 * n, cudaMemcpyHostToDevice, st));
+            d.id = (const int32_t*)q;
+            q += al256(4 * n);
+        }
+        launch_import<R>(d, n, x.p.origin[0], x.p.origin[1], x.p.origin[2], x.p.dx, x.p.Tamb, ps[cur], x.pbase, d_pos,
+                         st);
+        x.np = n;
+        fresh_[i] = 1;
+        CK(cudaGetLastError());
+        mpm_status s = push_insts();
+        if (s != MPM_OK) return s;
+        return rebin();
+    }
+
+    // ---------------------------------------------------------------- particles out
+
+    mpm_status download(int i, mpm_particles_soa* h) override {
+        InstHost& x = I[i];
+        if (!h || (h->elem != 4 && h->elem != 8)) {
+            err = "particles.elem must be 4 or 8";
+            return MPM_INVALID_ARG;
+        }
+        mpm_status s = ensure_binned();
+        if (s != MPM_OK) return s;
+        const int64_t n = x.np;
+        const int e = h->elem;
+        struct F { void* dst; size_t per; void** dev; };
+        DevSoAOut o{};
+        o.elem = e;
+        F fs[] = {{h->x, 1, &o.x}, {h->y, 1, &o.y}, {h->z, 1, &o.z}, {h->vx, 1, &o.vx}, {h->vy, 1, &o.vy},
+                  {h->vz, 1, &o.vz}, {h->F, 9, &o.F}, {h->Fp, 9, &o.Fp}, {h->C, 9, &o.C}, {h->stress, 6, &o.stress},
+                  {h->backstress, 6, &o.bs}, {h->plastic_strain, 1, &o.eps}, {h->strain_rate, 1, &o.edot},
+                  {h->temperature, 1, &o.T}, {h->damage, 1, &o.D}, {h->residual_stress, 1, &o.sres}};
+        size_t need = 0;
+        for (auto& f : fs) need += fbytes(f.dst, e, n, (int)f.per);
+        need += (h->status ? al256(4 * n) : 0) + (h->id ? al256(4 * n) : 0);
+        if (stage_bytes < need) {
+            CK(cudaStreamSynchronize(st));
+            if (d_stage) cudaFree(d_stage);
+            d_stage = nullptr;
+            CK(cudaMalloc(&d_stage, need));
+            stage_bytes = need;
+        }
+        char* q = (char*)d_stage;
+        for (auto& f : fs) {
+            if (!f.dst) { *f.dev = nullptr; continue; }
+            *f.dev = q;
+            q += al256((size_t)e * n * f.per);
+        }
+        o.status = nullptr;
+        o.id = nullptr;
+        if (h->status) { o.status = (int32_t*)q; q += al256(4 * n); }
+        if (h->id) { o.id = (int32_t*)q; q += al256(4 * n); }
+        launch_export<R>(d_inst + i, ps[cur], x.pbase, n, x.p.Tamb, o, st);
+        for (auto& f : fs)
+            if (f.dst) CK(cudaMemcpyAsync(f.dst, *f.dev, (size_t)e * n * f.per, cudaMemcpyDeviceToHost, st));
+        if (h->status) CK(cudaMemcpyAsync(h->status, o.status, 4 * n, cudaMemcpyDeviceToHost, st));
+        if (h->id) CK(cudaMemcpyAsync(h->id, o.id, 4 * n, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return device_status();
+    }
+
+    mpm_status export_aos(int i, void* dst, int64_t bytes) override {
+        InstHost& x = I[i];
+        if (!dst || bytes < x.np * 504) {
+            err = "destination smaller than np * sizeof(MPMParticle) (504 bytes)";
+            return MPM_INVALID_ARG;
+        }
+        mpm_status s = ensure_binned();
+        if (s != MPM_OK) return s;
+        cudaPointerAttributes at{};
+        const bool dev = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeDevice;
+        cudaGetLastError();
+        void* out = dst;
+        if (!dev) {
+            const size_t need = (size_t)504 * std::max<int64_t>(x.np, 1);
+            if (stage_bytes < need) {
+                CK(cudaStreamSynchronize(st));
+                if (d_stage) cudaFree(d_stage);
+                d_stage = nullptr;
+                CK(cudaMalloc(&d_stage, need));
+                stage_bytes = need;
+            }
+            out = d_stage;
+        }
+        launch_export_aos<R>(d_inst + i, ps[cur], x.pbase, x.np, x.p.Tamb, x.p.rho_phys, out, st);
+        if (!dev) CK(cudaMemcpyAsync(dst, out, (size_t)504 * x.np, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return device_status();
+    }
+
+    // ---------------------------------------------------------------- tool
+
+    mpm_status set_tool(int i, const mpm_tool_desc* t) override {
+        InstHost& x = I[i];
+        if (!t || t->mode < MPM_TOOL_NONE || t->mode > MPM_TOOL_SDF_SLIP || t->shape < 0 || t->shape > 1) {
+            err = "invalid tool descriptor";
+            return MPM_INVALID_ARG;
+        }
+        if (t->mode == MPM_TOOL_RASTER && t->n_samples > 0 && (!t->sample_dx || !t->sample_dy || !t->sample_dz)) {
+            err = "raster tool needs sample offsets";
+            return MPM_INVALID_ARG;
+        }
+        x.tool = *t;
+        x.tool.sample_dx = x.tool.sample_dy = x.tool.sample_dz = nullptr;
+        tool_t0_[i] = x.time;
+        if (t->mode == MPM_TOOL_RASTER) {
+            const int ns = std::max(t->n_samples, 0);
+            if (x.d_samples) {
+                CK(cudaStreamSynchronize(st));
+                cudaFree(x.d_samples);
+                x.d_samples = nullptr;
+            }
+            x.n_samples = ns;
+            if (ns > 0) {
+                CK(cudaMalloc(&x.d_samples, 3 * sizeof(double) * ns));
+                CK(cudaMemcpyAsync(x.d_samples, t->sample_dx, 8 * ns, cudaMemcpyHostToDevice, st));
+                CK(cudaMemcpyAsync(x.d_samples + ns, t->sample_dy, 8 * ns, cudaMemcpyHostToDevice, st));
+                CK(cudaMemcpyAsync(x.d_samples + 2 * ns, t->sample_dz, 8 * ns, cudaMemcpyHostToDevice, st));
+                CK(cudaStreamSynchronize(st));
+            }
+        }
+        return push_insts();
+    }
+
+    // ---------------------------------------------------------------- step
+
+    void raster_all(int k) {
+        for (auto& x : I) {
+            if (x.tool.mode != MPM_TOOL_RASTER || x.n_samples <= 0) continue;
+            const int ii = (int)(&x - &I[0]);
+            const double t = x.time + (double)k * x.dt;
+            const double px = x.tool.position[0] + x.tool.velocity[0] * (t - tool_t0_[ii]);
+            const double py = x.tool.position[1] + x.tool.velocity[1] * (t - tool_t0_[ii]);
+            const double pz = x.tool.position[2] + x.tool.velocity[2] * (t - tool_t0_[ii]);
+            cudaMemsetAsync(mask_pool + x.grid_off, 0, x.nn, st);
+            launch_raster(x.d_samples, x.d_samples + x.n_samples, x.d_samples + 2 * x.n_samples, x.n_samples, px, py,
+                          pz, x.p.origin[0], x.p.origin[1], x.p.origin[2], x.p.dx, x.p.nx, x.p.ny, x.p.nz,
+                          mask_pool + x.grid_off, st);
+        }
+    }
+
+    mpm_status step(int32_t N, const double* dts) override {
+        if (N < 0) {
+            err = "nsteps must be >= 0";
+            return MPM_INVALID_ARG;
+        }
+        if (N == 0) return MPM_OK;
+        for (int i = 0; i < (int)I.size(); ++i) {
+            if (!(dts[i] > 0.0) || !std::isfinite(dts[i])) {
+                err = "dt must be positive";
+                return MPM_INVALID_ARG;
+            }
+            I[i].dt = dts[i];
+        }
+        mpm_status s = ensure_binned();
+        if (s != MPM_OK) return s;
+        s = push_insts();
+        if (s != MPM_OK) return s;
+        const size_t gbytes = sizeof(V4<R>) * nn_total;
+        const bool fused = I[0].p.schedule == MPM_SCHED_FUSED;
+        int w = rbuf;
+        bool ext = false;
+        for (auto& x : I) ext |= x.ext_pending;
+        auto maybe_sort = [&]() -> mpm_status {
+            if (since_sort >= sort_every) return rebin_regular();
+            return MPM_OK;
+        };
+        if (fused) {
+            CK(cudaMemsetAsync(gpool[w], 0, gbytes, st));
+            StepArgs a{0, 0, N == 1 ? 1 : 0, ext ? 1 : 0, 0};
+            launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], a, w, false, true, threads, 0, d_err, d_ctr, st);
+            for (int k = 0; k + 1 < N; ++k) {
+                if ((s = maybe_sort()) != MPM_OK) return s;
+                CK(cudaMemsetAsync(gpool[w ^ 1], 0, gbytes, st));
+                raster_all(k);
+                StepArgs b{k, 0, (k + 2 == N) ? 1 : 0, 0, k + 1};
+                launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], b, w, true, true, threads, 0, d_err, d_ctr,
+                               st);
+                w ^= 1;
+                ++since_sort;
+            }
+            raster_all(N - 1);
+            StepArgs c{N - 1, 1, 0, 0, N - 1};
+            launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], c, w, true, false, threads, 0, d_err, d_ctr, st);
+            ++since_sort;
+        } else {
+            for (int k = 0; k < N; ++k) {
+                if ((s = maybe_sort()) != MPM_OK) return s;
+                CK(cudaMemsetAsync(gpool[w], 0, gbytes, st));
+                StepArgs a{k, 0, 1, (ext && k == 0) ? 1 : 0, k};
+                launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], a, w, false, true, threads, 0, d_err, d_ctr,
+                               st);
+                raster_all(k);
+                StepArgs c{k, 1, 0, 0, k};
+                launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], c, w, true, false, threads, 0, d_err, d_ctr,
+                               st);
+                ++since_sort;
+            }
+        }
+        rbuf = w;
+        for (auto& x : I) {
+            x.time += (double)N * x.dt;
+            x.step += N;
+            x.ext_pending = false;
+        }
+        CK(cudaGetLastError());
+        return MPM_OK;
+    }
+
+    mpm_status rebin_regular() {
+        // positions are bin-local (no instance is fresh here)
+        CK(cudaMemsetAsync(d_count, 0, 4 * (nkeys + 1), st));
+        launch_pad_counts<R>(d_inst, (int)I.size(), d_key_base, d_count, st);
+        launch_bin_count<R>(d_inst, (int)I.size(), ps[cur], d_key_base, false, d_pos, d_key, d_rank, d_count,
+                            d_newbin, cap_total, st);
+        exclusive_scan(d_count, d_offset, nkeys, d_scan_tmp, st);
+        launch_bin_scatter<R>(ps[cur], ps[cur ^ 1], d_inst, (int)I.size(), d_key, d_rank, d_offset, d_newbin, false,
+                              d_pos, has_K, cap_total, st);
+        build_work(d_count, d_offset, d_key_inst, d_key_bin, d_inst_pbase, nkeys, d_flag, d_flag_scan, d_scan_tmp,
+                   d_work, d_nwork, st);
+        cur ^= 1;
+        since_sort = 0;
+        ++n_sorts;
+        return MPM_OK;
+    }
+
+    // ---------------------------------------------------------------- metrics
+
+    mpm_status device_status() {
+        int e = 0;
+        CK(cudaMemcpyAsync(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (e & ERR_TIMEOUT) {
+            err = "a bounded device wait timed out (TMA tile load)";
+            return MPM_TIMEOUT;
+        }
+        if (e & ERR_NEWTON) {
+            err = "a Newton return did not converge";
+            return MPM_NUMERIC;
+        }
+        return MPM_OK;
+    }
+
+    mpm_status metrics(int i, mpm_metrics* out) override {
+        if (!out) {
+            err = "metrics output is NULL";
+            return MPM_INVALID_ARG;
+        }
+        InstHost& x = I[i];
+        mpm_status s = ensure_binned();
+        if (s != MPM_OK) return s;
+        const double mu = x.p.E / (2.0 * (1.0 + x.p.nu));
+        const double K = x.p.E / (3.0 * (1.0 - 2.0 * x.p.nu));
+        launch_stats<R>(d_inst + i, ps[cur], x.pbase, x.np, mu, K, x.p.rho_phys, x.p.cp, x.p.Tamb, d_stat_part,
+                        stat_blocks, d_stat_out, st);
+        double v[kStatSlots];
+        unsigned long long ctr[4];
+        CK(cudaMemcpyAsync(v, d_stat_out, sizeof(v), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(ctr, d_ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        std::memset(out, 0, sizeof(*out));
+        out->mass = v[0];
+        out->momentum[0] = v[1]; out->momentum[1] = v[2]; out->momentum[2] = v[3];
+        out->kinetic = v[4];
+        out->internal_elastic = v[5];
+        out->thermal = v[6];
+        out->max_temperature = x.p.Tamb + (std::isfinite(v[7]) ? v[7] : 0.0);
+        out->max_von_mises = v[8];
+        out->max_plastic_strain = std::isfinite(v[9]) ? v[9] : 0.0;
+        const double nl = v[15] + v[16] + v[17] + (double)0;
+        const double nlive = (double)x.np - v[18];
+        out->mean_plastic_strain = nlive > 0 ? v[10] / nlive : 0.0;
+        (void)nl;
+        out->ref_max_stress = v[11];
+        out->ref_max_temperature = v[12];
+        out->ref_kinetic = v[13];
+        out->ref_internal = v[14];
+        out->n_active = (int64_t)v[15];
+        out->n_chip = (int64_t)v[16];
+        out->n_fixed = (int64_t)v[17];
+        out->n_inactive = (int64_t)v[18];
+        for (int a = 0; a < 3; ++a) {
+            out->bounds_min[a] = v[19 + a];
+            out->bounds_max[a] = v[22 + a];
+        }
+        out->n_escaped = (int64_t)ctr[0];
+        out->n_sorts = n_sorts;
+        return device_status();
+    }
+
+    // ---------------------------------------------------------------- misc
+
+    mpm_status set_mass_scaling(int i, double f) override {
+        InstHost& x = I[i];
+        if (!(f > 0.0)) {
+            err = "mass scaling factor must be positive";
+            return MPM_INVALID_ARG;
+        }
+        const double rho = std::max(x.p.rho_phys * f, x.p.rho_phys);
+        x.p.particle_mass = rho * x.p.particle_volume;
+        return push_insts();
+    }
+    mpm_status ext_force(int i, const double c[3], double r, const double f[3]) override {
+        InstHost& x = I[i];
+        if (!c || !f || !(r > 0.0)) {
+            err = "external force needs a center, a positive radius and a force";
+            return MPM_INVALID_ARG;
+        }
+        for (int a = 0; a < 3; ++a) { x.ext_c[a] = c[a]; x.ext_f[a] = f[a]; }
+        x.ext_r = r;
+        x.ext_pending = true;
+        return MPM_OK;
+    }
+    mpm_status set_temps(int i, const double* T, int64_t count) override {
+        InstHost& x = I[i];
+        if (!T || count < 0 || count > x.np) {
+            err = "temperature count out of range";
+            return MPM_INVALID_ARG;
+        }
+        mpm_status s = ensure_binned();
+        if (s != MPM_OK) return s;
+        double* d = nullptr;
+        CK(cudaMalloc(&d, 8 * std::max<int64_t>(count, 1)));
+        CK(cudaMemcpyAsync(d, T, 8 * count, cudaMemcpyHostToDevice, st));
+        launch_set_temps<R>(ps[cur], x.pbase, x.np, d, count, x.p.Tamb, st);
+        CK(cudaStreamSynchronize(st));
+        cudaFree(d);
+        return MPM_OK;
+    }
+    mpm_status reset_clock(int i) override {
+        I[i].time = 0.0;
+        I[i].step = 0;
+        tool_t0_[i] = 0.0;
+        return push_insts();
+    }
+    mpm_status sync() override {
+        CK(cudaStreamSynchronize(st));
+        return device_status();
+    }
+};
+
+std::unique_ptr<EngineBase> make_engine(const mpm_params* params, const int64_t* caps, int n, cudaStream_t st,
+                                        mpm_status* status, std::string* err) {
+    if (!params || !caps || n <= 0) {
+        *status = MPM_INVALID_ARG;
+        *err = "no instances";
+        return nullptr;
+    }
+    if (params[0].precision == MPM_PREC_F64) {
+        auto e = std::make_unique<Engine<double>>();
+        e->tool_t0_.assign(n, 0.0);
+        e->fresh_.assign(n, 0);
+        *status = e->init(params, caps, n, st);
+        if (*status != MPM_OK) {
+            *err = e->err;
+            return nullptr;
+        }
+        return e;
+    }
+    auto e = std::make_unique<Engine<float>>();
+    e->tool_t0_.assign(n, 0.0);
+    e->fresh_.assign(n, 0);
+    *status = e->init(params, caps, n, st);
+    if (*status != MPM_OK) {
+        *err = e->err;
+        return nullptr;
+    }
+    return e;
+}
+
+}  // namespace mpmb

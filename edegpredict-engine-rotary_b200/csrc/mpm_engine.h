@@ -1,0 +1,70 @@
+// mpm_engine.h -- host engine behind the C ABI: owns the device state of one
+// or more workpiece instances and drives the step kernel.  Not a public
+// header; the ABI is include/mpm_capi.h.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/mpm_capi.h"
+#include "mpm_device.cuh"
+#include "mpm_internal.h"
+
+namespace mpmb {
+
+struct InstHost {
+    mpm_params p;
+    mpm_tool_desc tool;
+    std::vector<double> samples;  // raster samples: x..., y..., z...
+    int64_t cap = 0, np = 0, pbase = 0;
+    int64_t nn = 0, grid_off = 0;  // grid nodes and offset (in nodes) in the grid pools
+    int nbx = 0, nby = 0, nbz = 0;
+    double time = 0.0, dt = 0.0;
+    int64_t step = 0;
+    double* d_samples = nullptr;
+    int n_samples = 0;
+    double ext_c[3] = {0, 0, 0}, ext_r = 0.0, ext_f[3] = {0, 0, 0};
+    bool ext_pending = false;
+};
+
+class EngineBase {
+   public:
+    virtual ~EngineBase() = default;
+    std::string err;
+    virtual mpm_status init_box(int inst, const int32_t c0[3], const int32_t c1[3], int32_t ppc, uint64_t seed,
+                                uint32_t instance, int32_t fixed_layers, double T0, const mpm_tool_desc* tool) = 0;
+    virtual mpm_status upload(int inst, const mpm_particles_soa* host, int64_t n) = 0;
+    virtual mpm_status download(int inst, mpm_particles_soa* host) = 0;
+    virtual mpm_status export_aos(int inst, void* dst, int64_t bytes) = 0;
+    virtual mpm_status set_tool(int inst, const mpm_tool_desc* t) = 0;
+    virtual mpm_status step(int32_t nsteps, const double* dt_per_inst) = 0;
+    virtual mpm_status metrics(int inst, mpm_metrics* out) = 0;
+    virtual mpm_status set_mass_scaling(int inst, double f) = 0;
+    virtual mpm_status ext_force(int inst, const double c[3], double r, const double f[3]) = 0;
+    virtual mpm_status set_temps(int inst, const double* T, int64_t count) = 0;
+    virtual mpm_status reset_clock(int inst) = 0;
+    virtual mpm_status sync() = 0;
+    virtual int n_inst() const = 0;
+    virtual const InstHost& inst(int i) const = 0;
+    virtual cudaStream_t stream() const = 0;
+    virtual int64_t launches() const = 0;
+};
+
+// Creates an engine for n instances (all of the same precision).  Returns
+// nullptr with a message in `err` on failure.
+std::unique_ptr<EngineBase> make_engine(const mpm_params* params, const int64_t* caps, int n, cudaStream_t st,
+                                        mpm_status* status, std::string* err);
+
+mpm_status check_params(const mpm_params* p, std::string* err);
+
+}  // namespace mpmb
+
+// The opaque C handle.
+struct mpm_handle {
+    std::unique_ptr<mpmb::EngineBase> eng;
+};

@@ -1,0 +1,88 @@
+// mpm_internal.h -- launchers shared by the C ABI (mpm_capi.cu) and the
+// kernels (mpm_step.cu, mpm_aux.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mpm_device.cuh"
+
+namespace mpmb {
+
+// Device copies of an upload (NULL field = MPMParticle default).
+struct DevSoA {
+    int elem;  // 4 or 8
+    const void *x, *y, *z, *vx, *vy, *vz, *F, *Fp, *C, *stress, *bs, *eps, *edot, *T, *D, *sres;
+    const int32_t *status, *id;
+};
+
+struct DevSoAOut {
+    int elem;
+    void *x, *y, *z, *vx, *vy, *vz, *F, *Fp, *C, *stress, *bs, *eps, *edot, *T, *D, *sres;
+    int32_t *status, *id;
+};
+
+// Number of stats accumulators (see k_stats).
+constexpr int kStatSlots = 32;
+
+template <typename R>
+void launch_step(const Inst<R>* insts, const Work* work, const int* n_work, int max_work, const PState<R>& ps,
+                 const StepArgs& a, int rbuf, bool g2p, bool p2g, int threads, int ctas_per_sm, int* err,
+                 unsigned long long* counters, cudaStream_t st);
+
+template <typename R>
+void launch_bin_count(const Inst<R>* insts, int n_inst, const PState<R>& ps, const int32_t* key_base, bool initial,
+                      const double* pos_scratch, int32_t* key, int32_t* rank, int32_t* count, int32_t* newbin,
+                      int64_t np, cudaStream_t st);
+
+template <typename R>
+void launch_bin_scatter(const PState<R>& src, const PState<R>& dst, const Inst<R>* insts, int n_inst,
+                        const int32_t* key, const int32_t* rank, const int32_t* offset, const int32_t* newbin,
+                        bool initial, const double* pos_scratch, bool has_K, int64_t np, cudaStream_t st);
+
+template <typename R>
+void launch_pad_counts(const Inst<R>* insts, int n_inst, const int32_t* key_base, int32_t* count, cudaStream_t st);
+
+void launch_raster(const double* sx, const double* sy, const double* sz, int ns, double px, double py, double pz,
+                   double ox, double oy, double oz, double dx, int nx, int ny, int nz, uint8_t* mask, cudaStream_t st);
+
+template <typename R>
+void launch_import(const DevSoA& in, int64_t n, double ox, double oy, double oz, double dx, double Tamb,
+                   const PState<R>& ps, int64_t pbase, double* pos_scratch, cudaStream_t st);
+
+// Seeded box generator: writes the kept candidates at [pbase, pbase + kept).
+// flag/idx hold ncand int32 each; scan_tmp >= scan_tmp_size(ncand).
+template <typename R>
+void launch_gen(const Inst<R>& P, const int32_t c0[3], const int32_t c1[3], int ppc, uint64_t seed, uint32_t inst,
+                int fixed_layers, double dT0, int tool_check, int32_t* flag, int32_t* idx, int32_t* scan_tmp,
+                const PState<R>& ps, int64_t pbase, double* pos_scratch, cudaStream_t st);
+
+template <typename R>
+void launch_export(const Inst<R>* inst_dev, const PState<R>& ps, int64_t pbase, int64_t n, double Tamb,
+                   const DevSoAOut& out, cudaStream_t st);
+
+template <typename R>
+void launch_export_aos(const Inst<R>* inst_dev, const PState<R>& ps, int64_t pbase, int64_t n, double Tamb,
+                       double rho, void* out, cudaStream_t st);
+
+template <typename R>
+void launch_stats(const Inst<R>* inst_dev, const PState<R>& ps, int64_t pbase, int64_t n, double mu, double K,
+                  double rho, double cp, double Tamb, double* partial, int nblocks, double* out, cudaStream_t st);
+
+template <typename R>
+void launch_set_temps(const PState<R>& ps, int64_t pbase, int64_t n, const double* T, int64_t count, double Tamb,
+                      cudaStream_t st);
+
+// Device-wide exclusive scan of n int32 (in -> out), tmp >= scan_tmp_size(n).
+int64_t scan_tmp_size(int64_t n);
+void exclusive_scan(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t st);
+// Ordered work list (one item per non-empty bin) from per-key counts/offsets.
+void build_work(const int32_t* count, const int32_t* offset, const int32_t* key_inst, const int32_t* key_bin,
+                const int64_t* inst_pbase, int64_t nkeys, int32_t* flag, int32_t* flag_scan, int32_t* tmp,
+                Work* work, int* n_work, cudaStream_t st);
+void fill_i32(int32_t* p, int32_t v, int64_t n, cudaStream_t st);
+
+// Kernel launches issued by this process (all handles).
+int64_t& launch_counter();
+
+}  // namespace mpmb

@@ -1,0 +1,875 @@
+// mpm_step.cu -- the MPM step kernel for sm_100a.
+//
+// One CTA takes one bin (4^3 stencil-base cells = the particles whose 3^3
+// quadratic stencils start inside the bin) at a time:
+//   G2P part  : the bin's 6^3 node tile of the previous grid is fetched by TMA
+//               into shared memory; the grid update (gravity, fixture damping,
+//               tool boundary) is applied per node while it is staged; each
+//               particle gathers v, the APIC moments and the velocity gradient
+//               through separable tensor-product contractions, then moves and
+//               updates C, F - I and the strain rate (restates g2pKernel,
+//               reference src/MPMSolver.cu:506-605, and chip separation :1002-1060).
+//   P2G part  : the Johnson-Cook return (p2gKernel :123-365) and the APIC
+//               scatter of mass and momentum+force impulse into a shared-memory
+//               tile (:370-421), pre-reduced there by shared atomics; the tile
+//               is then flushed into the next grid with one 128-bit vector
+//               atomic per node.
+// FUSED schedule: launch k runs G2P of step k and P2G of step k+1 on the same
+// particle without a round trip through memory (velocity, C and strain rate
+// stay in registers), so a step costs one pass over the particles.  SPLIT
+// schedule: separate P2G and G2P launches per step, like the reference.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "mpm_device.cuh"
+#include "mpm_internal.h"
+
+namespace mpmb {
+
+// ------------------------------------------------------------------ PTX helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tmap_acquire(const CUtensorMap* map) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+}
+// 4-D tiled TMA load (no multicast): coordinates innermost first.
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2,
+                                            int c3) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], "
+        "[%2];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t gtimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Wait for the mbarrier phase with a time limit (ns); false on timeout.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+    const uint64_t t0 = gtimer();
+    while (!mbar_try_wait(bar, parity)) {
+        if (gtimer() - t0 > limit_ns) return false;
+    }
+    return true;
+}
+
+template <typename R> __device__ __forceinline__ void vec_atomic_add(V4<R>* dst, R a, R b, R c, R d);
+template <> __device__ __forceinline__ void vec_atomic_add<float>(float4* dst, float a, float b, float c, float d) {
+    atomicAdd(dst, make_float4(a, b, c, d));  // one 128-bit vector reduction (sm_90+)
+}
+template <> __device__ __forceinline__ void vec_atomic_add<double>(D4* dst, double a, double b, double c, double d) {
+    atomicAdd(&dst->x, a);
+    atomicAdd(&dst->y, b);
+    atomicAdd(&dst->z, c);
+    atomicAdd(&dst->w, d);
+}
+
+// ------------------------------------------------------------------ grid node update
+
+// Grid update of one node, restating updateGridKernel (src/MPMSolver.cu:424-442),
+// applyFixtureBCKernel (:82-110) and the tool boundary: rasterizeToolKernel +
+// applyGridCollisionKernel (:444-492) in raster mode, or the analytic SDF.
+// Nodes at or below the mass threshold have zero velocity and contribute
+// nothing to the gather, as g2pKernel skips them (:543).
+template <typename R>
+__device__ __forceinline__ void node_vel(const Inst<R>& P, const V4<R>& g, int gx, int gy, int gz, double pr0,
+                                         double pr2, R out[3]) {
+    const R m = g.x;
+    out[0] = out[1] = out[2] = R(0);
+    if (!(m > (R)P.mthr)) return;
+    R vx = g.y / m, vy = g.z / m, vz = (g.w + m * (R)(P.grav * P.dt)) / m;
+    if (P.fix_thick > 0.0) {
+        const double zr = (((double)gz * P.dx + P.oz) - P.oz) / P.fix_thick;
+        if (zr <= 1.0) {
+            if (gz == 0) {
+                vx = vy = vz = R(0);
+            } else if (zr > 0.0) {
+                const double s = P.fix_damp * (1.0 - zr) * (1.0 - zr);
+                const R f = (R)(1.0 / (1.0 + s * P.dt));
+                vx *= f; vy *= f; vz *= f;
+            }
+        }
+    }
+    if (P.tool_mode == TOOL_RASTER) {
+        if (P.tool_mask[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)]) {
+            vx = (R)P.tool_v[0]; vy = (R)P.tool_v[1]; vz = (R)P.tool_v[2];
+        }
+    } else if (P.tool_mode == TOOL_SDF_STICKY || P.tool_mode == TOOL_SDF_SLIP) {
+        double nrm[3];
+        const double phi = tool_sdf(P, (double)gx * P.dx + P.ox, (double)gz * P.dx + P.oz, pr0, pr2, nrm);
+        if (phi <= 0.0) {
+            if (P.tool_mode == TOOL_SDF_STICKY) {
+                vx = (R)P.tool_v[0]; vy = (R)P.tool_v[1]; vz = (R)P.tool_v[2];
+            } else {
+                const double rx = (double)vx - P.tool_v[0], ry = (double)vy - P.tool_v[1], rz = (double)vz - P.tool_v[2];
+                const double vn = rx * nrm[0] + ry * nrm[1] + rz * nrm[2];
+                if (vn < 0.0) {
+                    vx = (R)((double)vx - vn * nrm[0]);
+                    vy = (R)((double)vy - vn * nrm[1]);
+                    vz = (R)((double)vz - vn * nrm[2]);
+                }
+            }
+        }
+    }
+    out[0] = vx; out[1] = vy; out[2] = vz;
+}
+
+// ------------------------------------------------------------------ gather (G2P)
+
+// Separable contraction over the 3x3x3 stencil from the velocity tile:
+//   v_a   = sum w v_a,  M_ab = sum w v_a o_b  (o = stencil offset 0,1,2),
+//   L_ab  = sum v_a dw_b  (cell units).
+// k (z) first: Z0 = sum wz v, Z1 = sum k wz v, Z2 = sum dwz v; then j; then i.
+template <typename R>
+__device__ __forceinline__ void gather_tile(const R (*vel)[kPlane], int base, const R (&w)[3][3], const R (&dw)[3][3],
+                                            R v[3], R M[3][3], R L[3][3]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        v[c] = R(0);
+#pragma unroll
+        for (int b = 0; b < 3; ++b) { M[c][b] = R(0); L[c][b] = R(0); }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        R Y00[3] = {0, 0, 0}, Y01[3] = {0, 0, 0}, Y02[3] = {0, 0, 0}, Y10[3] = {0, 0, 0}, Y20[3] = {0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            R Z0[3] = {0, 0, 0}, Z1[3] = {0, 0, 0}, Z2[3] = {0, 0, 0};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int idx = base + i + kSY * j + kSZ * k;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const R vv = vel[c][idx];
+                    Z0[c] = fma(w[2][k], vv, Z0[c]);
+                    if (k == 1) Z1[c] = fma(w[2][1], vv, Z1[c]);
+                    if (k == 2) Z1[c] = fma(R(2) * w[2][2], vv, Z1[c]);
+                    Z2[c] = fma(dw[2][k], vv, Z2[c]);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                Y00[c] = fma(w[1][j], Z0[c], Y00[c]);
+                if (j) Y01[c] = fma(R(j) * w[1][j], Z0[c], Y01[c]);
+                Y02[c] = fma(dw[1][j], Z0[c], Y02[c]);
+                Y10[c] = fma(w[1][j], Z1[c], Y10[c]);
+                Y20[c] = fma(w[1][j], Z2[c], Y20[c]);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            v[c] = fma(w[0][i], Y00[c], v[c]);
+            if (i) M[c][0] = fma(R(i) * w[0][i], Y00[c], M[c][0]);
+            L[c][0] = fma(dw[0][i], Y00[c], L[c][0]);
+            M[c][1] = fma(w[0][i], Y01[c], M[c][1]);
+            L[c][1] = fma(w[0][i], Y02[c], L[c][1]);
+            M[c][2] = fma(w[0][i], Y10[c], M[c][2]);
+            L[c][2] = fma(w[0][i], Y20[c], L[c][2]);
+        }
+    }
+}
+
+// Same sums for a particle whose stencil left its bin's tile: nodes are read
+// and updated straight from the grid (rare; the re-bin brings it back).
+template <typename R>
+__device__ __noinline__ void gather_global(const Inst<R>& P, const V4<R>* __restrict__ grid, const int gb[3],
+                                           const R (&w)[3][3], const R (&dw)[3][3], double pr0, double pr2, R v[3],
+                                           R M[3][3], R L[3][3]) {
+    for (int c = 0; c < 3; ++c) {
+        v[c] = R(0);
+        for (int b = 0; b < 3; ++b) { M[c][b] = R(0); L[c][b] = R(0); }
+    }
+    for (int i = 0; i < 3; ++i) {
+        const int gx = gb[0] + i;
+        if (gx < 0 || gx >= P.nx) continue;
+        for (int j = 0; j < 3; ++j) {
+            const int gy = gb[1] + j;
+            if (gy < 0 || gy >= P.ny) continue;
+            for (int k = 0; k < 3; ++k) {
+                const int gz = gb[2] + k;
+                if (gz < 0 || gz >= P.nz) continue;
+                R nv[3];
+                node_vel(P, grid[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], gx, gy, gz, pr0, pr2, nv);
+                const R ww = w[0][i] * w[1][j] * w[2][k];
+                const R g0 = dw[0][i] * w[1][j] * w[2][k], g1 = w[0][i] * dw[1][j] * w[2][k],
+                        g2 = w[0][i] * w[1][j] * dw[2][k];
+                for (int c = 0; c < 3; ++c) {
+                    v[c] += ww * nv[c];
+                    M[c][0] += ww * nv[c] * R(i);
+                    M[c][1] += ww * nv[c] * R(j);
+                    M[c][2] += ww * nv[c] * R(k);
+                    L[c][0] += nv[c] * g0;
+                    L[c][1] += nv[c] * g1;
+                    L[c][2] += nv[c] * g2;
+                }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ scatter (P2G)
+
+// Momentum + impulse at node (i,j,k):
+//   p_a = w_ijk (Q_a + R_ax i + R_ay j + R_az k) + S_ax dwx wy wz + S_ay wx dwy wz + S_az wx wy dwz
+// with Q = m (v - dx C d), R = m dx C, S = -dt V J sigma / dx.  Separable in k.
+template <typename R>
+__device__ __forceinline__ void scatter_tile(R (*acc)[kPlane], int base, const R (&w)[3][3], const R (&dw)[3][3], R m,
+                                             const R (&Q)[3], const R (&Rm)[3][3], const R (&S)[3][3], bool mass_only) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const R wij = w[0][i] * w[1][j];
+            const R gx = dw[0][i] * w[1][j], gy = w[0][i] * dw[1][j];
+            const R mij = wij * m;
+            R U[3], Up[3], Zs[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                U[a] = wij * (Q[a] + Rm[a][0] * R(i) + Rm[a][1] * R(j)) + S[a][0] * gx + S[a][1] * gy;
+                Up[a] = wij * Rm[a][2];
+                Zs[a] = wij * S[a][2];
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int idx = base + i + kSY * j + kSZ * k;
+                atomicAdd(&acc[0][idx], mij * w[2][k]);
+                if (!mass_only) {
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) atomicAdd(&acc[1 + a][idx], fma(w[2][k], fma(R(k), Up[a], U[a]), dw[2][k] * Zs[a]));
+                }
+            }
+        }
+    }
+}
+
+template <typename R>
+__device__ __noinline__ void scatter_global(const Inst<R>& P, V4<R>* __restrict__ grid, const int gb[3],
+                                            const R (&w)[3][3], const R (&dw)[3][3], R m, const R (&Q)[3],
+                                            const R (&Rm)[3][3], const R (&S)[3][3], bool mass_only) {
+    for (int i = 0; i < 3; ++i) {
+        const int gx = gb[0] + i;
+        if (gx < 0 || gx >= P.nx) continue;
+        for (int j = 0; j < 3; ++j) {
+            const int gy = gb[1] + j;
+            if (gy < 0 || gy >= P.ny) continue;
+            for (int k = 0; k < 3; ++k) {
+                const int gz = gb[2] + k;
+                if (gz < 0 || gz >= P.nz) continue;
+                const R ww = w[0][i] * w[1][j] * w[2][k];
+                const R g0 = dw[0][i] * w[1][j] * w[2][k], g1 = w[0][i] * dw[1][j] * w[2][k],
+                        g2 = w[0][i] * w[1][j] * dw[2][k];
+                R p[3] = {0, 0, 0};
+                if (!mass_only)
+                    for (int a = 0; a < 3; ++a)
+                        p[a] = ww * (Q[a] + Rm[a][0] * R(i) + Rm[a][1] * R(j) + Rm[a][2] * R(k)) + S[a][0] * g0 +
+                               S[a][1] * g1 + S[a][2] * g2;
+                vec_atomic_add<R>(&grid[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], ww * m, p[0], p[1], p[2]);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ Johnson-Cook
+
+// Consistent return (extension of this build), FP64: q - 3 mu dg = Y(eps + dg)
+// on [0, q/3mu], Newton steps safeguarded by bisection; rate and temperature
+// terms frozen at the step start.  Returns false when it did not converge.
+__device__ __noinline__ bool newton_return(double q, double mu, double eps0, double A, double B, double n, double rt,
+                                           double tt, double tol_rel, int maxit, double* out) {
+    double lo = 0.0, hi = q / (3.0 * mu);
+    double x = (q - (A + B * pow(eps0, n)) * rt * tt) / (3.0 * mu);
+    if (!(x > lo)) x = 0.5 * (lo + hi);
+    if (x > hi) x = hi;
+    const double tol = tol_rel * q;
+    for (int it = 0; it < maxit; ++it) {
+        const double e = eps0 + x;
+        const double fx = q - 3.0 * mu * x - (A + B * pow(e, n)) * rt * tt;
+        if (fabs(fx) <= tol) { *out = x; return true; }
+        if (fx > 0.0) lo = x; else hi = x;
+        const double dY = (e > 0.0) ? B * n * pow(e, n - 1.0) * rt * tt : (double)INFINITY;
+        const double d = -3.0 * mu - dY;
+        double xn = x - fx / d;
+        if (!(xn > lo && xn < hi)) xn = 0.5 * (lo + hi);
+        if (hi - lo <= 1e-15 * hi) { *out = xn; return true; }
+        x = xn;
+    }
+    *out = x;
+    return false;
+}
+
+// det(I + X) - 1 without cancellation.
+template <typename R> __device__ __forceinline__ R detm1(const R X[9]) {
+    const R tr = X[0] + X[4] + X[8];
+    const R i2 = X[0] * X[4] - X[1] * X[3] + X[0] * X[8] - X[2] * X[6] + X[4] * X[8] - X[5] * X[7];
+    const R i3 = X[0] * (X[4] * X[8] - X[5] * X[7]) - X[1] * (X[3] * X[8] - X[5] * X[6]) +
+                 X[2] * (X[3] * X[7] - X[4] * X[6]);
+    return tr + i2 + i3;
+}
+
+struct JCOut {
+    bool ran, yielded, to_chip;
+};
+
+// Elastic stress and Johnson-Cook return of one ACTIVE particle, restating
+// p2gKernel (src/MPMSolver.cu:164-365) on F - I and F_p - I:
+//   F_e - I = (H - Hp)(I + Hp)^-1,  J - 1 = det(I + E) - 1 (clamped to +-0.1),
+//   B - I = E + E^T + E E^T,  sigma = mu/J (B - I) + lambda (J - 1) I.
+// The return rescales only the diagonal and upper off-diagonal entries of the
+// deviator (:239-248); the lower entries yx, zx, zy keep their trial values and
+// enter the force (:406-408) and the F_p update (:282-294).  sl[3] carries them.
+template <typename R>
+__device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[9], R& eps, R& dT, R& D, R edot,
+                                           R sig[6], R sl[3], R& J, R* sres_p, R* bsx, int& errf) {
+    JCOut o{true, false, false};
+    // inverse of G = I + Hp (identity when |det G| < 1e-12, inv3x3 :50-57)
+    R E[9];
+    {
+        const R dgm1 = detm1(Hp);
+        const R det = R(1) + dgm1;
+        R Gi[9];
+        if (fabs(det) < R(1e-12)) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) Gi[q] = (q % 4 == 0) ? R(1) : R(0);
+        } else {
+            const R g0 = R(1) + Hp[0], g4 = R(1) + Hp[4], g8 = R(1) + Hp[8];
+            const R id = R(1) / det;
+            Gi[0] = (g4 * g8 - Hp[5] * Hp[7]) * id;
+            Gi[1] = -(Hp[1] * g8 - Hp[2] * Hp[7]) * id;
+            Gi[2] = (Hp[1] * Hp[5] - Hp[2] * g4) * id;
+            Gi[3] = -(Hp[3] * g8 - Hp[5] * Hp[6]) * id;
+            Gi[4] = (g0 * g8 - Hp[2] * Hp[6]) * id;
+            Gi[5] = -(g0 * Hp[5] - Hp[2] * Hp[3]) * id;
+            Gi[6] = (Hp[3] * Hp[7] - g4 * Hp[6]) * id;
+            Gi[7] = -(g0 * Hp[7] - Hp[1] * Hp[6]) * id;
+            Gi[8] = (g0 * g4 - Hp[1] * Hp[3]) * id;
+        }
+        // F_e - I = (I + H) G^-1 - I = (H - Hp) G^-1 when G^-1 is exact; with the
+        // identity fallback F_e = F, so F_e - I = H.
+        if (fabs(det) < R(1e-12)) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) E[q] = H[q];
+        } else {
+            R Dm[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) Dm[q] = H[q] - Hp[q];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    E[r * 3 + c] = Dm[r * 3] * Gi[c] + Dm[r * 3 + 1] * Gi[3 + c] + Dm[r * 3 + 2] * Gi[6 + c];
+        }
+    }
+    R jm1 = detm1(E);
+    jm1 = fmin(fmax(jm1, R(-0.1)), R(0.1));  // J clamp [0.9, 1.1], :174-175
+    J = R(1) + jm1;
+    // B - I (symmetric)
+    R b00 = R(2) * E[0] + E[0] * E[0] + E[1] * E[1] + E[2] * E[2];
+    R b11 = R(2) * E[4] + E[3] * E[3] + E[4] * E[4] + E[5] * E[5];
+    R b22 = R(2) * E[8] + E[6] * E[6] + E[7] * E[7] + E[8] * E[8];
+    R b01 = E[1] + E[3] + E[0] * E[3] + E[1] * E[4] + E[2] * E[5];
+    R b02 = E[2] + E[6] + E[0] * E[6] + E[1] * E[7] + E[2] * E[8];
+    R b12 = E[5] + E[7] + E[3] * E[6] + E[4] * E[7] + E[5] * E[8];
+    const R muJ = P.mu / J, lj = P.lam * jm1;
+    R s[6] = {muJ * b00 + lj, muJ * b11 + lj, muJ * b22 + lj, muJ * b01, muJ * b02, muJ * b12};
+    // Johnson-Cook return, :205-360
+    const R tr = s[0] + s[1] + s[2];
+    const R p3 = tr / R(3);
+    R sd[6] = {s[0] - p3, s[1] - p3, s[2] - p3, s[3], s[4], s[5]};
+    R bs[6] = {0, 0, 0, 0, 0, 0};
+    if (bsx) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) bs[q] = bsx[q];
+    }
+    const R ex = sd[0] - bs[0], ey = sd[1] - bs[1], ez = sd[2] - bs[2], exy = sd[3] - bs[3], exz = sd[4] - bs[4],
+            eyz = sd[5] - bs[5];
+    const R q = sqrt(R(1.5) * (ex * ex + ey * ey + ez * ez + R(2) * (exy * exy + exz * exz + eyz * eyz)));
+    R Ts = dT / P.Tspan;
+    Ts = fmin(fmax(Ts, R(0)), R(1));
+    const R es = fmax(edot / P.edot0, R(1e-5));
+    const R rt = R(1) + P.C * log(es);
+    const R tt = R(1) - pow(Ts, P.m);
+    const R Y = (P.A + P.B * pow(eps, P.n)) * rt * tt;
+#pragma unroll
+    for (int q2 = 0; q2 < 6; ++q2) sig[q2] = s[q2];
+    sl[0] = s[3]; sl[1] = s[4]; sl[2] = s[5];
+    if (q > Y && q > R(1e-12)) {
+        R dE, Yr = Y;
+        if (P.plast == 1) {
+            double dg;
+            if (!newton_return((double)q, (double)P.mu, (double)eps, (double)P.A, (double)P.B, (double)P.n, (double)rt,
+                               (double)tt, P.newton_tol, P.newton_maxit, &dg))
+                errf |= ERR_NEWTON;
+            dE = (R)dg;
+            Yr = (R)((double)q - 3.0 * (double)P.mu * dg);
+        } else {
+            dE = (q - Y) / fmax(R(3) * P.mu, R(1e-12));
+            if (dE > P.deps_cap) dE = P.deps_cap;
+        }
+        const R sc = Yr / q;
+        sd[0] = bs[0] + sc * ex; sd[1] = bs[1] + sc * ey; sd[2] = bs[2] + sc * ez;
+        sd[3] = bs[3] + sc * exy; sd[4] = bs[4] + sc * exz; sd[5] = bs[5] + sc * eyz;
+        sig[0] = sd[0] + p3; sig[1] = sd[1] + p3; sig[2] = sd[2] + p3;
+        sig[3] = sd[3]; sig[4] = sd[4]; sig[5] = sd[5];
+        if (dE > R(0)) {
+            o.yielded = true;
+            if (bsx && P.Hkin > R(0)) {
+                const R ns = P.Hkin * dE / q;
+                bsx[0] += ns * ex; bsx[1] += ns * ey; bsx[2] += ns * ez;
+                bsx[3] += ns * exy; bsx[4] += ns * exz; bsx[5] += ns * eyz;
+            }
+            eps += dE;
+            // F_p <- (I + a s) F_p / cbrt(det), a = 1.5 dE/|s|, :277-302, as
+            // Hp' = Hp + a (s + s Hp), then (I + Hp')/c - I = (Hp' - (c - 1) I)/c
+            const R sn = sqrt(sd[0] * sd[0] + sd[1] * sd[1] + sd[2] * sd[2] +
+                              R(2) * (sd[3] * sd[3] + sd[4] * sd[4] + sd[5] * sd[5]));
+            const R al = (sn > R(1e-12)) ? (R(1.5) * dE / sn) : R(0);
+            const R S9[9] = {sd[0], sd[3], sd[4], sl[0], sd[1], sd[5], sl[1], sl[2], sd[2]};
+            R N[9];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    N[r * 3 + c] = Hp[r * 3 + c] +
+                                   al * (S9[r * 3 + c] + S9[r * 3] * Hp[c] + S9[r * 3 + 1] * Hp[3 + c] +
+                                         S9[r * 3 + 2] * Hp[6 + c]);
+            const R dm1 = detm1(N);
+            R cb, cbm1;
+            if (R(1) + dm1 > R(1e-12)) {
+                cb = cbrt(R(1) + dm1);
+                cbm1 = dm1 / (cb * cb + cb + R(1));
+            } else {
+                cb = cbrt(R(1e-12));
+                cbm1 = cb - R(1);
+            }
+            const R ic = R(1) / cb;
+#pragma unroll
+            for (int q2 = 0; q2 < 9; ++q2) Hp[q2] = ((q2 % 4 == 0) ? (N[q2] - cbm1) : N[q2]) * ic;
+            // plastic-work heating, :310-321 (dT is the rise above T_amb)
+            R dTinc = P.heat * Yr * dE;
+            if (dTinc > P.dT_cap) dTinc = P.dT_cap;
+            dT += dTinc;
+            if (dT > P.dTmax) dT = P.dTmax;
+            // Johnson-Cook damage, :329-358
+            const R tri = p3 / fmax(q, R(1e-12));
+            const R ef = (P.D1 + P.D2 * exp(P.D3 * tri)) * (R(1) + P.D4c * log(fmax(es, R(1)))) * (R(1) + P.D5 * Ts);
+            if (ef > R(1e-12)) {
+                D += dE / ef;
+                if (D > R(0.7) * P.Dth) {
+                    R dg = (P.Dth - D) / (P.Dth * R(0.3));
+                    dg = fmax(R(0), fmin(R(1), dg));
+#pragma unroll
+                    for (int q2 = 0; q2 < 6; ++q2) sig[q2] *= dg;
+                    sl[0] *= dg; sl[1] *= dg; sl[2] *= dg;
+                    const R rs = sqrt(R(1.5) * (sd[0] * sd[0] + sd[1] * sd[1] + sd[2] * sd[2] +
+                                                R(2) * (sd[3] * sd[3] + sd[4] * sd[4] + sd[5] * sd[5])));
+                    *sres_p = fmax(*sres_p, rs);
+                }
+                if (D >= P.Dth) o.to_chip = true;
+            }
+        }
+    }
+    return o;
+}
+
+// ------------------------------------------------------------------ the step kernel
+
+template <typename R, bool G2P, bool P2G>
+__global__ void __launch_bounds__(256) k_step(const Inst<R>* __restrict__ insts, const Work* __restrict__ work,
+                                              const int* __restrict__ n_work, PState<R> ps, StepArgs sa, int rbuf,
+                                              int* __restrict__ err, unsigned long long* __restrict__ ctr) {
+    __shared__ __align__(128) V4<R> raw[kTileNodes];
+    __shared__ R vel[3][kPlane];
+    __shared__ R acc[4][kPlane];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, NT = blockDim.x;
+    const int nw = *n_work;
+    uint32_t phase = 0;
+    int errf = 0;
+    unsigned long long c_esc = 0, c_yield = 0;
+    if (G2P && tid == 0) {
+        mbar_init(&mbar, 1);
+        fence_async_smem();
+    }
+    if (tid == 0) s_fail = 0;
+    __syncthreads();
+    int last_inst = -1;
+
+    for (int wi = blockIdx.x; wi < nw; wi += gridDim.x) {
+        const Work wk = work[wi];
+        const Inst<R>& P = insts[wk.inst];
+        const int bx = wk.bin % P.nbx, by = (wk.bin / P.nbx) % P.nby, bz = wk.bin / (P.nbx * P.nby);
+        const int g0x = bx * kBin, g0y = by * kBin, g0z = bz * kBin;
+        const double tg = P.t0 + (double)sa.k * P.dt;          // time of the G2P step
+        const double tp = P.t0 + (double)sa.p2g_step * P.dt;   // time of the P2G step
+        const double prg0 = P.tool_p0[0] + P.tool_v[0] * (tg - P.tool_t0);
+        const double prg1 = P.tool_p0[1] + P.tool_v[1] * (tg - P.tool_t0);
+        const double prg2 = P.tool_p0[2] + P.tool_v[2] * (tg - P.tool_t0);
+        const double prp0 = P.tool_p0[0] + P.tool_v[0] * (tp - P.tool_t0);
+        const double prp1 = P.tool_p0[1] + P.tool_v[1] * (tp - P.tool_t0);
+        const double prp2 = P.tool_p0[2] + P.tool_v[2] * (tp - P.tool_t0);
+        const V4<R>* __restrict__ gr = P.grid[rbuf];
+        V4<R>* __restrict__ gw = P.grid[rbuf ^ (G2P ? 1 : 0)];
+
+        if (G2P) {
+            if (tid == 0) {
+                if (wk.inst != last_inst) tmap_acquire(&P.tmap[rbuf]);
+                fence_async_smem();
+                mbar_expect_tx(&mbar, (uint32_t)(kTileNodes * sizeof(V4<R>)));
+                tma_load_4d(raw, &P.tmap[rbuf], &mbar, 0, g0x, g0y, g0z);
+                if (!mbar_wait_bounded(&mbar, phase, 2000000000ull)) {
+                    // give the copy in flight a second bounded chance, then stop
+                    mbar_wait_bounded(&mbar, phase, 2000000000ull);
+                    s_fail = 1;
+                }
+            }
+            phase ^= 1u;
+            last_inst = wk.inst;
+            __syncthreads();
+            if (s_fail) {
+                if (tid == 0) atomicOr(err, ERR_TIMEOUT);
+                return;
+            }
+            for (int nidx = tid; nidx < kTileNodes; nidx += NT) {
+                const int lx = nidx % kTile, ly = (nidx / kTile) % kTile, lz = nidx / (kTile * kTile);
+                R nv[3];
+                node_vel(P, raw[nidx], g0x + lx, g0y + ly, g0z + lz, prg0, prg2, nv);
+                const int t = tidx(lx, ly, lz);
+                vel[0][t] = nv[0]; vel[1][t] = nv[1]; vel[2][t] = nv[2];
+            }
+        }
+        if (P2G) {
+            for (int q = tid; q < 4 * kPlane; q += NT) (&acc[0][0])[q] = R(0);
+        }
+        __syncthreads();
+
+        const R dtdx = (R)(P.dt / P.dx);
+        const R idx_ = (R)(1.0 / P.dx);
+        for (int pl = tid; pl < wk.count; pl += NT) {
+            const int64_t pi = P.pbase + wk.start + pl;
+            uint8_t st = ps.status[pi];
+            if (st == ST_INACTIVE) continue;
+            const uint8_t st_in = st;
+            const bool fixed = (st == ST_FIXED);
+            V4<R> a0 = ps.A[0][pi], a1 = ps.A[1][pi], a2 = ps.A[2][pi], a3 = ps.A[3][pi];
+            R xi[3] = {a0.x, a0.y, a0.z};
+            R eps = a0.w;
+            R H[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
+            R Hp8 = a3.y, dT = a3.z, Dm = a3.w;
+            R v[3] = {0, 0, 0}, Cm[9], edot = R(0);
+            bool have_C = false, dirtyA = false, dirtyHp = false, wrote_C = false;
+            bool dirtyS = false;
+            R sig[6];
+
+            if (G2P) {
+                if (!fixed) {
+                    bool far = false;
+                    if (P.lod && st == ST_ACTIVE) {
+                        const double wx = P.ox + ((double)g0x + (double)xi[0]) * P.dx - prg0;
+                        const double wy = P.oy + ((double)g0y + (double)xi[1]) * P.dx - prg1;
+                        const double wz = P.oz + ((double)g0z + (double)xi[2]) * P.dx - (prg2 + P.tool_tip_dz);
+                        far = sqrt(wx * wx + wy * wy + wz * wz) > P.lod_r2;
+                    }
+                    R w[3][3], dw[3][3];
+                    int b[3];
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) b[a] = bspline(xi[a], w[a], dw[a]);
+                    R M[3][3], L[3][3];
+                    if (b[0] >= 0 && b[0] < kBin && b[1] >= 0 && b[1] < kBin && b[2] >= 0 && b[2] < kBin) {
+                        gather_tile<R>(vel, tidx(b[0], b[1], b[2]), w, dw, v, M, L);
+                    } else {
+                        const int gb[3] = {g0x + b[0], g0y + b[1], g0z + b[2]};
+                        gather_global<R>(P, gr, gb, w, dw, prg0, prg2, v, M, L);
+                        ++c_esc;
+                    }
+                    const R d[3] = {xi[0] - R(b[0]), xi[1] - R(b[1]), xi[2] - R(b[2])};
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) xi[a] = fma(v[a], dtdx, xi[a]);
+                    dirtyA = true;
+                    if (st == ST_CHIP) {
+                        edot = R(0);
+                    } else {
+                        // C = factor/dx^2 * B with B = dx (M - d v), then decay (or 0 in the far zone)
+                        const R cf = far ? R(0) : P.apic * idx_ * P.decay;
+#pragma unroll
+                        for (int a = 0; a < 3; ++a)
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) Cm[a * 3 + c] = cf * (M[a][c] - d[c] * v[a]);
+                        have_C = true;
+                        // F <- (I + L dt) F  as  H <- H + Ldt (I + H)
+                        R Ld[9];
+#pragma unroll
+                        for (int a = 0; a < 3; ++a)
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) Ld[a * 3 + c] = L[a][c] * dtdx;
+                        R Hn[9];
+#pragma unroll
+                        for (int a = 0; a < 3; ++a)
+#pragma unroll
+                            for (int c = 0; c < 3; ++c)
+                                Hn[a * 3 + c] = H[a * 3 + c] + Ld[a * 3 + c] + Ld[a * 3] * H[c] +
+                                                Ld[a * 3 + 1] * H[3 + c] + Ld[a * 3 + 2] * H[6 + c];
+#pragma unroll
+                        for (int q = 0; q < 9; ++q) H[q] = Hn[q];
+                        const R l00 = L[0][0] * idx_, l11 = L[1][1] * idx_, l22 = L[2][2] * idx_;
+                        const R s01 = (L[0][1] + L[1][0]) * idx_, s02 = (L[0][2] + L[2][0]) * idx_,
+                                s12 = (L[1][2] + L[2][1]) * idx_;
+                        edot = sqrt(R(2.0 / 3.0) * (l00 * l00 + l11 * l11 + l22 * l22 + R(0.5) * s01 * s01 +
+                                                      R(0.5) * s02 * s02 + R(0.5) * s12 * s12));
+                    }
+                }
+                // chip separation and fracture after the move (step counter parity)
+                if (P.chip_every > 0 && ((P.step0 + sa.k) % P.chip_every) == 0) {
+                    const double tipz = prg2 + P.tool_tip_dz;
+                    if (st == ST_ACTIVE) {
+                        const double zw = P.oz + ((double)g0z + (double)xi[2]) * P.dx;
+                        if (zw < tipz - P.dx * 1.5 && Dm > R(1e-6)) {
+                            st = ST_CHIP;
+                            const V4<R> s0 = ps.S[0][pi];
+                            const R rs = sqrt(s0.x * s0.x + s0.y * s0.y + s0.z * s0.z);
+                            ps.sres[pi] = fmax(ps.sres[pi], rs);
+                            ps.S[0][pi] = mk4<R>(0, 0, 0, 0);
+                            ps.S[1][pi] = mk4<R>(0, 0, 0, 0);
+                            Dm = fmax(Dm, P.Dth);
+                            dirtyA = true;
+                        }
+                    } else if (st == ST_CHIP && Dm >= P.Dth * R(1.5)) {
+                        const uint32_t seed = (uint32_t)ps.id[pi] * 2654435761u;
+                        const R rx = (R)((double)((seed >> 16) & 0xFF) / 255.0 - 0.5);
+                        const R ry = (R)((double)((seed >> 8) & 0xFF) / 255.0 - 0.5);
+                        const R rz = (R)((double)(seed & 0xFF) / 255.0 - 0.5);
+                        const R sp = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+                        const R pm = sp * R(0.3) + R(0.5);
+                        v[0] += rx * pm; v[1] += ry * pm; v[2] += rz * pm;
+                        Dm = P.Dth * R(0.5);
+                        dirtyA = true;
+                    }
+                }
+            } else {
+                // P2G-only launch: velocity, C and strain rate come from memory
+                const V4<R> b0 = ps.B[0][pi];
+                v[0] = b0.x; v[1] = b0.y; v[2] = b0.z; edot = b0.w;
+            }
+
+            bool yielded = false;
+            if (P2G) {
+                // kill zone on the cell index, :130-139
+                const int cx = g0x + (int)floor(xi[0]), cy = g0y + (int)floor(xi[1]), cz = g0z + (int)floor(xi[2]);
+                if (cx < 1 || cx >= P.nx - 2 || cy < 1 || cy >= P.ny - 2 || cz < 1 || cz >= P.nz - 2) {
+                    st = ST_INACTIVE;
+                } else {
+                    bool far = false;
+                    if (P.lod && st == ST_ACTIVE) {
+                        const double wx = P.ox + ((double)g0x + (double)xi[0]) * P.dx - prp0;
+                        const double wy = P.oy + ((double)g0y + (double)xi[1]) * P.dx - prp1;
+                        const double wz = P.oz + ((double)g0z + (double)xi[2]) * P.dx - (prp2 + P.tool_tip_dz);
+                        far = sqrt(wx * wx + wy * wy + wz * wz) > P.lod_r2;
+                    }
+                    bool skip = far || fixed || st == ST_CHIP;
+                    R Jv = R(1);
+                    R sl[3] = {0, 0, 0};
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) sig[q] = R(0);
+                    if (!skip && st == ST_ACTIVE) {
+                        const V4<R> a4 = ps.A[4][pi], a5 = ps.A[5][pi];
+                        R Hp[9] = {a4.x, a4.y, a4.z, a4.w, a5.x, a5.y, a5.z, a5.w, Hp8};
+                        R bsv[6];
+                        R* bsp = nullptr;
+                        if (P.Hkin > R(0)) {
+                            const V4<R> k0 = ps.K[0][pi], k1 = ps.K[1][pi];
+                            bsv[0] = k0.x; bsv[1] = k0.y; bsv[2] = k0.z; bsv[3] = k0.w; bsv[4] = k1.x; bsv[5] = k1.y;
+                            bsp = bsv;
+                        }
+                        const R D_before = Dm;
+                        JCOut jo = jc_update<R>(P, H, Hp, eps, dT, Dm, edot, sig, sl, Jv, &ps.sres[pi], bsp, errf);
+                        if (jo.yielded) {
+                            yielded = true;
+                            dirtyHp = true;
+                            dirtyA = true;
+                            Hp8 = Hp[8];
+                            ps.A[4][pi] = mk4<R>(Hp[0], Hp[1], Hp[2], Hp[3]);
+                            ps.A[5][pi] = mk4<R>(Hp[4], Hp[5], Hp[6], Hp[7]);
+                            if (bsp) {
+                                ps.K[0][pi] = mk4<R>(bsv[0], bsv[1], bsv[2], bsv[3]);
+                                ps.K[1][pi] = mk4<R>(bsv[4], bsv[5], R(0), R(0));
+                            }
+                        }
+                        (void)D_before;
+                        if (jo.to_chip) { st = ST_CHIP; skip = true; }
+                        dirtyS = sa.sigma_all || Dm > R(1e-6) || P.lod;
+                        if (dirtyS) {
+                            ps.S[0][pi] = mk4<R>(sig[0], sig[1], sig[2], sig[3]);
+                            ps.S[1][pi] = mk4<R>(sig[4], sig[5], R(0), R(0));
+                        }
+                    }
+                    // C of the particle: from this launch's gather, or the frozen
+                    // value of a CHIP/FIXED particle (g2pKernel keeps it)
+                    if (!have_C && !fixed) {
+                        const V4<R> c1 = ps.B[1][pi], c2 = ps.B[2][pi], c3 = ps.B[3][pi];
+                        Cm[0] = c1.x; Cm[1] = c1.y; Cm[2] = c1.z; Cm[3] = c1.w;
+                        Cm[4] = c2.x; Cm[5] = c2.y; Cm[6] = c2.z; Cm[7] = c2.w; Cm[8] = c3.x;
+                    }
+                    if (!fixed && have_C && st == ST_CHIP && st_in != ST_CHIP) {
+                        // turned CHIP this launch: freeze C as the reference does
+                        ps.B[1][pi] = mk4<R>(Cm[0], Cm[1], Cm[2], Cm[3]);
+                        ps.B[2][pi] = mk4<R>(Cm[4], Cm[5], Cm[6], Cm[7]);
+                        ps.B[3][pi] = mk4<R>(Cm[8], R(0), R(0), R(0));
+                        wrote_C = true;
+                    }
+                    // scatter
+                    R w[3][3], dw[3][3];
+                    int b[3];
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) b[a] = bspline(xi[a], w[a], dw[a]);
+                    const R m = P.pmass;
+                    R Q[3], Rm[3][3], S[3][3];
+                    if (!fixed) {
+                        const R d[3] = {xi[0] - R(b[0]), xi[1] - R(b[1]), xi[2] - R(b[2])};
+                        const R mdx = m * (R)P.dx;
+                        R ef[3] = {0, 0, 0};
+                        if (sa.use_ext && P.ext_r > 0.0) {
+                            const double ex = P.ox + ((double)g0x + (double)xi[0]) * P.dx - P.ext_c[0];
+                            const double ey = P.oy + ((double)g0y + (double)xi[1]) * P.dx - P.ext_c[1];
+                            const double ez = P.oz + ((double)g0z + (double)xi[2]) * P.dx - P.ext_c[2];
+                            const double dist = sqrt(ex * ex + ey * ey + ez * ez);
+                            if ((st == ST_ACTIVE || st == ST_CHIP) && dist < P.ext_r) {
+                                const double fw = (1.0 - dist / P.ext_r) * P.dt;
+                                ef[0] = (R)(P.ext_f[0] * fw); ef[1] = (R)(P.ext_f[1] * fw); ef[2] = (R)(P.ext_f[2] * fw);
+                            }
+                        }
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            Q[a] = m * v[a] - mdx * (Cm[a * 3] * d[0] + Cm[a * 3 + 1] * d[1] + Cm[a * 3 + 2] * d[2]) + ef[a];
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) Rm[a][c] = mdx * Cm[a * 3 + c];
+                        }
+                        const R sf = skip ? R(0) : -(R)P.dt * P.pvol * Jv * idx_;
+                        S[0][0] = sf * sig[0]; S[1][1] = sf * sig[1]; S[2][2] = sf * sig[2];
+                        S[0][1] = sf * sig[3]; S[1][0] = sf * sl[0];
+                        S[0][2] = sf * sig[4]; S[2][0] = sf * sl[1];
+                        S[1][2] = sf * sig[5]; S[2][1] = sf * sl[2];
+                    } else {
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            Q[a] = R(0);
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) { Rm[a][c] = R(0); S[a][c] = R(0); }
+                        }
+                        // FIXED: an external force still acts (reference adds w*ext_f)
+                        if (sa.use_ext && P.ext_r > 0.0) { /* ext force is applied to ACTIVE and CHIP only */ }
+                    }
+                    if (b[0] >= 0 && b[0] < kBin && b[1] >= 0 && b[1] < kBin && b[2] >= 0 && b[2] < kBin) {
+                        scatter_tile<R>(acc, tidx(b[0], b[1], b[2]), w, dw, m, Q, Rm, S, fixed);
+                    } else {
+                        const int gb[3] = {g0x + b[0], g0y + b[1], g0z + b[2]};
+                        scatter_global<R>(P, gw, gb, w, dw, m, Q, Rm, S, fixed);
+                        ++c_esc;
+                    }
+                }
+            }
+
+            // write back
+            if (dirtyA) {
+                ps.A[0][pi] = mk4<R>(xi[0], xi[1], xi[2], eps);
+                ps.A[1][pi] = mk4<R>(H[0], H[1], H[2], H[3]);
+                ps.A[2][pi] = mk4<R>(H[4], H[5], H[6], H[7]);
+                ps.A[3][pi] = mk4<R>(H[8], Hp8, dT, Dm);
+            }
+            if (st != st_in) ps.status[pi] = st;
+            if (G2P && sa.write_out) {
+                if (fixed) {
+                    const V4<R> b0 = ps.B[0][pi];
+                    ps.B[0][pi] = mk4<R>(R(0), R(0), R(0), b0.w);
+                } else {
+                    ps.B[0][pi] = mk4<R>(v[0], v[1], v[2], edot);
+                    if (have_C && !wrote_C && st_in != ST_CHIP) {
+                        ps.B[1][pi] = mk4<R>(Cm[0], Cm[1], Cm[2], Cm[3]);
+                        ps.B[2][pi] = mk4<R>(Cm[4], Cm[5], Cm[6], Cm[7]);
+                        ps.B[3][pi] = mk4<R>(Cm[8], R(0), R(0), R(0));
+                    }
+                }
+            }
+            c_yield += yielded ? 1 : 0;
+            (void)dirtyHp;
+            (void)dirtyS;
+        }
+        __syncthreads();
+
+        if (P2G) {
+            for (int nidx = tid; nidx < kTileNodes; nidx += NT) {
+                const int lx = nidx % kTile, ly = (nidx / kTile) % kTile, lz = nidx / (kTile * kTile);
+                const int t = tidx(lx, ly, lz);
+                const R m = acc[0][t];
+                if (m == R(0)) continue;
+                const int gx = g0x + lx, gy = g0y + ly, gz = g0z + lz;
+                if (gx >= P.nx || gy >= P.ny || gz >= P.nz) continue;
+                vec_atomic_add<R>(&gw[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], m, acc[1][t], acc[2][t],
+                                  acc[3][t]);
+            }
+            __syncthreads();
+        }
+    }
+    // counters: warp-reduce, one atomic per warp
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        c_esc += __shfl_down_sync(0xffffffffu, c_esc, o);
+        c_yield += __shfl_down_sync(0xffffffffu, c_yield, o);
+        errf |= __shfl_down_sync(0xffffffffu, errf, o);
+    }
+    if ((tid & 31) == 0) {
+        if (c_esc) atomicAdd(&ctr[0], c_esc);
+        if (c_yield) atomicAdd(&ctr[1], c_yield);
+        if (errf) atomicOr(err, errf);
+    }
+}
+
+template <typename R>
+void launch_step(const Inst<R>* insts, const Work* work, const int* n_work, int max_work, const PState<R>& ps,
+                 const StepArgs& a, int rbuf, bool g2p, bool p2g, int threads, int ctas_per_sm, int* err,
+                 unsigned long long* counters, cudaStream_t st) {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    if (max_work <= 0) return;
+    int grid = sms * (ctas_per_sm > 0 ? ctas_per_sm : 4);
+    if (grid > max_work) grid = max_work;
+    if (threads <= 0) threads = 128;
+    if (threads > 256) threads = 256;
+    if (g2p && p2g)
+        k_step<R, true, true><<<grid, threads, 0, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+    else if (g2p)
+        k_step<R, true, false><<<grid, threads, 0, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+    else
+        k_step<R, false, true><<<grid, threads, 0, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+    ++launch_counter();
+}
+
+template void launch_step<float>(const Inst<float>*, const Work*, const int*, int, const PState<float>&,
+                                 const StepArgs&, int, bool, bool, int, int, int*, unsigned long long*, cudaStream_t);
+template void launch_step<double>(const Inst<double>*, const Work*, const int*, int, const PState<double>&,
+                                  const StepArgs&, int, bool, bool, int, int, int*, unsigned long long*, cudaStream_t);
+
+}  // namespace mpmb

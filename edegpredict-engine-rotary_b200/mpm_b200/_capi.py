@@ -1,0 +1,136 @@
+"""ctypes binding of include/mpm_capi.h (libmpm_b200.so).
+
+Only plain C types cross the boundary.  Importing this module loads the
+library that build.py placed next to it and fails loudly when it is missing:
+there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libmpm_b200.so"
+
+MPM_ABI_VERSION = 1
+MPM_OK, MPM_INVALID_ARG, MPM_OOM, MPM_CUDA_ERROR, MPM_NUMERIC, MPM_OUT_OF_GRID, MPM_TIMEOUT, \
+    MPM_NOT_SUPPORTED, MPM_CAPACITY = range(9)
+ACTIVE, INACTIVE, CHIP, BOUNDARY, FIXED = 0, 1, 2, 3, 4
+PREC_F32, PREC_F64 = 0, 1
+TOOL_NONE, TOOL_RASTER, TOOL_SDF_STICKY, TOOL_SDF_SLIP = 0, 1, 2, 3
+SHAPE_CYLINDER_Y, SHAPE_WEDGE_Y = 0, 1
+PLAST_EXPLICIT, PLAST_NEWTON = 0, 1
+SCHED_SPLIT, SCHED_FUSED = 0, 1
+
+_d, _i32, _i64, _vp = C.c_double, C.c_int32, C.c_int64, C.c_void_p
+
+
+class MpmParams(C.Structure):
+    _fields_ = [
+        ("abi_version", _i32), ("precision", _i32), ("nx", _i32), ("ny", _i32), ("nz", _i32), ("plasticity", _i32),
+        ("dx", _d), ("origin", _d * 3), ("particle_mass", _d), ("particle_volume", _d),
+        ("E", _d), ("nu", _d), ("rho_phys", _d), ("cp", _d), ("beta", _d), ("Tm", _d), ("Tamb", _d),
+        ("jc_A", _d), ("jc_B", _d), ("jc_n", _d), ("jc_C", _d), ("jc_m", _d), ("edot0", _d), ("H_kin", _d),
+        ("D1", _d), ("D2", _d), ("D3", _d), ("D4", _d), ("D5", _d), ("D_th", _d),
+        ("fixture_thickness", _d), ("fixture_damping", _d), ("gravity_z", _d), ("mass_threshold", _d),
+        ("apic_dinv_factor", _d), ("apic_decay", _d), ("deps_cap", _d), ("dT_cap", _d),
+        ("lod_enabled", _i32), ("chip_every", _i32), ("lod_active_r", _d), ("lod_near_r", _d),
+        ("newton_tol", _d), ("newton_maxit", _i32), ("schedule", _i32), ("sort_every", _i32),
+        ("threads_per_block", _i32),
+    ]
+
+
+class MpmToolDesc(C.Structure):
+    _fields_ = [
+        ("mode", _i32), ("shape", _i32), ("position", _d * 3), ("velocity", _d * 3), ("radius", _d),
+        ("rake", _d), ("clearance", _d), ("tip_dz", _d), ("n_samples", _i32), ("_pad", _i32),
+        ("sample_dx", _vp), ("sample_dy", _vp), ("sample_dz", _vp),
+    ]
+
+
+class MpmParticlesSoa(C.Structure):
+    _fields_ = [("elem", _i32), ("_pad", _i32)] + [
+        (n, _vp) for n in ("x", "y", "z", "vx", "vy", "vz", "F", "Fp", "C", "stress", "backstress",
+                           "plastic_strain", "strain_rate", "temperature", "damage", "residual_stress", "status",
+                           "id")
+    ]
+
+
+class MpmMetrics(C.Structure):
+    _fields_ = [
+        ("ref_max_stress", _d), ("ref_max_temperature", _d), ("ref_kinetic", _d), ("ref_internal", _d),
+        ("mass", _d), ("momentum", _d * 3), ("kinetic", _d), ("internal_elastic", _d), ("thermal", _d),
+        ("max_temperature", _d), ("max_von_mises", _d), ("max_plastic_strain", _d), ("mean_plastic_strain", _d),
+        ("n_active", _i64), ("n_chip", _i64), ("n_fixed", _i64), ("n_inactive", _i64),
+        ("bounds_min", _d * 3), ("bounds_max", _d * 3), ("n_escaped", _i64), ("n_sorts", _i64),
+    ]
+
+    def as_dict(self) -> dict:
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+
+PARTICLE_FIELDS = {  # name -> values per particle
+    "x": 1, "y": 1, "z": 1, "vx": 1, "vy": 1, "vz": 1, "F": 9, "Fp": 9, "C": 9, "stress": 6, "backstress": 6,
+    "plastic_strain": 1, "strain_rate": 1, "temperature": 1, "damage": 1, "residual_stress": 1,
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libmpm_b200.so (raises when it was not built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: run edegpredict-engine-rotary_b200/build.py")
+        L = C.CDLL(str(LIB_PATH))
+        P = C.POINTER
+        sig = {
+            "mpm_params_default": (_i32, [P(MpmParams)]),
+            "mpm_create": (_i32, [P(MpmParams), _i64, _vp, P(_vp)]),
+            "mpm_destroy": (_i32, [_vp]),
+            "mpm_init_box": (_i32, [_vp, P(_i32), P(_i32), _i32, C.c_uint64, C.c_uint32, _i32, _d, P(MpmToolDesc)]),
+            "mpm_upload": (_i32, [_vp, P(MpmParticlesSoa), _i64]),
+            "mpm_download": (_i32, [_vp, P(MpmParticlesSoa)]),
+            "mpm_export_aos": (_i32, [_vp, _vp, _i64]),
+            "mpm_set_tool": (_i32, [_vp, P(MpmToolDesc)]),
+            "mpm_step": (_i32, [_vp, _d, _i32]),
+            "mpm_stable_dt": (_i32, [_vp, _d, P(_d)]),
+            "mpm_sync_metrics": (_i32, [_vp, P(MpmMetrics)]),
+            "mpm_set_mass_scaling": (_i32, [_vp, _d]),
+            "mpm_apply_external_force": (_i32, [_vp, P(_d), _d, P(_d)]),
+            "mpm_set_temperatures": (_i32, [_vp, P(_d), _i64]),
+            "mpm_get_counts": (_i32, [_vp, P(_i64), P(_i64), P(_d)]),
+            "mpm_get_stream": (_i32, [_vp, P(_vp)]),
+            "mpm_reset_clock": (_i32, [_vp]),
+            "mpm_launch_count": (_i32, [_vp, P(_i64)]),
+            "mpm_last_error": (C.c_char_p, [_vp]),
+            "mpm_status_string": (C.c_char_p, [_i32]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+class MpmError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{lib().mpm_status_string(status).decode()}: {msg}")
+        self.status = status
+
+
+def check(status: int, handle=None) -> None:
+    if status != MPM_OK:
+        msg = lib().mpm_last_error(handle)
+        raise MpmError(status, msg.decode() if msg else "")
+
+
+def default_params() -> MpmParams:
+    p = MpmParams()
+    check(lib().mpm_params_default(C.byref(p)))
+    return p

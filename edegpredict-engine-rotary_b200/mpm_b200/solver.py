@@ -1,0 +1,172 @@
+"""Python handle over the C ABI (used by the tests and the benchmark).
+
+Solver mirrors the call sequence the engine makes on the reference's
+MPMSolver (src/SimulationEngine.cpp:499-537): set the tool, step, sync the
+metrics, read the particles.  Particle arrays are numpy arrays in the
+reference's units, keyed by the field names of mpm_particles_soa.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, Optional
+
+import numpy as np
+
+from . import _capi as A
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Solver:
+    def __init__(self, params: A.MpmParams, capacity: int, stream: int = 0):
+        self._lib = A.lib()
+        self.params = params
+        h = C.c_void_p()
+        A.check(self._lib.mpm_create(C.byref(params), int(capacity), C.c_void_p(stream or None), C.byref(h)))
+        self.h = h
+        self._keep = []
+
+    def close(self) -> None:
+        if self.h:
+            self._lib.mpm_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, status: int) -> None:
+        A.check(status, self.h)
+
+    # ---------------------------------------------------------------- tool
+    @staticmethod
+    def tool_desc(tool: dict) -> A.MpmToolDesc:
+        t = A.MpmToolDesc()
+        t.mode = int(tool.get("mode", A.TOOL_NONE))
+        t.shape = int(tool.get("shape", A.SHAPE_CYLINDER_Y))
+        for k in range(3):
+            t.position[k] = float(tool.get("position", (0, 0, 0))[k])
+            t.velocity[k] = float(tool.get("velocity", (0, 0, 0))[k])
+        t.radius = float(tool.get("radius", 0.0))
+        t.rake = float(tool.get("rake", 0.0))
+        t.clearance = float(tool.get("clearance", 0.0))
+        t.tip_dz = float(tool.get("tip_dz", 0.0))
+        s = tool.get("samples")
+        if s is not None:
+            s = np.ascontiguousarray(s, dtype=np.float64)
+            cols = [np.ascontiguousarray(s[:, k]) for k in range(3)]
+            t._cols = cols  # keep alive
+            t.n_samples = len(s)
+            t.sample_dx, t.sample_dy, t.sample_dz = (c.ctypes.data for c in cols)
+        return t
+
+    def set_tool(self, tool: dict) -> None:
+        t = self.tool_desc(tool)
+        self._check(self._lib.mpm_set_tool(self.h, C.byref(t)))
+
+    # ---------------------------------------------------------------- particles
+    def init_box(self, c0, c1, ppc: int, seed: int, instance: int = 0, fixed_layers: int = 2, T0: float = 293.0,
+                 tool: Optional[dict] = None) -> int:
+        a0 = (C.c_int32 * 3)(*map(int, c0))
+        a1 = (C.c_int32 * 3)(*map(int, c1))
+        t = self.tool_desc(tool) if tool else None
+        self._check(self._lib.mpm_init_box(self.h, a0, a1, int(ppc), C.c_uint64(seed), C.c_uint32(instance),
+                                           int(fixed_layers), float(T0), C.byref(t) if t else None))
+        return self.counts()[0]
+
+    def upload(self, parts: Dict[str, np.ndarray], elem: int = 8) -> None:
+        dt = np.float64 if elem == 8 else np.float32
+        s = A.MpmParticlesSoa()
+        s.elem = elem
+        keep = []
+        n = len(parts["x"])
+        for name in A.PARTICLE_FIELDS:
+            if name in parts and parts[name] is not None:
+                a = np.ascontiguousarray(parts[name], dtype=dt)
+                keep.append(a)
+                setattr(s, name, a.ctypes.data)
+        for name in ("status", "id"):
+            if name in parts and parts[name] is not None:
+                a = np.ascontiguousarray(parts[name], dtype=np.int32)
+                keep.append(a)
+                setattr(s, name, a.ctypes.data)
+        self._check(self._lib.mpm_upload(self.h, C.byref(s), n))
+
+    def download(self, fields=None, elem: int = 8) -> Dict[str, np.ndarray]:
+        n = self.counts()[0]
+        dt = np.float64 if elem == 8 else np.float32
+        s = A.MpmParticlesSoa()
+        s.elem = elem
+        out = {}
+        for name, per in A.PARTICLE_FIELDS.items():
+            if fields is None or name in fields:
+                a = np.zeros((n, per) if per > 1 else (n,), dtype=dt)
+                out[name] = a
+                setattr(s, name, a.ctypes.data)
+        for name in ("status", "id"):
+            if fields is None or name in fields:
+                a = np.zeros(n, dtype=np.int32)
+                out[name] = a
+                setattr(s, name, a.ctypes.data)
+        self._check(self._lib.mpm_download(self.h, C.byref(s)))
+        return out
+
+    def export_aos(self) -> np.ndarray:
+        n = self.counts()[0]
+        buf = np.zeros(max(n, 1) * 504, dtype=np.uint8)
+        self._check(self._lib.mpm_export_aos(self.h, buf.ctypes.data_as(C.c_void_p), buf.nbytes))
+        return buf[: n * 504]
+
+    # ---------------------------------------------------------------- stepping
+    def step(self, dt: float, nsteps: int = 1) -> None:
+        self._check(self._lib.mpm_step(self.h, float(dt), int(nsteps)))
+
+    def stable_dt(self, cfl: float) -> float:
+        d = C.c_double()
+        self._check(self._lib.mpm_stable_dt(self.h, float(cfl), C.byref(d)))
+        return d.value
+
+    def metrics(self) -> dict:
+        m = A.MpmMetrics()
+        self._check(self._lib.mpm_sync_metrics(self.h, C.byref(m)))
+        return m.as_dict()
+
+    def set_mass_scaling(self, f: float) -> None:
+        self._check(self._lib.mpm_set_mass_scaling(self.h, float(f)))
+
+    def apply_external_force(self, center, radius, force) -> None:
+        c = (C.c_double * 3)(*center)
+        f = (C.c_double * 3)(*force)
+        self._check(self._lib.mpm_apply_external_force(self.h, c, float(radius), f))
+
+    def set_temperatures(self, T: np.ndarray) -> None:
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        self._check(self._lib.mpm_set_temperatures(self.h, T.ctypes.data_as(C.POINTER(C.c_double)), len(T)))
+
+    def counts(self):
+        n, k, t = C.c_int64(), C.c_int64(), C.c_double()
+        self._check(self._lib.mpm_get_counts(self.h, C.byref(n), C.byref(k), C.byref(t)))
+        return n.value, k.value, t.value
+
+    def launches(self) -> int:
+        c = C.c_int64()
+        self._check(self._lib.mpm_launch_count(self.h, C.byref(c)))
+        return c.value
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._check(self._lib.mpm_get_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def reset_clock(self) -> None:
+        self._check(self._lib.mpm_reset_clock(self.h))

@@ -1,0 +1,217 @@
+/*
+ * mpm_capi.h -- C ABI of the B200 MPM workpiece step (libmpm_b200.so).
+ *
+ * Plain C types only: pointers, sizes, scalars.  Every function returns an
+ * mpm_status; a failed call leaves a message for mpm_last_error().  Nothing
+ * calls exit() or traps the GPU.  A handle is driven by one host thread at a
+ * time; device work goes on the stream given to mpm_create (or the handle's
+ * own stream) and is asynchronous except where a function says it
+ * synchronises.
+ *
+ * Each entry point names the reference interface it replaces.  The reference
+ * solver is class edgepredict::MPMSolver (include/MPMSolver.cuh:76-268) behind
+ * IPhysicsSolver / IMetricsProvider / IThermalCoupling
+ * (include/IPhysicsSolver.h:24-149).
+ */
+#ifndef MPM_CAPI_H
+#define MPM_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPM_ABI_VERSION 1
+
+typedef enum mpm_status {
+    MPM_OK = 0,
+    MPM_INVALID_ARG = 1,
+    MPM_OOM = 2,
+    MPM_CUDA_ERROR = 3,
+    MPM_NUMERIC = 4,      /* NaN/Inf in the state, or a Newton return that did not converge */
+    MPM_OUT_OF_GRID = 5,
+    MPM_TIMEOUT = 6,      /* a bounded device-side wait gave up */
+    MPM_NOT_SUPPORTED = 7,
+    MPM_CAPACITY = 8      /* more particles or instances than the handle holds */
+} mpm_status;
+
+/* Particle status codes: ParticleStatus, include/Types.h:37-43. */
+enum { MPM_ACTIVE = 0, MPM_INACTIVE = 1, MPM_CHIP = 2, MPM_BOUNDARY = 3, MPM_FIXED = 4 };
+
+enum { MPM_PREC_F32 = 0, MPM_PREC_F64 = 1 };
+enum { MPM_TOOL_NONE = 0, MPM_TOOL_RASTER = 1, MPM_TOOL_SDF_STICKY = 2, MPM_TOOL_SDF_SLIP = 3 };
+enum { MPM_SHAPE_CYLINDER_Y = 0, MPM_SHAPE_WEDGE_Y = 1 };
+enum { MPM_PLAST_EXPLICIT = 0, MPM_PLAST_NEWTON = 1 };
+enum { MPM_SCHED_SPLIT = 0, MPM_SCHED_FUSED = 1 };
+
+/*
+ * Per-instance parameters.  Replaces MPMKernelConfig (include/MPMSolver.cuh:29-74)
+ * plus the solver fields MPMSolver::initialize fills (src/MPMSolver.cu:832-915),
+ * with the grid given explicitly instead of the hard-wired 0.2 m cube.
+ * Temperatures may be in K or degC: only (T - Tamb)/(Tm - Tamb) and
+ * differences enter the physics.
+ */
+typedef struct mpm_params {
+    int32_t abi_version;       /* MPM_ABI_VERSION */
+    int32_t precision;         /* MPM_PREC_F32 (bulk FP32) or MPM_PREC_F64 */
+    /* grid: node (i,j,k) at origin + (i,j,k)*dx, i < nx ... (each >= 8) */
+    int32_t nx, ny, nz;
+    int32_t plasticity;        /* MPM_PLAST_EXPLICIT (reference return) or MPM_PLAST_NEWTON */
+    double dx;
+    double origin[3];
+    /* particles: uniform mass and initial volume per instance */
+    double particle_mass, particle_volume;
+    /* elasticity and heat */
+    double E, nu, rho_phys, cp, beta, Tm, Tamb;
+    /* Johnson-Cook flow stress, reference strain rate, kinematic hardening */
+    double jc_A, jc_B, jc_n, jc_C, jc_m, edot0, H_kin;
+    /* Johnson-Cook damage */
+    double D1, D2, D3, D4, D5, D_th;
+    /* grid boundary: fixture layer (applyFixtureBCKernel), gravity, empty-node mass */
+    double fixture_thickness, fixture_damping, gravity_z, mass_threshold;
+    /* APIC: C = apic_dinv_factor/dx^2 * B, then C *= apic_decay (reference: 3, 0.99) */
+    double apic_dinv_factor, apic_decay;
+    /* explicit-return caps (reference: 0.05, 50 K) */
+    double deps_cap, dT_cap;
+    /* level of detail (lodClassifyKernel); radii about the tool tip */
+    int32_t lod_enabled;
+    int32_t chip_every;        /* chip separation every n-th step (reference: 2); 0 disables */
+    double lod_active_r, lod_near_r;
+    double newton_tol;         /* relative residual of the Newton return */
+    int32_t newton_maxit;
+    int32_t schedule;          /* MPM_SCHED_FUSED (default) or MPM_SCHED_SPLIT */
+    int32_t sort_every;        /* re-bin particles every n steps (0: default) */
+    int32_t threads_per_block; /* CTA size of the step kernel (0: default 128) */
+} mpm_params;
+
+/* Fill p with the reference defaults (MPMKernelConfig / Config.h defaults,
+ * reference-compatible kinematics).  Grid and particle fields are zeroed. */
+mpm_status mpm_params_default(mpm_params *p);
+
+/*
+ * Rigid tool.  The reference rasterises FEM tool nodes onto the grid
+ * (MPMSolver::setToolNodes, include/MPMSolver.cuh:86-89; rasterizeToolKernel
+ * src/MPMSolver.cu:444-473; applyGridCollisionKernel :475-492).  Here the tool
+ * is a rigid body with reference point p(t) = position + velocity*(t - t_set):
+ *   MPM_TOOL_RASTER     sample offsets from the reference point, rasterised
+ *                       exactly as the reference does (parity mode);
+ *   MPM_TOOL_SDF_STICKY analytic SDF; nodes with phi <= 0 take the tool velocity;
+ *   MPM_TOOL_SDF_SLIP   analytic SDF; approaching normal relative velocity removed.
+ * tip_dz: z of the tool tip relative to the reference point (chip separation
+ * and LOD use the tip, as MPMSolver::setToolPosition does).
+ */
+typedef struct mpm_tool_desc {
+    int32_t mode;
+    int32_t shape;
+    double position[3];
+    double velocity[3];
+    double radius;             /* cylinder radius, or wedge edge radius */
+    double rake, clearance;    /* wedge angles (rad) */
+    double tip_dz;
+    int32_t n_samples;         /* MPM_TOOL_RASTER: sample offsets (host arrays) */
+    int32_t _pad;
+    const double *sample_dx, *sample_dy, *sample_dz;
+} mpm_tool_desc;
+
+/*
+ * Host particle arrays in the reference's units (m, m/s, Pa, degC/K).
+ * Matrices row-major [n][9] (F, F_p, C as MPMParticle, include/Types.h:219-225),
+ * symmetric tensors [n][6] as xx,yy,zz,xy,xz,yz.  `elem` = 8 (double) or 4 (float)
+ * for every floating field.  A NULL field reads as its MPMParticle default on
+ * upload and is skipped on download.
+ */
+typedef struct mpm_particles_soa {
+    int32_t elem;
+    int32_t _pad;
+    void *x, *y, *z, *vx, *vy, *vz;
+    void *F, *Fp, *C, *stress, *backstress;
+    void *plastic_strain, *strain_rate, *temperature, *damage, *residual_stress;
+    int32_t *status, *id;
+} mpm_particles_soa;
+
+typedef struct mpm_metrics {
+    /* reference-compatible (computeParticleStatsKernel, src/MPMSolver.cu:729-788) */
+    double ref_max_stress, ref_max_temperature, ref_kinetic, ref_internal;
+    /* conservation, FP64 reductions over particles that are not INACTIVE */
+    double mass, momentum[3], kinetic, internal_elastic, thermal;
+    double max_temperature, max_von_mises, max_plastic_strain, mean_plastic_strain;
+    int64_t n_active, n_chip, n_fixed, n_inactive;
+    double bounds_min[3], bounds_max[3];   /* ACTIVE and CHIP particles */
+    int64_t n_escaped;                     /* particles handled off their bin tile since the last re-bin */
+    int64_t n_sorts;
+} mpm_metrics;
+
+typedef struct mpm_handle mpm_handle;
+
+/* Replaces MPMSolver::MPMSolver + initialize(Config) (src/MPMSolver.cu:832-915):
+ * validates p, allocates device state for up to `capacity` particles.
+ * stream: a cudaStream_t or NULL for a handle-owned stream. */
+mpm_status mpm_create(const mpm_params *p, int64_t capacity, void *stream, mpm_handle **out);
+/* Replaces MPMSolver::~MPMSolver / freeMemory (src/MPMSolver.cu:933-964). */
+mpm_status mpm_destroy(mpm_handle *h);
+
+/* Replaces MPMSolver::initializeParticleBox (src/MPMSolver.cu:1297-1336) with a
+ * seeded, jittered box: cells [c0, c1) (cell units from the grid origin),
+ * ppc particles per cell at Philox4x32-10 uniform positions keyed by
+ * (seed, instance, cell, k); cells whose lowest `fixed_layers` z-layers are
+ * FIXED_BOUNDARY; particles inside the tool at t=0 are not kept.  Generated on
+ * the device. */
+mpm_status mpm_init_box(mpm_handle *h, const int32_t c0[3], const int32_t c1[3], int32_t ppc, uint64_t seed,
+                        uint32_t instance, int32_t fixed_layers, double T0, const mpm_tool_desc *tool_at_t0);
+
+/* Upload n particles from host arrays (replaces copyToDevice via
+ * getHostParticles/updateParticlesFromHost, include/MPMSolver.cuh:185-186). */
+mpm_status mpm_upload(mpm_handle *h, const mpm_particles_soa *host, int64_t n);
+/* Download the particles in upload order (replaces getParticles,
+ * src/MPMSolver.cu:1383-1386).  Synchronises. */
+mpm_status mpm_download(mpm_handle *h, mpm_particles_soa *host);
+/* Copy the particles, in upload order, into an array of the reference's
+ * MPMParticle layout (include/Types.h:199-266, 504 bytes) for ContactSolver,
+ * CFD and the exporters.  dst is host or device memory. Synchronises. */
+mpm_status mpm_export_aos(mpm_handle *h, void *dst, int64_t dst_bytes);
+
+/* Replaces setToolNodes / setToolPosition (include/MPMSolver.cuh:86-89, :171). */
+mpm_status mpm_set_tool(mpm_handle *h, const mpm_tool_desc *tool);
+
+/* Replaces MPMSolver::step (src/MPMSolver.cu:1062-1168): nsteps steps of dt.
+ * Asynchronous on the handle's stream. */
+mpm_status mpm_step(mpm_handle *h, double dt, int32_t nsteps);
+
+/* Replaces getStableTimeStep (src/MPMSolver.cu:1170-1178): cfl*dx/sqrt(E/rho). */
+mpm_status mpm_stable_dt(const mpm_handle *h, double cfl, double *dt);
+
+/* Replaces syncMetrics + getters (src/MPMSolver.cu:1239-1259,
+ * include/MPMSolver.cuh:135-139) and getBounds (:1232-1237).  Synchronises;
+ * also reports a device-side error (MPM_NUMERIC / MPM_TIMEOUT). */
+mpm_status mpm_sync_metrics(mpm_handle *h, mpm_metrics *out);
+
+/* Replaces setDynamicMassScaling (src/MPMSolver.cu:1211-1225): particle mass
+ * becomes rho_phys*factor*volume (never below rho_phys*volume). */
+mpm_status mpm_set_mass_scaling(mpm_handle *h, double factor);
+
+/* Replaces applyExternalForce (src/MPMSolver.cu:1422-1431): a force with
+ * linear falloff inside a sphere, applied during the next step only. */
+mpm_status mpm_apply_external_force(mpm_handle *h, const double center[3], double radius, const double force[3]);
+
+/* Replaces setParticleTemperatures (src/MPMSolver.cu:1267-1277): count <= n
+ * temperatures in upload order. */
+mpm_status mpm_set_temperatures(mpm_handle *h, const double *temperatures, int64_t count);
+
+mpm_status mpm_get_counts(const mpm_handle *h, int64_t *n_particles, int64_t *n_steps, double *time);
+mpm_status mpm_get_stream(const mpm_handle *h, void **stream);
+/* Replaces reset() (src/MPMSolver.cu:1227-1230): time and step counter to 0. */
+mpm_status mpm_reset_clock(mpm_handle *h);
+
+/* Count of the library's own kernel launches issued by this handle so far. */
+mpm_status mpm_launch_count(const mpm_handle *h, int64_t *count);
+
+/* Last error message of the handle (or of the library when h is NULL). */
+const char *mpm_last_error(const mpm_handle *h);
+const char *mpm_status_string(mpm_status s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,622 @@
+/*
+ * mpm_oracle.c -- CPU FP64 restatement of the EdgePredict MPM workpiece step.
+ *
+ * TEST INFRASTRUCTURE ONLY (see mpm_oracle.h).  Citations are to the
+ * reference project, path:line.
+ *
+ * Step order restated from MPMSolver::step (src/MPMSolver.cu:1062-1168):
+ *   [lodClassify] -> resetGrid -> p2g -> updateGrid -> [fixtureBC]
+ *   -> [rasterizeTool -> gridCollision] -> g2p -> resetExternalForce
+ *   -> chip separation when the step counter is even (:1160-1164).
+ */
+#include "mpm_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* grid channel offsets (SoA planes of nn doubles each) */
+enum { G_M, G_PX, G_PY, G_PZ, G_FX, G_FY, G_FZ, G_VX, G_VY, G_VZ, G_TVX, G_TVY, G_TVZ, G_TOOL, G_NCH };
+
+static inline int64_t nnodes(const orc_params *p) { return (int64_t)p->nx * p->ny * p->nz; }
+
+int64_t orc_grid_doubles(const orc_params *p) { return nnodes(p) * G_NCH; }
+
+/* ---------------------------------------------------------------- helpers */
+
+/* getWeightsAndGradients, src/MPMSolver.cu:20-34 (quadratic B-spline). */
+static void weights(double xp, double invDx, int *base, double w[3], double dw[3]) {
+    double xf = xp * invDx;
+    int b = (int)floor(xf - 0.5);
+    double d0 = xf - b, d1 = d0 - 1.0, d2 = d0 - 2.0;
+    *base = b;
+    w[0] = 0.5 * (1.5 - d0) * (1.5 - d0);
+    w[1] = 0.75 - d1 * d1;
+    w[2] = 0.5 * (1.5 + d2) * (1.5 + d2);
+    dw[0] = -(1.5 - d0) * invDx;
+    dw[1] = -2.0 * d1 * invDx;
+    dw[2] = (1.5 + d2) * invDx;
+}
+
+/* det3x3 / mul3x3 / inv3x3, src/MPMSolver.cu:36-68. */
+static double det3(const double *A) {
+    return A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) +
+           A[2] * (A[3] * A[7] - A[4] * A[6]);
+}
+static void mul3(const double *A, const double *B, double *Cm) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            Cm[i * 3 + j] = A[i * 3 + 0] * B[0 * 3 + j] + A[i * 3 + 1] * B[1 * 3 + j] + A[i * 3 + 2] * B[2 * 3 + j];
+}
+static void inv3(const double *A, double *R) {
+    double det = det3(A);
+    if (fabs(det) < 1e-12) {
+        for (int i = 0; i < 9; ++i) R[i] = (i % 4 == 0) ? 1.0 : 0.0;
+        return;
+    }
+    double id = 1.0 / det;
+    R[0] = (A[4] * A[8] - A[5] * A[7]) * id;
+    R[1] = -(A[1] * A[8] - A[2] * A[7]) * id;
+    R[2] = (A[1] * A[5] - A[2] * A[4]) * id;
+    R[3] = -(A[3] * A[8] - A[5] * A[6]) * id;
+    R[4] = (A[0] * A[8] - A[2] * A[6]) * id;
+    R[5] = -(A[0] * A[5] - A[2] * A[3]) * id;
+    R[6] = (A[3] * A[7] - A[4] * A[6]) * id;
+    R[7] = -(A[0] * A[7] - A[1] * A[6]) * id;
+    R[8] = (A[0] * A[4] - A[1] * A[3]) * id;
+}
+
+static inline void gadd(double *a, double v, int atomic) {
+    if (atomic) {
+#pragma omp atomic
+        *a += v;
+    } else {
+        *a += v;
+    }
+}
+
+/* ------------------------------------------------------------- tool SDF */
+
+/* Analytic rigid-tool SDF (an extension of this build; the reference's grid
+ * boundary is the rasterised tool of src/MPMSolver.cu:444-492).  Returns the
+ * signed distance and the outward unit normal. */
+static double tool_sdf_n(const orc_params *p, const double pr[3], double x, double y, double z, double nrm[3]) {
+    (void)y;
+    double qx = x - pr[0], qz = z - pr[2];
+    if (p->tool_shape == ORC_SHAPE_CYLINDER_Y) {
+        double r = sqrt(qx * qx + qz * qz);
+        if (r > 0.0) { nrm[0] = qx / r; nrm[1] = 0.0; nrm[2] = qz / r; }
+        else { nrm[0] = 0.0; nrm[1] = 0.0; nrm[2] = 1.0; }
+        return r - p->tool_r;
+    }
+    /* rounded wedge extruded along y: a sharp core wedge with its apex at the
+     * edge-circle centre, offset outward by the edge radius.  Rake face
+     * direction t1 (up), flank face direction t2 (back, rising by the
+     * clearance angle); outward normals n1 (+x side), n2 (below). */
+    double sg = sin(p->tool_rake), cg = cos(p->tool_rake);
+    double sa = sin(p->tool_clear), ca = cos(p->tool_clear);
+    double t1x = -sg, t1z = cg, n1x = cg, n1z = sg;
+    double t2x = -ca, t2z = sa, n2x = -sa, n2z = -ca;
+    double d1 = n1x * qx + n1z * qz, d2 = n2x * qx + n2z * qz;
+    double core;
+    if (d1 <= 0.0 && d2 <= 0.0) {
+        if (d1 >= d2) { core = d1; nrm[0] = n1x; nrm[2] = n1z; }
+        else { core = d2; nrm[0] = n2x; nrm[2] = n2z; }
+    } else {
+        double s1 = qx * t1x + qz * t1z; if (s1 < 0.0) s1 = 0.0;
+        double s2 = qx * t2x + qz * t2z; if (s2 < 0.0) s2 = 0.0;
+        double e1x = qx - s1 * t1x, e1z = qz - s1 * t1z;
+        double e2x = qx - s2 * t2x, e2z = qz - s2 * t2z;
+        double l1 = sqrt(e1x * e1x + e1z * e1z), l2 = sqrt(e2x * e2x + e2z * e2z);
+        if (l1 <= l2) { core = l1; if (l1 > 0) { nrm[0] = e1x / l1; nrm[2] = e1z / l1; } else { nrm[0] = n1x; nrm[2] = n1z; } }
+        else { core = l2; if (l2 > 0) { nrm[0] = e2x / l2; nrm[2] = e2z / l2; } else { nrm[0] = n2x; nrm[2] = n2z; } }
+    }
+    nrm[1] = 0.0;
+    return core - p->tool_r;
+}
+
+double orc_tool_sdf(const orc_params *p, const double pr[3], double x, double y, double z) {
+    double n[3];
+    return tool_sdf_n(p, pr, x, y, z, n);
+}
+
+/* ------------------------------------------------------ constitutive update */
+
+static double jc_flow(const orc_params *p, double eps, double rate_term, double th_term) {
+    return (p->A + p->B * pow(eps, p->n)) * rate_term * th_term;
+}
+
+/* Consistent return (extension): solve q - 3 mu dg = Y(eps + dg) for dg in
+ * [0, q/(3 mu)] by Newton steps safeguarded with bisection, rate and
+ * temperature frozen at the step start.  Returns 0 on convergence. */
+static int newton_return(const orc_params *p, double q, double mu, double eps0, double rt, double tt, double *dg_out) {
+    double lo = 0.0, hi = q / (3.0 * mu);
+    double x = (q - jc_flow(p, eps0, rt, tt)) / (3.0 * mu);
+    if (!(x > lo)) x = 0.5 * (lo + hi);
+    if (x > hi) x = hi;
+    double tol = p->newton_tol * q;
+    int maxit = p->newton_maxit > 0 ? p->newton_maxit : 60;
+    for (int it = 0; it < maxit; ++it) {
+        double e = eps0 + x;
+        double fx = q - 3.0 * mu * x - jc_flow(p, e, rt, tt);
+        if (fabs(fx) <= tol) { *dg_out = x; return 0; }
+        if (fx > 0.0) lo = x; else hi = x;
+        double dY = (e > 0.0) ? p->B * p->n * pow(e, p->n - 1.0) * rt * tt : INFINITY;
+        double d = -3.0 * mu - dY;
+        double xn = x - fx / d;
+        if (!(xn > lo && xn < hi)) xn = 0.5 * (lo + hi);
+        if (hi - lo <= 1e-15 * hi) { *dg_out = xn; return 0; }
+        x = xn;
+    }
+    *dg_out = x;
+    return 1;
+}
+
+/* ------------------------------------------------------------ step kernels */
+
+/* lodClassifyKernel, src/MPMSolver.cu:656-676 (ACTIVE/CHIP only). */
+static void lod_classify(const orc_params *p, orc_state *s, const double tip[3]) {
+    for (int i = 0; i < s->n; ++i) {
+        if (s->status[i] != ORC_ACTIVE && s->status[i] != ORC_CHIP) continue;
+        double dx = s->x[i] - tip[0], dy = s->y[i] - tip[1], dz = s->z[i] - tip[2];
+        double d = sqrt(dx * dx + dy * dy + dz * dz);
+        s->lod[i] = (d <= p->lod_active_r) ? 0 : (d <= p->lod_near_r ? 1 : 2);
+    }
+}
+
+/* p2gKernel, src/MPMSolver.cu:123-422. */
+static int p2g(const orc_params *p, orc_state *s, double *g, int nthreads) {
+    const int64_t nn = nnodes(p);
+    const double invDx = 1.0 / p->dx;
+    const double mu = p->E / (2.0 * (1.0 + p->nu));
+    const double lambda = p->E * p->nu / ((1.0 + p->nu) * (1.0 - 2.0 * p->nu));
+    const int atomic = nthreads > 1;
+    int err = 0;
+#pragma omp parallel for num_threads(nthreads) schedule(static) reduction(| : err) if (nthreads > 1)
+    for (int ip = 0; ip < s->n; ++ip) {
+        if (s->status[ip] == ORC_INACTIVE) continue;
+        /* kill zone, :130-139 */
+        int cx = (int)floor((s->x[ip] - p->ox) * invDx);
+        int cy = (int)floor((s->y[ip] - p->oy) * invDx);
+        int cz = (int)floor((s->z[ip] - p->oz) * invDx);
+        if (cx < 1 || cx >= p->nx - 2 || cy < 1 || cy >= p->ny - 2 || cz < 1 || cz >= p->nz - 2) {
+            s->status[ip] = ORC_INACTIVE;
+            continue;
+        }
+        int skipStress = (s->lod[ip] == 2);
+        int isFixed = (s->status[ip] == ORC_FIXED);
+        int isChip = (s->status[ip] == ORC_CHIP);
+        if (isFixed || isChip) skipStress = 1;
+        int bx, by, bz;
+        double wx[3], wy[3], wz[3], dwx[3], dwy[3], dwz[3];
+        weights(s->x[ip] - p->ox, invDx, &bx, wx, dwx);
+        weights(s->y[ip] - p->oy, invDx, &by, wy, dwy);
+        weights(s->z[ip] - p->oz, invDx, &bz, wz, dwz);
+
+        double sigma[9] = {0};
+        double V0 = s->vol[ip];
+        double J = 1.0;
+        if (!skipStress && s->status[ip] == ORC_ACTIVE) {
+            double *F = s->F + 9 * (int64_t)ip, *Fp = s->Fp + 9 * (int64_t)ip;
+            double *bs = s->bs + 6 * (int64_t)ip;
+            double invFp[9], Fe[9], Bm[9];
+            inv3(Fp, invFp);
+            mul3(F, invFp, Fe);
+            J = det3(Fe);
+            if (J < 0.9) J = 0.9;          /* :174-175 */
+            if (J > 1.1) J = 1.1;
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j)
+                    Bm[i * 3 + j] = Fe[i * 3 + 0] * Fe[j * 3 + 0] + Fe[i * 3 + 1] * Fe[j * 3 + 1] + Fe[i * 3 + 2] * Fe[j * 3 + 2];
+            /* sigma = mu/J (B - I) + lambda (J - 1) I, :192-200 */
+            double Js = fmax(J, 1e-12), Jpow = Js - 1.0, muJ = mu / Js;
+            for (int i = 0; i < 9; ++i) {
+                sigma[i] = muJ * Bm[i];
+                if (i % 4 == 0) sigma[i] += lambda * Jpow - muJ;
+            }
+            /* Johnson-Cook return, :205-360 */
+            double tr = sigma[0] + sigma[4] + sigma[8];
+            double sd[9];
+            for (int i = 0; i < 9; ++i) sd[i] = sigma[i];
+            sd[0] -= tr / 3.0; sd[4] -= tr / 3.0; sd[8] -= tr / 3.0;
+            double ex = sd[0] - bs[0], ey = sd[4] - bs[1], ez = sd[8] - bs[2];
+            double exy = sd[1] - bs[3], exz = sd[2] - bs[4], eyz = sd[5] - bs[5];
+            double q = sqrt(1.5 * (ex * ex + ey * ey + ez * ez + 2.0 * (exy * exy + exz * exz + eyz * eyz)));
+            double Ts = (s->T[ip] - p->Tamb) / fmax(p->Tm - p->Tamb, 1.0);
+            if (Ts < 0) Ts = 0;
+            if (Ts > 1) Ts = 1;
+            double es = fmax(s->edot[ip] / fmax(p->edot0, 1e-12), 1e-5);
+            double rt = 1.0 + p->C * log(es), tt = 1.0 - pow(Ts, p->m);
+            double Y = (p->A + p->B * pow(s->eps[ip], p->n)) * rt * tt;
+            double dEps = 0.0;
+            if (q > Y && q > 1e-12) {
+                double Yr = Y;
+                if (p->plasticity_mode == ORC_PLAST_NEWTON) {
+                    double dg;
+                    if (newton_return(p, q, mu, s->eps[ip], rt, tt, &dg)) err |= 1;
+                    dEps = dg;
+                    Yr = q - 3.0 * mu * dg;
+                } else {
+                    dEps = (q - Y) / fmax(3.0 * mu, 1e-12);
+                    if (dEps > p->deps_cap) dEps = p->deps_cap;
+                }
+                double scale = Yr / q;
+                sd[0] = bs[0] + scale * ex; sd[4] = bs[1] + scale * ey; sd[8] = bs[2] + scale * ez;
+                sd[1] = bs[3] + scale * exy; sd[2] = bs[4] + scale * exz; sd[5] = bs[5] + scale * eyz;
+                for (int i = 0; i < 9; ++i) {
+                    sigma[i] = sd[i];
+                    if (i % 4 == 0) sigma[i] += tr / 3.0;
+                }
+                if (dEps > 0) {
+                    if (p->Hkin > 0.0) {     /* :259-267 */
+                        double ns = p->Hkin * dEps / q;
+                        bs[0] += ns * ex; bs[1] += ns * ey; bs[2] += ns * ez;
+                        bs[3] += ns * exy; bs[4] += ns * exz; bs[5] += ns * eyz;
+                    }
+                    s->eps[ip] += dEps;
+                    /* Fp <- (I + 1.5 dEps/|s| s) Fp / cbrt(det), :277-302 */
+                    double sn = sqrt(sd[0] * sd[0] + sd[4] * sd[4] + sd[8] * sd[8] + 2.0 * (sd[1] * sd[1] + sd[2] * sd[2] + sd[5] * sd[5]));
+                    double al = (sn > 1e-12) ? (1.5 * dEps / sn) : 0.0;
+                    double Ia[9], nFp[9];
+                    for (int i = 0; i < 9; ++i) Ia[i] = al * sd[i];
+                    Ia[0] += 1.0; Ia[4] += 1.0; Ia[8] += 1.0;
+                    for (int i = 0; i < 3; ++i)
+                        for (int j = 0; j < 3; ++j) {
+                            nFp[i * 3 + j] = 0;
+                            for (int k = 0; k < 3; ++k) nFp[i * 3 + j] += Ia[i * 3 + k] * Fp[k * 3 + j];
+                        }
+                    double dFp = nFp[0] * (nFp[4] * nFp[8] - nFp[5] * nFp[7]) - nFp[1] * (nFp[3] * nFp[8] - nFp[5] * nFp[6]) +
+                                 nFp[2] * (nFp[3] * nFp[7] - nFp[4] * nFp[6]);
+                    double cb = cbrt(fmax(dFp, 1e-12));
+                    for (int i = 0; i < 9; ++i) Fp[i] = nFp[i] / cb;
+                    /* plastic-work heating, :310-321 */
+                    double dT = p->beta * Yr * dEps / fmax(p->rho_phys * p->cp, 1e-12);
+                    if (dT > p->dT_cap) dT = p->dT_cap;
+                    s->T[ip] += dT;
+                    if (s->T[ip] > p->Tm) s->T[ip] = p->Tm;
+                    /* JC damage, :329-358 */
+                    double tri = (tr / 3.0) / fmax(q, 1e-12);
+                    double ef = (p->D1 + p->D2 * exp(p->D3 * tri)) * (1.0 + p->D4 * log(fmax(es, 1.0))) * (1.0 + p->D5 * Ts);
+                    if (ef > 1e-12) {
+                        s->D[ip] += dEps / ef;
+                        if (s->D[ip] > 0.7 * p->Dth) {
+                            double dg = (p->Dth - s->D[ip]) / (p->Dth * 0.3);
+                            dg = fmax(0.0, fmin(1.0, dg));
+                            for (int i = 0; i < 9; ++i) sigma[i] *= dg;
+                            s->sres[ip] = fmax(s->sres[ip], sqrt(1.5 * (sd[0] * sd[0] + sd[4] * sd[4] + sd[8] * sd[8] +
+                                                                         2.0 * (sd[1] * sd[1] + sd[2] * sd[2] + sd[5] * sd[5]))));
+                        }
+                        if (s->D[ip] >= p->Dth) {
+                            s->status[ip] = ORC_CHIP;
+                            skipStress = 1;
+                        }
+                    }
+                }
+            }
+            double *sg = s->sig + 6 * (int64_t)ip;  /* :363-364 */
+            sg[0] = sigma[0]; sg[1] = sigma[4]; sg[2] = sigma[8];
+            sg[3] = sigma[1]; sg[4] = sigma[2]; sg[5] = sigma[5];
+        }
+        /* APIC scatter, :370-421 */
+        const double *Cp = s->C + 9 * (int64_t)ip;
+        const double m = s->mass[ip];
+        const double efx = s->extf ? s->extf[3 * (int64_t)ip] : 0.0;
+        const double efy = s->extf ? s->extf[3 * (int64_t)ip + 1] : 0.0;
+        const double efz = s->extf ? s->extf[3 * (int64_t)ip + 2] : 0.0;
+        for (int i = 0; i < 3; ++i) {
+            int gx = bx + i;
+            if (gx < 0 || gx >= p->nx) continue;
+            for (int j = 0; j < 3; ++j) {
+                int gy = by + j;
+                if (gy < 0 || gy >= p->ny) continue;
+                for (int k = 0; k < 3; ++k) {
+                    int gz = bz + k;
+                    if (gz < 0 || gz >= p->nz) continue;
+                    double w = wx[i] * wy[j] * wz[k];
+                    double gdx = dwx[i] * wy[j] * wz[k], gdy = wx[i] * dwy[j] * wz[k], gdz = wx[i] * wy[j] * dwz[k];
+                    int64_t gi = gx + (int64_t)p->nx * (gy + (int64_t)p->ny * gz);
+                    double dpx = (gx * p->dx + p->ox) - s->x[ip];
+                    double dpy = (gy * p->dx + p->oy) - s->y[ip];
+                    double dpz = (gz * p->dx + p->oz) - s->z[ip];
+                    double ax = Cp[0] * dpx + Cp[1] * dpy + Cp[2] * dpz;
+                    double ay = Cp[3] * dpx + Cp[4] * dpy + Cp[5] * dpz;
+                    double az = Cp[6] * dpx + Cp[7] * dpy + Cp[8] * dpz;
+                    gadd(&g[G_M * nn + gi], w * m, atomic);
+                    if (!isFixed) {
+                        gadd(&g[G_PX * nn + gi], w * m * (s->vx[ip] + ax), atomic);
+                        gadd(&g[G_PY * nn + gi], w * m * (s->vy[ip] + ay), atomic);
+                        gadd(&g[G_PZ * nn + gi], w * m * (s->vz[ip] + az), atomic);
+                    }
+                    double fxi = 0, fyi = 0, fzi = 0;
+                    if (!skipStress) {
+                        fxi = -V0 * J * (sigma[0] * gdx + sigma[1] * gdy + sigma[2] * gdz);
+                        fyi = -V0 * J * (sigma[3] * gdx + sigma[4] * gdy + sigma[5] * gdz);
+                        fzi = -V0 * J * (sigma[6] * gdx + sigma[7] * gdy + sigma[8] * gdz);
+                    }
+                    gadd(&g[G_FX * nn + gi], fxi + w * efx, atomic);
+                    gadd(&g[G_FY * nn + gi], fyi + w * efy, atomic);
+                    gadd(&g[G_FZ * nn + gi], fzi + w * efz, atomic);
+                }
+            }
+        }
+    }
+    return err;
+}
+
+/* updateGridKernel (:424-442), applyFixtureBCKernel (:82-110) and the tool
+ * boundary: rasterizeToolKernel + applyGridCollisionKernel (:444-492) or the
+ * analytic SDF of this build. */
+static void grid_update(const orc_params *p, double *g, double dt, const orc_tool_samples *tool, const double pr[3]) {
+    const int64_t nn = nnodes(p);
+    const double thr = p->mass_threshold;
+    for (int64_t i = 0; i < nn; ++i) {
+        if (g[G_M * nn + i] > thr) {
+            g[G_PZ * nn + i] += g[G_M * nn + i] * p->gravity_z * dt;
+            g[G_PX * nn + i] += g[G_FX * nn + i] * dt;
+            g[G_PY * nn + i] += g[G_FY * nn + i] * dt;
+            g[G_PZ * nn + i] += g[G_FZ * nn + i] * dt;
+            g[G_VX * nn + i] = g[G_PX * nn + i] / g[G_M * nn + i];
+            g[G_VY * nn + i] = g[G_PY * nn + i] / g[G_M * nn + i];
+            g[G_VZ * nn + i] = g[G_PZ * nn + i] / g[G_M * nn + i];
+        }
+    }
+    if (p->fixture_thickness > 0.0) {
+        const int64_t nxy = (int64_t)p->nx * p->ny;
+        for (int64_t i = 0; i < nn; ++i) {
+            int gz = (int)(i / nxy);
+            double wz = gz * p->dx + p->oz;
+            double zr = (wz - p->oz) / p->fixture_thickness;
+            if (zr <= 1.0) {
+                if (gz == 0) {
+                    g[G_VX * nn + i] = 0.0; g[G_VY * nn + i] = 0.0; g[G_VZ * nn + i] = 0.0;
+                } else if (zr > 0.0) {
+                    double sgm = p->fixture_damping * (1.0 - zr) * (1.0 - zr);
+                    double f = 1.0 / (1.0 + sgm * dt);
+                    g[G_VX * nn + i] *= f; g[G_VY * nn + i] *= f; g[G_VZ * nn + i] *= f;
+                }
+            }
+        }
+    }
+    if (p->tool_mode == ORC_TOOL_RASTER && tool && tool->n > 0) {
+        const double invDx = 1.0 / p->dx;
+        for (int t = 0; t < tool->n; ++t) {
+            double sx = pr[0] + tool->ox[t], sy = pr[1] + tool->oy[t], sz = pr[2] + tool->oz[t];
+            int gx = (int)round((sx - p->ox) * invDx);
+            int gy = (int)round((sy - p->oy) * invDx);
+            int gz = (int)round((sz - p->oz) * invDx);
+            for (int a = 0; a < 2; ++a) {
+                int cx = gx + a;
+                if (cx < 0 || cx >= p->nx) continue;
+                for (int b = 0; b < 2; ++b) {
+                    int cy = gy + b;
+                    if (cy < 0 || cy >= p->ny) continue;
+                    for (int c = 0; c < 2; ++c) {
+                        int cz = gz + c;
+                        if (cz < 0 || cz >= p->nz) continue;
+                        int64_t gi = cx + (int64_t)p->nx * (cy + (int64_t)p->ny * cz);
+                        g[G_TOOL * nn + gi] = 1.0;
+                        g[G_TVX * nn + gi] = p->tool_v[0];
+                        g[G_TVY * nn + gi] = p->tool_v[1];
+                        g[G_TVZ * nn + gi] = p->tool_v[2];
+                    }
+                }
+            }
+        }
+        for (int64_t i = 0; i < nn; ++i) {
+            if (g[G_M * nn + i] > thr && g[G_TOOL * nn + i] == 1.0) {
+                g[G_VX * nn + i] = g[G_TVX * nn + i];
+                g[G_VY * nn + i] = g[G_TVY * nn + i];
+                g[G_VZ * nn + i] = g[G_TVZ * nn + i];
+                g[G_PX * nn + i] = g[G_M * nn + i] * g[G_VX * nn + i];
+                g[G_PY * nn + i] = g[G_M * nn + i] * g[G_VY * nn + i];
+                g[G_PZ * nn + i] = g[G_M * nn + i] * g[G_VZ * nn + i];
+            }
+        }
+    } else if (p->tool_mode == ORC_TOOL_SDF_STICKY || p->tool_mode == ORC_TOOL_SDF_SLIP) {
+        for (int64_t i = 0; i < nn; ++i) {
+            if (!(g[G_M * nn + i] > thr)) continue;
+            int gx = (int)(i % p->nx), gy = (int)((i / p->nx) % p->ny), gz = (int)(i / ((int64_t)p->nx * p->ny));
+            double nrm[3];
+            double phi = tool_sdf_n(p, pr, gx * p->dx + p->ox, gy * p->dx + p->oy, gz * p->dx + p->oz, nrm);
+            if (phi > 0.0) continue;
+            if (p->tool_mode == ORC_TOOL_SDF_STICKY) {
+                g[G_VX * nn + i] = p->tool_v[0];
+                g[G_VY * nn + i] = p->tool_v[1];
+                g[G_VZ * nn + i] = p->tool_v[2];
+            } else {
+                double rx = g[G_VX * nn + i] - p->tool_v[0];
+                double ry = g[G_VY * nn + i] - p->tool_v[1];
+                double rz = g[G_VZ * nn + i] - p->tool_v[2];
+                double vn = rx * nrm[0] + ry * nrm[1] + rz * nrm[2];
+                if (vn < 0.0) {
+                    g[G_VX * nn + i] -= vn * nrm[0];
+                    g[G_VY * nn + i] -= vn * nrm[1];
+                    g[G_VZ * nn + i] -= vn * nrm[2];
+                }
+            }
+        }
+    }
+}
+
+/* g2pKernel, src/MPMSolver.cu:506-605. */
+static void g2p(const orc_params *p, orc_state *s, const double *g, double dt, int nthreads) {
+    const int64_t nn = nnodes(p);
+    const double invDx = 1.0 / p->dx;
+    (void)nthreads;
+#pragma omp parallel for num_threads(nthreads) schedule(static) if (nthreads > 1)
+    for (int ip = 0; ip < s->n; ++ip) {
+        if (s->status[ip] == ORC_INACTIVE) continue;
+        if (s->status[ip] == ORC_FIXED) {
+            s->vx[ip] = 0; s->vy[ip] = 0; s->vz[ip] = 0;
+            continue;
+        }
+        int bx, by, bz;
+        double wx[3], wy[3], wz[3], dwx[3], dwy[3], dwz[3];
+        weights(s->x[ip] - p->ox, invDx, &bx, wx, dwx);
+        weights(s->y[ip] - p->oy, invDx, &by, wy, dwy);
+        weights(s->z[ip] - p->oz, invDx, &bz, wz, dwz);
+        double vx = 0, vy = 0, vz = 0, Bm[9] = {0}, L[9] = {0};
+        for (int i = 0; i < 3; ++i) {
+            int gx = bx + i;
+            if (gx < 0 || gx >= p->nx) continue;
+            for (int j = 0; j < 3; ++j) {
+                int gy = by + j;
+                if (gy < 0 || gy >= p->ny) continue;
+                for (int k = 0; k < 3; ++k) {
+                    int gz = bz + k;
+                    if (gz < 0 || gz >= p->nz) continue;
+                    int64_t gi = gx + (int64_t)p->nx * (gy + (int64_t)p->ny * gz);
+                    if (g[G_M * nn + gi] < p->mass_threshold) continue;
+                    double w = wx[i] * wy[j] * wz[k];
+                    double gdx = dwx[i] * wy[j] * wz[k], gdy = wx[i] * dwy[j] * wz[k], gdz = wx[i] * wy[j] * dwz[k];
+                    double gvx = g[G_VX * nn + gi], gvy = g[G_VY * nn + gi], gvz = g[G_VZ * nn + gi];
+                    vx += w * gvx; vy += w * gvy; vz += w * gvz;
+                    double dpx = (gx * p->dx + p->ox) - s->x[ip];
+                    double dpy = (gy * p->dx + p->oy) - s->y[ip];
+                    double dpz = (gz * p->dx + p->oz) - s->z[ip];
+                    Bm[0] += w * gvx * dpx; Bm[1] += w * gvx * dpy; Bm[2] += w * gvx * dpz;
+                    Bm[3] += w * gvy * dpx; Bm[4] += w * gvy * dpy; Bm[5] += w * gvy * dpz;
+                    Bm[6] += w * gvz * dpx; Bm[7] += w * gvz * dpy; Bm[8] += w * gvz * dpz;
+                    L[0] += gvx * gdx; L[1] += gvx * gdy; L[2] += gvx * gdz;
+                    L[3] += gvy * gdx; L[4] += gvy * gdy; L[5] += gvy * gdz;
+                    L[6] += gvz * gdx; L[7] += gvz * gdy; L[8] += gvz * gdz;
+                }
+            }
+        }
+        s->vx[ip] = vx; s->vy[ip] = vy; s->vz[ip] = vz;
+        s->x[ip] += vx * dt; s->y[ip] += vy * dt; s->z[ip] += vz * dt;
+        if (s->status[ip] == ORC_CHIP) { s->edot[ip] = 0; continue; }
+        double *Cp = s->C + 9 * (int64_t)ip;
+        double Dinv = p->apic_dinv_factor * invDx * invDx;
+        for (int i = 0; i < 9; ++i) Cp[i] = Bm[i] * Dinv;
+        if (s->lod[ip] == 2) { for (int i = 0; i < 9; ++i) Cp[i] = 0.0; }
+        else { for (int i = 0; i < 9; ++i) Cp[i] *= p->apic_decay; }
+        double IL[9], Fn[9], *F = s->F + 9 * (int64_t)ip;
+        for (int i = 0; i < 9; ++i) { IL[i] = L[i] * dt; if (i % 4 == 0) IL[i] += 1.0; }
+        mul3(IL, F, Fn);
+        for (int i = 0; i < 9; ++i) F[i] = Fn[i];
+        s->edot[ip] = sqrt(2.0 / 3.0 * (L[0] * L[0] + L[4] * L[4] + L[8] * L[8] + 0.5 * (L[1] + L[3]) * (L[1] + L[3]) +
+                                        0.5 * (L[2] + L[6]) * (L[2] + L[6]) + 0.5 * (L[5] + L[7]) * (L[5] + L[7])));
+    }
+}
+
+/* chipFractureAndSeparationKernel, src/MPMSolver.cu:1002-1060. */
+static void chip_separation(const orc_params *p, orc_state *s, double tipZ) {
+    const double Dth = p->Dth;
+    for (int i = 0; i < s->n; ++i) {
+        if (s->status[i] == ORC_INACTIVE) continue;
+        if (s->status[i] == ORC_ACTIVE) {
+            if (s->z[i] < tipZ - p->dx * 1.5 && s->D[i] > 1e-6) {
+                double *sg = s->sig + 6 * (int64_t)i;
+                s->status[i] = ORC_CHIP;
+                s->sres[i] = fmax(s->sres[i], sqrt(sg[0] * sg[0] + sg[1] * sg[1] + sg[2] * sg[2]));
+                for (int k = 0; k < 6; ++k) sg[k] = 0.0;
+                s->D[i] = fmax(s->D[i], Dth);
+            }
+            continue;
+        }
+        if (s->status[i] == ORC_CHIP) {
+            if (s->D[i] < Dth * 1.5) continue;
+            uint32_t seed = (uint32_t)s->id[i] * 2654435761U;
+            double rx = (double)((seed >> 16) & 0xFF) / 255.0 - 0.5;
+            double ry = (double)((seed >> 8) & 0xFF) / 255.0 - 0.5;
+            double rz = (double)(seed & 0xFF) / 255.0 - 0.5;
+            double sp = sqrt(s->vx[i] * s->vx[i] + s->vy[i] * s->vy[i] + s->vz[i] * s->vz[i]);
+            double pm = sp * 0.3 + 0.5;
+            s->vx[i] += rx * pm; s->vy[i] += ry * pm; s->vz[i] += rz * pm;
+            s->D[i] = Dth * 0.5;
+        }
+    }
+}
+
+int orc_step(const orc_params *p, orc_state *s, const orc_tool_samples *tool, double *grid, double dt, int32_t nsteps,
+             int64_t step0, double t0, int32_t nthreads) {
+    int err = 0;
+    if (nthreads < 1) nthreads = 1;
+    const int64_t ng = orc_grid_doubles(p);
+    for (int32_t k = 0; k < nsteps; ++k) {
+        const double t = t0 + (double)k * dt;
+        double pr[3], tip[3];
+        for (int d = 0; d < 3; ++d) pr[d] = p->tool_p0[d] + p->tool_v[d] * t;
+        tip[0] = pr[0]; tip[1] = pr[1]; tip[2] = pr[2] + p->tool_tip_dz;
+        if (p->lod_enabled) lod_classify(p, s, tip);
+        memset(grid, 0, sizeof(double) * (size_t)ng);                 /* resetGridKernel :112 */
+        err |= p2g(p, s, grid, nthreads);
+        grid_update(p, grid, dt, tool, pr);
+        g2p(p, s, grid, dt, nthreads);
+        if (s->extf) memset(s->extf, 0, sizeof(double) * 3 * (size_t)s->n);  /* :682-688 */
+        const int64_t cnt = step0 + k;
+        if (p->chip_sep_enabled && p->chip_every > 0 && (cnt % p->chip_every) == 0) chip_separation(p, s, tip[2]);
+    }
+    return err;
+}
+
+/* ---------------------------------------------------------------- metrics */
+
+/* Reference-compatible stats: computeParticleStatsKernel (:729-788) over
+ * ACTIVE and CHIP, initial values 0 (syncMetrics :1242-1246).  Conservation
+ * metrics (this build) over every particle that is not INACTIVE. */
+void orc_metrics_compute(const orc_params *p, const orc_state *s, orc_metrics *o) {
+    memset(o, 0, sizeof(*o));
+    const double mu = p->E / (2.0 * (1.0 + p->nu));
+    const double K = p->E / (3.0 * (1.0 - 2.0 * p->nu));
+    for (int d = 0; d < 3; ++d) { o->bmin[d] = INFINITY; o->bmax[d] = -INFINITY; }
+    for (int i = 0; i < s->n; ++i) {
+        int st = s->status[i];
+        if (st == ORC_INACTIVE) { o->n_inactive++; continue; }
+        if (st == ORC_ACTIVE) o->n_active++;
+        else if (st == ORC_CHIP) o->n_chip++;
+        else if (st == ORC_FIXED) o->n_fixed++;
+        const double *sg = s->sig + 6 * (int64_t)i;
+        double tr = sg[0] + sg[1] + sg[2];
+        double sxx = sg[0] - tr / 3.0, syy = sg[1] - tr / 3.0, szz = sg[2] - tr / 3.0;
+        double vm = sqrt(1.5 * (sxx * sxx + syy * syy + szz * szz + 2.0 * (sg[3] * sg[3] + sg[4] * sg[4] + sg[5] * sg[5])));
+        double m = s->mass[i];
+        double v2 = s->vx[i] * s->vx[i] + s->vy[i] * s->vy[i] + s->vz[i] * s->vz[i];
+        o->mass += m;
+        o->px += m * s->vx[i]; o->py += m * s->vy[i]; o->pz += m * s->vz[i];
+        o->kinetic += 0.5 * m * v2;
+        double pr = tr / 3.0;
+        o->internal_elastic += s->vol[i] * (vm * vm / (6.0 * mu) + pr * pr / (2.0 * K));
+        o->thermal += p->rho_phys * s->vol[i] * p->cp * (s->T[i] - p->Tamb);
+        if (s->T[i] > o->max_T) o->max_T = s->T[i];
+        if (vm > o->max_vm) o->max_vm = vm;
+        if (s->eps[i] > o->max_eps) o->max_eps = s->eps[i];
+        o->sum_eps += s->eps[i];
+        if (st == ORC_ACTIVE || st == ORC_CHIP) {
+            if (vm > o->ref_max_stress) o->ref_max_stress = vm;
+            if (s->T[i] > o->ref_max_T) o->ref_max_T = s->T[i];
+            o->ref_kinetic += 0.5 * m * v2;
+            o->ref_internal += (vm * vm * m) / (6.0 * 80e9) + s->vol[i] * s->eps[i] * vm;
+            double xyz[3] = {s->x[i], s->y[i], s->z[i]};
+            for (int d = 0; d < 3; ++d) {
+                if (xyz[d] < o->bmin[d]) o->bmin[d] = xyz[d];
+                if (xyz[d] > o->bmax[d]) o->bmax[d] = xyz[d];
+            }
+        }
+    }
+}
+
+/* ---------------------------------------------------------------- Philox */
+
+static inline void mulhilo(uint32_t a, uint32_t b, uint32_t *hi, uint32_t *lo) {
+    uint64_t p = (uint64_t)a * (uint64_t)b;
+    *hi = (uint32_t)(p >> 32);
+    *lo = (uint32_t)p;
+}
+
+void orc_philox_uniform4(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, float out[4]) {
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0, lo0, hi1, lo1;
+        mulhilo(0xD2511F53u, c0, &hi0, &lo0);
+        mulhilo(0xCD9E8D57u, c2, &hi1, &lo1);
+        uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+    uint32_t c[4] = {c0, c1, c2, c3};
+    for (int i = 0; i < 4; ++i) out[i] = (float)(c[i] >> 8) * (1.0f / 16777216.0f);
+}

@@ -1,0 +1,137 @@
+/*
+ * mpm_oracle.h -- CPU FP64 restatement of the EdgePredict MPM workpiece step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the oracle that the CUDA path is checked
+ * against; it is never linked into, loaded by, or called from the product
+ * library.  Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline
+ * leg may use it.
+ *
+ * It follows the reference's engine-wired solver, src/MPMSolver.cu, kernel by
+ * kernel (citations per function in mpm_oracle.c), on plain SoA double
+ * arrays.  Beyond the reference it restates three extensions of this build
+ * with the same arithmetic that the CUDA path uses: an analytic tool SDF
+ * boundary (sticky and slip), a consistent Newton return for Johnson-Cook
+ * plasticity, and FP64 conservation metrics.
+ *
+ * Parity pin: the reference ships no tests or golden vectors.  The oracle is
+ * pinned against the reference's own CUDA kernels (built from its sources by
+ * oracle/Makefile into oracle/_ref/) through the fixtures in tests/golden/.
+ */
+#ifndef MPM_ORACLE_H
+#define MPM_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Particle status codes: include/Types.h:37-43 (ParticleStatus). */
+enum { ORC_ACTIVE = 0, ORC_INACTIVE = 1, ORC_CHIP = 2, ORC_BOUNDARY = 3, ORC_FIXED = 4 };
+
+/* Tool boundary modes. */
+enum {
+    ORC_TOOL_NONE = 0,
+    ORC_TOOL_RASTER = 1,      /* reference: rasterizeToolKernel + applyGridCollisionKernel */
+    ORC_TOOL_SDF_STICKY = 2,  /* analytic SDF, nodes inside take the tool velocity */
+    ORC_TOOL_SDF_SLIP = 3     /* analytic SDF, approaching normal velocity removed */
+};
+enum { ORC_SHAPE_CYLINDER_Y = 0, ORC_SHAPE_WEDGE_Y = 1 };
+enum { ORC_PLAST_EXPLICIT = 0, ORC_PLAST_NEWTON = 1 };
+
+typedef struct orc_params {
+    /* background grid: node (i,j,k) sits at origin + (i,j,k)*dx */
+    int32_t nx, ny, nz;
+    int32_t _pad0;
+    double dx;
+    double ox, oy, oz;
+    /* elasticity and heat */
+    double E, nu;
+    double rho_phys, cp, beta, Tm, Tamb;
+    /* Johnson-Cook flow stress and kinematic hardening */
+    double A, B, n, C, m, edot0, Hkin;
+    /* Johnson-Cook damage */
+    double D1, D2, D3, D4, D5, Dth;
+    /* grid boundary conditions */
+    double fixture_thickness, fixture_damping, gravity_z, mass_threshold;
+    /* APIC: C = factor/dx^2 * B, then C *= decay */
+    double apic_dinv_factor, apic_decay;
+    /* level of detail (src/MPMSolver.cu:656-676) */
+    int32_t lod_enabled;
+    int32_t plasticity_mode;
+    double lod_active_r, lod_near_r;
+    /* explicit-return safety caps (src/MPMSolver.cu:255, :315) */
+    double deps_cap, dT_cap;
+    /* chip separation every `chip_every` steps (src/MPMSolver.cu:1160) */
+    int32_t chip_sep_enabled, chip_every;
+    /* rigid tool: reference point p(t) = p0 + v*t */
+    int32_t tool_mode, tool_shape;
+    double tool_p0[3];
+    double tool_v[3];
+    double tool_r;          /* cylinder radius, or wedge edge radius */
+    double tool_rake;       /* wedge rake angle (rad) */
+    double tool_clear;      /* wedge clearance angle (rad) */
+    double tool_tip_dz;     /* tool tip z relative to the reference point */
+    double newton_tol;      /* relative residual for the Newton return */
+    int32_t newton_maxit;
+    int32_t _pad1;
+} orc_params;
+
+/* Particle state, SoA, one entry per particle (matrices row-major [n][9],
+ * symmetric tensors [n][6] as xx,yy,zz,xy,xz,yz). */
+typedef struct orc_state {
+    int32_t n;
+    int32_t _pad;
+    double *x, *y, *z;
+    double *vx, *vy, *vz;
+    double *F, *Fp, *C;
+    double *sig, *bs;
+    double *eps, *edot, *T, *D, *sres;
+    double *mass, *vol;
+    double *extf;            /* [n][3] or NULL: applied for one step, then zeroed */
+    int32_t *status, *id;
+    int32_t *lod;            /* [n] LOD zone, persists like MPMParticle::lodZone */
+} orc_state;
+
+/* Rasterised tool samples: offsets from the tool reference point. */
+typedef struct orc_tool_samples {
+    int32_t n;
+    int32_t _pad;
+    const double *ox, *oy, *oz;
+} orc_tool_samples;
+
+/* Conservation and reference-compatible metrics (all FP64). */
+typedef struct orc_metrics {
+    double mass, px, py, pz, kinetic, internal_elastic, thermal;
+    double max_T, max_vm, max_eps, sum_eps;
+    double ref_max_stress, ref_max_T, ref_kinetic, ref_internal;
+    int64_t n_active, n_chip, n_fixed, n_inactive;
+    double bmin[3], bmax[3];
+} orc_metrics;
+
+/* Size in doubles of the grid scratch that orc_step needs. */
+int64_t orc_grid_doubles(const orc_params *p);
+
+/* Advance `nsteps` steps of size dt.  step0 is the solver's step counter
+ * before the first step (chip separation runs when the counter is a
+ * multiple of chip_every) and t0 the simulation time.  grid is scratch of
+ * orc_grid_doubles() doubles.  Returns 0, or a nonzero error code (1: a
+ * Newton return did not converge). */
+int orc_step(const orc_params *p, orc_state *s, const orc_tool_samples *tool,
+             double *grid, double dt, int32_t nsteps, int64_t step0, double t0,
+             int32_t nthreads);
+
+/* Tool SDF at a world point for the tool reference point pr. */
+double orc_tool_sdf(const orc_params *p, const double pr[3], double x, double y, double z);
+
+void orc_metrics_compute(const orc_params *p, const orc_state *s, orc_metrics *out);
+
+/* Philox4x32-10 (Salmon et al., SC'11): 4 uniform floats in [0,1) per call,
+ * 24-bit resolution.  Used by the seeded workpiece generator. */
+void orc_philox_uniform4(uint32_t seed_lo, uint32_t seed_hi, uint32_t c0, uint32_t c1,
+                         uint32_t c2, uint32_t c3, float out[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

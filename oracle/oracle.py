@@ -1,0 +1,243 @@
+"""Python access to the test-only checkers built by oracle/Makefile.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline leg / reference arm.  Never imported by the product.
+
+  Oracle   -- liboracle_mpm.so, the CPU FP64 restatement (mpm_oracle.c)
+  RefKern  -- _ref/libmpm_ref.so, the reference's own CUDA kernels
+              (src/MPMSolver.cu compiled from its sources, GPU only)
+
+States are dicts of float64 numpy arrays keyed like mpm_particles_soa fields
+(x, y, z, vx, vy, vz, F[n,9], Fp[n,9], C[n,9], stress[n,6], backstress[n,6],
+plastic_strain, strain_rate, temperature, damage, residual_stress, status, id).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+from typing import Dict, Optional
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_LIB = HERE / "liboracle_mpm.so"
+REF_LIB = HERE / "_ref" / "libmpm_ref.so"
+
+_d, _i32, _i64, _vp = C.c_double, C.c_int32, C.c_int64, C.c_void_p
+TOOL_NONE, TOOL_RASTER, TOOL_SDF_STICKY, TOOL_SDF_SLIP = 0, 1, 2, 3
+
+
+class OrcParams(C.Structure):
+    _fields_ = [
+        ("nx", _i32), ("ny", _i32), ("nz", _i32), ("_pad0", _i32), ("dx", _d), ("ox", _d), ("oy", _d), ("oz", _d),
+        ("E", _d), ("nu", _d), ("rho_phys", _d), ("cp", _d), ("beta", _d), ("Tm", _d), ("Tamb", _d),
+        ("A", _d), ("B", _d), ("n", _d), ("C", _d), ("m", _d), ("edot0", _d), ("Hkin", _d),
+        ("D1", _d), ("D2", _d), ("D3", _d), ("D4", _d), ("D5", _d), ("Dth", _d),
+        ("fixture_thickness", _d), ("fixture_damping", _d), ("gravity_z", _d), ("mass_threshold", _d),
+        ("apic_dinv_factor", _d), ("apic_decay", _d),
+        ("lod_enabled", _i32), ("plasticity_mode", _i32), ("lod_active_r", _d), ("lod_near_r", _d),
+        ("deps_cap", _d), ("dT_cap", _d), ("chip_sep_enabled", _i32), ("chip_every", _i32),
+        ("tool_mode", _i32), ("tool_shape", _i32), ("tool_p0", _d * 3), ("tool_v", _d * 3), ("tool_r", _d),
+        ("tool_rake", _d), ("tool_clear", _d), ("tool_tip_dz", _d), ("newton_tol", _d), ("newton_maxit", _i32),
+        ("_pad1", _i32),
+    ]
+
+
+class OrcState(C.Structure):
+    _fields_ = [("n", _i32), ("_pad", _i32)] + [
+        (k, _vp) for k in ("x", "y", "z", "vx", "vy", "vz", "F", "Fp", "C", "sig", "bs", "eps", "edot", "T", "D",
+                           "sres", "mass", "vol", "extf", "status", "id", "lod")
+    ]
+
+
+class OrcTool(C.Structure):
+    _fields_ = [("n", _i32), ("_pad", _i32), ("ox", _vp), ("oy", _vp), ("oz", _vp)]
+
+
+class OrcMetrics(C.Structure):
+    _fields_ = [(k, _d) for k in ("mass", "px", "py", "pz", "kinetic", "internal_elastic", "thermal", "max_T",
+                                  "max_vm", "max_eps", "sum_eps", "ref_max_stress", "ref_max_T", "ref_kinetic",
+                                  "ref_internal")] + \
+               [(k, _i64) for k in ("n_active", "n_chip", "n_fixed", "n_inactive")] + \
+               [("bmin", _d * 3), ("bmax", _d * 3)]
+
+
+FIELD_MAP = [("x", "x", 1), ("y", "y", 1), ("z", "z", 1), ("vx", "vx", 1), ("vy", "vy", 1), ("vz", "vz", 1),
+             ("F", "F", 9), ("Fp", "Fp", 9), ("C", "C", 9), ("stress", "sig", 6), ("backstress", "bs", 6),
+             ("plastic_strain", "eps", 1), ("strain_rate", "edot", 1), ("temperature", "T", 1),
+             ("damage", "D", 1), ("residual_stress", "sres", 1)]
+
+
+def build(ref: bool = False) -> None:
+    """make -C oracle [ref]; the reference harness only when its sources exist."""
+    targets = ["all"]
+    if ref:
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
+
+
+def orc_params(case: dict) -> OrcParams:
+    p, t = case["params"], case["tool"]
+    o = OrcParams()
+    o.nx, o.ny, o.nz = p["nx"], p["ny"], p["nz"]
+    o.dx = p["dx"]
+    o.ox, o.oy, o.oz = p["origin"]
+    for k in ("E", "nu", "rho_phys", "cp", "beta", "Tm", "Tamb", "edot0", "D1", "D2", "D3", "D4", "D5",
+              "fixture_thickness", "fixture_damping", "gravity_z", "mass_threshold", "apic_dinv_factor",
+              "apic_decay", "lod_active_r", "lod_near_r", "deps_cap", "dT_cap", "newton_tol"):
+        setattr(o, k, float(p[k]))
+    o.A, o.B, o.n, o.C, o.m, o.Hkin = p["jc_A"], p["jc_B"], p["jc_n"], p["jc_C"], p["jc_m"], p["H_kin"]
+    o.Dth = p["D_th"]
+    o.lod_enabled = int(p["lod_enabled"])
+    o.plasticity_mode = int(p["plasticity"])
+    o.chip_every = int(p["chip_every"])
+    o.chip_sep_enabled = 1 if p["chip_every"] > 0 else 0
+    o.newton_maxit = int(p["newton_maxit"])
+    o.tool_mode = int(t.get("mode", TOOL_NONE))
+    o.tool_shape = int(t.get("shape", 0))
+    for i in range(3):
+        o.tool_p0[i] = t.get("position", (0, 0, 0))[i]
+        o.tool_v[i] = t.get("velocity", (0, 0, 0))[i]
+    o.tool_r = t.get("radius", 0.0)
+    o.tool_rake = t.get("rake", 0.0)
+    o.tool_clear = t.get("clearance", 0.0)
+    o.tool_tip_dz = t.get("tip_dz", 0.0)
+    return o
+
+
+class _Bound:
+    """Keeps numpy arrays alive while a C call uses them."""
+
+    def __init__(self, case: dict, state: Dict[str, np.ndarray], extf: Optional[np.ndarray] = None):
+        n = len(state["x"])
+        self.arrs = {}
+        s = OrcState()
+        s.n = n
+        for ext, intn, per in FIELD_MAP:
+            a = np.ascontiguousarray(state[ext], dtype=np.float64).reshape((n, per) if per > 1 else (n,)).copy()
+            self.arrs[ext] = a
+            setattr(s, intn, a.ctypes.data)
+        p = case["params"]
+        self.arrs["mass"] = np.full(n, float(p["particle_mass"]))
+        self.arrs["vol"] = np.full(n, float(p["particle_volume"]))
+        s.mass = self.arrs["mass"].ctypes.data
+        s.vol = self.arrs["vol"].ctypes.data
+        self.arrs["status"] = np.ascontiguousarray(state["status"], dtype=np.int32).copy()
+        self.arrs["id"] = np.ascontiguousarray(state["id"], dtype=np.int32).copy()
+        lod = state.get("lod")
+        self.arrs["lod"] = np.zeros(n, np.int32) if lod is None else np.ascontiguousarray(lod, np.int32).copy()
+        s.status = self.arrs["status"].ctypes.data
+        s.id = self.arrs["id"].ctypes.data
+        s.lod = self.arrs["lod"].ctypes.data
+        if extf is not None:
+            self.arrs["extf"] = np.ascontiguousarray(extf, np.float64).reshape(n, 3).copy()
+            s.extf = self.arrs["extf"].ctypes.data
+        self.state = s
+        samples = case["tool"].get("samples")
+        self.tool = OrcTool()
+        if samples is not None:
+            smp = np.ascontiguousarray(samples, np.float64)
+            self.cols = [np.ascontiguousarray(smp[:, k]) for k in range(3)]
+            self.tool.n = len(smp)
+            self.tool.ox, self.tool.oy, self.tool.oz = (c.ctypes.data for c in self.cols)
+
+    def result(self) -> Dict[str, np.ndarray]:
+        out = {k: v for k, v in self.arrs.items() if k not in ("mass", "vol", "extf")}
+        return out
+
+
+class Oracle:
+    def __init__(self):
+        if not ORACLE_LIB.exists():
+            build()
+        L = C.CDLL(str(ORACLE_LIB))
+        L.orc_grid_doubles.restype = _i64
+        L.orc_grid_doubles.argtypes = [C.POINTER(OrcParams)]
+        L.orc_step.restype = _i32
+        L.orc_step.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcState), C.POINTER(OrcTool), C.POINTER(_d), _d,
+                               _i32, _i64, _d, _i32]
+        L.orc_metrics_compute.restype = None
+        L.orc_metrics_compute.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcState), C.POINTER(OrcMetrics)]
+        L.orc_philox_uniform4.restype = None
+        L.orc_philox_uniform4.argtypes = [C.c_uint32] * 6 + [C.POINTER(C.c_float)]
+        L.orc_tool_sdf.restype = _d
+        L.orc_tool_sdf.argtypes = [C.POINTER(OrcParams), C.POINTER(_d), _d, _d, _d]
+        self.L = L
+
+    def step(self, case: dict, state: Dict[str, np.ndarray], nsteps: int, step0: int = 0, t0: float = 0.0,
+             nthreads: int = 1, dt: Optional[float] = None, extf: Optional[np.ndarray] = None):
+        p = orc_params(case)
+        b = _Bound(case, state, extf)
+        grid = np.zeros(int(self.L.orc_grid_doubles(C.byref(p))), dtype=np.float64)
+        rc = self.L.orc_step(C.byref(p), C.byref(b.state), C.byref(b.tool),
+                             grid.ctypes.data_as(C.POINTER(_d)), float(dt if dt is not None else case["dt"]),
+                             int(nsteps), int(step0), float(t0), int(nthreads))
+        return b.result(), rc
+
+    def metrics(self, case: dict, state: Dict[str, np.ndarray]) -> dict:
+        p = orc_params(case)
+        b = _Bound(case, state)
+        m = OrcMetrics()
+        self.L.orc_metrics_compute(C.byref(p), C.byref(b.state), C.byref(m))
+        out = {}
+        for name, _ in m._fields_:
+            v = getattr(m, name)
+            out[name] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+    def philox(self, seed: int, c0: int, c1: int, c2: int, c3: int) -> np.ndarray:
+        out = (C.c_float * 4)()
+        self.L.orc_philox_uniform4(seed & 0xFFFFFFFF, seed >> 32, c0, c1, c2, c3, out)
+        return np.array(out[:], dtype=np.float32)
+
+
+class RefKern:
+    """The reference's own CUDA kernels (needs a GPU)."""
+
+    def __init__(self):
+        if not REF_LIB.exists():
+            raise RuntimeError(f"{REF_LIB} is missing: build it with `make -C oracle ref` where the reference "
+                               "sources are present")
+        L = C.CDLL(str(REF_LIB))
+        L.ref_last_error.restype = C.c_char_p
+        L.ref_device_count.restype = _i32
+        L.ref_sizeof_particle.restype = _i32
+        L.ref_run.restype = _i32
+        L.ref_run.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcState), C.POINTER(OrcTool), _d, _i32, C.c_longlong,
+                              _d]
+        L.ref_stats.restype = _i32
+        L.ref_stats.argtypes = [C.POINTER(OrcState), C.POINTER(_d)]
+        L.ref_bench.restype = _i32
+        L.ref_bench.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcState), C.POINTER(OrcTool), _d, _i32, _i32,
+                                C.POINTER(_d)]
+        self.L = L
+
+    def step(self, case: dict, state: Dict[str, np.ndarray], nsteps: int, step0: int = 0, t0: float = 0.0,
+             dt: Optional[float] = None, extf: Optional[np.ndarray] = None):
+        p = orc_params(case)
+        b = _Bound(case, state, extf)
+        rc = self.L.ref_run(C.byref(p), C.byref(b.state), C.byref(b.tool), float(dt if dt is not None else case["dt"]),
+                            int(nsteps), int(step0), float(t0))
+        if rc != 0:
+            raise RuntimeError(f"reference run failed ({rc}): {self.L.ref_last_error().decode()}")
+        return b.result()
+
+    def stats(self, case: dict, state: Dict[str, np.ndarray]) -> np.ndarray:
+        b = _Bound(case, state)
+        out = (C.c_double * 4)()
+        rc = self.L.ref_stats(C.byref(b.state), out)
+        if rc != 0:
+            raise RuntimeError(self.L.ref_last_error().decode())
+        return np.array(out[:])
+
+    def bench(self, case: dict, state: Dict[str, np.ndarray], warmup: int, steps: int, dt: Optional[float] = None):
+        p = orc_params(case)
+        b = _Bound(case, state)
+        ms = C.c_double()
+        rc = self.L.ref_bench(C.byref(p), C.byref(b.state), C.byref(b.tool),
+                              float(dt if dt is not None else case["dt"]), int(warmup), int(steps), C.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"reference bench failed ({rc}): {self.L.ref_last_error().decode()}")
+        return ms.value, b.result()
