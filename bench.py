@@ -1,0 +1,385 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 MPM workpiece step (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config large|small|precision]
+
+Workload (default `large`): the plain large single-instance step -- 256x128x128
+cells, dx 0.02 mm, 8 particles/cell (~33.5M particles), Ti-6Al-4V, rounded
+wedge tool, CFL 0.3.  A step is one MPM time step over every particle
+(P2G with the Johnson-Cook return, grid update with the tool boundary, G2P).
+Metric: particle-updates/s = live particles x K / device time of the K steps.
+The working set (~7 GB of particle state per step) is far larger than the
+126 MB L2, so no flush is needed between steps.
+
+N > 1 (torchrun): every rank runs its own replica (the path does not shard a
+single instance; replicas only, no data-path collective); the timing is the
+max over ranks, value = total particle-updates / that time.
+
+--impl reference: the reference's own CUDA kernels (src/MPMSolver.cu, built from
+its sources into oracle/_ref/) on the same workload -- rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import signal
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "edegpredict-engine-rotary_b200"))
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+METRIC = "particle-updates/s"
+UNIT = "particle-updates/s"
+# Algorithmic bytes per particle-update of the two-pass FP32 step (P2G pass
+# 38 words read + 6 written, G2P pass 13 read + 25 written = 328 B), plus 56 B
+# of plastic-state writes per yielding update and 48/ppc B of grid traffic.
+B_ALG_BASE, B_ALG_YIELD, B_ALG_GRID = 328.0, 56.0, 48.0
+
+
+def load_peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(config: str):
+    f = ROOT / "profiles" / "traffic.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        v = d.get(config)
+        if v:
+            return float(v["bytes_per_launch"]), v.get("source", "")
+    return None, ""
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"mpm_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.idx), "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+            time.sleep(0.6)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.send_signal(signal.SIGINT)
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        try:
+            self.path.unlink()
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        load = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for k, nm in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def dist_setup(n_gpus: int):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return rank, world, local, pg
+
+
+def physical_gpu_index(local: int) -> int:
+    cvd = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if cvd:
+        ids = [x.strip() for x in cvd.split(",") if x.strip()]
+        if local < len(ids) and ids[local].isdigit():
+            return int(ids[local])
+    return local
+
+
+def make_case(name: str):
+    from mpm_b200 import workpiece as W
+    if name == "small":
+        return W.config1(), "plain small: 64x32x32 cells, dx 0.05 mm, 8 ppc, AISI 4340, cylinder R 0.5 mm"
+    if name == "precision":
+        return W.config4(), "precision study geometry: 128x64x64 cells, dx 0.02 mm, 8 ppc, Ti-6Al-4V, wedge"
+    return W.config2(), ("plain large single instance: 256x128x128 cells, dx 0.02 mm, 8 ppc (~33.5M particles), "
+                         "Ti-6Al-4V, rounded wedge r_e 0.3 mm at 2.5 m/s, doc 0.05 mm, CFL 0.3")
+
+
+# ----------------------------------------------------------------- CPU baseline
+
+def cpu_baseline(case_name: str, budget_s: float = 15.0) -> dict:
+    """The FP64 C restatement (oracle/) on the host cores, on a bounded sample
+    of the workload: same material, tool and cell size, a 48x24x24-cell box."""
+    from mpm_b200 import workpiece as W
+    from oracle.oracle import Oracle
+    o = Oracle()
+    base, _ = make_case(case_name)
+    cells = (48, 24, 24)
+    if case_name == "small":
+        case = W.config1(cells=cells)
+    else:
+        case = W.config2(cells=cells) if case_name == "large" else W.config4(cells=cells)
+    st = W.full_state(W.generate_box(case), case)
+    n_live = int((st["status"] != 1).sum())
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    st, _ = o.step(case, st, 1, nthreads=threads)
+    t1 = time.perf_counter() - t0
+    steps = max(1, min(200, int(budget_s / max(t1, 1e-3))))
+    t0 = time.perf_counter()
+    st, _ = o.step(case, st, steps, step0=1, t0=case["dt"], nthreads=threads)
+    el = time.perf_counter() - t0
+    return {"value": n_live * steps / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"FP64 C restatement (oracle/mpm_oracle.c, OpenMP) of the same step: {cells[0]}x{cells[1]}x"
+                      f"{cells[2]} cells of the workload's material/tool/cell size ({n_live} particles), "
+                      f"{steps} steps, {el:.1f} s"}
+
+
+# ----------------------------------------------------------------- our arm
+
+def run_ours(args):
+    import torch
+    rank, world, local, dist = dist_setup(args.gpus)
+    from mpm_b200 import Solver, capi as A, workpiece as W
+    case, desc = make_case(args.config)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    p = W.to_mpm_params(case)
+    box = case["box"]
+    cap = int(np.prod([box["c1"][i] - box["c0"][i] for i in range(3)]) * box["ppc"])
+    s = Solver(p, cap, stream=stream.cuda_stream)
+    n = s.init_box(box["c0"], box["c1"], box["ppc"], box["seed"] + rank, box["instance"], box["fixed_layers"],
+                   box["T0"], tool=case["tool"])
+    m0 = s.metrics()
+    n_live = n - m0["n_inactive"]
+    dt = case["dt"]
+    # warm-up (untimed)
+    s.step(dt, args.warmup)
+    torch.cuda.synchronize(dev)
+    y0 = s.metrics()["n_yielded"]
+    launches0 = s.launches()
+    sampler = ClockSampler(physical_gpu_index(local))
+    sampler.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    s.profile(True)
+    s.profile_read()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        s.step(dt, args.steps)
+        e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    k_ms, k_n = s.profile_read()
+    s.profile(False)
+    launches = s.launches() - launches0
+    m1 = s.metrics()
+    f_yield = (m1["n_yielded"] - y0) / max(1, n_live * args.steps)
+    if dist:
+        t = torch.tensor([ms, float(n_live)], device=dev, dtype=torch.float64)
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        tot = t.clone()
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        ms_max, live_tot = float(mx[0]), float(tot[1])
+    else:
+        ms_max, live_tot = ms, float(n_live)
+    value = live_tot * args.steps / (ms_max / 1e3)
+
+    # end to end through the C ABI with host buffers (per replica)
+    e2e = run_e2e(s, case, args, n, dev, stream)
+    if dist:
+        t = torch.tensor([e2e["seconds"]], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_val = live_tot * args.steps / float(t[0])
+    else:
+        e2e_val = float(n_live) * args.steps / e2e["seconds"]
+
+    peak, peak_kind = load_peaks()
+    b_alg = B_ALG_BASE + B_ALG_YIELD * f_yield + B_ALG_GRID / box["ppc"]
+    avg_launch_s = (k_ms / max(k_n, 1)) / 1e3
+    achieved = b_alg * n_live / avg_launch_s / 1e9 if k_n else None
+    traffic, traffic_src = load_traffic(args.config)
+    s.close()
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            cpu = cpu_baseline(args.config, args.cpu_seconds)
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": desc, "particles_per_gpu": int(n_live), "cells": list(case["cells"]),
+                       "dx_m": case["params"]["dx"], "dt_s": dt, "ppc": box["ppc"],
+                       "schedule": "fused G2P->P2G, one kernel per step", "parallelism": f"replicas{world}",
+                       "l2": "working set >> L2 (no flush needed)", "yield_fraction": f_yield,
+                       "escaped_updates": int(m1["n_escaped"]), "rebins": int(m1["n_sorts"])},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None,
+                         "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                         else "fallback",
+                         "traffic": traffic, "traffic_source": traffic_src,
+                         "kernel": "k_step<float,G2P,P2G> (fused)", "kernel_launches_timed": int(k_n),
+                         "kernel_ms_avg": k_ms / max(k_n, 1), "bytes_alg_per_update": b_alg},
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": e2e["h2d"] / args.steps,
+                    "d2h_bytes_per_step": e2e["d2h"] / args.steps, "seconds": e2e["seconds"],
+                    "path": e2e["path"]},
+            "clocks": clocks,
+        }
+        if cpu:
+            out["cpu_baseline"] = cpu
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def run_e2e(s, case, args, n, dev, stream) -> dict:
+    """Through the C ABI with host buffers: upload the particles from pinned
+    host memory, step in macro steps of 8 sub-steps (set the tool pose, step,
+    read the metrics, as SimulationEngine does), download the exported
+    fields into pinned host memory."""
+    import torch
+    parts = s.download(fields=("x", "y", "z", "temperature", "status", "id"), elem=4)
+    pin = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in parts.items()}
+    outf = ("x", "y", "z", "vx", "vy", "vz", "stress", "temperature", "plastic_strain", "status")
+    from mpm_b200 import capi as A
+    out_bufs = {}
+    for k in outf:
+        per = A.PARTICLE_FIELDS.get(k, 1)
+        dt_ = np.int32 if k == "status" else np.float32
+        out_bufs[k] = torch.from_numpy(np.zeros((n, per) if per > 1 else (n,), dtype=dt_)).pin_memory().numpy()
+    h2d = sum(v.nbytes for v in pin.values())
+    d2h = sum(v.nbytes for v in out_bufs.values())
+    tool = dict(case["tool"])
+    dt = case["dt"]
+    macro = 8
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    s.upload(pin, elem=4)
+    done = 0
+    while done < args.steps:
+        k = min(macro, args.steps - done)
+        s.set_tool(tool)
+        s.step(dt, k)
+        s.metrics()
+        h2d += ctypes.sizeof(A.MpmToolDesc)
+        d2h += ctypes.sizeof(A.MpmMetrics)
+        done += k
+    s.download_into(out_bufs, elem=4)
+    torch.cuda.synchronize(dev)
+    sec = time.perf_counter() - t0
+    return {"seconds": sec, "h2d": h2d, "d2h": d2h,
+            "path": "mpm_upload (pinned f32 SoA) -> per 8 sub-steps: mpm_set_tool + mpm_step + mpm_sync_metrics -> "
+                    "mpm_download (pinned f32 SoA)"}
+
+
+# ----------------------------------------------------------------- reference arm
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    try:
+        from oracle.oracle import RefKern
+        from mpm_b200 import workpiece as W
+        rk = RefKern()
+    except Exception as exc:  # the harness was not built here
+        return {"impl": "reference", "unavailable": f"reference kernels not built: {exc}"}
+    import torch
+    torch.cuda.set_device(0)
+    case, desc = make_case(args.config)
+    x, y, z, status = W.generate_box_chunked(case)
+    samples = W.tool_samples(case)
+    ms, live = rk.bench_positions(case, x, y, z, status, args.warmup, args.steps, samples=samples)
+    n_live = int((status != 1).sum())
+    value = n_live * args.steps / (ms / 1e3)
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "particles_per_gpu": n_live, "tool_boundary": "rasterised tool samples "
+                       "(rasterizeToolKernel), the reference's only grid tool boundary"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "kind": "reference", "cores": 0,
+                             "sample": "the reference has no CPU implementation of this path; its own CUDA kernels "
+                                       "(src/MPMSolver.cu, FP64 AoS, CUDA graph per step as MPMSolver::step) on the "
+                                       "B200, full workload"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="large", choices=["large", "small", "precision"])
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

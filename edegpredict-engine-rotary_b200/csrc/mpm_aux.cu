@@ -120,42 +120,48 @@ void fill_i32(int32_t* p, int32_t v, int64_t n, cudaStream_t st) {
 
 // ------------------------------------------------------------------ work list
 
-__global__ void k_work_flags(const int32_t* count, const int32_t* key_bin, const int32_t* key_inst, int64_t nkeys,
-                             int32_t* flag) {
-    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < nkeys) flag[k] = (key_bin[k] >= 0 && count[k] > 0) ? 1 : 0;
+// One work item per non-empty bin.  A bin's keys are contiguous (bin*64 +
+// cell), so its particles are [offset[first], offset[first + 64]).
+__global__ void k_work_flags(const int32_t* offset, const int32_t* bin_key, int64_t nbins_total, int32_t* flag) {
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nbins_total) {
+        const int32_t fk = bin_key[b];
+        flag[b] = (offset[fk + kCellsPerBin] - offset[fk]) > 0 ? 1 : 0;
+    }
 }
 
-__global__ void k_work_emit(const int32_t* count, const int32_t* offset, const int32_t* key_inst,
-                            const int32_t* key_bin, const int64_t* inst_pbase, const int32_t* flag,
-                            const int32_t* flag_scan, int64_t nkeys, Work* work, int* n_work) {
-    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < nkeys && flag[k]) {
-        const int i = key_inst[k];
+__global__ void k_work_emit(const int32_t* offset, const int32_t* bin_key, const int32_t* bin_inst,
+                            const int32_t* bin_local, const int64_t* inst_pbase, const int32_t* flag,
+                            const int32_t* flag_scan, int64_t nbins_total, Work* work, int* n_work) {
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nbins_total && flag[b]) {
+        const int32_t fk = bin_key[b];
+        const int i = bin_inst[b];
         Work w;
         w.inst = i;
-        w.bin = key_bin[k];
-        w.start = (int)(offset[k] - inst_pbase[i]);
-        w.count = count[k];
-        work[flag_scan[k]] = w;
+        w.bin = bin_local[b];
+        w.start = (int)(offset[fk] - inst_pbase[i]);
+        w.count = offset[fk + kCellsPerBin] - offset[fk];
+        work[flag_scan[b]] = w;
     }
-    if (k == nkeys - 1) *n_work = flag_scan[k] + flag[k];
+    if (b == nbins_total - 1) *n_work = flag_scan[b] + flag[b];
 }
 
-void build_work(const int32_t* count, const int32_t* offset, const int32_t* key_inst, const int32_t* key_bin,
-                const int64_t* inst_pbase, int64_t nkeys, int32_t* flag, int32_t* flag_scan, int32_t* tmp, Work* work,
-                int* n_work, cudaStream_t st) {
-    k_work_flags<<<nblk(nkeys), kT, 0, st>>>(count, key_bin, key_inst, nkeys, flag);
-    exclusive_scan(flag, flag_scan, nkeys, tmp, st);
-    k_work_emit<<<nblk(nkeys), kT, 0, st>>>(count, offset, key_inst, key_bin, inst_pbase, flag, flag_scan, nkeys,
-                                            work, n_work);
+void build_work(const int32_t* offset, const int32_t* bin_key, const int32_t* bin_inst, const int32_t* bin_local,
+                const int64_t* inst_pbase, int64_t nbins_total, int32_t* flag, int32_t* flag_scan, int32_t* tmp,
+                Work* work, int* n_work, cudaStream_t st) {
+    k_work_flags<<<nblk(nbins_total), kT, 0, st>>>(offset, bin_key, nbins_total, flag);
+    exclusive_scan(flag, flag_scan, nbins_total, tmp, st);
+    k_work_emit<<<nblk(nbins_total), kT, 0, st>>>(offset, bin_key, bin_inst, bin_local, inst_pbase, flag, flag_scan,
+                                                  nbins_total, work, n_work);
     launch_counter() += 2;
 }
 
 // ------------------------------------------------------------------ re-bin
 
-// New key of every particle: the bin of its stencil base node, or the
-// instance's sentinel key when INACTIVE; rank = order of arrival in the key.
+// Key of every particle: instance key base + bin*64 + cell within the bin,
+// where the cell is the stencil base node; INACTIVE particles take the
+// instance's sentinel key (after all bins).  rank = arrival order in the key.
 template <typename R>
 __global__ void k_bin_count(const Inst<R>* insts, int n_inst, PState<R> ps, const int32_t* key_base, bool initial,
                             const double* pos_scratch, int32_t* key, int32_t* rank, int32_t* count, int32_t* newbin,
@@ -168,40 +174,96 @@ __global__ void k_bin_count(const Inst<R>* insts, int n_inst, PState<R> ps, cons
     const bool fresh = initial && P.fresh;
     int b[3];
     if (fresh) {
-        for (int a = 0; a < 3; ++a) b[a] = (int)floor(pos_scratch[3 * pi + a] - 0.5);
+        for (int a = 0; a < 3; ++a) {
+            const double f = floor(pos_scratch[3 * pi + a] - 0.5);
+            b[a] = f < -1e9 ? -1000000000 : (f > 1e9 ? 1000000000 : (int)f);
+        }
     } else {
         const int bn = ps.bin[pi];
         const int ob[3] = {bn % P.nbx, (bn / P.nbx) % P.nby, bn / (P.nbx * P.nby)};
         const V4<R> a0 = ps.A[0][pi];
         const R xl[3] = {a0.x, a0.y, a0.z};
-        for (int a = 0; a < 3; ++a) b[a] = ob[a] * kBin + (int)floor(xl[a] - R(0.5));
+        for (int a = 0; a < 3; ++a) {
+            const R f = floor(xl[a] - R(0.5));
+            const int fi = f < R(-1e8) ? -100000000 : (f > R(1e8) ? 100000000 : (int)f);
+            b[a] = ob[a] * kBin + fi;
+        }
     }
     const int nb[3] = {P.nbx, P.nby, P.nbz};
-    int B[3];
+    int B[3], L[3];
     for (int a = 0; a < 3; ++a) {
-        int q = b[a] >= 0 ? b[a] / kBin : -1;
+        const int q = b[a] >= 0 ? b[a] / kBin : -1;
         B[a] = q < 0 ? 0 : (q >= nb[a] ? nb[a] - 1 : q);
+        const int l = b[a] - B[a] * kBin;
+        L[a] = l < 0 ? 0 : (l >= kBin ? kBin - 1 : l);
     }
     const int bin = B[0] + P.nbx * (B[1] + P.nby * B[2]);
-    const int nbins = P.nbx * P.nby * P.nbz;
-    const int32_t kk = key_base[ii] + ((ps.status[pi] == ST_INACTIVE) ? nbins : bin);
+    const int cell = L[0] + kBin * (L[1] + kBin * L[2]);
+    const int32_t kk = key_base[ii] + ((ps.status[pi] == ST_INACTIVE) ? P.nbins * kCellsPerBin
+                                                                       : bin * kCellsPerBin + cell);
     key[pi] = kk;
     newbin[pi] = bin;
     rank[pi] = atomicAdd(&count[kk], 1);
 }
 
+__device__ __forceinline__ int gcd_i(int a, int b) {
+    while (b) {
+        const int t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+// x with (s * x) mod n == 1, for gcd(s, n) == 1 (extended Euclid).
+__device__ __forceinline__ int64_t inv_mod(int64_t s, int64_t n) {
+    int64_t t = 0, nt = 1, r = n, nr = s % n;
+    while (nr != 0) {
+        const int64_t q = r / nr;
+        int64_t tmp = t - q * nt;
+        t = nt;
+        nt = tmp;
+        tmp = r - q * nr;
+        r = nr;
+        nr = tmp;
+    }
+    return t < 0 ? t + n : t;
+}
+
+// Position in the bin of the particle of (cell-major) rank r among n: the
+// bin is laid out so that position p holds rank (p * s) mod n, s coprime to n
+// and about n/8 (a cell holds ~8 of a bin's ~512 particles).  Consecutive
+// positions -- the lanes of a warp -- then hold particles ~8 cells apart.
+__device__ __forceinline__ int64_t in_bin_slot(int r, int n) {
+    if (n <= 2) return r;
+    int s = (n >> 3) | 1;
+    while (gcd_i(s, n) != 1) s += 2;
+    return ((int64_t)r * inv_mod(s, n)) % n;
+}
+
 template <typename R>
 __global__ void k_bin_scatter(PState<R> src, PState<R> dst, const Inst<R>* insts, int n_inst, const int32_t* key,
-                              const int32_t* rank, const int32_t* offset, const int32_t* newbin, bool initial,
-                              const double* pos_scratch, bool has_K, int64_t np) {
+                              const int32_t* rank, const int32_t* offset, const int32_t* key_base,
+                              const int32_t* newbin, bool initial, const double* pos_scratch, bool has_K,
+                              int64_t np) {
     const int64_t pi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pi >= np) return;
     const int ii = find_inst(insts, n_inst, pi);
     const Inst<R>& P = insts[ii];
     if (pi >= P.pbase + P.np) return;
     const bool fresh = initial && P.fresh;
-    const int64_t d = offset[key[pi]] + rank[pi];
+    const int32_t kk = key[pi];
     const int nbn = newbin[pi];
+    int64_t d;
+    if (kk - key_base[ii] >= P.nbins * kCellsPerBin) {
+        d = offset[kk] + rank[pi];  // INACTIVE: after the bins, in arrival order
+    } else {
+        const int32_t fk = key_base[ii] + nbn * kCellsPerBin;
+        const int64_t b0 = offset[fk];
+        const int n = offset[fk + kCellsPerBin] - (int)b0;
+        const int r = (int)(offset[kk] - b0) + rank[pi];
+        d = b0 + in_bin_slot(r, n);
+    }
     const int nbv[3] = {nbn % P.nbx, (nbn / P.nbx) % P.nby, nbn / (P.nbx * P.nby)};
     V4<R> a0 = src.A[0][pi];
     if (fresh) {
@@ -241,7 +303,7 @@ template <typename R>
 __global__ void k_pad_counts(const Inst<R>* insts, int n_inst, const int32_t* key_base, int32_t* count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_inst) return;
-    count[key_base[i] + insts[i].nbins + 1] = (int32_t)(insts[i].pcap - insts[i].np);
+    count[key_base[i] + insts[i].nbins * kCellsPerBin + 1] = (int32_t)(insts[i].pcap - insts[i].np);
 }
 
 template <typename R>
@@ -645,11 +707,12 @@ void launch_bin_count(const Inst<R>* insts, int n_inst, const PState<R>& ps, con
 
 template <typename R>
 void launch_bin_scatter(const PState<R>& src, const PState<R>& dst, const Inst<R>* insts, int n_inst,
-                        const int32_t* key, const int32_t* rank, const int32_t* offset, const int32_t* newbin,
-                        bool initial, const double* pos_scratch, bool has_K, int64_t np, cudaStream_t st) {
+                        const int32_t* key, const int32_t* rank, const int32_t* offset, const int32_t* key_base,
+                        const int32_t* newbin, bool initial, const double* pos_scratch, bool has_K, int64_t np,
+                        cudaStream_t st) {
     if (np <= 0) return;
-    k_bin_scatter<R><<<(int)((np + kT - 1) / kT), kT, 0, st>>>(src, dst, insts, n_inst, key, rank, offset, newbin,
-                                                               initial, pos_scratch, has_K, np);
+    k_bin_scatter<R><<<(int)((np + kT - 1) / kT), kT, 0, st>>>(src, dst, insts, n_inst, key, rank, offset,
+                                                               key_base, newbin, initial, pos_scratch, has_K, np);
     ++launch_counter();
 }
 
@@ -720,8 +783,8 @@ void launch_set_temps(const PState<R>& ps, int64_t pbase, int64_t n, const doubl
     template void launch_bin_count<R>(const Inst<R>*, int, const PState<R>&, const int32_t*, bool, const double*,   \
                                       int32_t*, int32_t*, int32_t*, int32_t*, int64_t, cudaStream_t);               \
     template void launch_bin_scatter<R>(const PState<R>&, const PState<R>&, const Inst<R>*, int, const int32_t*,    \
-                                        const int32_t*, const int32_t*, const int32_t*, bool, const double*, bool,  \
-                                        int64_t, cudaStream_t);                                                      \
+                                        const int32_t*, const int32_t*, const int32_t*, const int32_t*, bool,       \
+                                        const double*, bool, int64_t, cudaStream_t);                                 \
     template void launch_import<R>(const DevSoA&, int64_t, double, double, double, double, double, const PState<R>&, \
                                    int64_t, double*, cudaStream_t);                                                  \
     template void launch_gen<R>(const Inst<R>&, const int32_t*, const int32_t*, int, uint64_t, uint32_t, int, double, \

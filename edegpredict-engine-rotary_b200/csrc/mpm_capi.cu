@@ -177,6 +177,17 @@ mpm_status mpm_reset_clock(mpm_handle* h) {
     return ret(h, h->eng->reset_clock(0));
 }
 
+mpm_status mpm_profile_enable(mpm_handle* h, int32_t enable) {
+    NEED_H(h);
+    return ret(h, h->eng->profile_enable(enable != 0));
+}
+
+mpm_status mpm_profile_read(mpm_handle* h, double* kernel_ms, int64_t* kernel_launches) {
+    NEED_H(h);
+    if (!kernel_ms || !kernel_launches) return fail(h, MPM_INVALID_ARG, "output is NULL");
+    return ret(h, h->eng->profile_read(kernel_ms, kernel_launches));
+}
+
 mpm_status mpm_launch_count(const mpm_handle* h, int64_t* count) {
     if (!h || !h->eng || !count) return fail(nullptr, MPM_INVALID_ARG, "handle or output is NULL");
     *count = h->eng->launches();

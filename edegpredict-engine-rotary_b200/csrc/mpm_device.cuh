@@ -93,6 +93,7 @@ template <typename R> struct alignas(128) Inst {
     int tool_mode, tool_shape;
     double tool_p0[3], tool_v[3], tool_t0;
     double tool_r, tool_rake, tool_clear, tool_tip_dz;
+    double tool_sg, tool_cg, tool_sa, tool_ca;   // sin/cos of rake and clearance, computed on the host
     // external force for one step (radius 0: none)
     double ext_c[3], ext_r, ext_f[3];
     int64_t pbase;                 // first particle slot of this instance in the batch arrays
@@ -101,6 +102,12 @@ template <typename R> struct alignas(128) Inst {
     int fresh;                     // positions still in the upload scratch (not yet binned)
     int nbins;                     // nbx * nby * nbz
 };
+
+// Threads per CTA of the step kernel (four warps, each with its own P2G tile).
+constexpr int kNT = 128;
+constexpr int kWarps = kNT / 32;
+// Cells per bin (4x4x4): the sort key of a particle is bin*64 + cell in bin.
+constexpr int kCellsPerBin = kBin * kBin * kBin;
 
 // One unit of work: the particles of one bin of one instance.
 struct Work {
@@ -144,25 +151,34 @@ __device__ __forceinline__ int tidx(int x, int y, int z) { return x + kSY * y + 
 // reference boundary is the rasterised tool, src/MPMSolver.cu:444-492).
 // Cylinder with axis along y, or a rounded wedge extruded along y (sharp core
 // wedge with apex at the edge-circle centre, offset by the edge radius).
+// Every product and sum is rounded separately (no FMA contraction), so that
+// the inside/outside decision of a node lying on the tool surface is the same
+// as in a plain IEEE evaluation of the formula.
+__device__ __forceinline__ double dm(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double da(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double ds(double a, double b) { return __dsub_rn(a, b); }
+
 template <typename I>
 __device__ inline double tool_sdf(const I& P, double x, double z, double pr0, double pr2, double nrm[3]) {
-    double qx = x - pr0, qz = z - pr2;
+    const double qx = ds(x, pr0), qz = ds(z, pr2);
     nrm[1] = 0.0;
     if (P.tool_shape == 0) {
-        double r = sqrt(qx * qx + qz * qz);
+        const double r = sqrt(da(dm(qx, qx), dm(qz, qz)));
         if (r > 0.0) { nrm[0] = qx / r; nrm[2] = qz / r; } else { nrm[0] = 0.0; nrm[2] = 1.0; }
-        return r - P.tool_r;
+        return ds(r, P.tool_r);
     }
-    double sg = sin(P.tool_rake), cg = cos(P.tool_rake), sa = sin(P.tool_clear), ca = cos(P.tool_clear);
-    double t1x = -sg, t1z = cg, n1x = cg, n1z = sg;
-    double t2x = -ca, t2z = sa, n2x = -sa, n2z = -ca;
-    double d1 = n1x * qx + n1z * qz, d2 = n2x * qx + n2z * qz, core;
+    const double sg = P.tool_sg, cg = P.tool_cg, sa = P.tool_sa, ca = P.tool_ca;
+    const double t1x = -sg, t1z = cg, n1x = cg, n1z = sg;
+    const double t2x = -ca, t2z = sa, n2x = -sa, n2z = -ca;
+    const double d1 = da(dm(n1x, qx), dm(n1z, qz)), d2 = da(dm(n2x, qx), dm(n2z, qz));
+    double core;
     if (d1 <= 0.0 && d2 <= 0.0) {
         if (d1 >= d2) { core = d1; nrm[0] = n1x; nrm[2] = n1z; } else { core = d2; nrm[0] = n2x; nrm[2] = n2z; }
     } else {
-        double s1 = fmax(qx * t1x + qz * t1z, 0.0), s2 = fmax(qx * t2x + qz * t2z, 0.0);
-        double e1x = qx - s1 * t1x, e1z = qz - s1 * t1z, e2x = qx - s2 * t2x, e2z = qz - s2 * t2z;
-        double l1 = sqrt(e1x * e1x + e1z * e1z), l2 = sqrt(e2x * e2x + e2z * e2z);
+        const double s1 = fmax(da(dm(qx, t1x), dm(qz, t1z)), 0.0), s2 = fmax(da(dm(qx, t2x), dm(qz, t2z)), 0.0);
+        const double e1x = ds(qx, dm(s1, t1x)), e1z = ds(qz, dm(s1, t1z));
+        const double e2x = ds(qx, dm(s2, t2x)), e2z = ds(qz, dm(s2, t2z));
+        const double l1 = sqrt(da(dm(e1x, e1x), dm(e1z, e1z))), l2 = sqrt(da(dm(e2x, e2x), dm(e2z, e2z)));
         if (l1 <= l2) {
             core = l1;
             if (l1 > 0) { nrm[0] = e1x / l1; nrm[2] = e1z / l1; } else { nrm[0] = n1x; nrm[2] = n1z; }
@@ -171,8 +187,12 @@ __device__ inline double tool_sdf(const I& P, double x, double z, double pr0, do
             if (l2 > 0) { nrm[0] = e2x / l2; nrm[2] = e2z / l2; } else { nrm[0] = n2x; nrm[2] = n2z; }
         }
     }
-    return core - P.tool_r;
+    return ds(core, P.tool_r);
 }
+
+// World coordinate of grid node index g on one axis: g*dx + origin, rounded
+// like the reference's (gx * config.dx + domainMin.x) (src/MPMSolver.cu:387).
+__device__ __forceinline__ double node_coord(int g, double dx, double o) { return da(dm((double)g, dx), o); }
 
 // ------------------------------------------------------------------ Philox
 

@@ -84,7 +84,7 @@ class Engine final : public EngineBase {
     uint8_t* mask_pool = nullptr;
     Inst<R>* d_inst = nullptr;
     std::vector<Inst<R>> h_inst;
-    int32_t *d_key_base = nullptr, *d_key_inst = nullptr, *d_key_bin = nullptr;
+    int32_t *d_key_base = nullptr, *d_bin_key = nullptr, *d_bin_inst = nullptr, *d_bin_local = nullptr;
     int64_t* d_inst_pbase = nullptr;
     int32_t *d_key = nullptr, *d_rank = nullptr, *d_newbin = nullptr, *d_count = nullptr, *d_offset = nullptr;
     int32_t *d_flag = nullptr, *d_flag_scan = nullptr, *d_scan_tmp = nullptr;
@@ -105,16 +105,56 @@ class Engine final : public EngineBase {
     int64_t launch_base = 0;
     int sort_every = 16, threads = 128;
     int rbuf = 0;
+    // step-kernel timing (mpm_profile_enable)
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+
+    void prof_begin() {
+        if (!prof) return;
+        if (ev_used + 2 > ev_pool.size()) {
+            cudaEvent_t a, b;
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            ev_pool.push_back(a);
+            ev_pool.push_back(b);
+        }
+        cudaEventRecord(ev_pool[ev_used], st);
+    }
+    void prof_end() {
+        if (!prof) return;
+        cudaEventRecord(ev_pool[ev_used + 1], st);
+        ev_used += 2;
+    }
+    mpm_status profile_enable(bool on) override {
+        prof = on;
+        return MPM_OK;
+    }
+    mpm_status profile_read(double* ms, int64_t* n) override {
+        CK(cudaStreamSynchronize(st));
+        double tot = 0.0;
+        for (size_t k = 0; k + 1 < ev_used; k += 2) {
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, ev_pool[k], ev_pool[k + 1]));
+            tot += t;
+        }
+        *ms = tot;
+        *n = (int64_t)(ev_used / 2);
+        ev_used = 0;
+        return MPM_OK;
+    }
 
     ~Engine() override {
         if (st) cudaStreamSynchronize(st);
-        void* ptrs[] = {pbuf[0], pbuf[1], gpool[0], gpool[1], mask_pool, d_inst, d_key_base, d_key_inst, d_key_bin,
+        void* ptrs[] = {pbuf[0], pbuf[1], gpool[0], gpool[1], mask_pool, d_inst, d_key_base, d_bin_key, d_bin_inst,
+                        d_bin_local,
                         d_inst_pbase, d_key, d_rank, d_newbin, d_count, d_offset, d_flag, d_flag_scan, d_scan_tmp,
                         d_pos, d_work, d_nwork, d_err, d_ctr, d_stat_part, d_stat_out, d_stage, d_gen};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         for (auto& x : I)
             if (x.d_samples) cudaFree(x.d_samples);
+        for (auto e : ev_pool) cudaEventDestroy(e);
         if (own_st && st) cudaStreamDestroy(st);
     }
 
@@ -155,7 +195,7 @@ class Engine final : public EngineBase {
         }
         // layout of instances
         int64_t pb = 0, go = 0, kb = 0;
-        std::vector<int32_t> key_base(n), key_inst, key_bin;
+        std::vector<int32_t> key_base(n), bin_key, bin_inst, bin_local;
         std::vector<int64_t> inst_pbase(n);
         for (int i = 0; i < n; ++i) {
             InstHost& x = I[i];
@@ -167,15 +207,17 @@ class Engine final : public EngineBase {
             x.nbx = (x.p.nx + kBin - 1) / kBin;
             x.nby = (x.p.ny + kBin - 1) / kBin;
             x.nbz = (x.p.nz + kBin - 1) / kBin;
-            const int nbins = x.nbx * x.nby * x.nbz;
+            const int64_t nbins = (int64_t)x.nbx * x.nby * x.nbz;
             key_base[i] = (int32_t)kb;
-            for (int b = 0; b < nbins + 2; ++b) {
-                key_inst.push_back(i);
-                key_bin.push_back(b < nbins ? b : -1);
+            for (int64_t b = 0; b < nbins; ++b) {
+                bin_key.push_back((int32_t)(kb + b * kCellsPerBin));
+                bin_inst.push_back(i);
+                bin_local.push_back((int32_t)b);
             }
-            kb += nbins + 2;
+            // keys: bin*64 + cell for every bin, then the INACTIVE sentinel and the unused-slot pad
+            kb += nbins * kCellsPerBin + 2;
             inst_pbase[i] = x.pbase;
-            max_work += nbins;
+            max_work += (int)nbins;
         }
         if (kb > ((int64_t)1 << 31) - 1 || pb > ((int64_t)1 << 31) - 1) {
             err = "too many bins or particles for one engine";
@@ -223,16 +265,19 @@ class Engine final : public EngineBase {
         CK(cudaMalloc(&d_pos, 3 * sizeof(double) * cp));
         CK(cudaMalloc(&d_count, 4 * (nkeys + 1)));
         CK(cudaMalloc(&d_offset, 4 * (nkeys + 1)));
-        CK(cudaMalloc(&d_flag, 4 * (nkeys + 1)));
-        CK(cudaMalloc(&d_flag_scan, 4 * (nkeys + 1)));
+        const int64_t nb_tot = std::max<int64_t>(max_work, 1);
+        CK(cudaMalloc(&d_flag, 4 * (nb_tot + 1)));
+        CK(cudaMalloc(&d_flag_scan, 4 * (nb_tot + 1)));
         CK(cudaMalloc(&d_scan_tmp, 4 * std::max<int64_t>(scan_tmp_size(nkeys + 1), scan_tmp_size(cp))));
         CK(cudaMalloc(&d_key_base, 4 * n));
-        CK(cudaMalloc(&d_key_inst, 4 * nkeys));
-        CK(cudaMalloc(&d_key_bin, 4 * nkeys));
+        CK(cudaMalloc(&d_bin_key, 4 * nb_tot));
+        CK(cudaMalloc(&d_bin_inst, 4 * nb_tot));
+        CK(cudaMalloc(&d_bin_local, 4 * nb_tot));
         CK(cudaMalloc(&d_inst_pbase, 8 * n));
         CK(cudaMemcpyAsync(d_key_base, key_base.data(), 4 * n, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_key_inst, key_inst.data(), 4 * nkeys, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_key_bin, key_bin.data(), 4 * nkeys, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_bin_key, bin_key.data(), 4 * bin_key.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_bin_inst, bin_inst.data(), 4 * bin_inst.size(), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_bin_local, bin_local.data(), 4 * bin_local.size(), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(d_inst_pbase, inst_pbase.data(), 8 * n, cudaMemcpyHostToDevice, st));
         CK(cudaMalloc(&d_work, sizeof(Work) * std::max(max_work, 1)));
         CK(cudaMalloc(&d_nwork, sizeof(int)));
@@ -282,6 +327,16 @@ class Engine final : public EngineBase {
                 return MPM_CUDA_ERROR;
             }
         }
+        fill_mutable(i);
+        return MPM_OK;
+    }
+
+    // Every field except the TMA descriptors and grid pointers (which depend
+    // only on the grid layout).
+    void fill_mutable(int i) {
+        InstHost& x = I[i];
+        const mpm_params& p = x.p;
+        Inst<R>& d = h_inst[i];
         d.tool_mask = mask_pool + x.grid_off;
         d.nx = p.nx; d.ny = p.ny; d.nz = p.nz;
         d.nbx = x.nbx; d.nby = x.nby; d.nbz = x.nbz;
@@ -316,82 +371,19 @@ class Engine final : public EngineBase {
         for (int a = 0; a < 3; ++a) { d.tool_p0[a] = t.position[a]; d.tool_v[a] = t.velocity[a]; }
         d.tool_t0 = tool_t0_[i];
         d.tool_r = t.radius; d.tool_rake = t.rake; d.tool_clear = t.clearance; d.tool_tip_dz = t.tip_dz;
+        d.tool_sg = std::sin(t.rake); d.tool_cg = std::cos(t.rake);
+        d.tool_sa = std::sin(t.clearance); d.tool_ca = std::cos(t.clearance);
         for (int a = 0; a < 3; ++a) { d.ext_c[a] = x.ext_c[a]; d.ext_f[a] = x.ext_f[a]; }
         d.ext_r = x.ext_pending ? x.ext_r : 0.0;
         d.pbase = x.pbase; d.np = x.np; d.pcap = x.cap;
         d.fresh = fresh_[i];
-        return MPM_OK;
     }
     std::vector<double> tool_t0_;
     std::vector<int> fresh_;
 
     mpm_status push_insts() {
-        for (int i = 0; i < (int)I.size(); ++i) {
-            mpm_status s = refresh_inst(i);
-            if (s != MPM_OK) return s;
-        }
+        for (int i = 0; i < (int)I.size(); ++i) fill_mutable(i);
         CK(cudaMemcpyAsync(d_inst, h_inst.data(), sizeof(Inst<R>) * I.size(), cudaMemcpyHostToDevice, st));
-        return MPM_OK;
-    }
-    // update the mutable fields without re-encoding the tensor maps
-    mpm_status refresh_inst(int i) {
-        CUtensorMap t0 = h_inst[i].tmap[0], t1 = h_inst[i].tmap[1];
-        mpm_status s = build_inst_noenc(i);
-        h_inst[i].tmap[0] = t0;
-        h_inst[i].tmap[1] = t1;
-        return s;
-    }
-    mpm_status build_inst_noenc(int i) {
-        // same as build_inst but keep descriptors (they only depend on the grid)
-        CUtensorMap keep[2] = {h_inst[i].tmap[0], h_inst[i].tmap[1]};
-        InstHost& x = I[i];
-        const mpm_params& p = x.p;
-        Inst<R>& d = h_inst[i];
-        V4<R>* g0 = d.grid[0];
-        V4<R>* g1 = d.grid[1];
-        std::memset((void*)&d, 0, sizeof(d));
-        d.tmap[0] = keep[0];
-        d.tmap[1] = keep[1];
-        d.grid[0] = g0;
-        d.grid[1] = g1;
-        d.tool_mask = mask_pool + x.grid_off;
-        d.nx = p.nx; d.ny = p.ny; d.nz = p.nz;
-        d.nbx = x.nbx; d.nby = x.nby; d.nbz = x.nbz;
-        d.nbins = x.nbx * x.nby * x.nbz;
-        d.nn = x.nn;
-        d.dx = p.dx; d.ox = p.origin[0]; d.oy = p.origin[1]; d.oz = p.origin[2];
-        d.dt = x.dt; d.t0 = x.time; d.step0 = x.step;
-        const double mu = p.E / (2.0 * (1.0 + p.nu));
-        const double lam = p.E * p.nu / ((1.0 + p.nu) * (1.0 - 2.0 * p.nu));
-        d.mu = (R)mu; d.lam = (R)lam;
-        d.pmass = (R)p.particle_mass; d.pvol = (R)p.particle_volume;
-        d.A = (R)p.jc_A; d.B = (R)p.jc_B; d.n = (R)p.jc_n; d.C = (R)p.jc_C; d.m = (R)p.jc_m;
-        d.edot0 = (R)std::max(p.edot0, 1e-12);
-        d.Hkin = (R)p.H_kin;
-        d.D1 = (R)p.D1; d.D2 = (R)p.D2; d.D3 = (R)p.D3; d.D4c = (R)p.D4; d.D5 = (R)p.D5; d.Dth = (R)p.D_th;
-        d.Tspan = (R)std::max(p.Tm - p.Tamb, 1.0);
-        d.dTmax = (R)(p.Tm - p.Tamb);
-        d.heat = (R)(p.beta / std::max(p.rho_phys * p.cp, 1e-12));
-        d.apic = (R)p.apic_dinv_factor;
-        d.decay = (R)p.apic_decay;
-        d.deps_cap = (R)p.deps_cap;
-        d.dT_cap = (R)p.dT_cap;
-        d.fix_thick = p.fixture_thickness; d.fix_damp = p.fixture_damping;
-        d.grav = p.gravity_z; d.mthr = p.mass_threshold;
-        d.lod = p.lod_enabled; d.plast = p.plasticity;
-        d.lod_r1 = p.lod_active_r; d.lod_r2 = p.lod_near_r;
-        d.chip_every = p.chip_every;
-        d.newton_maxit = p.newton_maxit > 0 ? p.newton_maxit : 60;
-        d.newton_tol = p.newton_tol > 0 ? p.newton_tol : 1e-12;
-        const mpm_tool_desc& t = x.tool;
-        d.tool_mode = t.mode; d.tool_shape = t.shape;
-        for (int a = 0; a < 3; ++a) { d.tool_p0[a] = t.position[a]; d.tool_v[a] = t.velocity[a]; }
-        d.tool_t0 = tool_t0_[i];
-        d.tool_r = t.radius; d.tool_rake = t.rake; d.tool_clear = t.clearance; d.tool_tip_dz = t.tip_dz;
-        for (int a = 0; a < 3; ++a) { d.ext_c[a] = x.ext_c[a]; d.ext_f[a] = x.ext_f[a]; }
-        d.ext_r = x.ext_pending ? x.ext_r : 0.0;
-        d.pbase = x.pbase; d.np = x.np; d.pcap = x.cap;
-        d.fresh = fresh_[i];
         return MPM_OK;
     }
 
@@ -403,10 +395,10 @@ class Engine final : public EngineBase {
         launch_bin_count<R>(d_inst, (int)I.size(), ps[cur], d_key_base, true, d_pos, d_key, d_rank, d_count, d_newbin,
                             cap_total, st);
         exclusive_scan(d_count, d_offset, nkeys, d_scan_tmp, st);
-        launch_bin_scatter<R>(ps[cur], ps[cur ^ 1], d_inst, (int)I.size(), d_key, d_rank, d_offset, d_newbin, true,
-                              d_pos, has_K, cap_total, st);
-        build_work(d_count, d_offset, d_key_inst, d_key_bin, d_inst_pbase, nkeys, d_flag, d_flag_scan, d_scan_tmp,
-                   d_work, d_nwork, st);
+        launch_bin_scatter<R>(ps[cur], ps[cur ^ 1], d_inst, (int)I.size(), d_key, d_rank, d_offset, d_key_base,
+                              d_newbin, true, d_pos, has_K, cap_total, st);
+        build_work(d_offset, d_bin_key, d_bin_inst, d_bin_local, d_inst_pbase, max_work, d_flag, d_flag_scan,
+                   d_scan_tmp, d_work, d_nwork, st);
         cur ^= 1;
         since_sort = 0;
         ++n_sorts;
@@ -703,8 +695,10 @@ class Engine final : public EngineBase {
                 CK(cudaMemsetAsync(gpool[w ^ 1], 0, gbytes, st));
                 raster_all(k);
                 StepArgs b{k, 0, (k + 2 == N) ? 1 : 0, 0, k + 1};
+                prof_begin();
                 launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], b, w, true, true, threads, 0, d_err, d_ctr,
                                st);
+                prof_end();
                 w ^= 1;
                 ++since_sort;
             }
@@ -717,12 +711,16 @@ class Engine final : public EngineBase {
                 if ((s = maybe_sort()) != MPM_OK) return s;
                 CK(cudaMemsetAsync(gpool[w], 0, gbytes, st));
                 StepArgs a{k, 0, 1, (ext && k == 0) ? 1 : 0, k};
+                prof_begin();
                 launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], a, w, false, true, threads, 0, d_err, d_ctr,
                                st);
+                prof_end();
                 raster_all(k);
                 StepArgs c{k, 1, 0, 0, k};
+                prof_begin();
                 launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], c, w, true, false, threads, 0, d_err, d_ctr,
                                st);
+                prof_end();
                 ++since_sort;
             }
         }
@@ -743,10 +741,10 @@ class Engine final : public EngineBase {
         launch_bin_count<R>(d_inst, (int)I.size(), ps[cur], d_key_base, false, d_pos, d_key, d_rank, d_count,
                             d_newbin, cap_total, st);
         exclusive_scan(d_count, d_offset, nkeys, d_scan_tmp, st);
-        launch_bin_scatter<R>(ps[cur], ps[cur ^ 1], d_inst, (int)I.size(), d_key, d_rank, d_offset, d_newbin, false,
-                              d_pos, has_K, cap_total, st);
-        build_work(d_count, d_offset, d_key_inst, d_key_bin, d_inst_pbase, nkeys, d_flag, d_flag_scan, d_scan_tmp,
-                   d_work, d_nwork, st);
+        launch_bin_scatter<R>(ps[cur], ps[cur ^ 1], d_inst, (int)I.size(), d_key, d_rank, d_offset, d_key_base,
+                              d_newbin, false, d_pos, has_K, cap_total, st);
+        build_work(d_offset, d_bin_key, d_bin_inst, d_bin_local, d_inst_pbase, max_work, d_flag, d_flag_scan,
+                   d_scan_tmp, d_work, d_nwork, st);
         cur ^= 1;
         since_sort = 0;
         ++n_sorts;
@@ -814,6 +812,7 @@ class Engine final : public EngineBase {
         }
         out->n_escaped = (int64_t)ctr[0];
         out->n_sorts = n_sorts;
+        out->n_yielded = (int64_t)ctr[1];
         return device_status();
     }
 

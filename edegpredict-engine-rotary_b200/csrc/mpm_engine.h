@@ -53,6 +53,8 @@ class EngineBase {
     virtual const InstHost& inst(int i) const = 0;
     virtual cudaStream_t stream() const = 0;
     virtual int64_t launches() const = 0;
+    virtual mpm_status profile_enable(bool on) = 0;
+    virtual mpm_status profile_read(double* ms, int64_t* n) = 0;
 };
 
 // Creates an engine for n instances (all of the same precision).  Returns

@@ -37,8 +37,9 @@ void launch_bin_count(const Inst<R>* insts, int n_inst, const PState<R>& ps, con
 
 template <typename R>
 void launch_bin_scatter(const PState<R>& src, const PState<R>& dst, const Inst<R>* insts, int n_inst,
-                        const int32_t* key, const int32_t* rank, const int32_t* offset, const int32_t* newbin,
-                        bool initial, const double* pos_scratch, bool has_K, int64_t np, cudaStream_t st);
+                        const int32_t* key, const int32_t* rank, const int32_t* offset, const int32_t* key_base,
+                        const int32_t* newbin, bool initial, const double* pos_scratch, bool has_K, int64_t np,
+                        cudaStream_t st);
 
 template <typename R>
 void launch_pad_counts(const Inst<R>* insts, int n_inst, const int32_t* key_base, int32_t* count, cudaStream_t st);
@@ -76,9 +77,10 @@ void launch_set_temps(const PState<R>& ps, int64_t pbase, int64_t n, const doubl
 // Device-wide exclusive scan of n int32 (in -> out), tmp >= scan_tmp_size(n).
 int64_t scan_tmp_size(int64_t n);
 void exclusive_scan(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t st);
-// Ordered work list (one item per non-empty bin) from per-key counts/offsets.
-void build_work(const int32_t* count, const int32_t* offset, const int32_t* key_inst, const int32_t* key_bin,
-                const int64_t* inst_pbase, int64_t nkeys, int32_t* flag, int32_t* flag_scan, int32_t* tmp,
+// Ordered work list (one item per non-empty bin) from the key offsets; the
+// bin table gives each global bin its first key, instance and local index.
+void build_work(const int32_t* offset, const int32_t* bin_key, const int32_t* bin_inst, const int32_t* bin_local,
+                const int64_t* inst_pbase, int64_t nbins_total, int32_t* flag, int32_t* flag_scan, int32_t* tmp,
                 Work* work, int* n_work, cudaStream_t st);
 void fill_i32(int32_t* p, int32_t v, int64_t n, cudaStream_t st);
 

@@ -98,13 +98,13 @@ __device__ __forceinline__ void node_vel(const Inst<R>& P, const V4<R>& g, int g
     if (!(m > (R)P.mthr)) return;
     R vx = g.y / m, vy = g.z / m, vz = (g.w + m * (R)(P.grav * P.dt)) / m;
     if (P.fix_thick > 0.0) {
-        const double zr = (((double)gz * P.dx + P.oz) - P.oz) / P.fix_thick;
+        const double zr = ds(node_coord(gz, P.dx, P.oz), P.oz) / P.fix_thick;
         if (zr <= 1.0) {
             if (gz == 0) {
                 vx = vy = vz = R(0);
             } else if (zr > 0.0) {
-                const double s = P.fix_damp * (1.0 - zr) * (1.0 - zr);
-                const R f = (R)(1.0 / (1.0 + s * P.dt));
+                const double s = dm(dm(P.fix_damp, ds(1.0, zr)), ds(1.0, zr));
+                const R f = (R)(1.0 / da(1.0, dm(s, P.dt)));
                 vx *= f; vy *= f; vz *= f;
             }
         }
@@ -115,17 +115,18 @@ __device__ __forceinline__ void node_vel(const Inst<R>& P, const V4<R>& g, int g
         }
     } else if (P.tool_mode == TOOL_SDF_STICKY || P.tool_mode == TOOL_SDF_SLIP) {
         double nrm[3];
-        const double phi = tool_sdf(P, (double)gx * P.dx + P.ox, (double)gz * P.dx + P.oz, pr0, pr2, nrm);
+        const double phi = tool_sdf(P, node_coord(gx, P.dx, P.ox), node_coord(gz, P.dx, P.oz), pr0, pr2, nrm);
         if (phi <= 0.0) {
             if (P.tool_mode == TOOL_SDF_STICKY) {
                 vx = (R)P.tool_v[0]; vy = (R)P.tool_v[1]; vz = (R)P.tool_v[2];
             } else {
-                const double rx = (double)vx - P.tool_v[0], ry = (double)vy - P.tool_v[1], rz = (double)vz - P.tool_v[2];
-                const double vn = rx * nrm[0] + ry * nrm[1] + rz * nrm[2];
+                const double rx = ds((double)vx, P.tool_v[0]), ry = ds((double)vy, P.tool_v[1]),
+                             rz = ds((double)vz, P.tool_v[2]);
+                const double vn = da(da(dm(rx, nrm[0]), dm(ry, nrm[1])), dm(rz, nrm[2]));
                 if (vn < 0.0) {
-                    vx = (R)((double)vx - vn * nrm[0]);
-                    vy = (R)((double)vy - vn * nrm[1]);
-                    vz = (R)((double)vz - vn * nrm[2]);
+                    vx = (R)ds((double)vx, dm(vn, nrm[0]));
+                    vy = (R)ds((double)vy, dm(vn, nrm[1]));
+                    vz = (R)ds((double)vz, dm(vn, nrm[2]));
                 }
             }
         }
@@ -191,19 +192,24 @@ __device__ __forceinline__ void gather_tile(const R (*vel)[kPlane], int base, co
 // Same sums for a particle whose stencil left its bin's tile: nodes are read
 // and updated straight from the grid (rare; the re-bin brings it back).
 template <typename R>
-__device__ __noinline__ void gather_global(const Inst<R>& P, const V4<R>* __restrict__ grid, const int gb[3],
+__device__ __forceinline__ void gather_global(const Inst<R>& P, const V4<R>* __restrict__ grid, const int gb[3],
                                            const R (&w)[3][3], const R (&dw)[3][3], double pr0, double pr2, R v[3],
                                            R M[3][3], R L[3][3]) {
+#pragma unroll
     for (int c = 0; c < 3; ++c) {
         v[c] = R(0);
+#pragma unroll
         for (int b = 0; b < 3; ++b) { M[c][b] = R(0); L[c][b] = R(0); }
     }
+#pragma unroll
     for (int i = 0; i < 3; ++i) {
         const int gx = gb[0] + i;
         if (gx < 0 || gx >= P.nx) continue;
+#pragma unroll
         for (int j = 0; j < 3; ++j) {
             const int gy = gb[1] + j;
             if (gy < 0 || gy >= P.ny) continue;
+#pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const int gz = gb[2] + k;
                 if (gz < 0 || gz >= P.nz) continue;
@@ -212,6 +218,7 @@ __device__ __noinline__ void gather_global(const Inst<R>& P, const V4<R>* __rest
                 const R ww = w[0][i] * w[1][j] * w[2][k];
                 const R g0 = dw[0][i] * w[1][j] * w[2][k], g1 = w[0][i] * dw[1][j] * w[2][k],
                         g2 = w[0][i] * w[1][j] * dw[2][k];
+#pragma unroll
                 for (int c = 0; c < 3; ++c) {
                     v[c] += ww * nv[c];
                     M[c][0] += ww * nv[c] * R(i);
@@ -232,45 +239,18 @@ __device__ __noinline__ void gather_global(const Inst<R>& P, const V4<R>* __rest
 //   p_a = w_ijk (Q_a + R_ax i + R_ay j + R_az k) + S_ax dwx wy wz + S_ay wx dwy wz + S_az wx wy dwz
 // with Q = m (v - dx C d), R = m dx C, S = -dt V J sigma / dx.  Separable in k.
 template <typename R>
-__device__ __forceinline__ void scatter_tile(R (*acc)[kPlane], int base, const R (&w)[3][3], const R (&dw)[3][3], R m,
-                                             const R (&Q)[3], const R (&Rm)[3][3], const R (&S)[3][3], bool mass_only) {
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const R wij = w[0][i] * w[1][j];
-            const R gx = dw[0][i] * w[1][j], gy = w[0][i] * dw[1][j];
-            const R mij = wij * m;
-            R U[3], Up[3], Zs[3];
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                U[a] = wij * (Q[a] + Rm[a][0] * R(i) + Rm[a][1] * R(j)) + S[a][0] * gx + S[a][1] * gy;
-                Up[a] = wij * Rm[a][2];
-                Zs[a] = wij * S[a][2];
-            }
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const int idx = base + i + kSY * j + kSZ * k;
-                atomicAdd(&acc[0][idx], mij * w[2][k]);
-                if (!mass_only) {
-#pragma unroll
-                    for (int a = 0; a < 3; ++a) atomicAdd(&acc[1 + a][idx], fma(w[2][k], fma(R(k), Up[a], U[a]), dw[2][k] * Zs[a]));
-                }
-            }
-        }
-    }
-}
-
-template <typename R>
-__device__ __noinline__ void scatter_global(const Inst<R>& P, V4<R>* __restrict__ grid, const int gb[3],
+__device__ __forceinline__ void scatter_global(const Inst<R>& P, V4<R>* __restrict__ grid, const int gb[3],
                                             const R (&w)[3][3], const R (&dw)[3][3], R m, const R (&Q)[3],
                                             const R (&Rm)[3][3], const R (&S)[3][3], bool mass_only) {
+#pragma unroll
     for (int i = 0; i < 3; ++i) {
         const int gx = gb[0] + i;
         if (gx < 0 || gx >= P.nx) continue;
+#pragma unroll
         for (int j = 0; j < 3; ++j) {
             const int gy = gb[1] + j;
             if (gy < 0 || gy >= P.ny) continue;
+#pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const int gz = gb[2] + k;
                 if (gz < 0 || gz >= P.nz) continue;
@@ -279,6 +259,7 @@ __device__ __noinline__ void scatter_global(const Inst<R>& P, V4<R>* __restrict_
                         g2 = w[0][i] * w[1][j] * dw[2][k];
                 R p[3] = {0, 0, 0};
                 if (!mass_only)
+#pragma unroll
                     for (int a = 0; a < 3; ++a)
                         p[a] = ww * (Q[a] + Rm[a][0] * R(i) + Rm[a][1] * R(j) + Rm[a][2] * R(k)) + S[a][0] * g0 +
                                S[a][1] * g1 + S[a][2] * g2;
@@ -492,25 +473,119 @@ __device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[
 
 // ------------------------------------------------------------------ the step kernel
 
+// Particles staged per pass and scatter payload per particle:
+//   [0..2] xi (bin-local, after the move)  [3..5] Q = m (v - dx C d) + f_ext dt
+//   [6..14] R = m dx C (row-major)         [15..23] S = -dt V J sigma / dx (row-major)
+template <typename R> struct StepCfg {
+    static constexpr int kChunk = sizeof(R) == 4 ? 2 * kNT : kNT;
+    static constexpr int kPerThread = kChunk / kNT;
+};
+constexpr int kPay = 24;
+constexpr int kOff = 27;  // stencil offsets, off = i + 3j + 9k
+
+template <typename R> struct StepSmem {
+    V4<R> raw[kTileNodes];                 // TMA destination (offset 0 of the 128-byte aligned block)
+    R vel[3][kPlane];                      // node velocities after the grid update
+    R cacc[4][kOff][kCellsPerBin];         // per-cell sums of the 27 stencil nodes: m, p_x, p_y, p_z
+    R pay[kPay][StepCfg<R>::kChunk];       // scatter payload of the staged particles
+    short order[StepCfg<R>::kChunk];       // staged particles grouped by base cell
+    int cnt[kCellsPerBin];                 // staged particles per cell (filled by atomics)
+    int ccount[kCellsPerBin];              // copy of cnt for the accumulation pass
+    int cstart[kCellsPerBin];
+    uint64_t mbar;
+    int fail;
+};
+
+template <typename R> constexpr size_t step_smem_bytes() { return sizeof(StepSmem<R>); }
+
+// Accumulation of one cell's staged particles (two channels per thread:
+// h = 0 -> m, p_x; h = 1 -> p_y, p_z) in registers, then added to the cell's
+// private block of cacc.  Each cell block has exactly one writer per
+// channel, so no atomics are needed.  The momentum + impulse of node (i,j,k)
+// relative to the cell's base node is
+//   w_ijk (Q_a + R_ax i + R_ay j + R_az k) + S_ax dwx wy wz + S_ay wx dwy wz + S_az wx wy dwz,
+// evaluated separably (k innermost).
+template <typename R>
+__device__ __forceinline__ void cell_accumulate(StepSmem<R>& Sm, int cell, int h, R pm) {
+    R a0[kOff], a1[kOff];
+#pragma unroll
+    for (int o = 0; o < kOff; ++o) { a0[o] = R(0); a1[o] = R(0); }
+    const int s0 = Sm.cstart[cell], n = Sm.ccount[cell];
+    for (int q = 0; q < n; ++q) {
+        const int e = Sm.order[s0 + q];
+        R w[3][3], dw[3][3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) (void)bspline(Sm.pay[a][e], w[a], dw[a]);
+        if (h == 0) {
+            const R Q0 = Sm.pay[3][e], r0 = Sm.pay[6][e], r1 = Sm.pay[7][e], r2 = Sm.pay[8][e];
+            const R t0 = Sm.pay[15][e], t1 = Sm.pay[16][e], t2 = Sm.pay[17][e];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const R wij = w[0][i] * w[1][j];
+                    const R gx = dw[0][i] * w[1][j], gy = w[0][i] * dw[1][j];
+                    const R mij = wij * pm;
+                    const R U = wij * (Q0 + r0 * R(i) + r1 * R(j)) + t0 * gx + t1 * gy;
+                    const R Up = wij * r2, Zs = wij * t2;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const int o = i + 3 * j + 9 * k;
+                        a0[o] = fma(mij, w[2][k], a0[o]);
+                        a1[o] += fma(w[2][k], fma(R(k), Up, U), dw[2][k] * Zs);
+                    }
+                }
+        } else {
+            const R Q1 = Sm.pay[4][e], Q2 = Sm.pay[5][e];
+            const R r10 = Sm.pay[9][e], r11 = Sm.pay[10][e], r12 = Sm.pay[11][e];
+            const R r20 = Sm.pay[12][e], r21 = Sm.pay[13][e], r22 = Sm.pay[14][e];
+            const R t10 = Sm.pay[18][e], t11 = Sm.pay[19][e], t12 = Sm.pay[20][e];
+            const R t20 = Sm.pay[21][e], t21 = Sm.pay[22][e], t22 = Sm.pay[23][e];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const R wij = w[0][i] * w[1][j];
+                    const R gx = dw[0][i] * w[1][j], gy = w[0][i] * dw[1][j];
+                    const R U1 = wij * (Q1 + r10 * R(i) + r11 * R(j)) + t10 * gx + t11 * gy;
+                    const R U2 = wij * (Q2 + r20 * R(i) + r21 * R(j)) + t20 * gx + t21 * gy;
+                    const R Up1 = wij * r12, Zs1 = wij * t12, Up2 = wij * r22, Zs2 = wij * t22;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const int o = i + 3 * j + 9 * k;
+                        a0[o] += fma(w[2][k], fma(R(k), Up1, U1), dw[2][k] * Zs1);
+                        a1[o] += fma(w[2][k], fma(R(k), Up2, U2), dw[2][k] * Zs2);
+                    }
+                }
+        }
+    }
+    if (n > 0) {
+#pragma unroll
+        for (int o = 0; o < kOff; ++o) {
+            Sm.cacc[2 * h][o][cell] += a0[o];
+            Sm.cacc[2 * h + 1][o][cell] += a1[o];
+        }
+    }
+}
+
 template <typename R, bool G2P, bool P2G>
-__global__ void __launch_bounds__(256) k_step(const Inst<R>* __restrict__ insts, const Work* __restrict__ work,
+__global__ void __launch_bounds__(kNT) k_step(const Inst<R>* __restrict__ insts, const Work* __restrict__ work,
                                               const int* __restrict__ n_work, PState<R> ps, StepArgs sa, int rbuf,
                                               int* __restrict__ err, unsigned long long* __restrict__ ctr) {
-    __shared__ __align__(128) V4<R> raw[kTileNodes];
-    __shared__ R vel[3][kPlane];
-    __shared__ R acc[4][kPlane];
-    __shared__ __align__(8) uint64_t mbar;
-    __shared__ int s_fail;
-    const int tid = threadIdx.x, NT = blockDim.x;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    StepSmem<R>& Sm = *reinterpret_cast<StepSmem<R>*>(smem_raw);
+    constexpr int kChunk = StepCfg<R>::kChunk;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nw = *n_work;
     uint32_t phase = 0;
     int errf = 0;
     unsigned long long c_esc = 0, c_yield = 0;
     if (G2P && tid == 0) {
-        mbar_init(&mbar, 1);
+        mbar_init(&Sm.mbar, 1);
         fence_async_smem();
     }
-    if (tid == 0) s_fail = 0;
+    if (tid == 0) Sm.fail = 0;
+    if (tid < kCellsPerBin) Sm.cnt[tid] = 0;
     __syncthreads();
     int last_inst = -1;
 
@@ -519,14 +594,14 @@ __global__ void __launch_bounds__(256) k_step(const Inst<R>* __restrict__ insts,
         const Inst<R>& P = insts[wk.inst];
         const int bx = wk.bin % P.nbx, by = (wk.bin / P.nbx) % P.nby, bz = wk.bin / (P.nbx * P.nby);
         const int g0x = bx * kBin, g0y = by * kBin, g0z = bz * kBin;
-        const double tg = P.t0 + (double)sa.k * P.dt;          // time of the G2P step
-        const double tp = P.t0 + (double)sa.p2g_step * P.dt;   // time of the P2G step
-        const double prg0 = P.tool_p0[0] + P.tool_v[0] * (tg - P.tool_t0);
-        const double prg1 = P.tool_p0[1] + P.tool_v[1] * (tg - P.tool_t0);
-        const double prg2 = P.tool_p0[2] + P.tool_v[2] * (tg - P.tool_t0);
-        const double prp0 = P.tool_p0[0] + P.tool_v[0] * (tp - P.tool_t0);
-        const double prp1 = P.tool_p0[1] + P.tool_v[1] * (tp - P.tool_t0);
-        const double prp2 = P.tool_p0[2] + P.tool_v[2] * (tp - P.tool_t0);
+        const double tg = da(P.t0, dm((double)sa.k, P.dt));         // time of the G2P step
+        const double tp = da(P.t0, dm((double)sa.p2g_step, P.dt));  // time of the P2G step
+        const double prg0 = da(P.tool_p0[0], dm(P.tool_v[0], ds(tg, P.tool_t0)));
+        const double prg1 = da(P.tool_p0[1], dm(P.tool_v[1], ds(tg, P.tool_t0)));
+        const double prg2 = da(P.tool_p0[2], dm(P.tool_v[2], ds(tg, P.tool_t0)));
+        const double prp0 = da(P.tool_p0[0], dm(P.tool_v[0], ds(tp, P.tool_t0)));
+        const double prp1 = da(P.tool_p0[1], dm(P.tool_v[1], ds(tp, P.tool_t0)));
+        const double prp2 = da(P.tool_p0[2], dm(P.tool_v[2], ds(tp, P.tool_t0)));
         const V4<R>* __restrict__ gr = P.grid[rbuf];
         V4<R>* __restrict__ gw = P.grid[rbuf ^ (G2P ? 1 : 0)];
 
@@ -534,299 +609,359 @@ __global__ void __launch_bounds__(256) k_step(const Inst<R>* __restrict__ insts,
             if (tid == 0) {
                 if (wk.inst != last_inst) tmap_acquire(&P.tmap[rbuf]);
                 fence_async_smem();
-                mbar_expect_tx(&mbar, (uint32_t)(kTileNodes * sizeof(V4<R>)));
-                tma_load_4d(raw, &P.tmap[rbuf], &mbar, 0, g0x, g0y, g0z);
-                if (!mbar_wait_bounded(&mbar, phase, 2000000000ull)) {
+                mbar_expect_tx(&Sm.mbar, (uint32_t)(kTileNodes * sizeof(V4<R>)));
+                tma_load_4d(Sm.raw, &P.tmap[rbuf], &Sm.mbar, 0, g0x, g0y, g0z);
+                if (!mbar_wait_bounded(&Sm.mbar, phase, 2000000000ull)) {
                     // give the copy in flight a second bounded chance, then stop
-                    mbar_wait_bounded(&mbar, phase, 2000000000ull);
-                    s_fail = 1;
+                    mbar_wait_bounded(&Sm.mbar, phase, 2000000000ull);
+                    Sm.fail = 1;
                 }
             }
             phase ^= 1u;
             last_inst = wk.inst;
             __syncthreads();
-            if (s_fail) {
+            if (Sm.fail) {
                 if (tid == 0) atomicOr(err, ERR_TIMEOUT);
                 return;
             }
-            for (int nidx = tid; nidx < kTileNodes; nidx += NT) {
+            for (int nidx = tid; nidx < kTileNodes; nidx += kNT) {
                 const int lx = nidx % kTile, ly = (nidx / kTile) % kTile, lz = nidx / (kTile * kTile);
                 R nv[3];
-                node_vel(P, raw[nidx], g0x + lx, g0y + ly, g0z + lz, prg0, prg2, nv);
+                node_vel(P, Sm.raw[nidx], g0x + lx, g0y + ly, g0z + lz, prg0, prg2, nv);
                 const int t = tidx(lx, ly, lz);
-                vel[0][t] = nv[0]; vel[1][t] = nv[1]; vel[2][t] = nv[2];
+                Sm.vel[0][t] = nv[0]; Sm.vel[1][t] = nv[1]; Sm.vel[2][t] = nv[2];
             }
         }
         if (P2G) {
-            for (int q = tid; q < 4 * kPlane; q += NT) (&acc[0][0])[q] = R(0);
+            for (int q = tid; q < 4 * kOff * kCellsPerBin; q += kNT) (&Sm.cacc[0][0][0])[q] = R(0);
         }
         __syncthreads();
 
         const R dtdx = (R)(P.dt / P.dx);
         const R idx_ = (R)(1.0 / P.dx);
-        for (int pl = tid; pl < wk.count; pl += NT) {
-            const int64_t pi = P.pbase + wk.start + pl;
-            uint8_t st = ps.status[pi];
-            if (st == ST_INACTIVE) continue;
-            const uint8_t st_in = st;
-            const bool fixed = (st == ST_FIXED);
-            V4<R> a0 = ps.A[0][pi], a1 = ps.A[1][pi], a2 = ps.A[2][pi], a3 = ps.A[3][pi];
-            R xi[3] = {a0.x, a0.y, a0.z};
-            R eps = a0.w;
-            R H[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
-            R Hp8 = a3.y, dT = a3.z, Dm = a3.w;
-            R v[3] = {0, 0, 0}, Cm[9], edot = R(0);
-            bool have_C = false, dirtyA = false, dirtyHp = false, wrote_C = false;
-            bool dirtyS = false;
-            R sig[6];
+        const bool chip_now = G2P && P.chip_every > 0 && ((P.step0 + sa.k) % P.chip_every) == 0;
+        for (int base = 0; base < wk.count; base += kChunk) {
+            int myc[StepCfg<R>::kPerThread], myr[StepCfg<R>::kPerThread];
+#pragma unroll 1
+            for (int sidx = 0; sidx < StepCfg<R>::kPerThread; ++sidx) {
+                const int slot = tid + sidx * kNT;
+                const int pl = base + slot;
+                const int64_t pi = P.pbase + wk.start + pl;
+                int scell = -1;  // base cell of this particle's tile scatter, or -1
+                uint8_t st = (pl < wk.count) ? ps.status[pi] : (uint8_t)ST_INACTIVE;
+                if (st != ST_INACTIVE) {
+                    const uint8_t st_in = st;
+                    const bool fixed = (st == ST_FIXED);
+                    V4<R> a0 = ps.A[0][pi], a1 = ps.A[1][pi], a2 = ps.A[2][pi], a3 = ps.A[3][pi];
+                    R xi[3] = {a0.x, a0.y, a0.z};
+                    R eps = a0.w;
+                    R H[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
+                    R Hp8 = a3.y, dT = a3.z, Dm = a3.w;
+                    R v[3] = {0, 0, 0}, Cm[9], edot = R(0);
+                    bool have_C = false, dirtyA = false, wrote_C = false;
 
-            if (G2P) {
-                if (!fixed) {
-                    bool far = false;
-                    if (P.lod && st == ST_ACTIVE) {
-                        const double wx = P.ox + ((double)g0x + (double)xi[0]) * P.dx - prg0;
-                        const double wy = P.oy + ((double)g0y + (double)xi[1]) * P.dx - prg1;
-                        const double wz = P.oz + ((double)g0z + (double)xi[2]) * P.dx - (prg2 + P.tool_tip_dz);
-                        far = sqrt(wx * wx + wy * wy + wz * wz) > P.lod_r2;
-                    }
-                    R w[3][3], dw[3][3];
-                    int b[3];
+                    if (G2P) {
+                        if (!fixed) {
+                            bool far = false;
+                            if (P.lod && st == ST_ACTIVE) {
+                                const double wx = P.ox + ((double)g0x + (double)xi[0]) * P.dx - prg0;
+                                const double wy = P.oy + ((double)g0y + (double)xi[1]) * P.dx - prg1;
+                                const double wz = P.oz + ((double)g0z + (double)xi[2]) * P.dx - (prg2 + P.tool_tip_dz);
+                                far = sqrt(wx * wx + wy * wy + wz * wz) > P.lod_r2;
+                            }
+                            R w[3][3], dw[3][3];
+                            int b[3];
 #pragma unroll
-                    for (int a = 0; a < 3; ++a) b[a] = bspline(xi[a], w[a], dw[a]);
-                    R M[3][3], L[3][3];
-                    if (b[0] >= 0 && b[0] < kBin && b[1] >= 0 && b[1] < kBin && b[2] >= 0 && b[2] < kBin) {
-                        gather_tile<R>(vel, tidx(b[0], b[1], b[2]), w, dw, v, M, L);
-                    } else {
-                        const int gb[3] = {g0x + b[0], g0y + b[1], g0z + b[2]};
-                        gather_global<R>(P, gr, gb, w, dw, prg0, prg2, v, M, L);
-                        ++c_esc;
-                    }
-                    const R d[3] = {xi[0] - R(b[0]), xi[1] - R(b[1]), xi[2] - R(b[2])};
+                            for (int a = 0; a < 3; ++a) b[a] = bspline(xi[a], w[a], dw[a]);
+                            R M[3][3], L[3][3];
+                            if (b[0] >= 0 && b[0] < kBin && b[1] >= 0 && b[1] < kBin && b[2] >= 0 && b[2] < kBin) {
+                                gather_tile<R>(Sm.vel, tidx(b[0], b[1], b[2]), w, dw, v, M, L);
+                            } else {
+                                const int gb[3] = {g0x + b[0], g0y + b[1], g0z + b[2]};
+                                gather_global<R>(P, gr, gb, w, dw, prg0, prg2, v, M, L);
+                                ++c_esc;
+                            }
+                            const R d[3] = {xi[0] - R(b[0]), xi[1] - R(b[1]), xi[2] - R(b[2])};
 #pragma unroll
-                    for (int a = 0; a < 3; ++a) xi[a] = fma(v[a], dtdx, xi[a]);
-                    dirtyA = true;
-                    if (st == ST_CHIP) {
-                        edot = R(0);
-                    } else {
-                        // C = factor/dx^2 * B with B = dx (M - d v), then decay (or 0 in the far zone)
-                        const R cf = far ? R(0) : P.apic * idx_ * P.decay;
-#pragma unroll
-                        for (int a = 0; a < 3; ++a)
-#pragma unroll
-                            for (int c = 0; c < 3; ++c) Cm[a * 3 + c] = cf * (M[a][c] - d[c] * v[a]);
-                        have_C = true;
-                        // F <- (I + L dt) F  as  H <- H + Ldt (I + H)
-                        R Ld[9];
-#pragma unroll
-                        for (int a = 0; a < 3; ++a)
-#pragma unroll
-                            for (int c = 0; c < 3; ++c) Ld[a * 3 + c] = L[a][c] * dtdx;
-                        R Hn[9];
-#pragma unroll
-                        for (int a = 0; a < 3; ++a)
-#pragma unroll
-                            for (int c = 0; c < 3; ++c)
-                                Hn[a * 3 + c] = H[a * 3 + c] + Ld[a * 3 + c] + Ld[a * 3] * H[c] +
-                                                Ld[a * 3 + 1] * H[3 + c] + Ld[a * 3 + 2] * H[6 + c];
-#pragma unroll
-                        for (int q = 0; q < 9; ++q) H[q] = Hn[q];
-                        const R l00 = L[0][0] * idx_, l11 = L[1][1] * idx_, l22 = L[2][2] * idx_;
-                        const R s01 = (L[0][1] + L[1][0]) * idx_, s02 = (L[0][2] + L[2][0]) * idx_,
-                                s12 = (L[1][2] + L[2][1]) * idx_;
-                        edot = sqrt(R(2.0 / 3.0) * (l00 * l00 + l11 * l11 + l22 * l22 + R(0.5) * s01 * s01 +
-                                                      R(0.5) * s02 * s02 + R(0.5) * s12 * s12));
-                    }
-                }
-                // chip separation and fracture after the move (step counter parity)
-                if (P.chip_every > 0 && ((P.step0 + sa.k) % P.chip_every) == 0) {
-                    const double tipz = prg2 + P.tool_tip_dz;
-                    if (st == ST_ACTIVE) {
-                        const double zw = P.oz + ((double)g0z + (double)xi[2]) * P.dx;
-                        if (zw < tipz - P.dx * 1.5 && Dm > R(1e-6)) {
-                            st = ST_CHIP;
-                            const V4<R> s0 = ps.S[0][pi];
-                            const R rs = sqrt(s0.x * s0.x + s0.y * s0.y + s0.z * s0.z);
-                            ps.sres[pi] = fmax(ps.sres[pi], rs);
-                            ps.S[0][pi] = mk4<R>(0, 0, 0, 0);
-                            ps.S[1][pi] = mk4<R>(0, 0, 0, 0);
-                            Dm = fmax(Dm, P.Dth);
+                            for (int a = 0; a < 3; ++a) xi[a] = fma(v[a], dtdx, xi[a]);
                             dirtyA = true;
+                            if (st == ST_CHIP) {
+                                edot = R(0);
+                            } else {
+                                // C = factor/dx^2 * B with B = dx (M - d v), then decay (0 in the far zone)
+                                const R cf = far ? R(0) : P.apic * idx_ * P.decay;
+#pragma unroll
+                                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                                    for (int c = 0; c < 3; ++c) Cm[a * 3 + c] = cf * (M[a][c] - d[c] * v[a]);
+                                have_C = true;
+                                // F <- (I + L dt) F  as  H <- H + Ldt (I + H)
+                                R Ld[9];
+#pragma unroll
+                                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                                    for (int c = 0; c < 3; ++c) Ld[a * 3 + c] = L[a][c] * dtdx;
+                                R Hn[9];
+#pragma unroll
+                                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                                    for (int c = 0; c < 3; ++c)
+                                        Hn[a * 3 + c] = H[a * 3 + c] + Ld[a * 3 + c] + Ld[a * 3] * H[c] +
+                                                        Ld[a * 3 + 1] * H[3 + c] + Ld[a * 3 + 2] * H[6 + c];
+#pragma unroll
+                                for (int q = 0; q < 9; ++q) H[q] = Hn[q];
+                                const R l00 = L[0][0] * idx_, l11 = L[1][1] * idx_, l22 = L[2][2] * idx_;
+                                const R s01 = (L[0][1] + L[1][0]) * idx_, s02 = (L[0][2] + L[2][0]) * idx_,
+                                        s12 = (L[1][2] + L[2][1]) * idx_;
+                                edot = sqrt(R(2.0 / 3.0) * (l00 * l00 + l11 * l11 + l22 * l22 + R(0.5) * s01 * s01 +
+                                                              R(0.5) * s02 * s02 + R(0.5) * s12 * s12));
+                            }
                         }
-                    } else if (st == ST_CHIP && Dm >= P.Dth * R(1.5)) {
-                        const uint32_t seed = (uint32_t)ps.id[pi] * 2654435761u;
-                        const R rx = (R)((double)((seed >> 16) & 0xFF) / 255.0 - 0.5);
-                        const R ry = (R)((double)((seed >> 8) & 0xFF) / 255.0 - 0.5);
-                        const R rz = (R)((double)(seed & 0xFF) / 255.0 - 0.5);
-                        const R sp = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-                        const R pm = sp * R(0.3) + R(0.5);
-                        v[0] += rx * pm; v[1] += ry * pm; v[2] += rz * pm;
-                        Dm = P.Dth * R(0.5);
-                        dirtyA = true;
+                        // chip separation and fracture after the move (step counter parity)
+                        if (chip_now) {
+                            if (st == ST_ACTIVE) {
+                                const double tipz = ds(da(prg2, P.tool_tip_dz), dm(P.dx, 1.5));
+                                const double zw = P.oz + ((double)g0z + (double)xi[2]) * P.dx;
+                                if (zw < tipz && Dm > R(1e-6)) {
+                                    st = ST_CHIP;
+                                    const V4<R> s0 = ps.S[0][pi];
+                                    const R rs = sqrt(s0.x * s0.x + s0.y * s0.y + s0.z * s0.z);
+                                    ps.sres[pi] = fmax(ps.sres[pi], rs);
+                                    ps.S[0][pi] = mk4<R>(0, 0, 0, 0);
+                                    ps.S[1][pi] = mk4<R>(0, 0, 0, 0);
+                                    Dm = fmax(Dm, P.Dth);
+                                    dirtyA = true;
+                                }
+                            } else if (st == ST_CHIP && Dm >= P.Dth * R(1.5)) {
+                                const uint32_t seed = (uint32_t)ps.id[pi] * 2654435761u;
+                                const R rx = (R)((double)((seed >> 16) & 0xFF) / 255.0 - 0.5);
+                                const R ry = (R)((double)((seed >> 8) & 0xFF) / 255.0 - 0.5);
+                                const R rz = (R)((double)(seed & 0xFF) / 255.0 - 0.5);
+                                const R sp = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+                                const R pm = sp * R(0.3) + R(0.5);
+                                v[0] += rx * pm; v[1] += ry * pm; v[2] += rz * pm;
+                                Dm = P.Dth * R(0.5);
+                                dirtyA = true;
+                            }
+                        }
+                    } else {
+                        // P2G-only launch: velocity and strain rate come from memory
+                        const V4<R> b0 = ps.B[0][pi];
+                        v[0] = b0.x; v[1] = b0.y; v[2] = b0.z; edot = b0.w;
                     }
-                }
-            } else {
-                // P2G-only launch: velocity, C and strain rate come from memory
-                const V4<R> b0 = ps.B[0][pi];
-                v[0] = b0.x; v[1] = b0.y; v[2] = b0.z; edot = b0.w;
-            }
 
-            bool yielded = false;
+                    bool yielded = false;
+                    if (P2G) {
+                        // kill zone on the cell index, :130-139
+                        const int cx = g0x + (int)floor(xi[0]), cy = g0y + (int)floor(xi[1]),
+                                  cz = g0z + (int)floor(xi[2]);
+                        if (cx < 1 || cx >= P.nx - 2 || cy < 1 || cy >= P.ny - 2 || cz < 1 || cz >= P.nz - 2) {
+                            st = ST_INACTIVE;
+                            if (G2P) {
+                                // no later G2P writes this particle: store this step's v, strain rate and C
+                                ps.B[0][pi] = mk4<R>(v[0], v[1], v[2], edot);
+                                if (have_C) {
+                                    ps.B[1][pi] = mk4<R>(Cm[0], Cm[1], Cm[2], Cm[3]);
+                                    ps.B[2][pi] = mk4<R>(Cm[4], Cm[5], Cm[6], Cm[7]);
+                                    ps.B[3][pi] = mk4<R>(Cm[8], R(0), R(0), R(0));
+                                }
+                            }
+                        } else {
+                            // within one cell of the kill zone the stress is kept in memory, since a
+                            // kill in the next launch leaves the last computed stress as the state
+                            const bool near_kill = cx < 3 || cx >= P.nx - 4 || cy < 3 || cy >= P.ny - 4 ||
+                                                   cz < 3 || cz >= P.nz - 4;
+                            bool far = false;
+                            if (P.lod && st == ST_ACTIVE) {
+                                const double wx = P.ox + ((double)g0x + (double)xi[0]) * P.dx - prp0;
+                                const double wy = P.oy + ((double)g0y + (double)xi[1]) * P.dx - prp1;
+                                const double wz = P.oz + ((double)g0z + (double)xi[2]) * P.dx - (prp2 + P.tool_tip_dz);
+                                far = sqrt(wx * wx + wy * wy + wz * wz) > P.lod_r2;
+                            }
+                            bool skip = far || fixed || st == ST_CHIP;
+                            R Jv = R(1);
+                            R sig[6] = {0, 0, 0, 0, 0, 0};
+                            R sl[3] = {0, 0, 0};
+                            if (!skip && st == ST_ACTIVE) {
+                                const V4<R> a4 = ps.A[4][pi], a5 = ps.A[5][pi];
+                                R Hp[9] = {a4.x, a4.y, a4.z, a4.w, a5.x, a5.y, a5.z, a5.w, Hp8};
+                                R bsv[6];
+                                R* bsp = nullptr;
+                                if (P.Hkin > R(0)) {
+                                    const V4<R> k0 = ps.K[0][pi], k1 = ps.K[1][pi];
+                                    bsv[0] = k0.x; bsv[1] = k0.y; bsv[2] = k0.z; bsv[3] = k0.w;
+                                    bsv[4] = k1.x; bsv[5] = k1.y;
+                                    bsp = bsv;
+                                }
+                                JCOut jo = jc_update<R>(P, H, Hp, eps, dT, Dm, edot, sig, sl, Jv, &ps.sres[pi], bsp,
+                                                        errf);
+                                if (jo.yielded) {
+                                    yielded = true;
+                                    dirtyA = true;
+                                    Hp8 = Hp[8];
+                                    ps.A[4][pi] = mk4<R>(Hp[0], Hp[1], Hp[2], Hp[3]);
+                                    ps.A[5][pi] = mk4<R>(Hp[4], Hp[5], Hp[6], Hp[7]);
+                                    if (bsp) {
+                                        ps.K[0][pi] = mk4<R>(bsv[0], bsv[1], bsv[2], bsv[3]);
+                                        ps.K[1][pi] = mk4<R>(bsv[4], bsv[5], R(0), R(0));
+                                    }
+                                }
+                                if (jo.to_chip) { st = ST_CHIP; skip = true; }
+                                if (sa.sigma_all || Dm > R(1e-6) || P.lod || near_kill) {
+                                    ps.S[0][pi] = mk4<R>(sig[0], sig[1], sig[2], sig[3]);
+                                    ps.S[1][pi] = mk4<R>(sig[4], sig[5], R(0), R(0));
+                                }
+                            }
+                            // C of the particle: from this launch's gather, or the frozen value of
+                            // a CHIP particle (g2pKernel keeps it)
+                            if (!have_C && !fixed) {
+                                const V4<R> c1 = ps.B[1][pi], c2 = ps.B[2][pi], c3 = ps.B[3][pi];
+                                Cm[0] = c1.x; Cm[1] = c1.y; Cm[2] = c1.z; Cm[3] = c1.w;
+                                Cm[4] = c2.x; Cm[5] = c2.y; Cm[6] = c2.z; Cm[7] = c2.w; Cm[8] = c3.x;
+                            }
+                            if (!fixed && have_C && st == ST_CHIP && st_in != ST_CHIP) {
+                                // turned CHIP this launch: freeze C as the reference does
+                                ps.B[1][pi] = mk4<R>(Cm[0], Cm[1], Cm[2], Cm[3]);
+                                ps.B[2][pi] = mk4<R>(Cm[4], Cm[5], Cm[6], Cm[7]);
+                                ps.B[3][pi] = mk4<R>(Cm[8], R(0), R(0), R(0));
+                                wrote_C = true;
+                            }
+                            // scatter payload: Q = m (v - dx C d) + f_ext dt, R = m dx C,
+                            // S = -dt V J sigma / dx (sigma with the reference's trial lower triangle)
+                            const int bb[3] = {(int)floor(xi[0] - R(0.5)), (int)floor(xi[1] - R(0.5)),
+                                               (int)floor(xi[2] - R(0.5))};
+                            const R m = P.pmass;
+                            R Q[3] = {0, 0, 0}, Rm[9], S[9];
+#pragma unroll
+                            for (int q = 0; q < 9; ++q) { Rm[q] = R(0); S[q] = R(0); }
+                            if (!fixed) {
+                                const R d[3] = {xi[0] - R(bb[0]), xi[1] - R(bb[1]), xi[2] - R(bb[2])};
+                                const R mdx = m * (R)P.dx;
+                                R ef[3] = {0, 0, 0};
+                                if (sa.use_ext && P.ext_r > 0.0 && (st == ST_ACTIVE || st == ST_CHIP)) {
+                                    const double ex = P.ox + ((double)g0x + (double)xi[0]) * P.dx - P.ext_c[0];
+                                    const double ey = P.oy + ((double)g0y + (double)xi[1]) * P.dx - P.ext_c[1];
+                                    const double ez = P.oz + ((double)g0z + (double)xi[2]) * P.dx - P.ext_c[2];
+                                    const double dist = sqrt(ex * ex + ey * ey + ez * ez);
+                                    if (dist < P.ext_r) {
+                                        const double fw = (1.0 - dist / P.ext_r) * P.dt;
+                                        ef[0] = (R)(P.ext_f[0] * fw); ef[1] = (R)(P.ext_f[1] * fw);
+                                        ef[2] = (R)(P.ext_f[2] * fw);
+                                    }
+                                }
+#pragma unroll
+                                for (int a = 0; a < 3; ++a) {
+                                    Q[a] = m * v[a] -
+                                           mdx * (Cm[a * 3] * d[0] + Cm[a * 3 + 1] * d[1] + Cm[a * 3 + 2] * d[2]) + ef[a];
+#pragma unroll
+                                    for (int c = 0; c < 3; ++c) Rm[a * 3 + c] = mdx * Cm[a * 3 + c];
+                                }
+                                const R sf = skip ? R(0) : -(R)P.dt * P.pvol * Jv * idx_;
+                                S[0] = sf * sig[0]; S[4] = sf * sig[1]; S[8] = sf * sig[2];
+                                S[1] = sf * sig[3]; S[3] = sf * sl[0];
+                                S[2] = sf * sig[4]; S[6] = sf * sl[1];
+                                S[5] = sf * sig[5]; S[7] = sf * sl[2];
+                            }
+                            if (bb[0] >= 0 && bb[0] < kBin && bb[1] >= 0 && bb[1] < kBin && bb[2] >= 0 &&
+                                bb[2] < kBin) {
+                                scell = bb[0] + kBin * (bb[1] + kBin * bb[2]);
+                                Sm.pay[0][slot] = xi[0]; Sm.pay[1][slot] = xi[1]; Sm.pay[2][slot] = xi[2];
+#pragma unroll
+                                for (int a = 0; a < 3; ++a) Sm.pay[3 + a][slot] = Q[a];
+#pragma unroll
+                                for (int q = 0; q < 9; ++q) { Sm.pay[6 + q][slot] = Rm[q]; Sm.pay[15 + q][slot] = S[q]; }
+                            } else {
+                                R w[3][3], dw[3][3];
+                                int b2[3];
+#pragma unroll
+                                for (int a = 0; a < 3; ++a) b2[a] = bspline(xi[a], w[a], dw[a]);
+                                const R Qa[3] = {Q[0], Q[1], Q[2]};
+                                const R Rma[3][3] = {{Rm[0], Rm[1], Rm[2]}, {Rm[3], Rm[4], Rm[5]}, {Rm[6], Rm[7], Rm[8]}};
+                                const R Sa[3][3] = {{S[0], S[1], S[2]}, {S[3], S[4], S[5]}, {S[6], S[7], S[8]}};
+                                const int gb[3] = {g0x + b2[0], g0y + b2[1], g0z + b2[2]};
+                                scatter_global<R>(P, gw, gb, w, dw, m, Qa, Rma, Sa, fixed);
+                                ++c_esc;
+                            }
+                        }
+                    }
+
+                    // write back
+                    if (dirtyA) {
+                        ps.A[0][pi] = mk4<R>(xi[0], xi[1], xi[2], eps);
+                        ps.A[1][pi] = mk4<R>(H[0], H[1], H[2], H[3]);
+                        ps.A[2][pi] = mk4<R>(H[4], H[5], H[6], H[7]);
+                        ps.A[3][pi] = mk4<R>(H[8], Hp8, dT, Dm);
+                    }
+                    if (st != st_in) ps.status[pi] = st;
+                    if (G2P && sa.write_out && st != ST_INACTIVE) {
+                        if (fixed) {
+                            const V4<R> b0 = ps.B[0][pi];
+                            ps.B[0][pi] = mk4<R>(R(0), R(0), R(0), b0.w);
+                        } else {
+                            ps.B[0][pi] = mk4<R>(v[0], v[1], v[2], edot);
+                            if (have_C && !wrote_C && st_in != ST_CHIP) {
+                                ps.B[1][pi] = mk4<R>(Cm[0], Cm[1], Cm[2], Cm[3]);
+                                ps.B[2][pi] = mk4<R>(Cm[4], Cm[5], Cm[6], Cm[7]);
+                                ps.B[3][pi] = mk4<R>(Cm[8], R(0), R(0), R(0));
+                            }
+                        }
+                    }
+                    c_yield += yielded ? 1 : 0;
+                }
+                myc[sidx] = scell;
+                myr[sidx] = (P2G && scell >= 0) ? atomicAdd(&Sm.cnt[scell], 1) : 0;
+            }
             if (P2G) {
-                // kill zone on the cell index, :130-139
-                const int cx = g0x + (int)floor(xi[0]), cy = g0y + (int)floor(xi[1]), cz = g0z + (int)floor(xi[2]);
-                if (cx < 1 || cx >= P.nx - 2 || cy < 1 || cy >= P.ny - 2 || cz < 1 || cz >= P.nz - 2) {
-                    st = ST_INACTIVE;
-                } else {
-                    bool far = false;
-                    if (P.lod && st == ST_ACTIVE) {
-                        const double wx = P.ox + ((double)g0x + (double)xi[0]) * P.dx - prp0;
-                        const double wy = P.oy + ((double)g0y + (double)xi[1]) * P.dx - prp1;
-                        const double wz = P.oz + ((double)g0z + (double)xi[2]) * P.dx - (prp2 + P.tool_tip_dz);
-                        far = sqrt(wx * wx + wy * wy + wz * wz) > P.lod_r2;
-                    }
-                    bool skip = far || fixed || st == ST_CHIP;
-                    R Jv = R(1);
-                    R sl[3] = {0, 0, 0};
+                __syncthreads();
+                // group the staged particles by cell: exclusive scan of the 64 counts
+                if (warp == 0) {
+                    const int c0 = Sm.cnt[lane], c1 = Sm.cnt[lane + 32];
+                    int x0 = c0, x1 = c1;
 #pragma unroll
-                    for (int q = 0; q < 6; ++q) sig[q] = R(0);
-                    if (!skip && st == ST_ACTIVE) {
-                        const V4<R> a4 = ps.A[4][pi], a5 = ps.A[5][pi];
-                        R Hp[9] = {a4.x, a4.y, a4.z, a4.w, a5.x, a5.y, a5.z, a5.w, Hp8};
-                        R bsv[6];
-                        R* bsp = nullptr;
-                        if (P.Hkin > R(0)) {
-                            const V4<R> k0 = ps.K[0][pi], k1 = ps.K[1][pi];
-                            bsv[0] = k0.x; bsv[1] = k0.y; bsv[2] = k0.z; bsv[3] = k0.w; bsv[4] = k1.x; bsv[5] = k1.y;
-                            bsp = bsv;
-                        }
-                        const R D_before = Dm;
-                        JCOut jo = jc_update<R>(P, H, Hp, eps, dT, Dm, edot, sig, sl, Jv, &ps.sres[pi], bsp, errf);
-                        if (jo.yielded) {
-                            yielded = true;
-                            dirtyHp = true;
-                            dirtyA = true;
-                            Hp8 = Hp[8];
-                            ps.A[4][pi] = mk4<R>(Hp[0], Hp[1], Hp[2], Hp[3]);
-                            ps.A[5][pi] = mk4<R>(Hp[4], Hp[5], Hp[6], Hp[7]);
-                            if (bsp) {
-                                ps.K[0][pi] = mk4<R>(bsv[0], bsv[1], bsv[2], bsv[3]);
-                                ps.K[1][pi] = mk4<R>(bsv[4], bsv[5], R(0), R(0));
-                            }
-                        }
-                        (void)D_before;
-                        if (jo.to_chip) { st = ST_CHIP; skip = true; }
-                        dirtyS = sa.sigma_all || Dm > R(1e-6) || P.lod;
-                        if (dirtyS) {
-                            ps.S[0][pi] = mk4<R>(sig[0], sig[1], sig[2], sig[3]);
-                            ps.S[1][pi] = mk4<R>(sig[4], sig[5], R(0), R(0));
-                        }
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y0 = __shfl_up_sync(0xffffffffu, x0, o), y1 = __shfl_up_sync(0xffffffffu, x1, o);
+                        if (lane >= o) { x0 += y0; x1 += y1; }
                     }
-                    // C of the particle: from this launch's gather, or the frozen
-                    // value of a CHIP/FIXED particle (g2pKernel keeps it)
-                    if (!have_C && !fixed) {
-                        const V4<R> c1 = ps.B[1][pi], c2 = ps.B[2][pi], c3 = ps.B[3][pi];
-                        Cm[0] = c1.x; Cm[1] = c1.y; Cm[2] = c1.z; Cm[3] = c1.w;
-                        Cm[4] = c2.x; Cm[5] = c2.y; Cm[6] = c2.z; Cm[7] = c2.w; Cm[8] = c3.x;
-                    }
-                    if (!fixed && have_C && st == ST_CHIP && st_in != ST_CHIP) {
-                        // turned CHIP this launch: freeze C as the reference does
-                        ps.B[1][pi] = mk4<R>(Cm[0], Cm[1], Cm[2], Cm[3]);
-                        ps.B[2][pi] = mk4<R>(Cm[4], Cm[5], Cm[6], Cm[7]);
-                        ps.B[3][pi] = mk4<R>(Cm[8], R(0), R(0), R(0));
-                        wrote_C = true;
-                    }
-                    // scatter
-                    R w[3][3], dw[3][3];
-                    int b[3];
-#pragma unroll
-                    for (int a = 0; a < 3; ++a) b[a] = bspline(xi[a], w[a], dw[a]);
-                    const R m = P.pmass;
-                    R Q[3], Rm[3][3], S[3][3];
-                    if (!fixed) {
-                        const R d[3] = {xi[0] - R(b[0]), xi[1] - R(b[1]), xi[2] - R(b[2])};
-                        const R mdx = m * (R)P.dx;
-                        R ef[3] = {0, 0, 0};
-                        if (sa.use_ext && P.ext_r > 0.0) {
-                            const double ex = P.ox + ((double)g0x + (double)xi[0]) * P.dx - P.ext_c[0];
-                            const double ey = P.oy + ((double)g0y + (double)xi[1]) * P.dx - P.ext_c[1];
-                            const double ez = P.oz + ((double)g0z + (double)xi[2]) * P.dx - P.ext_c[2];
-                            const double dist = sqrt(ex * ex + ey * ey + ez * ez);
-                            if ((st == ST_ACTIVE || st == ST_CHIP) && dist < P.ext_r) {
-                                const double fw = (1.0 - dist / P.ext_r) * P.dt;
-                                ef[0] = (R)(P.ext_f[0] * fw); ef[1] = (R)(P.ext_f[1] * fw); ef[2] = (R)(P.ext_f[2] * fw);
-                            }
-                        }
-#pragma unroll
-                        for (int a = 0; a < 3; ++a) {
-                            Q[a] = m * v[a] - mdx * (Cm[a * 3] * d[0] + Cm[a * 3 + 1] * d[1] + Cm[a * 3 + 2] * d[2]) + ef[a];
-#pragma unroll
-                            for (int c = 0; c < 3; ++c) Rm[a][c] = mdx * Cm[a * 3 + c];
-                        }
-                        const R sf = skip ? R(0) : -(R)P.dt * P.pvol * Jv * idx_;
-                        S[0][0] = sf * sig[0]; S[1][1] = sf * sig[1]; S[2][2] = sf * sig[2];
-                        S[0][1] = sf * sig[3]; S[1][0] = sf * sl[0];
-                        S[0][2] = sf * sig[4]; S[2][0] = sf * sl[1];
-                        S[1][2] = sf * sig[5]; S[2][1] = sf * sl[2];
-                    } else {
-#pragma unroll
-                        for (int a = 0; a < 3; ++a) {
-                            Q[a] = R(0);
-#pragma unroll
-                            for (int c = 0; c < 3; ++c) { Rm[a][c] = R(0); S[a][c] = R(0); }
-                        }
-                        // FIXED: an external force still acts (reference adds w*ext_f)
-                        if (sa.use_ext && P.ext_r > 0.0) { /* ext force is applied to ACTIVE and CHIP only */ }
-                    }
-                    if (b[0] >= 0 && b[0] < kBin && b[1] >= 0 && b[1] < kBin && b[2] >= 0 && b[2] < kBin) {
-                        scatter_tile<R>(acc, tidx(b[0], b[1], b[2]), w, dw, m, Q, Rm, S, fixed);
-                    } else {
-                        const int gb[3] = {g0x + b[0], g0y + b[1], g0z + b[2]};
-                        scatter_global<R>(P, gw, gb, w, dw, m, Q, Rm, S, fixed);
-                        ++c_esc;
-                    }
+                    const int tot0 = __shfl_sync(0xffffffffu, x0, 31);
+                    Sm.cstart[lane] = x0 - c0;
+                    Sm.cstart[lane + 32] = tot0 + x1 - c1;
+                    Sm.ccount[lane] = c0;
+                    Sm.ccount[lane + 32] = c1;
+                    Sm.cnt[lane] = 0;
+                    Sm.cnt[lane + 32] = 0;
                 }
+                __syncthreads();
+#pragma unroll
+                for (int sidx = 0; sidx < StepCfg<R>::kPerThread; ++sidx)
+                    if (myc[sidx] >= 0) Sm.order[Sm.cstart[myc[sidx]] + myr[sidx]] = (short)(tid + sidx * kNT);
+                __syncthreads();
+                cell_accumulate<R>(Sm, tid & (kCellsPerBin - 1), tid >> 6, P.pmass);
+                __syncthreads();
             }
-
-            // write back
-            if (dirtyA) {
-                ps.A[0][pi] = mk4<R>(xi[0], xi[1], xi[2], eps);
-                ps.A[1][pi] = mk4<R>(H[0], H[1], H[2], H[3]);
-                ps.A[2][pi] = mk4<R>(H[4], H[5], H[6], H[7]);
-                ps.A[3][pi] = mk4<R>(H[8], Hp8, dT, Dm);
-            }
-            if (st != st_in) ps.status[pi] = st;
-            if (G2P && sa.write_out) {
-                if (fixed) {
-                    const V4<R> b0 = ps.B[0][pi];
-                    ps.B[0][pi] = mk4<R>(R(0), R(0), R(0), b0.w);
-                } else {
-                    ps.B[0][pi] = mk4<R>(v[0], v[1], v[2], edot);
-                    if (have_C && !wrote_C && st_in != ST_CHIP) {
-                        ps.B[1][pi] = mk4<R>(Cm[0], Cm[1], Cm[2], Cm[3]);
-                        ps.B[2][pi] = mk4<R>(Cm[4], Cm[5], Cm[6], Cm[7]);
-                        ps.B[3][pi] = mk4<R>(Cm[8], R(0), R(0), R(0));
-                    }
-                }
-            }
-            c_yield += yielded ? 1 : 0;
-            (void)dirtyHp;
-            (void)dirtyS;
         }
-        __syncthreads();
 
         if (P2G) {
-            for (int nidx = tid; nidx < kTileNodes; nidx += NT) {
-                const int lx = nidx % kTile, ly = (nidx / kTile) % kTile, lz = nidx / (kTile * kTile);
-                const int t = tidx(lx, ly, lz);
-                const R m = acc[0][t];
+            // tile node = sum of the cell blocks whose stencils cover it
+            for (int nidx = tid; nidx < kTileNodes; nidx += kNT) {
+                const int X = nidx % kTile, Y = (nidx / kTile) % kTile, Z = nidx / (kTile * kTile);
+                R m = R(0), px = R(0), py = R(0), pz = R(0);
+                for (int cz = max(0, Z - 2); cz <= min(kBin - 1, Z); ++cz)
+                    for (int cy = max(0, Y - 2); cy <= min(kBin - 1, Y); ++cy)
+                        for (int cx = max(0, X - 2); cx <= min(kBin - 1, X); ++cx) {
+                            const int cell = cx + kBin * (cy + kBin * cz);
+                            const int o = (X - cx) + 3 * (Y - cy) + 9 * (Z - cz);
+                            m += Sm.cacc[0][o][cell];
+                            px += Sm.cacc[1][o][cell];
+                            py += Sm.cacc[2][o][cell];
+                            pz += Sm.cacc[3][o][cell];
+                        }
                 if (m == R(0)) continue;
-                const int gx = g0x + lx, gy = g0y + ly, gz = g0z + lz;
+                const int gx = g0x + X, gy = g0y + Y, gz = g0z + Z;
                 if (gx >= P.nx || gy >= P.ny || gz >= P.nz) continue;
-                vec_atomic_add<R>(&gw[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], m, acc[1][t], acc[2][t],
-                                  acc[3][t]);
+                vec_atomic_add<R>(&gw[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], m, px, py, pz);
             }
-            __syncthreads();
         }
+        __syncthreads();
     }
     // counters: warp-reduce, one atomic per warp
 #pragma unroll
@@ -835,10 +970,19 @@ __global__ void __launch_bounds__(256) k_step(const Inst<R>* __restrict__ insts,
         c_yield += __shfl_down_sync(0xffffffffu, c_yield, o);
         errf |= __shfl_down_sync(0xffffffffu, errf, o);
     }
-    if ((tid & 31) == 0) {
+    if (lane == 0) {
         if (c_esc) atomicAdd(&ctr[0], c_esc);
         if (c_yield) atomicAdd(&ctr[1], c_yield);
         if (errf) atomicOr(err, errf);
+    }
+}
+
+template <typename R, bool G2P, bool P2G> static void set_smem_attr() {
+    static bool done = false;
+    if (!done) {
+        cudaFuncSetAttribute(k_step<R, G2P, P2G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)step_smem_bytes<R>());
+        done = true;
     }
 }
 
@@ -846,6 +990,7 @@ template <typename R>
 void launch_step(const Inst<R>* insts, const Work* work, const int* n_work, int max_work, const PState<R>& ps,
                  const StepArgs& a, int rbuf, bool g2p, bool p2g, int threads, int ctas_per_sm, int* err,
                  unsigned long long* counters, cudaStream_t st) {
+    (void)threads;
     static int sms = 0;
     if (!sms) {
         int dev = 0;
@@ -856,14 +1001,17 @@ void launch_step(const Inst<R>* insts, const Work* work, const int* n_work, int 
     if (max_work <= 0) return;
     int grid = sms * (ctas_per_sm > 0 ? ctas_per_sm : 4);
     if (grid > max_work) grid = max_work;
-    if (threads <= 0) threads = 128;
-    if (threads > 256) threads = 256;
-    if (g2p && p2g)
-        k_step<R, true, true><<<grid, threads, 0, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
-    else if (g2p)
-        k_step<R, true, false><<<grid, threads, 0, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
-    else
-        k_step<R, false, true><<<grid, threads, 0, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+    const size_t smem = step_smem_bytes<R>();
+    if (g2p && p2g) {
+        set_smem_attr<R, true, true>();
+        k_step<R, true, true><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+    } else if (g2p) {
+        set_smem_attr<R, true, false>();
+        k_step<R, true, false><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+    } else {
+        set_smem_attr<R, false, true>();
+        k_step<R, false, true><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+    }
     ++launch_counter();
 }
 

@@ -62,6 +62,7 @@ class MpmMetrics(C.Structure):
         ("max_temperature", _d), ("max_von_mises", _d), ("max_plastic_strain", _d), ("mean_plastic_strain", _d),
         ("n_active", _i64), ("n_chip", _i64), ("n_fixed", _i64), ("n_inactive", _i64),
         ("bounds_min", _d * 3), ("bounds_max", _d * 3), ("n_escaped", _i64), ("n_sorts", _i64),
+        ("n_yielded", _i64),
     ]
 
     def as_dict(self) -> dict:
@@ -107,6 +108,8 @@ def lib() -> C.CDLL:
             "mpm_get_stream": (_i32, [_vp, P(_vp)]),
             "mpm_reset_clock": (_i32, [_vp]),
             "mpm_launch_count": (_i32, [_vp, P(_i64)]),
+            "mpm_profile_enable": (_i32, [_vp, _i32]),
+            "mpm_profile_read": (_i32, [_vp, P(_d), P(_i64)]),
             "mpm_last_error": (C.c_char_p, [_vp]),
             "mpm_status_string": (C.c_char_p, [_i32]),
         }

@@ -121,6 +121,14 @@ class Solver:
         self._check(self._lib.mpm_download(self.h, C.byref(s)))
         return out
 
+    def download_into(self, bufs: Dict[str, np.ndarray], elem: int = 8) -> None:
+        """Download into caller-owned arrays (e.g. pinned host memory)."""
+        s = A.MpmParticlesSoa()
+        s.elem = elem
+        for name, a in bufs.items():
+            setattr(s, name, a.ctypes.data)
+        self._check(self._lib.mpm_download(self.h, C.byref(s)))
+
     def export_aos(self) -> np.ndarray:
         n = self.counts()[0]
         buf = np.zeros(max(n, 1) * 504, dtype=np.uint8)
@@ -157,6 +165,14 @@ class Solver:
         n, k, t = C.c_int64(), C.c_int64(), C.c_double()
         self._check(self._lib.mpm_get_counts(self.h, C.byref(n), C.byref(k), C.byref(t)))
         return n.value, k.value, t.value
+
+    def profile(self, enable: bool = True) -> None:
+        self._check(self._lib.mpm_profile_enable(self.h, 1 if enable else 0))
+
+    def profile_read(self):
+        ms, n = C.c_double(), C.c_int64()
+        self._check(self._lib.mpm_profile_read(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
 
     def launches(self) -> int:
         c = C.c_int64()

@@ -216,3 +216,76 @@ def cylinder_samples(case: dict, spacing_cells: float = 0.5) -> np.ndarray:
     ys = p["origin"][1] + np.arange(0.0, (p["ny"] - 1) * dx + 1e-12, h) - tool["position"][1]
     T, Y = np.meshgrid(th, ys, indexing="ij")
     return np.stack([R * np.cos(T).ravel(), Y.ravel(), R * np.sin(T).ravel()], axis=1)
+
+
+def wedge_samples(case: dict, spacing_cells: float = 0.5) -> np.ndarray:
+    """Surface samples of the rounded wedge (offsets from the edge-circle
+    centre): the edge arc between the flank and rake normals, the rake face up
+    to the top of the grid and the flank face back to the grid's -x side,
+    extruded over the grid's y extent."""
+    p, tool = case["params"], case["tool"]
+    dx, r = p["dx"], tool["radius"]
+    h = spacing_cells * dx
+    g, a = tool["rake"], tool["clearance"]
+    th0, th1 = math.atan2(-math.cos(a), -math.sin(a)), g  # flank normal .. rake normal (exterior arc)
+    nth = max(4, int(math.ceil(r * (th1 - th0) / h)) + 1)
+    th = np.linspace(th0, th1, nth)
+    pts = [np.stack([r * np.cos(th), r * np.sin(th)], axis=1)]
+    px, pz = tool["position"][0], tool["position"][2]
+    ztop = p["origin"][2] + (p["nz"] - 1) * dx
+    up = max(0.0, ztop - (pz + r * math.sin(g)))
+    s = np.arange(h, up + h, h)
+    pts.append(np.stack([r * math.cos(g) - s * math.sin(g), r * math.sin(g) + s * math.cos(g)], axis=1))
+    back = max(0.0, (px - r * math.sin(a)) - p["origin"][0])
+    s = np.arange(h, back + h, h)
+    pts.append(np.stack([-r * math.sin(a) - s * math.cos(a), -r * math.cos(a) + s * math.sin(a)], axis=1))
+    xz = np.concatenate(pts, axis=0)
+    ys = p["origin"][1] + np.arange(0.0, (p["ny"] - 1) * dx + 1e-12, h) - tool["position"][1]
+    XZ = np.repeat(xz, len(ys), axis=0)
+    Y = np.tile(ys, len(xz))
+    return np.stack([XZ[:, 0], Y, XZ[:, 1]], axis=1)
+
+
+def tool_samples(case: dict, spacing_cells: float = 0.5) -> np.ndarray:
+    if case["tool"]["shape"] == A.SHAPE_CYLINDER_Y:
+        return cylinder_samples(case, spacing_cells)
+    return wedge_samples(case, spacing_cells)
+
+
+def generate_box_chunked(case: dict, zchunk: int = 8):
+    """generate_box for large boxes, `zchunk` cell layers at a time; returns
+    (x, y, z, status) with the ids implied by the order."""
+    box = case["box"]
+    c0, c1 = list(box["c0"]), list(box["c1"])
+    xs, ys, zs, sts = [], [], [], []
+    for z0 in range(c0[2], c1[2], zchunk):
+        sub = dict(case)
+        b = dict(box)
+        b["c0"] = (c0[0], c0[1], z0)
+        b["c1"] = (c1[0], c1[1], min(z0 + zchunk, c1[2]))
+        b["fixed_layers"] = box["fixed_layers"] - (z0 - c0[2])
+        sub["box"] = b
+        part = _generate_box_offset(sub, cell_offset=(z0 - c0[2]) * (c1[0] - c0[0]) * (c1[1] - c0[1]))
+        xs.append(part["x"]); ys.append(part["y"]); zs.append(part["z"]); sts.append(part["status"])
+    return np.concatenate(xs), np.concatenate(ys), np.concatenate(zs), np.concatenate(sts)
+
+
+def _generate_box_offset(case: dict, cell_offset: int) -> Dict[str, np.ndarray]:
+    p, box, tool = case["params"], case["box"], case["tool"]
+    c0, c1, ppc = box["c0"], box["c1"], box["ppc"]
+    wx, wy, wz = (c1[i] - c0[i] for i in range(3))
+    cand = np.arange(wx * wy * wz * ppc, dtype=np.int64)
+    cell, k = cand // ppc, cand % ppc
+    ix, iy, iz = cell % wx, (cell // wx) % wy, cell // (wx * wy)
+    seed = int(box["seed"])
+    u = philox4x32_10(seed & 0xFFFFFFFF, seed >> 32, cell + cell_offset, k, np.full_like(cell, box["instance"]),
+                      np.zeros_like(cell))
+    dx, org = p["dx"], p["origin"]
+    x = org[0] + ((c0[0] + ix) + u[0].astype(np.float64)) * dx
+    y = org[1] + ((c0[1] + iy) + u[1].astype(np.float64)) * dx
+    z = org[2] + ((c0[2] + iz) + u[2].astype(np.float64)) * dx
+    keep = np.ones(len(cand), dtype=bool)
+    if tool and tool.get("mode", A.TOOL_NONE) != A.TOOL_NONE:
+        keep = tool_sdf(tool, x, z, tool["position"][0], tool["position"][2]) > 0.0
+    status = np.where(iz[keep] < box["fixed_layers"], A.FIXED, A.ACTIVE).astype(np.int32)
+    return dict(x=x[keep], y=y[keep], z=z[keep], status=status)

@@ -139,8 +139,9 @@ typedef struct mpm_metrics {
     double max_temperature, max_von_mises, max_plastic_strain, mean_plastic_strain;
     int64_t n_active, n_chip, n_fixed, n_inactive;
     double bounds_min[3], bounds_max[3];   /* ACTIVE and CHIP particles */
-    int64_t n_escaped;                     /* particles handled off their bin tile since the last re-bin */
-    int64_t n_sorts;
+    int64_t n_escaped;                     /* particle updates done off their bin tile (cumulative) */
+    int64_t n_sorts;                       /* re-bins so far */
+    int64_t n_yielded;                     /* particle updates that took a plastic return (cumulative) */
 } mpm_metrics;
 
 typedef struct mpm_handle mpm_handle;
@@ -203,6 +204,14 @@ mpm_status mpm_get_counts(const mpm_handle *h, int64_t *n_particles, int64_t *n_
 mpm_status mpm_get_stream(const mpm_handle *h, void **stream);
 /* Replaces reset() (src/MPMSolver.cu:1227-1230): time and step counter to 0. */
 mpm_status mpm_reset_clock(mpm_handle *h);
+
+/* Record CUDA events around every launch of the step kernel (enable != 0),
+ * for timing the dominant kernel inside a longer run.  mpm_profile_read
+ * synchronises, returns the summed device time (ms) and count of the fused
+ * G2P+P2G launches (or of all step launches under the split schedule) since
+ * the last read, and clears them. */
+mpm_status mpm_profile_enable(mpm_handle *h, int32_t enable);
+mpm_status mpm_profile_read(mpm_handle *h, double *kernel_ms, int64_t *kernel_launches);
 
 /* Count of the library's own kernel launches issued by this handle so far. */
 mpm_status mpm_launch_count(const mpm_handle *h, int64_t *count);

@@ -212,6 +212,9 @@ class RefKern:
         L.ref_bench.restype = _i32
         L.ref_bench.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcState), C.POINTER(OrcTool), _d, _i32, _i32,
                                 C.POINTER(_d)]
+        L.ref_bench_positions.restype = _i32
+        L.ref_bench_positions.argtypes = [C.POINTER(OrcParams), _vp, _vp, _vp, _vp, _i32, _d, _d, _d,
+                                          C.POINTER(OrcTool), _d, _i32, _i32, C.POINTER(_d), C.POINTER(C.c_longlong)]
         self.L = L
 
     def step(self, case: dict, state: Dict[str, np.ndarray], nsteps: int, step0: int = 0, t0: float = 0.0,
@@ -241,3 +244,29 @@ class RefKern:
         if rc != 0:
             raise RuntimeError(f"reference bench failed ({rc}): {self.L.ref_last_error().decode()}")
         return ms.value, b.result()
+
+    def bench_positions(self, case: dict, x, y, z, status, warmup: int, steps: int, samples=None):
+        """Time the reference kernels on particles given by position and status
+        (MPMParticle defaults elsewhere), with the tool rasterised from
+        `samples`.  Returns (device ms of the timed steps, live particles)."""
+        p = orc_params(case)
+        if samples is not None:
+            p.tool_mode = TOOL_RASTER
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (x, y, z)]
+        st = np.ascontiguousarray(status, np.int32)
+        tool = OrcTool()
+        cols = []
+        if samples is not None:
+            smp = np.ascontiguousarray(samples, np.float64)
+            cols = [np.ascontiguousarray(smp[:, k]) for k in range(3)]
+            tool.n = len(smp)
+            tool.ox, tool.oy, tool.oz = (c.ctypes.data for c in cols)
+        ms, live = C.c_double(), C.c_longlong()
+        pr = case["params"]
+        rc = self.L.ref_bench_positions(C.byref(p), arrs[0].ctypes.data, arrs[1].ctypes.data, arrs[2].ctypes.data,
+                                        st.ctypes.data, len(st), float(pr["particle_mass"]),
+                                        float(pr["particle_volume"]), float(case["box"]["T0"]), C.byref(tool),
+                                        float(case["dt"]), int(warmup), int(steps), C.byref(ms), C.byref(live))
+        if rc != 0:
+            raise RuntimeError(f"reference bench failed ({rc}): {self.L.ref_last_error().decode()}")
+        return ms.value, live.value

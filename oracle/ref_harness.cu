@@ -200,6 +200,21 @@ int setup(RefRun& r, const orc_params* p, int n, int ntool) {
     return 0;
 }
 
+// MPMParticle defaults (its constructor) with the given position, status,
+// id, mass, volume and temperature: the state MPMSolver::initializeParticleBox
+// writes (src/MPMSolver.cu:1315-1327).
+__global__ void fill_particles(MPMParticle* out, const double* x, const double* y, const double* z, const int* status,
+                               int n, double mass, double vol, double T0) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    MPMParticle p;
+    p.x = x[i]; p.y = y[i]; p.z = z[i];
+    p.mass = mass; p.volume = vol; p.density = mass / vol; p.temperature = T0;
+    p.id = i;
+    p.status = static_cast<ParticleStatus>(status[i]);
+    out[i] = p;
+}
+
 }  // namespace
 
 extern "C" {
@@ -277,6 +292,9 @@ int ref_stats(orc_state* s, double out[4]) {
 // even steps, and the tool nodes moved by the reference's own
 // interpolateToolNodesKernel (:494-504).  Returns device milliseconds of the
 // timed steps in *ms_out and leaves the final state in s.
+static int bench_loaded(RefRun& r, const orc_params* p, const orc_tool_samples* tool, double dt, int warmup,
+                        int steps, double* ms_out);
+
 int ref_bench(const orc_params* p, orc_state* s, const orc_tool_samples* tool, double dt, int warmup, int steps,
               double* ms_out) {
     int rc = check_reference_constants(p);
@@ -289,6 +307,54 @@ int ref_bench(const orc_params* p, orc_state* s, const orc_tool_samples* tool, d
         soa_to_aos(s, h);
         HCHECK(cudaMemcpy(r.d_p, h.data(), sizeof(MPMParticle) * (size_t)s->n, cudaMemcpyHostToDevice));
     }
+    if ((rc = bench_loaded(r, p, tool, dt, warmup, steps, ms_out))) return rc;
+    std::vector<MPMParticle> h(s->n);
+    HCHECK(cudaMemcpy(h.data(), r.d_p, sizeof(MPMParticle) * (size_t)s->n, cudaMemcpyDeviceToHost));
+    aos_to_soa(h, s);
+    return 0;
+}
+
+// Same timing from particle positions only (large workloads): the AoS array is
+// filled on the device.  Returns the count of non-INACTIVE particles at the
+// end in *n_live.
+int ref_bench_positions(const orc_params* p, const double* x, const double* y, const double* z, const int* status,
+                        int n, double mass, double vol, double T0, const orc_tool_samples* tool, double dt,
+                        int warmup, int steps, double* ms_out, long long* n_live) {
+    int rc = check_reference_constants(p);
+    if (rc) return rc;
+    const int ntool = (p->tool_mode == ORC_TOOL_RASTER && tool) ? tool->n : 0;
+    RefRun r;
+    if ((rc = setup(r, p, n, ntool))) return rc;
+    double *dx_ = nullptr, *dy_ = nullptr, *dz_ = nullptr;
+    int* ds = nullptr;
+    HCHECK(cudaMalloc(&dx_, 8 * (size_t)n));
+    HCHECK(cudaMalloc(&dy_, 8 * (size_t)n));
+    HCHECK(cudaMalloc(&dz_, 8 * (size_t)n));
+    HCHECK(cudaMalloc(&ds, 4 * (size_t)n));
+    HCHECK(cudaMemcpy(dx_, x, 8 * (size_t)n, cudaMemcpyHostToDevice));
+    HCHECK(cudaMemcpy(dy_, y, 8 * (size_t)n, cudaMemcpyHostToDevice));
+    HCHECK(cudaMemcpy(dz_, z, 8 * (size_t)n, cudaMemcpyHostToDevice));
+    HCHECK(cudaMemcpy(ds, status, 4 * (size_t)n, cudaMemcpyHostToDevice));
+    fill_particles<<<(n + 255) / 256, 256>>>(r.d_p, dx_, dy_, dz_, ds, n, mass, vol, T0);
+    HCHECK(cudaGetLastError());
+    HCHECK(cudaDeviceSynchronize());
+    cudaFree(dx_); cudaFree(dy_); cudaFree(dz_); cudaFree(ds);
+    if ((rc = bench_loaded(r, p, tool, dt, warmup, steps, ms_out))) return rc;
+    int* dcnt = nullptr;
+    int active = 0, chip = 0;
+    HCHECK(cudaMalloc(&dcnt, 2 * sizeof(int)));
+    HCHECK(cudaMemset(dcnt, 0, 2 * sizeof(int)));
+    countParticleStatusKernel<<<(n + 255) / 256, 256>>>(r.d_p, n, dcnt, dcnt + 1);
+    HCHECK(cudaMemcpy(&active, dcnt, sizeof(int), cudaMemcpyDeviceToHost));
+    HCHECK(cudaMemcpy(&chip, dcnt + 1, sizeof(int), cudaMemcpyDeviceToHost));
+    cudaFree(dcnt);
+    *n_live = (long long)active + chip;
+    return 0;
+}
+
+static int bench_loaded(RefRun& r, const orc_params* p, const orc_tool_samples* tool, double dt, int warmup,
+                        int steps, double* ms_out) {
+    const int ntool = r.ntool;
     const int total = warmup + steps;
     std::vector<FEMNodeGPU> nodes;
     if (ntool > 0) {
@@ -299,7 +365,13 @@ int ref_bench(const orc_params* p, orc_state* s, const orc_tool_samples* tool, d
     }
     MPMKernelConfig cfg = make_config(p);
     const double inf = std::numeric_limits<double>::infinity();
-    static double hBmin[3], hBmax[3];
+    // the bounds sentinels that each step copies host->device (the reference
+    // copies them from its stack, src/MPMSolver.cu:1073-1075, :1134-1135);
+    // pinned here so that the captured copy is valid for the whole run
+    double* hB = nullptr;
+    HCHECK(cudaMallocHost(&hB, 6 * sizeof(double)));
+    double* hBmin = hB;
+    double* hBmax = hB + 3;
     for (int d = 0; d < 3; ++d) { hBmin[d] = inf; hBmax[d] = -inf; }
     double tip0[3] = {p->tool_p0[0], p->tool_p0[1], p->tool_p0[2] + p->tool_tip_dz};
 
@@ -318,7 +390,7 @@ int ref_bench(const orc_params* p, orc_state* s, const orc_tool_samples* tool, d
     cudaEvent_t e0, e1;
     HCHECK(cudaEventCreate(&e0));
     HCHECK(cudaEventCreate(&e1));
-    const int T = 256, pb = (s->n + T - 1) / T;
+    const int T = 256, pb = (r.n + T - 1) / T;
     for (int k = 0; k < total; ++k) {
         if (k == warmup) HCHECK(cudaEventRecord(e0, r.st));
         if (ntool > 0)
@@ -338,11 +410,7 @@ int ref_bench(const orc_params* p, orc_state* s, const orc_tool_samples* tool, d
     cudaGraphExecDestroy(exec);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    {
-        std::vector<MPMParticle> h(s->n);
-        HCHECK(cudaMemcpy(h.data(), r.d_p, sizeof(MPMParticle) * (size_t)s->n, cudaMemcpyDeviceToHost));
-        aos_to_soa(h, s);
-    }
+    cudaFreeHost(hB);
     return 0;
 }
 
