@@ -90,12 +90,16 @@ template <> __device__ __forceinline__ void vec_atomic_add<double>(D4* dst, doub
 // applyGridCollisionKernel (:444-492) in raster mode, or the analytic SDF.
 // Nodes at or below the mass threshold have zero velocity and contribute
 // nothing to the gather, as g2pKernel skips them (:543).
+template <typename R> struct NV {
+    R x, y, z;
+};
+
 template <typename R>
-__device__ __forceinline__ void node_vel(const Inst<R>& P, const V4<R>& g, int gx, int gy, int gz, double pr0,
-                                         double pr2, R out[3]) {
+__device__ __forceinline__ NV<R> node_vel_inl(const Inst<R>& P, const V4<R> g, int gx, int gy, int gz, double pr0,
+                                              double pr2) {
     const R m = g.x;
-    out[0] = out[1] = out[2] = R(0);
-    if (!(m > (R)P.mthr)) return;
+    NV<R> out{R(0), R(0), R(0)};
+    if (!(m > (R)P.mthr)) return out;
     R vx = g.y / m, vy = g.z / m, vz = (g.w + m * (R)(P.grav * P.dt)) / m;
     if (P.fix_thick > 0.0) {
         const double zr = ds(node_coord(gz, P.dx, P.oz), P.oz) / P.fix_thick;
@@ -131,7 +135,14 @@ __device__ __forceinline__ void node_vel(const Inst<R>& P, const V4<R>& g, int g
             }
         }
     }
-    out[0] = vx; out[1] = vy; out[2] = vz;
+    out.x = vx; out.y = vy; out.z = vz;
+    return out;
+}
+
+// Out-of-line copy for the slow-path gather (keeps its 27 node updates small).
+template <typename R>
+__device__ __noinline__ NV<R> node_vel(const Inst<R>& P, const V4<R> g, int gx, int gy, int gz, double pr0, double pr2) {
+    return node_vel_inl<R>(P, g, gx, gy, gz, pr0, pr2);
 }
 
 // ------------------------------------------------------------------ gather (G2P)
@@ -190,47 +201,53 @@ __device__ __forceinline__ void gather_tile(const R (*vel)[kPlane], int base, co
 }
 
 // Same sums for a particle whose stencil left its bin's tile: nodes are read
-// and updated straight from the grid (rare; the re-bin brings it back).
+// and updated straight from the grid (rare; the re-bin brings it back).  Out
+// of line, with its inputs and result by value, so that the hot path keeps
+// its arrays in registers.
+template <typename R> struct GatherOut {
+    R v[3], M[3][3], L[3][3];
+};
+
 template <typename R>
-__device__ __forceinline__ void gather_global(const Inst<R>& P, const V4<R>* __restrict__ grid, const int gb[3],
-                                           const R (&w)[3][3], const R (&dw)[3][3], double pr0, double pr2, R v[3],
-                                           R M[3][3], R L[3][3]) {
-#pragma unroll
+__device__ __noinline__ GatherOut<R> gather_global(const Inst<R>& P, const V4<R>* __restrict__ grid, int g0x, int g0y,
+                                                   int g0z, R x0, R x1, R x2, double pr0, double pr2) {
+    GatherOut<R> o;
+    R w[3][3], dw[3][3];
+    int gb[3];
+    gb[0] = g0x + bspline(x0, w[0], dw[0]);
+    gb[1] = g0y + bspline(x1, w[1], dw[1]);
+    gb[2] = g0z + bspline(x2, w[2], dw[2]);
     for (int c = 0; c < 3; ++c) {
-        v[c] = R(0);
-#pragma unroll
-        for (int b = 0; b < 3; ++b) { M[c][b] = R(0); L[c][b] = R(0); }
+        o.v[c] = R(0);
+        for (int b = 0; b < 3; ++b) { o.M[c][b] = R(0); o.L[c][b] = R(0); }
     }
-#pragma unroll
     for (int i = 0; i < 3; ++i) {
         const int gx = gb[0] + i;
         if (gx < 0 || gx >= P.nx) continue;
-#pragma unroll
         for (int j = 0; j < 3; ++j) {
             const int gy = gb[1] + j;
             if (gy < 0 || gy >= P.ny) continue;
-#pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const int gz = gb[2] + k;
                 if (gz < 0 || gz >= P.nz) continue;
-                R nv[3];
-                node_vel(P, grid[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], gx, gy, gz, pr0, pr2, nv);
+                const NV<R> nv = node_vel(P, grid[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], gx, gy, gz, pr0, pr2);
+                const R vv[3] = {nv.x, nv.y, nv.z};
                 const R ww = w[0][i] * w[1][j] * w[2][k];
                 const R g0 = dw[0][i] * w[1][j] * w[2][k], g1 = w[0][i] * dw[1][j] * w[2][k],
                         g2 = w[0][i] * w[1][j] * dw[2][k];
-#pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    v[c] += ww * nv[c];
-                    M[c][0] += ww * nv[c] * R(i);
-                    M[c][1] += ww * nv[c] * R(j);
-                    M[c][2] += ww * nv[c] * R(k);
-                    L[c][0] += nv[c] * g0;
-                    L[c][1] += nv[c] * g1;
-                    L[c][2] += nv[c] * g2;
+                    o.v[c] += ww * vv[c];
+                    o.M[c][0] += ww * vv[c] * R(i);
+                    o.M[c][1] += ww * vv[c] * R(j);
+                    o.M[c][2] += ww * vv[c] * R(k);
+                    o.L[c][0] += vv[c] * g0;
+                    o.L[c][1] += vv[c] * g1;
+                    o.L[c][2] += vv[c] * g2;
                 }
             }
         }
     }
+    return o;
 }
 
 // ------------------------------------------------------------------ scatter (P2G)
@@ -238,31 +255,34 @@ __device__ __forceinline__ void gather_global(const Inst<R>& P, const V4<R>* __r
 // Momentum + impulse at node (i,j,k):
 //   p_a = w_ijk (Q_a + R_ax i + R_ay j + R_az k) + S_ax dwx wy wz + S_ay wx dwy wz + S_az wx wy dwz
 // with Q = m (v - dx C d), R = m dx C, S = -dt V J sigma / dx.  Separable in k.
+// Scatter of a particle whose stencil left its bin's tile: straight into the
+// grid with vector atomics (rare; out of line, inputs by value).
+template <typename R> struct ScatterIn {
+    R xi[3], Q[3], Rm[9], S[9];
+    int g0[3];
+};
+
 template <typename R>
-__device__ __forceinline__ void scatter_global(const Inst<R>& P, V4<R>* __restrict__ grid, const int gb[3],
-                                            const R (&w)[3][3], const R (&dw)[3][3], R m, const R (&Q)[3],
-                                            const R (&Rm)[3][3], const R (&S)[3][3], bool mass_only) {
-#pragma unroll
+__device__ __noinline__ void scatter_global(const Inst<R>& P, V4<R>* __restrict__ grid, const ScatterIn<R> in, R m) {
+    R w[3][3], dw[3][3];
+    int gb[3];
+    for (int a = 0; a < 3; ++a) gb[a] = in.g0[a] + bspline(in.xi[a], w[a], dw[a]);
     for (int i = 0; i < 3; ++i) {
         const int gx = gb[0] + i;
         if (gx < 0 || gx >= P.nx) continue;
-#pragma unroll
         for (int j = 0; j < 3; ++j) {
             const int gy = gb[1] + j;
             if (gy < 0 || gy >= P.ny) continue;
-#pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const int gz = gb[2] + k;
                 if (gz < 0 || gz >= P.nz) continue;
                 const R ww = w[0][i] * w[1][j] * w[2][k];
                 const R g0 = dw[0][i] * w[1][j] * w[2][k], g1 = w[0][i] * dw[1][j] * w[2][k],
                         g2 = w[0][i] * w[1][j] * dw[2][k];
-                R p[3] = {0, 0, 0};
-                if (!mass_only)
-#pragma unroll
-                    for (int a = 0; a < 3; ++a)
-                        p[a] = ww * (Q[a] + Rm[a][0] * R(i) + Rm[a][1] * R(j) + Rm[a][2] * R(k)) + S[a][0] * g0 +
-                               S[a][1] * g1 + S[a][2] * g2;
+                R p[3];
+                for (int a = 0; a < 3; ++a)
+                    p[a] = ww * (in.Q[a] + in.Rm[a * 3] * R(i) + in.Rm[a * 3 + 1] * R(j) + in.Rm[a * 3 + 2] * R(k)) +
+                           in.S[a * 3] * g0 + in.S[a * 3 + 1] * g1 + in.S[a * 3 + 2] * g2;
                 vec_atomic_add<R>(&grid[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], ww * m, p[0], p[1], p[2]);
             }
         }
@@ -476,8 +496,14 @@ __device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[
 // Particles staged per pass and scatter payload per particle:
 //   [0..2] xi (bin-local, after the move)  [3..5] Q = m (v - dx C d) + f_ext dt
 //   [6..14] R = m dx C (row-major)         [15..23] S = -dt V J sigma / dx (row-major)
+#ifndef MPMB_CHUNK_F32
+#define MPMB_CHUNK_F32 1
+#endif
+#ifndef MPMB_MIN_CTAS
+#define MPMB_MIN_CTAS 4
+#endif
 template <typename R> struct StepCfg {
-    static constexpr int kChunk = sizeof(R) == 4 ? 2 * kNT : kNT;
+    static constexpr int kChunk = sizeof(R) == 4 ? MPMB_CHUNK_F32 * kNT : kNT;
     static constexpr int kPerThread = kChunk / kNT;
 };
 constexpr int kPay = 24;
@@ -498,13 +524,43 @@ template <typename R> struct StepSmem {
 
 template <typename R> constexpr size_t step_smem_bytes() { return sizeof(StepSmem<R>); }
 
-// Accumulation of one cell's staged particles (two channels per thread:
-// h = 0 -> m, p_x; h = 1 -> p_y, p_z) in registers, then added to the cell's
-// private block of cacc.  Each cell block has exactly one writer per
-// channel, so no atomics are needed.  The momentum + impulse of node (i,j,k)
-// relative to the cell's base node is
-//   w_ijk (Q_a + R_ax i + R_ay j + R_az k) + S_ax dwx wy wz + S_ay wx dwy wz + S_az wx wy dwz,
-// evaluated separably (k innermost).
+// Momentum + impulse of one channel a over the 27 stencil nodes (i,j,k) of a
+// particle, relative to its base node:
+//   w_ijk (Q + rx i + ry j + rz k) + sx dwx_i wy_j wz_k + sy wx_i dwy_j wz_k + sz wx_i wy_j dwz_k
+// = wy_j (wx_i Az_k + Bx_i wz_k) + (wx_i Cy_j) wz_k
+// with Az_k = Q wz_k + rz k wz_k + sz dwz_k, Bx_i = rx i wx_i + sx dwx_i,
+// Cy_j = ry j wy_j + sy dwy_j: two FMAs per node.
+template <typename R>
+__device__ __forceinline__ void channel_add(const R (&w)[3][3], const R (&dw)[3][3], R Q, R rx, R ry, R rz, R sx,
+                                            R sy, R sz, R (&acc)[27]) {
+    R Az[3], Bx[3], Cy[3];
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        Az[t] = fma(Q, w[2][t], fma(rz * R(t), w[2][t], sz * dw[2][t]));
+        Bx[t] = fma(rx * R(t), w[0][t], sx * dw[0][t]);
+        Cy[t] = fma(ry * R(t), w[1][t], sy * dw[1][t]);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        R Pk[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) Pk[k] = fma(w[0][i], Az[k], Bx[i] * w[2][k]);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const R Qij = w[0][i] * Cy[j];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int o = i + 3 * j + 9 * k;
+                acc[o] = fma(w[1][j], Pk[k], fma(Qij, w[2][k], acc[o]));
+            }
+        }
+    }
+}
+
+// Accumulation of one cell's staged particles (thread pair per cell: h = 0
+// takes m and p_x, h = 1 takes p_y and p_z) in registers, then added to the
+// cell's private block of cacc.  Each cell block has exactly one writer per
+// channel, so no atomics are needed.
 template <typename R>
 __device__ __forceinline__ void cell_accumulate(StepSmem<R>& Sm, int cell, int h, R pm) {
     R a0[kOff], a1[kOff];
@@ -517,46 +573,23 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R>& Sm, int cell, int h
 #pragma unroll
         for (int a = 0; a < 3; ++a) (void)bspline(Sm.pay[a][e], w[a], dw[a]);
         if (h == 0) {
-            const R Q0 = Sm.pay[3][e], r0 = Sm.pay[6][e], r1 = Sm.pay[7][e], r2 = Sm.pay[8][e];
-            const R t0 = Sm.pay[15][e], t1 = Sm.pay[16][e], t2 = Sm.pay[17][e];
 #pragma unroll
-            for (int i = 0; i < 3; ++i)
+            for (int i = 0; i < 3; ++i) {
+                const R mx = pm * w[0][i];
 #pragma unroll
                 for (int j = 0; j < 3; ++j) {
-                    const R wij = w[0][i] * w[1][j];
-                    const R gx = dw[0][i] * w[1][j], gy = w[0][i] * dw[1][j];
-                    const R mij = wij * pm;
-                    const R U = wij * (Q0 + r0 * R(i) + r1 * R(j)) + t0 * gx + t1 * gy;
-                    const R Up = wij * r2, Zs = wij * t2;
+                    const R mxy = mx * w[1][j];
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        const int o = i + 3 * j + 9 * k;
-                        a0[o] = fma(mij, w[2][k], a0[o]);
-                        a1[o] += fma(w[2][k], fma(R(k), Up, U), dw[2][k] * Zs);
-                    }
+                    for (int k = 0; k < 3; ++k) a0[i + 3 * j + 9 * k] = fma(mxy, w[2][k], a0[i + 3 * j + 9 * k]);
                 }
+            }
+            channel_add<R>(w, dw, Sm.pay[3][e], Sm.pay[6][e], Sm.pay[7][e], Sm.pay[8][e], Sm.pay[15][e],
+                           Sm.pay[16][e], Sm.pay[17][e], a1);
         } else {
-            const R Q1 = Sm.pay[4][e], Q2 = Sm.pay[5][e];
-            const R r10 = Sm.pay[9][e], r11 = Sm.pay[10][e], r12 = Sm.pay[11][e];
-            const R r20 = Sm.pay[12][e], r21 = Sm.pay[13][e], r22 = Sm.pay[14][e];
-            const R t10 = Sm.pay[18][e], t11 = Sm.pay[19][e], t12 = Sm.pay[20][e];
-            const R t20 = Sm.pay[21][e], t21 = Sm.pay[22][e], t22 = Sm.pay[23][e];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const R wij = w[0][i] * w[1][j];
-                    const R gx = dw[0][i] * w[1][j], gy = w[0][i] * dw[1][j];
-                    const R U1 = wij * (Q1 + r10 * R(i) + r11 * R(j)) + t10 * gx + t11 * gy;
-                    const R U2 = wij * (Q2 + r20 * R(i) + r21 * R(j)) + t20 * gx + t21 * gy;
-                    const R Up1 = wij * r12, Zs1 = wij * t12, Up2 = wij * r22, Zs2 = wij * t22;
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        const int o = i + 3 * j + 9 * k;
-                        a0[o] += fma(w[2][k], fma(R(k), Up1, U1), dw[2][k] * Zs1);
-                        a1[o] += fma(w[2][k], fma(R(k), Up2, U2), dw[2][k] * Zs2);
-                    }
-                }
+            channel_add<R>(w, dw, Sm.pay[4][e], Sm.pay[9][e], Sm.pay[10][e], Sm.pay[11][e], Sm.pay[18][e],
+                           Sm.pay[19][e], Sm.pay[20][e], a0);
+            channel_add<R>(w, dw, Sm.pay[5][e], Sm.pay[12][e], Sm.pay[13][e], Sm.pay[14][e], Sm.pay[21][e],
+                           Sm.pay[22][e], Sm.pay[23][e], a1);
         }
     }
     if (n > 0) {
@@ -569,7 +602,7 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R>& Sm, int cell, int h
 }
 
 template <typename R, bool G2P, bool P2G>
-__global__ void __launch_bounds__(kNT) k_step(const Inst<R>* __restrict__ insts, const Work* __restrict__ work,
+__global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __restrict__ insts, const Work* __restrict__ work,
                                               const int* __restrict__ n_work, PState<R> ps, StepArgs sa, int rbuf,
                                               int* __restrict__ err, unsigned long long* __restrict__ ctr) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -626,10 +659,9 @@ __global__ void __launch_bounds__(kNT) k_step(const Inst<R>* __restrict__ insts,
             }
             for (int nidx = tid; nidx < kTileNodes; nidx += kNT) {
                 const int lx = nidx % kTile, ly = (nidx / kTile) % kTile, lz = nidx / (kTile * kTile);
-                R nv[3];
-                node_vel(P, Sm.raw[nidx], g0x + lx, g0y + ly, g0z + lz, prg0, prg2, nv);
+                const NV<R> nv = node_vel_inl(P, Sm.raw[nidx], g0x + lx, g0y + ly, g0z + lz, prg0, prg2);
                 const int t = tidx(lx, ly, lz);
-                Sm.vel[0][t] = nv[0]; Sm.vel[1][t] = nv[1]; Sm.vel[2][t] = nv[2];
+                Sm.vel[0][t] = nv.x; Sm.vel[1][t] = nv.y; Sm.vel[2][t] = nv.z;
             }
         }
         if (P2G) {
@@ -677,8 +709,14 @@ __global__ void __launch_bounds__(kNT) k_step(const Inst<R>* __restrict__ insts,
                             if (b[0] >= 0 && b[0] < kBin && b[1] >= 0 && b[1] < kBin && b[2] >= 0 && b[2] < kBin) {
                                 gather_tile<R>(Sm.vel, tidx(b[0], b[1], b[2]), w, dw, v, M, L);
                             } else {
-                                const int gb[3] = {g0x + b[0], g0y + b[1], g0z + b[2]};
-                                gather_global<R>(P, gr, gb, w, dw, prg0, prg2, v, M, L);
+                                const GatherOut<R> go = gather_global<R>(P, gr, g0x, g0y, g0z, xi[0], xi[1], xi[2],
+                                                                         prg0, prg2);
+#pragma unroll
+                                for (int c = 0; c < 3; ++c) {
+                                    v[c] = go.v[c];
+#pragma unroll
+                                    for (int q = 0; q < 3; ++q) { M[c][q] = go.M[c][q]; L[c][q] = go.L[c][q]; }
+                                }
                                 ++c_esc;
                             }
                             const R d[3] = {xi[0] - R(b[0]), xi[1] - R(b[1]), xi[2] - R(b[2])};
@@ -871,15 +909,13 @@ __global__ void __launch_bounds__(kNT) k_step(const Inst<R>* __restrict__ insts,
 #pragma unroll
                                 for (int q = 0; q < 9; ++q) { Sm.pay[6 + q][slot] = Rm[q]; Sm.pay[15 + q][slot] = S[q]; }
                             } else {
-                                R w[3][3], dw[3][3];
-                                int b2[3];
+                                ScatterIn<R> si;
 #pragma unroll
-                                for (int a = 0; a < 3; ++a) b2[a] = bspline(xi[a], w[a], dw[a]);
-                                const R Qa[3] = {Q[0], Q[1], Q[2]};
-                                const R Rma[3][3] = {{Rm[0], Rm[1], Rm[2]}, {Rm[3], Rm[4], Rm[5]}, {Rm[6], Rm[7], Rm[8]}};
-                                const R Sa[3][3] = {{S[0], S[1], S[2]}, {S[3], S[4], S[5]}, {S[6], S[7], S[8]}};
-                                const int gb[3] = {g0x + b2[0], g0y + b2[1], g0z + b2[2]};
-                                scatter_global<R>(P, gw, gb, w, dw, m, Qa, Rma, Sa, fixed);
+                                for (int a = 0; a < 3; ++a) { si.xi[a] = xi[a]; si.Q[a] = Q[a]; }
+#pragma unroll
+                                for (int q = 0; q < 9; ++q) { si.Rm[q] = Rm[q]; si.S[q] = S[q]; }
+                                si.g0[0] = g0x; si.g0[1] = g0y; si.g0[2] = g0z;
+                                scatter_global<R>(P, gw, si, m);
                                 ++c_esc;
                             }
                         }

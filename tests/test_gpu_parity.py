@@ -179,6 +179,10 @@ def test_fp32_matches_reference_kernels():
 def _sdf_case(mode, shape="cylinder", **kw):
     if shape == "cylinder":
         case = W.config1(cells=(12, 8, 8), speed=20.0, tool_mode=mode, **kw)
+        # the cylinder's centre sits at the box's +x face: drive it into the
+        # material (-x) so that the slip branch (approaching normal velocity)
+        # is taken on the contact nodes
+        case["tool"]["velocity"] = (-20.0, 0.0, 0.0)
     else:
         case = W.config2(cells=(24, 8, 12), speed=20.0, tool_mode=mode, radius=6e-5, doc=4e-5, **kw)
     st = W.full_state(W.generate_box(case), case)
