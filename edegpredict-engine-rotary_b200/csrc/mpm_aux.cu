@@ -519,20 +519,6 @@ __global__ void k_export(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64
     if (o.id) o.id[i] = ps.id[pi];
 }
 
-// MPMParticle, include/Types.h:199-266 (504 bytes): the byte layout that the
-// reference's ContactSolver, CFD coupling and exporters read.
-struct AosParticle {
-    double x, y, z, vx, vy, vz, fx, fy, fz, ext_fx, ext_fy, ext_fz;
-    double density, pressure, volume, mass, temperature;
-    double F[9], F_p[9], C[9];
-    double stress_xx, stress_yy, stress_zz, stress_xy, stress_xz, stress_yz;
-    double backstress_xx, backstress_yy, backstress_zz, backstress_xy, backstress_xz, backstress_yz;
-    double plasticStrain, strainRate, damage, residualStress;
-    int32_t id, status, cellHash, lodZone, lastUpdateStep;
-    uint8_t asbCounter;
-};
-static_assert(sizeof(AosParticle) == 504, "MPMParticle layout is 504 bytes");
-
 template <typename R>
 __global__ void k_export_aos(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64_t n, double Tamb, double rho,
                              AosParticle* out) {

@@ -34,6 +34,10 @@ mpm_status ret(mpm_handle* h, mpm_status s) {
 
 }  // namespace
 
+namespace mpmb {
+void set_lib_error(const std::string& m) { lib_err() = m; }
+}  // namespace mpmb
+
 extern "C" {
 
 mpm_status mpm_params_default(mpm_params* p) {

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "mpm_device.cuh"
 
 namespace mpmb {
@@ -21,6 +23,20 @@ struct DevSoAOut {
     void *x, *y, *z, *vx, *vy, *vz, *F, *Fp, *C, *stress, *bs, *eps, *edot, *T, *D, *sres;
     int32_t *status, *id;
 };
+
+// MPMParticle, include/Types.h:199-266 (504 bytes): the byte layout that the
+// reference's ContactSolver, CFD coupling and exporters read.
+struct AosParticle {
+    double x, y, z, vx, vy, vz, fx, fy, fz, ext_fx, ext_fy, ext_fz;
+    double density, pressure, volume, mass, temperature;
+    double F[9], F_p[9], C[9];
+    double stress_xx, stress_yy, stress_zz, stress_xy, stress_xz, stress_yz;
+    double backstress_xx, backstress_yy, backstress_zz, backstress_xy, backstress_xz, backstress_yz;
+    double plasticStrain, strainRate, damage, residualStress;
+    int32_t id, status, cellHash, lodZone, lastUpdateStep;
+    uint8_t asbCounter;
+};
+static_assert(sizeof(AosParticle) == 504, "MPMParticle layout is 504 bytes");
 
 // Number of stats accumulators (see k_stats).
 constexpr int kStatSlots = 32;
@@ -86,5 +102,8 @@ void fill_i32(int32_t* p, int32_t v, int64_t n, cudaStream_t st);
 
 // Kernel launches issued by this process (all handles).
 int64_t& launch_counter();
+
+// The calling thread's error string, returned by mpm_last_error(NULL).
+void set_lib_error(const std::string& m);
 
 }  // namespace mpmb

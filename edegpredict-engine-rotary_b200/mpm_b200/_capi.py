@@ -101,6 +101,7 @@ def lib() -> C.CDLL:
             "mpm_step": (_i32, [_vp, _d, _i32]),
             "mpm_stable_dt": (_i32, [_vp, _d, P(_d)]),
             "mpm_sync_metrics": (_i32, [_vp, P(MpmMetrics)]),
+            "mpm_metrics_aos_noalloc": (_i32, [P(MpmParams), _vp, _i64, _vp, P(MpmMetrics)]),
             "mpm_set_mass_scaling": (_i32, [_vp, _d]),
             "mpm_apply_external_force": (_i32, [_vp, P(_d), _d, P(_d)]),
             "mpm_set_temperatures": (_i32, [_vp, P(_d), _i64]),

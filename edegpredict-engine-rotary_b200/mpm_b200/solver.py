@@ -186,3 +186,13 @@ class Solver:
 
     def reset_clock(self) -> None:
         self._check(self._lib.mpm_reset_clock(self.h))
+
+
+def metrics_aos_noalloc(params: A.MpmParams, d_particles: int, n: int, stream: int = 0) -> dict:
+    """mpm_metrics_aos_noalloc: metrics of n MPMParticle records (504 bytes
+    each) at device address d_particles, without a handle or any allocation.
+    Calls on one device must not overlap."""
+    m = A.MpmMetrics()
+    A.check(A.lib().mpm_metrics_aos_noalloc(C.byref(params), C.c_void_p(d_particles or None), int(n),
+                                            C.c_void_p(stream or None), C.byref(m)))
+    return m.as_dict()

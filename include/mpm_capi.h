@@ -188,6 +188,25 @@ mpm_status mpm_stable_dt(const mpm_handle *h, double cfl, double *dt);
  * also reports a device-side error (MPM_NUMERIC / MPM_TIMEOUT). */
 mpm_status mpm_sync_metrics(mpm_handle *h, mpm_metrics *out);
 
+/* No counterpart in the reference (which copies every particle to the host to
+ * compute these, src/MPMSolver.cu:1239-1259).  The metrics of mpm_sync_metrics
+ * for n particles held in DEVICE memory in the reference's MPMParticle layout
+ * (include/Types.h:199-266, 504 bytes each: the reference's own d_particles,
+ * or mpm_export_aos written to device memory), with no handle and no
+ * allocation, for callers that cannot allocate device memory.  Mass, volume,
+ * density and temperature are read per record; p supplies E, nu, cp and Tamb.
+ * n_escaped, n_sorts and n_yielded are 0.
+ *   - Scratch is a 1 MiB static device array inside the library; n above
+ *     67,108,864 is refused with MPM_CAPACITY.  Nothing has to be zeroed first.
+ *   - The first call on a device sets the scratch up there (and loads the
+ *     library's kernels on it): make it before any stream capture.
+ *   - Calls on one device must not overlap (two host threads, or two streams
+ *     in flight at once): they share the scratch and race.
+ *   - stream: a cudaStream_t or NULL (legacy default stream).  Synchronises
+ *     that stream before returning. */
+mpm_status mpm_metrics_aos_noalloc(const mpm_params *p, const void *d_particles, int64_t n, void *stream,
+                                   mpm_metrics *out);
+
 /* Replaces setDynamicMassScaling (src/MPMSolver.cu:1211-1225): particle mass
  * becomes rho_phys*factor*volume (never below rho_phys*volume). */
 mpm_status mpm_set_mass_scaling(mpm_handle *h, double factor);
