@@ -765,6 +765,47 @@ void launch_set_temps(const PState<R>& ps, int64_t pbase, int64_t n, const doubl
     ++launch_counter();
 }
 
+// ------------------------------------------------------------------ relayout
+
+template <typename R>
+__global__ void k_relayout(PState<R> src, PState<R> dst, const RelayoutMap* __restrict__ map, int n_inst,
+                           int64_t total) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= total) return;
+    int lo = 0, hi = n_inst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (map[mid].new_pbase <= s) lo = mid; else hi = mid - 1;
+    }
+    const RelayoutMap m = map[lo];
+    const int64_t r = s - m.new_pbase;
+    if (r < 0 || r >= m.np) return;
+    const int64_t o = m.old_pbase + r;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) dst.A[q][s] = src.A[q][o];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) dst.B[q][s] = src.B[q][o];
+    dst.S[0][s] = src.S[0][o];
+    dst.S[1][s] = src.S[1][o];
+    if (src.K[0] && dst.K[0]) {
+        dst.K[0][s] = src.K[0][o];
+        dst.K[1][s] = src.K[1][o];
+    }
+    dst.sres[s] = src.sres[o];
+    dst.status[s] = src.status[o];
+    dst.id[s] = src.id[o];
+    dst.orig[s] = src.orig[o];
+    dst.bin[s] = src.bin[o];
+}
+
+template <typename R>
+void launch_relayout(const PState<R>& src, const PState<R>& dst, const RelayoutMap* map, int n_inst, int64_t total,
+                     cudaStream_t st) {
+    if (total <= 0 || n_inst <= 0) return;
+    k_relayout<R><<<(int)((total + kT - 1) / kT), kT, 0, st>>>(src, dst, map, n_inst, total);
+    ++launch_counter();
+}
+
 #define MPMB_INST(R)                                                                                                  \
     template void launch_bin_count<R>(const Inst<R>*, int, const PState<R>&, const int32_t*, bool, const double*,   \
                                       int32_t*, int32_t*, int32_t*, int32_t*, int64_t, cudaStream_t);               \
@@ -781,7 +822,8 @@ void launch_set_temps(const PState<R>& ps, int64_t pbase, int64_t n, const doubl
                                        cudaStream_t);                                                                \
     template void launch_stats<R>(const Inst<R>*, const PState<R>&, int64_t, int64_t, double, double, double, double, \
                                   double, double*, int, double*, cudaStream_t);                                      \
-    template void launch_set_temps<R>(const PState<R>&, int64_t, int64_t, const double*, int64_t, double, cudaStream_t);
+    template void launch_set_temps<R>(const PState<R>&, int64_t, int64_t, const double*, int64_t, double, cudaStream_t); \
+    template void launch_relayout<R>(const PState<R>&, const PState<R>&, const RelayoutMap*, int, int64_t, cudaStream_t);
 
 MPMB_INST(float)
 MPMB_INST(double)

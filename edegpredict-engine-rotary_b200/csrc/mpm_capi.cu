@@ -5,6 +5,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/mpm_capi.h"
 #include "mpm_engine.h"
@@ -129,7 +130,9 @@ mpm_status mpm_set_tool(mpm_handle* h, const mpm_tool_desc* tool) {
 
 mpm_status mpm_step(mpm_handle* h, double dt, int32_t nsteps) {
     NEED_H(h);
-    return ret(h, h->eng->step(nsteps, &dt));
+    if (h->eng->n_inst() == 1) return ret(h, h->eng->step(nsteps, &dt));
+    std::vector<double> dts((size_t)h->eng->n_inst(), dt);
+    return ret(h, h->eng->step(nsteps, dts.data()));
 }
 
 mpm_status mpm_stable_dt(const mpm_handle* h, double cfl, double* dt) {
@@ -179,6 +182,107 @@ mpm_status mpm_get_stream(const mpm_handle* h, void** stream) {
 mpm_status mpm_reset_clock(mpm_handle* h) {
     NEED_H(h);
     return ret(h, h->eng->reset_clock(0));
+}
+
+// ---------------------------------------------------------------- batched form
+
+#define NEED_I(h, i)                                                                                  \
+    do {                                                                                              \
+        NEED_H(h);                                                                                    \
+        if ((i) < 0 || (i) >= (h)->eng->n_inst()) return fail(h, MPM_INVALID_ARG, "instance index out of range"); \
+    } while (0)
+
+mpm_status mpm_batch_create(const mpm_params* params, const int64_t* capacities, int32_t n_instances, void* stream,
+                            mpm_handle** out) {
+    if (!out) return fail(nullptr, MPM_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    if (!params || !capacities || n_instances <= 0)
+        return fail(nullptr, MPM_INVALID_ARG, "a batch needs at least one instance");
+    mpm_status s = MPM_OK;
+    std::string e;
+    auto eng = mpmb::make_engine(params, capacities, n_instances, (cudaStream_t)stream, &s, &e);
+    if (!eng) return fail(nullptr, s, e);
+    *out = new mpm_handle{std::move(eng)};
+    return MPM_OK;
+}
+
+mpm_status mpm_batch_count(const mpm_handle* h, int32_t* n_instances) {
+    if (!h || !h->eng || !n_instances) return fail(nullptr, MPM_INVALID_ARG, "handle or output is NULL");
+    *n_instances = h->eng->n_inst();
+    return MPM_OK;
+}
+
+mpm_status mpm_batch_init_box(mpm_handle* h, int32_t inst, const int32_t c0[3], const int32_t c1[3], int32_t ppc,
+                              uint64_t seed, uint32_t instance_key, int32_t fixed_layers, double T0,
+                              const mpm_tool_desc* tool_at_t0) {
+    NEED_I(h, inst);
+    if (!c0 || !c1) return fail(h, MPM_INVALID_ARG, "cell box is NULL");
+    return ret(h, h->eng->init_box(inst, c0, c1, ppc, seed, instance_key, fixed_layers, T0, tool_at_t0));
+}
+
+mpm_status mpm_batch_upload(mpm_handle* h, int32_t inst, const mpm_particles_soa* host, int64_t n) {
+    NEED_I(h, inst);
+    return ret(h, h->eng->upload(inst, host, n));
+}
+
+mpm_status mpm_batch_download(mpm_handle* h, int32_t inst, mpm_particles_soa* host) {
+    NEED_I(h, inst);
+    return ret(h, h->eng->download(inst, host));
+}
+
+mpm_status mpm_batch_set_tool(mpm_handle* h, int32_t inst, const mpm_tool_desc* tool) {
+    NEED_I(h, inst);
+    return ret(h, h->eng->set_tool(inst, tool));
+}
+
+mpm_status mpm_batch_step(mpm_handle* h, const double* dt, int32_t nsteps) {
+    NEED_H(h);
+    if (!dt) return fail(h, MPM_INVALID_ARG, "dt is NULL");
+    return ret(h, h->eng->step(nsteps, dt));
+}
+
+mpm_status mpm_batch_sync_metrics(mpm_handle* h, int32_t inst, mpm_metrics* out) {
+    NEED_I(h, inst);
+    return ret(h, h->eng->metrics(inst, out));
+}
+
+mpm_status mpm_batch_get_counts(const mpm_handle* h, int32_t inst, int64_t* n_particles, int64_t* n_steps,
+                                double* time) {
+    if (!h || !h->eng) return fail(nullptr, MPM_INVALID_ARG, "handle is NULL");
+    if (inst < 0 || inst >= h->eng->n_inst()) return fail(nullptr, MPM_INVALID_ARG, "instance index out of range");
+    const auto& x = h->eng->inst(inst);
+    if (n_particles) *n_particles = x.np;
+    if (n_steps) *n_steps = x.step;
+    if (time) *time = x.time;
+    return MPM_OK;
+}
+
+mpm_status mpm_batch_change(mpm_handle* h, const mpm_params* add, const int64_t* add_capacities, int32_t n_add,
+                            const int32_t* remove, int32_t n_remove, int32_t* first_added) {
+    NEED_H(h);
+    if (n_add < 0 || n_remove < 0) return fail(h, MPM_INVALID_ARG, "negative count");
+    if (n_add > 0 && (!add || !add_capacities)) return fail(h, MPM_INVALID_ARG, "new instances need parameters");
+    if (n_remove > 0 && !remove) return fail(h, MPM_INVALID_ARG, "remove list is NULL");
+    int first = 0;
+    mpm_status s = h->eng->change_instances(add, add_capacities, n_add, remove, n_remove, &first);
+    if (s == MPM_OK && first_added) *first_added = first;
+    return ret(h, s);
+}
+
+mpm_status mpm_get_launch_config(const mpm_handle* h, mpm_launch_config* out) {
+    if (!h || !h->eng || !out) return fail(nullptr, MPM_INVALID_ARG, "handle or output is NULL");
+    return h->eng->get_config(out);
+}
+
+mpm_status mpm_set_launch_config(mpm_handle* h, const mpm_launch_config* cfg) {
+    NEED_H(h);
+    return ret(h, h->eng->set_config(cfg));
+}
+
+mpm_status mpm_autotune(mpm_handle* h, const double* dt, mpm_launch_config* chosen) {
+    NEED_H(h);
+    if (!dt) return fail(h, MPM_INVALID_ARG, "dt is NULL");
+    return ret(h, h->eng->autotune(dt, chosen));
 }
 
 mpm_status mpm_profile_enable(mpm_handle* h, int32_t enable) {

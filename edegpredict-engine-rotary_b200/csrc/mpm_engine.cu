@@ -46,6 +46,12 @@ inline size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
         }                                                                                            \
     } while (0)
 
+#define MS(call)                     \
+    do {                             \
+        mpm_status s_ = (call);      \
+        if (s_ != MPM_OK) return s_; \
+    } while (0)
+
 }  // namespace
 
 mpm_status check_params(const mpm_params* p, std::string* err) {
@@ -76,6 +82,11 @@ class Engine final : public EngineBase {
     cudaStream_t st = nullptr;
     bool own_st = false;
     int64_t cap_total = 0, nn_total = 0, nkeys = 0;
+    // allocated sizes (grow-only)
+    int64_t pcap_alloc = -1, pcap_alloc_next = 0, nn_alloc = 0, scan_alloc = 0, map_alloc = 0;
+    int64_t slot_alloc[4] = {0, 0, 0, 0}, key_alloc[2] = {0, 0}, bin_alloc[6] = {0, 0, 0, 0, 0, 0};
+    int64_t inst_alloc[3] = {0, 0, 0};
+    RelayoutMap* d_map = nullptr;
     void* pbuf[2] = {nullptr, nullptr};
     PState<R> ps[2];
     int cur = 0;
@@ -103,7 +114,8 @@ class Engine final : public EngineBase {
     bool binned = false;
     int64_t since_sort = 0, n_sorts = 0;
     int64_t launch_base = 0;
-    int sort_every = 16, threads = 128;
+    int sort_every = 16, threads = 128, ctas_per_sm = 4;
+    bool use_graph = false;
     int rbuf = 0;
     // step-kernel timing (mpm_profile_enable)
     bool prof = false;
@@ -146,10 +158,11 @@ class Engine final : public EngineBase {
 
     ~Engine() override {
         if (st) cudaStreamSynchronize(st);
+        drop_graphs();
         void* ptrs[] = {pbuf[0], pbuf[1], gpool[0], gpool[1], mask_pool, d_inst, d_key_base, d_bin_key, d_bin_inst,
                         d_bin_local,
                         d_inst_pbase, d_key, d_rank, d_newbin, d_count, d_offset, d_flag, d_flag_scan, d_scan_tmp,
-                        d_pos, d_work, d_nwork, d_err, d_ctr, d_stat_part, d_stat_out, d_stage, d_gen};
+                        d_pos, d_work, d_nwork, d_err, d_ctr, d_stat_part, d_stat_out, d_stage, d_gen, d_map};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         for (auto& x : I)
@@ -167,24 +180,9 @@ class Engine final : public EngineBase {
 
     mpm_status init(const mpm_params* params, const int64_t* caps, int n, cudaStream_t stream_in) {
         launch_base = launch_counter();
-        I.resize(n);
-        for (int i = 0; i < n; ++i) {
-            mpm_status s = check_params(&params[i], &err);
-            if (s != MPM_OK) return s;
-            if (params[i].precision != params[0].precision) {
-                err = "all instances of an engine share one precision";
-                return MPM_INVALID_ARG;
-            }
-            if (caps[i] < 0 || caps[i] > ((int64_t)1 << 31) - 1) {
-                err = "capacity out of range";
-                return MPM_INVALID_ARG;
-            }
-            I[i].p = params[i];
-            I[i].cap = caps[i];
-            I[i].tool = mpm_tool_desc{};
-            I[i].tool.mode = MPM_TOOL_NONE;
-            if (params[i].H_kin > 0.0) has_K = true;
-        }
+        std::vector<InstHost> nI;
+        mpm_status s = make_insts(params, caps, n, &nI);
+        if (s != MPM_OK) return s;
         sort_every = params[0].sort_every > 0 ? params[0].sort_every : 16;
         threads = params[0].threads_per_block > 0 ? params[0].threads_per_block : 128;
         if (stream_in) {
@@ -193,8 +191,114 @@ class Engine final : public EngineBase {
             CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
             own_st = true;
         }
-        // layout of instances
+        CK(cudaMalloc(&d_nwork, sizeof(int)));
+        CK(cudaMemsetAsync(d_nwork, 0, sizeof(int), st));
+        CK(cudaMalloc(&d_err, sizeof(int)));
+        CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+        CK(cudaMalloc(&d_ctr, 4 * sizeof(unsigned long long)));
+        CK(cudaMemsetAsync(d_ctr, 0, 4 * sizeof(unsigned long long), st));
+        stat_blocks = 592;
+        CK(cudaMalloc(&d_stat_part, sizeof(double) * kStatSlots * stat_blocks));
+        CK(cudaMalloc(&d_stat_out, sizeof(double) * kStatSlots));
+        return relayout(std::move(nI), std::vector<int>(n, -1));
+    }
+
+    // Host records of new instances (validated, default tool, clock at 0).
+    mpm_status make_insts(const mpm_params* params, const int64_t* caps, int n, std::vector<InstHost>* out) {
+        out->assign(n, InstHost{});
+        for (int i = 0; i < n; ++i) {
+            mpm_status s = check_params(&params[i], &err);
+            if (s != MPM_OK) return s;
+            const int prec = I.empty() ? params[0].precision : I[0].p.precision;
+            if (params[i].precision != prec) {
+                err = "all instances of an engine share one precision";
+                return MPM_INVALID_ARG;
+            }
+            if (caps[i] < 0 || caps[i] > ((int64_t)1 << 31) - 1) {
+                err = "capacity out of range";
+                return MPM_INVALID_ARG;
+            }
+            InstHost& x = (*out)[i];
+            x.p = params[i];
+            x.cap = caps[i];
+            x.tool = mpm_tool_desc{};
+            x.tool.mode = MPM_TOOL_NONE;
+        }
+        return MPM_OK;
+    }
+
+    // Grow-only device buffer: reallocates (contents dropped) when `need`
+    // elements do not fit, with a quarter of headroom.
+    template <typename T>
+    mpm_status grow(T*& p, int64_t& have, int64_t need) {
+        need = std::max<int64_t>(need, 1);
+        if (p && need <= have) return MPM_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        const int64_t n = need + need / 4;
+        CK(cudaMalloc(&p, sizeof(T) * n));
+        have = n;
+        return MPM_OK;
+    }
+
+    static size_t pstate_bytes(int64_t cp, bool withK) {
+        const size_t v4 = sizeof(V4<R>);
+        return 12 * al256(v4 * cp) + (withK ? 2 * al256(v4 * cp) : 0) + al256(sizeof(R) * cp) + al256(cp) +
+               3 * al256(4 * cp);
+    }
+    static void carve(void* base, int64_t cp, bool withK, PState<R>& s) {
+        char* q = (char*)base;
+        const size_t v4 = sizeof(V4<R>);
+        auto take = [&](size_t bytes) {
+            void* r = q;
+            q += al256(bytes);
+            return r;
+        };
+        for (int k = 0; k < 6; ++k) s.A[k] = (V4<R>*)take(v4 * cp);
+        for (int k = 0; k < 4; ++k) s.B[k] = (V4<R>*)take(v4 * cp);
+        for (int k = 0; k < 2; ++k) s.S[k] = (V4<R>*)take(v4 * cp);
+        for (int k = 0; k < 2; ++k) s.K[k] = withK ? (V4<R>*)take(v4 * cp) : nullptr;
+        s.sres = (R*)take(sizeof(R) * cp);
+        s.status = (uint8_t*)take(cp);
+        s.id = (int32_t*)take(4 * cp);
+        s.bin = (int32_t*)take(4 * cp);
+        s.orig = (int32_t*)take(4 * cp);
+    }
+
+    // Replaces the instance set by nI; from[j] is the old index of new
+    // instance j (-1: new, empty).  Instances are laid out contiguously in
+    // the new order: particle slots [pbase, pbase + cap), grid nodes, sort keys
+    // (bin*64 + cell per bin, then the INACTIVE sentinel and the unused-slot
+    // pad) and bins.  The particles of kept instances move to their new slots
+    // in one copy into the other state buffer; grids are not carried (every
+    // step call starts from a cleared grid).  Allocations only grow.  The next
+    // step re-bins.
+    mpm_status relayout(std::vector<InstHost> nI, const std::vector<int>& from) {
+        CK(cudaStreamSynchronize(st));
+        drop_graphs();
+        const int n = (int)nI.size();
+        std::vector<RelayoutMap> map(n);
+        std::vector<char> kept(I.size(), 0);
+        bool any_kept = false;
+        for (int j = 0; j < n; ++j) {
+            map[j].old_pbase = 0;
+            map[j].np = 0;
+            if (from[j] >= 0) {
+                kept[from[j]] = 1;
+                map[j].old_pbase = I[from[j]].pbase;
+                map[j].np = I[from[j]].np;
+                any_kept |= I[from[j]].np > 0;
+            }
+        }
+        for (size_t i = 0; i < I.size(); ++i)
+            if (!kept[i] && I[i].d_samples) {
+                cudaFree(I[i].d_samples);
+                I[i].d_samples = nullptr;
+            }
+        I = std::move(nI);
+        // layout
         int64_t pb = 0, go = 0, kb = 0;
+        bool wantK = false;
         std::vector<int32_t> key_base(n), bin_key, bin_inst, bin_local;
         std::vector<int64_t> inst_pbase(n);
         for (int i = 0; i < n; ++i) {
@@ -214,10 +318,10 @@ class Engine final : public EngineBase {
                 bin_inst.push_back(i);
                 bin_local.push_back((int32_t)b);
             }
-            // keys: bin*64 + cell for every bin, then the INACTIVE sentinel and the unused-slot pad
             kb += nbins * kCellsPerBin + 2;
             inst_pbase[i] = x.pbase;
-            max_work += (int)nbins;
+            map[i].new_pbase = x.pbase;
+            wantK |= x.p.H_kin > 0.0;
         }
         if (kb > ((int64_t)1 << 31) - 1 || pb > ((int64_t)1 << 31) - 1) {
             err = "too many bins or particles for one engine";
@@ -226,79 +330,145 @@ class Engine final : public EngineBase {
         cap_total = pb;
         nn_total = go;
         nkeys = kb;
-        // particle buffers
+        max_work = (int)bin_key.size();
         const int64_t cp = std::max<int64_t>(cap_total, 1);
-        const size_t v4 = sizeof(V4<R>);
-        size_t need = 0;
-        need += 6 * al256(v4 * cp) + 4 * al256(v4 * cp) + 2 * al256(v4 * cp) + (has_K ? 2 * al256(v4 * cp) : 0);
-        need += al256(sizeof(R) * cp) + al256(cp) + 3 * al256(4 * cp);
-        for (int b = 0; b < 2; ++b) {
-            CK(cudaMalloc(&pbuf[b], need));
-            char* q = (char*)pbuf[b];
-            auto take = [&](size_t bytes) {
-                void* r = q;
-                q += al256(bytes);
-                return r;
-            };
-            PState<R>& s = ps[b];
-            for (int k = 0; k < 6; ++k) s.A[k] = (V4<R>*)take(v4 * cp);
-            for (int k = 0; k < 4; ++k) s.B[k] = (V4<R>*)take(v4 * cp);
-            for (int k = 0; k < 2; ++k) s.S[k] = (V4<R>*)take(v4 * cp);
-            for (int k = 0; k < 2; ++k) s.K[k] = has_K ? (V4<R>*)take(v4 * cp) : nullptr;
-            s.sres = (R*)take(sizeof(R) * cp);
-            s.status = (uint8_t*)take(cp);
-            s.id = (int32_t*)take(4 * cp);
-            s.bin = (int32_t*)take(4 * cp);
-            s.orig = (int32_t*)take(4 * cp);
+        // particle state: copy kept instances into the other buffer (or into
+        // new, larger buffers)
+        const bool had = pcap_alloc >= 0;
+        const bool newbufs = !had || cap_total > pcap_alloc || (wantK && !has_K);
+        PState<R> dst[2];
+        void* nbuf[2] = {nullptr, nullptr};
+        const bool withK = wantK || has_K;
+        if (newbufs) {
+            const int64_t cnew = had ? std::max<int64_t>(cp, pcap_alloc + pcap_alloc / 4) : cp;
+            const size_t bytes = pstate_bytes(cnew, withK);
+            for (int b = 0; b < 2; ++b) {
+                cudaError_t e = cudaMalloc(&nbuf[b], bytes);
+                if (e != cudaSuccess) {
+                    if (nbuf[0]) cudaFree(nbuf[0]);
+                    cudaGetLastError();
+                    err = std::string("particle state: ") + cudaGetErrorString(e);
+                    return e == cudaErrorMemoryAllocation ? MPM_OOM : MPM_CUDA_ERROR;
+                }
+                carve(nbuf[b], cnew, withK, dst[b]);
+                if (withK) {
+                    CK(cudaMemsetAsync(dst[b].K[0], 0, sizeof(V4<R>) * cnew, st));
+                    CK(cudaMemsetAsync(dst[b].K[1], 0, sizeof(V4<R>) * cnew, st));
+                }
+            }
+            pcap_alloc_next = cnew;
         }
-        // grids, tool masks
-        for (int b = 0; b < 2; ++b) {
-            CK(cudaMalloc(&gpool[b], sizeof(V4<R>) * std::max<int64_t>(nn_total, 1)));
-            CK(cudaMemsetAsync(gpool[b], 0, sizeof(V4<R>) * nn_total, st));
+        if (had && any_kept) {
+            MS(grow(d_map, map_alloc, n));
+            CK(cudaMemcpyAsync(d_map, map.data(), sizeof(RelayoutMap) * n, cudaMemcpyHostToDevice, st));
+            launch_relayout<R>(ps[cur], newbufs ? dst[0] : ps[cur ^ 1], d_map, n, cap_total, st);
         }
-        CK(cudaMalloc(&mask_pool, std::max<int64_t>(nn_total, 1)));
-        CK(cudaMemsetAsync(mask_pool, 0, nn_total, st));
-        // sort scratch
-        CK(cudaMalloc(&d_key, 4 * cp));
-        CK(cudaMalloc(&d_rank, 4 * cp));
-        CK(cudaMalloc(&d_newbin, 4 * cp));
-        CK(cudaMalloc(&d_pos, 3 * sizeof(double) * cp));
-        CK(cudaMalloc(&d_count, 4 * (nkeys + 1)));
-        CK(cudaMalloc(&d_offset, 4 * (nkeys + 1)));
+        if (newbufs) {
+            CK(cudaStreamSynchronize(st));
+            for (int b = 0; b < 2; ++b) {
+                if (pbuf[b]) cudaFree(pbuf[b]);
+                pbuf[b] = nbuf[b];
+                ps[b] = dst[b];
+            }
+            pcap_alloc = pcap_alloc_next;
+            has_K = withK;
+            cur = 0;
+        } else if (had && any_kept) {
+            cur ^= 1;
+        }
+        // grids and tool masks (not carried across a relayout)
+        if (nn_total > nn_alloc) {
+            CK(cudaStreamSynchronize(st));
+            for (int b = 0; b < 2; ++b) {
+                if (gpool[b]) cudaFree(gpool[b]);
+                gpool[b] = nullptr;
+            }
+            if (mask_pool) cudaFree(mask_pool);
+            mask_pool = nullptr;
+            const int64_t nn = std::max<int64_t>(nn_total + nn_total / 4, 1);
+            for (int b = 0; b < 2; ++b) CK(cudaMalloc(&gpool[b], sizeof(V4<R>) * nn));
+            CK(cudaMalloc(&mask_pool, nn));
+            nn_alloc = nn;
+        }
+        CK(cudaMemsetAsync(gpool[0], 0, sizeof(V4<R>) * std::max<int64_t>(nn_total, 1), st));
+        CK(cudaMemsetAsync(gpool[1], 0, sizeof(V4<R>) * std::max<int64_t>(nn_total, 1), st));
+        CK(cudaMemsetAsync(mask_pool, 0, std::max<int64_t>(nn_total, 1), st));
+        rbuf = 0;
+        // sort scratch, key and bin tables
+        MS(grow(d_key, slot_alloc[0], cp));
+        MS(grow(d_rank, slot_alloc[1], cp));
+        MS(grow(d_newbin, slot_alloc[2], cp));
+        MS(grow(d_pos, slot_alloc[3], 3 * cp));
+        MS(grow(d_count, key_alloc[0], nkeys + 1));
+        MS(grow(d_offset, key_alloc[1], nkeys + 1));
         const int64_t nb_tot = std::max<int64_t>(max_work, 1);
-        CK(cudaMalloc(&d_flag, 4 * (nb_tot + 1)));
-        CK(cudaMalloc(&d_flag_scan, 4 * (nb_tot + 1)));
-        CK(cudaMalloc(&d_scan_tmp, 4 * std::max<int64_t>(scan_tmp_size(nkeys + 1), scan_tmp_size(cp))));
-        CK(cudaMalloc(&d_key_base, 4 * n));
-        CK(cudaMalloc(&d_bin_key, 4 * nb_tot));
-        CK(cudaMalloc(&d_bin_inst, 4 * nb_tot));
-        CK(cudaMalloc(&d_bin_local, 4 * nb_tot));
-        CK(cudaMalloc(&d_inst_pbase, 8 * n));
-        CK(cudaMemcpyAsync(d_key_base, key_base.data(), 4 * n, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_bin_key, bin_key.data(), 4 * bin_key.size(), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_bin_inst, bin_inst.data(), 4 * bin_inst.size(), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_bin_local, bin_local.data(), 4 * bin_local.size(), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_inst_pbase, inst_pbase.data(), 8 * n, cudaMemcpyHostToDevice, st));
-        CK(cudaMalloc(&d_work, sizeof(Work) * std::max(max_work, 1)));
-        CK(cudaMalloc(&d_nwork, sizeof(int)));
+        MS(grow(d_flag, bin_alloc[0], nb_tot + 1));
+        MS(grow(d_flag_scan, bin_alloc[1], nb_tot + 1));
+        MS(grow(d_bin_key, bin_alloc[2], nb_tot));
+        MS(grow(d_bin_inst, bin_alloc[3], nb_tot));
+        MS(grow(d_bin_local, bin_alloc[4], nb_tot));
+        MS(grow(d_work, bin_alloc[5], nb_tot));
+        MS(grow(d_scan_tmp, scan_alloc, std::max<int64_t>(scan_tmp_size(nkeys + 1), scan_tmp_size(cp))));
+        MS(grow(d_key_base, inst_alloc[0], n));
+        MS(grow(d_inst_pbase, inst_alloc[1], n));
+        MS(grow(d_inst, inst_alloc[2], n));
+        if (n > 0) {
+            CK(cudaMemcpyAsync(d_key_base, key_base.data(), 4 * n, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(d_inst_pbase, inst_pbase.data(), 8 * n, cudaMemcpyHostToDevice, st));
+        }
+        if (!bin_key.empty()) {
+            CK(cudaMemcpyAsync(d_bin_key, bin_key.data(), 4 * bin_key.size(), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(d_bin_inst, bin_inst.data(), 4 * bin_inst.size(), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(d_bin_local, bin_local.data(), 4 * bin_local.size(), cudaMemcpyHostToDevice, st));
+        }
         CK(cudaMemsetAsync(d_nwork, 0, sizeof(int), st));
-        CK(cudaMalloc(&d_err, sizeof(int)));
-        CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
-        CK(cudaMalloc(&d_ctr, 4 * sizeof(unsigned long long)));
-        CK(cudaMemsetAsync(d_ctr, 0, 4 * sizeof(unsigned long long), st));
-        stat_blocks = 592;
-        CK(cudaMalloc(&d_stat_part, sizeof(double) * kStatSlots * stat_blocks));
-        CK(cudaMalloc(&d_stat_out, sizeof(double) * kStatSlots));
         // instance table with TMA descriptors
-        h_inst.resize(n);
-        CK(cudaMalloc(&d_inst, sizeof(Inst<R>) * n));
+        h_inst.assign(n, Inst<R>{});
         for (int i = 0; i < n; ++i) {
             mpm_status s = build_inst(i);
             if (s != MPM_OK) return s;
         }
-        CK(cudaMemcpyAsync(d_inst, h_inst.data(), sizeof(Inst<R>) * n, cudaMemcpyHostToDevice, st));
+        if (n > 0) CK(cudaMemcpyAsync(d_inst, h_inst.data(), sizeof(Inst<R>) * n, cudaMemcpyHostToDevice, st));
         CK(cudaStreamSynchronize(st));
+        binned = false;
+        since_sort = 0;
         return MPM_OK;
+    }
+
+    // Adds instances at the end and drops the listed ones (state of the
+    // others is kept).  New instances start empty; fill them with init_box or
+    // upload.  Returns the index of the first added instance in *first.
+    mpm_status change_instances(const mpm_params* params, const int64_t* caps, int n_add, const int32_t* remove,
+                                int n_remove, int* first) override {
+        // uploaded-but-unbinned positions sit in per-slot scratch that the
+        // relayout does not move: bin them first
+        if (!I.empty()) MS(ensure_binned());
+        std::vector<InstHost> add;
+        if (n_add > 0) {
+            mpm_status s = make_insts(params, caps, n_add, &add);
+            if (s != MPM_OK) return s;
+        }
+        std::vector<char> drop(I.size(), 0);
+        for (int k = 0; k < n_remove; ++k) {
+            if (remove[k] < 0 || remove[k] >= (int)I.size()) {
+                err = "instance index out of range";
+                return MPM_INVALID_ARG;
+            }
+            drop[remove[k]] = 1;
+        }
+        std::vector<InstHost> nI;
+        std::vector<int> from;
+        for (int i = 0; i < (int)I.size(); ++i)
+            if (!drop[i]) {
+                nI.push_back(I[i]);
+                from.push_back(i);
+            }
+        if (first) *first = (int)nI.size();
+        for (auto& x : add) {
+            nI.push_back(x);
+            from.push_back(-1);
+        }
+        return relayout(std::move(nI), from);
     }
 
     mpm_status build_inst(int i) {
@@ -369,17 +539,15 @@ class Engine final : public EngineBase {
         const mpm_tool_desc& t = x.tool;
         d.tool_mode = t.mode; d.tool_shape = t.shape;
         for (int a = 0; a < 3; ++a) { d.tool_p0[a] = t.position[a]; d.tool_v[a] = t.velocity[a]; }
-        d.tool_t0 = tool_t0_[i];
+        d.tool_t0 = x.tool_t0;
         d.tool_r = t.radius; d.tool_rake = t.rake; d.tool_clear = t.clearance; d.tool_tip_dz = t.tip_dz;
         d.tool_sg = std::sin(t.rake); d.tool_cg = std::cos(t.rake);
         d.tool_sa = std::sin(t.clearance); d.tool_ca = std::cos(t.clearance);
         for (int a = 0; a < 3; ++a) { d.ext_c[a] = x.ext_c[a]; d.ext_f[a] = x.ext_f[a]; }
         d.ext_r = x.ext_pending ? x.ext_r : 0.0;
         d.pbase = x.pbase; d.np = x.np; d.pcap = x.cap;
-        d.fresh = fresh_[i];
+        d.fresh = x.fresh;
     }
-    std::vector<double> tool_t0_;
-    std::vector<int> fresh_;
 
     mpm_status push_insts() {
         for (int i = 0; i < (int)I.size(); ++i) fill_mutable(i);
@@ -404,14 +572,14 @@ class Engine final : public EngineBase {
         ++n_sorts;
         binned = true;
         bool any_fresh = false;
-        for (auto& f : fresh_) { any_fresh |= (f != 0); f = 0; }
+        for (auto& x : I) { any_fresh |= (x.fresh != 0); x.fresh = 0; }
         if (any_fresh) return push_insts();
         return MPM_OK;
     }
 
     mpm_status ensure_binned() {
         bool any_fresh = false;
-        for (auto f : fresh_) any_fresh |= (f != 0);
+        for (const auto& x : I) any_fresh |= (x.fresh != 0);
         if (!binned || any_fresh) return rebin();
         return MPM_OK;
     }
@@ -462,11 +630,9 @@ class Engine final : public EngineBase {
         CK(cudaStreamSynchronize(st));
         cudaFree(tmp);
         x.np = (int64_t)lasti + lastf;
-        fresh_[i] = 1;
+        x.fresh = 1;
         CK(cudaGetLastError());
-        mpm_status s = push_insts();
-        if (s != MPM_OK) return s;
-        return rebin();
+        return push_insts();  // binned by the next call that needs it
     }
 
     static size_t fbytes(const void* p, int elem, int64_t n, int per) { return p ? al256((size_t)elem * n * per) : 0; }
@@ -525,11 +691,9 @@ class Engine final : public EngineBase {
         launch_import<R>(d, n, x.p.origin[0], x.p.origin[1], x.p.origin[2], x.p.dx, x.p.Tamb, ps[cur], x.pbase, d_pos,
                          st);
         x.np = n;
-        fresh_[i] = 1;
+        x.fresh = 1;
         CK(cudaGetLastError());
-        mpm_status s = push_insts();
-        if (s != MPM_OK) return s;
-        return rebin();
+        return push_insts();  // binned by the next call that needs it
     }
 
     // ---------------------------------------------------------------- particles out
@@ -623,7 +787,7 @@ class Engine final : public EngineBase {
         }
         x.tool = *t;
         x.tool.sample_dx = x.tool.sample_dy = x.tool.sample_dz = nullptr;
-        tool_t0_[i] = x.time;
+        x.tool_t0 = x.time;
         if (t->mode == MPM_TOOL_RASTER) {
             const int ns = std::max(t->n_samples, 0);
             if (x.d_samples) {
@@ -648,11 +812,10 @@ class Engine final : public EngineBase {
     void raster_all(int k) {
         for (auto& x : I) {
             if (x.tool.mode != MPM_TOOL_RASTER || x.n_samples <= 0) continue;
-            const int ii = (int)(&x - &I[0]);
             const double t = x.time + (double)k * x.dt;
-            const double px = x.tool.position[0] + x.tool.velocity[0] * (t - tool_t0_[ii]);
-            const double py = x.tool.position[1] + x.tool.velocity[1] * (t - tool_t0_[ii]);
-            const double pz = x.tool.position[2] + x.tool.velocity[2] * (t - tool_t0_[ii]);
+            const double px = x.tool.position[0] + x.tool.velocity[0] * (t - x.tool_t0);
+            const double py = x.tool.position[1] + x.tool.velocity[1] * (t - x.tool_t0);
+            const double pz = x.tool.position[2] + x.tool.velocity[2] * (t - x.tool_t0);
             cudaMemsetAsync(mask_pool + x.grid_off, 0, x.nn, st);
             launch_raster(x.d_samples, x.d_samples + x.n_samples, x.d_samples + 2 * x.n_samples, x.n_samples, px, py,
                           pz, x.p.origin[0], x.p.origin[1], x.p.origin[2], x.p.dx, x.p.nx, x.p.ny, x.p.nz,
@@ -677,54 +840,16 @@ class Engine final : public EngineBase {
         if (s != MPM_OK) return s;
         s = push_insts();
         if (s != MPM_OK) return s;
-        const size_t gbytes = sizeof(V4<R>) * nn_total;
-        const bool fused = I[0].p.schedule == MPM_SCHED_FUSED;
-        int w = rbuf;
-        bool ext = false;
-        for (auto& x : I) ext |= x.ext_pending;
-        auto maybe_sort = [&]() -> mpm_status {
-            if (since_sort >= sort_every) return rebin_regular();
-            return MPM_OK;
-        };
-        if (fused) {
-            CK(cudaMemsetAsync(gpool[w], 0, gbytes, st));
-            StepArgs a{0, 0, N == 1 ? 1 : 0, ext ? 1 : 0, 0};
-            launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], a, w, false, true, threads, 0, d_err, d_ctr, st);
-            for (int k = 0; k + 1 < N; ++k) {
-                if ((s = maybe_sort()) != MPM_OK) return s;
-                CK(cudaMemsetAsync(gpool[w ^ 1], 0, gbytes, st));
-                raster_all(k);
-                StepArgs b{k, 0, (k + 2 == N) ? 1 : 0, 0, k + 1};
-                prof_begin();
-                launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], b, w, true, true, threads, 0, d_err, d_ctr,
-                               st);
-                prof_end();
-                w ^= 1;
-                ++since_sort;
-            }
-            raster_all(N - 1);
-            StepArgs c{N - 1, 1, 0, 0, N - 1};
-            launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], c, w, true, false, threads, 0, d_err, d_ctr, st);
-            ++since_sort;
-        } else {
-            for (int k = 0; k < N; ++k) {
-                if ((s = maybe_sort()) != MPM_OK) return s;
-                CK(cudaMemsetAsync(gpool[w], 0, gbytes, st));
-                StepArgs a{k, 0, 1, (ext && k == 0) ? 1 : 0, k};
-                prof_begin();
-                launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], a, w, false, true, threads, 0, d_err, d_ctr,
-                               st);
-                prof_end();
-                raster_all(k);
-                StepArgs c{k, 1, 0, 0, k};
-                prof_begin();
-                launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], c, w, true, false, threads, 0, d_err, d_ctr,
-                               st);
-                prof_end();
-                ++since_sort;
-            }
+        bool ext = false, raster = false;
+        for (auto& x : I) {
+            ext |= x.ext_pending;
+            raster |= (x.tool.mode == MPM_TOOL_RASTER && x.n_samples > 0);
         }
-        rbuf = w;
+        if (use_graph && !raster && !prof && max_work > 0)
+            s = step_graph(N, ext);
+        else
+            s = issue_steps(N, ext);
+        if (s != MPM_OK) return s;
         for (auto& x : I) {
             x.time += (double)N * x.dt;
             x.step += N;
@@ -732,6 +857,213 @@ class Engine final : public EngineBase {
         }
         CK(cudaGetLastError());
         return MPM_OK;
+    }
+
+    // The launches of one step call.  Fused schedule: N+1 launches (P2G of
+    // step 0, then G2P k + P2G k+1, then G2P of step N-1); split: 2N.  Only
+    // device work and host counters (re-bin cadence, buffer parity), so the
+    // sequence can be captured in a graph.
+    mpm_status issue_steps(int32_t N, bool ext) {
+        mpm_status s = MPM_OK;
+        const size_t gbytes = sizeof(V4<R>) * nn_total;
+        const bool fused = I[0].p.schedule == MPM_SCHED_FUSED;
+        int w = rbuf;
+        auto maybe_sort = [&]() -> mpm_status {
+            if (since_sort >= sort_every) return rebin_regular();
+            return MPM_OK;
+        };
+        const int cps = ctas_per_sm;
+        if (fused) {
+            CK(cudaMemsetAsync(gpool[w], 0, gbytes, st));
+            StepArgs a{0, 0, N == 1 ? 1 : 0, ext ? 1 : 0, 0};
+            launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], a, w, false, true, threads, cps, d_err, d_ctr,
+                           st);
+            for (int k = 0; k + 1 < N; ++k) {
+                if ((s = maybe_sort()) != MPM_OK) return s;
+                CK(cudaMemsetAsync(gpool[w ^ 1], 0, gbytes, st));
+                raster_all(k);
+                StepArgs b{k, 0, (k + 2 == N) ? 1 : 0, 0, k + 1};
+                prof_begin();
+                launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], b, w, true, true, threads, cps, d_err,
+                               d_ctr, st);
+                prof_end();
+                w ^= 1;
+                ++since_sort;
+            }
+            raster_all(N - 1);
+            StepArgs c{N - 1, 1, 0, 0, N - 1};
+            launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], c, w, true, false, threads, cps, d_err, d_ctr,
+                           st);
+            ++since_sort;
+        } else {
+            for (int k = 0; k < N; ++k) {
+                if ((s = maybe_sort()) != MPM_OK) return s;
+                CK(cudaMemsetAsync(gpool[w], 0, gbytes, st));
+                StepArgs a{k, 0, 1, (ext && k == 0) ? 1 : 0, k};
+                prof_begin();
+                launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], a, w, false, true, threads, cps, d_err,
+                               d_ctr, st);
+                prof_end();
+                raster_all(k);
+                StepArgs c{k, 1, 0, 0, k};
+                prof_begin();
+                launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], c, w, true, false, threads, cps, d_err,
+                               d_ctr, st);
+                prof_end();
+                ++since_sort;
+            }
+        }
+        rbuf = w;
+        return MPM_OK;
+    }
+
+    // ---------------------------------------------------------------- graphs
+
+    // A captured step call, valid for one layout and launch configuration; the
+    // host counters it leaves behind are replayed with it.
+    struct GraphEntry {
+        int32_t N;
+        int64_t since_sort0;
+        int cur0, rbuf0, ext;
+        cudaGraphExec_t exec;
+        int64_t since_sort1, sorts, launches;
+        int cur1, rbuf1;
+        uint64_t use;
+    };
+    std::vector<GraphEntry> graphs;
+    uint64_t graph_clock = 0;
+    static constexpr size_t kMaxGraphs = 32;
+
+    void drop_graphs() {
+        for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+    }
+
+    mpm_status step_graph(int32_t N, bool ext) {
+        for (auto& g : graphs) {
+            if (g.N == N && g.since_sort0 == since_sort && g.cur0 == cur && g.rbuf0 == rbuf && g.ext == (int)ext) {
+                CK(cudaGraphLaunch(g.exec, st));
+                since_sort = g.since_sort1;
+                n_sorts += g.sorts;
+                cur = g.cur1;
+                rbuf = g.rbuf1;
+                launch_counter() += g.launches;
+                g.use = ++graph_clock;
+                return MPM_OK;
+            }
+        }
+        GraphEntry e{};
+        e.N = N;
+        e.since_sort0 = since_sort;
+        e.cur0 = cur;
+        e.rbuf0 = rbuf;
+        e.ext = (int)ext;
+        const int64_t sorts0 = n_sorts, l0 = launch_counter();
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        mpm_status s = issue_steps(N, ext);
+        cudaError_t ce = cudaStreamEndCapture(st, &g);
+        if (s != MPM_OK) {
+            if (g) cudaGraphDestroy(g);
+            return s;
+        }
+        if (ce != cudaSuccess) {
+            err = std::string("step graph capture: ") + cudaGetErrorString(ce);
+            return MPM_CUDA_ERROR;
+        }
+        ce = cudaGraphInstantiate(&e.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) {
+            err = std::string("step graph instantiate: ") + cudaGetErrorString(ce);
+            return MPM_CUDA_ERROR;
+        }
+        CK(cudaGraphLaunch(e.exec, st));
+        e.since_sort1 = since_sort;
+        e.sorts = n_sorts - sorts0;
+        e.launches = launch_counter() - l0;
+        e.cur1 = cur;
+        e.rbuf1 = rbuf;
+        e.use = ++graph_clock;
+        if (graphs.size() >= kMaxGraphs) {
+            size_t old = 0;
+            for (size_t k = 1; k < graphs.size(); ++k)
+                if (graphs[k].use < graphs[old].use) old = k;
+            cudaGraphExecDestroy(graphs[old].exec);
+            graphs.erase(graphs.begin() + old);
+        }
+        graphs.push_back(e);
+        return MPM_OK;
+    }
+
+    // ---------------------------------------------------------------- launch configuration
+
+    mpm_status get_config(mpm_launch_config* c) override {
+        c->ctas_per_sm = ctas_per_sm;
+        c->sort_every = sort_every;
+        c->use_graph = use_graph ? 1 : 0;
+        c->_pad = 0;
+        return MPM_OK;
+    }
+
+    mpm_status set_config(const mpm_launch_config* c) override {
+        if (!c || c->ctas_per_sm < 1 || c->ctas_per_sm > 8 || c->sort_every < 1 || c->sort_every > 1024) {
+            err = "launch config: ctas_per_sm in [1, 8], sort_every in [1, 1024]";
+            return MPM_INVALID_ARG;
+        }
+        if (c->ctas_per_sm != ctas_per_sm || c->sort_every != sort_every) drop_graphs();
+        ctas_per_sm = c->ctas_per_sm;
+        sort_every = c->sort_every;
+        use_graph = c->use_graph != 0;
+        if (!use_graph) drop_graphs();
+        return MPM_OK;
+    }
+
+    // Times each candidate (persistent CTAs per SM x re-bin cadence) over one
+    // re-bin period of real steps and keeps the fastest.  The trial steps
+    // advance the simulation like any other steps.
+    mpm_status autotune(const double* dts, mpm_launch_config* best) override {
+        const int cand_ctas[3] = {2, 3, 4};
+        const int cand_sort[3] = {8, 16, 32};
+        mpm_launch_config cur_cfg{};
+        get_config(&cur_cfg);
+        mpm_launch_config win = cur_cfg;
+        double win_ms = 1e300;
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        mpm_status s = MPM_OK;
+        for (int a = 0; a < 3 && s == MPM_OK; ++a)
+            for (int b = 0; b < 3 && s == MPM_OK; ++b) {
+                mpm_launch_config c = cur_cfg;
+                c.ctas_per_sm = cand_ctas[a];
+                c.sort_every = cand_sort[b];
+                if ((s = set_config(&c)) != MPM_OK) break;
+                since_sort = 0;
+                const int n = cand_sort[b];
+                cudaEventRecord(e0, st);
+                if ((s = step(n, dts)) != MPM_OK) break;
+                // the re-bin of this period (the cadence counter is at n)
+                if ((s = rebin_regular()) != MPM_OK) break;
+                cudaEventRecord(e1, st);
+                if (cudaEventSynchronize(e1) != cudaSuccess) {
+                    s = MPM_CUDA_ERROR;
+                    err = "autotune: event sync failed";
+                    break;
+                }
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                const double per = ms / n;
+                if (per < win_ms) {
+                    win_ms = per;
+                    win = c;
+                }
+            }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (s != MPM_OK) return s;
+        s = set_config(&win);
+        if (best) *best = win;
+        return s == MPM_OK ? device_status() : s;
     }
 
     mpm_status rebin_regular() {
@@ -858,7 +1190,7 @@ class Engine final : public EngineBase {
     mpm_status reset_clock(int i) override {
         I[i].time = 0.0;
         I[i].step = 0;
-        tool_t0_[i] = 0.0;
+        I[i].tool_t0 = 0.0;
         return push_insts();
     }
     mpm_status sync() override {
@@ -876,8 +1208,6 @@ std::unique_ptr<EngineBase> make_engine(const mpm_params* params, const int64_t*
     }
     if (params[0].precision == MPM_PREC_F64) {
         auto e = std::make_unique<Engine<double>>();
-        e->tool_t0_.assign(n, 0.0);
-        e->fresh_.assign(n, 0);
         *status = e->init(params, caps, n, st);
         if (*status != MPM_OK) {
             *err = e->err;
@@ -886,8 +1216,6 @@ std::unique_ptr<EngineBase> make_engine(const mpm_params* params, const int64_t*
         return e;
     }
     auto e = std::make_unique<Engine<float>>();
-    e->tool_t0_.assign(n, 0.0);
-    e->fresh_.assign(n, 0);
     *status = e->init(params, caps, n, st);
     if (*status != MPM_OK) {
         *err = e->err;

@@ -30,6 +30,8 @@ struct InstHost {
     int n_samples = 0;
     double ext_c[3] = {0, 0, 0}, ext_r = 0.0, ext_f[3] = {0, 0, 0};
     bool ext_pending = false;
+    double tool_t0 = 0.0;   // time at which the tool descriptor was set
+    int fresh = 0;          // particles uploaded or generated, not yet binned
 };
 
 class EngineBase {
@@ -48,6 +50,13 @@ class EngineBase {
     virtual mpm_status ext_force(int inst, const double c[3], double r, const double f[3]) = 0;
     virtual mpm_status set_temps(int inst, const double* T, int64_t count) = 0;
     virtual mpm_status reset_clock(int inst) = 0;
+    // Appends n_add instances and drops the listed ones; kept instances keep
+    // their state (indices of the instances after a dropped one shift down).
+    virtual mpm_status get_config(mpm_launch_config* c) = 0;
+    virtual mpm_status set_config(const mpm_launch_config* c) = 0;
+    virtual mpm_status autotune(const double* dt_per_inst, mpm_launch_config* best) = 0;
+    virtual mpm_status change_instances(const mpm_params* params, const int64_t* caps, int n_add,
+                                        const int32_t* remove, int n_remove, int* first) = 0;
     virtual mpm_status sync() = 0;
     virtual int n_inst() const = 0;
     virtual const InstHost& inst(int i) const = 0;

@@ -38,6 +38,12 @@ struct AosParticle {
 };
 static_assert(sizeof(AosParticle) == 504, "MPMParticle layout is 504 bytes");
 
+// One instance of a relayout: its first slot in the new layout, its first
+// slot in the old one and the particles to carry over (0 for a new instance).
+struct RelayoutMap {
+    int64_t new_pbase, old_pbase, np;
+};
+
 // Number of stats accumulators (see k_stats).
 constexpr int kStatSlots = 32;
 
@@ -85,6 +91,13 @@ void launch_export_aos(const Inst<R>* inst_dev, const PState<R>& ps, int64_t pba
 template <typename R>
 void launch_stats(const Inst<R>* inst_dev, const PState<R>& ps, int64_t pbase, int64_t n, double mu, double K,
                   double rho, double cp, double Tamb, double* partial, int nblocks, double* out, cudaStream_t st);
+
+// Copies particles [old_pbase, old_pbase + np) of every instance of `map`
+// (sorted by new_pbase) from src to [new_pbase, ...) of dst; total = slots of
+// the new layout.
+template <typename R>
+void launch_relayout(const PState<R>& src, const PState<R>& dst, const RelayoutMap* map, int n_inst, int64_t total,
+                     cudaStream_t st);
 
 template <typename R>
 void launch_set_temps(const PState<R>& ps, int64_t pbase, int64_t n, const double* T, int64_t count, double Tamb,

@@ -78,6 +78,14 @@ PARTICLE_FIELDS = {  # name -> values per particle
     "plastic_strain": 1, "strain_rate": 1, "temperature": 1, "damage": 1, "residual_stress": 1,
 }
 
+class MpmLaunchConfig(C.Structure):
+    _fields_ = [("ctas_per_sm", C.c_int32), ("sort_every", C.c_int32), ("use_graph", C.c_int32),
+                ("_pad", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {"ctas_per_sm": self.ctas_per_sm, "sort_every": self.sort_every, "use_graph": self.use_graph}
+
+
 _lib = None
 
 
@@ -102,6 +110,20 @@ def lib() -> C.CDLL:
             "mpm_stable_dt": (_i32, [_vp, _d, P(_d)]),
             "mpm_sync_metrics": (_i32, [_vp, P(MpmMetrics)]),
             "mpm_metrics_aos_noalloc": (_i32, [P(MpmParams), _vp, _i64, _vp, P(MpmMetrics)]),
+            "mpm_batch_create": (_i32, [P(MpmParams), P(_i64), _i32, _vp, P(_vp)]),
+            "mpm_batch_count": (_i32, [_vp, P(_i32)]),
+            "mpm_batch_init_box": (_i32, [_vp, _i32, P(_i32), P(_i32), _i32, C.c_uint64, C.c_uint32, _i32, _d,
+                                          P(MpmToolDesc)]),
+            "mpm_batch_upload": (_i32, [_vp, _i32, P(MpmParticlesSoa), _i64]),
+            "mpm_batch_download": (_i32, [_vp, _i32, P(MpmParticlesSoa)]),
+            "mpm_batch_set_tool": (_i32, [_vp, _i32, P(MpmToolDesc)]),
+            "mpm_batch_step": (_i32, [_vp, P(_d), _i32]),
+            "mpm_batch_sync_metrics": (_i32, [_vp, _i32, P(MpmMetrics)]),
+            "mpm_batch_get_counts": (_i32, [_vp, _i32, P(_i64), P(_i64), P(_d)]),
+            "mpm_batch_change": (_i32, [_vp, P(MpmParams), P(_i64), _i32, P(_i32), _i32, P(_i32)]),
+            "mpm_get_launch_config": (_i32, [_vp, P(MpmLaunchConfig)]),
+            "mpm_set_launch_config": (_i32, [_vp, P(MpmLaunchConfig)]),
+            "mpm_autotune": (_i32, [_vp, P(_d), P(MpmLaunchConfig)]),
             "mpm_set_mass_scaling": (_i32, [_vp, _d]),
             "mpm_apply_external_force": (_i32, [_vp, P(_d), _d, P(_d)]),
             "mpm_set_temperatures": (_i32, [_vp, P(_d), _i64]),

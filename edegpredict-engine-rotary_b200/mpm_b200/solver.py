@@ -19,6 +19,44 @@ def _ptr(a: Optional[np.ndarray]):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
+def soa_in(parts: Dict[str, np.ndarray], elem: int = 8):
+    """mpm_particles_soa over host copies of `parts` (returned to keep alive)."""
+    dt = np.float64 if elem == 8 else np.float32
+    s = A.MpmParticlesSoa()
+    s.elem = elem
+    keep = []
+    for name in A.PARTICLE_FIELDS:
+        if name in parts and parts[name] is not None:
+            a = np.ascontiguousarray(parts[name], dtype=dt)
+            keep.append(a)
+            setattr(s, name, a.ctypes.data)
+    for name in ("status", "id"):
+        if name in parts and parts[name] is not None:
+            a = np.ascontiguousarray(parts[name], dtype=np.int32)
+            keep.append(a)
+            setattr(s, name, a.ctypes.data)
+    return s, keep, len(parts["x"])
+
+
+def soa_out(n: int, fields=None, elem: int = 8):
+    """mpm_particles_soa over new host arrays for n particles."""
+    dt = np.float64 if elem == 8 else np.float32
+    s = A.MpmParticlesSoa()
+    s.elem = elem
+    out = {}
+    for name, per in A.PARTICLE_FIELDS.items():
+        if fields is None or name in fields:
+            a = np.zeros((n, per) if per > 1 else (n,), dtype=dt)
+            out[name] = a
+            setattr(s, name, a.ctypes.data)
+    for name in ("status", "id"):
+        if fields is None or name in fields:
+            a = np.zeros(n, dtype=np.int32)
+            out[name] = a
+            setattr(s, name, a.ctypes.data)
+    return s, out
+
+
 class Solver:
     def __init__(self, params: A.MpmParams, capacity: int, stream: int = 0):
         self._lib = A.lib()
@@ -85,39 +123,11 @@ class Solver:
         return self.counts()[0]
 
     def upload(self, parts: Dict[str, np.ndarray], elem: int = 8) -> None:
-        dt = np.float64 if elem == 8 else np.float32
-        s = A.MpmParticlesSoa()
-        s.elem = elem
-        keep = []
-        n = len(parts["x"])
-        for name in A.PARTICLE_FIELDS:
-            if name in parts and parts[name] is not None:
-                a = np.ascontiguousarray(parts[name], dtype=dt)
-                keep.append(a)
-                setattr(s, name, a.ctypes.data)
-        for name in ("status", "id"):
-            if name in parts and parts[name] is not None:
-                a = np.ascontiguousarray(parts[name], dtype=np.int32)
-                keep.append(a)
-                setattr(s, name, a.ctypes.data)
+        s, keep, n = soa_in(parts, elem)
         self._check(self._lib.mpm_upload(self.h, C.byref(s), n))
 
     def download(self, fields=None, elem: int = 8) -> Dict[str, np.ndarray]:
-        n = self.counts()[0]
-        dt = np.float64 if elem == 8 else np.float32
-        s = A.MpmParticlesSoa()
-        s.elem = elem
-        out = {}
-        for name, per in A.PARTICLE_FIELDS.items():
-            if fields is None or name in fields:
-                a = np.zeros((n, per) if per > 1 else (n,), dtype=dt)
-                out[name] = a
-                setattr(s, name, a.ctypes.data)
-        for name in ("status", "id"):
-            if fields is None or name in fields:
-                a = np.zeros(n, dtype=np.int32)
-                out[name] = a
-                setattr(s, name, a.ctypes.data)
+        s, out = soa_out(self.counts()[0], fields, elem)
         self._check(self._lib.mpm_download(self.h, C.byref(s)))
         return out
 
@@ -196,3 +206,88 @@ def metrics_aos_noalloc(params: A.MpmParams, d_particles: int, n: int, stream: i
     A.check(A.lib().mpm_metrics_aos_noalloc(C.byref(params), C.c_void_p(d_particles or None), int(n),
                                             C.c_void_p(stream or None), C.byref(m)))
     return m.as_dict()
+
+
+class Batch(Solver):
+    """Many independent workpieces in one handle (mpm_batch_*): every step of
+    all of them is one persistent launch over the bins of all instances.
+    Solver's own methods act on instance 0."""
+
+    def __init__(self, params, capacities, stream: int = 0):
+        self._lib = A.lib()
+        n = len(params)
+        arr = (A.MpmParams * n)(*params)
+        caps = (C.c_int64 * n)(*map(int, capacities))
+        h = C.c_void_p()
+        A.check(self._lib.mpm_batch_create(arr, caps, n, C.c_void_p(stream or None), C.byref(h)))
+        self.h = h
+        self.params = list(params)
+        self._keep = []
+
+    def count(self) -> int:
+        c = C.c_int32()
+        self._check(self._lib.mpm_batch_count(self.h, C.byref(c)))
+        return c.value
+
+    def init_box_i(self, i: int, c0, c1, ppc: int, seed: int, instance_key: int = 0, fixed_layers: int = 2,
+                   T0: float = 293.0, tool: Optional[dict] = None) -> int:
+        a0 = (C.c_int32 * 3)(*map(int, c0))
+        a1 = (C.c_int32 * 3)(*map(int, c1))
+        t = self.tool_desc(tool) if tool else None
+        self._check(self._lib.mpm_batch_init_box(self.h, int(i), a0, a1, int(ppc), C.c_uint64(seed),
+                                                 C.c_uint32(instance_key), int(fixed_layers), float(T0),
+                                                 C.byref(t) if t else None))
+        return self.counts_i(i)[0]
+
+    def set_tool_i(self, i: int, tool: dict) -> None:
+        t = self.tool_desc(tool)
+        self._check(self._lib.mpm_batch_set_tool(self.h, int(i), C.byref(t)))
+
+    def upload_i(self, i: int, parts: Dict[str, np.ndarray], elem: int = 8) -> None:
+        s, keep, n = soa_in(parts, elem)
+        self._check(self._lib.mpm_batch_upload(self.h, int(i), C.byref(s), n))
+
+    def download_i(self, i: int, fields=None, elem: int = 8) -> Dict[str, np.ndarray]:
+        s, out = soa_out(self.counts_i(i)[0], fields, elem)
+        self._check(self._lib.mpm_batch_download(self.h, int(i), C.byref(s)))
+        return out
+
+    def step_all(self, dts, nsteps: int = 1) -> None:
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        self._check(self._lib.mpm_batch_step(self.h, d.ctypes.data_as(C.POINTER(C.c_double)), int(nsteps)))
+
+    def metrics_i(self, i: int) -> dict:
+        m = A.MpmMetrics()
+        self._check(self._lib.mpm_batch_sync_metrics(self.h, int(i), C.byref(m)))
+        return m.as_dict()
+
+    def counts_i(self, i: int):
+        n, k, t = C.c_int64(), C.c_int64(), C.c_double()
+        self._check(self._lib.mpm_batch_get_counts(self.h, int(i), C.byref(n), C.byref(k), C.byref(t)))
+        return n.value, k.value, t.value
+
+    def change(self, add_params=(), add_caps=(), remove=()) -> int:
+        na, nr = len(add_params), len(remove)
+        arr = (A.MpmParams * max(na, 1))(*add_params)
+        caps = (C.c_int64 * max(na, 1))(*map(int, add_caps))
+        rem = (C.c_int32 * max(nr, 1))(*map(int, remove))
+        first = C.c_int32()
+        self._check(self._lib.mpm_batch_change(self.h, arr, caps, na, rem, nr, C.byref(first)))
+        self.params = [p for k, p in enumerate(self.params) if k not in set(remove)] + list(add_params)
+        return first.value
+
+    def launch_config(self) -> dict:
+        c = A.MpmLaunchConfig()
+        self._check(self._lib.mpm_get_launch_config(self.h, C.byref(c)))
+        return c.as_dict()
+
+    def set_launch_config(self, ctas_per_sm: int = 4, sort_every: int = 16, use_graph: bool = False) -> None:
+        c = A.MpmLaunchConfig(int(ctas_per_sm), int(sort_every), 1 if use_graph else 0, 0)
+        self._check(self._lib.mpm_set_launch_config(self.h, C.byref(c)))
+
+    def autotune(self, dts) -> dict:
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        c = A.MpmLaunchConfig()
+        self._check(self._lib.mpm_autotune(self.h, d.ctypes.data_as(C.POINTER(C.c_double)), C.byref(c)))
+        return c.as_dict()
+

@@ -108,6 +108,37 @@ def config4(**kw) -> dict:
     return make_case(**args)
 
 
+def config3_case(rng: np.random.Generator, index: int, *, cells_lo: int = 16, cells_hi: int = 64, steps: int = 300,
+                 dx: float = 2e-5, seed: int = 1234, precision=A.PREC_F32) -> dict:
+    """One instance of the batched sweep: cell count log-uniform in
+    [cells_lo^3, cells_hi^3] with aspect ratios (Wx/Wz, Wy/Wz) uniform in
+    [1, 4], 4-8 ppc, Johnson-Cook A in [300, 1200] MPa, B in [200, 1100] MPa,
+    n in [0.1, 0.9], C in [0.005, 0.03], m in [0.8, 1.4], cutting speed in
+    [0.5, 5] m/s, depth of cut in [0.02, 0.2] mm (capped at half the height),
+    elastic and thermal rows interpolated between AISI 4340 and Ti-6Al-4V;
+    rounded wedge with edge radius 2 x depth of cut at mid-length."""
+    C = math.exp(rng.uniform(math.log(cells_lo ** 3), math.log(cells_hi ** 3)))
+    ax, ay = rng.uniform(1.0, 4.0, 2)
+    wz = max(4, int(round((C / (ax * ay)) ** (1.0 / 3.0))))
+    wx, wy = max(4, int(round(ax * wz))), max(4, int(round(ay * wz)))
+    ppc = int(rng.integers(4, 9))
+    f = rng.uniform()
+    mat = {k: (1.0 - f) * AISI_4340[k] + f * TI_6AL_4V[k] for k in ("E", "nu", "rho_phys", "cp", "Tm")}
+    mat.update(beta=0.9, Tamb=293.0, edot0=1.0, H_kin=0.0, D1=0.05, D2=3.44, D3=-2.12, D4=0.002, D5=0.61, D_th=1.0,
+               jc_A=rng.uniform(300e6, 1200e6), jc_B=rng.uniform(200e6, 1100e6), jc_n=rng.uniform(0.1, 0.9),
+               jc_C=rng.uniform(0.005, 0.03), jc_m=rng.uniform(0.8, 1.4))
+    speed = rng.uniform(0.5, 5.0)
+    doc = min(rng.uniform(2e-5, 2e-4), 0.5 * wz * dx)
+    return make_case((wx, wy, wz), dx, ppc, mat, "wedge", doc=doc, speed=speed, radius=max(2.0 * doc, 2.0 * dx),
+                     steps=steps, seed=seed, instance=index, tool_x_cells=wx / 2.0, precision=precision)
+
+
+def config3(n_instances: int = 512, seed: int = 7, **kw) -> list:
+    """The batched sweep: n_instances independent workpieces (config3_case)."""
+    rng = np.random.default_rng(seed)
+    return [config3_case(rng, i, **kw) for i in range(n_instances)]
+
+
 def to_mpm_params(case: dict, **over) -> A.MpmParams:
     p = A.default_params()
     vals = dict(case["params"])

@@ -224,6 +224,52 @@ mpm_status mpm_get_stream(const mpm_handle *h, void **stream);
 /* Replaces reset() (src/MPMSolver.cu:1227-1230): time and step counter to 0. */
 mpm_status mpm_reset_clock(mpm_handle *h);
 
+/*
+ * Batched form.  No counterpart in the reference, which runs one MPMSolver
+ * per simulation (src/main.cpp:307).  One handle holds many independent
+ * workpieces (instances), each with its own grid, material, tool and time
+ * step; every step of all of them is one persistent launch over the bins of
+ * all instances.  The single-instance functions above act on instance 0 of
+ * a batch handle (mpm_step: the same dt for every instance).
+ */
+mpm_status mpm_batch_create(const mpm_params *params, const int64_t *capacities, int32_t n_instances, void *stream,
+                            mpm_handle **out);
+mpm_status mpm_batch_count(const mpm_handle *h, int32_t *n_instances);
+mpm_status mpm_batch_init_box(mpm_handle *h, int32_t inst, const int32_t c0[3], const int32_t c1[3], int32_t ppc,
+                              uint64_t seed, uint32_t instance_key, int32_t fixed_layers, double T0,
+                              const mpm_tool_desc *tool_at_t0);
+mpm_status mpm_batch_upload(mpm_handle *h, int32_t inst, const mpm_particles_soa *host, int64_t n);
+mpm_status mpm_batch_download(mpm_handle *h, int32_t inst, mpm_particles_soa *host);
+mpm_status mpm_batch_set_tool(mpm_handle *h, int32_t inst, const mpm_tool_desc *tool);
+/* nsteps steps of every instance; dt[i] is instance i's step (n_instances values). */
+mpm_status mpm_batch_step(mpm_handle *h, const double *dt, int32_t nsteps);
+mpm_status mpm_batch_sync_metrics(mpm_handle *h, int32_t inst, mpm_metrics *out);
+mpm_status mpm_batch_get_counts(const mpm_handle *h, int32_t inst, int64_t *n_particles, int64_t *n_steps,
+                                double *time);
+/* Drops the n_remove listed instances (their state is freed; the indices of
+ * the instances after them shift down) and appends n_add new, empty ones
+ * (fill them with mpm_batch_init_box / mpm_batch_upload).  The other
+ * instances keep their state and clock.  *first_added (may be NULL) receives
+ * the index of the first new instance. */
+mpm_status mpm_batch_change(mpm_handle *h, const mpm_params *add, const int64_t *add_capacities, int32_t n_add,
+                            const int32_t *remove, int32_t n_remove, int32_t *first_added);
+
+/* Launch shape of the step kernel.  Not part of the physics: any setting
+ * gives the same results up to FP32 summation order. */
+typedef struct mpm_launch_config {
+    int32_t ctas_per_sm;   /* persistent CTAs per SM of the step kernel, 1..8 (default 4) */
+    int32_t sort_every;    /* re-bin every n steps, 1..1024 (default mpm_params.sort_every) */
+    int32_t use_graph;     /* replay each step call's launches from a captured CUDA graph */
+    int32_t _pad;
+} mpm_launch_config;
+mpm_status mpm_get_launch_config(const mpm_handle *h, mpm_launch_config *out);
+mpm_status mpm_set_launch_config(mpm_handle *h, const mpm_launch_config *cfg);
+/* Times every candidate launch shape (CTAs per SM in {2,3,4} x re-bin every
+ * {8,16,32} steps) over one re-bin period of real steps each (168 steps in
+ * all, dt[i] per instance, counted like any other steps) and keeps the
+ * fastest; *chosen (may be NULL) receives it. */
+mpm_status mpm_autotune(mpm_handle *h, const double *dt, mpm_launch_config *chosen);
+
 /* Record CUDA events around every launch of the step kernel (enable != 0),
  * for timing the dominant kernel inside a longer run.  mpm_profile_read
  * synchronises, returns the summed device time (ms) and count of the fused
