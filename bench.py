@@ -2,7 +2,7 @@
 """Benchmark of the B200 MPM workpiece step (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config large|small|precision]
+                    [--config large|small|precision|batched|serving] [--instances M]
 
 Workload (default `large`): the plain large single-instance step -- 256x128x128
 cells, dx 0.02 mm, 8 particles/cell (~33.5M particles), Ti-6Al-4V, rounded
@@ -15,6 +15,17 @@ The working set (~7 GB of particle state per step) is far larger than the
 N > 1 (torchrun): every rank runs its own replica (the path does not shard a
 single instance; replicas only, no data-path collective); the timing is the
 max over ranks, value = total particle-updates / that time.
+
+--config batched: the config-3 sweep (M = 512 uneven workpieces, 300 steps) in
+one batch handle -- one persistent launch per step for all of them, launch shape
+autotuned, step calls replayed from a CUDA graph -- reported beside the same
+workpieces stepped one at a time through the plain handle (a 32-instance
+sample), as `plain_sequential` and `batched_over_plain`.
+
+--config serving: the serving loop under Poisson arrivals (200 requests/s for
+60 s, 16^3..96^3-cell requests at 8 ppc, 200-2000 steps, 150 GB budget):
+throughput, p50/p99/p99.9 latency of the requests completed in the window,
+offered/admitted/completed counts.
 
 --impl reference: the reference's own CUDA kernels (src/MPMSolver.cu, built from
 its sources into oracle/_ref/) on the same workload -- rank 0 only.
@@ -334,6 +345,222 @@ def run_e2e(s, case, args, n, dev, stream) -> dict:
 
 # ----------------------------------------------------------------- reference arm
 
+# ----------------------------------------------------------------- batched arm
+
+def _cap(case) -> int:
+    b = case["box"]
+    return int(np.prod([b["c1"][i] - b["c0"][i] for i in range(3)]) * b["ppc"])
+
+
+def _init(obj, case, i=None, rank=0):
+    b = case["box"]
+    args = (b["c0"], b["c1"], b["ppc"], b["seed"] + rank, b["instance"], b["fixed_layers"], b["T0"])
+    if i is None:
+        return obj.init_box(*args, tool=case["tool"])
+    return obj.init_box_i(i, *args, tool=case["tool"])
+
+
+def plain_sequential(cases, steps: int, stream) -> dict:
+    """The same workpieces one at a time through the plain single-instance
+    handle (mpm_create / mpm_step), each timed with CUDA events on its stream."""
+    import torch
+    from mpm_b200 import Solver, workpiece as W
+    tot_pu, tot_ms = 0.0, 0.0
+    for c in cases:
+        s = Solver(W.to_mpm_params(c), _cap(c), stream=stream.cuda_stream)
+        n = _init(s, c)
+        s.step(c["dt"], 3)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            s.step(c["dt"], steps)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        tot_ms += e0.elapsed_time(e1)
+        tot_pu += n * steps
+        s.close()
+    return {"value": tot_pu / (tot_ms / 1e3), "unit": UNIT, "instances": len(cases), "steps": steps}
+
+
+def run_batched(args):
+    import torch
+    rank, world, local, dist = dist_setup(args.gpus)
+    from mpm_b200 import Batch, workpiece as W
+    cases = W.config3(args.instances, seed=7 + rank)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    bt = Batch([W.to_mpm_params(c) for c in cases], [_cap(c) for c in cases], stream=stream.cuda_stream)
+    n_live = 0
+    for i, c in enumerate(cases):
+        n_live += _init(bt, c, i, rank)
+    dts = [c["dt"] for c in cases]
+    # autotune (real steps, untimed) then warm-up
+    tune = bt.autotune(dts) if not args.no_tune else bt.launch_config()
+    bt.set_launch_config(tune["ctas_per_sm"], tune["sort_every"], use_graph=True)
+    tune = bt.launch_config()
+    bt.step_all(dts, args.warmup)
+    torch.cuda.synchronize(dev)
+    launches0 = bt.launches()
+    sampler = ClockSampler(physical_gpu_index(local))
+    sampler.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        bt.step_all(dts, args.steps)
+        e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    launches = bt.launches() - launches0
+    # kernel time of the fused launches (separate pass of the same length, not graph-replayed)
+    bt.set_launch_config(tune["ctas_per_sm"], tune["sort_every"], use_graph=False)
+    bt.profile(True)
+    bt.profile_read()
+    bt.step_all(dts, min(args.steps, 50))
+    k_ms, k_n = bt.profile_read()
+    bt.profile(False)
+    yielded = bt.metrics_i(0)["n_yielded"]   # the counter covers every instance of the handle
+    bt.close()
+    if dist:
+        t = torch.tensor([ms, float(n_live)], device=dev, dtype=torch.float64)
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        tot = t.clone()
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        ms_max, live_tot = float(mx[0]), float(tot[1])
+    else:
+        ms_max, live_tot = ms, float(n_live)
+    value = live_tot * args.steps / (ms_max / 1e3)
+    out = None
+    if rank == 0:
+        rng = np.random.default_rng(3)
+        sample = [cases[i] for i in rng.choice(len(cases), size=min(32, len(cases)), replace=False)]
+        plain = plain_sequential(sample, 20, stream)
+        peak, peak_kind = load_peaks()
+        ppc_mean = float(np.mean([c["box"]["ppc"] for c in cases]))
+        steps_total = args.steps + args.warmup + (0 if args.no_tune else 168) + min(args.steps, 50)
+        f_yield = yielded / max(1.0, n_live * steps_total)
+        b_alg = B_ALG_BASE + B_ALG_YIELD * f_yield + B_ALG_GRID / ppc_mean
+        avg = (k_ms / max(k_n, 1)) / 1e3
+        achieved = b_alg * n_live / avg / 1e9 if k_n else None
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+               "config": {"workload": f"batched: {len(cases)} workpieces of the config-3 sweep (cells log-uniform "
+                                      "16^3..64^3, aspect 1-4, 4-8 ppc, per-instance Johnson-Cook, speed and depth "
+                                      "of cut, rounded-wedge tool), one persistent launch per step, CUDA graph",
+                          "instances": len(cases), "particles_per_gpu": int(n_live), "launch_config": tune,
+                          "parallelism": f"replicas{world}", "l2": "working set >> L2 (no flush needed)",
+                          "yield_fraction": f_yield},
+               "gpu_launches": int(launches),
+               "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": (achieved / peak) if achieved else None,
+                            "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                            else "fallback", "traffic": None,
+                            "kernel": "k_step<float,G2P,P2G> (fused)", "kernel_launches_timed": int(k_n),
+                            "kernel_ms_avg": k_ms / max(k_n, 1), "bytes_alg_per_update": b_alg},
+               "plain_sequential": dict(plain, sample=f"{len(sample)} of the same workpieces, one at a time through "
+                                                      "mpm_create/mpm_step, 20 timed steps each"),
+               "batched_over_plain": value / plain["value"],
+               "clocks": clocks}
+    if dist:
+        dist.barrier()
+    return out
+
+
+# ----------------------------------------------------------------- serving arm
+
+def run_serving(args):
+    """Continuous batching under Poisson arrivals: a submitter thread submits
+    each request at its arrival time (the server stamps it then) while this
+    thread runs the server's ticks; after the window, throughput = particle
+    updates done in the window / its length, latency = done - submit of the
+    requests that completed in it."""
+    import threading
+    import torch
+    rank, world, local, dist = dist_setup(args.gpus)
+    from mpm_b200 import Server, capi as A, workpiece as W
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    rng = np.random.default_rng(17 + rank)
+    n_arr = int(args.rate * args.duration * 1.5) + 16
+    gaps = rng.exponential(1.0 / args.rate, n_arr)
+    arrivals = np.cumsum(gaps)
+    arrivals = arrivals[arrivals < args.duration]
+    reqs = []
+    for i in range(len(arrivals)):
+        c = W.config3_case(rng, i, cells_lo=16, cells_hi=96, ppc=8)
+        reqs.append((c, int(rng.integers(200, 2001))))
+    srv = Server(precision=A.PREC_F32, hbm_budget_bytes=int(args.budget_gb * 1e9), max_chunk=args.chunk,
+                 use_graph=True, stream=stream.cuda_stream)
+    ids = []
+    stop = threading.Event()
+
+    def submitter(t0):
+        for k, (c, n) in enumerate(reqs):
+            delay = t0 + arrivals[k] - time.perf_counter()
+            if delay > 0 and stop.wait(delay):
+                return
+            ids.append(srv.submit(c, n))
+
+    sampler = ClockSampler(physical_gpu_index(local))
+    sampler.start()
+    t0 = time.perf_counter()
+    th = threading.Thread(target=submitter, args=(t0,), daemon=True)
+    th.start()
+    ticks = 0
+    while time.perf_counter() - t0 < args.duration:
+        if srv.tick() == 0:
+            time.sleep(0.001)
+        ticks += 1
+    elapsed = time.perf_counter() - t0
+    stop.set()
+    th.join()
+    st = srv.stats()
+    clocks = sampler.stop()
+    lat, done_particles = [], 0
+    for i in list(ids):
+        r = srv.poll(i)
+        if r["state"] == A.REQ_DONE and r["t_done"] <= elapsed:
+            lat.append(r["t_done"] - r["t_submit"])
+            done_particles += r["n_particles"] * r["steps_done"]
+    srv.close()
+    value = st["particle_updates"] / elapsed
+    out = None
+    if rank == 0:
+        sample = [c for c, _ in reqs[:16]]
+        plain = plain_sequential(sample, 20, stream)
+        q = (lambda p: float(np.percentile(lat, p))) if lat else (lambda p: None)
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": None,
+               "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+               "dtype": "f32", "data": "synthetic",
+               "config": {"workload": f"serving: Poisson arrivals at {args.rate:g} requests/s for {args.duration:g} s, "
+                                      "requests of 16^3..96^3 cells (log-uniform, aspect 1-4) at 8 ppc, parameters as "
+                                      "the config-3 sweep, 200-2000 steps each; continuous batching, state resident "
+                                      f"on the device, admission by a {args.budget_gb:g} GB budget, chunks of "
+                                      f"{args.chunk} steps per tick",
+                          "parallelism": f"replicas{world}", "budget_gb": args.budget_gb, "max_chunk": args.chunk},
+               "requests": {"offered": st["offered"], "admitted": st["admitted"], "completed_in_window": len(lat),
+                            "queued_at_end": st["queued"], "resident_at_end": st["resident"],
+                            "resident_particles_at_end": st["resident_particles"], "ticks": st["ticks"]},
+               "latency_s": {"p50": q(50), "p99": q(99), "p999": q(99.9), "of": "requests completed in the window"},
+               "completed_particle_updates_per_s": done_particles / elapsed,
+               "plain_sequential": dict(plain, sample="the first 16 requests, one at a time through mpm_create/"
+                                                      "mpm_step, 20 timed steps each"),
+               "served_over_plain": value / plain["value"],
+               "clocks": clocks}
+    if dist:
+        dist.barrier()
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -367,16 +594,31 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="large", choices=["large", "small", "precision"])
+    ap.add_argument("--config", default="large", choices=["large", "small", "precision", "batched", "serving"])
+    ap.add_argument("--instances", type=int, default=512)
+    ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
+    ap.add_argument("--duration", type=float, default=60.0, help="serving: window in seconds")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
+    ap.add_argument("--chunk", type=int, default=50, help="serving: steps per tick at most")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if args.steps is None:
+        args.steps = 300 if args.config == "batched" else 500
+    if args.impl == "reference":
+        out = run_reference(args)
+    elif args.config == "batched":
+        out = run_batched(args)
+    elif args.config == "serving":
+        out = run_serving(args)
+    else:
+        out = run_ours(args)
     if out is not None:
         print(json.dumps(out), flush=True)
 

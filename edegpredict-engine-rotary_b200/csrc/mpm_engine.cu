@@ -114,7 +114,7 @@ class Engine final : public EngineBase {
     bool binned = false;
     int64_t since_sort = 0, n_sorts = 0;
     int64_t launch_base = 0;
-    int sort_every = 16, threads = 128, ctas_per_sm = 4;
+    int sort_every = 16, threads = 128, ctas_per_sm = 4, prec_ = MPM_PREC_F32;
     bool use_graph = false;
     int rbuf = 0;
     // step-kernel timing (mpm_profile_enable)
@@ -181,7 +181,10 @@ class Engine final : public EngineBase {
     mpm_status init(const mpm_params* params, const int64_t* caps, int n, cudaStream_t stream_in) {
         launch_base = launch_counter();
         std::vector<InstHost> nI;
-        mpm_status s = make_insts(params, caps, n, &nI);
+        mpm_status s = check_params(&params[0], &err);
+        if (s != MPM_OK) return s;
+        prec_ = params[0].precision;
+        s = make_insts(params, caps, n, &nI);
         if (s != MPM_OK) return s;
         sort_every = params[0].sort_every > 0 ? params[0].sort_every : 16;
         threads = params[0].threads_per_block > 0 ? params[0].threads_per_block : 128;
@@ -209,8 +212,7 @@ class Engine final : public EngineBase {
         for (int i = 0; i < n; ++i) {
             mpm_status s = check_params(&params[i], &err);
             if (s != MPM_OK) return s;
-            const int prec = I.empty() ? params[0].precision : I[0].p.precision;
-            if (params[i].precision != prec) {
+            if (params[i].precision != prec_) {
                 err = "all instances of an engine share one precision";
                 return MPM_INVALID_ARG;
             }
@@ -230,12 +232,12 @@ class Engine final : public EngineBase {
     // Grow-only device buffer: reallocates (contents dropped) when `need`
     // elements do not fit, with a quarter of headroom.
     template <typename T>
-    mpm_status grow(T*& p, int64_t& have, int64_t need) {
+    mpm_status grow(T*& p, int64_t& have, int64_t need, bool headroom = true) {
         need = std::max<int64_t>(need, 1);
         if (p && need <= have) return MPM_OK;
         if (p) cudaFree(p);
         p = nullptr;
-        const int64_t n = need + need / 4;
+        const int64_t n = headroom ? need + need / 4 : need;
         CK(cudaMalloc(&p, sizeof(T) * n));
         have = n;
         return MPM_OK;
@@ -390,9 +392,11 @@ class Engine final : public EngineBase {
             CK(cudaMalloc(&mask_pool, nn));
             nn_alloc = nn;
         }
-        CK(cudaMemsetAsync(gpool[0], 0, sizeof(V4<R>) * std::max<int64_t>(nn_total, 1), st));
-        CK(cudaMemsetAsync(gpool[1], 0, sizeof(V4<R>) * std::max<int64_t>(nn_total, 1), st));
-        CK(cudaMemsetAsync(mask_pool, 0, std::max<int64_t>(nn_total, 1), st));
+        if (nn_total > 0) {
+            CK(cudaMemsetAsync(gpool[0], 0, sizeof(V4<R>) * nn_total, st));
+            CK(cudaMemsetAsync(gpool[1], 0, sizeof(V4<R>) * nn_total, st));
+            CK(cudaMemsetAsync(mask_pool, 0, nn_total, st));
+        }
         rbuf = 0;
         // sort scratch, key and bin tables
         MS(grow(d_key, slot_alloc[0], cp));
@@ -432,6 +436,66 @@ class Engine final : public EngineBase {
         CK(cudaStreamSynchronize(st));
         binned = false;
         since_sort = 0;
+        return MPM_OK;
+    }
+
+    // Allocates every pool for the given totals up front (only while the
+    // engine holds no instance), so that later instance changes within them
+    // never reallocate.
+    mpm_status reserve(int64_t particles, int64_t nodes, int64_t keys, int64_t bins, int max_inst,
+                       bool backstress) override {
+        if (!I.empty()) {
+            err = "reserve needs an engine without instances";
+            return MPM_INVALID_ARG;
+        }
+        if (particles < 1 || nodes < 1 || keys < 1 || bins < 1 || max_inst < 1) {
+            err = "reserve sizes must be positive";
+            return MPM_INVALID_ARG;
+        }
+        CK(cudaStreamSynchronize(st));
+        drop_graphs();
+        for (int b = 0; b < 2; ++b) {
+            if (pbuf[b]) cudaFree(pbuf[b]);
+            pbuf[b] = nullptr;
+        }
+        for (int b = 0; b < 2; ++b) {
+            CK(cudaMalloc(&pbuf[b], pstate_bytes(particles, backstress)));
+            carve(pbuf[b], particles, backstress, ps[b]);
+            if (backstress) {
+                CK(cudaMemsetAsync(ps[b].K[0], 0, sizeof(V4<R>) * particles, st));
+                CK(cudaMemsetAsync(ps[b].K[1], 0, sizeof(V4<R>) * particles, st));
+            }
+        }
+        pcap_alloc = particles;
+        has_K = backstress;
+        cur = 0;
+        for (int b = 0; b < 2; ++b) {
+            if (gpool[b]) cudaFree(gpool[b]);
+            gpool[b] = nullptr;
+            CK(cudaMalloc(&gpool[b], sizeof(V4<R>) * nodes));
+        }
+        if (mask_pool) cudaFree(mask_pool);
+        mask_pool = nullptr;
+        CK(cudaMalloc(&mask_pool, nodes));
+        nn_alloc = nodes;
+        MS(grow(d_key, slot_alloc[0], particles, false));
+        MS(grow(d_rank, slot_alloc[1], particles, false));
+        MS(grow(d_newbin, slot_alloc[2], particles, false));
+        MS(grow(d_pos, slot_alloc[3], 3 * particles, false));
+        MS(grow(d_count, key_alloc[0], keys + 1, false));
+        MS(grow(d_offset, key_alloc[1], keys + 1, false));
+        MS(grow(d_flag, bin_alloc[0], bins + 1, false));
+        MS(grow(d_flag_scan, bin_alloc[1], bins + 1, false));
+        MS(grow(d_bin_key, bin_alloc[2], bins, false));
+        MS(grow(d_bin_inst, bin_alloc[3], bins, false));
+        MS(grow(d_bin_local, bin_alloc[4], bins, false));
+        MS(grow(d_work, bin_alloc[5], bins, false));
+        MS(grow(d_scan_tmp, scan_alloc, std::max<int64_t>(scan_tmp_size(keys + 1), scan_tmp_size(particles)), false));
+        MS(grow(d_key_base, inst_alloc[0], max_inst, false));
+        MS(grow(d_inst_pbase, inst_alloc[1], max_inst, false));
+        MS(grow(d_inst, inst_alloc[2], max_inst, false));
+        MS(grow(d_map, map_alloc, max_inst, false));
+        CK(cudaStreamSynchronize(st));
         return MPM_OK;
     }
 
@@ -1201,7 +1265,7 @@ class Engine final : public EngineBase {
 
 std::unique_ptr<EngineBase> make_engine(const mpm_params* params, const int64_t* caps, int n, cudaStream_t st,
                                         mpm_status* status, std::string* err) {
-    if (!params || !caps || n <= 0) {
+    if (!params || n < 0 || (n > 0 && !caps)) {
         *status = MPM_INVALID_ARG;
         *err = "no instances";
         return nullptr;

@@ -55,6 +55,8 @@ class EngineBase {
     virtual mpm_status get_config(mpm_launch_config* c) = 0;
     virtual mpm_status set_config(const mpm_launch_config* c) = 0;
     virtual mpm_status autotune(const double* dt_per_inst, mpm_launch_config* best) = 0;
+    virtual mpm_status reserve(int64_t particles, int64_t nodes, int64_t keys, int64_t bins, int max_inst,
+                               bool backstress) = 0;
     virtual mpm_status change_instances(const mpm_params* params, const int64_t* caps, int n_add,
                                         const int32_t* remove, int n_remove, int* first) = 0;
     virtual mpm_status sync() = 0;
@@ -66,7 +68,8 @@ class EngineBase {
     virtual mpm_status profile_read(double* ms, int64_t* n) = 0;
 };
 
-// Creates an engine for n instances (all of the same precision).  Returns
+// Creates an engine for n instances (all of the same precision; n may be 0,
+// params[0] then only sets the precision and launch defaults).  Returns
 // nullptr with a message in `err` on failure.
 std::unique_ptr<EngineBase> make_engine(const mpm_params* params, const int64_t* caps, int n, cudaStream_t st,
                                         mpm_status* status, std::string* err);

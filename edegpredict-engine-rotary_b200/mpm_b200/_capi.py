@@ -78,6 +78,39 @@ PARTICLE_FIELDS = {  # name -> values per particle
     "plastic_strain": 1, "strain_rate": 1, "temperature": 1, "damage": 1, "residual_stress": 1,
 }
 
+REQ_UNKNOWN, REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = range(5)
+
+
+class MpmRequest(C.Structure):
+    _fields_ = [("params", MpmParams), ("tool", MpmToolDesc), ("c0", _i32 * 3), ("c1", _i32 * 3), ("ppc", _i32),
+                ("fixed_layers", _i32), ("seed", C.c_uint64), ("instance_key", C.c_uint32), ("nsteps", _i32),
+                ("dt", _d), ("T0", _d)]
+
+
+class MpmResult(C.Structure):
+    _fields_ = [("state", _i32), ("status", _i32), ("n_particles", _i64), ("steps_done", _i64),
+                ("t_submit", _d), ("t_admit", _d), ("t_done", _d), ("metrics", MpmMetrics)]
+
+    def as_dict(self) -> dict:
+        return {"state": self.state, "status": self.status, "n_particles": self.n_particles,
+                "steps_done": self.steps_done, "t_submit": self.t_submit, "t_admit": self.t_admit,
+                "t_done": self.t_done, "metrics": self.metrics.as_dict()}
+
+
+class MpmServerConfig(C.Structure):
+    _fields_ = [("precision", _i32), ("max_chunk", _i32), ("hbm_budget_bytes", _i64), ("max_resident", _i32),
+                ("use_graph", _i32), ("backstress", _i32), ("_pad", _i32)]
+
+
+class MpmServerStats(C.Structure):
+    _fields_ = [("offered", _i64), ("admitted", _i64), ("completed", _i64), ("failed", _i64), ("queued", _i64),
+                ("resident", _i64), ("particle_updates", _i64), ("resident_particles", _i64), ("ticks", _i64),
+                ("busy_seconds", _d)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class MpmLaunchConfig(C.Structure):
     _fields_ = [("ctas_per_sm", C.c_int32), ("sort_every", C.c_int32), ("use_graph", C.c_int32),
                 ("_pad", C.c_int32)]
@@ -121,6 +154,13 @@ def lib() -> C.CDLL:
             "mpm_batch_sync_metrics": (_i32, [_vp, _i32, P(MpmMetrics)]),
             "mpm_batch_get_counts": (_i32, [_vp, _i32, P(_i64), P(_i64), P(_d)]),
             "mpm_batch_change": (_i32, [_vp, P(MpmParams), P(_i64), _i32, P(_i32), _i32, P(_i32)]),
+            "mpm_server_create": (_i32, [P(MpmServerConfig), _vp, P(_vp)]),
+            "mpm_server_destroy": (_i32, [_vp]),
+            "mpm_server_submit": (_i32, [_vp, P(MpmRequest), P(_i64)]),
+            "mpm_server_tick": (_i32, [_vp, P(_i32)]),
+            "mpm_server_poll": (_i32, [_vp, _i64, P(MpmResult)]),
+            "mpm_server_stats_get": (_i32, [_vp, P(MpmServerStats)]),
+            "mpm_server_footprint": (_i32, [P(MpmServerConfig), P(MpmRequest), P(_i64)]),
             "mpm_get_launch_config": (_i32, [_vp, P(MpmLaunchConfig)]),
             "mpm_set_launch_config": (_i32, [_vp, P(MpmLaunchConfig)]),
             "mpm_autotune": (_i32, [_vp, P(_d), P(MpmLaunchConfig)]),

@@ -291,3 +291,76 @@ class Batch(Solver):
         self._check(self._lib.mpm_autotune(self.h, d.ctypes.data_as(C.POINTER(C.c_double)), C.byref(c)))
         return c.as_dict()
 
+
+def make_request(case: dict, nsteps: int, precision: int = A.PREC_F32, dt: Optional[float] = None) -> A.MpmRequest:
+    """mpm_request of a workpiece case (workpiece.make_case layout)."""
+    from . import workpiece as W
+    r = A.MpmRequest()
+    r.params = W.to_mpm_params(case, precision=precision)
+    r.tool = Solver.tool_desc(case["tool"])
+    b = case["box"]
+    for k in range(3):
+        r.c0[k] = int(b["c0"][k])
+        r.c1[k] = int(b["c1"][k])
+    r.ppc = int(b["ppc"])
+    r.fixed_layers = int(b["fixed_layers"])
+    r.seed = int(b["seed"])
+    r.instance_key = int(b["instance"])
+    r.nsteps = int(nsteps)
+    r.dt = float(dt if dt is not None else case["dt"])
+    r.T0 = float(b["T0"])
+    return r
+
+
+class Server:
+    """The serving loop (mpm_server_*): submit requests at any time, call
+    tick() to admit, step and retire; poll() for results."""
+
+    def __init__(self, precision: int = A.PREC_F32, hbm_budget_bytes: int = 8 << 30, max_chunk: int = 50,
+                 max_resident: int = 0, use_graph: bool = True, backstress: bool = False, stream: int = 0):
+        self._lib = A.lib()
+        self.precision = precision
+        self.cfg = A.MpmServerConfig(int(precision), int(max_chunk), int(hbm_budget_bytes), int(max_resident),
+                                     1 if use_graph else 0, 1 if backstress else 0, 0)
+        h = C.c_void_p()
+        A.check(self._lib.mpm_server_create(C.byref(self.cfg), C.c_void_p(stream or None), C.byref(h)))
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            self._lib.mpm_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, case: dict, nsteps: int, dt: Optional[float] = None) -> int:
+        r = make_request(case, nsteps, self.precision, dt)
+        i = C.c_int64()
+        A.check(self._lib.mpm_server_submit(self.h, C.byref(r), C.byref(i)))
+        return i.value
+
+    def tick(self) -> int:
+        n = C.c_int32()
+        A.check(self._lib.mpm_server_tick(self.h, C.byref(n)))
+        return n.value
+
+    def poll(self, rid: int) -> dict:
+        r = A.MpmResult()
+        A.check(self._lib.mpm_server_poll(self.h, int(rid), C.byref(r)))
+        return r.as_dict()
+
+    def stats(self) -> dict:
+        s = A.MpmServerStats()
+        A.check(self._lib.mpm_server_stats_get(self.h, C.byref(s)))
+        return s.as_dict()
+
+    def footprint(self, case: dict, nsteps: int = 1) -> int:
+        r = make_request(case, nsteps, self.precision)
+        b = C.c_int64()
+        A.check(self._lib.mpm_server_footprint(C.byref(self.cfg), C.byref(r), C.byref(b)))
+        return b.value
+

@@ -109,19 +109,20 @@ def config4(**kw) -> dict:
 
 
 def config3_case(rng: np.random.Generator, index: int, *, cells_lo: int = 16, cells_hi: int = 64, steps: int = 300,
-                 dx: float = 2e-5, seed: int = 1234, precision=A.PREC_F32) -> dict:
+                 dx: float = 2e-5, seed: int = 1234, precision=A.PREC_F32, ppc: Optional[int] = None) -> dict:
     """One instance of the batched sweep: cell count log-uniform in
     [cells_lo^3, cells_hi^3] with aspect ratios (Wx/Wz, Wy/Wz) uniform in
     [1, 4], 4-8 ppc, Johnson-Cook A in [300, 1200] MPa, B in [200, 1100] MPa,
     n in [0.1, 0.9], C in [0.005, 0.03], m in [0.8, 1.4], cutting speed in
     [0.5, 5] m/s, depth of cut in [0.02, 0.2] mm (capped at half the height),
     elastic and thermal rows interpolated between AISI 4340 and Ti-6Al-4V;
-    rounded wedge with edge radius 2 x depth of cut at mid-length."""
+    rounded wedge with edge radius 2 x depth of cut at mid-length.  `ppc`
+    fixes the particles per cell (the serving workload uses 8)."""
     C = math.exp(rng.uniform(math.log(cells_lo ** 3), math.log(cells_hi ** 3)))
     ax, ay = rng.uniform(1.0, 4.0, 2)
     wz = max(4, int(round((C / (ax * ay)) ** (1.0 / 3.0))))
     wx, wy = max(4, int(round(ax * wz))), max(4, int(round(ay * wz)))
-    ppc = int(rng.integers(4, 9))
+    ppc = int(rng.integers(4, 9)) if ppc is None else int(ppc)
     f = rng.uniform()
     mat = {k: (1.0 - f) * AISI_4340[k] + f * TI_6AL_4V[k] for k in ("E", "nu", "rho_phys", "cp", "Tm")}
     mat.update(beta=0.9, Tamb=293.0, edot0=1.0, H_kin=0.0, D1=0.05, D2=3.44, D3=-2.12, D4=0.002, D5=0.61, D_th=1.0,

@@ -139,9 +139,10 @@ typedef struct mpm_metrics {
     double max_temperature, max_von_mises, max_plastic_strain, mean_plastic_strain;
     int64_t n_active, n_chip, n_fixed, n_inactive;
     double bounds_min[3], bounds_max[3];   /* ACTIVE and CHIP particles */
-    int64_t n_escaped;                     /* particle updates done off their bin tile (cumulative) */
+    /* counters of the whole handle (all instances of a batch), cumulative */
+    int64_t n_escaped;                     /* particle updates done off their bin tile */
     int64_t n_sorts;                       /* re-bins so far */
-    int64_t n_yielded;                     /* particle updates that took a plastic return (cumulative) */
+    int64_t n_yielded;                     /* particle updates that took a plastic return */
 } mpm_metrics;
 
 typedef struct mpm_handle mpm_handle;
@@ -269,6 +270,70 @@ mpm_status mpm_set_launch_config(mpm_handle *h, const mpm_launch_config *cfg);
  * all, dt[i] per instance, counted like any other steps) and keeps the
  * fastest; *chosen (may be NULL) receives it. */
 mpm_status mpm_autotune(mpm_handle *h, const double *dt, mpm_launch_config *chosen);
+
+/*
+ * Serving loop (continuous batching).  No counterpart in the reference.
+ * Solve requests -- a workpiece, its tool and a number of steps -- are
+ * submitted at any time; each mpm_server_tick retires finished requests,
+ * admits queued ones in arrival order while their footprint fits the device
+ * pools reserved from hbm_budget_bytes (88 % particle state, 8 % grids, 3 %
+ * sort keys, 0.5 % bin tables), and advances every resident request by the
+ * same number of steps (at most max_chunk) in one batch step call, so
+ * requests admitted while others run share their launches.  The state of
+ * every resident request stays on the device.  submit and poll may be
+ * called from other threads than tick; tick from one thread at a time.
+ */
+typedef struct mpm_request {
+    mpm_params params;         /* grid, material and options of this workpiece */
+    mpm_tool_desc tool;        /* tool at t = 0: MPM_TOOL_NONE or an SDF mode */
+    int32_t c0[3], c1[3];      /* workpiece box in cells (as mpm_init_box) */
+    int32_t ppc, fixed_layers;
+    uint64_t seed;
+    uint32_t instance_key;
+    int32_t nsteps;
+    double dt, T0;
+} mpm_request;
+
+enum { MPM_REQ_UNKNOWN = 0, MPM_REQ_QUEUED = 1, MPM_REQ_RUNNING = 2, MPM_REQ_DONE = 3, MPM_REQ_FAILED = 4 };
+
+typedef struct mpm_result {
+    int32_t state;             /* MPM_REQ_* */
+    int32_t status;            /* mpm_status of a FAILED request */
+    int64_t n_particles;
+    int64_t steps_done;
+    double t_submit, t_admit, t_done;   /* seconds on the server's clock */
+    mpm_metrics metrics;       /* at completion (DONE) */
+} mpm_result;
+
+typedef struct mpm_server_config {
+    int32_t precision;         /* MPM_PREC_F32 or MPM_PREC_F64, for every request */
+    int32_t max_chunk;         /* steps per tick at most (0: 50) */
+    int64_t hbm_budget_bytes;  /* device memory reserved at creation for resident requests */
+    int32_t max_resident;      /* requests resident at once at most (0: 4096) */
+    int32_t use_graph;         /* replay the tick's step calls from captured CUDA graphs */
+    int32_t backstress;        /* also reserve backstress state (requests with H_kin > 0) */
+    int32_t _pad;
+} mpm_server_config;
+
+typedef struct mpm_server_stats {
+    int64_t offered, admitted, completed, failed, queued, resident;
+    int64_t particle_updates;  /* particles x steps of all requests so far */
+    int64_t resident_particles;
+    int64_t ticks;
+    double busy_seconds;       /* time spent inside mpm_server_tick */
+} mpm_server_stats;
+
+typedef struct mpm_server mpm_server;
+mpm_status mpm_server_create(const mpm_server_config *cfg, void *stream, mpm_server **out);
+mpm_status mpm_server_destroy(mpm_server *s);
+/* Queues a request; *id identifies it for mpm_server_poll.  MPM_CAPACITY when
+ * its footprint can never fit the pools. */
+mpm_status mpm_server_submit(mpm_server *s, const mpm_request *req, int64_t *id);
+mpm_status mpm_server_tick(mpm_server *s, int32_t *n_resident);
+mpm_status mpm_server_poll(mpm_server *s, int64_t id, mpm_result *out);
+mpm_status mpm_server_stats_get(mpm_server *s, mpm_server_stats *out);
+/* Device bytes a request holds while resident (host-only arithmetic). */
+mpm_status mpm_server_footprint(const mpm_server_config *cfg, const mpm_request *req, int64_t *bytes);
 
 /* Record CUDA events around every launch of the step kernel (enable != 0),
  * for timing the dominant kernel inside a longer run.  mpm_profile_read
