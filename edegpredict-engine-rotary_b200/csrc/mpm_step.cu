@@ -341,9 +341,16 @@ template <typename R>
 __device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[9], R& eps, R& dT, R& D, R edot,
                                            R sig[6], R sl[3], R& J, R* sres_p, R* bsx, int& errf) {
     JCOut o{true, false, false};
-    // inverse of G = I + Hp (identity when |det G| < 1e-12, inv3x3 :50-57)
+    // inverse of G = I + Hp (identity when |det G| < 1e-12, inv3x3 :50-57);
+    // a particle that never yielded has Hp = 0 exactly and F_e = F
     R E[9];
-    {
+    bool hp0 = true;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) hp0 = hp0 && (Hp[q] == R(0));
+    if (hp0) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) E[q] = H[q];
+    } else {
         const R dgm1 = detm1(Hp);
         const R det = R(1) + dgm1;
         R Gi[9];
@@ -407,8 +414,9 @@ __device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[
     Ts = fmin(fmax(Ts, R(0)), R(1));
     const R es = fmax(edot / P.edot0, R(1e-5));
     const R rt = R(1) + P.C * log(es);
-    const R tt = R(1) - pow(Ts, P.m);
-    const R Y = (P.A + P.B * pow(eps, P.n)) * rt * tt;
+    // pow(0, y) is +0 for y > 0: skipped for the common unheated, unyielded particle
+    const R tt = R(1) - ((Ts > R(0) || !(P.m > R(0))) ? pow(Ts, P.m) : R(0));
+    const R Y = (P.A + P.B * ((eps > R(0) || !(P.n > R(0))) ? pow(eps, P.n) : R(0))) * rt * tt;
 #pragma unroll
     for (int q2 = 0; q2 < 6; ++q2) sig[q2] = s[q2];
     sl[0] = s[3]; sl[1] = s[4]; sl[2] = s[5];
@@ -509,15 +517,17 @@ template <typename R> struct StepCfg {
 constexpr int kPay = 24;
 constexpr int kOff = 27;  // stencil offsets, off = i + 3j + 9k
 
+// Staging slots per base cell and pass; a particle beyond them scatters
+// straight to the grid (counted with the escaped updates).
+constexpr int kCellCap = 16;
+
 template <typename R> struct StepSmem {
     V4<R> raw[kTileNodes];                 // TMA destination (offset 0 of the 128-byte aligned block)
     R vel[3][kPlane];                      // node velocities after the grid update
     R cacc[4][kOff][kCellsPerBin];         // per-cell sums of the 27 stencil nodes: m, p_x, p_y, p_z
     R pay[kPay][StepCfg<R>::kChunk];       // scatter payload of the staged particles
-    short order[StepCfg<R>::kChunk];       // staged particles grouped by base cell
-    int cnt[kCellsPerBin];                 // staged particles per cell (filled by atomics)
-    int ccount[kCellsPerBin];              // copy of cnt for the accumulation pass
-    int cstart[kCellsPerBin];
+    short slot[kCellsPerBin][kCellCap];    // staged particles of each base cell
+    int cnt[2][kCellsPerBin];              // staged particles per cell (atomic ranks), by pass parity
     uint64_t mbar;
     int fail;
 };
@@ -560,15 +570,18 @@ __device__ __forceinline__ void channel_add(const R (&w)[3][3], const R (&dw)[3]
 // Accumulation of one cell's staged particles (thread pair per cell: h = 0
 // takes m and p_x, h = 1 takes p_y and p_z) in registers, then added to the
 // cell's private block of cacc.  Each cell block has exactly one writer per
-// channel, so no atomics are needed.
+// channel, so no atomics are needed.  par: parity of the staging pass.
 template <typename R>
-__device__ __forceinline__ void cell_accumulate(StepSmem<R>& Sm, int cell, int h, R pm) {
+__device__ __forceinline__ void cell_accumulate(StepSmem<R>& Sm, int cell, int h, R pm, int par) {
     R a0[kOff], a1[kOff];
 #pragma unroll
     for (int o = 0; o < kOff; ++o) { a0[o] = R(0); a1[o] = R(0); }
-    const int s0 = Sm.cstart[cell], n = Sm.ccount[cell];
+    const int n = min(Sm.cnt[par][cell], kCellCap);
+    // the other parity's counts were last read in the previous pass: clear
+    // them for the next one
+    if (h == 0) Sm.cnt[par ^ 1][cell] = 0;
     for (int q = 0; q < n; ++q) {
-        const int e = Sm.order[s0 + q];
+        const int e = Sm.slot[cell][q];
         R w[3][3], dw[3][3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) (void)bspline(Sm.pay[a][e], w[a], dw[a]);
@@ -608,7 +621,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
     extern __shared__ __align__(128) unsigned char smem_raw[];
     StepSmem<R>& Sm = *reinterpret_cast<StepSmem<R>*>(smem_raw);
     constexpr int kChunk = StepCfg<R>::kChunk;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31;
     const int nw = *n_work;
     uint32_t phase = 0;
     int errf = 0;
@@ -618,8 +631,9 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
         fence_async_smem();
     }
     if (tid == 0) Sm.fail = 0;
-    if (tid < kCellsPerBin) Sm.cnt[tid] = 0;
+    if (tid < 2 * kCellsPerBin) (&Sm.cnt[0][0])[tid] = 0;
     __syncthreads();
+    int par = 0;  // parity of the staging pass (counts double-buffered across passes)
     int last_inst = -1;
 
     for (int wi = blockIdx.x; wi < nw; wi += gridDim.x) {
@@ -673,13 +687,11 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
         const R idx_ = (R)(1.0 / P.dx);
         const bool chip_now = G2P && P.chip_every > 0 && ((P.step0 + sa.k) % P.chip_every) == 0;
         for (int base = 0; base < wk.count; base += kChunk) {
-            int myc[StepCfg<R>::kPerThread], myr[StepCfg<R>::kPerThread];
 #pragma unroll 1
             for (int sidx = 0; sidx < StepCfg<R>::kPerThread; ++sidx) {
                 const int slot = tid + sidx * kNT;
                 const int pl = base + slot;
                 const int64_t pi = P.pbase + wk.start + pl;
-                int scell = -1;  // base cell of this particle's tile scatter, or -1
                 uint8_t st = (pl < wk.count) ? ps.status[pi] : (uint8_t)ST_INACTIVE;
                 if (st != ST_INACTIVE) {
                     const uint8_t st_in = st;
@@ -900,9 +912,14 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                 S[2] = sf * sig[4]; S[6] = sf * sl[1];
                                 S[5] = sf * sig[5]; S[7] = sf * sl[2];
                             }
+                            int rank = kCellCap;
                             if (bb[0] >= 0 && bb[0] < kBin && bb[1] >= 0 && bb[1] < kBin && bb[2] >= 0 &&
                                 bb[2] < kBin) {
-                                scell = bb[0] + kBin * (bb[1] + kBin * bb[2]);
+                                const int scell = bb[0] + kBin * (bb[1] + kBin * bb[2]);
+                                rank = atomicAdd(&Sm.cnt[par][scell], 1);
+                                if (rank < kCellCap) Sm.slot[scell][rank] = (short)slot;
+                            }
+                            if (rank < kCellCap) {
                                 Sm.pay[0][slot] = xi[0]; Sm.pay[1][slot] = xi[1]; Sm.pay[2][slot] = xi[2];
 #pragma unroll
                                 for (int a = 0; a < 3; ++a) Sm.pay[3 + a][slot] = Q[a];
@@ -944,34 +961,11 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                     }
                     c_yield += yielded ? 1 : 0;
                 }
-                myc[sidx] = scell;
-                myr[sidx] = (P2G && scell >= 0) ? atomicAdd(&Sm.cnt[scell], 1) : 0;
             }
             if (P2G) {
                 __syncthreads();
-                // group the staged particles by cell: exclusive scan of the 64 counts
-                if (warp == 0) {
-                    const int c0 = Sm.cnt[lane], c1 = Sm.cnt[lane + 32];
-                    int x0 = c0, x1 = c1;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int y0 = __shfl_up_sync(0xffffffffu, x0, o), y1 = __shfl_up_sync(0xffffffffu, x1, o);
-                        if (lane >= o) { x0 += y0; x1 += y1; }
-                    }
-                    const int tot0 = __shfl_sync(0xffffffffu, x0, 31);
-                    Sm.cstart[lane] = x0 - c0;
-                    Sm.cstart[lane + 32] = tot0 + x1 - c1;
-                    Sm.ccount[lane] = c0;
-                    Sm.ccount[lane + 32] = c1;
-                    Sm.cnt[lane] = 0;
-                    Sm.cnt[lane + 32] = 0;
-                }
-                __syncthreads();
-#pragma unroll
-                for (int sidx = 0; sidx < StepCfg<R>::kPerThread; ++sidx)
-                    if (myc[sidx] >= 0) Sm.order[Sm.cstart[myc[sidx]] + myr[sidx]] = (short)(tid + sidx * kNT);
-                __syncthreads();
-                cell_accumulate<R>(Sm, tid & (kCellsPerBin - 1), tid >> 6, P.pmass);
+                cell_accumulate<R>(Sm, tid & (kCellsPerBin - 1), tid >> 6, P.pmass, par);
+                par ^= 1;
                 __syncthreads();
             }
         }
