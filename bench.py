@@ -2,7 +2,8 @@
 """Benchmark of the B200 MPM workpiece step (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config large|small|precision|batched|serving] [--instances M]
+                    [--config large|small|precision|batched|serving|precision_study]
+                    [--instances M]
 
 Workload (default `large`): the plain large single-instance step -- 256x128x128
 cells, dx 0.02 mm, 8 particles/cell (~33.5M particles), Ti-6Al-4V, rounded
@@ -26,6 +27,10 @@ sample), as `plain_sequential` and `batched_over_plain`.
 60 s, 16^3..96^3-cell requests at 8 ppc, 200-2000 steps, 150 GB budget):
 throughput, p50/p99/p99.9 latency of the requests completed in the window,
 offered/admitted/completed counts.
+
+--config precision_study: config 4 (128x64x64 cells) for 1000 steps in FP32 and
+in FP64 from the same seeded state; relative errors of momentum, kinetic +
+internal energy, peak von Mises stress, max temperature and mean plastic strain.
 
 --impl reference: the reference's own CUDA kernels (src/MPMSolver.cu, built from
 its sources into oracle/_ref/) on the same workload -- rank 0 only.
@@ -475,6 +480,64 @@ def run_batched(args):
     return out
 
 
+# ----------------------------------------------------------------- precision study
+
+def run_precision_study(args):
+    """Config 4: the same workpiece stepped in FP32 (the product) and in FP64
+    (the oracle run of the same kernels) from the same seeded state; relative
+    errors of the conservation and peak quantities after K steps."""
+    import torch
+    rank, world, local, dist = dist_setup(args.gpus)
+    from mpm_b200 import Solver, capi as A, workpiece as W
+    case = W.config4()
+    b = case["box"]
+    cap = int(np.prod([b["c1"][i] - b["c0"][i] for i in range(3)]) * b["ppc"])
+    out = {}
+    times = {}
+    for name, prec in (("f32", A.PREC_F32), ("f64", A.PREC_F64)):
+        s = Solver(W.to_mpm_params(case, precision=prec), cap)
+        n = _init(s, case, rank=rank)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.step(case["dt"], args.steps)
+        m = s.metrics()
+        times[name] = time.perf_counter() - t0
+        out[name] = m
+        s.close()
+    a, r = out["f32"], out["f64"]
+    p32, p64 = np.array(a["momentum"]), np.array(r["momentum"])
+    pscale = max(np.linalg.norm(p64), r["mass"] * np.linalg.norm(case["tool"]["velocity"]) * 1e-3, 1e-300)
+
+    def rel(x, y):
+        return abs(x - y) / max(abs(y), 1e-300)
+    e32 = a["kinetic"] + a["internal_elastic"]
+    e64 = r["kinetic"] + r["internal_elastic"]
+    errs = {"momentum": float(np.linalg.norm(p32 - p64) / pscale),
+            "kinetic_plus_internal": rel(e32, e64),
+            "peak_von_mises": rel(a["max_von_mises"], r["max_von_mises"]),
+            "max_temperature_rise": rel(a["max_temperature"] - 293.0, r["max_temperature"] - 293.0)
+            if r["max_temperature"] > 293.0 else abs(a["max_temperature"] - r["max_temperature"]),
+            "mean_plastic_strain": rel(a["mean_plastic_strain"], r["mean_plastic_strain"])
+            if r["mean_plastic_strain"] > 0 else abs(a["mean_plastic_strain"])}
+    if rank != 0:
+        return None
+    return {"metric": "relative error FP32 vs FP64 after K steps", "value": max(errs["momentum"],
+                                                                              errs["kinetic_plus_internal"]),
+            "unit": "relative", "n_gpus": 1, "steps": args.steps, "warmup": 0, "ms_per_step": None,
+            "higher_is_better": False, "scaling": None, "vs_baseline": None, "dtype": "f32 vs f64",
+            "data": "synthetic",
+            "config": {"workload": "precision study: 128x64x64 cells, dx 0.02 mm, 8 ppc, Ti-6Al-4V, rounded wedge "
+                                   "r_e 0.3 mm at 2.5 m/s, doc 0.05 mm; the Johnson-Cook return and the "
+                                   "conservation reductions are FP64 in both runs",
+                       "particles": int(n), "target": "momentum and kinetic+internal energy within 1e-4"},
+            "errors": errs,
+            "f32": {k: a[k] for k in ("mass", "momentum", "kinetic", "internal_elastic", "max_von_mises",
+                                      "max_temperature", "mean_plastic_strain", "n_chip", "n_inactive")},
+            "f64": {k: r[k] for k in ("mass", "momentum", "kinetic", "internal_elastic", "max_von_mises",
+                                      "max_temperature", "mean_plastic_strain", "n_chip", "n_inactive")},
+            "wall_s": times}
+
+
 # ----------------------------------------------------------------- serving arm
 
 def run_serving(args):
@@ -499,7 +562,7 @@ def run_serving(args):
         c = W.config3_case(rng, i, cells_lo=16, cells_hi=96, ppc=8)
         reqs.append((c, int(rng.integers(200, 2001))))
     srv = Server(precision=A.PREC_F32, hbm_budget_bytes=int(args.budget_gb * 1e9), max_chunk=args.chunk,
-                 use_graph=True, stream=stream.cuda_stream)
+                 use_graph=True, stream=stream.cuda_stream, max_resident_particles=int(args.resident_particles))
     ids = []
     stop = threading.Event()
 
@@ -546,7 +609,8 @@ def run_serving(args):
                                       "the config-3 sweep, 200-2000 steps each; continuous batching, state resident "
                                       f"on the device, admission by a {args.budget_gb:g} GB budget, chunks of "
                                       f"{args.chunk} steps per tick",
-                          "parallelism": f"replicas{world}", "budget_gb": args.budget_gb, "max_chunk": args.chunk},
+                          "parallelism": f"replicas{world}", "budget_gb": args.budget_gb, "max_chunk": args.chunk,
+                          "max_resident_particles": int(args.resident_particles)},
                "requests": {"offered": st["offered"], "admitted": st["admitted"], "completed_in_window": len(lat),
                             "queued_at_end": st["queued"], "resident_at_end": st["resident"],
                             "resident_particles_at_end": st["resident_particles"], "ticks": st["ticks"]},
@@ -597,26 +661,31 @@ def main():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="large", choices=["large", "small", "precision", "batched", "serving"])
+    ap.add_argument("--config", default="large", choices=["large", "small", "precision", "batched", "serving",
+                                                           "precision_study"])
     ap.add_argument("--instances", type=int, default=512)
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: window in seconds")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
     ap.add_argument("--chunk", type=int, default=50, help="serving: steps per tick at most")
+    ap.add_argument("--resident-particles", type=float, default=0,
+                    help="serving: admission cap on resident particles (0: the HBM budget alone)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.steps is None:
-        args.steps = 300 if args.config == "batched" else 500
+        args.steps = {"batched": 300, "precision_study": 1000}.get(args.config, 500)
     if args.impl == "reference":
         out = run_reference(args)
     elif args.config == "batched":
         out = run_batched(args)
     elif args.config == "serving":
         out = run_serving(args)
+    elif args.config == "precision_study":
+        out = run_precision_study(args)
     else:
         out = run_ours(args)
     if out is not None:

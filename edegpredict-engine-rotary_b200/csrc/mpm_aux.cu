@@ -267,10 +267,15 @@ __global__ void k_bin_scatter(PState<R> src, PState<R> dst, const Inst<R>* insts
     const int nbv[3] = {nbn % P.nbx, (nbn / P.nbx) % P.nby, nbn / (P.nbx * P.nby)};
     V4<R> a0 = src.A[0][pi];
     if (fresh) {
-        a0.x = (R)(pos_scratch[3 * pi + 0] - (double)(nbv[0] * kBin));
-        a0.y = (R)(pos_scratch[3 * pi + 1] - (double)(nbv[1] * kBin));
-        a0.z = (R)(pos_scratch[3 * pi + 2] - (double)(nbv[2] * kBin));
+        const double p[3] = {pos_scratch[3 * pi + 0] - (double)(nbv[0] * kBin),
+                             pos_scratch[3 * pi + 1] - (double)(nbv[1] * kBin),
+                             pos_scratch[3 * pi + 2] - (double)(nbv[2] * kBin)};
+        a0.x = (R)p[0];
+        a0.y = (R)p[1];
+        a0.z = (R)p[2];
+        if (dst.X) dst.X[d] = mk4<R>((R)(p[0] - (double)a0.x), (R)(p[1] - (double)a0.y), (R)(p[2] - (double)a0.z), R(0));
     } else {
+        if (dst.X && src.X) dst.X[d] = src.X[pi];
         const int ob = src.bin[pi];
         const int obv[3] = {ob % P.nbx, (ob / P.nbx) % P.nby, ob / (P.nbx * P.nby)};
         if (ob != nbn) {
@@ -461,12 +466,21 @@ __global__ void k_gen_write(Inst<R> P, int c0x, int c0y, int c0z, int wx, int wy
 
 // ------------------------------------------------------------------ download
 
+// World position of slot pi: grid origin + (bin origin + xi) dx, with the
+// low parts of xi where the state keeps them.
 template <typename R>
-__device__ __forceinline__ void world_pos(const Inst<R>& P, int bin, const V4<R>& a0, double out[3]) {
+__device__ __forceinline__ void world_pos(const Inst<R>& P, const PState<R>& ps, int64_t pi, const V4<R>& a0,
+                                          double out[3]) {
+    const int bin = ps.bin[pi];
     const int bx = bin % P.nbx, by = (bin / P.nbx) % P.nby, bz = bin / (P.nbx * P.nby);
-    out[0] = P.ox + ((double)(bx * kBin) + (double)a0.x) * P.dx;
-    out[1] = P.oy + ((double)(by * kBin) + (double)a0.y) * P.dx;
-    out[2] = P.oz + ((double)(bz * kBin) + (double)a0.z) * P.dx;
+    double lo[3] = {0.0, 0.0, 0.0};
+    if (ps.X) {
+        const V4<R> x = ps.X[pi];
+        lo[0] = (double)x.x; lo[1] = (double)x.y; lo[2] = (double)x.z;
+    }
+    out[0] = P.ox + ((double)(bx * kBin) + ((double)a0.x + lo[0])) * P.dx;
+    out[1] = P.oy + ((double)(by * kBin) + ((double)a0.y + lo[1])) * P.dx;
+    out[2] = P.oz + ((double)(bz * kBin) + ((double)a0.z + lo[2])) * P.dx;
 }
 
 template <typename R>
@@ -481,7 +495,7 @@ __global__ void k_export(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64
                 a5 = ps.A[5][pi];
     const V4<R> b0 = ps.B[0][pi], b1 = ps.B[1][pi], b2 = ps.B[2][pi], b3 = ps.B[3][pi];
     double xw[3];
-    world_pos(P, ps.bin[pi], a0, xw);
+    world_pos(P, ps, pi, a0, xw);
     if (o.x) st_user(o.x, e, i, xw[0]);
     if (o.y) st_user(o.y, e, i, xw[1]);
     if (o.z) st_user(o.z, e, i, xw[2]);
@@ -531,7 +545,7 @@ __global__ void k_export_aos(const Inst<R>* inst, PState<R> ps, int64_t pbase, i
                 a5 = ps.A[5][pi];
     const V4<R> b0 = ps.B[0][pi], b1 = ps.B[1][pi], b2 = ps.B[2][pi], b3 = ps.B[3][pi];
     double xw[3];
-    world_pos(P, ps.bin[pi], a0, xw);
+    world_pos(P, ps, pi, a0, xw);
     q.x = xw[0]; q.y = xw[1]; q.z = xw[2];
     q.vx = b0.x; q.vy = b0.y; q.vz = b0.z;
     q.fx = q.fy = q.fz = 0.0;
@@ -619,7 +633,7 @@ __global__ void k_stats(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64_
             acc[13] += 0.5 * m * v2;
             acc[14] += (vm * vm * m) / (6.0 * 80e9) + V * eps * vm;
             double xw[3];
-            world_pos(P, ps.bin[pi], a0, xw);
+            world_pos(P, ps, pi, a0, xw);
             for (int q = 0; q < 3; ++q) {
                 acc[19 + q] = fmin(acc[19 + q], xw[q]);
                 acc[22 + q] = fmax(acc[22 + q], xw[q]);
@@ -794,6 +808,7 @@ __global__ void k_relayout(PState<R> src, PState<R> dst, const RelayoutMap* __re
     dst.sres[s] = src.sres[o];
     dst.status[s] = src.status[o];
     dst.id[s] = src.id[o];
+    if (src.X && dst.X) dst.X[s] = src.X[o];
     dst.orig[s] = src.orig[o];
     dst.bin[s] = src.bin[o];
 }

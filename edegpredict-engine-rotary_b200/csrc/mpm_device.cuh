@@ -13,8 +13,11 @@
 //     S0 = (sxx, syy, szz, sxy) S1 = (sxz, syz, 0, 0)
 //     K0/K1 backstress (same packing as S; only with H_kin > 0)
 //     sres (scalar), status (u8), id (i32)
-//   Storing F - I and F_p - I keeps FP32 relative precision on small strains;
-//   block-local positions keep ~5e-7-cell resolution for the per-step move.
+//     X  = (xi_x, xi_y, xi_z, 0) low parts  (FP32 state only: xi = A0.xyz + X.xyz)
+//   Storing F - I and F_p - I keeps FP32 relative precision on small strains.
+//   A per-step move is ~1e-4 cell, a few hundred ulps of a bin-local FP32
+//   coordinate, so its rounding would bias the trajectory by ~1e-3 of the
+//   displacement; the hi + lo pair (updated by an exact two-sum) removes that.
 //   grid: per node one vector (m, p_x, p_y, p_z), row-major (x fastest); p
 //   already contains the internal and external force impulse f*dt.
 #pragma once
@@ -55,6 +58,7 @@ template <typename R> struct PState {
     V4<R>* B[4];
     V4<R>* S[2];
     V4<R>* K[2];
+    V4<R>* X;           // FP32 state: low parts of the bin-local position (x, y, z, 0); NULL for FP64
     R* sres;
     uint8_t* status;
     int32_t* id;

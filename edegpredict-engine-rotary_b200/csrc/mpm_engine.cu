@@ -243,10 +243,11 @@ class Engine final : public EngineBase {
         return MPM_OK;
     }
 
+    static constexpr bool kPosLo = sizeof(R) == 4;   // FP32 state keeps position low parts
     static size_t pstate_bytes(int64_t cp, bool withK) {
         const size_t v4 = sizeof(V4<R>);
-        return 12 * al256(v4 * cp) + (withK ? 2 * al256(v4 * cp) : 0) + al256(sizeof(R) * cp) + al256(cp) +
-               3 * al256(4 * cp);
+        return (12 + (kPosLo ? 1 : 0)) * al256(v4 * cp) + (withK ? 2 * al256(v4 * cp) : 0) + al256(sizeof(R) * cp) +
+               al256(cp) + 3 * al256(4 * cp);
     }
     static void carve(void* base, int64_t cp, bool withK, PState<R>& s) {
         char* q = (char*)base;
@@ -260,6 +261,7 @@ class Engine final : public EngineBase {
         for (int k = 0; k < 4; ++k) s.B[k] = (V4<R>*)take(v4 * cp);
         for (int k = 0; k < 2; ++k) s.S[k] = (V4<R>*)take(v4 * cp);
         for (int k = 0; k < 2; ++k) s.K[k] = withK ? (V4<R>*)take(v4 * cp) : nullptr;
+        s.X = kPosLo ? (V4<R>*)take(v4 * cp) : nullptr;
         s.sres = (R*)take(sizeof(R) * cp);
         s.status = (uint8_t*)take(cp);
         s.id = (int32_t*)take(4 * cp);

@@ -101,7 +101,8 @@ mpm_status mpm_server_create(const mpm_server_config* cfg, void* stream, mpm_ser
     const auto t0 = srv->t0;
     srv->sched = std::make_unique<Scheduler<GpuOps>>(
         &srv->ops, pools, cfg->max_chunk, max_res,
-        [t0]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); });
+        [t0]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); },
+        cfg->max_resident_particles);
     *out = srv;
     return MPM_OK;
 }

@@ -54,9 +54,11 @@ struct PoolBytes {
 inline PoolBytes pool_bytes(int precision, bool backstress) {
     const double v4 = precision == MPM_PREC_F64 ? 32.0 : 16.0, r = precision == MPM_PREC_F64 ? 8.0 : 4.0;
     PoolBytes b;
-    // A0-A5, B0-B3, S0-S1 (+K0-K1), sres, status, id, bin, orig; two buffers;
-    // sort key, rank, new bin (int32) and the FP64 position scratch
-    b.particle = 2.0 * ((12.0 + (backstress ? 2.0 : 0.0)) * v4 + r + 1.0 + 12.0) + 12.0 + 24.0;
+    // A0-A5, B0-B3, S0-S1 (+K0-K1), X (FP32 only), sres, status, id, bin,
+    // orig; two buffers; sort key, rank, new bin (int32) and the FP64
+    // position scratch
+    const double nv4 = 12.0 + (backstress ? 2.0 : 0.0) + (precision == MPM_PREC_F64 ? 0.0 : 1.0);
+    b.particle = 2.0 * (nv4 * v4 + r + 1.0 + 12.0) + 12.0 + 24.0;
     b.node = 2.0 * v4 + 1.0;     // two grid buffers and the tool mask
     b.key = 8.0;                 // count and offset
     b.bin = 40.0;                // bin tables, flags and the work item
@@ -92,9 +94,11 @@ class Scheduler {
         mpm_result res{};
     };
 
-    Scheduler(Engine* eng, Pools pools, int max_chunk, int max_resident, std::function<double()> clock)
+    Scheduler(Engine* eng, Pools pools, int max_chunk, int max_resident, std::function<double()> clock,
+              int64_t max_resident_particles = 0)
         : eng_(eng), pools_(pools), max_chunk_(max_chunk > 0 ? max_chunk : 50),
-          max_resident_(max_resident > 0 ? max_resident : 4096), clock_(std::move(clock)) {}
+          max_resident_(max_resident > 0 ? max_resident : 4096), clock_(std::move(clock)),
+          max_particles_(max_resident_particles) {}
 
     // Queues a request (stamped with the clock); MPM_CAPACITY when it could
     // never fit the pools.
@@ -158,6 +162,9 @@ class Scheduler {
             while (!queue_.empty() && keep.size() + add.size() < (size_t)max_resident_) {
                 Req& q = all_[queue_.front()];
                 if (!pools_.fits(used, q.f)) break;
+                // the resident-particle cap never keeps the device empty
+                const bool empty = keep.empty() && add.empty();
+                if (max_particles_ > 0 && !empty && used.particles + q.f.particles > max_particles_) break;
                 addf(used, q.f);
                 add.push_back(q.id);
                 queue_.pop_front();
@@ -259,6 +266,7 @@ class Scheduler {
     Pools pools_;
     int max_chunk_, max_resident_;
     std::function<double()> clock_;
+    int64_t max_particles_ = 0;
     std::mutex mu_;
     std::unordered_map<int64_t, Req> all_;
     std::deque<int64_t> queue_;

@@ -701,6 +701,13 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                     R eps = a0.w;
                     R H[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
                     R Hp8 = a3.y, dT = a3.z, Dm = a3.w;
+                    // low parts of the position (FP32 state); the move is an exact two-sum
+                    R lo[3] = {R(0), R(0), R(0)};
+                    const bool has_lo = G2P && !fixed && ps.X != nullptr;
+                    if (has_lo) {
+                        const V4<R> xl = ps.X[pi];
+                        lo[0] = xl.x; lo[1] = xl.y; lo[2] = xl.z;
+                    }
                     R v[3] = {0, 0, 0}, Cm[9], edot = R(0);
                     bool have_C = false, dirtyA = false, wrote_C = false;
 
@@ -708,9 +715,10 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                         if (!fixed) {
                             bool far = false;
                             if (P.lod && st == ST_ACTIVE) {
-                                const double wx = P.ox + ((double)g0x + (double)xi[0]) * P.dx - prg0;
-                                const double wy = P.oy + ((double)g0y + (double)xi[1]) * P.dx - prg1;
-                                const double wz = P.oz + ((double)g0z + (double)xi[2]) * P.dx - (prg2 + P.tool_tip_dz);
+                                const double wx = P.ox + ((double)g0x + ((double)xi[0] + (double)lo[0])) * P.dx - prg0;
+                                const double wy = P.oy + ((double)g0y + ((double)xi[1] + (double)lo[1])) * P.dx - prg1;
+                                const double wz =
+                                    P.oz + ((double)g0z + ((double)xi[2] + (double)lo[2])) * P.dx - (prg2 + P.tool_tip_dz);
                                 far = sqrt(wx * wx + wy * wy + wz * wz) > P.lod_r2;
                             }
                             R w[3][3], dw[3][3];
@@ -733,7 +741,18 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                             }
                             const R d[3] = {xi[0] - R(b[0]), xi[1] - R(b[1]), xi[2] - R(b[2])};
 #pragma unroll
-                            for (int a = 0; a < 3; ++a) xi[a] = fma(v[a], dtdx, xi[a]);
+                            for (int a = 0; a < 3; ++a) {
+                                if (has_lo) {
+                                    // (xi, lo) <- xi + (lo + v dt/dx), Knuth's two-sum: exact
+                                    const R inc = fma(v[a], dtdx, lo[a]);
+                                    const R s = xi[a] + inc;
+                                    const R bv = s - xi[a];
+                                    lo[a] = (xi[a] - (s - bv)) + (inc - bv);
+                                    xi[a] = s;
+                                } else {
+                                    xi[a] = fma(v[a], dtdx, xi[a]);
+                                }
+                            }
                             dirtyA = true;
                             if (st == ST_CHIP) {
                                 edot = R(0);
@@ -771,7 +790,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                         if (chip_now) {
                             if (st == ST_ACTIVE) {
                                 const double tipz = ds(da(prg2, P.tool_tip_dz), dm(P.dx, 1.5));
-                                const double zw = P.oz + ((double)g0z + (double)xi[2]) * P.dx;
+                                const double zw = P.oz + ((double)g0z + ((double)xi[2] + (double)lo[2])) * P.dx;
                                 if (zw < tipz && Dm > R(1e-6)) {
                                     st = ST_CHIP;
                                     const V4<R> s0 = ps.S[0][pi];
@@ -823,9 +842,10 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                                    cz < 3 || cz >= P.nz - 4;
                             bool far = false;
                             if (P.lod && st == ST_ACTIVE) {
-                                const double wx = P.ox + ((double)g0x + (double)xi[0]) * P.dx - prp0;
-                                const double wy = P.oy + ((double)g0y + (double)xi[1]) * P.dx - prp1;
-                                const double wz = P.oz + ((double)g0z + (double)xi[2]) * P.dx - (prp2 + P.tool_tip_dz);
+                                const double wx = P.ox + ((double)g0x + ((double)xi[0] + (double)lo[0])) * P.dx - prp0;
+                                const double wy = P.oy + ((double)g0y + ((double)xi[1] + (double)lo[1])) * P.dx - prp1;
+                                const double wz =
+                                    P.oz + ((double)g0z + ((double)xi[2] + (double)lo[2])) * P.dx - (prp2 + P.tool_tip_dz);
                                 far = sqrt(wx * wx + wy * wy + wz * wz) > P.lod_r2;
                             }
                             bool skip = far || fixed || st == ST_CHIP;
@@ -889,9 +909,9 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                 const R mdx = m * (R)P.dx;
                                 R ef[3] = {0, 0, 0};
                                 if (sa.use_ext && P.ext_r > 0.0 && (st == ST_ACTIVE || st == ST_CHIP)) {
-                                    const double ex = P.ox + ((double)g0x + (double)xi[0]) * P.dx - P.ext_c[0];
-                                    const double ey = P.oy + ((double)g0y + (double)xi[1]) * P.dx - P.ext_c[1];
-                                    const double ez = P.oz + ((double)g0z + (double)xi[2]) * P.dx - P.ext_c[2];
+                                    const double ex = P.ox + ((double)g0x + ((double)xi[0] + (double)lo[0])) * P.dx - P.ext_c[0];
+                                    const double ey = P.oy + ((double)g0y + ((double)xi[1] + (double)lo[1])) * P.dx - P.ext_c[1];
+                                    const double ez = P.oz + ((double)g0z + ((double)xi[2] + (double)lo[2])) * P.dx - P.ext_c[2];
                                     const double dist = sqrt(ex * ex + ey * ey + ez * ez);
                                     if (dist < P.ext_r) {
                                         const double fw = (1.0 - dist / P.ext_r) * P.dt;
@@ -940,6 +960,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
 
                     // write back
                     if (dirtyA) {
+                        if (has_lo) ps.X[pi] = mk4<R>(lo[0], lo[1], lo[2], R(0));
                         ps.A[0][pi] = mk4<R>(xi[0], xi[1], xi[2], eps);
                         ps.A[1][pi] = mk4<R>(H[0], H[1], H[2], H[3]);
                         ps.A[2][pi] = mk4<R>(H[4], H[5], H[6], H[7]);

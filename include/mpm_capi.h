@@ -313,6 +313,10 @@ typedef struct mpm_server_config {
     int32_t use_graph;         /* replay the tick's step calls from captured CUDA graphs */
     int32_t backstress;        /* also reserve backstress state (requests with H_kin > 0) */
     int32_t _pad;
+    /* admission also stops at this many resident particles (0: the budget
+     * alone); fewer resident particles step faster, so requests finish
+     * sooner, at the same throughput once the GPU is full */
+    int64_t max_resident_particles;
 } mpm_server_config;
 
 typedef struct mpm_server_stats {

@@ -117,6 +117,17 @@ int main() {
     assert(nres == 3);
     s2.tick(&nres);
     assert(nres == 2);
+    // the resident-particle cap: 40 particles; a 60-particle request still runs when alone
+    FakeOps ops3;
+    Scheduler<FakeOps> s3(&ops3, pools, 50, 8, [&]() { now += 1.0; return now; }, 40);
+    s3.submit(req(60, 5), &id[0]);
+    s3.submit(req(10, 5), &id[1]);
+    s3.tick(&nres);
+    assert(nres == 1);          // 60 alone; 10 more would exceed the cap
+    s3.tick(&nres);
+    assert(nres == 1);          // the 60 left, the 10 came in
+    s3.poll(id[1], &r1);
+    assert(r1.state == MPM_REQ_DONE);
     std::printf("OK\n");
     return 0;
 }
