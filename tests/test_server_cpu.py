@@ -173,7 +173,8 @@ def test_server_structs_match_ctypes(tmp_path):
 
 def test_footprint_is_host_arithmetic():
     """mpm_server_footprint needs no device: bytes = particles x state bytes +
-    nodes x grid bytes + keys x 8 + bins x 40."""
+    nodes x grid bytes + keys x 8 + bins x 40 (FP32 state: 13 vectors of 16 B
+    per particle and buffer)."""
     from mpm_b200 import workpiece as W
     from mpm_b200.solver import make_request
     case = W.config1(cells=(16, 16, 16))
@@ -185,6 +186,6 @@ def test_footprint_is_host_arithmetic():
     nodes = p["nx"] * p["ny"] * p["nz"]
     bins = ((p["nx"] + 3) // 4) * ((p["ny"] + 3) // 4) * ((p["nz"] + 3) // 4)
     particles = 16 ** 3 * 8
-    per_particle = 2 * (12 * 16 + 4 + 1 + 12) + 36
+    per_particle = 2 * (13 * 16 + 4 + 1 + 12) + 36   # 12 state vectors + the position low parts
     want = particles * per_particle + nodes * 33 + (bins * 64 + 2) * 8 + bins * 40
     assert abs(b.value - want) <= 1
