@@ -691,12 +691,21 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
             for (int sidx = 0; sidx < StepCfg<R>::kPerThread; ++sidx) {
                 const int slot = tid + sidx * kNT;
                 const int pl = base + slot;
-                const int64_t pi = P.pbase + wk.start + pl;
-                uint8_t st = (pl < wk.count) ? ps.status[pi] : (uint8_t)ST_INACTIVE;
+                // every load of the particle is issued here, before any branch on its
+                // state: one memory round trip.  Slots past the bin's end read the
+                // bin's first particle (bins are never empty) and are discarded.
+                const bool valid = pl < wk.count;
+                const int64_t pi = P.pbase + wk.start + (valid ? pl : 0);
+                const uint8_t st_ld = ps.status[pi];
+                const V4<R> a0 = ps.A[0][pi], a1 = ps.A[1][pi], a2 = ps.A[2][pi], a3 = ps.A[3][pi];
+                const V4<R> xl = (G2P && ps.X) ? ps.X[pi] : mk4<R>(0, 0, 0, 0);
+                const V4<R> a4 = P2G ? ps.A[4][pi] : mk4<R>(0, 0, 0, 0);
+                const V4<R> a5 = P2G ? ps.A[5][pi] : mk4<R>(0, 0, 0, 0);
+                const V4<R> b0_ld = G2P ? mk4<R>(0, 0, 0, 0) : ps.B[0][pi];
+                uint8_t st = valid ? st_ld : (uint8_t)ST_INACTIVE;
                 if (st != ST_INACTIVE) {
                     const uint8_t st_in = st;
                     const bool fixed = (st == ST_FIXED);
-                    V4<R> a0 = ps.A[0][pi], a1 = ps.A[1][pi], a2 = ps.A[2][pi], a3 = ps.A[3][pi];
                     R xi[3] = {a0.x, a0.y, a0.z};
                     R eps = a0.w;
                     R H[9] = {a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w, a3.x};
@@ -704,10 +713,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                     // low parts of the position (FP32 state); the move is an exact two-sum
                     R lo[3] = {R(0), R(0), R(0)};
                     const bool has_lo = G2P && !fixed && ps.X != nullptr;
-                    if (has_lo) {
-                        const V4<R> xl = ps.X[pi];
-                        lo[0] = xl.x; lo[1] = xl.y; lo[2] = xl.z;
-                    }
+                    if (has_lo) { lo[0] = xl.x; lo[1] = xl.y; lo[2] = xl.z; }
                     R v[3] = {0, 0, 0}, Cm[9], edot = R(0);
                     bool have_C = false, dirtyA = false, wrote_C = false;
 
@@ -815,8 +821,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                         }
                     } else {
                         // P2G-only launch: velocity and strain rate come from memory
-                        const V4<R> b0 = ps.B[0][pi];
-                        v[0] = b0.x; v[1] = b0.y; v[2] = b0.z; edot = b0.w;
+                        v[0] = b0_ld.x; v[1] = b0_ld.y; v[2] = b0_ld.z; edot = b0_ld.w;
                     }
 
                     bool yielded = false;
@@ -853,7 +858,6 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                             R sig[6] = {0, 0, 0, 0, 0, 0};
                             R sl[3] = {0, 0, 0};
                             if (!skip && st == ST_ACTIVE) {
-                                const V4<R> a4 = ps.A[4][pi], a5 = ps.A[5][pi];
                                 R Hp[9] = {a4.x, a4.y, a4.z, a4.w, a5.x, a5.y, a5.z, a5.w, Hp8};
                                 R bsv[6];
                                 R* bsp = nullptr;
