@@ -83,6 +83,7 @@ template <typename R> struct alignas(128) Inst {
     R A, B, n, C, m, edot0, Hkin;
     R D1, D2, D3, D4c, D5, Dth;
     R Tspan;                       // max(Tm - Tamb, 1)
+    R ylo;                         // lower bound of the flow stress of an unheated particle (0: none)
     R dTmax;                       // Tm - Tamb (temperature cap as a rise)
     R heat;                        // beta / max(rho_phys cp, 1e-12)
     R apic;                        // apic_dinv_factor, applied as factor/dx
@@ -192,6 +193,20 @@ __device__ inline double tool_sdf(const I& P, double x, double z, double pr0, do
         }
     }
     return ds(core, P.tool_r);
+}
+
+// True when the point is certainly outside the tool (phi > 0), from a bound
+// that needs no square root: the cylinder's squared radius, or for the
+// convex core wedge the larger face-plane distance (a lower bound of the
+// distance to it).  The margin is far above the rounding of either path.
+template <typename I>
+__device__ __forceinline__ bool tool_far(const I& P, double x, double z, double pr0, double pr2) {
+    const double qx = ds(x, pr0), qz = ds(z, pr2);
+    const double m = P.tool_r + 1e-9 * (P.tool_r + fabs(qx) + fabs(qz));
+    if (P.tool_shape == 0) return da(dm(qx, qx), dm(qz, qz)) > m * m;
+    const double d1 = da(dm(P.tool_cg, qx), dm(P.tool_sg, qz));
+    const double d2 = da(dm(-P.tool_sa, qx), dm(-P.tool_ca, qz));
+    return fmax(d1, d2) > m;
 }
 
 // World coordinate of grid node index g on one axis: g*dx + origin, rounded

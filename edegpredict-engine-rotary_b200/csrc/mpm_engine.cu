@@ -589,6 +589,15 @@ class Engine final : public EngineBase {
         d.Hkin = (R)p.H_kin;
         d.D1 = (R)p.D1; d.D2 = (R)p.D2; d.D3 = (R)p.D3; d.D4c = (R)p.D4; d.D5 = (R)p.D5; d.Dth = (R)p.D_th;
         d.Tspan = (R)std::max(p.Tm - p.Tamb, 1.0);
+        // flow stress of an unheated particle: (A + B eps^n)(1 + C ln es)(1 - 0) with eps >= 0 and
+        // es >= 1e-5, so Y >= A (1 + C ln 1e-5) when A > 0, B >= 0, C >= 0 (with a margin far above
+        // the rounding of Y); 0 disables the bound
+        {
+            const double rt_lo = 1.0 + p.jc_C * std::log(1e-5);
+            d.ylo = (p.jc_A > 0.0 && p.jc_B >= 0.0 && p.jc_C >= 0.0 && rt_lo > 0.0)
+                        ? (R)(p.jc_A * rt_lo * (1.0 - 1e-4))
+                        : R(0);
+        }
         d.dTmax = (R)(p.Tm - p.Tamb);
         d.heat = (R)(p.beta / std::max(p.rho_phys * p.cp, 1e-12));
         d.apic = (R)p.apic_dinv_factor;

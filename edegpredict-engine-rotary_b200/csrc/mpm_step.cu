@@ -117,7 +117,8 @@ __device__ __forceinline__ NV<R> node_vel_inl(const Inst<R>& P, const V4<R> g, i
         if (P.tool_mask[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)]) {
             vx = (R)P.tool_v[0]; vy = (R)P.tool_v[1]; vz = (R)P.tool_v[2];
         }
-    } else if (P.tool_mode == TOOL_SDF_STICKY || P.tool_mode == TOOL_SDF_SLIP) {
+    } else if ((P.tool_mode == TOOL_SDF_STICKY || P.tool_mode == TOOL_SDF_SLIP) &&
+               !tool_far(P, node_coord(gx, P.dx, P.ox), node_coord(gz, P.dx, P.oz), pr0, pr2)) {
         double nrm[3];
         const double phi = tool_sdf(P, node_coord(gx, P.dx, P.ox), node_coord(gz, P.dx, P.oz), pr0, pr2, nrm);
         if (phi <= 0.0) {
@@ -412,14 +413,17 @@ __device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[
     const R q = sqrt(R(1.5) * (ex * ex + ey * ey + ez * ez + R(2) * (exy * exy + exz * exz + eyz * eyz)));
     R Ts = dT / P.Tspan;
     Ts = fmin(fmax(Ts, R(0)), R(1));
+#pragma unroll
+    for (int q2 = 0; q2 < 6; ++q2) sig[q2] = s[q2];
+    sl[0] = s[3]; sl[1] = s[4]; sl[2] = s[5];
+    // an unheated particle with q below the smallest flow stress the step can
+    // have (ylo) cannot yield: the flow stress itself is not needed
+    if (Ts == R(0) && q < P.ylo) return o;
     const R es = fmax(edot / P.edot0, R(1e-5));
     const R rt = R(1) + P.C * log(es);
     // pow(0, y) is +0 for y > 0: skipped for the common unheated, unyielded particle
     const R tt = R(1) - ((Ts > R(0) || !(P.m > R(0))) ? pow(Ts, P.m) : R(0));
     const R Y = (P.A + P.B * ((eps > R(0) || !(P.n > R(0))) ? pow(eps, P.n) : R(0))) * rt * tt;
-#pragma unroll
-    for (int q2 = 0; q2 < 6; ++q2) sig[q2] = s[q2];
-    sl[0] = s[3]; sl[1] = s[4]; sl[2] = s[5];
     if (q > Y && q > R(1e-12)) {
         R dE, Yr = Y;
         if (P.plast == 1) {
@@ -632,6 +636,9 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
     }
     if (tid == 0) Sm.fail = 0;
     if (tid < 2 * kCellsPerBin) (&Sm.cnt[0][0])[tid] = 0;
+    // per-cell node sums start at zero; the end-of-bin reduction clears what it reads
+    if (P2G)
+        for (int q = tid; q < 4 * kOff * kCellsPerBin; q += kNT) (&Sm.cacc[0][0][0])[q] = R(0);
     __syncthreads();
     int par = 0;  // parity of the staging pass (counts double-buffered across passes)
     int last_inst = -1;
@@ -677,9 +684,6 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                 const int t = tidx(lx, ly, lz);
                 Sm.vel[0][t] = nv.x; Sm.vel[1][t] = nv.y; Sm.vel[2][t] = nv.z;
             }
-        }
-        if (P2G) {
-            for (int q = tid; q < 4 * kOff * kCellsPerBin; q += kNT) (&Sm.cacc[0][0][0])[q] = R(0);
         }
         __syncthreads();
 
@@ -1005,10 +1009,15 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                         for (int cx = max(0, X - 2); cx <= min(kBin - 1, X); ++cx) {
                             const int cell = cx + kBin * (cy + kBin * cz);
                             const int o = (X - cx) + 3 * (Y - cy) + 9 * (Z - cz);
+                            // each (offset, cell) entry belongs to exactly one tile node
                             m += Sm.cacc[0][o][cell];
                             px += Sm.cacc[1][o][cell];
                             py += Sm.cacc[2][o][cell];
                             pz += Sm.cacc[3][o][cell];
+                            Sm.cacc[0][o][cell] = R(0);
+                            Sm.cacc[1][o][cell] = R(0);
+                            Sm.cacc[2][o][cell] = R(0);
+                            Sm.cacc[3][o][cell] = R(0);
                         }
                 if (m == R(0)) continue;
                 const int gx = g0x + X, gy = g0y + Y, gz = g0z + Z;
