@@ -20,17 +20,18 @@ max over ranks, value = total particle-updates / that time.
 --config batched: the config-3 sweep (M = 512 uneven workpieces, 300 steps) in
 one batch handle -- one persistent launch per step for all of them, launch shape
 autotuned, step calls replayed from a CUDA graph -- reported beside the same
-workpieces stepped one at a time through the plain handle (a 32-instance
-sample), as `plain_sequential` and `batched_over_plain`.
+workpieces stepped one at a time through the plain handle (all of them, 20
+steps each), as `plain_sequential` and `batched_over_plain`.
 
 --config serving: the serving loop under Poisson arrivals (200 requests/s for
 60 s, 16^3..96^3-cell requests at 8 ppc, 200-2000 steps, 150 GB budget):
 throughput, p50/p99/p99.9 latency of the requests completed in the window,
 offered/admitted/completed counts.
 
---config precision_study: config 4 (128x64x64 cells) for 1000 steps in FP32 and
-in FP64 from the same seeded state; relative errors of momentum, kinetic +
-internal energy, peak von Mises stress, max temperature and mean plastic strain.
+--config precision_study: config 4 (128x64x64 cells) for 1000 steps in FP64 and
+(--repeats times) in FP32 from the same seeded state; relative errors of
+momentum, kinetic + internal energy, peak von Mises stress, max temperature and
+mean plastic strain, per FP32 run, median and worst.
 
 --impl reference: the reference's own CUDA kernels (src/MPMSolver.cu, built from
 its sources into oracle/_ref/) on the same workload -- rank 0 only.
@@ -445,8 +446,7 @@ def run_batched(args):
     value = live_tot * args.steps / (ms_max / 1e3)
     out = None
     if rank == 0:
-        rng = np.random.default_rng(3)
-        sample = [cases[i] for i in rng.choice(len(cases), size=min(32, len(cases)), replace=False)]
+        sample = cases   # every workpiece of the batch, each alone
         plain = plain_sequential(sample, 20, stream)
         peak, peak_kind = load_peaks()
         ppc_mean = float(np.mean([c["box"]["ppc"] for c in cases]))
@@ -471,8 +471,8 @@ def run_batched(args):
                             else "fallback", "traffic": None,
                             "kernel": "k_step<float,G2P,P2G> (fused)", "kernel_launches_timed": int(k_n),
                             "kernel_ms_avg": k_ms / max(k_n, 1), "bytes_alg_per_update": b_alg},
-               "plain_sequential": dict(plain, sample=f"{len(sample)} of the same workpieces, one at a time through "
-                                                      "mpm_create/mpm_step, 20 timed steps each"),
+               "plain_sequential": dict(plain, sample=f"all {len(sample)} workpieces of the batch, one at a time "
+                                                      "through mpm_create/mpm_step, 20 timed steps each"),
                "batched_over_plain": value / plain["value"],
                "clocks": clocks}
     if dist:
@@ -485,57 +485,67 @@ def run_batched(args):
 def run_precision_study(args):
     """Config 4: the same workpiece stepped in FP32 (the product) and in FP64
     (the oracle run of the same kernels) from the same seeded state; relative
-    errors of the conservation and peak quantities after K steps."""
+    errors of the conservation and peak quantities after K steps.  FP32 runs
+    are not bitwise reproducible (the grid sums use atomics), and the fracture
+    zone under the tool edge can branch on a ~1e-7 difference, so the FP32 run
+    is repeated and every run is reported."""
     import torch
     rank, world, local, dist = dist_setup(args.gpus)
     from mpm_b200 import Solver, capi as A, workpiece as W
     case = W.config4()
     b = case["box"]
     cap = int(np.prod([b["c1"][i] - b["c0"][i] for i in range(3)]) * b["ppc"])
-    out = {}
-    times = {}
-    for name, prec in (("f32", A.PREC_F32), ("f64", A.PREC_F64)):
+
+    def run(prec):
         s = Solver(W.to_mpm_params(case, precision=prec), cap)
         n = _init(s, case, rank=rank)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         s.step(case["dt"], args.steps)
         m = s.metrics()
-        times[name] = time.perf_counter() - t0
-        out[name] = m
+        sec = time.perf_counter() - t0
         s.close()
-    a, r = out["f32"], out["f64"]
-    p32, p64 = np.array(a["momentum"]), np.array(r["momentum"])
-    pscale = max(np.linalg.norm(p64), r["mass"] * np.linalg.norm(case["tool"]["velocity"]) * 1e-3, 1e-300)
+        return n, m, sec
+
+    n, r, t64 = run(A.PREC_F64)
+    e64 = r["kinetic"] + r["internal_elastic"]
 
     def rel(x, y):
         return abs(x - y) / max(abs(y), 1e-300)
-    e32 = a["kinetic"] + a["internal_elastic"]
-    e64 = r["kinetic"] + r["internal_elastic"]
-    errs = {"momentum": float(np.linalg.norm(p32 - p64) / pscale),
-            "kinetic_plus_internal": rel(e32, e64),
-            "peak_von_mises": rel(a["max_von_mises"], r["max_von_mises"]),
-            "max_temperature_rise": rel(a["max_temperature"] - 293.0, r["max_temperature"] - 293.0)
-            if r["max_temperature"] > 293.0 else abs(a["max_temperature"] - r["max_temperature"]),
-            "mean_plastic_strain": rel(a["mean_plastic_strain"], r["mean_plastic_strain"])
-            if r["mean_plastic_strain"] > 0 else abs(a["mean_plastic_strain"])}
+
+    def errors(a):
+        p32, p64 = np.array(a["momentum"]), np.array(r["momentum"])
+        return {"momentum": float(np.linalg.norm(p32 - p64) / max(np.linalg.norm(p64), 1e-300)),
+                "kinetic_plus_internal": rel(a["kinetic"] + a["internal_elastic"], e64),
+                "peak_von_mises": rel(a["max_von_mises"], r["max_von_mises"]),
+                "max_temperature_rise": rel(a["max_temperature"] - a_tamb, r["max_temperature"] - a_tamb),
+                "mean_plastic_strain": rel(a["mean_plastic_strain"], r["mean_plastic_strain"]),
+                "n_chip": [a["n_chip"], r["n_chip"]], "n_yielded": [a["n_yielded"], r["n_yielded"]]}
+    a_tamb = case["params"]["Tamb"]
+    runs, t32 = [], []
+    for _ in range(max(1, args.repeats)):
+        _, a, sec = run(A.PREC_F32)
+        runs.append(errors(a))
+        t32.append(sec)
     if rank != 0:
         return None
-    return {"metric": "relative error FP32 vs FP64 after K steps", "value": max(errs["momentum"],
-                                                                              errs["kinetic_plus_internal"]),
-            "unit": "relative", "n_gpus": 1, "steps": args.steps, "warmup": 0, "ms_per_step": None,
-            "higher_is_better": False, "scaling": None, "vs_baseline": None, "dtype": "f32 vs f64",
-            "data": "synthetic",
+    worst = {k: max(x[k] for x in runs) for k in ("momentum", "kinetic_plus_internal", "peak_von_mises",
+                                                     "max_temperature_rise", "mean_plastic_strain")}
+    med = {k: float(np.median([x[k] for x in runs])) for k in worst}
+    within = sum(1 for x in runs if x["momentum"] <= 1e-4 and x["kinetic_plus_internal"] <= 1e-4)
+    return {"metric": "relative error FP32 vs FP64 after K steps (median of the FP32 runs)",
+            "value": max(med["momentum"], med["kinetic_plus_internal"]), "unit": "relative", "n_gpus": 1,
+            "steps": args.steps, "warmup": 0, "ms_per_step": None, "higher_is_better": False, "scaling": None,
+            "vs_baseline": None, "dtype": "f32 vs f64", "data": "synthetic",
             "config": {"workload": "precision study: 128x64x64 cells, dx 0.02 mm, 8 ppc, Ti-6Al-4V, rounded wedge "
-                                   "r_e 0.3 mm at 2.5 m/s, doc 0.05 mm; the Johnson-Cook return and the "
+                                   "r_e 0.3 mm at 2.5 m/s, doc 0.05 mm; the Johnson-Cook Newton solve and the "
                                    "conservation reductions are FP64 in both runs",
-                       "particles": int(n), "target": "momentum and kinetic+internal energy within 1e-4"},
-            "errors": errs,
-            "f32": {k: a[k] for k in ("mass", "momentum", "kinetic", "internal_elastic", "max_von_mises",
-                                      "max_temperature", "mean_plastic_strain", "n_chip", "n_inactive")},
+                       "particles": int(n), "fp32_runs": len(runs),
+                       "target": "momentum and kinetic+internal energy within 1e-4"},
+            "errors_median": med, "errors_worst": worst, "runs_within_1e-4": within, "runs": runs,
             "f64": {k: r[k] for k in ("mass", "momentum", "kinetic", "internal_elastic", "max_von_mises",
                                       "max_temperature", "mean_plastic_strain", "n_chip", "n_inactive")},
-            "wall_s": times}
+            "wall_s": {"f64": t64, "f32_each": t32}}
 
 
 # ----------------------------------------------------------------- serving arm
@@ -665,6 +675,7 @@ def main():
                                                            "precision_study"])
     ap.add_argument("--instances", type=int, default=512)
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--repeats", type=int, default=5, help="precision_study: FP32 runs")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: window in seconds")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
