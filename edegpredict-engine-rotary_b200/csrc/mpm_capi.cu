@@ -285,6 +285,15 @@ mpm_status mpm_autotune(mpm_handle* h, const double* dt, mpm_launch_config* chos
     return ret(h, h->eng->autotune(dt, chosen));
 }
 
+mpm_status mpm_selftest_bounded_wait(int64_t limit_ns, void* stream) {
+    if (limit_ns < 1000000 || limit_ns > 1000000000)
+        return fail(nullptr, MPM_INVALID_ARG, "limit_ns must be in [1e6, 1e9]");
+    std::string e;
+    const mpm_status s = mpmb::wait_selftest(limit_ns, (cudaStream_t)stream, &e);
+    lib_err() = e;
+    return s;
+}
+
 mpm_status mpm_profile_enable(mpm_handle* h, int32_t enable) {
     NEED_H(h);
     return ret(h, h->eng->profile_enable(enable != 0));

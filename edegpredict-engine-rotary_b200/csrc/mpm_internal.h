@@ -7,6 +7,7 @@
 
 #include <string>
 
+#include "../../include/mpm_capi.h"
 #include "mpm_device.cuh"
 
 namespace mpmb {
@@ -118,5 +119,9 @@ int64_t& launch_counter();
 
 // The calling thread's error string, returned by mpm_last_error(NULL).
 void set_lib_error(const std::string& m);
+
+// Runs a kernel whose bounded mbarrier wait (the one guarding the step
+// kernel's tile loads) must give up after limit_ns: MPM_TIMEOUT when it did.
+mpm_status wait_selftest(int64_t limit_ns, cudaStream_t st, std::string* err);
 
 }  // namespace mpmb

@@ -72,6 +72,43 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return true;
 }
 
+// Self-test of mbar_wait_bounded: one thread waits on an mbarrier that nothing
+// arrives at (no copy in flight), gives up after limit_ns, invalidates the
+// barrier and records the outcome (1: gave up, 0: completed).
+__global__ void k_wait_selftest(uint64_t limit_ns, int* out) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    const bool done = mbar_wait_bounded(&bar, 0, limit_ns);
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&bar)) : "memory");
+    *out = done ? 0 : 1;
+}
+
+mpm_status wait_selftest(int64_t limit_ns, cudaStream_t st, std::string* err) {
+    int* d = nullptr;
+    int h = -1;
+    cudaError_t e = cudaMalloc(&d, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(d, 0xff, sizeof(int), st);
+    if (e == cudaSuccess) {
+        k_wait_selftest<<<1, 32, 0, st>>>((uint64_t)limit_ns, d);
+        ++launch_counter();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (d) cudaFree(d);
+    if (e != cudaSuccess) {
+        *err = std::string("bounded-wait self-test: ") + cudaGetErrorString(e);
+        return MPM_CUDA_ERROR;
+    }
+    if (h != 1) {
+        *err = "bounded-wait self-test: the wait did not give up";
+        return MPM_CUDA_ERROR;
+    }
+    *err = "bounded-wait self-test: the device wait gave up after its limit (expected)";
+    return MPM_TIMEOUT;
+}
+
 template <typename R> __device__ __forceinline__ void vec_atomic_add(V4<R>* dst, R a, R b, R c, R d);
 template <> __device__ __forceinline__ void vec_atomic_add<float>(float4* dst, float a, float b, float c, float d) {
     atomicAdd(dst, make_float4(a, b, c, d));  // one 128-bit vector reduction (sm_90+)

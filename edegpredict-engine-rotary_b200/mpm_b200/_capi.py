@@ -164,6 +164,7 @@ def lib() -> C.CDLL:
             "mpm_get_launch_config": (_i32, [_vp, P(MpmLaunchConfig)]),
             "mpm_set_launch_config": (_i32, [_vp, P(MpmLaunchConfig)]),
             "mpm_autotune": (_i32, [_vp, P(_d), P(MpmLaunchConfig)]),
+            "mpm_selftest_bounded_wait": (_i32, [_i64, _vp]),
             "mpm_set_mass_scaling": (_i32, [_vp, _d]),
             "mpm_apply_external_force": (_i32, [_vp, P(_d), _d, P(_d)]),
             "mpm_set_temperatures": (_i32, [_vp, P(_d), _i64]),

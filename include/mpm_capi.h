@@ -339,6 +339,14 @@ mpm_status mpm_server_stats_get(mpm_server *s, mpm_server_stats *out);
 /* Device bytes a request holds while resident (host-only arithmetic). */
 mpm_status mpm_server_footprint(const mpm_server_config *cfg, const mpm_request *req, int64_t *bytes);
 
+/* Self-test of the bounded device-side wait that guards the step kernel's
+ * tile loads (no counterpart in the reference): a one-thread kernel waits on
+ * an mbarrier that nothing completes, gives up after limit_ns (1e6..1e9 ns)
+ * and records it.  Returns MPM_TIMEOUT when the wait gave up (the expected
+ * outcome; the context stays usable), MPM_CUDA_ERROR otherwise.  Synchronises
+ * the stream (NULL: legacy default stream). */
+mpm_status mpm_selftest_bounded_wait(int64_t limit_ns, void *stream);
+
 /* Record CUDA events around every launch of the step kernel (enable != 0),
  * for timing the dominant kernel inside a longer run.  mpm_profile_read
  * synchronises, returns the summed device time (ms) and count of the fused
