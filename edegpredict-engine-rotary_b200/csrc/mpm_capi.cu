@@ -82,6 +82,11 @@ mpm_status mpm_params_default(mpm_params* p) {
     p->schedule = MPM_SCHED_FUSED;
     p->sort_every = 16;
     p->threads_per_block = 128;
+    // ContactConfig defaults (include/ContactSolver.cuh:30-34); off until contact_every > 0
+    p->contact_every = 0;
+    p->contact_radius = 0.0002;
+    p->contact_friction = 0.3;
+    p->contact_heat_partition = 0.5;
     return MPM_OK;
 }
 

@@ -99,6 +99,10 @@ template <typename R> struct alignas(128) Inst {
     double tool_p0[3], tool_v[3], tool_t0;
     double tool_r, tool_rake, tool_clear, tool_tip_dz;
     double tool_sg, tool_cg, tool_sa, tool_ca;   // sin/cos of rake and clearance, computed on the host
+    // particle-side tool contact after every contact_every-th step (0: off)
+    int contact_every;
+    double contact_r, contact_mu, contact_hp;
+    double rho_phys, cp;           // physical density and specific heat (contact heating)
     // external force for one step (radius 0: none)
     double ext_c[3], ext_r, ext_f[3];
     int64_t pbase;                 // first particle slot of this instance in the batch arrays

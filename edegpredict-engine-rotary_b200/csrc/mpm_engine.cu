@@ -72,6 +72,10 @@ mpm_status check_params(const mpm_params* p, std::string* err) {
     if (p->schedule != MPM_SCHED_FUSED && p->schedule != MPM_SCHED_SPLIT) return bad("schedule");
     if (p->threads_per_block < 0 || p->threads_per_block > 256 || (p->threads_per_block % 32) != 0)
         return bad("threads_per_block must be 0 or a multiple of 32 up to 256");
+    if (p->contact_every < 0) return bad("contact_every must be >= 0");
+    if (p->contact_every > 0 && (!(p->contact_radius > 0.0) || !(p->contact_friction >= 0.0) ||
+                                 !(p->contact_heat_partition >= 0.0 && p->contact_heat_partition <= 1.0)))
+        return bad("contact needs radius > 0, friction >= 0 and 0 <= heat partition <= 1");
     return MPM_OK;
 }
 
@@ -105,6 +109,7 @@ class Engine final : public EngineBase {
     int max_work = 0;
     int* d_err = nullptr;
     unsigned long long* d_ctr = nullptr;
+    static constexpr size_t kCtrBytes = 4 * sizeof(unsigned long long) + 2 * sizeof(double);
     double *d_stat_part = nullptr, *d_stat_out = nullptr;
     int stat_blocks = 0;
     void* d_stage = nullptr;
@@ -198,8 +203,10 @@ class Engine final : public EngineBase {
         CK(cudaMemsetAsync(d_nwork, 0, sizeof(int), st));
         CK(cudaMalloc(&d_err, sizeof(int)));
         CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
-        CK(cudaMalloc(&d_ctr, 4 * sizeof(unsigned long long)));
-        CK(cudaMemsetAsync(d_ctr, 0, 4 * sizeof(unsigned long long), st));
+        // counters: [0] escaped updates, [1] yields, [2] contacts, [3] spare, then two FP64
+        // sums (contact friction work, contact normal force)
+        CK(cudaMalloc(&d_ctr, kCtrBytes));
+        CK(cudaMemsetAsync(d_ctr, 0, kCtrBytes, st));
         stat_blocks = 592;
         CK(cudaMalloc(&d_stat_part, sizeof(double) * kStatSlots * stat_blocks));
         CK(cudaMalloc(&d_stat_out, sizeof(double) * kStatSlots));
@@ -609,6 +616,12 @@ class Engine final : public EngineBase {
         d.lod = p.lod_enabled; d.plast = p.plasticity;
         d.lod_r1 = p.lod_active_r; d.lod_r2 = p.lod_near_r;
         d.chip_every = p.chip_every;
+        d.contact_every = p.contact_every > 0 ? p.contact_every : 0;
+        d.contact_r = p.contact_radius;
+        d.contact_mu = p.contact_friction;
+        d.contact_hp = p.contact_heat_partition;
+        d.rho_phys = p.rho_phys;
+        d.cp = p.cp;
         d.newton_maxit = p.newton_maxit > 0 ? p.newton_maxit : 60;
         d.newton_tol = p.newton_tol > 0 ? p.newton_tol : 1e-12;
         const mpm_tool_desc& t = x.tool;
@@ -1189,8 +1202,10 @@ class Engine final : public EngineBase {
                         stat_blocks, d_stat_out, st);
         double v[kStatSlots];
         unsigned long long ctr[4];
+        double fsum[2];
         CK(cudaMemcpyAsync(v, d_stat_out, sizeof(v), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(ctr, d_ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(fsum, d_ctr + 4, sizeof(fsum), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         std::memset(out, 0, sizeof(*out));
         out->mass = v[0];
@@ -1220,6 +1235,9 @@ class Engine final : public EngineBase {
         out->n_escaped = (int64_t)ctr[0];
         out->n_sorts = n_sorts;
         out->n_yielded = (int64_t)ctr[1];
+        out->n_contacts = (int64_t)ctr[2];
+        out->contact_work = fsum[0];
+        out->contact_force = fsum[1];
         return device_status();
     }
 

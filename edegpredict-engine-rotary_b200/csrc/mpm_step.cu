@@ -540,6 +540,60 @@ __device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[
     return o;
 }
 
+// ------------------------------------------------------------------ particle contact
+
+// Particle-side tool contact of one particle after its move, restating
+// xpbdContactSDFKernel (reference src/ContactSolver.cu:797-923) on the analytic
+// SDF with its exact normal: within contact_r of the surface the particle is
+// pushed out to contact_r, loses an approaching normal velocity, takes Coulomb
+// friction on the tangential velocity taken with the normal component before
+// that removal (:870-873), and is heated by (1 - heat partition) of the
+// friction work, T capped at Tm (:885-904).  The scalar chain is FP64.  The
+// push-out comes back as a displacement in cells (hit = false: no contact).
+struct ContactOut {
+    bool hit;
+    double dxi[3];
+    double work, force;
+};
+
+template <typename R>
+__device__ __noinline__ ContactOut particle_contact(const Inst<R>& P, double wx, double wz, double pe0, double pe2,
+                                                    R& vx, R& vy, R& vz, R& dT) {
+    ContactOut o{false, {0.0, 0.0, 0.0}, 0.0, 0.0};
+    double nrm[3];
+    const double sdf = tool_sdf(P, wx, wz, pe0, pe2, nrm);
+    if (!(sdf < P.contact_r)) return o;
+    const double pen = P.contact_r - sdf;
+    if (!(pen > 0.0)) return o;
+    o.hit = true;
+    const double idx = 1.0 / P.dx;
+    for (int a = 0; a < 3; ++a) o.dxi[a] = nrm[a] * pen * idx;
+    double v[3] = {(double)vx, (double)vy, (double)vz};
+    const double vdn = v[0] * nrm[0] + v[1] * nrm[1] + v[2] * nrm[2];
+    if (vdn < 0.0)
+        for (int a = 0; a < 3; ++a) v[a] -= vdn * nrm[a];
+    double tv[3];
+    for (int a = 0; a < 3; ++a) tv[a] = v[a] - vdn * nrm[a];
+    const double tvm = sqrt(tv[0] * tv[0] + tv[1] * tv[1] + tv[2] * tv[2]);
+    const double m = (double)P.pmass;
+    const double nf = tvm > 0.0 ? fmax(m * pen / (P.dt * P.dt), 1e-15) : 1e-15;
+    const double fimp = P.contact_mu * nf * P.dt;
+    if (tvm > 0.0 && fimp > 0.0) {
+        const double sc = fmin(1.0, (fimp / fmax(m, 1e-15)) / tvm);
+        for (int a = 0; a < 3; ++a) v[a] -= tv[a] * sc;
+    }
+    const double slip = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    o.work = nf * slip * P.dt;
+    o.force = nf;
+    const double heat = o.work * (1.0 - P.contact_hp);
+    if (heat > 0.0) {
+        const double pm = fmax(P.rho_phys, 1.0) * fmax((double)P.pvol, 1e-24);
+        dT = (R)fmin((double)dT + heat / (fmax(pm, 1e-15) * P.cp), (double)P.dTmax);
+    }
+    vx = (R)v[0]; vy = (R)v[1]; vz = (R)v[2];
+    return o;
+}
+
 // ------------------------------------------------------------------ the step kernel
 
 // Particles staged per pass and scatter payload per particle:
@@ -666,7 +720,8 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
     const int nw = *n_work;
     uint32_t phase = 0;
     int errf = 0;
-    unsigned long long c_esc = 0, c_yield = 0;
+    unsigned long long c_esc = 0, c_yield = 0, c_contact = 0;
+    double f_work = 0.0, f_force = 0.0;
     if (G2P && tid == 0) {
         mbar_init(&Sm.mbar, 1);
         fence_async_smem();
@@ -858,6 +913,34 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                 v[0] += rx * pm; v[1] += ry * pm; v[2] += rz * pm;
                                 Dm = P.Dth * R(0.5);
                                 dirtyA = true;
+                            }
+                        }
+                        // particle-side tool contact after the move, at the tool pose of the
+                        // step's end (every contact_every-th step)
+                        if (P.contact_every > 0 && !fixed && ((P.step0 + sa.k + 1) % P.contact_every) == 0) {
+                            const double te = da(P.t0, dm((double)(sa.k + 1), P.dt));
+                            const double pe0 = da(P.tool_p0[0], dm(P.tool_v[0], ds(te, P.tool_t0)));
+                            const double pe2 = da(P.tool_p0[2], dm(P.tool_v[2], ds(te, P.tool_t0)));
+                            const double wx = P.ox + ((double)g0x + ((double)xi[0] + (double)lo[0])) * P.dx;
+                            const double wz = P.oz + ((double)g0z + ((double)xi[2] + (double)lo[2])) * P.dx;
+                            const ContactOut co = particle_contact<R>(P, wx, wz, pe0, pe2, v[0], v[1], v[2], dT);
+                            if (co.hit) {
+#pragma unroll
+                                for (int a = 0; a < 3; ++a) {
+                                    if (has_lo) {
+                                        const R inc = (R)co.dxi[a] + lo[a];
+                                        const R s = xi[a] + inc;
+                                        const R bv = s - xi[a];
+                                        lo[a] = (xi[a] - (s - bv)) + (inc - bv);
+                                        xi[a] = s;
+                                    } else {
+                                        xi[a] = (R)((double)xi[a] + co.dxi[a]);
+                                    }
+                                }
+                                dirtyA = true;
+                                ++c_contact;
+                                f_work += co.work;
+                                f_force += co.force;
                             }
                         }
                     } else {
@@ -1069,11 +1152,20 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
     for (int o = 16; o > 0; o >>= 1) {
         c_esc += __shfl_down_sync(0xffffffffu, c_esc, o);
         c_yield += __shfl_down_sync(0xffffffffu, c_yield, o);
+        c_contact += __shfl_down_sync(0xffffffffu, c_contact, o);
+        f_work += __shfl_down_sync(0xffffffffu, f_work, o);
+        f_force += __shfl_down_sync(0xffffffffu, f_force, o);
         errf |= __shfl_down_sync(0xffffffffu, errf, o);
     }
     if (lane == 0) {
         if (c_esc) atomicAdd(&ctr[0], c_esc);
         if (c_yield) atomicAdd(&ctr[1], c_yield);
+        if (c_contact) {
+            // ctr[2] counts contacts; two FP64 sums follow the four counters
+            atomicAdd(&ctr[2], c_contact);
+            atomicAdd(reinterpret_cast<double*>(ctr + 4), f_work);
+            atomicAdd(reinterpret_cast<double*>(ctr + 4) + 1, f_force);
+        }
         if (errf) atomicOr(err, errf);
     }
 }

@@ -35,7 +35,8 @@ class MpmParams(C.Structure):
         ("apic_dinv_factor", _d), ("apic_decay", _d), ("deps_cap", _d), ("dT_cap", _d),
         ("lod_enabled", _i32), ("chip_every", _i32), ("lod_active_r", _d), ("lod_near_r", _d),
         ("newton_tol", _d), ("newton_maxit", _i32), ("schedule", _i32), ("sort_every", _i32),
-        ("threads_per_block", _i32),
+        ("threads_per_block", _i32), ("contact_every", _i32), ("_pad_contact", _i32), ("contact_radius", _d),
+        ("contact_friction", _d), ("contact_heat_partition", _d),
     ]
 
 
@@ -62,7 +63,7 @@ class MpmMetrics(C.Structure):
         ("max_temperature", _d), ("max_von_mises", _d), ("max_plastic_strain", _d), ("mean_plastic_strain", _d),
         ("n_active", _i64), ("n_chip", _i64), ("n_fixed", _i64), ("n_inactive", _i64),
         ("bounds_min", _d * 3), ("bounds_max", _d * 3), ("n_escaped", _i64), ("n_sorts", _i64),
-        ("n_yielded", _i64),
+        ("n_yielded", _i64), ("n_contacts", _i64), ("contact_work", _d), ("contact_force", _d),
     ]
 
     def as_dict(self) -> dict:

@@ -84,6 +84,16 @@ typedef struct mpm_params {
     int32_t schedule;          /* MPM_SCHED_FUSED (default) or MPM_SCHED_SPLIT */
     int32_t sort_every;        /* re-bin particles every n steps (0: default) */
     int32_t threads_per_block; /* CTA size of the step kernel (0: default 128) */
+    /* Particle-side tool contact, restating xpbdContactSDFKernel
+     * (src/ContactSolver.cu:797-923) on the analytic tool SDF, after the move
+     * of every contact_every-th step (0: off): particles within contact_radius
+     * of the tool surface are pushed out to it, lose an approaching normal
+     * velocity, take Coulomb friction and are heated by (1 - heat partition)
+     * of the friction work.  Reference defaults (ContactConfig,
+     * include/ContactSolver.cuh:30-34): 0.2 mm, 0.3, 0.5. */
+    int32_t contact_every;
+    int32_t _pad_contact;
+    double contact_radius, contact_friction, contact_heat_partition;
 } mpm_params;
 
 /* Fill p with the reference defaults (MPMKernelConfig / Config.h defaults,
@@ -143,6 +153,8 @@ typedef struct mpm_metrics {
     int64_t n_escaped;                     /* particle updates done off their bin tile */
     int64_t n_sorts;                       /* re-bins so far */
     int64_t n_yielded;                     /* particle updates that took a plastic return */
+    int64_t n_contacts;                    /* particle contact corrections */
+    double contact_work, contact_force;    /* friction work (J) and normal force (N) summed over them */
 } mpm_metrics;
 
 typedef struct mpm_handle mpm_handle;

@@ -532,6 +532,52 @@ static void chip_separation(const orc_params *p, orc_state *s, double tipZ) {
     }
 }
 
+/* xpbdContactSDFKernel, src/ContactSolver.cu:797-923, with the analytic tool
+ * SDF and its exact normal in place of the voxel texture and its central
+ * differences.  For every particle that is not INACTIVE or FIXED and lies
+ * within contact_radius of the tool surface: push it out to the radius along
+ * the normal; remove an approaching normal velocity; Coulomb friction on the
+ * tangential velocity taken with the normal component before that removal
+ * (:870-873); heat the particle with the friction work times
+ * (1 - heat partition), T capped at Tm (:885-904). */
+static void particle_contact(const orc_params *p, orc_state *s, const double pr[3], double dt) {
+    const double rc = p->contact_radius, mu = p->contact_friction, hp = p->contact_heat_partition;
+    for (int i = 0; i < s->n; ++i) {
+        if (s->status[i] == ORC_INACTIVE || s->status[i] == ORC_FIXED) continue;
+        double nrm[3];
+        const double sdf = tool_sdf_n(p, pr, s->x[i], s->y[i], s->z[i], nrm);
+        if (sdf >= rc) continue;
+        const double pen = rc - sdf;
+        if (pen <= 0.0) continue;
+        s->x[i] += nrm[0] * pen;
+        s->y[i] += nrm[1] * pen;
+        s->z[i] += nrm[2] * pen;
+        const double vdn = s->vx[i] * nrm[0] + s->vy[i] * nrm[1] + s->vz[i] * nrm[2];
+        if (vdn < 0.0) {
+            s->vx[i] -= vdn * nrm[0];
+            s->vy[i] -= vdn * nrm[1];
+            s->vz[i] -= vdn * nrm[2];
+        }
+        const double tvx = s->vx[i] - vdn * nrm[0], tvy = s->vy[i] - vdn * nrm[1], tvz = s->vz[i] - vdn * nrm[2];
+        const double tvm = sqrt(tvx * tvx + tvy * tvy + tvz * tvz);
+        const double m = s->mass[i];
+        const double nf = tvm > 0.0 ? fmax(m * pen / (dt * dt), 1e-15) : 1e-15;
+        const double fimp = mu * nf * dt;
+        if (tvm > 0.0 && fimp > 0.0) {
+            const double sc = fmin(1.0, (fimp / fmax(m, 1e-15)) / tvm);
+            s->vx[i] -= tvx * sc;
+            s->vy[i] -= tvy * sc;
+            s->vz[i] -= tvz * sc;
+        }
+        const double slip = sqrt(s->vx[i] * s->vx[i] + s->vy[i] * s->vy[i] + s->vz[i] * s->vz[i]);
+        const double heat = nf * slip * dt * (1.0 - hp);
+        if (heat > 0.0) {
+            const double pm = fmax(p->rho_phys, 1.0) * fmax(s->vol[i], 1e-24);
+            s->T[i] = fmin(s->T[i] + heat / (fmax(pm, 1e-15) * p->cp), p->Tm);
+        }
+    }
+}
+
 int orc_step(const orc_params *p, orc_state *s, const orc_tool_samples *tool, double *grid, double dt, int32_t nsteps,
              int64_t step0, double t0, int32_t nthreads) {
     int err = 0;
@@ -550,6 +596,12 @@ int orc_step(const orc_params *p, orc_state *s, const orc_tool_samples *tool, do
         if (s->extf) memset(s->extf, 0, sizeof(double) * 3 * (size_t)s->n);  /* :682-688 */
         const int64_t cnt = step0 + k;
         if (p->chip_sep_enabled && p->chip_every > 0 && (cnt % p->chip_every) == 0) chip_separation(p, s, tip[2]);
+        if (p->contact_every > 0 && ((cnt + 1) % p->contact_every) == 0) {
+            /* after the step, at the tool pose of its end time */
+            double pe[3];
+            for (int d = 0; d < 3; ++d) pe[d] = p->tool_p0[d] + p->tool_v[d] * (t + dt);
+            particle_contact(p, s, pe, dt);
+        }
     }
     return err;
 }

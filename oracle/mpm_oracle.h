@@ -74,7 +74,10 @@ typedef struct orc_params {
     double tool_tip_dz;     /* tool tip z relative to the reference point */
     double newton_tol;      /* relative residual for the Newton return */
     int32_t newton_maxit;
-    int32_t _pad1;
+    /* particle-side tool contact after every contact_every-th step (0: off),
+     * xpbdContactSDFKernel (src/ContactSolver.cu:797-923) on the analytic SDF */
+    int32_t contact_every;
+    double contact_radius, contact_friction, contact_heat_partition;
 } orc_params;
 
 /* Particle state, SoA, one entry per particle (matrices row-major [n][9],

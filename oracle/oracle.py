@@ -41,7 +41,7 @@ class OrcParams(C.Structure):
         ("deps_cap", _d), ("dT_cap", _d), ("chip_sep_enabled", _i32), ("chip_every", _i32),
         ("tool_mode", _i32), ("tool_shape", _i32), ("tool_p0", _d * 3), ("tool_v", _d * 3), ("tool_r", _d),
         ("tool_rake", _d), ("tool_clear", _d), ("tool_tip_dz", _d), ("newton_tol", _d), ("newton_maxit", _i32),
-        ("_pad1", _i32),
+        ("contact_every", _i32), ("contact_radius", _d), ("contact_friction", _d), ("contact_heat_partition", _d),
     ]
 
 
@@ -104,6 +104,10 @@ def orc_params(case: dict) -> OrcParams:
     o.tool_rake = t.get("rake", 0.0)
     o.tool_clear = t.get("clearance", 0.0)
     o.tool_tip_dz = t.get("tip_dz", 0.0)
+    o.contact_every = int(p.get("contact_every", 0))
+    o.contact_radius = float(p.get("contact_radius", 0.0))
+    o.contact_friction = float(p.get("contact_friction", 0.0))
+    o.contact_heat_partition = float(p.get("contact_heat_partition", 0.0))
     return o
 
 

@@ -1,0 +1,78 @@
+"""Particle-side tool contact (xpbdContactSDFKernel, src/ContactSolver.cu:797-923,
+restated on the analytic tool SDF): the oracle's contact pass, and the fused
+CUDA path against it.
+
+Tolerances: FP64 path vs oracle 1e-9 of each field's scale; FP32 path as the
+plain parity tests (positions 2e-4 cell, velocities 1e-3, other fields 2e-3).
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, str(Path(__file__).resolve().parent))
+from mpm_b200 import capi as A, workpiece as W  # noqa: E402
+
+
+def contact_case(shape="cylinder", every=1, radius_cells=1.5):
+    if shape == "cylinder":
+        case = W.config1(cells=(12, 8, 8), speed=20.0)
+        case["tool"]["velocity"] = (-20.0, 0.0, 0.0)   # into the material
+    else:
+        case = W.config2(cells=(24, 8, 12), speed=20.0, radius=6e-5, doc=4e-5)
+        case["tool"]["velocity"] = (-20.0, 0.0, 0.0)
+    p = case["params"]
+    p.update(contact_every=every, contact_radius=radius_cells * p["dx"], contact_friction=0.3,
+             contact_heat_partition=0.5)
+    st = W.full_state(W.generate_box(case), case)
+    return case, st
+
+
+def tool_sdf_np(case, x, z, t):
+    tool = case["tool"]
+    pr0 = tool["position"][0] + tool["velocity"][0] * t
+    pr2 = tool["position"][2] + tool["velocity"][2] * t
+    return W.tool_sdf(tool, x, z, pr0, pr2)
+
+
+@pytest.mark.parametrize("shape", ["cylinder", "wedge"])
+def test_oracle_contact_pushes_particles_out(oracle, shape):
+    case, st = contact_case(shape)
+    n = 3
+    out, rc = oracle.step(case, st, n)
+    assert rc == 0
+    live = (out["status"] != A.INACTIVE) & (out["status"] != A.FIXED)
+    sdf = tool_sdf_np(case, out["x"], out["z"], n * case["dt"])
+    r = case["params"]["contact_radius"]
+    # after the last step's contact pass every live particle is at least at the contact radius
+    assert sdf[live].min() >= r * (1 - 1e-9)
+    # the same run without contact leaves particles inside that radius
+    case0, st0 = contact_case(shape, every=0)
+    out0, _ = oracle.step(case0, st0, n)
+    sdf0 = tool_sdf_np(case0, out0["x"], out0["z"], n * case0["dt"])
+    assert (sdf0[live] < r).any()
+    # contact only heats
+    assert (out["temperature"] >= st["temperature"] - 1e-12).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", ["cylinder", "wedge"])
+def test_contact_matches_oracle(oracle, shape):
+    from test_gpu_parity import field_errors, run_ours
+    case, st = contact_case(shape)
+    n = 10
+    ref, rc = oracle.step(case, st, n)
+    assert rc == 0
+    out = run_ours(case, st, n, prec=A.PREC_F64)
+    assert out["metrics"]["n_contacts"] > 0 and out["metrics"]["contact_force"] > 0
+    assert (out["status"] == ref["status"]).all()
+    err = field_errors(out, ref, case)
+    assert max(err.values()) < 1e-9, err
+    out32 = run_ours(case, st, n, prec=A.PREC_F32)
+    e32 = field_errors(out32, ref, case)
+    tol = dict(x=2e-4, y=2e-4, z=2e-4, vx=1e-3, vy=1e-3, vz=1e-3)
+    bad = {k: v for k, v in e32.items() if v > tol.get(k, 2e-3)}
+    assert not bad, (bad, e32)
