@@ -212,6 +212,9 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     stream = torch.cuda.Stream(device=dev)
     p = W.to_mpm_params(case)
+    if args.contact_every > 0:
+        # particle-side tool contact fused into the step (reference ContactConfig defaults)
+        p.contact_every = int(args.contact_every)
     box = case["box"]
     cap = int(np.prod([box["c1"][i] - box["c0"][i] for i in range(3)]) * box["ppc"])
     s = Solver(p, cap, stream=stream.cuda_stream)
@@ -287,7 +290,8 @@ def run_ours(args):
                        "dx_m": case["params"]["dx"], "dt_s": dt, "ppc": box["ppc"],
                        "schedule": "fused G2P->P2G, one kernel per step", "parallelism": f"replicas{world}",
                        "l2": "working set >> L2 (no flush needed)", "yield_fraction": f_yield,
-                       "escaped_updates": int(m1["n_escaped"]), "rebins": int(m1["n_sorts"])},
+                       "escaped_updates": int(m1["n_escaped"]), "rebins": int(m1["n_sorts"]),
+                       "contact_every": int(args.contact_every), "contacts": int(m1["n_contacts"])},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
@@ -675,6 +679,8 @@ def main():
                                                            "precision_study"])
     ap.add_argument("--instances", type=int, default=512)
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--contact-every", type=int, default=0,
+                    help="plain configs: fuse the particle-side tool contact every n steps (0: off)")
     ap.add_argument("--repeats", type=int, default=5, help="precision_study: FP32 runs")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: window in seconds")

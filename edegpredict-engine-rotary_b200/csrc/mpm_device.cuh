@@ -204,9 +204,11 @@ __device__ inline double tool_sdf(const I& P, double x, double z, double pr0, do
 // convex core wedge the larger face-plane distance (a lower bound of the
 // distance to it).  The margin is far above the rounding of either path.
 template <typename I>
-__device__ __forceinline__ bool tool_far(const I& P, double x, double z, double pr0, double pr2) {
+__device__ __forceinline__ bool tool_far(const I& P, double x, double z, double pr0, double pr2, double extra = 0.0) {
+    // phi > extra for certain (extra = 0: outside the tool)
     const double qx = ds(x, pr0), qz = ds(z, pr2);
-    const double m = P.tool_r + 1e-9 * (P.tool_r + fabs(qx) + fabs(qz));
+    const double r = P.tool_r + extra;
+    const double m = r + 1e-9 * (r + fabs(qx) + fabs(qz));
     if (P.tool_shape == 0) return da(dm(qx, qx), dm(qz, qz)) > m * m;
     const double d1 = da(dm(P.tool_cg, qx), dm(P.tool_sg, qz));
     const double d2 = da(dm(-P.tool_sa, qx), dm(-P.tool_ca, qz));

@@ -560,6 +560,7 @@ template <typename R>
 __device__ __noinline__ ContactOut particle_contact(const Inst<R>& P, double wx, double wz, double pe0, double pe2,
                                                     R& vx, R& vy, R& vz, R& dT) {
     ContactOut o{false, {0.0, 0.0, 0.0}, 0.0, 0.0};
+    if (tool_far(P, wx, wz, pe0, pe2, P.contact_r)) return o;   // phi > contact radius: no contact
     double nrm[3];
     const double sdf = tool_sdf(P, wx, wz, pe0, pe2, nrm);
     if (!(sdf < P.contact_r)) return o;
