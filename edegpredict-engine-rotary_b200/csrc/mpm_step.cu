@@ -620,7 +620,7 @@ constexpr int kCellCap = 16;
 template <typename R> struct StepSmem {
     V4<R> raw[kTileNodes];                 // TMA destination (offset 0 of the 128-byte aligned block)
     R vel[3][kPlane];                      // node velocities after the grid update
-    R cacc[4][kOff][kCellsPerBin];         // per-cell sums of the 27 stencil nodes: m, p_x, p_y, p_z
+    R nacc[4][kPlane];                     // the bin's node sums m, p_x, p_y, p_z (tidx layout)
     R pay[kPay][StepCfg<R>::kChunk];       // scatter payload of the staged particles
     short slot[kCellsPerBin][kCellCap];    // staged particles of each base cell
     int cnt[2][kCellsPerBin];              // staged particles per cell (atomic ranks), by pass parity
@@ -665,8 +665,11 @@ __device__ __forceinline__ void channel_add(const R (&w)[3][3], const R (&dw)[3]
 
 // Accumulation of one cell's staged particles (thread pair per cell: h = 0
 // takes m and p_x, h = 1 takes p_y and p_z) in registers, then added to the
-// cell's private block of cacc.  Each cell block has exactly one writer per
-// channel, so no atomics are needed.  par: parity of the staging pass.
+// 27 nodes of the cell's stencil in the bin's node tile with shared-memory
+// atomics.  For one stencil offset the 32 cells of a warp (cz in {0,1} or
+// {2,3}) address 32 distinct nodes, and tidx's z stride of 68 (4 mod 32)
+// puts them in 32 distinct banks: the adds neither collide nor conflict.
+// par: parity of the staging pass.
 template <typename R>
 __device__ __forceinline__ void cell_accumulate(StepSmem<R>& Sm, int cell, int h, R pm, int par) {
     R a0[kOff], a1[kOff];
@@ -702,11 +705,17 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R>& Sm, int cell, int h
         }
     }
     if (n > 0) {
+        const int base = tidx(cell & (kBin - 1), (cell / kBin) & (kBin - 1), cell / (kBin * kBin));
 #pragma unroll
-        for (int o = 0; o < kOff; ++o) {
-            Sm.cacc[2 * h][o][cell] += a0[o];
-            Sm.cacc[2 * h + 1][o][cell] += a1[o];
-        }
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const int o = i + 3 * j + 9 * k, t = base + i + kSY * j + kSZ * k;
+                    atomicAdd(&Sm.nacc[2 * h][t], a0[o]);
+                    atomicAdd(&Sm.nacc[2 * h + 1][t], a1[o]);
+                }
     }
 }
 
@@ -729,9 +738,9 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
     }
     if (tid == 0) Sm.fail = 0;
     if (tid < 2 * kCellsPerBin) (&Sm.cnt[0][0])[tid] = 0;
-    // per-cell node sums start at zero; the end-of-bin reduction clears what it reads
+    // node sums start at zero; the end-of-bin flush clears what it reads
     if (P2G)
-        for (int q = tid; q < 4 * kOff * kCellsPerBin; q += kNT) (&Sm.cacc[0][0][0])[q] = R(0);
+        for (int q = tid; q < 4 * kPlane; q += kNT) (&Sm.nacc[0][0])[q] = R(0);
     __syncthreads();
     int par = 0;  // parity of the staging pass (counts double-buffered across passes)
     int last_inst = -1;
@@ -1121,25 +1130,12 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
         }
 
         if (P2G) {
-            // tile node = sum of the cell blocks whose stencils cover it
+            // flush the bin's node tile to the grid, clearing it for the next bin
             for (int nidx = tid; nidx < kTileNodes; nidx += kNT) {
                 const int X = nidx % kTile, Y = (nidx / kTile) % kTile, Z = nidx / (kTile * kTile);
-                R m = R(0), px = R(0), py = R(0), pz = R(0);
-                for (int cz = max(0, Z - 2); cz <= min(kBin - 1, Z); ++cz)
-                    for (int cy = max(0, Y - 2); cy <= min(kBin - 1, Y); ++cy)
-                        for (int cx = max(0, X - 2); cx <= min(kBin - 1, X); ++cx) {
-                            const int cell = cx + kBin * (cy + kBin * cz);
-                            const int o = (X - cx) + 3 * (Y - cy) + 9 * (Z - cz);
-                            // each (offset, cell) entry belongs to exactly one tile node
-                            m += Sm.cacc[0][o][cell];
-                            px += Sm.cacc[1][o][cell];
-                            py += Sm.cacc[2][o][cell];
-                            pz += Sm.cacc[3][o][cell];
-                            Sm.cacc[0][o][cell] = R(0);
-                            Sm.cacc[1][o][cell] = R(0);
-                            Sm.cacc[2][o][cell] = R(0);
-                            Sm.cacc[3][o][cell] = R(0);
-                        }
+                const int t = tidx(X, Y, Z);
+                const R m = Sm.nacc[0][t], px = Sm.nacc[1][t], py = Sm.nacc[2][t], pz = Sm.nacc[3][t];
+                Sm.nacc[0][t] = R(0); Sm.nacc[1][t] = R(0); Sm.nacc[2][t] = R(0); Sm.nacc[3][t] = R(0);
                 if (m == R(0)) continue;
                 const int gx = g0x + X, gy = g0y + Y, gz = g0z + Z;
                 if (gx >= P.nx || gy >= P.ny || gz >= P.nz) continue;
