@@ -600,8 +600,10 @@ __device__ __noinline__ ContactOut particle_contact(const Inst<R>& P, double wx,
 // Particles staged per pass and scatter payload per particle:
 //   [0..2] xi (bin-local, after the move)  [3..5] Q = m (v - dx C d) + f_ext dt
 //   [6..14] R = m dx C (row-major)         [15..23] S = -dt V J sigma / dx (row-major)
+// FP32 passes stage 2 x 128 particles (about 4 per cell at 8 per cell):
+// half the barriers and accumulation rounds of 128-particle passes
 #ifndef MPMB_CHUNK_F32
-#define MPMB_CHUNK_F32 1
+#define MPMB_CHUNK_F32 2
 #endif
 #ifndef MPMB_MIN_CTAS
 #define MPMB_MIN_CTAS 4
