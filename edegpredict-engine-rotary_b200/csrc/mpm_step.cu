@@ -620,10 +620,16 @@ constexpr int kOff = 27;  // stencil offsets, off = i + 3j + 9k
 constexpr int kCellCap = 16;
 
 template <typename R> struct StepSmem {
-    V4<R> raw[kTileNodes];                 // TMA destination (offset 0 of the 128-byte aligned block)
+    // The TMA tile is read only by the fill at the start of a bin and the payload
+    // only inside the bin's passes, with barriers between: one buffer holds both,
+    // which keeps four CTAs within the 164 KB shared-memory carveout (92 KB of L1
+    // left for the register spills).
+    union {
+        V4<R> raw[kTileNodes];             // TMA destination (offset 0 of the 128-byte aligned block)
+        R pay[kPay][StepCfg<R>::kChunk];   // scatter payload of the staged particles
+    };
     R vel[3][kPlane];                      // node velocities after the grid update
     R nacc[4][kPlane];                     // the bin's node sums m, p_x, p_y, p_z (tidx layout)
-    R pay[kPay][StepCfg<R>::kChunk];       // scatter payload of the staged particles
     short slot[kCellsPerBin][kCellCap];    // staged particles of each base cell
     int cnt[2][kCellsPerBin];              // staged particles per cell (atomic ranks), by pass parity
     uint64_t mbar;
