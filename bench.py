@@ -216,10 +216,17 @@ def run_ours(args):
         # particle-side tool contact fused into the step (reference ContactConfig defaults)
         p.contact_every = int(args.contact_every)
     box = case["box"]
+    T0 = box["T0"]
+    if args.asb:
+        # adiabatic shear band heating after the move (AdiabaticShearConfig defaults); the
+        # workpiece starts 1 K above ambient so that every particle is past the model's
+        # temperature guard and its strain-rate test decides
+        p.asb_enabled = 1
+        T0 = box["T0"] + 1.0
     cap = int(np.prod([box["c1"][i] - box["c0"][i] for i in range(3)]) * box["ppc"])
     s = Solver(p, cap, stream=stream.cuda_stream)
     n = s.init_box(box["c0"], box["c1"], box["ppc"], box["seed"] + rank, box["instance"], box["fixed_layers"],
-                   box["T0"], tool=case["tool"])
+                   T0, tool=case["tool"])
     m0 = s.metrics()
     n_live = n - m0["n_inactive"]
     dt = case["dt"]
@@ -291,7 +298,9 @@ def run_ours(args):
                        "schedule": "fused G2P->P2G, one kernel per step", "parallelism": f"replicas{world}",
                        "l2": "working set >> L2 (no flush needed)", "yield_fraction": f_yield,
                        "escaped_updates": int(m1["n_escaped"]), "rebins": int(m1["n_sorts"]),
-                       "contact_every": int(args.contact_every), "contacts": int(m1["n_contacts"])},
+                       "contact_every": int(args.contact_every), "contacts": int(m1["n_contacts"]),
+                       "adiabatic_shear": bool(args.asb), "asb_heated": int(m1["n_asb_heated"]),
+                       "initial_rise_K": float(T0 - box["T0"])},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
@@ -681,6 +690,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--contact-every", type=int, default=0,
                     help="plain configs: fuse the particle-side tool contact every n steps (0: off)")
+    ap.add_argument("--asb", action="store_true",
+                    help="plain configs: run the adiabatic shear band heating after every move")
     ap.add_argument("--repeats", type=int, default=5, help="precision_study: FP32 runs")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: window in seconds")

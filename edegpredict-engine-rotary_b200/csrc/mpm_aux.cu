@@ -297,6 +297,7 @@ __global__ void k_bin_scatter(PState<R> src, PState<R> dst, const Inst<R>* insts
     }
     dst.sres[d] = src.sres[pi];
     dst.status[d] = src.status[pi];
+    dst.asb[d] = src.asb[pi];
     dst.id[d] = src.id[pi];
     dst.orig[d] = src.orig[pi];
     dst.bin[d] = nbn;
@@ -395,6 +396,7 @@ __global__ void k_import(DevSoA in, int64_t n, double ox, double oy, double oz, 
     }
     ps.sres[d] = in.sres ? ld_user<R>(in.sres, e, i) : R(0);
     ps.status[d] = in.status ? (uint8_t)in.status[i] : (uint8_t)ST_ACTIVE;
+    ps.asb[d] = 0;
     ps.id[d] = in.id ? in.id[i] : (int32_t)i;
     ps.orig[d] = (int32_t)i;
     ps.bin[d] = 0;
@@ -457,6 +459,7 @@ __global__ void k_gen_write(Inst<R> P, int c0x, int c0y, int c0z, int wx, int wy
     }
     ps.sres[d] = R(0);
     ps.status[d] = (iz < fixed_layers) ? (uint8_t)ST_FIXED : (uint8_t)ST_ACTIVE;
+    ps.asb[d] = 0;
     ps.id[d] = (int32_t)i;
     ps.orig[d] = (int32_t)i;
     ps.bin[d] = 0;
@@ -581,7 +584,7 @@ __global__ void k_export_aos(const Inst<R>* inst, PState<R> ps, int64_t pbase, i
     q.cellHash = 0;
     q.lodZone = 0;
     q.lastUpdateStep = 0;
-    q.asbCounter = 0;
+    q.asbCounter = ps.asb[pi];
     out[ps.orig[pi]] = q;
 }
 
@@ -807,6 +810,7 @@ __global__ void k_relayout(PState<R> src, PState<R> dst, const RelayoutMap* __re
     }
     dst.sres[s] = src.sres[o];
     dst.status[s] = src.status[o];
+    dst.asb[s] = src.asb[o];
     dst.id[s] = src.id[o];
     if (src.X && dst.X) dst.X[s] = src.X[o];
     dst.orig[s] = src.orig[o];

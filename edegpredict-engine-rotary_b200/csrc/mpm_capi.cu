@@ -87,6 +87,12 @@ mpm_status mpm_params_default(mpm_params* p) {
     p->contact_radius = 0.0002;
     p->contact_friction = 0.3;
     p->contact_heat_partition = 0.5;
+    // AdiabaticShearConfig defaults (include/Types.h:90-94); off as in the reference
+    p->asb_enabled = 0;
+    p->asb_critical_rate = 1e4;
+    p->asb_taylor_quinney = 0.9;
+    p->asb_max_temp_ratio = 0.9;
+    p->asb_touch_rise = 0.5;
     return MPM_OK;
 }
 

@@ -61,6 +61,7 @@ template <typename R> struct PState {
     V4<R>* X;           // FP32 state: low parts of the bin-local position (x, y, z, 0); NULL for FP64
     R* sres;
     uint8_t* status;
+    uint8_t* asb;       // adiabatic shear counter (MPMParticle::asbCounter), 0..10
     int32_t* id;
     int32_t* bin;       // bin (block) index the particle is filed under, written by the re-bin
     int32_t* orig;      // position of the particle in upload order
@@ -103,6 +104,10 @@ template <typename R> struct alignas(128) Inst {
     int contact_every;
     double contact_r, contact_mu, contact_hp;
     double rho_phys, cp;           // physical density and specific heat (contact heating)
+    // adiabatic shear band heating after the move (asb_on = 0: off); temperatures as rises
+    // above Tamb: the heated-particle guard, the cap asb_max_temp_ratio * Tm - Tamb
+    int asb_on;
+    R asb_rise, asb_min_rate, asb_crit, asb_heat, asb_Tcap;
     // external force for one step (radius 0: none)
     double ext_c[3], ext_r, ext_f[3];
     int64_t pbase;                 // first particle slot of this instance in the batch arrays
@@ -132,6 +137,8 @@ struct StepArgs {
     int sigma_all;      // P2G: store stress for every ACTIVE particle (last P2G of a call)
     int use_ext;        // P2G: apply the one-step external force
     int p2g_step;       // step index of the P2G part
+    int asb;            // some instance runs the adiabatic shear model: G2P launches take the kernel
+                        // variant that has it (the others carry none of its code)
 };
 
 // ------------------------------------------------------------------ weights

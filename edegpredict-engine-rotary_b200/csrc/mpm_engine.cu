@@ -76,6 +76,10 @@ mpm_status check_params(const mpm_params* p, std::string* err) {
     if (p->contact_every > 0 && (!(p->contact_radius > 0.0) || !(p->contact_friction >= 0.0) ||
                                  !(p->contact_heat_partition >= 0.0 && p->contact_heat_partition <= 1.0)))
         return bad("contact needs radius > 0, friction >= 0 and 0 <= heat partition <= 1");
+    if (p->asb_enabled && (!(p->asb_critical_rate >= 0.0) || !(p->asb_taylor_quinney >= 0.0) ||
+                           !(p->asb_max_temp_ratio > 0.0) || !(p->asb_touch_rise >= 0.0)))
+        return bad("adiabatic shear model needs critical rate >= 0, Taylor-Quinney >= 0, max temperature ratio > 0 "
+                   "and touch rise >= 0");
     return MPM_OK;
 }
 
@@ -203,8 +207,8 @@ class Engine final : public EngineBase {
         CK(cudaMemsetAsync(d_nwork, 0, sizeof(int), st));
         CK(cudaMalloc(&d_err, sizeof(int)));
         CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
-        // counters: [0] escaped updates, [1] yields, [2] contacts, [3] spare, then two FP64
-        // sums (contact friction work, contact normal force)
+        // counters: [0] escaped updates, [1] yields, [2] contacts, [3] adiabatic shear heatings,
+        // then two FP64 sums (contact friction work, contact normal force)
         CK(cudaMalloc(&d_ctr, kCtrBytes));
         CK(cudaMemsetAsync(d_ctr, 0, kCtrBytes, st));
         stat_blocks = 592;
@@ -254,7 +258,7 @@ class Engine final : public EngineBase {
     static size_t pstate_bytes(int64_t cp, bool withK) {
         const size_t v4 = sizeof(V4<R>);
         return (12 + (kPosLo ? 1 : 0)) * al256(v4 * cp) + (withK ? 2 * al256(v4 * cp) : 0) + al256(sizeof(R) * cp) +
-               al256(cp) + 3 * al256(4 * cp);
+               2 * al256(cp) + 3 * al256(4 * cp);
     }
     static void carve(void* base, int64_t cp, bool withK, PState<R>& s) {
         char* q = (char*)base;
@@ -271,6 +275,7 @@ class Engine final : public EngineBase {
         s.X = kPosLo ? (V4<R>*)take(v4 * cp) : nullptr;
         s.sres = (R*)take(sizeof(R) * cp);
         s.status = (uint8_t*)take(cp);
+        s.asb = (uint8_t*)take(cp);
         s.id = (int32_t*)take(4 * cp);
         s.bin = (int32_t*)take(4 * cp);
         s.orig = (int32_t*)take(4 * cp);
@@ -622,6 +627,13 @@ class Engine final : public EngineBase {
         d.contact_hp = p.contact_heat_partition;
         d.rho_phys = p.rho_phys;
         d.cp = p.cp;
+        // applyAdiabaticHeatingKernel constants (src/AdiabaticShearModel.cu:131-176)
+        d.asb_on = p.asb_enabled ? 1 : 0;
+        d.asb_rise = (R)p.asb_touch_rise;
+        d.asb_min_rate = (R)std::max(p.asb_critical_rate * 0.5, 5000.0);
+        d.asb_crit = (R)p.asb_critical_rate;
+        d.asb_heat = (R)(p.asb_taylor_quinney / std::max(p.rho_phys * p.cp, 1e-12));
+        d.asb_Tcap = (R)(p.asb_max_temp_ratio * p.Tm - p.Tamb);
         d.newton_maxit = p.newton_maxit > 0 ? p.newton_maxit : 60;
         d.newton_tol = p.newton_tol > 0 ? p.newton_tol : 1e-12;
         const mpm_tool_desc& t = x.tool;
@@ -961,16 +973,18 @@ class Engine final : public EngineBase {
             return MPM_OK;
         };
         const int cps = ctas_per_sm;
+        int asb = 0;
+        for (const InstHost& x : I) asb |= x.p.asb_enabled ? 1 : 0;
         if (fused) {
             CK(cudaMemsetAsync(gpool[w], 0, gbytes, st));
-            StepArgs a{0, 0, N == 1 ? 1 : 0, ext ? 1 : 0, 0};
+            StepArgs a{0, 0, N == 1 ? 1 : 0, ext ? 1 : 0, 0, asb};
             launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], a, w, false, true, threads, cps, d_err, d_ctr,
                            st);
             for (int k = 0; k + 1 < N; ++k) {
                 if ((s = maybe_sort()) != MPM_OK) return s;
                 CK(cudaMemsetAsync(gpool[w ^ 1], 0, gbytes, st));
                 raster_all(k);
-                StepArgs b{k, 0, (k + 2 == N) ? 1 : 0, 0, k + 1};
+                StepArgs b{k, 0, (k + 2 == N) ? 1 : 0, 0, k + 1, asb};
                 prof_begin();
                 launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], b, w, true, true, threads, cps, d_err,
                                d_ctr, st);
@@ -979,7 +993,7 @@ class Engine final : public EngineBase {
                 ++since_sort;
             }
             raster_all(N - 1);
-            StepArgs c{N - 1, 1, 0, 0, N - 1};
+            StepArgs c{N - 1, 1, 0, 0, N - 1, asb};
             launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], c, w, true, false, threads, cps, d_err, d_ctr,
                            st);
             ++since_sort;
@@ -987,13 +1001,13 @@ class Engine final : public EngineBase {
             for (int k = 0; k < N; ++k) {
                 if ((s = maybe_sort()) != MPM_OK) return s;
                 CK(cudaMemsetAsync(gpool[w], 0, gbytes, st));
-                StepArgs a{k, 0, 1, (ext && k == 0) ? 1 : 0, k};
+                StepArgs a{k, 0, 1, (ext && k == 0) ? 1 : 0, k, asb};
                 prof_begin();
                 launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], a, w, false, true, threads, cps, d_err,
                                d_ctr, st);
                 prof_end();
                 raster_all(k);
-                StepArgs c{k, 1, 0, 0, k};
+                StepArgs c{k, 1, 0, 0, k, asb};
                 prof_begin();
                 launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], c, w, true, false, threads, cps, d_err,
                                d_ctr, st);
@@ -1238,6 +1252,7 @@ class Engine final : public EngineBase {
         out->n_contacts = (int64_t)ctr[2];
         out->contact_work = fsum[0];
         out->contact_force = fsum[1];
+        out->n_asb_heated = (int64_t)ctr[3];
         return device_status();
     }
 

@@ -54,11 +54,11 @@ struct PoolBytes {
 inline PoolBytes pool_bytes(int precision, bool backstress) {
     const double v4 = precision == MPM_PREC_F64 ? 32.0 : 16.0, r = precision == MPM_PREC_F64 ? 8.0 : 4.0;
     PoolBytes b;
-    // A0-A5, B0-B3, S0-S1 (+K0-K1), X (FP32 only), sres, status, id, bin,
-    // orig; two buffers; sort key, rank, new bin (int32) and the FP64
-    // position scratch
+    // A0-A5, B0-B3, S0-S1 (+K0-K1), X (FP32 only), sres, status, shear
+    // counter, id, bin, orig; two buffers; sort key, rank, new bin (int32) and
+    // the FP64 position scratch
     const double nv4 = 12.0 + (backstress ? 2.0 : 0.0) + (precision == MPM_PREC_F64 ? 0.0 : 1.0);
-    b.particle = 2.0 * (nv4 * v4 + r + 1.0 + 12.0) + 12.0 + 24.0;
+    b.particle = 2.0 * (nv4 * v4 + r + 2.0 + 12.0) + 12.0 + 24.0;
     b.node = 2.0 * v4 + 1.0;     // two grid buffers and the tool mask
     b.key = 8.0;                 // count and offset
     b.bin = 40.0;                // bin tables, flags and the work item

@@ -540,6 +540,46 @@ __device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[
     return o;
 }
 
+// ------------------------------------------------------------------ adiabatic shear heating
+
+// Heating of one ACTIVE particle that passed the temperature and strain-rate
+// guards of applyAdiabaticHeatingKernel (reference src/AdiabaticShearModel.cu:
+// 139-176), temperatures as rises above Tamb: base heating
+// beta sigma_vM edot dt / (rho cp) from the stored stress (xx, yy, zz, xy |
+// xz, yz); the counter c of consecutive heated steps (capped at 10) switches
+// on the localisation factor 1 + 1.5 (edot / rate_crit - 1) <= 2.5 from the
+// third step above the critical rate; the step is then capped at the base
+// heating (at most 100 K), so the factor never raises it, as in the
+// reference; T is capped at max_temp_ratio * Tm (which can lower it).
+template <typename R>
+__device__ __forceinline__ R asb_heat(const Inst<R>& P, const V4<R>& s0, const V4<R>& s1, R edot, R dT, uint8_t& c) {
+    const R d1 = s0.x - s0.y, d2 = s0.y - s0.z, d3 = s0.z - s0.x;
+    const R seq = sqrt(R(0.5) * (d1 * d1 + d2 * d2 + d3 * d3 + R(6) * (s0.w * s0.w + s1.x * s1.x + s1.y * s1.y)));
+    const R base = P.asb_heat * seq * edot * (R)P.dt;
+    R inc = base;
+    c = (uint8_t)min((int)c + 1, 10);
+    if (edot > P.asb_crit && c >= 3) inc *= fmin(R(1) + R(1.5) * (edot / fmax(P.asb_crit, R(1)) - R(1)), R(2.5));
+    const R cap = fmin(base, R(100));
+    if (cap > R(0) && inc > cap) inc = cap;
+    return fmin(dT + inc, P.asb_Tcap);
+}
+
+// The adiabatic shear heating of an ACTIVE particle pi past the temperature
+// and strain-rate guards of applyAdiabaticHeatingKernel (:114-136), after its
+// move: asb_heat on the stored stress and the particle's counter; returns the
+// new temperature rise.  Out of line: only heated particles call it.
+template <typename R>
+__device__ __noinline__ R asb_update(const Inst<R>& P, const PState<R>& ps, int64_t pi, R edot, R dT,
+                                     unsigned long long* ctr) {
+    uint8_t c = ps.asb[pi];
+    dT = asb_heat<R>(P, ps.S[0][pi], ps.S[1][pi], edot, dT, c);
+    ps.asb[pi] = c;
+    // one counter add per warp for the lanes heated here
+    const unsigned hm = __activemask();
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(hm) - 1)) atomicAdd(&ctr[3], (unsigned long long)__popc(hm));
+    return dT;
+}
+
 // ------------------------------------------------------------------ particle contact
 
 // Particle-side tool contact of one particle after its move, restating
@@ -727,7 +767,7 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R>& Sm, int cell, int h
     }
 }
 
-template <typename R, bool G2P, bool P2G>
+template <typename R, bool G2P, bool P2G, bool ASB>
 __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __restrict__ insts, const Work* __restrict__ work,
                                               const int* __restrict__ n_work, PState<R> ps, StepArgs sa, int rbuf,
                                               int* __restrict__ err, unsigned long long* __restrict__ ctr) {
@@ -906,6 +946,23 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                                               R(0.5) * s02 * s02 + R(0.5) * s12 * s12));
                             }
                         }
+                        // adiabatic shear band heating after the move and before chip separation
+                        // (AdiabaticShearModel::update after g2pKernel, src/MPMSolver.cu:1130-1132;
+                        // guards of src/AdiabaticShearModel.cu:114-136); the stress is the one the
+                        // constitutive update of this step stored
+                        if (ASB && P.asb_on) {
+                            if (st == ST_CHIP) {
+                                if (ps.asb[pi] != 0) ps.asb[pi] = 0;   // :114-117
+                            } else if (st == ST_ACTIVE && dT > P.asb_rise) {   // :119-123
+                                if (edot < P.asb_min_rate) {                    // :131-136: decay
+                                    const uint8_t c = ps.asb[pi];
+                                    if (c != 0) ps.asb[pi] = (uint8_t)(c - 1);
+                                } else {
+                                    dT = asb_update<R>(P, ps, pi, edot, dT, ctr);
+                                    dirtyA = true;
+                                }
+                            }
+                        }
                         // chip separation and fracture after the move (step counter parity)
                         if (chip_now) {
                             if (st == ST_ACTIVE) {
@@ -1023,7 +1080,10 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                     }
                                 }
                                 if (jo.to_chip) { st = ST_CHIP; skip = true; }
-                                if (sa.sigma_all || Dm > R(1e-6) || P.lod || near_kill) {
+                                // with the shear model on, the next step's heating reads the stress
+                                // of every particle that passes its temperature guard
+                                if (sa.sigma_all || Dm > R(1e-6) || P.lod || near_kill ||
+                                    (P.asb_on && dT > P.asb_rise)) {
                                     ps.S[0][pi] = mk4<R>(sig[0], sig[1], sig[2], sig[3]);
                                     ps.S[1][pi] = mk4<R>(sig[4], sig[5], R(0), R(0));
                                 }
@@ -1175,10 +1235,10 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
     }
 }
 
-template <typename R, bool G2P, bool P2G> static void set_smem_attr() {
+template <typename R, bool G2P, bool P2G, bool ASB> static void set_smem_attr() {
     static bool done = false;
     if (!done) {
-        cudaFuncSetAttribute(k_step<R, G2P, P2G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_step<R, G2P, P2G, ASB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)step_smem_bytes<R>());
         done = true;
     }
@@ -1200,15 +1260,21 @@ void launch_step(const Inst<R>* insts, const Work* work, const int* n_work, int 
     int grid = sms * (ctas_per_sm > 0 ? ctas_per_sm : 4);
     if (grid > max_work) grid = max_work;
     const size_t smem = step_smem_bytes<R>();
-    if (g2p && p2g) {
-        set_smem_attr<R, true, true>();
-        k_step<R, true, true><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+    if (g2p && p2g && a.asb) {
+        set_smem_attr<R, true, true, true>();
+        k_step<R, true, true, true><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+    } else if (g2p && p2g) {
+        set_smem_attr<R, true, true, false>();
+        k_step<R, true, true, false><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+    } else if (g2p && a.asb) {
+        set_smem_attr<R, true, false, true>();
+        k_step<R, true, false, true><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
     } else if (g2p) {
-        set_smem_attr<R, true, false>();
-        k_step<R, true, false><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+        set_smem_attr<R, true, false, false>();
+        k_step<R, true, false, false><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
     } else {
-        set_smem_attr<R, false, true>();
-        k_step<R, false, true><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+        set_smem_attr<R, false, true, false>();
+        k_step<R, false, true, false><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
     }
     ++launch_counter();
 }

@@ -37,6 +37,8 @@ class MpmParams(C.Structure):
         ("newton_tol", _d), ("newton_maxit", _i32), ("schedule", _i32), ("sort_every", _i32),
         ("threads_per_block", _i32), ("contact_every", _i32), ("_pad_contact", _i32), ("contact_radius", _d),
         ("contact_friction", _d), ("contact_heat_partition", _d),
+        ("asb_enabled", _i32), ("_pad_asb", _i32), ("asb_critical_rate", _d), ("asb_taylor_quinney", _d),
+        ("asb_max_temp_ratio", _d), ("asb_touch_rise", _d),
     ]
 
 
@@ -64,6 +66,7 @@ class MpmMetrics(C.Structure):
         ("n_active", _i64), ("n_chip", _i64), ("n_fixed", _i64), ("n_inactive", _i64),
         ("bounds_min", _d * 3), ("bounds_max", _d * 3), ("n_escaped", _i64), ("n_sorts", _i64),
         ("n_yielded", _i64), ("n_contacts", _i64), ("contact_work", _d), ("contact_force", _d),
+        ("n_asb_heated", _i64),
     ]
 
     def as_dict(self) -> dict:

@@ -94,6 +94,22 @@ typedef struct mpm_params {
     int32_t contact_every;
     int32_t _pad_contact;
     double contact_radius, contact_friction, contact_heat_partition;
+    /* Adiabatic shear band heating, restating AdiabaticShearModel::update
+     * (src/AdiabaticShearModel.cu:262-279: applyAdiabaticHeatingKernel,
+     * :104-177), after the move of every step and before chip separation, as
+     * MPMSolver::step runs it (src/MPMSolver.cu:1130-1132); asb_enabled = 0:
+     * off (the reference never enables it).  An ACTIVE particle heated more
+     * than asb_touch_rise above Tamb whose strain rate reaches
+     * max(asb_critical_rate / 2, 5000 /s) is heated by
+     * asb_taylor_quinney * sigma_vM * edot * dt / (rho_phys * cp) (at most
+     * 100 K), with T capped at asb_max_temp_ratio * Tm; a per-particle counter
+     * of consecutive such steps (0..10) drives the reference's localisation
+     * factor.  Reference defaults (AdiabaticShearConfig, include/Types.h:90-94):
+     * 1e4 /s, 0.9, 0.9; the reference's guard T <= 25.5 degC with its 25 degC
+     * ambient is a rise of 0.5. */
+    int32_t asb_enabled;
+    int32_t _pad_asb;
+    double asb_critical_rate, asb_taylor_quinney, asb_max_temp_ratio, asb_touch_rise;
 } mpm_params;
 
 /* Fill p with the reference defaults (MPMKernelConfig / Config.h defaults,
@@ -155,6 +171,7 @@ typedef struct mpm_metrics {
     int64_t n_yielded;                     /* particle updates that took a plastic return */
     int64_t n_contacts;                    /* particle contact corrections */
     double contact_work, contact_force;    /* friction work (J) and normal force (N) summed over them */
+    int64_t n_asb_heated;                  /* particle updates heated by the adiabatic shear model */
 } mpm_metrics;
 
 typedef struct mpm_handle mpm_handle;

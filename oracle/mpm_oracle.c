@@ -578,6 +578,48 @@ static void particle_contact(const orc_params *p, orc_state *s, const double pr[
     }
 }
 
+/* applyAdiabaticHeatingKernel, src/AdiabaticShearModel.cu:104-177, as
+ * AdiabaticShearModel::update runs it after g2pKernel (:262-279;
+ * src/MPMSolver.cu:1130-1132).  detectShearBandsKernel (:32-67) only marks
+ * the LOD zone ACTIVE, which lodClassifyKernel rewrites before anything reads
+ * it, so it has no effect to restate.  The reference's guard
+ * T <= 25.5 degC with its 25 degC ambient is T <= Tamb + asb_touch_rise. */
+static void asb_heating(const orc_params *p, orc_state *s, double dt) {
+    const double rhocp = fmax(p->rho_phys * p->cp, 1e-12);
+    const double min_rate = fmax(p->asb_critical_rate * 0.5, 5000.0);
+    const double Tcap = p->asb_max_temp_ratio * p->Tm;
+    for (int i = 0; i < s->n; ++i) {
+        if (s->status[i] == ORC_CHIP) {             /* :114-117 */
+            s->asb[i] = 0;
+            continue;
+        }
+        if (s->status[i] != ORC_ACTIVE) continue;
+        if (s->T[i] <= p->Tamb + p->asb_touch_rise) continue;   /* :123 */
+        const double edot = s->edot[i];
+        if (edot < min_rate) {                                  /* :131-136 */
+            s->asb[i] = s->asb[i] > 0 ? s->asb[i] - 1 : 0;
+            continue;
+        }
+        const double *sg = s->sig + 6 * (int64_t)i;             /* :139-143 von Mises */
+        const double s1 = sg[0] - sg[1], s2 = sg[1] - sg[2], s3 = sg[2] - sg[0];
+        const double seq = sqrt(0.5 * (s1 * s1 + s2 * s2 + s3 * s3 + 6.0 * (sg[3] * sg[3] + sg[4] * sg[4] + sg[5] * sg[5])));
+        double dT = (p->asb_taylor_quinney * seq * edot * dt) / rhocp;      /* :148-149 */
+        s->asb[i] = s->asb[i] + 1 < 10 ? s->asb[i] + 1 : 10;                /* :155 */
+        if (edot > p->asb_critical_rate && s->asb[i] >= 3) {                /* :157-164 */
+            const double ratio = edot / fmax(p->asb_critical_rate, 1.0);
+            dT *= fmin(1.0 + 1.5 * (ratio - 1.0), 2.5);
+        }
+        double maxDT = p->asb_taylor_quinney * seq * (edot * dt) / rhocp;   /* :169-172 */
+        maxDT = fmin(maxDT, 100.0);
+        if (maxDT > 0.0 && dT > maxDT) dT = maxDT;
+        s->T[i] = fmin(s->T[i] + dT, Tcap);                                /* :175-176 */
+    }
+}
+
+void orc_asb_heat(const orc_params *p, orc_state *s, double dt) {
+    if (s->asb) asb_heating(p, s, dt);
+}
+
 int orc_step(const orc_params *p, orc_state *s, const orc_tool_samples *tool, double *grid, double dt, int32_t nsteps,
              int64_t step0, double t0, int32_t nthreads) {
     int err = 0;
@@ -593,6 +635,7 @@ int orc_step(const orc_params *p, orc_state *s, const orc_tool_samples *tool, do
         err |= p2g(p, s, grid, nthreads);
         grid_update(p, grid, dt, tool, pr);
         g2p(p, s, grid, dt, nthreads);
+        if (p->asb_enabled && s->asb) asb_heating(p, s, dt);
         if (s->extf) memset(s->extf, 0, sizeof(double) * 3 * (size_t)s->n);  /* :682-688 */
         const int64_t cnt = step0 + k;
         if (p->chip_sep_enabled && p->chip_every > 0 && (cnt % p->chip_every) == 0) chip_separation(p, s, tip[2]);

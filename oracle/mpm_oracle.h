@@ -78,6 +78,11 @@ typedef struct orc_params {
      * xpbdContactSDFKernel (src/ContactSolver.cu:797-923) on the analytic SDF */
     int32_t contact_every;
     double contact_radius, contact_friction, contact_heat_partition;
+    /* adiabatic shear band heating after g2p (asb_enabled != 0), restating
+     * applyAdiabaticHeatingKernel (src/AdiabaticShearModel.cu:104-177); the
+     * heated-particle guard is T > Tamb + asb_touch_rise */
+    int32_t asb_enabled;
+    double asb_critical_rate, asb_taylor_quinney, asb_max_temp_ratio, asb_touch_rise;
 } orc_params;
 
 /* Particle state, SoA, one entry per particle (matrices row-major [n][9],
@@ -94,6 +99,7 @@ typedef struct orc_state {
     double *extf;            /* [n][3] or NULL: applied for one step, then zeroed */
     int32_t *status, *id;
     int32_t *lod;            /* [n] LOD zone, persists like MPMParticle::lodZone */
+    int32_t *asb;            /* [n] or NULL: adiabatic shear counter, MPMParticle::asbCounter */
 } orc_state;
 
 /* Rasterised tool samples: offsets from the tool reference point. */
@@ -111,6 +117,11 @@ typedef struct orc_metrics {
     int64_t n_active, n_chip, n_fixed, n_inactive;
     double bmin[3], bmax[3];
 } orc_metrics;
+
+/* One pass of the adiabatic shear heating (applyAdiabaticHeatingKernel) over
+ * the particles, as orc_step runs it after g2p when asb_enabled is set; needs
+ * s->asb. */
+void orc_asb_heat(const orc_params *p, orc_state *s, double dt);
 
 /* Size in doubles of the grid scratch that orc_step needs. */
 int64_t orc_grid_doubles(const orc_params *p);

@@ -42,13 +42,15 @@ class OrcParams(C.Structure):
         ("tool_mode", _i32), ("tool_shape", _i32), ("tool_p0", _d * 3), ("tool_v", _d * 3), ("tool_r", _d),
         ("tool_rake", _d), ("tool_clear", _d), ("tool_tip_dz", _d), ("newton_tol", _d), ("newton_maxit", _i32),
         ("contact_every", _i32), ("contact_radius", _d), ("contact_friction", _d), ("contact_heat_partition", _d),
+        ("asb_enabled", _i32), ("asb_critical_rate", _d), ("asb_taylor_quinney", _d), ("asb_max_temp_ratio", _d),
+        ("asb_touch_rise", _d),
     ]
 
 
 class OrcState(C.Structure):
     _fields_ = [("n", _i32), ("_pad", _i32)] + [
         (k, _vp) for k in ("x", "y", "z", "vx", "vy", "vz", "F", "Fp", "C", "sig", "bs", "eps", "edot", "T", "D",
-                           "sres", "mass", "vol", "extf", "status", "id", "lod")
+                           "sres", "mass", "vol", "extf", "status", "id", "lod", "asb")
     ]
 
 
@@ -108,6 +110,11 @@ def orc_params(case: dict) -> OrcParams:
     o.contact_radius = float(p.get("contact_radius", 0.0))
     o.contact_friction = float(p.get("contact_friction", 0.0))
     o.contact_heat_partition = float(p.get("contact_heat_partition", 0.0))
+    o.asb_enabled = int(p.get("asb_enabled", 0))
+    o.asb_critical_rate = float(p.get("asb_critical_rate", 1e4))
+    o.asb_taylor_quinney = float(p.get("asb_taylor_quinney", 0.9))
+    o.asb_max_temp_ratio = float(p.get("asb_max_temp_ratio", 0.9))
+    o.asb_touch_rise = float(p.get("asb_touch_rise", 0.5))
     return o
 
 
@@ -132,9 +139,12 @@ class _Bound:
         self.arrs["id"] = np.ascontiguousarray(state["id"], dtype=np.int32).copy()
         lod = state.get("lod")
         self.arrs["lod"] = np.zeros(n, np.int32) if lod is None else np.ascontiguousarray(lod, np.int32).copy()
+        asb = state.get("asb")
+        self.arrs["asb"] = np.zeros(n, np.int32) if asb is None else np.ascontiguousarray(asb, np.int32).copy()
         s.status = self.arrs["status"].ctypes.data
         s.id = self.arrs["id"].ctypes.data
         s.lod = self.arrs["lod"].ctypes.data
+        s.asb = self.arrs["asb"].ctypes.data
         if extf is not None:
             self.arrs["extf"] = np.ascontiguousarray(extf, np.float64).reshape(n, 3).copy()
             s.extf = self.arrs["extf"].ctypes.data
@@ -168,6 +178,8 @@ class Oracle:
         L.orc_philox_uniform4.argtypes = [C.c_uint32] * 6 + [C.POINTER(C.c_float)]
         L.orc_tool_sdf.restype = _d
         L.orc_tool_sdf.argtypes = [C.POINTER(OrcParams), C.POINTER(_d), _d, _d, _d]
+        L.orc_asb_heat.restype = None
+        L.orc_asb_heat.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcState), _d]
         self.L = L
 
     def step(self, case: dict, state: Dict[str, np.ndarray], nsteps: int, step0: int = 0, t0: float = 0.0,
@@ -179,6 +191,13 @@ class Oracle:
                              grid.ctypes.data_as(C.POINTER(_d)), float(dt if dt is not None else case["dt"]),
                              int(nsteps), int(step0), float(t0), int(nthreads))
         return b.result(), rc
+
+    def asb_heat(self, case: dict, state: Dict[str, np.ndarray], dt: float) -> Dict[str, np.ndarray]:
+        """One adiabatic shear heating pass (no grid step)."""
+        p = orc_params(case)
+        b = _Bound(case, state)
+        self.L.orc_asb_heat(C.byref(p), C.byref(b.state), float(dt))
+        return b.result()
 
     def metrics(self, case: dict, state: Dict[str, np.ndarray]) -> dict:
         p = orc_params(case)
@@ -213,6 +232,8 @@ class RefKern:
                               _d]
         L.ref_stats.restype = _i32
         L.ref_stats.argtypes = [C.POINTER(OrcState), C.POINTER(_d)]
+        L.ref_asb_heat.restype = _i32
+        L.ref_asb_heat.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcState), _d]
         L.ref_bench.restype = _i32
         L.ref_bench.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcState), C.POINTER(OrcTool), _d, _i32, _i32,
                                 C.POINTER(_d)]
@@ -229,6 +250,15 @@ class RefKern:
                             int(nsteps), int(step0), float(t0))
         if rc != 0:
             raise RuntimeError(f"reference run failed ({rc}): {self.L.ref_last_error().decode()}")
+        return b.result()
+
+    def asb_heat(self, case: dict, state: Dict[str, np.ndarray], dt: float) -> Dict[str, np.ndarray]:
+        """The reference's detectShearBands + applyAdiabaticHeating kernels once."""
+        p = orc_params(case)
+        b = _Bound(case, state)
+        rc = self.L.ref_asb_heat(C.byref(p), C.byref(b.state), float(dt))
+        if rc != 0:
+            raise RuntimeError(f"reference shear pass failed ({rc}): {self.L.ref_last_error().decode()}")
         return b.result()
 
     def stats(self, case: dict, state: Dict[str, np.ndarray]) -> np.ndarray:

@@ -10,8 +10,9 @@
 // includes the reference translation unit and launches its kernels directly,
 // in the order that MPMSolver::step captures them (src/MPMSolver.cu:1092-1164):
 //   lodClassify? -> resetGrid -> p2g -> updateGrid -> fixtureBC? ->
-//   (rasterizeTool -> applyGridCollision)? -> g2p -> bounds -> resetExtForce,
-//   then chipFractureAndSeparation on even steps.
+//   (rasterizeTool -> applyGridCollision)? -> g2p -> (detectShearBands ->
+//   applyAdiabaticHeating)? -> bounds -> resetExtForce, then
+//   chipFractureAndSeparation on even steps.
 #include "src/MPMSolver.cu"
 
 #include <cstdint>
@@ -48,7 +49,29 @@ int check_reference_constants(const orc_params* p) {
         snprintf(g_err, sizeof(g_err), "parameters outside what the reference kernels implement");
         return -2;
     }
+    // applyAdiabaticHeatingKernel compares the absolute temperature with 25.5
+    // (src/AdiabaticShearModel.cu:123)
+    if (p->asb_enabled && p->Tamb + p->asb_touch_rise != 25.5) {
+        snprintf(g_err, sizeof(g_err), "the reference's shear model needs Tamb + touch rise = 25.5");
+        return -2;
+    }
     return 0;
+}
+
+// AdiabaticShearModel::initialize (src/AdiabaticShearModel.cu:229-241) with
+// the solver's material.
+ShearBandParams make_shear_params(const orc_params* p) {
+    ShearBandParams b;
+    b.criticalStrainRate = p->asb_critical_rate;
+    b.softeningThreshold = 0.95;
+    b.taylorQuinney = p->asb_taylor_quinney;
+    b.thermalDiffusivity = 2.9e-6;
+    b.bandWidth = 20e-6;
+    b.maxTempRatio = p->asb_max_temp_ratio;
+    b.meltingTemp = p->Tm;
+    b.specificHeat = p->cp;
+    b.density = p->rho_phys;
+    return b;
 }
 
 MPMKernelConfig make_config(const orc_params* p) {
@@ -92,6 +115,7 @@ void soa_to_aos(const orc_state* s, std::vector<MPMParticle>& a) {
         q.id = s->id[i];
         q.status = static_cast<ParticleStatus>(s->status[i]);
         q.lodZone = static_cast<LODZone>(s->lod ? s->lod[i] : 0);
+        q.asbCounter = static_cast<uint8_t>(s->asb ? s->asb[i] : 0);
     }
 }
 
@@ -112,6 +136,7 @@ void aos_to_soa(const std::vector<MPMParticle>& a, orc_state* s) {
         s->eps[i] = q.plasticStrain; s->edot[i] = q.strainRate; s->D[i] = q.damage; s->sres[i] = q.residualStress;
         s->status[i] = static_cast<int32_t>(q.status);
         if (s->lod) s->lod[i] = static_cast<int32_t>(q.lodZone);
+        if (s->asb) s->asb[i] = static_cast<int32_t>(q.asbCounter);
     }
 }
 
@@ -160,6 +185,12 @@ void launch_step(RefRun& r, const orc_params* p, const MPMKernelConfig& cfg, dou
         applyGridCollisionKernel<<<gb, T, 0, r.st>>>(r.d_g, (int)r.nn, dt);
     }
     g2pKernel<<<pb, T, 0, r.st>>>(r.d_p, r.n, r.d_g, dims, cfg, dt, dmin);
+    if (p->asb_enabled) {
+        // AdiabaticShearModel::update (src/AdiabaticShearModel.cu:262-279)
+        const ShearBandParams sb = make_shear_params(p);
+        detectShearBandsKernel<<<pb, T, 0, r.st>>>(r.d_p, r.n, sb);
+        applyAdiabaticHeatingKernel<<<pb, T, 0, r.st>>>(r.d_p, r.n, sb, dt);
+    }
     cudaMemcpyAsync(r.d_bmin, hBmin, 3 * sizeof(double), cudaMemcpyHostToDevice, r.st);
     cudaMemcpyAsync(r.d_bmax, hBmax, 3 * sizeof(double), cudaMemcpyHostToDevice, r.st);
     updateParticleBoundsKernel<<<pb, T, 0, r.st>>>(r.d_p, r.n, r.d_bmin, r.d_bmin + 1, r.d_bmin + 2, r.d_bmax,
@@ -268,6 +299,32 @@ int ref_run(const orc_params* p, orc_state* s, const orc_tool_samples* tool, dou
 // Reference-compatible stats through the reference's own kernel
 // (computeParticleStatsKernel, src/MPMSolver.cu:729-788): out = {max stress,
 // max T, kinetic, "internal"}.
+// AdiabaticShearModel::update (src/AdiabaticShearModel.cu:262-279) once over
+// the particles of s, with the solver material of p.
+int ref_asb_heat(const orc_params* p, orc_state* s, double dt) {
+    std::vector<MPMParticle> a;
+    soa_to_aos(s, a);
+    const int n = s->n;
+    MPMParticle* d = nullptr;
+    HCHECK(cudaMalloc(&d, sizeof(MPMParticle) * (size_t)(n > 0 ? n : 1)));
+    cudaError_t e = cudaMemcpy(d, a.data(), sizeof(MPMParticle) * (size_t)n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && n > 0) {
+        const ShearBandParams sb = make_shear_params(p);
+        const int pb = (n + 255) / 256;
+        detectShearBandsKernel<<<pb, 256>>>(d, n, sb);
+        applyAdiabaticHeatingKernel<<<pb, 256>>>(d, n, sb, dt);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(a.data(), d, sizeof(MPMParticle) * (size_t)n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) {
+        snprintf(g_err, sizeof(g_err), "ref_asb_heat: %s", cudaGetErrorString(e));
+        return -1;
+    }
+    aos_to_soa(a, s);
+    return 0;
+}
+
 int ref_stats(orc_state* s, double out[4]) {
     std::vector<MPMParticle> h;
     soa_to_aos(s, h);

@@ -1,13 +1,19 @@
 """Generates tests/golden/*.npz from the REFERENCE's own CUDA kernels.
 
-    python tests/golden/make_golden.py [outdir]
+    python tests/golden/make_golden.py [outdir] [scenario ...]
 
 Needs a GPU and oracle/_ref/libmpm_ref.so (the reference's src/MPMSolver.cu
-built from its sources by oracle/Makefile).  For every scenario of
-scenarios.py it stores the input state, the reference's state after n steps,
-and the reference's own stats kernel (computeParticleStatsKernel) on it.
-The reference kernels accumulate with FP64 atomics, so two runs differ in
-the last bits; the run-to-run spread of the reference is stored too.
+and src/AdiabaticShearModel.cu built from their sources by oracle/Makefile).
+For every scenario of scenarios.py (or the ones named) it stores the input
+state, the reference's state after n steps, and the reference's own stats
+kernel (computeParticleStatsKernel) on it.  The reference kernels accumulate
+with FP64 atomics, so two runs differ in the last bits; the run-to-run spread
+of the reference is stored too.
+
+kernels/asb_heating.npz holds one pass of the reference's adiabatic shear
+kernels (detectShearBandsKernel + applyAdiabaticHeatingKernel) over crafted
+particles that reach every branch (asb_pass_inputs); it is written when no
+scenario is named or when "asb_pass" is.
 """
 from __future__ import annotations
 
@@ -26,15 +32,67 @@ from oracle.oracle import RefKern  # noqa: E402
 from scenarios import SCENARIOS  # noqa: E402
 
 FIELDS = ("x", "y", "z", "vx", "vy", "vz", "F", "Fp", "C", "stress", "backstress", "plastic_strain", "strain_rate",
-          "temperature", "damage", "residual_stress", "status", "id")
+          "temperature", "damage", "residual_stress", "status", "id", "asb")
+
+ASB_DT = 1e-8
 
 
-def main(outdir: Path) -> None:
+def asb_pass_inputs():
+    """Crafted particles for one adiabatic shear pass: every status, the
+    temperature guard (below, exactly at and above 25.5 degC), strain rates
+    below, at and above the 5000 /s floor and the 1e4 /s critical rate,
+    counters 0..10, temperatures near and above the 0.9 Tm cap, stresses up to
+    2 GPa."""
+    case = {"params": dict(nx=8, ny=8, nz=8, dx=1e-4, origin=(0.0, 0.0, 0.0), E=113.8e9, nu=0.34,
+                           rho_phys=4430.0, cp=526.3, beta=0.9, Tm=1660.0, Tamb=25.0, jc_A=1e9, jc_B=1e9,
+                           jc_n=0.3, jc_C=0.01, jc_m=1.0, edot0=1.0, H_kin=0.0, D1=0.05, D2=3.44, D3=-2.12,
+                           D4=0.002, D5=0.61, D_th=1.0, fixture_thickness=0.0, fixture_damping=1e7,
+                           gravity_z=-9.81, mass_threshold=1e-12, apic_dinv_factor=3.0, apic_decay=0.99,
+                           lod_enabled=0, lod_active_r=0.0, lod_near_r=0.0, deps_cap=0.05, dT_cap=50.0,
+                           newton_tol=1e-12, plasticity=0, chip_every=2, newton_maxit=60, particle_mass=1e-9,
+                           particle_volume=1e-13, asb_enabled=1, asb_critical_rate=1e4, asb_taylor_quinney=0.9,
+                           asb_max_temp_ratio=0.9, asb_touch_rise=0.5),
+            "tool": {"mode": 0}}
+    rng = np.random.default_rng(23)
+    n = 4096
+    z = np.zeros(n)
+    eye = np.tile(np.eye(3).reshape(1, 9), (n, 1))
+    status = rng.choice([0, 0, 0, 0, 0, 0, 1, 2, 3, 4], n).astype(np.int32)
+    T = rng.choice([24.0, 25.0, 25.5, 25.5000001, 30.0, 300.0, 1000.0, 1493.9, 1500.0], n) + \
+        np.where(rng.uniform(0, 1, n) < 0.5, rng.uniform(0, 5, n), 0.0)
+    edot = rng.choice([0.0, 4999.0, 5000.0, 7000.0, 1e4, 1.00001e4, 2e4, 5e4, 1e6], n) * \
+        np.where(rng.uniform(0, 1, n) < 0.3, rng.uniform(0.9, 1.1, n), 1.0)
+    st = dict(x=z.copy(), y=z.copy(), z=z.copy(), vx=z.copy(), vy=z.copy(), vz=z.copy(), F=eye.copy(),
+              Fp=eye.copy(), C=np.zeros((n, 9)), stress=rng.uniform(-2e9, 2e9, (n, 6)) *
+              rng.choice([0.0, 1e-3, 1.0], (n, 1)), backstress=np.zeros((n, 6)), plastic_strain=z.copy(),
+              strain_rate=edot, temperature=T, damage=z.copy(), residual_stress=z.copy(), status=status,
+              id=np.arange(n, dtype=np.int32), asb=rng.integers(0, 11, n).astype(np.int32))
+    return case, st
+
+
+def write_asb_pass(rk, outdir: Path) -> None:
+    case, st = asb_pass_inputs()
+    out = rk.asb_heat(case, st, ASB_DT)
+    d = outdir / "kernels"
+    d.mkdir(parents=True, exist_ok=True)
+    np.savez_compressed(d / "asb_heating.npz", in_status=st["status"], in_temperature=st["temperature"],
+                        in_strain_rate=st["strain_rate"], in_stress=st["stress"], in_asb=st["asb"],
+                        out_temperature=out["temperature"], out_asb=out["asb"], dt=np.array(ASB_DT))
+    moved = int((out["temperature"] != st["temperature"]).sum())
+    print(f"asb_pass: n={len(st['status'])} heated={moved} counters changed={int((out['asb'] != st['asb']).sum())}")
+
+
+def main(outdir: Path, names=None) -> None:
     rk = RefKern()
     outdir.mkdir(parents=True, exist_ok=True)
+    if not names or "asb_pass" in names:
+        write_asb_pass(rk, outdir)
     for name, fn in SCENARIOS.items():
+        if names and name not in names:
+            continue
         case, st, n, extf = fn()
         st["lod"] = np.zeros(len(st["x"]), np.int32)
+        st.setdefault("asb", np.zeros(len(st["x"]), np.int32))
         out1 = rk.step(case, st, n, extf=extf)
         out2 = rk.step(case, st, n, extf=extf)
         spread = {k: float(np.abs(out1[k].astype(float) - out2[k].astype(float)).max()) for k in FIELDS if k in out1}
@@ -55,4 +113,4 @@ def main(outdir: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else HERE)
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else HERE, sys.argv[2:])

@@ -100,9 +100,31 @@ def lod_kinematic_extf():
     return case, st, 10, extf
 
 
+def adiabatic_shear():
+    """The adiabatic shear model on (AdiabaticShearModel::update after g2p):
+    the plastic_damage_chip tool path in degC with the reference's 25 degC
+    ambient and 0.5 degC touch guard.  Initial temperatures straddle the guard
+    (some exactly at 25.5) and a few lie near the 0.9 Tm cap, so that heating,
+    the counter ramp and localisation, the decay, the cap and the CHIP reset
+    all occur.  Counters start at 0."""
+    case, st, n, _ = plastic_damage_chip()
+    p = case["params"]
+    p.update(Tamb=25.0, Tm=1660.0, asb_enabled=1, asb_critical_rate=1e4, asb_taylor_quinney=0.9,
+             asb_max_temp_ratio=0.9, asb_touch_rise=0.5)
+    rng = np.random.default_rng(11)
+    nn = len(st["x"])
+    pick = rng.uniform(0, 1, nn)
+    T = np.where(pick < 0.3, 25.0, np.where(pick < 0.4, 25.5, 25.0 + rng.uniform(0.5, 400.0, nn)))
+    T = np.where(pick > 0.98, rng.uniform(1480.0, 1500.0, nn), T)
+    st["temperature"] = T
+    st["asb"] = np.zeros(nn, np.int32)
+    return case, st, n, None
+
+
 SCENARIOS = {
     "elastic_raster": elastic_raster,
     "plastic_damage_chip": plastic_damage_chip,
     "boundary_mix": boundary_mix,
     "lod_kinematic_extf": lod_kinematic_extf,
+    "adiabatic_shear": adiabatic_shear,
 }

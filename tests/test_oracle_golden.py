@@ -30,6 +30,8 @@ def load(path):
     case["params"]["origin"] = tuple(case["params"]["origin"])
     st = {k: d[f"in_{k}"] for k in FIELDS + ("status", "id")}
     ref = {k: d[f"out_{k}"] for k in FIELDS + ("status", "id")}
+    if "in_asb" in d:   # adiabatic shear counters (MPMParticle::asbCounter)
+        st["asb"], ref["asb"] = d["in_asb"], d["out_asb"]
     extf = d["extf"] if "extf" in d else None
     return case, st, ref, meta, extf, d["ref_stats"]
 
@@ -44,6 +46,8 @@ def test_oracle_reproduces_reference(path, oracle):
     out, rc = oracle.step(case, st, meta["nsteps"], extf=extf)
     assert rc == 0
     assert (out["status"] == ref["status"]).all()
+    if "asb" in ref:
+        assert (out["asb"] == ref["asb"]).all()
     dx = case["params"]["dx"]
     for k in FIELDS:
         scale = dx if k in ("x", "y", "z") else max(np.abs(ref[k]).max(), 1e-30)
@@ -74,7 +78,7 @@ def test_fixture_spread_is_small():
     for path in FILES:
         _, _, ref, meta, _, _ = load(path)
         for k, v in meta["spread"].items():
-            if k in ("status", "id"):
+            if k in ("status", "id", "asb"):
                 assert v == 0, (path.stem, k)
                 continue
             scale = max(float(np.abs(ref[k]).max()), 1e-30)
