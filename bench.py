@@ -223,6 +223,9 @@ def run_ours(args):
         # temperature guard and its strain-rate test decides
         p.asb_enabled = 1
         T0 = box["T0"] + 1.0
+    if args.heat:
+        # grid heat conduction (MPMWorkpieceSolver's scheme), reference default conductivity
+        p.heat_conduction = 1
     cap = int(np.prod([box["c1"][i] - box["c0"][i] for i in range(3)]) * box["ppc"])
     s = Solver(p, cap, stream=stream.cuda_stream)
     n = s.init_box(box["c0"], box["c1"], box["ppc"], box["seed"] + rank, box["instance"], box["fixed_layers"],
@@ -300,7 +303,7 @@ def run_ours(args):
                        "escaped_updates": int(m1["n_escaped"]), "rebins": int(m1["n_sorts"]),
                        "contact_every": int(args.contact_every), "contacts": int(m1["n_contacts"]),
                        "adiabatic_shear": bool(args.asb), "asb_heated": int(m1["n_asb_heated"]),
-                       "initial_rise_K": float(T0 - box["T0"])},
+                       "initial_rise_K": float(T0 - box["T0"]), "heat_conduction": bool(args.heat)},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
@@ -692,6 +695,8 @@ def main():
                     help="plain configs: fuse the particle-side tool contact every n steps (0: off)")
     ap.add_argument("--asb", action="store_true",
                     help="plain configs: run the adiabatic shear band heating after every move")
+    ap.add_argument("--heat", action="store_true",
+                    help="plain configs: grid heat conduction (scatter, diffusion step, gather) every step")
     ap.add_argument("--repeats", type=int, default=5, help="precision_study: FP32 runs")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: window in seconds")

@@ -1,7 +1,9 @@
 // mpm_aux.cu -- re-binning (counting sort by 4^3-cell bin), scans, upload and
 // download conversions, the reference-layout AoS export, FP64 metric
-// reductions, tool rasterisation and the seeded workpiece generator.
+// reductions, tool rasterisation, the seeded workpiece generator and the heat
+// conduction diffusion step.
 #include <cuda.h>
+#include <algorithm>
 #include <cuda_runtime.h>
 
 #include "mpm_device.cuh"
@@ -825,6 +827,61 @@ void launch_relayout(const PState<R>& src, const PState<R>& dst, const RelayoutM
     ++launch_counter();
 }
 
+// ------------------------------------------------------------------ heat conduction
+
+// mpmDiffuseTemperatureKernel (reference src/MPMWorkpieceSolver.cu:208-262) as
+// the Jacobi step it describes, over the nodes of every instance that conducts
+// heat: from grid buffer b (mass in .x) and its T m buffer to the node
+// temperatures tn.  A node with m >= 1e-15 takes T + alpha dt lap(T) / dx^2,
+// T = (T m)/m, 7-point Laplacian over the neighbours inside the domain, a
+// neighbour's T = (T m) / max(m, 1e-30) (0 at an empty node), then T >= 0; a
+// lighter node keeps (T m)/m.  (The reference updates in place, so there a
+// node can read a neighbour already updated, depending on the schedule.)
+template <typename R>
+__global__ void k_heat_diffuse(const Inst<R>* __restrict__ insts, int n_inst, int b, int64_t total) {
+    for (int64_t gi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gi < total;
+         gi += (int64_t)gridDim.x * blockDim.x) {
+        int lo = 0, hi = n_inst - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (insts[mid].gbase <= gi) lo = mid; else hi = mid - 1;
+        }
+        const Inst<R>& P = insts[lo];
+        if (!P.heat_on) continue;
+        const int64_t li = gi - P.gbase;
+        if (li < 0 || li >= P.nn) continue;
+        const V4<R>* __restrict__ g = P.grid[b];
+        const R* __restrict__ tm = P.tm[b];
+        const R m = g[li].x;
+        if (m < R(1e-15)) {
+            P.tn[li] = m > R(0) ? tm[li] / m : R(0);
+            continue;
+        }
+        const R T = tm[li] / m;
+        const int nx = P.nx, ny = P.ny, nz = P.nz;
+        const int64_t nxy = (int64_t)nx * ny;
+        const int i = (int)(li % nx);
+        const int64_t t = li / nx;
+        const int j = (int)(t % ny), k = (int)(t / ny);
+        R lap = R(0);
+        if (i > 0) lap += tm[li - 1] / fmax(g[li - 1].x, R(1e-30)) - T;
+        if (i < nx - 1) lap += tm[li + 1] / fmax(g[li + 1].x, R(1e-30)) - T;
+        if (j > 0) lap += tm[li - nx] / fmax(g[li - nx].x, R(1e-30)) - T;
+        if (j < ny - 1) lap += tm[li + nx] / fmax(g[li + nx].x, R(1e-30)) - T;
+        if (k > 0) lap += tm[li - nxy] / fmax(g[li - nxy].x, R(1e-30)) - T;
+        if (k < nz - 1) lap += tm[li + nxy] / fmax(g[li + nxy].x, R(1e-30)) - T;
+        P.tn[li] = fmax(T + (R)P.heat_c * lap, R(0));
+    }
+}
+
+template <typename R>
+void launch_heat_diffuse(const Inst<R>* insts, int n_inst, int b, int64_t total, cudaStream_t st) {
+    if (total <= 0 || n_inst <= 0) return;
+    const int64_t blocks = std::min<int64_t>((total + kT - 1) / kT, 148 * 16);
+    k_heat_diffuse<R><<<(int)blocks, kT, 0, st>>>(insts, n_inst, b, total);
+    ++launch_counter();
+}
+
 #define MPMB_INST(R)                                                                                                  \
     template void launch_bin_count<R>(const Inst<R>*, int, const PState<R>&, const int32_t*, bool, const double*,   \
                                       int32_t*, int32_t*, int32_t*, int32_t*, int64_t, cudaStream_t);               \
@@ -842,7 +899,8 @@ void launch_relayout(const PState<R>& src, const PState<R>& dst, const RelayoutM
     template void launch_stats<R>(const Inst<R>*, const PState<R>&, int64_t, int64_t, double, double, double, double, \
                                   double, double*, int, double*, cudaStream_t);                                      \
     template void launch_set_temps<R>(const PState<R>&, int64_t, int64_t, const double*, int64_t, double, cudaStream_t); \
-    template void launch_relayout<R>(const PState<R>&, const PState<R>&, const RelayoutMap*, int, int64_t, cudaStream_t);
+    template void launch_relayout<R>(const PState<R>&, const PState<R>&, const RelayoutMap*, int, int64_t, cudaStream_t); \
+    template void launch_heat_diffuse<R>(const Inst<R>*, int, int, int64_t, cudaStream_t);
 
 MPMB_INST(float)
 MPMB_INST(double)

@@ -93,6 +93,9 @@ mpm_status mpm_params_default(mpm_params* p) {
     p->asb_taylor_quinney = 0.9;
     p->asb_max_temp_ratio = 0.9;
     p->asb_touch_rise = 0.5;
+    // MPMMaterialParams::thermalConductivity (include/MPMWorkpieceSolver.cuh:88); off
+    p->heat_conduction = 0;
+    p->thermal_conductivity = 42.6;
     return MPM_OK;
 }
 

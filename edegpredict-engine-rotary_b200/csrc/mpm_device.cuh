@@ -108,6 +108,15 @@ template <typename R> struct alignas(128) Inst {
     // above Tamb: the heated-particle guard, the cap asb_max_temp_ratio * Tm - Tamb
     int asb_on;
     R asb_rise, asb_min_rate, asb_crit, asb_heat, asb_Tcap;
+    // grid heat conduction (heat_on = 0: off): T m scatter buffers (with grid[2]), the node
+    // temperatures after the diffusion step, alpha dt / dx^2, and the absolute ambient (the
+    // particles hold the rise above it)
+    int heat_on;
+    R* tm[2];
+    R* tn;
+    double heat_c;
+    R Tamb;
+    int64_t gbase;                 // first node of this instance in the batch grid arrays
     // external force for one step (radius 0: none)
     double ext_c[3], ext_r, ext_f[3];
     int64_t pbase;                 // first particle slot of this instance in the batch arrays
@@ -137,8 +146,8 @@ struct StepArgs {
     int sigma_all;      // P2G: store stress for every ACTIVE particle (last P2G of a call)
     int use_ext;        // P2G: apply the one-step external force
     int p2g_step;       // step index of the P2G part
-    int asb;            // some instance runs the adiabatic shear model: G2P launches take the kernel
-                        // variant that has it (the others carry none of its code)
+    int ext;            // some instance runs the adiabatic shear model or heat conduction: launches
+                        // take the kernel variant that has them (the others carry none of their code)
 };
 
 // ------------------------------------------------------------------ weights

@@ -80,6 +80,8 @@ mpm_status check_params(const mpm_params* p, std::string* err) {
                            !(p->asb_max_temp_ratio > 0.0) || !(p->asb_touch_rise >= 0.0)))
         return bad("adiabatic shear model needs critical rate >= 0, Taylor-Quinney >= 0, max temperature ratio > 0 "
                    "and touch rise >= 0");
+    if (p->heat_conduction && (!(p->thermal_conductivity >= 0.0) || !(p->rho_phys * p->cp > 0.0)))
+        return bad("heat conduction needs thermal_conductivity >= 0 and rho_phys * cp > 0");
     return MPM_OK;
 }
 
@@ -100,6 +102,9 @@ class Engine final : public EngineBase {
     int cur = 0;
     bool has_K = false;
     V4<R>* gpool[2] = {nullptr, nullptr};
+    // heat conduction node arrays, beside the grids: T m scatter (two buffers, paired with
+    // gpool) and the node temperatures after the diffusion step
+    R* tpool[3] = {nullptr, nullptr, nullptr};
     uint8_t* mask_pool = nullptr;
     Inst<R>* d_inst = nullptr;
     std::vector<Inst<R>> h_inst;
@@ -168,7 +173,8 @@ class Engine final : public EngineBase {
     ~Engine() override {
         if (st) cudaStreamSynchronize(st);
         drop_graphs();
-        void* ptrs[] = {pbuf[0], pbuf[1], gpool[0], gpool[1], mask_pool, d_inst, d_key_base, d_bin_key, d_bin_inst,
+        void* ptrs[] = {pbuf[0], pbuf[1], gpool[0], gpool[1], tpool[0], tpool[1], tpool[2], mask_pool, d_inst,
+                        d_key_base, d_bin_key, d_bin_inst,
                         d_bin_local,
                         d_inst_pbase, d_key, d_rank, d_newbin, d_count, d_offset, d_flag, d_flag_scan, d_scan_tmp,
                         d_pos, d_work, d_nwork, d_err, d_ctr, d_stat_part, d_stat_out, d_stage, d_gen, d_map};
@@ -399,16 +405,22 @@ class Engine final : public EngineBase {
                 if (gpool[b]) cudaFree(gpool[b]);
                 gpool[b] = nullptr;
             }
+            for (int b = 0; b < 3; ++b) {
+                if (tpool[b]) cudaFree(tpool[b]);
+                tpool[b] = nullptr;
+            }
             if (mask_pool) cudaFree(mask_pool);
             mask_pool = nullptr;
             const int64_t nn = std::max<int64_t>(nn_total + nn_total / 4, 1);
             for (int b = 0; b < 2; ++b) CK(cudaMalloc(&gpool[b], sizeof(V4<R>) * nn));
+            for (int b = 0; b < 3; ++b) CK(cudaMalloc(&tpool[b], sizeof(R) * nn));
             CK(cudaMalloc(&mask_pool, nn));
             nn_alloc = nn;
         }
         if (nn_total > 0) {
             CK(cudaMemsetAsync(gpool[0], 0, sizeof(V4<R>) * nn_total, st));
             CK(cudaMemsetAsync(gpool[1], 0, sizeof(V4<R>) * nn_total, st));
+            for (int b = 0; b < 3; ++b) CK(cudaMemsetAsync(tpool[b], 0, sizeof(R) * nn_total, st));
             CK(cudaMemsetAsync(mask_pool, 0, nn_total, st));
         }
         rbuf = 0;
@@ -487,6 +499,12 @@ class Engine final : public EngineBase {
             if (gpool[b]) cudaFree(gpool[b]);
             gpool[b] = nullptr;
             CK(cudaMalloc(&gpool[b], sizeof(V4<R>) * nodes));
+        }
+        for (int b = 0; b < 3; ++b) {
+            if (tpool[b]) cudaFree(tpool[b]);
+            tpool[b] = nullptr;
+            CK(cudaMalloc(&tpool[b], sizeof(R) * nodes));
+            CK(cudaMemsetAsync(tpool[b], 0, sizeof(R) * nodes, st));
         }
         if (mask_pool) cudaFree(mask_pool);
         mask_pool = nullptr;
@@ -586,6 +604,10 @@ class Engine final : public EngineBase {
         const mpm_params& p = x.p;
         Inst<R>& d = h_inst[i];
         d.tool_mask = mask_pool + x.grid_off;
+        d.tm[0] = tpool[0] + x.grid_off;
+        d.tm[1] = tpool[1] + x.grid_off;
+        d.tn = tpool[2] + x.grid_off;
+        d.gbase = x.grid_off;
         d.nx = p.nx; d.ny = p.ny; d.nz = p.nz;
         d.nbx = x.nbx; d.nby = x.nby; d.nbz = x.nbz;
         d.nbins = x.nbx * x.nby * x.nbz;
@@ -626,6 +648,10 @@ class Engine final : public EngineBase {
         d.contact_mu = p.contact_friction;
         d.contact_hp = p.contact_heat_partition;
         d.rho_phys = p.rho_phys;
+        // MPMWorkpieceSolver::step: alpha = k / (rho cp) (src/MPMWorkpieceSolver.cu:751-752)
+        d.heat_on = p.heat_conduction ? 1 : 0;
+        d.heat_c = p.thermal_conductivity / (p.rho_phys * p.cp) * x.dt / (p.dx * p.dx);
+        d.Tamb = (R)p.Tamb;
         d.cp = p.cp;
         // applyAdiabaticHeatingKernel constants (src/AdiabaticShearModel.cu:131-176)
         d.asb_on = p.asb_enabled ? 1 : 0;
@@ -973,18 +999,32 @@ class Engine final : public EngineBase {
             return MPM_OK;
         };
         const int cps = ctas_per_sm;
-        int asb = 0;
-        for (const InstHost& x : I) asb |= x.p.asb_enabled ? 1 : 0;
+        int xk = 0, heat = 0;
+        for (const InstHost& x : I) {
+            xk |= (x.p.asb_enabled || x.p.heat_conduction) ? 1 : 0;
+            heat |= x.p.heat_conduction ? 1 : 0;
+        }
+        // the grid buffer a P2G launch writes starts at zero, and so does its T m buffer
+        auto clear = [&](int b) -> mpm_status {
+            CK(cudaMemsetAsync(gpool[b], 0, gbytes, st));
+            if (heat) CK(cudaMemsetAsync(tpool[b], 0, sizeof(R) * nn_total, st));
+            return MPM_OK;
+        };
+        // heat conduction: the diffusion step on grid buffer b before the G2P that reads it
+        auto diffuse = [&](int b) {
+            if (heat) launch_heat_diffuse<R>(d_inst, (int)I.size(), b, nn_total, st);
+        };
         if (fused) {
-            CK(cudaMemsetAsync(gpool[w], 0, gbytes, st));
-            StepArgs a{0, 0, N == 1 ? 1 : 0, ext ? 1 : 0, 0, asb};
+            if ((s = clear(w)) != MPM_OK) return s;
+            StepArgs a{0, 0, N == 1 ? 1 : 0, ext ? 1 : 0, 0, xk};
             launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], a, w, false, true, threads, cps, d_err, d_ctr,
                            st);
             for (int k = 0; k + 1 < N; ++k) {
                 if ((s = maybe_sort()) != MPM_OK) return s;
-                CK(cudaMemsetAsync(gpool[w ^ 1], 0, gbytes, st));
+                if ((s = clear(w ^ 1)) != MPM_OK) return s;
                 raster_all(k);
-                StepArgs b{k, 0, (k + 2 == N) ? 1 : 0, 0, k + 1, asb};
+                diffuse(w);
+                StepArgs b{k, 0, (k + 2 == N) ? 1 : 0, 0, k + 1, xk};
                 prof_begin();
                 launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], b, w, true, true, threads, cps, d_err,
                                d_ctr, st);
@@ -993,21 +1033,23 @@ class Engine final : public EngineBase {
                 ++since_sort;
             }
             raster_all(N - 1);
-            StepArgs c{N - 1, 1, 0, 0, N - 1, asb};
+            diffuse(w);
+            StepArgs c{N - 1, 1, 0, 0, N - 1, xk};
             launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], c, w, true, false, threads, cps, d_err, d_ctr,
                            st);
             ++since_sort;
         } else {
             for (int k = 0; k < N; ++k) {
                 if ((s = maybe_sort()) != MPM_OK) return s;
-                CK(cudaMemsetAsync(gpool[w], 0, gbytes, st));
-                StepArgs a{k, 0, 1, (ext && k == 0) ? 1 : 0, k, asb};
+                if ((s = clear(w)) != MPM_OK) return s;
+                StepArgs a{k, 0, 1, (ext && k == 0) ? 1 : 0, k, xk};
                 prof_begin();
                 launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], a, w, false, true, threads, cps, d_err,
                                d_ctr, st);
                 prof_end();
                 raster_all(k);
-                StepArgs c{k, 1, 0, 0, k, asb};
+                diffuse(w);
+                StepArgs c{k, 1, 0, 0, k, xk};
                 prof_begin();
                 launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], c, w, true, false, threads, cps, d_err,
                                d_ctr, st);

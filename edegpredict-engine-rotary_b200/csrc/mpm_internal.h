@@ -48,6 +48,11 @@ struct RelayoutMap {
 // Number of stats accumulators (see k_stats).
 constexpr int kStatSlots = 32;
 
+// One heat-conduction diffusion step on grid buffer b of every instance that
+// conducts heat (node temperatures into Inst::tn).
+template <typename R>
+void launch_heat_diffuse(const Inst<R>* insts, int n_inst, int b, int64_t total, cudaStream_t st);
+
 template <typename R>
 void launch_step(const Inst<R>* insts, const Work* work, const int* n_work, int max_work, const PState<R>& ps,
                  const StepArgs& a, int rbuf, bool g2p, bool p2g, int threads, int ctas_per_sm, int* err,

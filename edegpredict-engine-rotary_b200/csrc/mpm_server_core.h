@@ -59,7 +59,7 @@ inline PoolBytes pool_bytes(int precision, bool backstress) {
     // the FP64 position scratch
     const double nv4 = 12.0 + (backstress ? 2.0 : 0.0) + (precision == MPM_PREC_F64 ? 0.0 : 1.0);
     b.particle = 2.0 * (nv4 * v4 + r + 2.0 + 12.0) + 12.0 + 24.0;
-    b.node = 2.0 * v4 + 1.0;     // two grid buffers and the tool mask
+    b.node = 2.0 * v4 + 3.0 * r + 1.0;   // two grid buffers, three heat-conduction arrays, tool mask
     b.key = 8.0;                 // count and offset
     b.bin = 40.0;                // bin tables, flags and the work item
     return b;

@@ -327,6 +327,65 @@ __device__ __noinline__ void scatter_global(const Inst<R>& P, V4<R>* __restrict_
     }
 }
 
+// Heat conduction on the global paths (particles whose stencil left the bin
+// tile): the T m scatter into the write buffer, and the temperature gather
+// over the nodes with m > 1e-18 (sum of w T and of w), as the tile paths do.
+template <typename R>
+__device__ __noinline__ void scatter_T_global(const Inst<R>& P, R* __restrict__ tw, int g0x, int g0y, int g0z, R x0,
+                                              R x1, R x2, R mT) {
+    R w[3][3], dw[3][3];
+    int gb[3];
+    gb[0] = g0x + bspline(x0, w[0], dw[0]);
+    gb[1] = g0y + bspline(x1, w[1], dw[1]);
+    gb[2] = g0z + bspline(x2, w[2], dw[2]);
+    for (int i = 0; i < 3; ++i) {
+        const int gx = gb[0] + i;
+        if (gx < 0 || gx >= P.nx) continue;
+        for (int j = 0; j < 3; ++j) {
+            const int gy = gb[1] + j;
+            if (gy < 0 || gy >= P.ny) continue;
+            for (int k = 0; k < 3; ++k) {
+                const int gz = gb[2] + k;
+                if (gz < 0 || gz >= P.nz) continue;
+                atomicAdd(&tw[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], w[0][i] * w[1][j] * w[2][k] * mT);
+            }
+        }
+    }
+}
+
+template <typename R> struct TSum {
+    R ts, ws;
+};
+
+template <typename R>
+__device__ __noinline__ TSum<R> gather_T_global(const Inst<R>& P, const V4<R>* __restrict__ grid, int g0x, int g0y,
+                                                int g0z, R x0, R x1, R x2) {
+    R w[3][3], dw[3][3];
+    int gb[3];
+    gb[0] = g0x + bspline(x0, w[0], dw[0]);
+    gb[1] = g0y + bspline(x1, w[1], dw[1]);
+    gb[2] = g0z + bspline(x2, w[2], dw[2]);
+    TSum<R> o{R(0), R(0)};
+    for (int i = 0; i < 3; ++i) {
+        const int gx = gb[0] + i;
+        if (gx < 0 || gx >= P.nx) continue;
+        for (int j = 0; j < 3; ++j) {
+            const int gy = gb[1] + j;
+            if (gy < 0 || gy >= P.ny) continue;
+            for (int k = 0; k < 3; ++k) {
+                const int gz = gb[2] + k;
+                if (gz < 0 || gz >= P.nz) continue;
+                const int64_t q = gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz);
+                const R ww = w[0][i] * w[1][j] * w[2][k];
+                if (!(ww > R(0)) || !(grid[q].x > R(1e-18))) continue;
+                o.ts += P.tn[q] * ww;
+                o.ws += ww;
+            }
+        }
+    }
+    return o;
+}
+
 // ------------------------------------------------------------------ Johnson-Cook
 
 // Consistent return (extension of this build), FP64: q - 3 mu dg = Y(eps + dg)
@@ -659,24 +718,29 @@ constexpr int kOff = 27;  // stencil offsets, off = i + 3j + 9k
 // straight to the grid (counted with the escaped updates).
 constexpr int kCellCap = 16;
 
-template <typename R> struct StepSmem {
+// EXT: the kernel variant with the extensions (adiabatic shear heating, heat
+// conduction), which adds the payload's absolute temperature (row kPay), the
+// T m node sums (nacc[4]) and the node temperature tile with its m > 1e-18
+// mask (ttile).
+template <typename R, bool EXT> struct StepSmem {
     // The TMA tile is read only by the fill at the start of a bin and the payload
     // only inside the bin's passes, with barriers between: one buffer holds both,
     // which keeps four CTAs within the 164 KB shared-memory carveout (92 KB of L1
     // left for the register spills).
     union {
-        V4<R> raw[kTileNodes];             // TMA destination (offset 0 of the 128-byte aligned block)
-        R pay[kPay][StepCfg<R>::kChunk];   // scatter payload of the staged particles
+        V4<R> raw[kTileNodes];                          // TMA destination (offset 0 of the 128-byte aligned block)
+        R pay[EXT ? kPay + 1 : kPay][StepCfg<R>::kChunk];  // scatter payload of the staged particles
     };
     R vel[3][kPlane];                      // node velocities after the grid update
-    R nacc[4][kPlane];                     // the bin's node sums m, p_x, p_y, p_z (tidx layout)
+    R nacc[EXT ? 5 : 4][kPlane];           // the bin's node sums m, p_x, p_y, p_z (, T m) (tidx layout)
+    R ttile[EXT ? 2 : 1][EXT ? kPlane : 1];  // node temperatures and their m > 1e-18 mask
     short slot[kCellsPerBin][kCellCap];    // staged particles of each base cell
     int cnt[2][kCellsPerBin];              // staged particles per cell (atomic ranks), by pass parity
     uint64_t mbar;
     int fail;
 };
 
-template <typename R> constexpr size_t step_smem_bytes() { return sizeof(StepSmem<R>); }
+template <typename R, bool EXT> constexpr size_t step_smem_bytes() { return sizeof(StepSmem<R, EXT>); }
 
 // Momentum + impulse of one channel a over the 27 stencil nodes (i,j,k) of a
 // particle, relative to its base node:
@@ -718,8 +782,8 @@ __device__ __forceinline__ void channel_add(const R (&w)[3][3], const R (&dw)[3]
 // {2,3}) address 32 distinct nodes, and tidx's z stride of 68 (4 mod 32)
 // puts them in 32 distinct banks: the adds neither collide nor conflict.
 // par: parity of the staging pass.
-template <typename R>
-__device__ __forceinline__ void cell_accumulate(StepSmem<R>& Sm, int cell, int h, R pm, int par) {
+template <typename R, bool EXT>
+__device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT>& Sm, int cell, int h, R pm, int par, bool heat) {
     R a0[kOff], a1[kOff];
 #pragma unroll
     for (int o = 0; o < kOff; ++o) { a0[o] = R(0); a1[o] = R(0); }
@@ -765,14 +829,45 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R>& Sm, int cell, int h
                     atomicAdd(&Sm.nacc[2 * h + 1][t], a1[o]);
                 }
     }
+    if (EXT && heat && h == 0 && n > 0) {
+        // heat conduction: the T m channel, w m T over the cell's particles (the
+        // lighter half of the pair takes it)
+#pragma unroll
+        for (int o = 0; o < kOff; ++o) a0[o] = R(0);
+        for (int q = 0; q < n; ++q) {
+            const int e = Sm.slot[cell][q];
+            R w[3][3], dw[3][3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) (void)bspline(Sm.pay[a][e], w[a], dw[a]);
+            const R mT = pm * Sm.pay[kPay][e];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const R mx = mT * w[0][i];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const R mxy = mx * w[1][j];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) a0[i + 3 * j + 9 * k] = fma(mxy, w[2][k], a0[i + 3 * j + 9 * k]);
+                }
+            }
+        }
+        const int base = tidx(cell & (kBin - 1), (cell / kBin) & (kBin - 1), cell / (kBin * kBin));
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    atomicAdd(&Sm.nacc[4][base + i + kSY * j + kSZ * k], a0[i + 3 * j + 9 * k]);
+    }
 }
 
-template <typename R, bool G2P, bool P2G, bool ASB>
+template <typename R, bool G2P, bool P2G, bool EXT>
 __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __restrict__ insts, const Work* __restrict__ work,
                                               const int* __restrict__ n_work, PState<R> ps, StepArgs sa, int rbuf,
                                               int* __restrict__ err, unsigned long long* __restrict__ ctr) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    StepSmem<R>& Sm = *reinterpret_cast<StepSmem<R>*>(smem_raw);
+    StepSmem<R, EXT>& Sm = *reinterpret_cast<StepSmem<R, EXT>*>(smem_raw);
     constexpr int kChunk = StepCfg<R>::kChunk;
     const int tid = threadIdx.x, lane = tid & 31;
     const int nw = *n_work;
@@ -788,7 +883,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
     if (tid < 2 * kCellsPerBin) (&Sm.cnt[0][0])[tid] = 0;
     // node sums start at zero; the end-of-bin flush clears what it reads
     if (P2G)
-        for (int q = tid; q < 4 * kPlane; q += kNT) (&Sm.nacc[0][0])[q] = R(0);
+        for (int q = tid; q < (EXT ? 5 : 4) * kPlane; q += kNT) (&Sm.nacc[0][0])[q] = R(0);
     __syncthreads();
     int par = 0;  // parity of the staging pass (counts double-buffered across passes)
     int last_inst = -1;
@@ -833,6 +928,14 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                 const NV<R> nv = node_vel_inl(P, Sm.raw[nidx], g0x + lx, g0y + ly, g0z + lz, prg0, prg2);
                 const int t = tidx(lx, ly, lz);
                 Sm.vel[0][t] = nv.x; Sm.vel[1][t] = nv.y; Sm.vel[2][t] = nv.z;
+                if (EXT && P.heat_on) {
+                    // node temperatures after the diffusion step, for the nodes the
+                    // temperature gather counts (m > 1e-18, inside the domain)
+                    const int gx = g0x + lx, gy = g0y + ly, gz = g0z + lz;
+                    const bool use = Sm.raw[nidx].x > R(1e-18) && gx < P.nx && gy < P.ny && gz < P.nz;
+                    Sm.ttile[0][t] = use ? P.tn[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)] : R(0);
+                    Sm.ttile[1][t] = use ? R(1) : R(0);
+                }
             }
         }
         __syncthreads();
@@ -886,8 +989,25 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
 #pragma unroll
                             for (int a = 0; a < 3; ++a) b[a] = bspline(xi[a], w[a], dw[a]);
                             R M[3][3], L[3][3];
+                            TSum<R> tsum{R(0), R(0)};
                             if (b[0] >= 0 && b[0] < kBin && b[1] >= 0 && b[1] < kBin && b[2] >= 0 && b[2] < kBin) {
                                 gather_tile<R>(Sm.vel, tidx(b[0], b[1], b[2]), w, dw, v, M, L);
+                                if (EXT && P.heat_on) {
+                                    const int tb = tidx(b[0], b[1], b[2]);
+#pragma unroll
+                                    for (int k = 0; k < 3; ++k)
+#pragma unroll
+                                        for (int j = 0; j < 3; ++j) {
+                                            const R wjk = w[1][j] * w[2][k];
+#pragma unroll
+                                            for (int i = 0; i < 3; ++i) {
+                                                const int q = tb + i + kSY * j + kSZ * k;
+                                                const R ww = w[0][i] * wjk;
+                                                tsum.ts = fma(ww, Sm.ttile[0][q], tsum.ts);
+                                                tsum.ws = fma(ww, Sm.ttile[1][q], tsum.ws);
+                                            }
+                                        }
+                                }
                             } else {
                                 const GatherOut<R> go = gather_global<R>(P, gr, g0x, g0y, g0z, xi[0], xi[1], xi[2],
                                                                          prg0, prg2);
@@ -898,6 +1018,12 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                     for (int q = 0; q < 3; ++q) { M[c][q] = go.M[c][q]; L[c][q] = go.L[c][q]; }
                                 }
                                 ++c_esc;
+                                if (EXT && P.heat_on) tsum = gather_T_global<R>(P, gr, g0x, g0y, g0z, xi[0], xi[1], xi[2]);
+                            }
+                            if (EXT && P.heat_on && tsum.ws > R(1e-8)) {
+                                // heat conduction: the temperature gather of mpmG2PKernel
+                                // (src/MPMWorkpieceSolver.cu:282-306), clamped to [Tamb, Tm]
+                                dT = fmin(fmax(tsum.ts / tsum.ws, P.Tamb), P.Tamb + P.dTmax) - P.Tamb;
                             }
                             const R d[3] = {xi[0] - R(b[0]), xi[1] - R(b[1]), xi[2] - R(b[2])};
 #pragma unroll
@@ -950,7 +1076,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                         // (AdiabaticShearModel::update after g2pKernel, src/MPMSolver.cu:1130-1132;
                         // guards of src/AdiabaticShearModel.cu:114-136); the stress is the one the
                         // constitutive update of this step stored
-                        if (ASB && P.asb_on) {
+                        if (EXT && P.asb_on) {
                             if (st == ST_CHIP) {
                                 if (ps.asb[pi] != 0) ps.asb[pi] = 0;   // :114-117
                             } else if (st == ST_ACTIVE && dT > P.asb_rise) {   // :119-123
@@ -1146,6 +1272,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                 if (rank < kCellCap) Sm.slot[scell][rank] = (short)slot;
                             }
                             if (rank < kCellCap) {
+                                if (EXT) Sm.pay[EXT ? kPay : 0][slot] = P.Tamb + dT;   // absolute T (heat conduction)
                                 Sm.pay[0][slot] = xi[0]; Sm.pay[1][slot] = xi[1]; Sm.pay[2][slot] = xi[2];
 #pragma unroll
                                 for (int a = 0; a < 3; ++a) Sm.pay[3 + a][slot] = Q[a];
@@ -1159,6 +1286,9 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                 for (int q = 0; q < 9; ++q) { si.Rm[q] = Rm[q]; si.S[q] = S[q]; }
                                 si.g0[0] = g0x; si.g0[1] = g0y; si.g0[2] = g0z;
                                 scatter_global<R>(P, gw, si, m);
+                                if (EXT && P.heat_on)
+                                    scatter_T_global<R>(P, P.tm[rbuf ^ (G2P ? 1 : 0)], g0x, g0y, g0z, xi[0], xi[1],
+                                                        xi[2], m * (P.Tamb + dT));
                                 ++c_esc;
                             }
                         }
@@ -1191,7 +1321,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
             }
             if (P2G) {
                 __syncthreads();
-                cell_accumulate<R>(Sm, tid & (kCellsPerBin - 1), tid >> 6, P.pmass, par);
+                cell_accumulate<R, EXT>(Sm, tid & (kCellsPerBin - 1), tid >> 6, P.pmass, par, P.heat_on != 0);
                 par ^= 1;
                 __syncthreads();
             }
@@ -1204,10 +1334,17 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                 const int t = tidx(X, Y, Z);
                 const R m = Sm.nacc[0][t], px = Sm.nacc[1][t], py = Sm.nacc[2][t], pz = Sm.nacc[3][t];
                 Sm.nacc[0][t] = R(0); Sm.nacc[1][t] = R(0); Sm.nacc[2][t] = R(0); Sm.nacc[3][t] = R(0);
+                R mT = R(0);
+                if (EXT) {
+                    mT = Sm.nacc[EXT ? 4 : 0][t];
+                    Sm.nacc[EXT ? 4 : 0][t] = R(0);
+                }
                 if (m == R(0)) continue;
                 const int gx = g0x + X, gy = g0y + Y, gz = g0z + Z;
                 if (gx >= P.nx || gy >= P.ny || gz >= P.nz) continue;
                 vec_atomic_add<R>(&gw[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], m, px, py, pz);
+                if (EXT && P.heat_on)
+                    atomicAdd(&P.tm[rbuf ^ (G2P ? 1 : 0)][gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], mT);
             }
         }
         __syncthreads();
@@ -1235,11 +1372,11 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
     }
 }
 
-template <typename R, bool G2P, bool P2G, bool ASB> static void set_smem_attr() {
+template <typename R, bool G2P, bool P2G, bool EXT> static void set_smem_attr() {
     static bool done = false;
     if (!done) {
-        cudaFuncSetAttribute(k_step<R, G2P, P2G, ASB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)step_smem_bytes<R>());
+        cudaFuncSetAttribute(k_step<R, G2P, P2G, EXT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)step_smem_bytes<R, EXT>());
         done = true;
     }
 }
@@ -1259,19 +1396,22 @@ void launch_step(const Inst<R>* insts, const Work* work, const int* n_work, int 
     if (max_work <= 0) return;
     int grid = sms * (ctas_per_sm > 0 ? ctas_per_sm : 4);
     if (grid > max_work) grid = max_work;
-    const size_t smem = step_smem_bytes<R>();
-    if (g2p && p2g && a.asb) {
+    const size_t smem = a.ext ? step_smem_bytes<R, true>() : step_smem_bytes<R, false>();
+    if (g2p && p2g && a.ext) {
         set_smem_attr<R, true, true, true>();
         k_step<R, true, true, true><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
     } else if (g2p && p2g) {
         set_smem_attr<R, true, true, false>();
         k_step<R, true, true, false><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
-    } else if (g2p && a.asb) {
+    } else if (g2p && a.ext) {
         set_smem_attr<R, true, false, true>();
         k_step<R, true, false, true><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
     } else if (g2p) {
         set_smem_attr<R, true, false, false>();
         k_step<R, true, false, false><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+    } else if (a.ext) {
+        set_smem_attr<R, false, true, true>();
+        k_step<R, false, true, true><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
     } else {
         set_smem_attr<R, false, true, false>();
         k_step<R, false, true, false><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);

@@ -39,6 +39,7 @@ class MpmParams(C.Structure):
         ("contact_friction", _d), ("contact_heat_partition", _d),
         ("asb_enabled", _i32), ("_pad_asb", _i32), ("asb_critical_rate", _d), ("asb_taylor_quinney", _d),
         ("asb_max_temp_ratio", _d), ("asb_touch_rise", _d),
+        ("heat_conduction", _i32), ("_pad_heat", _i32), ("thermal_conductivity", _d),
     ]
 
 

@@ -110,6 +110,22 @@ typedef struct mpm_params {
     int32_t asb_enabled;
     int32_t _pad_asb;
     double asb_critical_rate, asb_taylor_quinney, asb_max_temp_ratio, asb_touch_rise;
+    /* Grid heat conduction as MPMWorkpieceSolver does it, on this solver's
+     * quadratic weights (heat_conduction = 0: off; MPMSolver conducts no
+     * heat).  P2G scatters T m with the mass (src/MPMWorkpieceSolver.cu:118);
+     * between P2G and G2P every node with m >= 1e-15 takes one explicit step
+     * T += alpha dt lap(T) / dx^2 of T = (T m)/m, alpha = thermal_conductivity
+     * / (rho_phys cp), 7-point Laplacian, no flux through the domain faces, an
+     * empty neighbour counted as T = 0, T >= 0 (mpmDiffuseTemperatureKernel,
+     * :208-262); G2P then sets the temperature of every particle that is not
+     * FIXED to the weight-normalised mean over the nodes with m > 1e-18,
+     * clamped to [Tamb, Tm] (:282-306).  Temperatures are absolute here (the
+     * empty-node T = 0 is the unit's zero).  Reference default
+     * (MPMMaterialParams::thermalConductivity,
+     * include/MPMWorkpieceSolver.cuh:88): 42.6 W/(m K). */
+    int32_t heat_conduction;
+    int32_t _pad_heat;
+    double thermal_conductivity;
 } mpm_params;
 
 /* Fill p with the reference defaults (MPMKernelConfig / Config.h defaults,

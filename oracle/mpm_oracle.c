@@ -19,7 +19,8 @@
 #endif
 
 /* grid channel offsets (SoA planes of nn doubles each) */
-enum { G_M, G_PX, G_PY, G_PZ, G_FX, G_FY, G_FZ, G_VX, G_VY, G_VZ, G_TVX, G_TVY, G_TVZ, G_TOOL, G_NCH };
+/* G_TM: scattered T m; G_TN: node temperature after the diffusion step */
+enum { G_M, G_PX, G_PY, G_PZ, G_FX, G_FY, G_FZ, G_VX, G_VY, G_VZ, G_TVX, G_TVY, G_TVZ, G_TOOL, G_TM, G_TN, G_NCH };
 
 static inline int64_t nnodes(const orc_params *p) { return (int64_t)p->nx * p->ny * p->nz; }
 
@@ -325,6 +326,8 @@ static int p2g(const orc_params *p, orc_state *s, double *g, int nthreads) {
                     double ay = Cp[3] * dpx + Cp[4] * dpy + Cp[5] * dpz;
                     double az = Cp[6] * dpx + Cp[7] * dpy + Cp[8] * dpz;
                     gadd(&g[G_M * nn + gi], w * m, atomic);
+                    /* temperatureMass, src/MPMWorkpieceSolver.cu:118 */
+                    if (p->heat_conduction) gadd(&g[G_TM * nn + gi], s->T[ip] * (w * m), atomic);
                     if (!isFixed) {
                         gadd(&g[G_PX * nn + gi], w * m * (s->vx[ip] + ax), atomic);
                         gadd(&g[G_PY * nn + gi], w * m * (s->vy[ip] + ay), atomic);
@@ -344,6 +347,55 @@ static int p2g(const orc_params *p, orc_state *s, double *g, int nthreads) {
         }
     }
     return err;
+}
+
+/* mpmDiffuseTemperatureKernel (src/MPMWorkpieceSolver.cu:208-262): for a
+ * node with m >= 1e-15, T = (T m)/m takes T + alpha dt lap(T) / dx^2 with the
+ * 7-point Laplacian, no flux through the domain faces, a neighbour's
+ * temperature (T m) / max(m, 1e-30) (so 0 at an empty node), and T >= 0.
+ * The reference updates the grid in place, so a node can read a neighbour
+ * already updated, depending on the thread schedule; this is the Jacobi step
+ * it describes (every node from the temperatures before the step).  G_TN gets
+ * the node temperature g2p reads; nodes below 1e-15 keep (T m)/m. */
+static void heat_diffuse(const orc_params *p, double *g, double dt) {
+    const int64_t nn = nnodes(p);
+    const int nx = p->nx, ny = p->ny, nz = p->nz;
+    const int64_t nxy = (int64_t)nx * ny;
+    const double alpha = p->thermal_conductivity / (p->rho_phys * p->cp);
+    const double inv_h2 = 1.0 / (p->dx * p->dx);
+    for (int64_t idx = 0; idx < nn; ++idx) {
+        const double m = g[G_M * nn + idx];
+        if (m < 1e-15) {
+            g[G_TN * nn + idx] = m > 0.0 ? g[G_TM * nn + idx] / m : 0.0;
+            continue;
+        }
+        const double T = g[G_TM * nn + idx] / m;
+        const int i = (int)(idx % nx);
+        const int64_t t = idx / nx;
+        const int j = (int)(t % ny), k = (int)(t / ny);
+#define TNB(q) (g[G_TM * nn + (q)] / fmax(g[G_M * nn + (q)], 1e-30))
+        double lap = 0.0;
+        if (i > 0) lap += TNB(idx - 1) - T;
+        if (i < nx - 1) lap += TNB(idx + 1) - T;
+        if (j > 0) lap += TNB(idx - nx) - T;
+        if (j < ny - 1) lap += TNB(idx + nx) - T;
+        if (k > 0) lap += TNB(idx - nxy) - T;
+        if (k < nz - 1) lap += TNB(idx + nxy) - T;
+#undef TNB
+        const double Tn = T + alpha * dt * lap * inv_h2;
+        g[G_TN * nn + idx] = fmax(Tn, 0.0);
+    }
+}
+
+void orc_heat_diffuse(const orc_params *p, const double *mass, const double *tm, double *tn, double dt) {
+    const int64_t nn = nnodes(p);
+    double *g = (double *)calloc((size_t)(nn * G_NCH), sizeof(double));
+    if (!g) return;
+    memcpy(g + G_M * nn, mass, sizeof(double) * (size_t)nn);
+    memcpy(g + G_TM * nn, tm, sizeof(double) * (size_t)nn);
+    heat_diffuse(p, g, dt);
+    memcpy(tn, g + G_TN * nn, sizeof(double) * (size_t)nn);
+    free(g);
 }
 
 /* updateGridKernel (:424-442), applyFixtureBCKernel (:82-110) and the tool
@@ -485,6 +537,29 @@ static void g2p(const orc_params *p, orc_state *s, const double *g, double dt, i
                     L[6] += gvz * gdx; L[7] += gvz * gdy; L[8] += gvz * gdz;
                 }
             }
+        }
+        if (p->heat_conduction) {
+            /* temperature gather of mpmG2PKernel (src/MPMWorkpieceSolver.cu:282-306):
+             * weight-normalised mean over the nodes with m > 1e-18, clamped */
+            double ts = 0.0, ws = 0.0;
+            for (int i = 0; i < 3; ++i) {
+                int gx = bx + i;
+                if (gx < 0 || gx >= p->nx) continue;
+                for (int j = 0; j < 3; ++j) {
+                    int gy = by + j;
+                    if (gy < 0 || gy >= p->ny) continue;
+                    for (int k = 0; k < 3; ++k) {
+                        int gz = bz + k;
+                        if (gz < 0 || gz >= p->nz) continue;
+                        int64_t gi = gx + (int64_t)p->nx * (gy + (int64_t)p->ny * gz);
+                        const double w = wx[i] * wy[j] * wz[k];
+                        if (w <= 0.0 || g[G_M * nn + gi] <= 1e-18) continue;
+                        ts += g[G_TN * nn + gi] * w;
+                        ws += w;
+                    }
+                }
+            }
+            if (ws > 1e-8) s->T[ip] = fmin(fmax(ts / ws, p->Tamb), p->Tm);
         }
         s->vx[ip] = vx; s->vy[ip] = vy; s->vz[ip] = vz;
         s->x[ip] += vx * dt; s->y[ip] += vy * dt; s->z[ip] += vz * dt;
@@ -634,6 +709,7 @@ int orc_step(const orc_params *p, orc_state *s, const orc_tool_samples *tool, do
         memset(grid, 0, sizeof(double) * (size_t)ng);                 /* resetGridKernel :112 */
         err |= p2g(p, s, grid, nthreads);
         grid_update(p, grid, dt, tool, pr);
+        if (p->heat_conduction) heat_diffuse(p, grid, dt);
         g2p(p, s, grid, dt, nthreads);
         if (p->asb_enabled && s->asb) asb_heating(p, s, dt);
         if (s->extf) memset(s->extf, 0, sizeof(double) * 3 * (size_t)s->n);  /* :682-688 */

@@ -83,6 +83,12 @@ typedef struct orc_params {
      * heated-particle guard is T > Tamb + asb_touch_rise */
     int32_t asb_enabled;
     double asb_critical_rate, asb_taylor_quinney, asb_max_temp_ratio, asb_touch_rise;
+    /* grid heat conduction (heat_conduction != 0) as MPMWorkpieceSolver does
+     * it: T m scattered with the mass, one explicit diffusion step on the grid
+     * (mpmDiffuseTemperatureKernel, src/MPMWorkpieceSolver.cu:208-262), T
+     * gathered back in g2p (:282-306); alpha = k / (rho_phys cp) */
+    int32_t heat_conduction;
+    double thermal_conductivity;
 } orc_params;
 
 /* Particle state, SoA, one entry per particle (matrices row-major [n][9],
@@ -122,6 +128,10 @@ typedef struct orc_metrics {
  * the particles, as orc_step runs it after g2p when asb_enabled is set; needs
  * s->asb. */
 void orc_asb_heat(const orc_params *p, orc_state *s, double dt);
+
+/* One diffusion step on node arrays of nx*ny*nz doubles (mass, T m) -> the
+ * node temperatures, as orc_step runs it between the grid update and g2p. */
+void orc_heat_diffuse(const orc_params *p, const double *mass, const double *tm, double *tn, double dt);
 
 /* Size in doubles of the grid scratch that orc_step needs. */
 int64_t orc_grid_doubles(const orc_params *p);

@@ -43,7 +43,7 @@ class OrcParams(C.Structure):
         ("tool_rake", _d), ("tool_clear", _d), ("tool_tip_dz", _d), ("newton_tol", _d), ("newton_maxit", _i32),
         ("contact_every", _i32), ("contact_radius", _d), ("contact_friction", _d), ("contact_heat_partition", _d),
         ("asb_enabled", _i32), ("asb_critical_rate", _d), ("asb_taylor_quinney", _d), ("asb_max_temp_ratio", _d),
-        ("asb_touch_rise", _d),
+        ("asb_touch_rise", _d), ("heat_conduction", _i32), ("thermal_conductivity", _d),
     ]
 
 
@@ -115,6 +115,8 @@ def orc_params(case: dict) -> OrcParams:
     o.asb_taylor_quinney = float(p.get("asb_taylor_quinney", 0.9))
     o.asb_max_temp_ratio = float(p.get("asb_max_temp_ratio", 0.9))
     o.asb_touch_rise = float(p.get("asb_touch_rise", 0.5))
+    o.heat_conduction = int(p.get("heat_conduction", 0))
+    o.thermal_conductivity = float(p.get("thermal_conductivity", 42.6))
     return o
 
 
@@ -180,6 +182,8 @@ class Oracle:
         L.orc_tool_sdf.argtypes = [C.POINTER(OrcParams), C.POINTER(_d), _d, _d, _d]
         L.orc_asb_heat.restype = None
         L.orc_asb_heat.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcState), _d]
+        L.orc_heat_diffuse.restype = None
+        L.orc_heat_diffuse.argtypes = [C.POINTER(OrcParams), C.POINTER(_d), C.POINTER(_d), C.POINTER(_d), _d]
         self.L = L
 
     def step(self, case: dict, state: Dict[str, np.ndarray], nsteps: int, step0: int = 0, t0: float = 0.0,
@@ -198,6 +202,16 @@ class Oracle:
         b = _Bound(case, state)
         self.L.orc_asb_heat(C.byref(p), C.byref(b.state), float(dt))
         return b.result()
+
+    def heat_diffuse(self, case: dict, mass: np.ndarray, tm: np.ndarray, dt: float) -> np.ndarray:
+        """One grid diffusion step: node masses and T m (x fastest) -> node temperatures."""
+        p = orc_params(case)
+        m = np.ascontiguousarray(mass, np.float64).ravel()
+        q = np.ascontiguousarray(tm, np.float64).ravel()
+        out = np.zeros_like(m)
+        P = C.POINTER(_d)
+        self.L.orc_heat_diffuse(C.byref(p), m.ctypes.data_as(P), q.ctypes.data_as(P), out.ctypes.data_as(P), float(dt))
+        return out
 
     def metrics(self, case: dict, state: Dict[str, np.ndarray]) -> dict:
         p = orc_params(case)
@@ -234,6 +248,9 @@ class RefKern:
         L.ref_stats.argtypes = [C.POINTER(OrcState), C.POINTER(_d)]
         L.ref_asb_heat.restype = _i32
         L.ref_asb_heat.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcState), _d]
+        L.ref_heat_diffuse.restype = _i32
+        L.ref_heat_diffuse.argtypes = [C.POINTER(OrcParams), C.POINTER(_d), C.POINTER(_d), _d]
+        L.ref_heat_last_error.restype = C.c_char_p
         L.ref_bench.restype = _i32
         L.ref_bench.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcState), C.POINTER(OrcTool), _d, _i32, _i32,
                                 C.POINTER(_d)]
@@ -260,6 +277,17 @@ class RefKern:
         if rc != 0:
             raise RuntimeError(f"reference shear pass failed ({rc}): {self.L.ref_last_error().decode()}")
         return b.result()
+
+    def heat_diffuse(self, case: dict, mass: np.ndarray, tm: np.ndarray, dt: float) -> np.ndarray:
+        """The reference's mpmDiffuseTemperatureKernel once: returns its new T m."""
+        p = orc_params(case)
+        m = np.ascontiguousarray(mass, np.float64).ravel()
+        q = np.ascontiguousarray(tm, np.float64).ravel().copy()
+        P = C.POINTER(_d)
+        rc = self.L.ref_heat_diffuse(C.byref(p), m.ctypes.data_as(P), q.ctypes.data_as(P), float(dt))
+        if rc != 0:
+            raise RuntimeError(f"reference diffusion failed ({rc}): {self.L.ref_heat_last_error().decode()}")
+        return q
 
     def stats(self, case: dict, state: Dict[str, np.ndarray]) -> np.ndarray:
         b = _Bound(case, state)

@@ -14,6 +14,13 @@ kernels/asb_heating.npz holds one pass of the reference's adiabatic shear
 kernels (detectShearBandsKernel + applyAdiabaticHeatingKernel) over crafted
 particles that reach every branch (asb_pass_inputs); it is written when no
 scenario is named or when "asb_pass" is.
+
+kernels/heat_diffusion.npz holds one launch of the reference's grid heat
+diffusion kernel (mpmDiffuseTemperatureKernel, src/MPMWorkpieceSolver.cu) on a
+crafted grid (heat_pass_inputs); written when no scenario is named or when
+"heat_pass" is.  The kernel updates the grid in place, so in general its result
+depends on the thread schedule; on this grid every node it updates (mass >=
+1e-15) has only neighbours it never updates, so the result is deterministic.
 """
 from __future__ import annotations
 
@@ -70,6 +77,41 @@ def asb_pass_inputs():
     return case, st
 
 
+HEAT_DT = 1e-6
+
+
+def heat_pass_inputs():
+    """A 12x10x8 grid for one diffusion step: nodes of even parity i+j+k carry
+    1e-9..1e-8 kg (updated), a few of them below 1e-15 (kept); odd nodes carry
+    none (an empty neighbour counts as T = 0), 1e-16 or 1e-20 kg (never
+    updated).  Temperatures 300..1500 on every massive node; alpha dt / dx^2 =
+    0.05."""
+    case, _ = asb_pass_inputs()
+    p = case["params"]
+    nx, ny, nz, dx = 12, 10, 8, 1e-4
+    alpha = 0.05 * dx * dx / HEAT_DT
+    p.update(nx=nx, ny=ny, nz=nz, dx=dx, heat_conduction=1,
+             thermal_conductivity=alpha * p["rho_phys"] * p["cp"])
+    rng = np.random.default_rng(31)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    even = ((i + j + k) % 2 == 0).ravel()
+    n = nx * ny * nz
+    mass = np.where(even, rng.uniform(1e-9, 1e-8, n), rng.choice([0.0, 0.0, 1e-16, 1e-20], n))
+    mass = np.where(even & (rng.uniform(0, 1, n) < 0.05), 1e-16, mass)
+    T = rng.uniform(300.0, 1500.0, n)
+    return case, mass, T * mass
+
+
+def write_heat_pass(rk, outdir: Path) -> None:
+    case, mass, tm = heat_pass_inputs()
+    out = rk.heat_diffuse(case, mass, tm, HEAT_DT)
+    d = outdir / "kernels"
+    d.mkdir(parents=True, exist_ok=True)
+    np.savez_compressed(d / "heat_diffusion.npz", mass=mass, tm_in=tm, tm_out=out, dt=np.array(HEAT_DT))
+    print(f"heat_pass: nodes={len(mass)} updated={int((mass >= 1e-15).sum())} "
+          f"changed={int((out != tm).sum())}")
+
+
 def write_asb_pass(rk, outdir: Path) -> None:
     case, st = asb_pass_inputs()
     out = rk.asb_heat(case, st, ASB_DT)
@@ -87,6 +129,8 @@ def main(outdir: Path, names=None) -> None:
     outdir.mkdir(parents=True, exist_ok=True)
     if not names or "asb_pass" in names:
         write_asb_pass(rk, outdir)
+    if not names or "heat_pass" in names:
+        write_heat_pass(rk, outdir)
     for name, fn in SCENARIOS.items():
         if names and name not in names:
             continue

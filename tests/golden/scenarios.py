@@ -121,6 +121,24 @@ def adiabatic_shear():
     return case, st, n, None
 
 
+def heat_conduction():
+    """Grid heat conduction on (MPMWorkpieceSolver's scatter, diffusion and
+    gather on this solver's weights): the plastic_damage_chip tool path with
+    hot spots (up to 600 K above ambient) and a conductivity that makes
+    alpha dt / dx^2 = 0.05, so that both the diffusion step and the
+    temperature gather move temperatures.  The reference's MPMSolver conducts
+    no heat, so this scenario is checked against the oracle only."""
+    case, st, n, _ = plastic_damage_chip()
+    p = case["params"]
+    alpha = 0.05 * p["dx"] ** 2 / case["dt"]
+    p.update(heat_conduction=1, thermal_conductivity=alpha * p["rho_phys"] * p["cp"])
+    rng = np.random.default_rng(13)
+    nn = len(st["x"])
+    hot = rng.uniform(0, 1, nn) < 0.2
+    st["temperature"] = p["Tamb"] + np.where(hot, rng.uniform(0.0, 600.0, nn), 0.0)
+    return case, st, n, None
+
+
 SCENARIOS = {
     "elastic_raster": elastic_raster,
     "plastic_damage_chip": plastic_damage_chip,
@@ -128,3 +146,11 @@ SCENARIOS = {
     "lod_kinematic_extf": lod_kinematic_extf,
     "adiabatic_shear": adiabatic_shear,
 }
+
+# Scenarios of this build's extensions that the reference's MPMSolver does not
+# have: parity against the oracle only (no reference-kernel fixture).
+ORACLE_ONLY = {
+    "heat_conduction": heat_conduction,
+}
+
+PARITY_SCENARIOS = {**SCENARIOS, **ORACLE_ONLY}

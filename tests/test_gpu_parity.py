@@ -20,7 +20,7 @@ import pytest
 from conftest import max_rel
 
 sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
-from scenarios import SCENARIOS  # noqa: E402
+from scenarios import PARITY_SCENARIOS, SCENARIOS  # noqa: E402
 
 from mpm_b200 import Solver, capi as A, workpiece as W  # noqa: E402
 
@@ -81,7 +81,7 @@ def oracle_runs(oracle):
 
     def get(name):
         if name not in cache:
-            case, st, n, extf = SCENARIOS[name]()
+            case, st, n, extf = PARITY_SCENARIOS[name]()
             ref, rc = oracle.step(case, st, n, extf=extf)
             assert rc == 0
             cache[name] = (case, st, n, extf, ref)
@@ -91,7 +91,7 @@ def oracle_runs(oracle):
 
 
 @pytest.mark.parametrize("sched", [A.SCHED_FUSED, A.SCHED_SPLIT])
-@pytest.mark.parametrize("name", list(SCENARIOS))
+@pytest.mark.parametrize("name", list(PARITY_SCENARIOS))
 def test_fp64_matches_oracle(name, sched, oracle_runs):
     case, st, n, extf, ref = oracle_runs(name)
     out = run_ours(case, st, n, prec=A.PREC_F64, sched=sched)
@@ -102,7 +102,7 @@ def test_fp64_matches_oracle(name, sched, oracle_runs):
     assert not bad, bad
 
 
-@pytest.mark.parametrize("name", list(SCENARIOS))
+@pytest.mark.parametrize("name", list(PARITY_SCENARIOS))
 def test_fp32_matches_oracle(name, oracle_runs):
     case, st, n, extf, ref = oracle_runs(name)
     out = run_ours(case, st, n, prec=A.PREC_F32, sched=A.SCHED_FUSED)
