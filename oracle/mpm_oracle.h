@@ -133,6 +133,37 @@ void orc_asb_heat(const orc_params *p, orc_state *s, double dt);
  * node temperatures, as orc_step runs it between the grid update and g2p. */
 void orc_heat_diffuse(const orc_params *p, const double *mass, const double *tm, double *tn, double dt);
 
+/* A voxel signed-distance grid of the tool (ToolSDF, src/ToolSDF.cu):
+ * v[ix + nx (iy + ny iz)] is the distance at the centre of voxel (ix,iy,iz),
+ * o + (i + 1/2) voxel, negative inside the tool. */
+typedef struct orc_sdf_grid {
+    int32_t nx, ny, nz;
+    int32_t _pad;
+    const float *v;
+    float ox, oy, oz, voxel;
+} orc_sdf_grid;
+
+/* Arguments of xpbdContactSDFKernel (src/ContactSolver.cu:797-813): the tool
+ * transform (world -> SDF rest frame: translate by -c, rotate by -angle about
+ * z), contact radius, friction, heat partition, dt, and the workpiece's
+ * specific heat, physical density and melting temperature. */
+typedef struct orc_contact_sdf_args {
+    float cx, cy, cz, cos_a, sin_a;
+    float radius, friction, heat_partition, dt;
+    float _pad;
+    double cp, rho_phys, Tm;
+} orc_contact_sdf_args;
+
+/* A 3D float texture fetch with trilinear filtering, clamp addressing and
+ * unnormalised coordinates, as the texture unit computes it (the weights are
+ * held with 8 fractional bits; the exact split is in mpm_oracle.c). */
+float orc_tex3d(const orc_sdf_grid *g, float x, float y, float z);
+
+/* One pass of xpbdContactSDFKernel over the particles (not INACTIVE or
+ * FIXED); count, friction work and normal force summed as its metrics. */
+void orc_contact_sdf(const orc_sdf_grid *g, const orc_contact_sdf_args *a, orc_state *s, int64_t *count,
+                     double *heat, double *force);
+
 /* Size in doubles of the grid scratch that orc_step needs. */
 int64_t orc_grid_doubles(const orc_params *p);
 

@@ -54,6 +54,34 @@ class OrcState(C.Structure):
     ]
 
 
+class OrcSdfGrid(C.Structure):
+    _fields_ = [("nx", _i32), ("ny", _i32), ("nz", _i32), ("_pad", _i32), ("v", _vp), ("ox", C.c_float),
+                ("oy", C.c_float), ("oz", C.c_float), ("voxel", C.c_float)]
+
+
+class OrcContactArgs(C.Structure):
+    _fields_ = [(k, C.c_float) for k in ("cx", "cy", "cz", "cos_a", "sin_a", "radius", "friction", "heat_partition",
+                                         "dt", "_pad")] + [("cp", _d), ("rho_phys", _d), ("Tm", _d)]
+
+
+def sdf_grid(sdf: dict):
+    """(OrcSdfGrid, keep-alive array) from {"v": float32 [nz, ny, nx], "origin": (x, y, z), "voxel": h}."""
+    v = np.ascontiguousarray(sdf["v"], dtype=np.float32)
+    g = OrcSdfGrid()
+    g.nz, g.ny, g.nx = v.shape
+    g.v = v.ctypes.data
+    g.ox, g.oy, g.oz = (float(c) for c in sdf["origin"])
+    g.voxel = float(sdf["voxel"])
+    return g, v
+
+
+def contact_args(a: dict) -> OrcContactArgs:
+    o = OrcContactArgs()
+    for k in ("cx", "cy", "cz", "cos_a", "sin_a", "radius", "friction", "heat_partition", "dt", "cp", "rho_phys", "Tm"):
+        setattr(o, k, float(a[k]))
+    return o
+
+
 class OrcTool(C.Structure):
     _fields_ = [("n", _i32), ("_pad", _i32), ("ox", _vp), ("oy", _vp), ("oz", _vp)]
 
@@ -184,6 +212,11 @@ class Oracle:
         L.orc_asb_heat.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcState), _d]
         L.orc_heat_diffuse.restype = None
         L.orc_heat_diffuse.argtypes = [C.POINTER(OrcParams), C.POINTER(_d), C.POINTER(_d), C.POINTER(_d), _d]
+        L.orc_tex3d.restype = C.c_float
+        L.orc_tex3d.argtypes = [C.POINTER(OrcSdfGrid), C.c_float, C.c_float, C.c_float]
+        L.orc_contact_sdf.restype = None
+        L.orc_contact_sdf.argtypes = [C.POINTER(OrcSdfGrid), C.POINTER(OrcContactArgs), C.POINTER(OrcState),
+                                      C.POINTER(_i64), C.POINTER(_d), C.POINTER(_d)]
         self.L = L
 
     def step(self, case: dict, state: Dict[str, np.ndarray], nsteps: int, step0: int = 0, t0: float = 0.0,
@@ -212,6 +245,21 @@ class Oracle:
         P = C.POINTER(_d)
         self.L.orc_heat_diffuse(C.byref(p), m.ctypes.data_as(P), q.ctypes.data_as(P), out.ctypes.data_as(P), float(dt))
         return out
+
+    def tex3d(self, sdf: dict, xyz: np.ndarray) -> np.ndarray:
+        """Emulated texture fetches at voxel coordinates xyz [n, 3]."""
+        g, keep = sdf_grid(sdf)
+        q = np.asarray(xyz, np.float32).reshape(-1, 3)
+        return np.array([self.L.orc_tex3d(C.byref(g), float(a), float(b), float(c)) for a, b, c in q], np.float32)
+
+    def contact_sdf(self, case: dict, state: Dict[str, np.ndarray], sdf: dict, args: dict):
+        """One xpbdContactSDFKernel pass: (state after, (count, friction work, normal force))."""
+        g, keep = sdf_grid(sdf)
+        b = _Bound(case, state)
+        a = contact_args(args)
+        cnt, heat, force = _i64(), _d(), _d()
+        self.L.orc_contact_sdf(C.byref(g), C.byref(a), C.byref(b.state), C.byref(cnt), C.byref(heat), C.byref(force))
+        return b.result(), (cnt.value, heat.value, force.value)
 
     def metrics(self, case: dict, state: Dict[str, np.ndarray]) -> dict:
         p = orc_params(case)
@@ -251,6 +299,12 @@ class RefKern:
         L.ref_heat_diffuse.restype = _i32
         L.ref_heat_diffuse.argtypes = [C.POINTER(OrcParams), C.POINTER(_d), C.POINTER(_d), _d]
         L.ref_heat_last_error.restype = C.c_char_p
+        L.ref_contact_last_error.restype = C.c_char_p
+        L.ref_tex_probe.restype = _i32
+        L.ref_tex_probe.argtypes = [C.POINTER(OrcSdfGrid), _vp, _i32, _vp]
+        L.ref_contact_sdf.restype = _i32
+        L.ref_contact_sdf.argtypes = [C.POINTER(OrcSdfGrid), C.POINTER(OrcContactArgs), C.POINTER(OrcState),
+                                      C.POINTER(_i64), C.POINTER(_d), C.POINTER(_d)]
         L.ref_bench.restype = _i32
         L.ref_bench.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcState), C.POINTER(OrcTool), _d, _i32, _i32,
                                 C.POINTER(_d)]
@@ -288,6 +342,28 @@ class RefKern:
         if rc != 0:
             raise RuntimeError(f"reference diffusion failed ({rc}): {self.L.ref_heat_last_error().decode()}")
         return q
+
+    def tex_probe(self, sdf: dict, xyz: np.ndarray) -> np.ndarray:
+        """Hardware texture fetches (the reference's texture setup) at voxel coordinates xyz [n, 3]."""
+        g, keep = sdf_grid(sdf)
+        q = np.ascontiguousarray(np.asarray(xyz, np.float32).reshape(-1, 3))
+        out = np.zeros(len(q), np.float32)
+        rc = self.L.ref_tex_probe(C.byref(g), q.ctypes.data, len(q), out.ctypes.data)
+        if rc != 0:
+            raise RuntimeError(self.L.ref_contact_last_error().decode())
+        return out
+
+    def contact_sdf(self, case: dict, state: Dict[str, np.ndarray], sdf: dict, args: dict):
+        """The reference's xpbdContactSDFKernel once: (state after, (count, friction work, normal force))."""
+        g, keep = sdf_grid(sdf)
+        b = _Bound(case, state)
+        a = contact_args(args)
+        cnt, heat, force = _i64(), _d(), _d()
+        rc = self.L.ref_contact_sdf(C.byref(g), C.byref(a), C.byref(b.state), C.byref(cnt), C.byref(heat),
+                                    C.byref(force))
+        if rc != 0:
+            raise RuntimeError(self.L.ref_contact_last_error().decode())
+        return b.result(), (cnt.value, heat.value, force.value)
 
     def stats(self, case: dict, state: Dict[str, np.ndarray]) -> np.ndarray:
         b = _Bound(case, state)

@@ -15,6 +15,13 @@ kernels (detectShearBandsKernel + applyAdiabaticHeatingKernel) over crafted
 particles that reach every branch (asb_pass_inputs); it is written when no
 scenario is named or when "asb_pass" is.
 
+kernels/tex_probe.npz holds hardware texture fetches through the reference's
+SDF texture setup (ToolSDF::createTexture) at crafted coordinates, and
+kernels/contact_sdf.npz one launch of the reference's xpbdContactSDFKernel
+(src/ContactSolver.cu) on a sampled cylinder SDF with crafted particles
+(tex_probe_inputs, contact_pass_inputs); written when no scenario is named or
+when "contact_pass" is.
+
 kernels/heat_diffusion.npz holds one launch of the reference's grid heat
 diffusion kernel (mpmDiffuseTemperatureKernel, src/MPMWorkpieceSolver.cu) on a
 crafted grid (heat_pass_inputs); written when no scenario is named or when
@@ -80,6 +87,75 @@ def asb_pass_inputs():
 HEAT_DT = 1e-6
 
 
+def tex_probe_inputs():
+    """Random texels on a 9x7x5 grid and fetch points: random ones (some
+    outside the grid, where clamping applies), texel centres and integers."""
+    rng = np.random.default_rng(41)
+    v = rng.uniform(-1.0, 1.0, (5, 7, 9)).astype(np.float32)
+    n = np.array([9, 7, 5], np.float32)
+    pts = [rng.uniform(-1.5, 1.0, (3000, 3)) * 1.0 + rng.uniform(0, 1, (3000, 3)) * (n + 1.0)]
+    pts.append(rng.integers(0, 9, (200, 3)) + 0.5)
+    pts.append(rng.integers(-1, 10, (200, 3)).astype(np.float64))
+    xyz = np.concatenate(pts).astype(np.float32)
+    return {"v": v, "origin": (0.0, 0.0, 0.0), "voxel": 1.0}, xyz
+
+
+def cylinder_sdf(R: float, voxel: float, dims, origin):
+    """A cylinder of radius R along y, centred on the rest frame's origin,
+    sampled at voxel centres (float32 [nz, ny, nx])."""
+    nx, ny, nz = dims
+    xc = origin[0] + (np.arange(nx) + 0.5) * voxel
+    zc = origin[2] + (np.arange(nz) + 0.5) * voxel
+    r = np.sqrt(xc[None, :] ** 2 + zc[:, None] ** 2) - R
+    return np.ascontiguousarray(np.broadcast_to(r[:, None, :], (nz, ny, nx)), dtype=np.float32)
+
+
+def contact_pass_inputs():
+    """A 40x20x40 cylinder SDF (R = 0.3 mm, 20 um voxels) under a tool
+    transform (translated, rotated 0.3 rad about z) and 4000 particles within
+    +-3 voxels of its surface, a few outside the grid, all statuses; contact
+    radius 2 voxels, friction 0.3, heat partition 0.5, dt 1e-5 (so that the
+    friction cap binds for some particles and not for others)."""
+    case, _ = asb_pass_inputs()
+    voxel, R = 2e-5, 3e-4
+    dims = (40, 20, 40)
+    origin = (-20 * voxel, -10 * voxel, -20 * voxel)
+    sdf = {"v": cylinder_sdf(R, voxel, dims, origin), "origin": origin, "voxel": voxel}
+    ang = 0.3
+    args = dict(cx=1e-3, cy=5e-4, cz=8e-4, cos_a=np.cos(ang), sin_a=np.sin(ang), radius=2 * voxel, friction=0.3,
+                heat_partition=0.5, dt=1e-5, cp=526.3, rho_phys=4430.0, Tm=1878.0)
+    rng = np.random.default_rng(43)
+    n = 4000
+    th = rng.uniform(0, 2 * np.pi, n)
+    r = R + rng.uniform(-3, 3, n) * voxel
+    lx, ly, lz = r * np.cos(th), rng.uniform(-8, 8, n) * voxel, r * np.sin(th)
+    ly[:40] = 12 * voxel                     # outside the grid along y
+    wx = lx * args["cos_a"] - ly * args["sin_a"] + args["cx"]
+    wy = lx * args["sin_a"] + ly * args["cos_a"] + args["cy"]
+    wz = lz + args["cz"]
+    z = np.zeros(n)
+    eye = np.tile(np.eye(3).reshape(1, 9), (n, 1))
+    st = dict(x=wx, y=wy, z=wz, vx=rng.uniform(-3, 3, n), vy=rng.uniform(-3, 3, n), vz=rng.uniform(-3, 3, n),
+              F=eye.copy(), Fp=eye.copy(), C=np.zeros((n, 9)), stress=np.zeros((n, 6)), backstress=np.zeros((n, 6)),
+              plastic_strain=z.copy(), strain_rate=z.copy(), temperature=300.0 + rng.uniform(0, 500, n),
+              damage=z.copy(), residual_stress=z.copy(),
+              status=rng.choice([0, 0, 0, 0, 0, 0, 1, 2, 3, 4], n).astype(np.int32), id=np.arange(n, dtype=np.int32))
+    return case, st, sdf, args
+
+
+def write_contact_pass(rk, outdir: Path) -> None:
+    d = outdir / "kernels"
+    d.mkdir(parents=True, exist_ok=True)
+    sdf, xyz = tex_probe_inputs()
+    np.savez_compressed(d / "tex_probe.npz", v=sdf["v"], xyz=xyz, out=rk.tex_probe(sdf, xyz))
+    case, st, sdf, args = contact_pass_inputs()
+    out, (cnt, heat, force) = rk.contact_sdf(case, st, sdf, args)
+    keys = ("x", "y", "z", "vx", "vy", "vz", "temperature")
+    np.savez_compressed(d / "contact_sdf.npz", **{f"out_{k}": out[k] for k in keys},
+                        metrics=np.array([cnt, heat, force], np.float64))
+    print(f"contact_pass: n={len(st['x'])} contacts={cnt} work={heat:.3e} force={force:.3e}")
+
+
 def heat_pass_inputs():
     """A 12x10x8 grid for one diffusion step: nodes of even parity i+j+k carry
     1e-9..1e-8 kg (updated), a few of them below 1e-15 (kept); odd nodes carry
@@ -131,6 +207,8 @@ def main(outdir: Path, names=None) -> None:
         write_asb_pass(rk, outdir)
     if not names or "heat_pass" in names:
         write_heat_pass(rk, outdir)
+    if not names or "contact_pass" in names:
+        write_contact_pass(rk, outdir)
     for name, fn in SCENARIOS.items():
         if names and name not in names:
             continue
