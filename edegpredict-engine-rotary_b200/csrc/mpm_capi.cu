@@ -244,6 +244,16 @@ mpm_status mpm_batch_download(mpm_handle* h, int32_t inst, mpm_particles_soa* ho
     return ret(h, h->eng->download(inst, host));
 }
 
+mpm_status mpm_set_tool_sdf(mpm_handle* h, const mpm_tool_sdf* sdf) {
+    NEED_H(h);
+    return ret(h, h->eng->set_tool_sdf(0, sdf));
+}
+
+mpm_status mpm_batch_set_tool_sdf(mpm_handle* h, int32_t inst, const mpm_tool_sdf* sdf) {
+    NEED_I(h, inst);
+    return ret(h, h->eng->set_tool_sdf(inst, sdf));
+}
+
 mpm_status mpm_batch_set_tool(mpm_handle* h, int32_t inst, const mpm_tool_desc* tool) {
     NEED_I(h, inst);
     return ret(h, h->eng->set_tool(inst, tool));

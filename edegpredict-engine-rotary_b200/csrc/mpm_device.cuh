@@ -117,6 +117,12 @@ template <typename R> struct alignas(128) Inst {
     double heat_c;
     R Tamb;
     int64_t gbase;                 // first node of this instance in the batch grid arrays
+    // voxel tool SDF for the contact (sdf_on = 0: the analytic SDF): texture, voxels per axis,
+    // voxel (0,0,0) corner and edge in the tool frame, the frame's rotation about z
+    int sdf_on;
+    unsigned long long sdf_tex;
+    int sdf_n[3];
+    float sdf_o[3], sdf_vox, sdf_cos, sdf_sin;
     // external force for one step (radius 0: none)
     double ext_c[3], ext_r, ext_f[3];
     int64_t pbase;                 // first particle slot of this instance in the batch arrays

@@ -649,6 +649,12 @@ class Engine final : public EngineBase {
         d.contact_hp = p.contact_heat_partition;
         d.rho_phys = p.rho_phys;
         // MPMWorkpieceSolver::step: alpha = k / (rho cp) (src/MPMWorkpieceSolver.cu:751-752)
+        d.sdf_on = x.sdf ? 1 : 0;
+        if (x.sdf) {
+            d.sdf_tex = (unsigned long long)x.sdf->tex;
+            for (int a = 0; a < 3; ++a) { d.sdf_n[a] = x.sdf->n[a]; d.sdf_o[a] = x.sdf->origin[a]; }
+            d.sdf_vox = x.sdf->voxel; d.sdf_cos = x.sdf->cos_a; d.sdf_sin = x.sdf->sin_a;
+        }
         d.heat_on = p.heat_conduction ? 1 : 0;
         d.heat_c = p.thermal_conductivity / (p.rho_phys * p.cp) * x.dt / (p.dx * p.dx);
         d.Tamb = (R)p.Tamb;
@@ -901,6 +907,50 @@ class Engine final : public EngineBase {
 
     // ---------------------------------------------------------------- tool
 
+    // The voxel tool SDF as a 3D texture set up as ToolSDF::createTexture does
+    // (src/ToolSDF.cu:534-567): float texels, trilinear filtering, clamp
+    // addressing, unnormalised coordinates.
+    mpm_status set_tool_sdf(int i, const mpm_tool_sdf* s) override {
+        InstHost& x = I[i];
+        CK(cudaStreamSynchronize(st));
+        drop_graphs();
+        if (!s) {
+            x.sdf.reset();
+            return push_insts();
+        }
+        if (!s->values || s->nx < 2 || s->ny < 2 || s->nz < 2 || s->nx > 1024 || s->ny > 1024 || s->nz > 1024 ||
+            !(s->voxel > 0.0f) || !std::isfinite(s->angle)) {
+            err = "tool SDF: values, 2..1024 voxels per axis and a positive voxel edge";
+            return MPM_INVALID_ARG;
+        }
+        auto t = std::make_shared<ToolSdfTex>();
+        cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
+        const cudaExtent ext = make_cudaExtent(s->nx, s->ny, s->nz);
+        CK(cudaMalloc3DArray(&t->arr, &ch, ext));
+        cudaMemcpy3DParms cp = {};
+        cp.srcPtr = make_cudaPitchedPtr((void*)s->values, s->nx * sizeof(float), s->nx, s->ny);
+        cp.dstArray = t->arr;
+        cp.extent = ext;
+        cp.kind = cudaMemcpyHostToDevice;
+        CK(cudaMemcpy3D(&cp));
+        cudaResourceDesc rd = {};
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = t->arr;
+        cudaTextureDesc td = {};
+        td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 0;
+        CK(cudaCreateTextureObject(&t->tex, &rd, &td, nullptr));
+        t->n[0] = s->nx; t->n[1] = s->ny; t->n[2] = s->nz;
+        for (int a = 0; a < 3; ++a) t->origin[a] = s->origin[a];
+        t->voxel = s->voxel;
+        t->cos_a = std::cos(s->angle);
+        t->sin_a = std::sin(s->angle);
+        x.sdf = std::move(t);
+        return push_insts();
+    }
+
     mpm_status set_tool(int i, const mpm_tool_desc* t) override {
         InstHost& x = I[i];
         if (!t || t->mode < MPM_TOOL_NONE || t->mode > MPM_TOOL_SDF_SLIP || t->shape < 0 || t->shape > 1) {
@@ -1001,7 +1051,7 @@ class Engine final : public EngineBase {
         const int cps = ctas_per_sm;
         int xk = 0, heat = 0;
         for (const InstHost& x : I) {
-            xk |= (x.p.asb_enabled || x.p.heat_conduction) ? 1 : 0;
+            xk |= (x.p.asb_enabled || x.p.heat_conduction || (x.sdf && x.p.contact_every > 0)) ? 1 : 0;
             heat |= x.p.heat_conduction ? 1 : 0;
         }
         // the grid buffer a P2G launch writes starts at zero, and so does its T m buffer

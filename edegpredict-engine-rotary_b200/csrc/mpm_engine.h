@@ -17,6 +17,19 @@
 
 namespace mpmb {
 
+// A tool SDF as a 3D texture (trilinear filtering, clamp addressing,
+// unnormalised coordinates), shared by the copies of an instance record.
+struct ToolSdfTex {
+    cudaArray_t arr = nullptr;
+    cudaTextureObject_t tex = 0;
+    int n[3] = {0, 0, 0};
+    float origin[3] = {0, 0, 0}, voxel = 0.0f, cos_a = 1.0f, sin_a = 0.0f;
+    ~ToolSdfTex() {
+        if (tex) cudaDestroyTextureObject(tex);
+        if (arr) cudaFreeArray(arr);
+    }
+};
+
 struct InstHost {
     mpm_params p;
     mpm_tool_desc tool;
@@ -31,6 +44,7 @@ struct InstHost {
     double ext_c[3] = {0, 0, 0}, ext_r = 0.0, ext_f[3] = {0, 0, 0};
     bool ext_pending = false;
     double tool_t0 = 0.0;   // time at which the tool descriptor was set
+    std::shared_ptr<ToolSdfTex> sdf;   // voxel tool SDF for the contact (null: analytic SDF)
     int fresh = 0;          // particles uploaded or generated, not yet binned
 };
 
@@ -44,6 +58,7 @@ class EngineBase {
     virtual mpm_status download(int inst, mpm_particles_soa* host) = 0;
     virtual mpm_status export_aos(int inst, void* dst, int64_t bytes) = 0;
     virtual mpm_status set_tool(int inst, const mpm_tool_desc* t) = 0;
+    virtual mpm_status set_tool_sdf(int inst, const mpm_tool_sdf* s) = 0;
     virtual mpm_status step(int32_t nsteps, const double* dt_per_inst) = 0;
     virtual mpm_status metrics(int inst, mpm_metrics* out) = 0;
     virtual mpm_status set_mass_scaling(int inst, double f) = 0;

@@ -694,6 +694,88 @@ __device__ __noinline__ ContactOut particle_contact(const Inst<R>& P, double wx,
     return o;
 }
 
+// Particle-side contact on the voxel tool SDF, restating xpbdContactSDFKernel
+// (reference src/ContactSolver.cu:797-923) operation by operation in its float
+// and double arithmetic: world -> tool frame about the tool's reference point
+// pe (:825-829), voxel coordinates and the grid test (:832-840), the distance
+// through the texture (:843-845), the normal from central differences half a
+// voxel apart (:848-859), push-out to the contact radius (:863-869), removal
+// of an approaching normal velocity (:872-877), Coulomb friction with the
+// tangential velocity taken before that removal (:881-898), heating by
+// (1 - heat partition) of the friction work with T <= Tm (:901-916).  The
+// float operations are written as round-to-nearest intrinsics so that none is
+// contracted into a fused multiply-add.
+template <typename R>
+__device__ __noinline__ ContactOut particle_contact_sdf(const Inst<R>& P, double wx, double wy, double wz, double pe0,
+                                                        double pe1, double pe2, R& vx, R& vy, R& vz, R& dT) {
+    ContactOut o{false, {0.0, 0.0, 0.0}, 0.0, 0.0};
+    const cudaTextureObject_t tex = (cudaTextureObject_t)P.sdf_tex;
+    const float dx = __fsub_rn((float)wx, (float)pe0), dy = __fsub_rn((float)wy, (float)pe1);
+    const float lx = __fadd_rn(__fmul_rn(dx, P.sdf_cos), __fmul_rn(dy, P.sdf_sin));
+    const float ly = __fadd_rn(__fmul_rn(-dx, P.sdf_sin), __fmul_rn(dy, P.sdf_cos));
+    const float lz = __fsub_rn((float)wz, (float)pe2);
+    const float tx = __fdiv_rn(__fsub_rn(lx, P.sdf_o[0]), P.sdf_vox);
+    const float ty = __fdiv_rn(__fsub_rn(ly, P.sdf_o[1]), P.sdf_vox);
+    const float tz = __fdiv_rn(__fsub_rn(lz, P.sdf_o[2]), P.sdf_vox);
+    if (tx < 0.0f || ty < 0.0f || tz < 0.0f || tx > (float)(P.sdf_n[0] - 1) || ty > (float)(P.sdf_n[1] - 1) ||
+        tz > (float)(P.sdf_n[2] - 1))
+        return o;
+    const float rad = (float)P.contact_r;
+    const float sdf = tex3D<float>(tex, tx, ty, tz);
+    if (sdf >= rad) return o;
+    const float eps = 0.5f;
+    const float den = __fmul_rn(__fmul_rn(eps, 2.0f), P.sdf_vox);
+    const float gx = __fdiv_rn(__fsub_rn(tex3D<float>(tex, __fadd_rn(tx, eps), ty, tz),
+                                         tex3D<float>(tex, __fsub_rn(tx, eps), ty, tz)), den);
+    const float gy = __fdiv_rn(__fsub_rn(tex3D<float>(tex, tx, __fadd_rn(ty, eps), tz),
+                                         tex3D<float>(tex, tx, __fsub_rn(ty, eps), tz)), den);
+    const float gz = __fdiv_rn(__fsub_rn(tex3D<float>(tex, tx, ty, __fadd_rn(tz, eps)),
+                                         tex3D<float>(tex, tx, ty, __fsub_rn(tz, eps))), den);
+    const float glen = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy)), __fmul_rn(gz, gz)));
+    if (glen < 1e-10f) return o;
+    const float nx = __fdiv_rn(gx, glen), ny = __fdiv_rn(gy, glen), nz = __fdiv_rn(gz, glen);
+    const float pen = __fsub_rn(rad, sdf);
+    if (pen <= 0.0f) return o;
+    o.hit = true;
+    o.dxi[0] = (double)__fmul_rn(nx, pen) / P.dx;
+    o.dxi[1] = (double)__fmul_rn(ny, pen) / P.dx;
+    o.dxi[2] = (double)__fmul_rn(nz, pen) / P.dx;
+    double ux = (double)vx, uy = (double)vy, uz = (double)vz;
+    const float vdn = (float)__dadd_rn(__dadd_rn(__dmul_rn(ux, (double)nx), __dmul_rn(uy, (double)ny)),
+                                       __dmul_rn(uz, (double)nz));
+    if (vdn < 0.0f) {
+        ux = __dsub_rn(ux, (double)__fmul_rn(vdn, nx));
+        uy = __dsub_rn(uy, (double)__fmul_rn(vdn, ny));
+        uz = __dsub_rn(uz, (double)__fmul_rn(vdn, nz));
+    }
+    const float tvx = __fsub_rn((float)ux, __fmul_rn(vdn, nx));
+    const float tvy = __fsub_rn((float)uy, __fmul_rn(vdn, ny));
+    const float tvz = __fsub_rn((float)uz, __fmul_rn(vdn, nz));
+    const float tvm = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(tvx, tvx), __fmul_rn(tvy, tvy)), __fmul_rn(tvz, tvz)));
+    const float pm = (float)P.pmass, dt = (float)P.dt;
+    const float nf = (tvm > 0.0f) ? fmaxf(__fdiv_rn(__fmul_rn(pm, pen), __fmul_rn(dt, dt)), 1e-15f) : 1e-15f;
+    const float fimp = __fmul_rn(__fmul_rn((float)P.contact_mu, nf), dt);
+    if (tvm > 0.0f && fimp > 0.0f) {
+        const float sc = fminf(1.0f, __fdiv_rn(__fdiv_rn(fimp, fmaxf(pm, 1e-15f)), tvm));
+        ux = __dsub_rn(ux, (double)__fmul_rn(tvx, sc));
+        uy = __dsub_rn(uy, (double)__fmul_rn(tvy, sc));
+        uz = __dsub_rn(uz, (double)__fmul_rn(tvz, sc));
+    }
+    const float fx = (float)ux, fy = (float)uy, fz = (float)uz;
+    const float slip = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy)), __fmul_rn(fz, fz)));
+    o.work = (double)__fmul_rn(__fmul_rn(nf, slip), dt);
+    o.force = (double)fmaxf(nf, 1e-15f);
+    const double heat = o.work * (1.0 - (double)(float)P.contact_hp);
+    if (heat > 0.0) {
+        const double pv = (double)P.pvol;
+        const double vol = pv > 1e-24 ? pv : (double)P.pmass / fmax((double)P.pmass / pv, 1.0);
+        const double mass_phys = fmax(P.rho_phys, 1.0) * fmax(vol, 1e-24);
+        dT = (R)fmin((double)dT + heat / (fmax(mass_phys, 1e-15) * P.cp), (double)P.dTmax);
+    }
+    vx = (R)ux; vy = (R)uy; vz = (R)uz;
+    return o;
+}
+
 // ------------------------------------------------------------------ the step kernel
 
 // Particles staged per pass and scatter payload per particle:
@@ -1124,7 +1206,15 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                             const double pe2 = da(P.tool_p0[2], dm(P.tool_v[2], ds(te, P.tool_t0)));
                             const double wx = P.ox + ((double)g0x + ((double)xi[0] + (double)lo[0])) * P.dx;
                             const double wz = P.oz + ((double)g0z + ((double)xi[2] + (double)lo[2])) * P.dx;
-                            const ContactOut co = particle_contact<R>(P, wx, wz, pe0, pe2, v[0], v[1], v[2], dT);
+                            ContactOut co;
+                            if (EXT && P.sdf_on) {
+                                // voxel tool SDF (the extension variant)
+                                const double pe1 = da(P.tool_p0[1], dm(P.tool_v[1], ds(te, P.tool_t0)));
+                                const double wy = P.oy + ((double)g0y + ((double)xi[1] + (double)lo[1])) * P.dx;
+                                co = particle_contact_sdf<R>(P, wx, wy, wz, pe0, pe1, pe2, v[0], v[1], v[2], dT);
+                            } else {
+                                co = particle_contact<R>(P, wx, wz, pe0, pe2, v[0], v[1], v[2], dT);
+                            }
                             if (co.hit) {
 #pragma unroll
                                 for (int a = 0; a < 3; ++a) {

@@ -43,6 +43,11 @@ class MpmParams(C.Structure):
     ]
 
 
+class MpmToolSdf(C.Structure):
+    _fields_ = [("nx", _i32), ("ny", _i32), ("nz", _i32), ("_pad", _i32), ("values", _vp),
+                ("origin", C.c_float * 3), ("voxel", C.c_float), ("angle", C.c_float), ("_pad2", C.c_float)]
+
+
 class MpmToolDesc(C.Structure):
     _fields_ = [
         ("mode", _i32), ("shape", _i32), ("position", _d * 3), ("velocity", _d * 3), ("radius", _d),
@@ -144,6 +149,8 @@ def lib() -> C.CDLL:
             "mpm_download": (_i32, [_vp, P(MpmParticlesSoa)]),
             "mpm_export_aos": (_i32, [_vp, _vp, _i64]),
             "mpm_set_tool": (_i32, [_vp, P(MpmToolDesc)]),
+            "mpm_set_tool_sdf": (_i32, [_vp, P(MpmToolSdf)]),
+            "mpm_batch_set_tool_sdf": (_i32, [_vp, _i32, P(MpmToolSdf)]),
             "mpm_step": (_i32, [_vp, _d, _i32]),
             "mpm_stable_dt": (_i32, [_vp, _d, P(_d)]),
             "mpm_sync_metrics": (_i32, [_vp, P(MpmMetrics)]),

@@ -112,6 +112,28 @@ class Solver:
         t = self.tool_desc(tool)
         self._check(self._lib.mpm_set_tool(self.h, C.byref(t)))
 
+    @staticmethod
+    def tool_sdf(sdf: Optional[dict]):
+        """MpmToolSdf from {"v": float32 [nz, ny, nx], "origin": (x, y, z), "voxel": h, "angle": a}
+        (the array is kept alive on the structure), or None."""
+        if sdf is None:
+            return None
+        v = np.ascontiguousarray(sdf["v"], dtype=np.float32)
+        s = A.MpmToolSdf()
+        s.nz, s.ny, s.nx = v.shape
+        s._v = v
+        s.values = v.ctypes.data
+        for i in range(3):
+            s.origin[i] = float(sdf["origin"][i])
+        s.voxel = float(sdf["voxel"])
+        s.angle = float(sdf.get("angle", 0.0))
+        return s
+
+    def set_tool_sdf(self, sdf: Optional[dict]) -> None:
+        """Voxel tool SDF for the particle-side contact (None: the analytic SDF)."""
+        s = self.tool_sdf(sdf)
+        self._check(self._lib.mpm_set_tool_sdf(self.h, C.byref(s) if s is not None else None))
+
     # ---------------------------------------------------------------- particles
     def init_box(self, c0, c1, ppc: int, seed: int, instance: int = 0, fixed_layers: int = 2, T0: float = 293.0,
                  tool: Optional[dict] = None) -> int:
@@ -242,6 +264,10 @@ class Batch(Solver):
     def set_tool_i(self, i: int, tool: dict) -> None:
         t = self.tool_desc(tool)
         self._check(self._lib.mpm_batch_set_tool(self.h, int(i), C.byref(t)))
+
+    def set_tool_sdf_i(self, i: int, sdf: Optional[dict]) -> None:
+        s = self.tool_sdf(sdf)
+        self._check(self._lib.mpm_batch_set_tool_sdf(self.h, int(i), C.byref(s) if s is not None else None))
 
     def upload_i(self, i: int, parts: Dict[str, np.ndarray], elem: int = 8) -> None:
         s, keep, n = soa_in(parts, elem)

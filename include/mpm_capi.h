@@ -222,6 +222,30 @@ mpm_status mpm_export_aos(mpm_handle *h, void *dst, int64_t dst_bytes);
 /* Replaces setToolNodes / setToolPosition (include/MPMSolver.cuh:86-89, :171). */
 mpm_status mpm_set_tool(mpm_handle *h, const mpm_tool_desc *tool);
 
+/*
+ * Voxel signed-distance field of the tool for the particle-side contact
+ * (mpm_params.contact_every > 0).  Replaces ToolSDF::build / createTexture
+ * (src/ToolSDF.cu:212-280, :534-567) and setToolTransform (:569-576): the
+ * values are the tool's signed distances (m, negative inside) at the voxel
+ * centres origin + (i + 1/2) voxel of the tool frame, whose origin follows the
+ * tool's reference point and which is rotated by `angle` about z.  The step
+ * then resolves contact as xpbdContactSDFKernel (src/ContactSolver.cu:797-923)
+ * does, sampling the field through a trilinear 3D texture like the
+ * reference's; without one it uses the analytic tool SDF.  values are copied
+ * (host memory, x fastest); NULL sdf removes the field.
+ */
+typedef struct mpm_tool_sdf {
+    int32_t nx, ny, nz;        /* voxels per axis, 2 .. 1024 */
+    int32_t _pad;
+    const float *values;
+    float origin[3];           /* corner of voxel (0,0,0) in the tool frame (m) */
+    float voxel;               /* voxel edge (m) */
+    float angle;               /* rotation of the tool frame about z (rad) */
+    float _pad2;
+} mpm_tool_sdf;
+
+mpm_status mpm_set_tool_sdf(mpm_handle *h, const mpm_tool_sdf *sdf);
+
 /* Replaces MPMSolver::step (src/MPMSolver.cu:1062-1168): nsteps steps of dt.
  * Asynchronous on the handle's stream. */
 mpm_status mpm_step(mpm_handle *h, double dt, int32_t nsteps);
@@ -287,6 +311,7 @@ mpm_status mpm_batch_init_box(mpm_handle *h, int32_t inst, const int32_t c0[3], 
 mpm_status mpm_batch_upload(mpm_handle *h, int32_t inst, const mpm_particles_soa *host, int64_t n);
 mpm_status mpm_batch_download(mpm_handle *h, int32_t inst, mpm_particles_soa *host);
 mpm_status mpm_batch_set_tool(mpm_handle *h, int32_t inst, const mpm_tool_desc *tool);
+mpm_status mpm_batch_set_tool_sdf(mpm_handle *h, int32_t inst, const mpm_tool_sdf *sdf);
 /* nsteps steps of every instance; dt[i] is instance i's step (n_instances values). */
 mpm_status mpm_batch_step(mpm_handle *h, const double *dt, int32_t nsteps);
 mpm_status mpm_batch_sync_metrics(mpm_handle *h, int32_t inst, mpm_metrics *out);

@@ -718,24 +718,27 @@ static float clampc(float x, int n) {
  * so that they sum to 1: z exactly (1 - c, c); within a z slice the x = 1 side
  * rounded and x = 0 the rest; within the x = 1 half the y = 1 corner rounded
  * and y = 0 the rest, within the x = 0 half the y = 0 corner rounded and
- * y = 1 the rest. */
+ * y = 1 the rest.  The texels are then summed with these weights; the unit's
+ * own sum carries a little less than exact precision, so the result here (the
+ * exact sum rounded once) can differ from it by one float ulp (1.4 % of the
+ * probe points). */
 float orc_tex3d(const orc_sdf_grid *g, float x, float y, float z) {
     const float xb = clampc(x, g->nx) - 0.5f, yb = clampc(y, g->ny) - 0.5f, zb = clampc(z, g->nz) - 0.5f;
     const float fx = floorf(xb), fy = floorf(yb), fz = floorf(zb);
     const int i = (int)fx, j = (int)fy, k = (int)fz;
     const double a = q8(xb - fx), b = q8(yb - fy), c = q8(zb - fz);
-    float r = 0.0f;
+    double r = 0.0;   /* exact: 8-bit weights times 24-bit texels */
     for (int dk = 0; dk < 2; ++dk) {
         const double wz = dk ? c : 1.0 - c;
         const double wx1 = q8(wz * a), wx0 = wz - wx1;
         const double w11 = q8(wx1 * b), w10 = wx1 - w11;
         const double w00 = q8(wx0 * (1.0 - b)), w01 = wx0 - w00;
-        r += (float)w00 * texel(g, i, j, k + dk);
-        r += (float)w10 * texel(g, i + 1, j, k + dk);
-        r += (float)w01 * texel(g, i, j + 1, k + dk);
-        r += (float)w11 * texel(g, i + 1, j + 1, k + dk);
+        r += w00 * texel(g, i, j, k + dk);
+        r += w10 * texel(g, i + 1, j, k + dk);
+        r += w01 * texel(g, i, j + 1, k + dk);
+        r += w11 * texel(g, i + 1, j + 1, k + dk);
     }
-    return r;
+    return (float)r;
 }
 
 /* xpbdContactSDFKernel, src/ContactSolver.cu:797-923, with the same float and
@@ -838,7 +841,17 @@ int orc_step(const orc_params *p, orc_state *s, const orc_tool_samples *tool, do
             /* after the step, at the tool pose of its end time */
             double pe[3];
             for (int d = 0; d < 3; ++d) pe[d] = p->tool_p0[d] + p->tool_v[d] * (t + dt);
-            particle_contact(p, s, pe, dt);
+            if (p->tool_sdf) {
+                const orc_contact_sdf_args a = {(float)pe[0], (float)pe[1], (float)pe[2], cosf(p->tool_sdf_angle),
+                                                sinf(p->tool_sdf_angle), (float)p->contact_radius,
+                                                (float)p->contact_friction, (float)p->contact_heat_partition,
+                                                (float)dt, 0.0f, p->cp, p->rho_phys, p->Tm};
+                int64_t c;
+                double hw, fn;
+                orc_contact_sdf(p->tool_sdf, &a, s, &c, &hw, &fn);
+            } else {
+                particle_contact(p, s, pe, dt);
+            }
         }
     }
     return err;

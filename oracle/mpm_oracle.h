@@ -39,6 +39,8 @@ enum {
 enum { ORC_SHAPE_CYLINDER_Y = 0, ORC_SHAPE_WEDGE_Y = 1 };
 enum { ORC_PLAST_EXPLICIT = 0, ORC_PLAST_NEWTON = 1 };
 
+struct orc_sdf_grid;
+
 typedef struct orc_params {
     /* background grid: node (i,j,k) sits at origin + (i,j,k)*dx */
     int32_t nx, ny, nz;
@@ -89,6 +91,11 @@ typedef struct orc_params {
      * gathered back in g2p (:282-306); alpha = k / (rho_phys cp) */
     int32_t heat_conduction;
     double thermal_conductivity;
+    /* voxel tool SDF for the contact (NULL: the analytic SDF): its frame's
+     * origin follows the tool reference point, rotated by tool_sdf_angle
+     * about z; the contact then is xpbdContactSDFKernel's (orc_contact_sdf) */
+    const struct orc_sdf_grid *tool_sdf;
+    float tool_sdf_angle;
 } orc_params;
 
 /* Particle state, SoA, one entry per particle (matrices row-major [n][9],

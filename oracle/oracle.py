@@ -44,6 +44,7 @@ class OrcParams(C.Structure):
         ("contact_every", _i32), ("contact_radius", _d), ("contact_friction", _d), ("contact_heat_partition", _d),
         ("asb_enabled", _i32), ("asb_critical_rate", _d), ("asb_taylor_quinney", _d), ("asb_max_temp_ratio", _d),
         ("asb_touch_rise", _d), ("heat_conduction", _i32), ("thermal_conductivity", _d),
+        ("tool_sdf", _vp), ("tool_sdf_angle", C.c_float),
     ]
 
 
@@ -145,6 +146,11 @@ def orc_params(case: dict) -> OrcParams:
     o.asb_touch_rise = float(p.get("asb_touch_rise", 0.5))
     o.heat_conduction = int(p.get("heat_conduction", 0))
     o.thermal_conductivity = float(p.get("thermal_conductivity", 42.6))
+    if t.get("sdf") is not None:
+        g, arr = sdf_grid(t["sdf"])
+        o._keep = (g, arr)
+        o.tool_sdf = C.cast(C.pointer(g), C.c_void_p).value
+        o.tool_sdf_angle = float(t["sdf"].get("angle", 0.0))
     return o
 
 

@@ -54,8 +54,9 @@ def test_struct_sizes_match_header():
     src = r'''
 #include <stdio.h>
 #include "mpm_capi.h"
-int main(void){printf("%zu %zu %zu %zu\n", sizeof(mpm_params), sizeof(mpm_tool_desc), sizeof(mpm_particles_soa),
- sizeof(mpm_metrics));return 0;}
+#include <stddef.h>
+int main(void){printf("%zu %zu %zu %zu %zu %zu\n", sizeof(mpm_params), sizeof(mpm_tool_desc), sizeof(mpm_particles_soa),
+ sizeof(mpm_metrics), sizeof(mpm_tool_sdf), offsetof(mpm_tool_sdf, angle));return 0;}
 '''
     import tempfile
     with tempfile.TemporaryDirectory() as d:
@@ -65,7 +66,7 @@ int main(void){printf("%zu %zu %zu %zu\n", sizeof(mpm_params), sizeof(mpm_tool_d
         subprocess.run(["gcc", "-I", str(ROOT / "include"), str(c), "-o", str(exe)], check=True)
         sizes = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
     assert sizes == [C.sizeof(A.MpmParams), C.sizeof(A.MpmToolDesc), C.sizeof(A.MpmParticlesSoa),
-                     C.sizeof(A.MpmMetrics)]
+                     C.sizeof(A.MpmMetrics), C.sizeof(A.MpmToolSdf), A.MpmToolSdf.angle.offset]
 
 
 def test_invalid_params_rejected_before_device_use():

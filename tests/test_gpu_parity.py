@@ -35,6 +35,8 @@ def run_ours(case, st, n, *, prec=A.PREC_F64, sched=A.SCHED_FUSED, splits=None, 
     s = Solver(p, len(st["x"]) + 64)
     try:
         s.set_tool(case["tool"])
+        if case["tool"].get("sdf") is not None:
+            s.set_tool_sdf(case["tool"]["sdf"])
         s.upload(st)
         if "ext" in case:
             e = case["ext"]
