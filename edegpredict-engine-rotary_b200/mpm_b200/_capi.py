@@ -151,6 +151,7 @@ def lib() -> C.CDLL:
             "mpm_set_tool": (_i32, [_vp, P(MpmToolDesc)]),
             "mpm_set_tool_sdf": (_i32, [_vp, P(MpmToolSdf)]),
             "mpm_batch_set_tool_sdf": (_i32, [_vp, _i32, P(MpmToolSdf)]),
+            "mpm_tool_sdf_build": (_i32, [_vp, _i32, _vp, _i32, _vp, _d, _i32, P(MpmToolSdf), _vp]),
             "mpm_step": (_i32, [_vp, _d, _i32]),
             "mpm_stable_dt": (_i32, [_vp, _d, P(_d)]),
             "mpm_sync_metrics": (_i32, [_vp, P(MpmMetrics)]),

@@ -230,6 +230,23 @@ def metrics_aos_noalloc(params: A.MpmParams, d_particles: int, n: int, stream: i
     return m.as_dict()
 
 
+def tool_sdf_build(verts: np.ndarray, tris: np.ndarray, normals: Optional[np.ndarray] = None, padding: float = 0.002,
+                   voxels_per_axis: int = 128) -> dict:
+    """The voxel SDF of a closed tool mesh (mpm_tool_sdf_build) as the dict that
+    Solver.set_tool_sdf takes: {"v": float32 [nz, ny, nx], "origin", "voxel", "angle": 0}."""
+    L = A.lib()
+    v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+    t = np.ascontiguousarray(tris, np.int32).reshape(-1, 3)
+    nrm = None if normals is None else np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
+    d = A.MpmToolSdf()
+    args = (v.ctypes.data, len(v), t.ctypes.data, len(t), None if nrm is None else nrm.ctypes.data, float(padding),
+            int(voxels_per_axis))
+    A.check(L.mpm_tool_sdf_build(*args, C.byref(d), None))
+    out = np.zeros((d.nz, d.ny, d.nx), np.float32)
+    A.check(L.mpm_tool_sdf_build(*args, C.byref(d), out.ctypes.data))
+    return {"v": out, "origin": tuple(d.origin), "voxel": float(d.voxel), "angle": 0.0}
+
+
 class Batch(Solver):
     """Many independent workpieces in one handle (mpm_batch_*): every step of
     all of them is one persistent launch over the bins of all instances.

@@ -246,6 +246,25 @@ typedef struct mpm_tool_sdf {
 
 mpm_status mpm_set_tool_sdf(mpm_handle *h, const mpm_tool_sdf *sdf);
 
+/*
+ * The voxel SDF of a closed tool mesh, built as ToolSDF does
+ * (src/ToolSDF.cu:212-280 build, :348-377 buildFromVerts, :379-532
+ * computeSDFCPU): the mesh bounding box grown by `padding` (m), an isotropic
+ * voxel of the longest extent / voxels_per_axis, extent / voxel + 2 voxels
+ * per axis (at most 256); each triangle's distance to the voxel centres of its
+ * box grown by one voxel below and two above, the sign within two voxels of
+ * the surface from the nearest triangle's normal, three passes that reach the
+ * voxels no box covered (nearest |distance| + half a voxel) and a large
+ * distance beyond.  Distances and signs are computed on the current GPU, the
+ * passes on the host.  verts [n_verts][3], tris [n_tris][3], normals
+ * [n_tris][3] or NULL ((b - a) x (c - a) normalised).  With values NULL only
+ * desc is filled (nx, ny, nz, origin, voxel; angle 0); with values of
+ * nx*ny*nz floats the field is written there and desc->values points to it.
+ */
+mpm_status mpm_tool_sdf_build(const float *verts, int32_t n_verts, const int32_t *tris, int32_t n_tris,
+                              const float *normals, double padding, int32_t voxels_per_axis, mpm_tool_sdf *desc,
+                              float *values);
+
 /* Replaces MPMSolver::step (src/MPMSolver.cu:1062-1168): nsteps steps of dt.
  * Asynchronous on the handle's stream. */
 mpm_status mpm_step(mpm_handle *h, double dt, int32_t nsteps);

@@ -11,6 +11,7 @@
  */
 #include "mpm_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -693,6 +694,168 @@ static void asb_heating(const orc_params *p, orc_state *s, double dt) {
 
 void orc_asb_heat(const orc_params *p, orc_state *s, double dt) {
     if (s->asb) asb_heating(p, s, dt);
+}
+
+/* ---------------------------------------------------------------- voxel SDF build */
+
+/* Squared distance from p to triangle abc and the closest point: the region
+ * tests of Ericson's closest-point-on-triangle algorithm (Real-Time Collision
+ * Detection, 5.1.5), with the reference's interior case
+ * a + u (b - a) + v (c - a), u = 1 - v - w (src/ToolSDF.cu:92-167). */
+static float tri_dist2(const float p[3], const float a[3], const float b[3], const float c[3], float q[3]) {
+    float ab[3], ac[3], ap[3], bp[3], cp[3];
+    for (int k = 0; k < 3; ++k) { ab[k] = b[k] - a[k]; ac[k] = c[k] - a[k]; ap[k] = p[k] - a[k]; }
+    const float d1 = ab[0] * ap[0] + ab[1] * ap[1] + ab[2] * ap[2];
+    const float d2 = ac[0] * ap[0] + ac[1] * ap[1] + ac[2] * ap[2];
+    if (d1 <= 0.0f && d2 <= 0.0f) {
+        for (int k = 0; k < 3; ++k) q[k] = a[k];
+    } else {
+        for (int k = 0; k < 3; ++k) bp[k] = p[k] - b[k];
+        const float d3 = ab[0] * bp[0] + ab[1] * bp[1] + ab[2] * bp[2];
+        const float d4 = ac[0] * bp[0] + ac[1] * bp[1] + ac[2] * bp[2];
+        const float vc = d1 * d4 - d3 * d2;
+        if (d3 >= 0.0f && d4 <= d3) {
+            for (int k = 0; k < 3; ++k) q[k] = b[k];
+        } else if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
+            const float v = d1 / (d1 - d3);
+            for (int k = 0; k < 3; ++k) q[k] = a[k] + v * ab[k];
+        } else {
+            for (int k = 0; k < 3; ++k) cp[k] = p[k] - c[k];
+            const float d5 = ab[0] * cp[0] + ab[1] * cp[1] + ab[2] * cp[2];
+            const float d6 = ac[0] * cp[0] + ac[1] * cp[1] + ac[2] * cp[2];
+            const float vb = d5 * d2 - d1 * d6;
+            const float va = d3 * d6 - d5 * d4;
+            if (d6 >= 0.0f && d5 <= d6) {
+                for (int k = 0; k < 3; ++k) q[k] = c[k];
+            } else if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
+                const float w = d2 / (d2 - d6);
+                for (int k = 0; k < 3; ++k) q[k] = a[k] + w * ac[k];
+            } else if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+                const float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+                for (int k = 0; k < 3; ++k) q[k] = b[k] + w * (c[k] - b[k]);
+            } else {
+                const float den = 1.0f / (va + vb + vc);
+                const float v = vb * den, w = vc * den;
+                const float u = 1.0f - v - w;
+                for (int k = 0; k < 3; ++k) q[k] = a[k] + u * (b[k] - a[k]) + v * (c[k] - a[k]);
+            }
+        }
+    }
+    const float dx = p[0] - q[0], dy = p[1] - q[1], dz = p[2] - q[2];
+    return dx * dx + dy * dy + dz * dz;
+}
+
+int orc_tool_sdf_build(const float *verts, int32_t nv, const int32_t *tris, int32_t nt, const float *normals,
+                       double padding, int32_t voxels_per_axis, int32_t dims[3], float origin[3], float *voxel,
+                       float *values) {
+    if (nv <= 0 || nt <= 0 || voxels_per_axis <= 0) return -1;
+    /* ToolSDF::build: bounding box, padding, isotropic voxel on the longest
+     * axis, dims = extent / voxel + 2 (at most 256) */
+    float bmin[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, bmax[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int i = 0; i < nv; ++i)
+        for (int k = 0; k < 3; ++k) {
+            bmin[k] = fminf(bmin[k], verts[3 * i + k]);
+            bmax[k] = fmaxf(bmax[k], verts[3 * i + k]);
+        }
+    const float pad = (float)padding;
+    for (int k = 0; k < 3; ++k) { bmin[k] -= pad; bmax[k] += pad; }
+    const float ext[3] = {bmax[0] - bmin[0], bmax[1] - bmin[1], bmax[2] - bmin[2]};
+    const float vox = fmaxf(ext[0], fmaxf(ext[1], ext[2])) / (float)voxels_per_axis;
+    for (int k = 0; k < 3; ++k) {
+        origin[k] = bmin[k];
+        dims[k] = (int)(ext[k] / vox) + 2;
+        if (dims[k] > 256) dims[k] = 256;
+    }
+    *voxel = vox;
+    const int nx = dims[0], ny = dims[1], nz = dims[2];
+    const int64_t total = (int64_t)nx * ny * nz;
+    if (total <= 0) return -1;
+    if (!values) return 0;
+    float *g = values;
+    for (int64_t i = 0; i < total; ++i) g[i] = FLT_MAX;
+    const float inv = 1.0f / vox;
+    /* computeSDFCPU: each triangle's squared distance to the voxel centres of
+     * its bounding box grown by one voxel below and two above (:396-422) */
+    for (int t = 0; t < nt; ++t) {
+        const float *a = verts + 3 * tris[3 * t], *b = verts + 3 * tris[3 * t + 1], *c = verts + 3 * tris[3 * t + 2];
+        float lo[3], hi[3];
+        int i0[3], i1[3];
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = fminf(a[k], fminf(b[k], c[k]));
+            hi[k] = fmaxf(a[k], fmaxf(b[k], c[k]));
+            const int l = (int)((lo[k] - origin[k]) * inv) - 1, h = (int)((hi[k] - origin[k]) * inv) + 2;
+            i0[k] = l > 0 ? l : 0;
+            i1[k] = h < dims[k] - 1 ? h : dims[k] - 1;
+        }
+        for (int iz = i0[2]; iz <= i1[2]; ++iz)
+            for (int iy = i0[1]; iy <= i1[1]; ++iy)
+                for (int ix = i0[0]; ix <= i1[0]; ++ix) {
+                    const float p[3] = {origin[0] + (ix + 0.5f) * vox, origin[1] + (iy + 0.5f) * vox,
+                                        origin[2] + (iz + 0.5f) * vox};
+                    float q[3];
+                    const float d2 = tri_dist2(p, a, b, c, q);
+                    const int64_t idx = ix + (int64_t)nx * (iy + (int64_t)ny * iz);
+                    if (d2 < g[idx]) g[idx] = d2;
+                }
+    }
+    for (int64_t i = 0; i < total; ++i)
+        if (g[i] < FLT_MAX) g[i] = sqrtf(g[i]);
+    /* sign within two voxels of the surface from the nearest triangle's normal
+     * (:444-490; bounding boxes grown by one voxel; the first nearest wins) */
+    const float band = vox * 2.0f;
+    for (int iz = 0; iz < nz; ++iz)
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix) {
+                const int64_t idx = ix + (int64_t)nx * (iy + (int64_t)ny * iz);
+                const float dist = g[idx];
+                if (dist > band) continue;
+                const float p[3] = {origin[0] + (ix + 0.5f) * vox, origin[1] + (iy + 0.5f) * vox,
+                                    origin[2] + (iz + 0.5f) * vox};
+                float best = FLT_MAX, bn[3] = {0, 0, 0}, bq[3] = {0, 0, 0};
+                for (int t = 0; t < nt; ++t) {
+                    const float *a = verts + 3 * tris[3 * t], *b = verts + 3 * tris[3 * t + 1],
+                                *c = verts + 3 * tris[3 * t + 2];
+                    int skip = 0;
+                    for (int k = 0; k < 3; ++k) {
+                        const float lo = fminf(a[k], fminf(b[k], c[k])), hi = fmaxf(a[k], fmaxf(b[k], c[k]));
+                        if (p[k] < lo - vox || p[k] > hi + vox) skip = 1;
+                    }
+                    if (skip) continue;
+                    float q[3];
+                    const float d2 = tri_dist2(p, a, b, c, q);
+                    if (d2 < best) {
+                        best = d2;
+                        for (int k = 0; k < 3; ++k) { bn[k] = normals[3 * t + k]; bq[k] = q[k]; }
+                    }
+                }
+                if (best < FLT_MAX) {
+                    const float dot = (p[0] - bq[0]) * bn[0] + (p[1] - bq[1]) * bn[1] + (p[2] - bq[2]) * bn[2];
+                    if (dot < 0.0f) g[idx] = -dist;
+                }
+            }
+    /* three in-place passes give a voxel not reached yet its nearest known
+     * neighbour's |distance| + half a voxel (:494-524), then the rest a large
+     * distance (:526-531) */
+    for (int pass = 0; pass < 3; ++pass)
+        for (int iz = 1; iz < nz - 1; ++iz)
+            for (int iy = 1; iy < ny - 1; ++iy)
+                for (int ix = 1; ix < nx - 1; ++ix) {
+                    const int64_t idx = ix + (int64_t)nx * (iy + (int64_t)ny * iz);
+                    if (g[idx] < FLT_MAX) continue;
+                    float nd = FLT_MAX;
+                    for (int dz = -1; dz <= 1; ++dz)
+                        for (int dy = -1; dy <= 1; ++dy)
+                            for (int dx = -1; dx <= 1; ++dx) {
+                                if (!dx && !dy && !dz) continue;
+                                const float v = fabsf(g[(ix + dx) + (int64_t)nx * ((iy + dy) + (int64_t)ny * (iz + dz))]);
+                                if (v < nd) nd = v;
+                            }
+                    if (nd < FLT_MAX) g[idx] = nd + vox * 0.5f;
+                }
+    const int dmax = nx > ny ? (nx > nz ? nx : nz) : (ny > nz ? ny : nz);
+    for (int64_t i = 0; i < total; ++i)
+        if (g[i] >= FLT_MAX) g[i] = vox * (float)dmax;
+    return 0;
 }
 
 /* ---------------------------------------------------------------- voxel SDF contact */

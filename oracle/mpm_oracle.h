@@ -171,6 +171,16 @@ float orc_tex3d(const orc_sdf_grid *g, float x, float y, float z);
 void orc_contact_sdf(const orc_sdf_grid *g, const orc_contact_sdf_args *a, orc_state *s, int64_t *count,
                      double *heat, double *force);
 
+/* The voxel SDF of a closed triangle mesh as ToolSDF builds it
+ * (src/ToolSDF.cu:212-280 build, :348-377 buildFromVerts, :379-532
+ * computeSDFCPU): verts [nv][3], tris [nt][3] indices, normals [nt][3]
+ * (the mesh's triangle normals).  Always fills dims, origin and voxel; fills
+ * values (dims product, x fastest) when values is not NULL.  Returns 0, or -1
+ * for an empty mesh or grid. */
+int orc_tool_sdf_build(const float *verts, int32_t nv, const int32_t *tris, int32_t nt, const float *normals,
+                       double padding, int32_t voxels_per_axis, int32_t dims[3], float origin[3], float *voxel,
+                       float *values);
+
 /* Size in doubles of the grid scratch that orc_step needs. */
 int64_t orc_grid_doubles(const orc_params *p);
 

@@ -220,6 +220,9 @@ class Oracle:
         L.orc_heat_diffuse.argtypes = [C.POINTER(OrcParams), C.POINTER(_d), C.POINTER(_d), C.POINTER(_d), _d]
         L.orc_tex3d.restype = C.c_float
         L.orc_tex3d.argtypes = [C.POINTER(OrcSdfGrid), C.c_float, C.c_float, C.c_float]
+        L.orc_tool_sdf_build.restype = _i32
+        L.orc_tool_sdf_build.argtypes = [_vp, _i32, _vp, _i32, _vp, _d, _i32, C.POINTER(_i32 * 3),
+                                         C.POINTER(C.c_float * 3), C.POINTER(C.c_float), _vp]
         L.orc_contact_sdf.restype = None
         L.orc_contact_sdf.argtypes = [C.POINTER(OrcSdfGrid), C.POINTER(OrcContactArgs), C.POINTER(OrcState),
                                       C.POINTER(_i64), C.POINTER(_d), C.POINTER(_d)]
@@ -257,6 +260,19 @@ class Oracle:
         g, keep = sdf_grid(sdf)
         q = np.asarray(xyz, np.float32).reshape(-1, 3)
         return np.array([self.L.orc_tex3d(C.byref(g), float(a), float(b), float(c)) for a, b, c in q], np.float32)
+
+    def tool_sdf_build(self, verts, tris, normals, padding: float, voxels_per_axis: int) -> dict:
+        """The voxel SDF of a closed mesh as ToolSDF builds it."""
+        v = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(tris, np.int32).reshape(-1, 3)
+        n = np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
+        dims, org, vox = (_i32 * 3)(), (C.c_float * 3)(), C.c_float()
+        args = (v.ctypes.data, len(v), t.ctypes.data, len(t), n.ctypes.data, float(padding), int(voxels_per_axis))
+        if self.L.orc_tool_sdf_build(*args, C.byref(dims), C.byref(org), C.byref(vox), None) != 0:
+            raise ValueError("empty mesh or grid")
+        out = np.zeros((dims[2], dims[1], dims[0]), np.float32)
+        self.L.orc_tool_sdf_build(*args, C.byref(dims), C.byref(org), C.byref(vox), out.ctypes.data)
+        return {"v": out, "origin": tuple(org), "voxel": float(vox.value), "angle": 0.0}
 
     def contact_sdf(self, case: dict, state: Dict[str, np.ndarray], sdf: dict, args: dict):
         """One xpbdContactSDFKernel pass: (state after, (count, friction work, normal force))."""
