@@ -697,7 +697,8 @@ def main():
                     help="plain configs: run the adiabatic shear band heating after every move")
     ap.add_argument("--heat", action="store_true",
                     help="plain configs: grid heat conduction (scatter, diffusion step, gather) every step")
-    ap.add_argument("--repeats", type=int, default=5, help="precision_study: FP32 runs")
+    ap.add_argument("--repeats", type=int, default=11,
+                    help="precision_study: FP32 runs (odd; about one in five branches in the fracture zone)")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: window in seconds")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
