@@ -512,6 +512,8 @@ def run_precision_study(args):
     b = case["box"]
     cap = int(np.prod([b["c1"][i] - b["c0"][i] for i in range(3)]) * b["ppc"])
 
+    fields = ("x", "y", "z", "vx", "vy", "vz", "plastic_strain", "temperature", "stress", "status")
+
     def run(prec):
         s = Solver(W.to_mpm_params(case, precision=prec), cap)
         n = _init(s, case, rank=rank)
@@ -520,11 +522,32 @@ def run_precision_study(args):
         s.step(case["dt"], args.steps)
         m = s.metrics()
         sec = time.perf_counter() - t0
+        state = s.download(fields)      # generation order: the same particles in both precisions
         s.close()
-        return n, m, sec
+        return n, m, sec, state
 
-    n, r, t64 = run(A.PREC_F64)
+    n, r, t64, st64 = run(A.PREC_F64)
     e64 = r["kinetic"] + r["internal_elastic"]
+    a_tamb = case["params"]["Tamb"]
+    vt = float(np.linalg.norm(case["tool"]["velocity"]))
+    live = st64["status"] != A.INACTIVE
+    v64 = np.sqrt(st64["vx"] ** 2 + st64["vy"] ** 2 + st64["vz"] ** 2)
+    scales = {"position": case["params"]["dx"], "velocity": max(float(v64[live].max()), vt),
+              "plastic_strain": max(float(st64["plastic_strain"][live].max()), 1e-30),
+              "temperature_rise": max(float((st64["temperature"][live] - a_tamb).max()), 1e-30),
+              "stress": max(float(np.abs(st64["stress"][live]).max()), 1e-30)}
+
+    def particle_errors(st):
+        """Per-particle |FP32 - FP64| over the field scales: max and 99th percentile."""
+        d = {"position": np.sqrt((st["x"] - st64["x"]) ** 2 + (st["y"] - st64["y"]) ** 2 +
+                                 (st["z"] - st64["z"]) ** 2),
+             "velocity": np.sqrt((st["vx"] - st64["vx"]) ** 2 + (st["vy"] - st64["vy"]) ** 2 +
+                                 (st["vz"] - st64["vz"]) ** 2),
+             "plastic_strain": np.abs(st["plastic_strain"] - st64["plastic_strain"]),
+             "temperature_rise": np.abs(st["temperature"] - st64["temperature"]),
+             "stress": np.abs(st["stress"] - st64["stress"]).max(axis=1)}
+        return {k: {"max": float(v[live].max() / scales[k]), "p99": float(np.quantile(v[live], 0.99) / scales[k])}
+                for k, v in d.items()}
 
     def rel(x, y):
         return abs(x - y) / max(abs(y), 1e-300)
@@ -537,18 +560,23 @@ def run_precision_study(args):
                 "max_temperature_rise": rel(a["max_temperature"] - a_tamb, r["max_temperature"] - a_tamb),
                 "mean_plastic_strain": rel(a["mean_plastic_strain"], r["mean_plastic_strain"]),
                 "n_chip": [a["n_chip"], r["n_chip"]], "n_yielded": [a["n_yielded"], r["n_yielded"]]}
-    a_tamb = case["params"]["Tamb"]
     runs, t32 = [], []
     for _ in range(max(1, args.repeats)):
-        _, a, sec = run(A.PREC_F32)
-        runs.append(errors(a))
+        _, a, sec, st32 = run(A.PREC_F32)
+        e = errors(a)
+        e["particles"] = particle_errors(st32)
+        runs.append(e)
         t32.append(sec)
+        del st32
     if rank != 0:
         return None
     worst = {k: max(x[k] for x in runs) for k in ("momentum", "kinetic_plus_internal", "peak_von_mises",
                                                      "max_temperature_rise", "mean_plastic_strain")}
     med = {k: float(np.median([x[k] for x in runs])) for k in worst}
     within = sum(1 for x in runs if x["momentum"] <= 1e-4 and x["kinetic_plus_internal"] <= 1e-4)
+    # per-particle errors: median over the runs of each run's max and 99th percentile
+    part = {k: {s: float(np.median([x["particles"][k][s] for x in runs])) for s in ("max", "p99")}
+            for k in scales}
     return {"metric": "relative error FP32 vs FP64 after K steps (median of the FP32 runs)",
             "value": max(med["momentum"], med["kinetic_plus_internal"]), "unit": "relative", "n_gpus": 1,
             "steps": args.steps, "warmup": 0, "ms_per_step": None, "higher_is_better": False, "scaling": None,
@@ -558,7 +586,8 @@ def run_precision_study(args):
                                    "conservation reductions are FP64 in both runs",
                        "particles": int(n), "fp32_runs": len(runs),
                        "target": "momentum and kinetic+internal energy within 1e-4"},
-            "errors_median": med, "errors_worst": worst, "runs_within_1e-4": within, "runs": runs,
+            "errors_median": med, "errors_worst": worst, "runs_within_1e-4": within,
+            "particle_errors_median": part, "particle_error_scales": scales, "runs": runs,
             "f64": {k: r[k] for k in ("mass", "momentum", "kinetic", "internal_elastic", "max_von_mises",
                                       "max_temperature", "mean_plastic_strain", "n_chip", "n_inactive")},
             "wall_s": {"f64": t64, "f32_each": t32}}
