@@ -270,6 +270,12 @@ mpm_status mpm_batch_sync_metrics(mpm_handle* h, int32_t inst, mpm_metrics* out)
     return ret(h, h->eng->metrics(inst, out));
 }
 
+mpm_status mpm_batch_instance_status(mpm_handle* h, int32_t* status, int32_t n) {
+    NEED_H(h);
+    if (!status) return fail(h, MPM_INVALID_ARG, "status array is NULL");
+    return ret(h, h->eng->inst_statuses(status, n));
+}
+
 mpm_status mpm_batch_get_counts(const mpm_handle* h, int32_t inst, int64_t* n_particles, int64_t* n_steps,
                                 double* time) {
     if (!h || !h->eng) return fail(nullptr, MPM_INVALID_ARG, "handle is NULL");
@@ -351,6 +357,7 @@ const char* mpm_status_string(mpm_status s) {
         case MPM_TIMEOUT: return "MPM_TIMEOUT";
         case MPM_NOT_SUPPORTED: return "MPM_NOT_SUPPORTED";
         case MPM_CAPACITY: return "MPM_CAPACITY";
+        case MPM_CANCELLED: return "MPM_CANCELLED";
     }
     return "unknown";
 }

@@ -37,7 +37,11 @@ constexpr int kSY = 8, kSZ = 68, kPlane = 392;
 
 enum : uint8_t { ST_ACTIVE = 0, ST_INACTIVE = 1, ST_CHIP = 2, ST_BOUNDARY = 3, ST_FIXED = 4 };
 enum : int { TOOL_NONE = 0, TOOL_RASTER = 1, TOOL_SDF_STICKY = 2, TOOL_SDF_SLIP = 3 };
-enum : int { ERR_NUMERIC = 1, ERR_TIMEOUT = 2, ERR_NEWTON = 4 };
+// Error bits.  ERR_TIMEOUT lives in the handle's word (a bounded wait gave
+// up).  The instance words hold one byte per cause, each set by a plain byte
+// store of 1 (no read-modify-write): byte 0 a non-finite position, byte 1 a
+// Newton return that did not converge.
+enum : int { ERR_NUMERIC = 1, ERR_TIMEOUT = 2, ERR_NEWTON = 1 << 8 };
 
 struct alignas(32) D4 { double x, y, z, w; };
 
@@ -130,6 +134,7 @@ template <typename R> struct alignas(128) Inst {
     int64_t pcap;                  // particle slots of this instance
     int fresh;                     // positions still in the upload scratch (not yet binned)
     int nbins;                     // nbx * nby * nbz
+    int* ierr;                     // this instance's error word: byte 0 NaN/Inf, byte 1 Newton
 };
 
 // Threads per CTA of the step kernel (four warps, each with its own P2G tile).

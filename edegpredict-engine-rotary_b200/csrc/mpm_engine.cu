@@ -116,7 +116,9 @@ class Engine final : public EngineBase {
     Work* d_work = nullptr;
     int* d_nwork = nullptr;
     int max_work = 0;
-    int* d_err = nullptr;
+    int* d_err = nullptr;          // the handle's error word (ERR_TIMEOUT)
+    int* d_ierr = nullptr;         // one error word per instance (ERR_NUMERIC, ERR_NEWTON)
+    int64_t ierr_alloc = 0;
     unsigned long long* d_ctr = nullptr;
     static constexpr size_t kCtrBytes = 4 * sizeof(unsigned long long) + 2 * sizeof(double);
     double *d_stat_part = nullptr, *d_stat_out = nullptr;
@@ -177,7 +179,8 @@ class Engine final : public EngineBase {
                         d_key_base, d_bin_key, d_bin_inst,
                         d_bin_local,
                         d_inst_pbase, d_key, d_rank, d_newbin, d_count, d_offset, d_flag, d_flag_scan, d_scan_tmp,
-                        d_pos, d_work, d_nwork, d_err, d_ctr, d_stat_part, d_stat_out, d_stage, d_gen, d_map};
+                        d_pos, d_work, d_nwork, d_err, d_ierr, d_ctr, d_stat_part, d_stat_out, d_stage, d_gen,
+                        d_map};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         for (auto& x : I)
@@ -299,6 +302,12 @@ class Engine final : public EngineBase {
         CK(cudaStreamSynchronize(st));
         drop_graphs();
         const int n = (int)nI.size();
+        // error words follow their instances; new instances start clean
+        std::vector<int> old_words(I.size(), 0), words(n, 0);
+        if (!I.empty() && d_ierr)
+            CK(cudaMemcpy(old_words.data(), d_ierr, sizeof(int) * I.size(), cudaMemcpyDeviceToHost));
+        for (int j = 0; j < n; ++j)
+            if (from[j] >= 0) words[j] = old_words[from[j]];
         std::vector<RelayoutMap> map(n);
         std::vector<char> kept(I.size(), 0);
         bool any_kept = false;
@@ -442,6 +451,8 @@ class Engine final : public EngineBase {
         MS(grow(d_key_base, inst_alloc[0], n));
         MS(grow(d_inst_pbase, inst_alloc[1], n));
         MS(grow(d_inst, inst_alloc[2], n));
+        MS(grow(d_ierr, ierr_alloc, n));
+        if (n > 0) CK(cudaMemcpyAsync(d_ierr, words.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
         if (n > 0) {
             CK(cudaMemcpyAsync(d_key_base, key_base.data(), 4 * n, cudaMemcpyHostToDevice, st));
             CK(cudaMemcpyAsync(d_inst_pbase, inst_pbase.data(), 8 * n, cudaMemcpyHostToDevice, st));
@@ -526,6 +537,7 @@ class Engine final : public EngineBase {
         MS(grow(d_key_base, inst_alloc[0], max_inst, false));
         MS(grow(d_inst_pbase, inst_alloc[1], max_inst, false));
         MS(grow(d_inst, inst_alloc[2], max_inst, false));
+        MS(grow(d_ierr, ierr_alloc, max_inst, false));
         MS(grow(d_map, map_alloc, max_inst, false));
         CK(cudaStreamSynchronize(st));
         return MPM_OK;
@@ -604,6 +616,7 @@ class Engine final : public EngineBase {
         const mpm_params& p = x.p;
         Inst<R>& d = h_inst[i];
         d.tool_mask = mask_pool + x.grid_off;
+        d.ierr = d_ierr + i;
         d.tm[0] = tpool[0] + x.grid_off;
         d.tm[1] = tpool[1] + x.grid_off;
         d.tn = tpool[2] + x.grid_off;
@@ -730,6 +743,10 @@ class Engine final : public EngineBase {
             err = "ppc must be positive";
             return MPM_INVALID_ARG;
         }
+        if (!std::isfinite(T0)) {
+            err = "T0 must be finite";
+            return MPM_INVALID_ARG;
+        }
         const int64_t ncand = (int64_t)(c1[0] - c0[0]) * (c1[1] - c0[1]) * (c1[2] - c0[2]) * ppc;
         if (ncand > x.cap) {
             err = "box holds more candidates than the instance capacity";
@@ -763,6 +780,7 @@ class Engine final : public EngineBase {
         cudaFree(tmp);
         x.np = (int64_t)lasti + lastf;
         x.fresh = 1;
+        CK(cudaMemsetAsync(d_ierr + i, 0, sizeof(int), st));   // a new state starts without errors
         CK(cudaGetLastError());
         return push_insts();  // binned by the next call that needs it
     }
@@ -824,6 +842,7 @@ class Engine final : public EngineBase {
                          st);
         x.np = n;
         x.fresh = 1;
+        CK(cudaMemsetAsync(d_ierr + i, 0, sizeof(int), st));   // a new state starts without errors
         CK(cudaGetLastError());
         return push_insts();  // binned by the next call that needs it
     }
@@ -873,7 +892,7 @@ class Engine final : public EngineBase {
         if (h->status) CK(cudaMemcpyAsync(h->status, o.status, 4 * n, cudaMemcpyDeviceToHost, st));
         if (h->id) CK(cudaMemcpyAsync(h->id, o.id, 4 * n, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        return device_status();
+        return inst_status(i);
     }
 
     mpm_status export_aos(int i, void* dst, int64_t bytes) override {
@@ -902,7 +921,7 @@ class Engine final : public EngineBase {
         launch_export_aos<R>(d_inst + i, ps[cur], x.pbase, x.np, x.p.Tamb, x.p.rho_phys, out, st);
         if (!dev) CK(cudaMemcpyAsync(dst, out, (size_t)504 * x.np, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        return device_status();
+        return inst_status(i);
     }
 
     // ---------------------------------------------------------------- tool
@@ -1279,18 +1298,55 @@ class Engine final : public EngineBase {
 
     // ---------------------------------------------------------------- metrics
 
-    mpm_status device_status() {
+    // Status from the error words of the handle (ERR_TIMEOUT) and of
+    // instances [i0, i1).  Synchronises the stream.
+    mpm_status word_status(int i0, int i1, std::vector<int>* words = nullptr) {
         int e = 0;
+        std::vector<int> w((size_t)std::max(i1 - i0, 0), 0);
         CK(cudaMemcpyAsync(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        if (!w.empty()) CK(cudaMemcpyAsync(w.data(), d_ierr + i0, sizeof(int) * w.size(), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        if (e & ERR_NEWTON) {
+            // a thread saw Newton returns fail in more than one instance: every
+            // instance that runs the Newton return is marked (on the device, so
+            // that the mark stays with the instance) and the handle's bit cleared
+            const unsigned char one = 1;
+            for (size_t k = 0; k < I.size(); ++k)
+                if (I[k].p.plasticity == MPM_PLAST_NEWTON) {
+                    CK(cudaMemcpyAsync(reinterpret_cast<unsigned char*>(d_ierr + k) + 1, &one, 1,
+                                       cudaMemcpyHostToDevice, st));
+                    if ((int)k >= i0 && (int)k < i1) w[k - i0] |= ERR_NEWTON;
+                }
+            e &= ~ERR_NEWTON;
+            CK(cudaMemcpyAsync(d_err, &e, sizeof(int), cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        if (words) *words = w;
         if (e & ERR_TIMEOUT) {
             err = "a bounded device wait timed out (TMA tile load)";
             return MPM_TIMEOUT;
         }
-        if (e & ERR_NEWTON) {
-            err = "a Newton return did not converge";
+        for (size_t k = 0; k < w.size(); ++k) {
+            if (!w[k]) continue;
+            const std::string who = "instance " + std::to_string(i0 + (int)k) + ": ";
+            err = who + ((w[k] & 0xff) ? "a NaN or Inf in the particle state" : "a Newton return did not converge");
             return MPM_NUMERIC;
         }
+        return MPM_OK;
+    }
+    mpm_status device_status() { return word_status(0, (int)I.size()); }
+    mpm_status inst_status(int i) { return word_status(i, i + 1); }
+
+    mpm_status inst_statuses(int32_t* out, int n) override {
+        if (!out || n < (int)I.size()) {
+            err = "status array NULL or shorter than the instance count";
+            return MPM_INVALID_ARG;
+        }
+        std::vector<int> w;
+        const mpm_status s = word_status(0, (int)I.size(), &w);
+        if (s != MPM_OK && s != MPM_TIMEOUT && s != MPM_NUMERIC) return s;
+        for (size_t k = 0; k < w.size(); ++k)
+            out[k] = s == MPM_TIMEOUT ? MPM_TIMEOUT : (w[k] ? MPM_NUMERIC : MPM_OK);
         return MPM_OK;
     }
 
@@ -1313,6 +1369,16 @@ class Engine final : public EngineBase {
         CK(cudaMemcpyAsync(ctr, d_ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(fsum, d_ctr + 4, sizeof(fsum), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        // a NaN or Inf that never reached the positions (a temperature, stress or
+        // plastic strain of a live particle) shows in the FP64 sums: it marks the
+        // instance's word too (byte 0)
+        bool finite = true;
+        for (int k : {0, 1, 2, 3, 4, 5, 6, 10, 13, 14}) finite = finite && std::isfinite(v[k]);
+        if (!finite) {
+            const unsigned char one = 1;
+            CK(cudaMemcpyAsync(d_ierr + i, &one, 1, cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));
+        }
         std::memset(out, 0, sizeof(*out));
         out->mass = v[0];
         out->momentum[0] = v[1]; out->momentum[1] = v[2]; out->momentum[2] = v[3];
@@ -1322,10 +1388,8 @@ class Engine final : public EngineBase {
         out->max_temperature = x.p.Tamb + (std::isfinite(v[7]) ? v[7] : 0.0);
         out->max_von_mises = v[8];
         out->max_plastic_strain = std::isfinite(v[9]) ? v[9] : 0.0;
-        const double nl = v[15] + v[16] + v[17] + (double)0;
         const double nlive = (double)x.np - v[18];
         out->mean_plastic_strain = nlive > 0 ? v[10] / nlive : 0.0;
-        (void)nl;
         out->ref_max_stress = v[11];
         out->ref_max_temperature = v[12];
         out->ref_kinetic = v[13];
@@ -1345,7 +1409,7 @@ class Engine final : public EngineBase {
         out->contact_work = fsum[0];
         out->contact_force = fsum[1];
         out->n_asb_heated = (int64_t)ctr[3];
-        return device_status();
+        return inst_status(i);
     }
 
     // ---------------------------------------------------------------- misc

@@ -75,6 +75,9 @@ class EngineBase {
     virtual mpm_status change_instances(const mpm_params* params, const int64_t* caps, int n_add,
                                         const int32_t* remove, int n_remove, int* first) = 0;
     virtual mpm_status sync() = 0;
+    // Status of every instance from its error word (MPM_OK, MPM_NUMERIC; all
+    // MPM_TIMEOUT when a bounded wait gave up); synchronises the stream.
+    virtual mpm_status inst_statuses(int32_t* out, int n) = 0;
     virtual int n_inst() const = 0;
     virtual const InstHost& inst(int i) const = 0;
     virtual cudaStream_t stream() const = 0;

@@ -31,6 +31,7 @@ struct GpuOps {
     }
     mpm_status step(int k, const std::vector<double>& dts) { return e->step(k, dts.data()); }
     mpm_status metrics(int inst, mpm_metrics* m) { return e->metrics(inst, m); }
+    mpm_status health(std::vector<int32_t>& st) { return e->inst_statuses(st.data(), (int)st.size()); }
 };
 
 mpm_status fail(mpm_status s, const std::string& m) {
@@ -125,7 +126,7 @@ mpm_status mpm_server_submit(mpm_server* s, const mpm_request* req, int64_t* id)
         return fail(MPM_NOT_SUPPORTED, "raster tools are not served (the samples are not kept); use an SDF tool");
     st = s->sched->submit(*req, id);
     if (st == MPM_CAPACITY) return fail(st, "the request's footprint exceeds the server's pools");
-    if (st != MPM_OK) return fail(st, "nsteps >= 0, dt > 0 and ppc > 0 required");
+    if (st != MPM_OK) return fail(st, "nsteps >= 0, finite dt > 0, ppc > 0 and a finite T0 required");
     return MPM_OK;
 }
 
@@ -139,6 +140,13 @@ mpm_status mpm_server_tick(mpm_server* s, int32_t* n_resident) {
 mpm_status mpm_server_poll(mpm_server* s, int64_t id, mpm_result* out) {
     if (!s || !out) return mpmb::fail(MPM_INVALID_ARG, "server or output is NULL");
     const mpm_status st = s->sched->poll(id, out);
+    if (st != MPM_OK) return mpmb::fail(st, "unknown request id");
+    return MPM_OK;
+}
+
+mpm_status mpm_server_cancel(mpm_server* s, int64_t id) {
+    if (!s) return mpmb::fail(MPM_INVALID_ARG, "server is NULL");
+    const mpm_status st = s->sched->cancel(id);
     if (st != MPM_OK) return mpmb::fail(st, "unknown request id");
     return MPM_OK;
 }

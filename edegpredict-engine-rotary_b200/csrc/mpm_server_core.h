@@ -11,13 +11,18 @@
 //   4. steps every resident request by k = min(max_chunk, fewest remaining
 //      steps of any resident request) in one engine step call, so requests
 //      admitted while others run share their launches from then on;
-//   5. records the metrics of every request that reached its step count.
-// The engine is a template parameter: the GPU engine in the library, a fake
-// in the host tests.  submit() and poll() may run on other threads than
-// tick().
+//   5. reads the engine's per-instance status: a request whose workpiece
+//      failed (MPM_NUMERIC) ends FAILED and is dropped by the next tick's
+//      step 1, while the others run on;
+//   6. records the metrics of every request that reached its step count.
+// cancel() ends a queued request at once and marks a running one, which the
+// next tick's step 1 drops.  The engine is a template parameter: the GPU
+// engine in the library, a fake in the host tests.  submit(), poll() and
+// cancel() may run on other threads than tick().
 #pragma once
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <deque>
@@ -92,6 +97,7 @@ class Scheduler {
         mpm_request r{};
         Footprint f;
         mpm_result res{};
+        bool cancel = false;   // cancelled while resident: dropped by the next tick
     };
 
     Scheduler(Engine* eng, Pools pools, int max_chunk, int max_resident, std::function<double()> clock,
@@ -105,7 +111,8 @@ class Scheduler {
     mpm_status submit(const mpm_request& r, int64_t* id) {
         const Footprint f = request_footprint(r);
         if (!pools_.fits(Footprint{}, f)) return MPM_CAPACITY;
-        if (r.nsteps < 0 || !(r.dt > 0.0) || r.ppc <= 0) return MPM_INVALID_ARG;
+        if (r.nsteps < 0 || !(r.dt > 0.0) || !std::isfinite(r.dt) || r.ppc <= 0 || !std::isfinite(r.T0))
+            return MPM_INVALID_ARG;
         std::lock_guard<std::mutex> lock(mu_);
         Req q;
         q.id = next_id_++;
@@ -128,6 +135,21 @@ class Scheduler {
         return MPM_OK;
     }
 
+    // Cancels a request (see the file comment); MPM_INVALID_ARG for an unknown id.
+    mpm_status cancel(int64_t id) {
+        std::lock_guard<std::mutex> lock(mu_);
+        auto it = all_.find(id);
+        if (it == all_.end()) return MPM_INVALID_ARG;
+        Req& q = it->second;
+        if (q.res.state == MPM_REQ_QUEUED) {
+            queue_.erase(std::find(queue_.begin(), queue_.end(), id));
+            end_cancelled(q);
+        } else if (q.res.state == MPM_REQ_RUNNING) {
+            q.cancel = true;
+        }
+        return MPM_OK;
+    }
+
     mpm_server_stats stats() {
         std::lock_guard<std::mutex> lock(mu_);
         mpm_server_stats s = stats_;
@@ -146,13 +168,17 @@ class Scheduler {
         std::vector<int32_t> remove;
         std::vector<int64_t> keep;
         Footprint used = used_;
-        for (size_t i = 0; i < resident_.size(); ++i) {
-            Req& q = ref(resident_[i]);
-            if (q.res.state == MPM_REQ_DONE || q.res.state == MPM_REQ_FAILED) {
-                remove.push_back((int32_t)i);
-                sub(used, q.f);
-            } else {
-                keep.push_back(resident_[i]);
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            for (size_t i = 0; i < resident_.size(); ++i) {
+                Req& q = all_[resident_[i]];
+                if (q.res.state == MPM_REQ_RUNNING && q.cancel) end_cancelled(q);
+                if (q.res.state != MPM_REQ_RUNNING) {
+                    remove.push_back((int32_t)i);
+                    sub(used, q.f);
+                } else {
+                    keep.push_back(resident_[i]);
+                }
             }
         }
         // 2. admit in arrival order
@@ -215,17 +241,31 @@ class Scheduler {
             ++running;
             k = std::min<int64_t>(k, q.r.nsteps - q.res.steps_done);
         }
+        std::vector<int32_t> health(resident_.size(), MPM_OK);
         if (running > 0 && k > 0) {
             std::vector<double> dts;
             for (int64_t id : resident_) dts.push_back(ref(id).r.dt);
             mpm_status s = eng_->step(k, dts);
             if (s != MPM_OK) return s;
+            // 5. per-workpiece failures
+            s = eng_->health(health);
+            if (s != MPM_OK) return s;
         }
-        // 5. completions
+        // 6. completions
         for (size_t i = 0; i < resident_.size(); ++i) {
             Req& q = ref(resident_[i]);
             if (q.res.state != MPM_REQ_RUNNING) continue;
             const int kk = running > 0 ? std::max(k, 0) : 0;
+            if (health[i] != MPM_OK) {
+                std::lock_guard<std::mutex> lock(mu_);
+                q.res.steps_done += kk;
+                stats_.particle_updates += q.res.n_particles * kk;
+                q.res.t_done = clock_();
+                q.res.state = MPM_REQ_FAILED;
+                q.res.status = health[i];
+                ++stats_.failed;
+                continue;
+            }
             mpm_metrics m{};
             mpm_status sm = MPM_OK;
             const bool done = q.res.steps_done + kk >= q.r.nsteps;
@@ -251,6 +291,13 @@ class Scheduler {
     }
 
    private:
+    // (mu_ held)
+    void end_cancelled(Req& q) {
+        q.res.state = MPM_REQ_CANCELLED;
+        q.res.status = MPM_CANCELLED;
+        q.res.t_done = clock_();
+        ++stats_.cancelled;
+    }
     Req& ref(int64_t id) {
         std::lock_guard<std::mutex> lock(mu_);
         return all_[id];

@@ -436,7 +436,8 @@ struct JCOut {
 // enter the force (:406-408) and the F_p update (:282-294).  sl[3] carries them.
 template <typename R>
 __device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[9], R& eps, R& dT, R& D, R edot,
-                                           R sig[6], R sl[3], R& J, R* sres_p, R* bsx, int& errf) {
+                                           R sig[6], R sl[3], R& J, R* sres_p, R* bsx, int& errf,
+                                           const Inst<R>* insts) {
     JCOut o{true, false, false};
     // inverse of G = I + Hp (identity when |det G| < 1e-12, inv3x3 :50-57);
     // a particle that never yielded has Hp = 0 exactly and F_e = F
@@ -525,8 +526,12 @@ __device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[
         if (P.plast == 1) {
             double dg;
             if (!newton_return((double)q, (double)P.mu, (double)eps, (double)P.A, (double)P.B, (double)P.n, (double)rt,
-                               (double)tt, P.newton_tol, P.newton_maxit, &dg))
-                errf |= ERR_NEWTON;
+                               (double)tt, P.newton_tol, P.newton_maxit, &dg)) {
+                // the failing instance (tag = index + 1, from the record's address) in
+                // a register; a second instance failing on this thread makes it -1
+                const int tag = (int)(&P - insts) + 1;
+                errf = (errf == 0 || errf == tag) ? tag : -1;
+            }
             dE = (R)dg;
             Yr = (R)((double)q - 3.0 * (double)P.mu * dg);
         } else {
@@ -954,9 +959,9 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
     const int tid = threadIdx.x, lane = tid & 31;
     const int nw = *n_work;
     uint32_t phase = 0;
-    int errf = 0;
     unsigned long long c_esc = 0, c_yield = 0, c_contact = 0;
     double f_work = 0.0, f_force = 0.0;
+    int errf = 0;   // Newton failures: 0 none, k > 0 instance k - 1 only, -1 several instances
     if (G2P && tid == 0) {
         mbar_init(&Sm.mbar, 1);
         fence_async_smem();
@@ -1241,10 +1246,15 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
 
                     bool yielded = false;
                     if (P2G) {
-                        // kill zone on the cell index, :130-139
-                        const int cx = g0x + (int)floor(xi[0]), cy = g0y + (int)floor(xi[1]),
-                                  cz = g0z + (int)floor(xi[2]);
-                        if (cx < 1 || cx >= P.nx - 2 || cy < 1 || cy >= P.ny - 2 || cz < 1 || cz >= P.nz - 2) {
+                        // kill zone on the cell index, :130-139.  Written on the floored
+                        // bin-local position so that a NaN position fails every bound and is
+                        // killed, as in the reference, whose integer cell index of a NaN
+                        // position (0 from the GPU's conversion) is below 1; a non-finite
+                        // position also marks the instance's error word (byte 0)
+                        const R f0 = floor(xi[0]), f1 = floor(xi[1]), f2 = floor(xi[2]);
+                        if (!(f0 >= R(1 - g0x) && f0 < R(P.nx - 2 - g0x) && f1 >= R(1 - g0y) &&
+                              f1 < R(P.ny - 2 - g0y) && f2 >= R(1 - g0z) && f2 < R(P.nz - 2 - g0z))) {
+                            if (!isfinite(f0 + f1 + f2)) reinterpret_cast<unsigned char*>(P.ierr)[0] = 1;
                             st = ST_INACTIVE;
                             if (G2P) {
                                 // no later G2P writes this particle: store this step's v, strain rate and C
@@ -1258,6 +1268,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                         } else {
                             // within one cell of the kill zone the stress is kept in memory, since a
                             // kill in the next launch leaves the last computed stress as the state
+                            const int cx = g0x + (int)f0, cy = g0y + (int)f1, cz = g0z + (int)f2;
                             const bool near_kill = cx < 3 || cx >= P.nx - 4 || cy < 3 || cy >= P.ny - 4 ||
                                                    cz < 3 || cz >= P.nz - 4;
                             bool far = false;
@@ -1283,7 +1294,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                     bsp = bsv;
                                 }
                                 JCOut jo = jc_update<R>(P, H, Hp, eps, dT, Dm, edot, sig, sl, Jv, &ps.sres[pi], bsp,
-                                                        errf);
+                                                        errf, insts);
                                 if (jo.yielded) {
                                     yielded = true;
                                     dirtyA = true;
@@ -1447,7 +1458,6 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
         c_contact += __shfl_down_sync(0xffffffffu, c_contact, o);
         f_work += __shfl_down_sync(0xffffffffu, f_work, o);
         f_force += __shfl_down_sync(0xffffffffu, f_force, o);
-        errf |= __shfl_down_sync(0xffffffffu, errf, o);
     }
     if (lane == 0) {
         if (c_esc) atomicAdd(&ctr[0], c_esc);
@@ -1458,8 +1468,11 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
             atomicAdd(reinterpret_cast<double*>(ctr + 4), f_work);
             atomicAdd(reinterpret_cast<double*>(ctr + 4) + 1, f_force);
         }
-        if (errf) atomicOr(err, errf);
     }
+    // Newton failures to the failing instance's error word (byte 1), or to the
+    // handle's word when this thread saw more than one instance fail
+    if (errf > 0) reinterpret_cast<unsigned char*>(insts[errf - 1].ierr)[1] = 1;
+    else if (errf < 0) atomicOr(err, ERR_NEWTON);
 }
 
 template <typename R, bool G2P, bool P2G, bool EXT> static void set_smem_attr() {

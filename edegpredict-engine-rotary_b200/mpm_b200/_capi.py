@@ -13,7 +13,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libmpm_b200.so"
 
 MPM_ABI_VERSION = 1
 MPM_OK, MPM_INVALID_ARG, MPM_OOM, MPM_CUDA_ERROR, MPM_NUMERIC, MPM_OUT_OF_GRID, MPM_TIMEOUT, \
-    MPM_NOT_SUPPORTED, MPM_CAPACITY = range(9)
+    MPM_NOT_SUPPORTED, MPM_CAPACITY, MPM_CANCELLED = range(10)
 ACTIVE, INACTIVE, CHIP, BOUNDARY, FIXED = 0, 1, 2, 3, 4
 PREC_F32, PREC_F64 = 0, 1
 TOOL_NONE, TOOL_RASTER, TOOL_SDF_STICKY, TOOL_SDF_SLIP = 0, 1, 2, 3
@@ -88,7 +88,7 @@ PARTICLE_FIELDS = {  # name -> values per particle
     "plastic_strain": 1, "strain_rate": 1, "temperature": 1, "damage": 1, "residual_stress": 1,
 }
 
-REQ_UNKNOWN, REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = range(5)
+REQ_UNKNOWN, REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED = range(6)
 
 
 class MpmRequest(C.Structure):
@@ -115,7 +115,7 @@ class MpmServerConfig(C.Structure):
 class MpmServerStats(C.Structure):
     _fields_ = [("offered", _i64), ("admitted", _i64), ("completed", _i64), ("failed", _i64), ("queued", _i64),
                 ("resident", _i64), ("particle_updates", _i64), ("resident_particles", _i64), ("ticks", _i64),
-                ("busy_seconds", _d)]
+                ("busy_seconds", _d), ("cancelled", _i64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -166,12 +166,14 @@ def lib() -> C.CDLL:
             "mpm_batch_step": (_i32, [_vp, P(_d), _i32]),
             "mpm_batch_sync_metrics": (_i32, [_vp, _i32, P(MpmMetrics)]),
             "mpm_batch_get_counts": (_i32, [_vp, _i32, P(_i64), P(_i64), P(_d)]),
+            "mpm_batch_instance_status": (_i32, [_vp, P(_i32), _i32]),
             "mpm_batch_change": (_i32, [_vp, P(MpmParams), P(_i64), _i32, P(_i32), _i32, P(_i32)]),
             "mpm_server_create": (_i32, [P(MpmServerConfig), _vp, P(_vp)]),
             "mpm_server_destroy": (_i32, [_vp]),
             "mpm_server_submit": (_i32, [_vp, P(MpmRequest), P(_i64)]),
             "mpm_server_tick": (_i32, [_vp, P(_i32)]),
             "mpm_server_poll": (_i32, [_vp, _i64, P(MpmResult)]),
+            "mpm_server_cancel": (_i32, [_vp, _i64]),
             "mpm_server_stats_get": (_i32, [_vp, P(MpmServerStats)]),
             "mpm_server_footprint": (_i32, [P(MpmServerConfig), P(MpmRequest), P(_i64)]),
             "mpm_get_launch_config": (_i32, [_vp, P(MpmLaunchConfig)]),

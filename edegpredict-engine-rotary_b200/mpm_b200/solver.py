@@ -148,10 +148,24 @@ class Solver:
         s, keep, n = soa_in(parts, elem)
         self._check(self._lib.mpm_upload(self.h, C.byref(s), n))
 
-    def download(self, fields=None, elem: int = 8) -> Dict[str, np.ndarray]:
+    def download(self, fields=None, elem: int = 8, strict: bool = True) -> Dict[str, np.ndarray]:
+        """The particle state in upload order.  strict=False also returns the
+        state of a workpiece whose error word is set (MPM_NUMERIC), for
+        inspection."""
         s, out = soa_out(self.counts()[0], fields, elem)
-        self._check(self._lib.mpm_download(self.h, C.byref(s)))
+        self._check_state(self._lib.mpm_download(self.h, C.byref(s)), strict)
         return out
+
+    def status(self) -> int:
+        """mpm_status of the workpiece from its device error word (instance 0
+        of the handle): MPM_OK or MPM_NUMERIC."""
+        st = (C.c_int32 * 1)()
+        self._check(self._lib.mpm_batch_instance_status(self.h, st, 1))
+        return int(st[0])
+
+    def _check_state(self, status: int, strict: bool) -> None:
+        if strict or status != A.MPM_NUMERIC:
+            self._check(status)
 
     def download_into(self, bufs: Dict[str, np.ndarray], elem: int = 8) -> None:
         """Download into caller-owned arrays (e.g. pinned host memory)."""
@@ -290,9 +304,9 @@ class Batch(Solver):
         s, keep, n = soa_in(parts, elem)
         self._check(self._lib.mpm_batch_upload(self.h, int(i), C.byref(s), n))
 
-    def download_i(self, i: int, fields=None, elem: int = 8) -> Dict[str, np.ndarray]:
+    def download_i(self, i: int, fields=None, elem: int = 8, strict: bool = True) -> Dict[str, np.ndarray]:
         s, out = soa_out(self.counts_i(i)[0], fields, elem)
-        self._check(self._lib.mpm_batch_download(self.h, int(i), C.byref(s)))
+        self._check_state(self._lib.mpm_batch_download(self.h, int(i), C.byref(s)), strict)
         return out
 
     def step_all(self, dts, nsteps: int = 1) -> None:
@@ -303,6 +317,14 @@ class Batch(Solver):
         m = A.MpmMetrics()
         self._check(self._lib.mpm_batch_sync_metrics(self.h, int(i), C.byref(m)))
         return m.as_dict()
+
+    def instance_status(self) -> list:
+        """mpm_status of every instance from its device error word (MPM_OK or
+        MPM_NUMERIC; MPM_TIMEOUT for all after a bounded wait gave up)."""
+        n = self.count()
+        st = (C.c_int32 * max(n, 1))()
+        self._check(self._lib.mpm_batch_instance_status(self.h, st, n))
+        return list(st[:n])
 
     def counts_i(self, i: int):
         n, k, t = C.c_int64(), C.c_int64(), C.c_double()
@@ -382,10 +404,16 @@ class Server:
             pass
 
     def submit(self, case: dict, nsteps: int, dt: Optional[float] = None) -> int:
-        r = make_request(case, nsteps, self.precision, dt)
+        return self.submit_request(make_request(case, nsteps, self.precision, dt))
+
+    def submit_request(self, r: A.MpmRequest) -> int:
         i = C.c_int64()
         A.check(self._lib.mpm_server_submit(self.h, C.byref(r), C.byref(i)))
         return i.value
+
+    def cancel(self, rid: int) -> None:
+        """Cancels a queued request at once, a running one at the next tick."""
+        A.check(self._lib.mpm_server_cancel(self.h, int(rid)))
 
     def tick(self) -> int:
         n = C.c_int32()

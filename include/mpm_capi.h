@@ -34,7 +34,8 @@ typedef enum mpm_status {
     MPM_OUT_OF_GRID = 5,
     MPM_TIMEOUT = 6,      /* a bounded device-side wait gave up */
     MPM_NOT_SUPPORTED = 7,
-    MPM_CAPACITY = 8      /* more particles or instances than the handle holds */
+    MPM_CAPACITY = 8,     /* more particles or instances than the handle holds */
+    MPM_CANCELLED = 9     /* a served request cancelled by mpm_server_cancel */
 } mpm_status;
 
 /* Particle status codes: ParticleStatus, include/Types.h:37-43. */
@@ -334,6 +335,24 @@ mpm_status mpm_batch_set_tool_sdf(mpm_handle *h, int32_t inst, const mpm_tool_sd
 /* nsteps steps of every instance; dt[i] is instance i's step (n_instances values). */
 mpm_status mpm_batch_step(mpm_handle *h, const double *dt, int32_t nsteps);
 mpm_status mpm_batch_sync_metrics(mpm_handle *h, int32_t inst, mpm_metrics *out);
+/* Failure detection per workpiece (the reference has one host-side health
+ * check per simulation, SimulationHealthMonitor::check, which halts it:
+ * include/SimulationHealthMonitor.h:321-328).  Every instance has an error
+ * word that only its own failures mark: in the step kernel, a particle whose
+ * position is not finite (the kill zone deactivates it, as the reference's
+ * does) or a Newton return that did not converge; a NaN or Inf velocity or
+ * stress reaches the positions through the grid within one step.
+ * mpm_batch_sync_metrics also marks the word when a sum over the live
+ * particles (mass, momentum, energies, plastic strain) is not finite.
+ * status[i] (n >= the instance count) receives MPM_OK or MPM_NUMERIC per
+ * instance (MPM_TIMEOUT for all when a bounded device wait gave up).
+ * mpm_batch_sync_metrics, mpm_batch_download and mpm_export_aos report the
+ * status of their own instance (the data is written all the same), so a
+ * failed workpiece can be dropped (mpm_batch_change) while the others run
+ * on.  mpm_batch_upload and mpm_batch_init_box clear the instance's word;
+ * the word moves with its instance across mpm_batch_change.  Works on a
+ * plain handle too (one instance).  Synchronises the handle's stream. */
+mpm_status mpm_batch_instance_status(mpm_handle *h, int32_t *status, int32_t n);
 mpm_status mpm_batch_get_counts(const mpm_handle *h, int32_t inst, int64_t *n_particles, int64_t *n_steps,
                                 double *time);
 /* Drops the n_remove listed instances (their state is freed; the indices of
@@ -383,11 +402,12 @@ typedef struct mpm_request {
     double dt, T0;
 } mpm_request;
 
-enum { MPM_REQ_UNKNOWN = 0, MPM_REQ_QUEUED = 1, MPM_REQ_RUNNING = 2, MPM_REQ_DONE = 3, MPM_REQ_FAILED = 4 };
+enum { MPM_REQ_UNKNOWN = 0, MPM_REQ_QUEUED = 1, MPM_REQ_RUNNING = 2, MPM_REQ_DONE = 3, MPM_REQ_FAILED = 4,
+       MPM_REQ_CANCELLED = 5 };
 
 typedef struct mpm_result {
     int32_t state;             /* MPM_REQ_* */
-    int32_t status;            /* mpm_status of a FAILED request */
+    int32_t status;            /* mpm_status of a FAILED (or CANCELLED) request */
     int64_t n_particles;
     int64_t steps_done;
     double t_submit, t_admit, t_done;   /* seconds on the server's clock */
@@ -414,6 +434,7 @@ typedef struct mpm_server_stats {
     int64_t resident_particles;
     int64_t ticks;
     double busy_seconds;       /* time spent inside mpm_server_tick */
+    int64_t cancelled;
 } mpm_server_stats;
 
 typedef struct mpm_server mpm_server;
@@ -424,6 +445,15 @@ mpm_status mpm_server_destroy(mpm_server *s);
 mpm_status mpm_server_submit(mpm_server *s, const mpm_request *req, int64_t *id);
 mpm_status mpm_server_tick(mpm_server *s, int32_t *n_resident);
 mpm_status mpm_server_poll(mpm_server *s, int64_t id, mpm_result *out);
+/* Cancels a request: a queued one leaves the queue at once, a running one is
+ * dropped from the device at the next tick (its steps so far are counted);
+ * both end in MPM_REQ_CANCELLED with status MPM_CANCELLED.  A request that
+ * already ended keeps its state.  May be called from another thread than
+ * tick.  A running request whose workpiece fails (its instance error word is
+ * set, see mpm_batch_instance_status) ends in MPM_REQ_FAILED with status
+ * MPM_NUMERIC at the tick that stepped it and is dropped at the next one;
+ * the other requests run on. */
+mpm_status mpm_server_cancel(mpm_server *s, int64_t id);
 mpm_status mpm_server_stats_get(mpm_server *s, mpm_server_stats *out);
 /* Device bytes a request holds while resident (host-only arithmetic). */
 mpm_status mpm_server_footprint(const mpm_server_config *cfg, const mpm_request *req, int64_t *bytes);

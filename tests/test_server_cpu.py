@@ -56,6 +56,10 @@ struct FakeOps {
         m->mass = steps[inst];     // steps this instance has seen
         return MPM_OK;
     }
+    mpm_status health(std::vector<int32_t>& st) {
+        assert(st.size() == caps.size());
+        return MPM_OK;
+    }
 };
 
 static mpm_request req(int cells_x, int nsteps) {
@@ -151,6 +155,162 @@ def test_scheduler_with_fake_engine(tmp_path):
     src = tmp_path / "sched.cpp"
     src.write_text(PROG)
     exe = tmp_path / "sched"
+    r = subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-I", str(CORE), "-I", str(ROOT / "include"),
+                        str(src), "-o", str(exe), "-pthread"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0 and out.stdout.strip() == "OK", out.stderr
+
+
+FAULTS = r"""
+#include <cassert>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+#include "mpm_server_core.h"
+using namespace mpmb;
+
+// A fake engine whose faults are made on the host: instance errors that the
+// health read reports (as the device error words would), and an instance
+// change that fails like an allocator that is out of memory.
+struct FaultyOps {
+    std::vector<int64_t> caps;   // particles per instance: the request's tag
+    std::vector<int> steps;
+    int64_t bad_tag = -1;        // the instance holding this many particles fails after a step
+    int oom_changes = 0;         // the next n instance changes fail
+    std::vector<int> removed_tags;
+    mpm_status change(const std::vector<mpm_params>& add, const std::vector<int64_t>& c,
+                      const std::vector<int32_t>& remove, int* first) {
+        if (oom_changes > 0) {
+            --oom_changes;
+            return MPM_OOM;
+        }
+        for (auto it = remove.rbegin(); it != remove.rend(); ++it) {
+            removed_tags.push_back((int)caps[*it]);
+            caps.erase(caps.begin() + *it);
+            steps.erase(steps.begin() + *it);
+        }
+        *first = (int)caps.size();
+        for (size_t k = 0; k < add.size(); ++k) { caps.push_back(c[k]); steps.push_back(0); }
+        return MPM_OK;
+    }
+    mpm_status init(int inst, const mpm_request&, int64_t* np) { *np = caps[inst]; return MPM_OK; }
+    mpm_status step(int k, const std::vector<double>&) {
+        for (auto& s : steps) s += k;
+        return MPM_OK;
+    }
+    mpm_status metrics(int inst, mpm_metrics* m) { m->mass = steps[inst]; return MPM_OK; }
+    mpm_status health(std::vector<int32_t>& st) {
+        assert(st.size() == caps.size());
+        for (size_t i = 0; i < caps.size(); ++i) st[i] = caps[i] == bad_tag ? MPM_NUMERIC : MPM_OK;
+        return MPM_OK;
+    }
+};
+
+static mpm_request req(int cells_x, int nsteps) {
+    mpm_request r{};
+    r.params.nx = 16; r.params.ny = 16; r.params.nz = 16;
+    r.c1[0] = cells_x; r.c1[1] = 1; r.c1[2] = 1;
+    r.ppc = 1; r.nsteps = nsteps; r.dt = 1e-9;
+    return r;
+}
+
+int main() {
+    double now = 0.0;
+    Pools pools;
+    pools.particles = 1000; pools.nodes = 1 << 20; pools.keys = 1 << 20; pools.bins = 1 << 20;
+    int32_t nres = 0;
+    mpm_result r;
+
+    // 1. a workpiece that fails is ended FAILED and dropped; the others run on
+    {
+        FaultyOps ops;
+        ops.bad_tag = 20;
+        Scheduler<FaultyOps> s(&ops, pools, 10, 8, [&]() { now += 1.0; return now; });
+        int64_t a, b, c;
+        s.submit(req(10, 30), &a);
+        s.submit(req(20, 30), &b);   // fails at its first step
+        s.submit(req(30, 30), &c);
+        assert(s.tick(&nres) == MPM_OK && nres == 3);
+        s.poll(b, &r);
+        assert(r.state == MPM_REQ_FAILED && r.status == MPM_NUMERIC && r.steps_done == 10);
+        s.poll(a, &r);
+        assert(r.state == MPM_REQ_RUNNING && r.steps_done == 10);
+        assert(s.tick(&nres) == MPM_OK && nres == 2);        // evicted
+        assert(ops.removed_tags.size() == 1 && ops.removed_tags[0] == 20);
+        assert(s.tick(&nres) == MPM_OK);
+        s.poll(a, &r);
+        assert(r.state == MPM_REQ_DONE && r.steps_done == 30 && r.metrics.mass == 30);
+        s.poll(c, &r);
+        assert(r.state == MPM_REQ_DONE && r.metrics.mass == 30);
+        mpm_server_stats st = s.stats();
+        assert(st.completed == 2 && st.failed == 1 && st.cancelled == 0);
+        assert(st.particle_updates == 10 * 30 + 20 * 10 + 30 * 30);
+    }
+    // 2. cancel: a queued request leaves at once, a running one at the next tick
+    {
+        FaultyOps ops;
+        Scheduler<FaultyOps> s(&ops, pools, 10, 1, [&]() { now += 1.0; return now; });
+        int64_t a, b;
+        s.submit(req(10, 100), &a);
+        s.submit(req(20, 100), &b);
+        assert(s.cancel(b) == MPM_OK);
+        s.poll(b, &r);
+        assert(r.state == MPM_REQ_CANCELLED && r.status == MPM_CANCELLED && r.steps_done == 0);
+        assert(s.tick(&nres) == MPM_OK && nres == 1);
+        assert(s.cancel(a) == MPM_OK);
+        s.poll(a, &r);
+        assert(r.state == MPM_REQ_RUNNING);                  // still resident until the next tick
+        assert(s.tick(&nres) == MPM_OK && nres == 0);
+        s.poll(a, &r);
+        assert(r.state == MPM_REQ_CANCELLED && r.steps_done == 10);
+        assert(ops.removed_tags.size() == 1 && ops.removed_tags[0] == 10);
+        assert(s.cancel(a) == MPM_OK);                       // an ended request keeps its state
+        s.poll(a, &r);
+        assert(r.state == MPM_REQ_CANCELLED);
+        assert(s.cancel(12345) == MPM_INVALID_ARG);
+        mpm_request nan_t0 = req(5, 10);
+        nan_t0.T0 = std::nan("");
+        assert(s.submit(nan_t0, &b) == MPM_INVALID_ARG);     // refused at the door
+        mpm_server_stats st = s.stats();
+        assert(st.cancelled == 2 && st.completed == 0 && st.queued == 0);
+    }
+    // 3. an instance change that fails (out of memory) admits nothing and keeps
+    //    the queue in arrival order; the next tick admits the same requests
+    {
+        FaultyOps ops;
+        Scheduler<FaultyOps> s(&ops, pools, 10, 8, [&]() { now += 1.0; return now; });
+        int64_t a, b;
+        s.submit(req(10, 10), &a);
+        s.submit(req(20, 10), &b);
+        ops.oom_changes = 1;
+        assert(s.tick(&nres) == MPM_OOM);
+        s.poll(a, &r);
+        assert(r.state == MPM_REQ_QUEUED);
+        assert(s.stats().queued == 2 && s.stats().resident == 0);
+        assert(s.tick(&nres) == MPM_OK && nres == 2);
+        s.poll(a, &r);
+        assert(r.state == MPM_REQ_DONE && r.metrics.mass == 10);
+        s.poll(b, &r);
+        assert(r.state == MPM_REQ_DONE && r.metrics.mass == 10);
+    }
+    std::printf("OK\n");
+    return 0;
+}
+"""
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="g++ not available")
+def test_scheduler_faults_on_the_host(tmp_path):
+    """Fault injection without a GPU: a workpiece whose error word is set ends
+    FAILED (MPM_NUMERIC) and is dropped while the others finish with their full
+    step counts; cancel ends a queued request at once and a running one at the
+    next tick; a request with a NaN initial temperature is refused; an instance
+    change that fails like an out-of-memory allocator leaves the queue intact
+    for the next tick."""
+    src = tmp_path / "faults.cpp"
+    src.write_text(FAULTS)
+    exe = tmp_path / "faults"
     r = subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-I", str(CORE), "-I", str(ROOT / "include"),
                         str(src), "-o", str(exe), "-pthread"], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-3000:]
