@@ -270,6 +270,22 @@ mpm_status mpm_batch_sync_metrics(mpm_handle* h, int32_t inst, mpm_metrics* out)
     return ret(h, h->eng->metrics(inst, out));
 }
 
+mpm_status mpm_checkpoint_bytes(mpm_handle* h, int32_t inst, int64_t* bytes) {
+    NEED_I(h, inst);
+    if (!bytes) return fail(h, MPM_INVALID_ARG, "bytes is NULL");
+    return ret(h, h->eng->checkpoint_bytes(inst, bytes));
+}
+
+mpm_status mpm_checkpoint_save(mpm_handle* h, int32_t inst, void* buf, int64_t bytes) {
+    NEED_I(h, inst);
+    return ret(h, h->eng->checkpoint_save(inst, buf, bytes));
+}
+
+mpm_status mpm_checkpoint_load(mpm_handle* h, int32_t inst, const void* buf, int64_t bytes) {
+    NEED_I(h, inst);
+    return ret(h, h->eng->checkpoint_load(inst, buf, bytes));
+}
+
 mpm_status mpm_batch_instance_status(mpm_handle* h, int32_t* status, int32_t n) {
     NEED_H(h);
     if (!status) return fail(h, MPM_INVALID_ARG, "status array is NULL");

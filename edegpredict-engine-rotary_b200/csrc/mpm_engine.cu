@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "mpm_engine.h"
+#include "mpm_checkpoint.h"
 
 namespace mpmb {
 
@@ -1451,6 +1452,123 @@ class Engine final : public EngineBase {
         cudaFree(d);
         return MPM_OK;
     }
+    // ---------------------------------------------------------------- checkpoints
+
+    // Device pointer (at the instance's first slot) and bytes per particle of
+    // every array of a checkpoint, in the order of ckpt_array_elem.
+    std::vector<std::pair<char*, size_t>> ckpt_arrays(const PState<R>& s, int64_t pbase) const {
+        const size_t v4 = sizeof(V4<R>);
+        std::vector<std::pair<char*, size_t>> a;
+        for (int k = 0; k < 6; ++k) a.push_back({(char*)(s.A[k] + pbase), v4});
+        for (int k = 0; k < 4; ++k) a.push_back({(char*)(s.B[k] + pbase), v4});
+        for (int k = 0; k < 2; ++k) a.push_back({(char*)(s.S[k] + pbase), v4});
+        if (has_K)
+            for (int k = 0; k < 2; ++k) a.push_back({(char*)(s.K[k] + pbase), v4});
+        if (kPosLo) a.push_back({(char*)(s.X + pbase), v4});
+        a.push_back({(char*)(s.sres + pbase), sizeof(R)});
+        a.push_back({(char*)(s.status + pbase), 1});
+        a.push_back({(char*)(s.asb + pbase), 1});
+        a.push_back({(char*)(s.id + pbase), 4});
+        a.push_back({(char*)(s.bin + pbase), 4});
+        a.push_back({(char*)(s.orig + pbase), 4});
+        return a;
+    }
+    int ckpt_samples(const InstHost& x) const { return x.tool.mode == MPM_TOOL_RASTER ? x.n_samples : 0; }
+
+    mpm_status checkpoint_bytes(int i, int64_t* bytes) override {
+        const InstHost& x = I[i];
+        *bytes = (int64_t)(sizeof(CkptHeader) + ckpt_payload_bytes(prec_, has_K, x.np, ckpt_samples(x)));
+        return MPM_OK;
+    }
+
+    mpm_status checkpoint_save(int i, void* buf, int64_t bytes) override {
+        MS(ensure_binned());
+        InstHost& x = I[i];
+        const int ns = ckpt_samples(x);
+        const uint64_t pay = ckpt_payload_bytes(prec_, has_K, x.np, ns);
+        if (!buf || bytes < (int64_t)(sizeof(CkptHeader) + pay)) {
+            err = "checkpoint buffer NULL or smaller than mpm_checkpoint_bytes";
+            return MPM_INVALID_ARG;
+        }
+        unsigned char* q = static_cast<unsigned char*>(buf) + sizeof(CkptHeader);
+        for (const auto& a : ckpt_arrays(ps[cur], x.pbase)) {
+            if (x.np > 0) CK(cudaMemcpyAsync(q, a.first, a.second * x.np, cudaMemcpyDeviceToHost, st));
+            q += a.second * x.np;
+        }
+        if (ns > 0) CK(cudaMemcpyAsync(q, x.d_samples, 24 * (size_t)ns, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        CkptHeader h;
+        std::memset(&h, 0, sizeof(h));
+        std::memcpy(h.magic, kCkptMagic, sizeof(kCkptMagic));
+        h.version = kCkptVersion;
+        h.abi_version = MPM_ABI_VERSION;
+        h.precision = prec_;
+        h.has_K = has_K ? 1 : 0;
+        h.n_samples = ns;
+        h.np = x.np;
+        h.step = x.step;
+        h.time = x.time;
+        h.tool_t0 = x.tool_t0;
+        h.dt = x.dt;
+        h.payload_bytes = pay;
+        h.checksum = ckpt_checksum(static_cast<const unsigned char*>(buf) + sizeof(CkptHeader), pay);
+        h.params = x.p;
+        h.tool = x.tool;
+        h.tool.sample_dx = h.tool.sample_dy = h.tool.sample_dz = nullptr;
+        std::memcpy(buf, &h, sizeof(h));
+        return MPM_OK;
+    }
+
+    mpm_status checkpoint_load(int i, const void* buf, int64_t bytes) override {
+        InstHost& x = I[i];
+        CkptHeader h;
+        mpm_status s = ckpt_check(buf, bytes, prec_, has_K, x.p.nx, x.p.ny, x.p.nz, x.cap, &h, &err);
+        if (s != MPM_OK) return s;
+        if ((s = check_params(&h.params, &err)) != MPM_OK) return s;
+        if (h.params.H_kin > 0.0 && !has_K) {
+            err = "checkpoint uses backstress (H_kin > 0); the handle has no backstress state";
+            return MPM_NOT_SUPPORTED;
+        }
+        CK(cudaStreamSynchronize(st));   // nothing in flight uses the instance's slots
+        const unsigned char* q = static_cast<const unsigned char*>(buf) + sizeof(CkptHeader);
+        const int64_t n = h.np;
+        for (const auto& a : ckpt_arrays(ps[cur], x.pbase)) {
+            const bool is_K = has_K && !h.has_K && (a.first == (char*)(ps[cur].K[0] + x.pbase) ||
+                                                    a.first == (char*)(ps[cur].K[1] + x.pbase));
+            if (is_K) {
+                // a checkpoint without backstress into a handle that has it: zero
+                if (n > 0) CK(cudaMemsetAsync(a.first, 0, a.second * n, st));
+                continue;
+            }
+            if (n > 0) CK(cudaMemcpyAsync(a.first, q, a.second * n, cudaMemcpyHostToDevice, st));
+            q += a.second * n;
+        }
+        if (x.d_samples) {
+            CK(cudaStreamSynchronize(st));
+            cudaFree(x.d_samples);
+            x.d_samples = nullptr;
+        }
+        x.n_samples = 0;
+        if (h.n_samples > 0) {
+            CK(cudaMalloc(&x.d_samples, 24 * (size_t)h.n_samples));
+            CK(cudaMemcpyAsync(x.d_samples, q, 24 * (size_t)h.n_samples, cudaMemcpyHostToDevice, st));
+            x.n_samples = h.n_samples;
+        }
+        CK(cudaMemsetAsync(d_ierr + i, 0, sizeof(int), st));
+        CK(cudaStreamSynchronize(st));
+        x.p = h.params;
+        x.tool = h.tool;
+        x.np = n;
+        x.step = h.step;
+        x.time = h.time;
+        x.tool_t0 = h.tool_t0;
+        x.dt = h.dt;
+        x.fresh = 0;
+        x.ext_pending = false;
+        binned = false;   // the next call that needs bins re-bins from the loaded bins
+        return push_insts();
+    }
+
     mpm_status reset_clock(int i) override {
         I[i].time = 0.0;
         I[i].step = 0;

@@ -78,6 +78,10 @@ class EngineBase {
     // Status of every instance from its error word (MPM_OK, MPM_NUMERIC; all
     // MPM_TIMEOUT when a bounded wait gave up); synchronises the stream.
     virtual mpm_status inst_statuses(int32_t* out, int n) = 0;
+    // Checkpoint of one instance (format: mpm_checkpoint.h).
+    virtual mpm_status checkpoint_bytes(int inst, int64_t* bytes) = 0;
+    virtual mpm_status checkpoint_save(int inst, void* buf, int64_t bytes) = 0;
+    virtual mpm_status checkpoint_load(int inst, const void* buf, int64_t bytes) = 0;
     virtual int n_inst() const = 0;
     virtual const InstHost& inst(int i) const = 0;
     virtual cudaStream_t stream() const = 0;

@@ -167,6 +167,9 @@ def lib() -> C.CDLL:
             "mpm_batch_sync_metrics": (_i32, [_vp, _i32, P(MpmMetrics)]),
             "mpm_batch_get_counts": (_i32, [_vp, _i32, P(_i64), P(_i64), P(_d)]),
             "mpm_batch_instance_status": (_i32, [_vp, P(_i32), _i32]),
+            "mpm_checkpoint_bytes": (_i32, [_vp, _i32, P(_i64)]),
+            "mpm_checkpoint_save": (_i32, [_vp, _i32, _vp, _i64]),
+            "mpm_checkpoint_load": (_i32, [_vp, _i32, _vp, _i64]),
             "mpm_batch_change": (_i32, [_vp, P(MpmParams), P(_i64), _i32, P(_i32), _i32, P(_i32)]),
             "mpm_server_create": (_i32, [P(MpmServerConfig), _vp, P(_vp)]),
             "mpm_server_destroy": (_i32, [_vp]),

@@ -163,6 +163,21 @@ class Solver:
         self._check(self._lib.mpm_batch_instance_status(self.h, st, 1))
         return int(st[0])
 
+    def checkpoint(self, inst: int = 0) -> np.ndarray:
+        """The workpiece's checkpoint (mpm_checkpoint_save) as a byte array;
+        write it to a file with .tofile() or keep it in memory."""
+        n = C.c_int64()
+        self._check(self._lib.mpm_checkpoint_bytes(self.h, int(inst), C.byref(n)))
+        buf = np.empty(n.value, dtype=np.uint8)
+        self._check(self._lib.mpm_checkpoint_save(self.h, int(inst), buf.ctypes.data, buf.nbytes))
+        return buf
+
+    def restore(self, ckpt, inst: int = 0) -> None:
+        """Loads a checkpoint (bytes or a uint8 array) into the workpiece."""
+        buf = np.frombuffer(ckpt, dtype=np.uint8) if isinstance(ckpt, (bytes, bytearray)) else \
+            np.ascontiguousarray(ckpt, dtype=np.uint8)
+        self._check(self._lib.mpm_checkpoint_load(self.h, int(inst), buf.ctypes.data, buf.nbytes))
+
     def _check_state(self, status: int, strict: bool) -> None:
         if strict or status != A.MPM_NUMERIC:
             self._check(status)

@@ -353,6 +353,24 @@ mpm_status mpm_batch_sync_metrics(mpm_handle *h, int32_t inst, mpm_metrics *out)
  * the word moves with its instance across mpm_batch_change.  Works on a
  * plain handle too (one instance).  Synchronises the handle's stream. */
 mpm_status mpm_batch_instance_status(mpm_handle *h, int32_t *status, int32_t n);
+
+/* Checkpoint and resume of one workpiece (no counterpart in the reference,
+ * which serialises no state).  A checkpoint is a versioned header (format
+ * version, ABI version, precision, step count, clock, mpm_params, tool) and
+ * the instance's particle state exactly as it is held on the device, with a
+ * 64-bit checksum; a serving loop can preempt a workpiece and resume it later,
+ * in this handle or another.  Loading needs an instance of the same
+ * precision and grid size (nx, ny, nz) with room for the particles; it
+ * replaces the instance's parameters, tool, clock and particles, and clears
+ * its error word.  A voxel tool SDF (mpm_set_tool_sdf) is not part of the
+ * checkpoint: set it again after loading.  The state is written to and read
+ * from caller memory (host or pinned); _bytes gives the size.  The particle
+ * order within a cell after the reload's re-bin may differ, so continued
+ * runs agree to summation order (FP64 1e-9), as a batch does with its
+ * instances run alone.  Single-instance handles use inst 0. */
+mpm_status mpm_checkpoint_bytes(mpm_handle *h, int32_t inst, int64_t *bytes);
+mpm_status mpm_checkpoint_save(mpm_handle *h, int32_t inst, void *buf, int64_t bytes);
+mpm_status mpm_checkpoint_load(mpm_handle *h, int32_t inst, const void *buf, int64_t bytes);
 mpm_status mpm_batch_get_counts(const mpm_handle *h, int32_t inst, int64_t *n_particles, int64_t *n_steps,
                                 double *time);
 /* Drops the n_remove listed instances (their state is freed; the indices of
