@@ -877,6 +877,7 @@ __global__ void k_heat_diffuse(const Inst<R>* __restrict__ insts, int n_inst, in
 template <typename R>
 void launch_heat_diffuse(const Inst<R>* insts, int n_inst, int b, int64_t total, cudaStream_t st) {
     if (total <= 0 || n_inst <= 0) return;
+    Range nvtx_range("mpm.heat_diffuse");
     const int64_t blocks = std::min<int64_t>((total + kT - 1) / kT, 148 * 16);
     k_heat_diffuse<R><<<(int)blocks, kT, 0, st>>>(insts, n_inst, b, total);
     ++launch_counter();

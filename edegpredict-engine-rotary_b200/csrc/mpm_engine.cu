@@ -300,6 +300,7 @@ class Engine final : public EngineBase {
     // step call starts from a cleared grid).  Allocations only grow.  The next
     // step re-bins.
     mpm_status relayout(std::vector<InstHost> nI, const std::vector<int>& from) {
+        Range nvtx_range("mpm.relayout");
         CK(cudaStreamSynchronize(st));
         drop_graphs();
         const int n = (int)nI.size();
@@ -704,6 +705,7 @@ class Engine final : public EngineBase {
     // ---------------------------------------------------------------- binning
 
     mpm_status rebin() {
+        Range nvtx_range("mpm.rebin");
         CK(cudaMemsetAsync(d_count, 0, 4 * (nkeys + 1), st));
         launch_pad_counts<R>(d_inst, (int)I.size(), d_key_base, d_count, st);
         launch_bin_count<R>(d_inst, (int)I.size(), ps[cur], d_key_base, true, d_pos, d_key, d_rank, d_count, d_newbin,
@@ -734,6 +736,7 @@ class Engine final : public EngineBase {
 
     mpm_status init_box(int i, const int32_t c0[3], const int32_t c1[3], int32_t ppc, uint64_t seed, uint32_t instance,
                         int32_t fixed_layers, double T0, const mpm_tool_desc* tool) override {
+        Range nvtx_range("mpm.init_box");
         InstHost& x = I[i];
         for (int a = 0; a < 3; ++a)
             if (c1[a] <= c0[a] || c0[a] < 0) {
@@ -789,6 +792,7 @@ class Engine final : public EngineBase {
     static size_t fbytes(const void* p, int elem, int64_t n, int per) { return p ? al256((size_t)elem * n * per) : 0; }
 
     mpm_status upload(int i, const mpm_particles_soa* h, int64_t n) override {
+        Range nvtx_range("mpm.upload");
         InstHost& x = I[i];
         if (!h || (h->elem != 4 && h->elem != 8)) {
             err = "particles.elem must be 4 or 8";
@@ -851,6 +855,7 @@ class Engine final : public EngineBase {
     // ---------------------------------------------------------------- particles out
 
     mpm_status download(int i, mpm_particles_soa* h) override {
+        Range nvtx_range("mpm.download");
         InstHost& x = I[i];
         if (!h || (h->elem != 4 && h->elem != 8)) {
             err = "particles.elem must be 4 or 8";
@@ -897,6 +902,7 @@ class Engine final : public EngineBase {
     }
 
     mpm_status export_aos(int i, void* dst, int64_t bytes) override {
+        Range nvtx_range("mpm.export_aos");
         InstHost& x = I[i];
         if (!dst || bytes < x.np * 504) {
             err = "destination smaller than np * sizeof(MPMParticle) (504 bytes)";
@@ -1006,6 +1012,10 @@ class Engine final : public EngineBase {
     // ---------------------------------------------------------------- step
 
     void raster_all(int k) {
+        bool any = false;
+        for (const auto& x : I) any |= (x.tool.mode == MPM_TOOL_RASTER && x.n_samples > 0);
+        if (!any) return;
+        Range nvtx_range("mpm.tool_raster");
         for (auto& x : I) {
             if (x.tool.mode != MPM_TOOL_RASTER || x.n_samples <= 0) continue;
             const double t = x.time + (double)k * x.dt;
@@ -1020,6 +1030,7 @@ class Engine final : public EngineBase {
     }
 
     mpm_status step(int32_t N, const double* dts) override {
+        Range nvtx_range("mpm.step");
         if (N < 0) {
             err = "nsteps must be >= 0";
             return MPM_INVALID_ARG;
@@ -1154,6 +1165,7 @@ class Engine final : public EngineBase {
     }
 
     mpm_status step_graph(int32_t N, bool ext) {
+        Range nvtx_range("mpm.graph");
         for (auto& g : graphs) {
             if (g.N == N && g.since_sort0 == since_sort && g.cur0 == cur && g.rbuf0 == rbuf && g.ext == (int)ext) {
                 CK(cudaGraphLaunch(g.exec, st));
@@ -1281,6 +1293,7 @@ class Engine final : public EngineBase {
     }
 
     mpm_status rebin_regular() {
+        Range nvtx_range("mpm.rebin");
         // positions are bin-local (no instance is fresh here)
         CK(cudaMemsetAsync(d_count, 0, 4 * (nkeys + 1), st));
         launch_pad_counts<R>(d_inst, (int)I.size(), d_key_base, d_count, st);
@@ -1352,6 +1365,7 @@ class Engine final : public EngineBase {
     }
 
     mpm_status metrics(int i, mpm_metrics* out) override {
+        Range nvtx_range("mpm.metrics");
         if (!out) {
             err = "metrics output is NULL";
             return MPM_INVALID_ARG;
@@ -1482,6 +1496,7 @@ class Engine final : public EngineBase {
     }
 
     mpm_status checkpoint_save(int i, void* buf, int64_t bytes) override {
+        Range nvtx_range("mpm.checkpoint_save");
         MS(ensure_binned());
         InstHost& x = I[i];
         const int ns = ckpt_samples(x);
@@ -1520,6 +1535,7 @@ class Engine final : public EngineBase {
     }
 
     mpm_status checkpoint_load(int i, const void* buf, int64_t bytes) override {
+        Range nvtx_range("mpm.checkpoint_load");
         InstHost& x = I[i];
         CkptHeader h;
         mpm_status s = ckpt_check(buf, bytes, prec_, has_K, x.p.nx, x.p.ny, x.p.nz, x.cap, &h, &err);

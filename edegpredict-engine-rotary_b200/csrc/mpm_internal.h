@@ -5,12 +5,24 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <string>
 
 #include "../../include/mpm_capi.h"
 #include "mpm_device.cuh"
 
 namespace mpmb {
+
+// An NVTX range over a scope: the step's phases show by name on the timeline
+// of Nsight Systems or any other NVTX tool; without a tool attached the push
+// and pop are calls to no-ops.
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range&) = delete;
+    Range& operator=(const Range&) = delete;
+};
 
 // Device copies of an upload (NULL field = MPMParticle default).
 struct DevSoA {

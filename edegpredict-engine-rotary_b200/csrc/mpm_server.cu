@@ -10,6 +10,7 @@
 
 #include "../../include/mpm_capi.h"
 #include "mpm_engine.h"
+#include "mpm_internal.h"
 #include "mpm_server_core.h"
 
 namespace mpmb {
@@ -132,6 +133,7 @@ mpm_status mpm_server_submit(mpm_server* s, const mpm_request* req, int64_t* id)
 
 mpm_status mpm_server_tick(mpm_server* s, int32_t* n_resident) {
     if (!s) return mpmb::fail(MPM_INVALID_ARG, "server is NULL");
+    mpmb::Range nvtx_range("mpm.server_tick");
     const mpm_status st = s->sched->tick(n_resident);
     if (st != MPM_OK) return mpmb::fail(st, s->eng->err);
     return MPM_OK;

@@ -1489,6 +1489,7 @@ void launch_step(const Inst<R>* insts, const Work* work, const int* n_work, int 
                  const StepArgs& a, int rbuf, bool g2p, bool p2g, int threads, int ctas_per_sm, int* err,
                  unsigned long long* counters, cudaStream_t st) {
     (void)threads;
+    Range nvtx_range(g2p && p2g ? "mpm.launch.g2p_p2g" : (g2p ? "mpm.launch.g2p" : "mpm.launch.p2g"));
     static int sms = 0;
     if (!sms) {
         int dev = 0;
