@@ -6,6 +6,8 @@
 #include <algorithm>
 #include <cuda_runtime.h>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "mpm_device.cuh"
 #include "mpm_internal.h"
 
@@ -247,7 +249,7 @@ template <typename R>
 __global__ void k_bin_scatter(PState<R> src, PState<R> dst, const Inst<R>* insts, int n_inst, const int32_t* key,
                               const int32_t* rank, const int32_t* offset, const int32_t* key_base,
                               const int32_t* newbin, bool initial, const double* pos_scratch, bool has_K,
-                              int64_t np) {
+                              int64_t np, bool det) {
     const int64_t pi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pi >= np) return;
     const int ii = find_inst(insts, n_inst, pi);
@@ -264,7 +266,8 @@ __global__ void k_bin_scatter(PState<R> src, PState<R> dst, const Inst<R>* insts
         const int64_t b0 = offset[fk];
         const int n = offset[fk + kCellsPerBin] - (int)b0;
         const int r = (int)(offset[kk] - b0) + rank[pi];
-        d = b0 + in_bin_slot(r, n);
+        // deterministic mode keeps each cell's particles together, in rank order
+        d = b0 + (det ? (int64_t)r : in_bin_slot(r, n));
     }
     const int nbv[3] = {nbn % P.nbx, (nbn / P.nbx) % P.nby, nbn / (P.nbx * P.nby)};
     V4<R> a0 = src.A[0][pi];
@@ -307,6 +310,64 @@ __global__ void k_bin_scatter(PState<R> src, PState<R> dst, const Inst<R>* insts
 
 // Unused slots of each instance are counted into the instance's last key so
 // that the global scan keeps every instance at its own slot range.
+// ------------------------------------------------------------------ deterministic ranks
+
+// Every slot's sort key (unused slots: their instance's pad key) and its index.
+template <typename R>
+__global__ void k_det_keys(const Inst<R>* insts, int n_inst, const int32_t* key_base, const int32_t* key,
+                           int32_t* keys2, int32_t* slots, int64_t np) {
+    const int64_t pi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pi >= np) return;
+    const int ii = find_inst(insts, n_inst, pi);
+    const Inst<R>& P = insts[ii];
+    keys2[pi] = pi < P.pbase + P.np ? key[pi] : key_base[ii] + P.nbins * kCellsPerBin + 1;
+    slots[pi] = (int32_t)pi;
+}
+
+// The rank of each live slot within its key: its place in the stably sorted
+// order less the key's first place.
+template <typename R>
+__global__ void k_det_rank(const Inst<R>* insts, int n_inst, const int32_t* sorted_keys, const int32_t* perm,
+                           const int32_t* offset, int32_t* rank, int64_t np) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= np) return;
+    const int32_t pi = perm[j];
+    rank[pi] = (int32_t)(j - offset[sorted_keys[j]]);
+}
+
+static int key_bits(int64_t nkeys) {
+    int b = 1;
+    while (b < 31 && ((int64_t)1 << b) <= nkeys) ++b;
+    return b;
+}
+
+size_t det_rank_tmp_bytes(int64_t np, int64_t nkeys) {
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const int32_t*)nullptr, (int32_t*)nullptr,
+                                    (const int32_t*)nullptr, (int32_t*)nullptr, (int)np, 0, key_bits(nkeys));
+    return bytes;
+}
+
+template <typename R>
+void launch_det_ranks(const Inst<R>* insts, int n_inst, const int32_t* key_base, int32_t* key, const int32_t* offset,
+                      int32_t* rank, int64_t np, int64_t nkeys, int32_t* keys2, int32_t* slots, int32_t* perm,
+                      int32_t* sorted, void* tmp, size_t tmp_bytes, cudaStream_t st) {
+    if (np <= 0) return;
+    const int blocks = (int)((np + kT - 1) / kT);
+    k_det_keys<R><<<blocks, kT, 0, st>>>(insts, n_inst, key_base, key, keys2, slots, np);
+    // the radix sort is stable: slots with equal keys keep their order
+    size_t bytes = tmp_bytes;
+    cub::DeviceRadixSort::SortPairs(tmp, bytes, keys2, sorted, slots, perm, (int)np, 0, key_bits(nkeys), st);
+    k_det_rank<R><<<blocks, kT, 0, st>>>(insts, n_inst, sorted, perm, offset, rank, np);
+    launch_counter() += 2;
+}
+template void launch_det_ranks<float>(const Inst<float>*, int, const int32_t*, int32_t*, const int32_t*, int32_t*,
+                                      int64_t, int64_t, int32_t*, int32_t*, int32_t*, int32_t*, void*, size_t,
+                                      cudaStream_t);
+template void launch_det_ranks<double>(const Inst<double>*, int, const int32_t*, int32_t*, const int32_t*, int32_t*,
+                                       int64_t, int64_t, int32_t*, int32_t*, int32_t*, int32_t*, void*, size_t,
+                                       cudaStream_t);
+
 template <typename R>
 __global__ void k_pad_counts(const Inst<R>* insts, int n_inst, const int32_t* key_base, int32_t* count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -714,10 +775,11 @@ template <typename R>
 void launch_bin_scatter(const PState<R>& src, const PState<R>& dst, const Inst<R>* insts, int n_inst,
                         const int32_t* key, const int32_t* rank, const int32_t* offset, const int32_t* key_base,
                         const int32_t* newbin, bool initial, const double* pos_scratch, bool has_K, int64_t np,
-                        cudaStream_t st) {
+                        cudaStream_t st, bool det) {
     if (np <= 0) return;
     k_bin_scatter<R><<<(int)((np + kT - 1) / kT), kT, 0, st>>>(src, dst, insts, n_inst, key, rank, offset,
-                                                               key_base, newbin, initial, pos_scratch, has_K, np);
+                                                               key_base, newbin, initial, pos_scratch, has_K, np,
+                                                               det);
     ++launch_counter();
 }
 
@@ -888,7 +950,7 @@ void launch_heat_diffuse(const Inst<R>* insts, int n_inst, int b, int64_t total,
                                       int32_t*, int32_t*, int32_t*, int32_t*, int64_t, cudaStream_t);               \
     template void launch_bin_scatter<R>(const PState<R>&, const PState<R>&, const Inst<R>*, int, const int32_t*,    \
                                         const int32_t*, const int32_t*, const int32_t*, const int32_t*, bool,       \
-                                        const double*, bool, int64_t, cudaStream_t);                                 \
+                                        const double*, bool, int64_t, cudaStream_t, bool);                           \
     template void launch_import<R>(const DevSoA&, int64_t, double, double, double, double, double, const PState<R>&, \
                                    int64_t, double*, cudaStream_t);                                                  \
     template void launch_gen<R>(const Inst<R>&, const int32_t*, const int32_t*, int, uint64_t, uint32_t, int, double, \

@@ -134,6 +134,15 @@ class Engine final : public EngineBase {
     int sort_every = 16, threads = 128, ctas_per_sm = 4, prec_ = MPM_PREC_F32;
     bool use_graph = false;
     int rbuf = 0;
+    // deterministic mode (mpm_launch_config.deterministic): the scatter payload
+    // (24 rows of cap_total reals) and the stable-sort scratch of the re-bin
+    bool det = false;
+    R* d_det_pay = nullptr;
+    int64_t det_pay_alloc = 0;
+    int32_t* d_det_i32[4] = {nullptr, nullptr, nullptr, nullptr};
+    int64_t det_i32_alloc[4] = {0, 0, 0, 0};
+    unsigned char* d_det_tmp = nullptr;
+    int64_t det_tmp_alloc = 0;
     // step-kernel timing (mpm_profile_enable)
     bool prof = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -181,7 +190,7 @@ class Engine final : public EngineBase {
                         d_bin_local,
                         d_inst_pbase, d_key, d_rank, d_newbin, d_count, d_offset, d_flag, d_flag_scan, d_scan_tmp,
                         d_pos, d_work, d_nwork, d_err, d_ierr, d_ctr, d_stat_part, d_stat_out, d_stage, d_gen,
-                        d_map};
+                        d_map, d_det_pay, d_det_i32[0], d_det_i32[1], d_det_i32[2], d_det_i32[3], d_det_tmp};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         for (auto& x : I)
@@ -704,6 +713,30 @@ class Engine final : public EngineBase {
 
     // ---------------------------------------------------------------- binning
 
+    // Deterministic mode: scratch for the payload and the stable sort (grown
+    // outside any graph capture: the mode runs without graphs).
+    mpm_status det_scratch() {
+        const int64_t tmp = (int64_t)det_rank_tmp_bytes(cap_total, nkeys);
+        bool more = det_pay_alloc < 24 * std::max<int64_t>(cap_total, 1) || det_tmp_alloc < std::max<int64_t>(tmp, 1);
+        for (int k = 0; k < 4; ++k) more = more || det_i32_alloc[k] < std::max<int64_t>(cap_total, 1);
+        if (!more) return MPM_OK;
+        CK(cudaStreamSynchronize(st));   // nothing in flight uses the old buffers
+        MS(grow(d_det_pay, det_pay_alloc, 24 * std::max<int64_t>(cap_total, 1), false));
+        for (int k = 0; k < 4; ++k) MS(grow(d_det_i32[k], det_i32_alloc[k], cap_total));
+        MS(grow(d_det_tmp, det_tmp_alloc, tmp));
+        return MPM_OK;
+    }
+    // Deterministic mode: ranks within each key in slot order (the scatter then
+    // keeps every cell's particles together in that order).
+    mpm_status det_ranks() {
+        if (!det) return MPM_OK;
+        MS(det_scratch());
+        launch_det_ranks<R>(d_inst, (int)I.size(), d_key_base, d_key, d_offset, d_rank, cap_total, nkeys,
+                            d_det_i32[0], d_det_i32[1], d_det_i32[2], d_det_i32[3], d_det_tmp,
+                            (size_t)det_tmp_alloc, st);
+        return MPM_OK;
+    }
+
     mpm_status rebin() {
         Range nvtx_range("mpm.rebin");
         CK(cudaMemsetAsync(d_count, 0, 4 * (nkeys + 1), st));
@@ -711,8 +744,9 @@ class Engine final : public EngineBase {
         launch_bin_count<R>(d_inst, (int)I.size(), ps[cur], d_key_base, true, d_pos, d_key, d_rank, d_count, d_newbin,
                             cap_total, st);
         exclusive_scan(d_count, d_offset, nkeys, d_scan_tmp, st);
+        MS(det_ranks());
         launch_bin_scatter<R>(ps[cur], ps[cur ^ 1], d_inst, (int)I.size(), d_key, d_rank, d_offset, d_key_base,
-                              d_newbin, true, d_pos, has_K, cap_total, st);
+                              d_newbin, true, d_pos, has_K, cap_total, st, det);
         build_work(d_offset, d_bin_key, d_bin_inst, d_bin_local, d_inst_pbase, max_work, d_flag, d_flag_scan,
                    d_scan_tmp, d_work, d_nwork, st);
         cur ^= 1;
@@ -1052,7 +1086,16 @@ class Engine final : public EngineBase {
             ext |= x.ext_pending;
             raster |= (x.tool.mode == MPM_TOOL_RASTER && x.n_samples > 0);
         }
-        if (use_graph && !raster && !prof && max_work > 0)
+        if (det) {
+            for (const auto& x : I)
+                if (x.p.asb_enabled || x.p.heat_conduction || (x.sdf && x.p.contact_every > 0)) {
+                    err = "deterministic mode does not cover the adiabatic shear model, heat conduction or the "
+                          "voxel tool SDF contact";
+                    return MPM_NOT_SUPPORTED;
+                }
+            MS(det_scratch());
+        }
+        if (use_graph && !raster && !prof && max_work > 0 && !det)
             s = step_graph(N, ext);
         else
             s = issue_steps(N, ext);
@@ -1073,10 +1116,11 @@ class Engine final : public EngineBase {
     mpm_status issue_steps(int32_t N, bool ext) {
         mpm_status s = MPM_OK;
         const size_t gbytes = sizeof(V4<R>) * nn_total;
-        const bool fused = I[0].p.schedule == MPM_SCHED_FUSED;
+        // deterministic mode: split schedule, re-binned before every P2G
+        const bool fused = I[0].p.schedule == MPM_SCHED_FUSED && !det;
         int w = rbuf;
         auto maybe_sort = [&]() -> mpm_status {
-            if (since_sort >= sort_every) return rebin_regular();
+            if (since_sort >= sort_every || (det && since_sort > 0)) return rebin_regular();
             return MPM_OK;
         };
         const int cps = ctas_per_sm;
@@ -1124,10 +1168,16 @@ class Engine final : public EngineBase {
                 if ((s = maybe_sort()) != MPM_OK) return s;
                 if ((s = clear(w)) != MPM_OK) return s;
                 StepArgs a{k, 0, 1, (ext && k == 0) ? 1 : 0, k, xk};
+                a.det = det ? 1 : 0;
+                a.det_pay = d_det_pay;
+                a.det_stride = cap_total;
                 prof_begin();
                 launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], a, w, false, true, threads, cps, d_err,
                                d_ctr, st);
                 prof_end();
+                if (det)
+                    launch_p2g_det<R>(d_inst, (int)I.size(), ps[cur], d_det_pay, cap_total, d_key_base, d_offset, w,
+                                      nn_total, st);
                 raster_all(k);
                 diffuse(w);
                 StepArgs c{k, 1, 0, 0, k, xk};
@@ -1227,16 +1277,19 @@ class Engine final : public EngineBase {
         c->ctas_per_sm = ctas_per_sm;
         c->sort_every = sort_every;
         c->use_graph = use_graph ? 1 : 0;
-        c->_pad = 0;
+        c->deterministic = det ? 1 : 0;
         return MPM_OK;
     }
 
     mpm_status set_config(const mpm_launch_config* c) override {
-        if (!c || c->ctas_per_sm < 1 || c->ctas_per_sm > 8 || c->sort_every < 1 || c->sort_every > 1024) {
-            err = "launch config: ctas_per_sm in [1, 8], sort_every in [1, 1024]";
+        if (!c || c->ctas_per_sm < 1 || c->ctas_per_sm > 8 || c->sort_every < 1 || c->sort_every > 1024 ||
+            (c->deterministic != 0 && c->deterministic != 1)) {
+            err = "launch config: ctas_per_sm in [1, 8], sort_every in [1, 1024], deterministic 0 or 1";
             return MPM_INVALID_ARG;
         }
-        if (c->ctas_per_sm != ctas_per_sm || c->sort_every != sort_every) drop_graphs();
+        if (c->ctas_per_sm != ctas_per_sm || c->sort_every != sort_every || (c->deterministic != 0) != det)
+            drop_graphs();
+        det = c->deterministic != 0;
         ctas_per_sm = c->ctas_per_sm;
         sort_every = c->sort_every;
         use_graph = c->use_graph != 0;
@@ -1300,8 +1353,9 @@ class Engine final : public EngineBase {
         launch_bin_count<R>(d_inst, (int)I.size(), ps[cur], d_key_base, false, d_pos, d_key, d_rank, d_count,
                             d_newbin, cap_total, st);
         exclusive_scan(d_count, d_offset, nkeys, d_scan_tmp, st);
+        MS(det_ranks());
         launch_bin_scatter<R>(ps[cur], ps[cur ^ 1], d_inst, (int)I.size(), d_key, d_rank, d_offset, d_key_base,
-                              d_newbin, false, d_pos, has_K, cap_total, st);
+                              d_newbin, false, d_pos, has_K, cap_total, st, det);
         build_work(d_offset, d_bin_key, d_bin_inst, d_bin_local, d_inst_pbase, max_work, d_flag, d_flag_scan,
                    d_scan_tmp, d_work, d_nwork, st);
         cur ^= 1;

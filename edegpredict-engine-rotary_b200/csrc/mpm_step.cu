@@ -949,7 +949,7 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT>& Sm, int cell, 
     }
 }
 
-template <typename R, bool G2P, bool P2G, bool EXT>
+template <typename R, bool G2P, bool P2G, bool EXT, bool DET = false>
 __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __restrict__ insts, const Work* __restrict__ work,
                                               const int* __restrict__ n_work, PState<R> ps, StepArgs sa, int rbuf,
                                               int* __restrict__ err, unsigned long long* __restrict__ ctr) {
@@ -1365,6 +1365,20 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                 S[2] = sf * sig[4]; S[6] = sf * sl[1];
                                 S[5] = sf * sig[5]; S[7] = sf * sl[2];
                             }
+                            if (DET) {
+                                // deterministic mode: the payload goes to global memory and
+                                // k_p2g_det sums it per node in a fixed order (no atomics)
+                                R* dp = static_cast<R*>(sa.det_pay) + pi;
+                                const int64_t ds = sa.det_stride;
+#pragma unroll
+                                for (int a = 0; a < 3; ++a) { dp[a * ds] = xi[a]; dp[(3 + a) * ds] = Q[a]; }
+#pragma unroll
+                                for (int q = 0; q < 9; ++q) { dp[(6 + q) * ds] = Rm[q]; dp[(15 + q) * ds] = S[q]; }
+                                // binned just before this launch, so the base lies in the bin
+                                if (!(bb[0] >= 0 && bb[0] < kBin && bb[1] >= 0 && bb[1] < kBin && bb[2] >= 0 &&
+                                      bb[2] < kBin))
+                                    ++c_esc;
+                            } else {
                             int rank = kCellCap;
                             if (bb[0] >= 0 && bb[0] < kBin && bb[1] >= 0 && bb[1] < kBin && bb[2] >= 0 &&
                                 bb[2] < kBin) {
@@ -1391,6 +1405,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                     scatter_T_global<R>(P, P.tm[rbuf ^ (G2P ? 1 : 0)], g0x, g0y, g0z, xi[0], xi[1],
                                                         xi[2], m * (P.Tamb + dT));
                                 ++c_esc;
+                            }
                             }
                         }
                     }
@@ -1420,7 +1435,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                     c_yield += yielded ? 1 : 0;
                 }
             }
-            if (P2G) {
+            if (P2G && !DET) {
                 __syncthreads();
                 cell_accumulate<R, EXT>(Sm, tid & (kCellsPerBin - 1), tid >> 6, P.pmass, par, P.heat_on != 0);
                 par ^= 1;
@@ -1428,7 +1443,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
             }
         }
 
-        if (P2G) {
+        if (P2G && !DET) {
             // flush the bin's node tile to the grid, clearing it for the next bin
             for (int nidx = tid; nidx < kTileNodes; nidx += kNT) {
                 const int X = nidx % kTile, Y = (nidx / kTile) % kTile, Z = nidx / (kTile * kTile);
@@ -1475,13 +1490,78 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
     else if (errf < 0) atomicOr(err, ERR_NEWTON);
 }
 
-template <typename R, bool G2P, bool P2G, bool EXT> static void set_smem_attr() {
+template <typename R, bool G2P, bool P2G, bool EXT, bool DET = false> static void set_smem_attr() {
     static bool done = false;
     if (!done) {
-        cudaFuncSetAttribute(k_step<R, G2P, P2G, EXT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_step<R, G2P, P2G, EXT, DET>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)step_smem_bytes<R, EXT>());
         done = true;
     }
+}
+
+// Deterministic mode, the P2G sums: one thread per grid node adds the payloads
+// (written by the P2G-only step launch) of the particles in the 27 cells whose
+// stencil covers the node, cells in z-y-x order and particles in their binned
+// order, which the deterministic re-bin fixes.  No atomics, so the grid is the
+// same bit for bit on every run and launch shape.  Every node is written (zero
+// where no particle reaches it).
+template <typename R>
+__global__ void k_p2g_det(const Inst<R>* __restrict__ insts, int n_inst, PState<R> ps, const R* __restrict__ pay,
+                          int64_t stride, const int32_t* __restrict__ key_base, const int32_t* __restrict__ offset,
+                          int rbuf, int64_t nn_total) {
+    const int64_t gn = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gn >= nn_total) return;
+    int lo = 0, hi = n_inst - 1;   // the instance whose grid holds node gn
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (insts[mid].gbase <= gn) lo = mid; else hi = mid - 1;
+    }
+    const Inst<R>& P = insts[lo];
+    const int64_t ln = gn - P.gbase;
+    if (ln < 0 || ln >= P.nn) return;
+    const int gx = (int)(ln % P.nx), gy = (int)((ln / P.nx) % P.ny), gz = (int)(ln / ((int64_t)P.nx * P.ny));
+    const R pm = P.pmass;
+    R m = R(0), p[3] = {R(0), R(0), R(0)};
+    for (int cz = max(gz - 2, 0); cz <= gz; ++cz)
+        for (int cy = max(gy - 2, 0); cy <= gy; ++cy)
+            for (int cx = max(gx - 2, 0); cx <= gx; ++cx) {
+                const int bx = cx / kBin, by = cy / kBin, bz = cz / kBin;
+                if (bx >= P.nbx || by >= P.nby || bz >= P.nbz) continue;
+                const int bin = bx + P.nbx * (by + P.nby * bz);
+                const int cell = (cx - bx * kBin) + kBin * ((cy - by * kBin) + kBin * (cz - bz * kBin));
+                const int key = key_base[lo] + bin * kCellsPerBin + cell;
+                const int64_t s1 = offset[key + 1];
+                for (int64_t s = offset[key]; s < s1; ++s) {
+                    if (ps.status[s] == ST_INACTIVE) continue;   // killed in the P2G launch
+                    R w[3][3], dw[3][3];
+                    const int i = gx - (bx * kBin + bspline(pay[s], w[0], dw[0]));
+                    const int j = gy - (by * kBin + bspline(pay[stride + s], w[1], dw[1]));
+                    const int k = gz - (bz * kBin + bspline(pay[2 * stride + s], w[2], dw[2]));
+                    if ((unsigned)i > 2u || (unsigned)j > 2u || (unsigned)k > 2u) continue;
+                    const R wijk = w[0][i] * w[1][j] * w[2][k];
+                    const R gxw = dw[0][i] * w[1][j] * w[2][k], gyw = w[0][i] * dw[1][j] * w[2][k],
+                            gzw = w[0][i] * w[1][j] * dw[2][k];
+                    m += pm * wijk;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const R q = pay[(3 + a) * stride + s] + pay[(6 + 3 * a) * stride + s] * R(i) +
+                                    pay[(7 + 3 * a) * stride + s] * R(j) + pay[(8 + 3 * a) * stride + s] * R(k);
+                        p[a] += wijk * q + pay[(15 + 3 * a) * stride + s] * gxw +
+                                pay[(16 + 3 * a) * stride + s] * gyw + pay[(17 + 3 * a) * stride + s] * gzw;
+                    }
+                }
+            }
+    P.grid[rbuf][ln] = mk4<R>(m, p[0], p[1], p[2]);
+}
+
+template <typename R>
+void launch_p2g_det(const Inst<R>* insts, int n_inst, const PState<R>& ps, const R* pay, int64_t stride,
+                    const int32_t* key_base, const int32_t* offset, int rbuf, int64_t nn_total, cudaStream_t st) {
+    if (nn_total <= 0 || n_inst <= 0) return;
+    Range nvtx_range("mpm.p2g_det");
+    k_p2g_det<R><<<(int)((nn_total + 127) / 128), 128, 0, st>>>(insts, n_inst, ps, pay, stride, key_base, offset,
+                                                                rbuf, nn_total);
+    ++launch_counter();
 }
 
 template <typename R>
@@ -1501,7 +1581,10 @@ void launch_step(const Inst<R>* insts, const Work* work, const int* n_work, int 
     int grid = sms * (ctas_per_sm > 0 ? ctas_per_sm : 4);
     if (grid > max_work) grid = max_work;
     const size_t smem = a.ext ? step_smem_bytes<R, true>() : step_smem_bytes<R, false>();
-    if (g2p && p2g && a.ext) {
+    if (a.det && !g2p && p2g && !a.ext) {
+        set_smem_attr<R, false, true, false, true>();
+        k_step<R, false, true, false, true><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+    } else if (g2p && p2g && a.ext) {
         set_smem_attr<R, true, true, true>();
         k_step<R, true, true, true><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
     } else if (g2p && p2g) {
@@ -1523,6 +1606,10 @@ void launch_step(const Inst<R>* insts, const Work* work, const int* n_work, int 
     ++launch_counter();
 }
 
+template void launch_p2g_det<float>(const Inst<float>*, int, const PState<float>&, const float*, int64_t,
+                                    const int32_t*, const int32_t*, int, int64_t, cudaStream_t);
+template void launch_p2g_det<double>(const Inst<double>*, int, const PState<double>&, const double*, int64_t,
+                                     const int32_t*, const int32_t*, int, int64_t, cudaStream_t);
 template void launch_step<float>(const Inst<float>*, const Work*, const int*, int, const PState<float>&,
                                  const StepArgs&, int, bool, bool, int, int, int*, unsigned long long*, cudaStream_t);
 template void launch_step<double>(const Inst<double>*, const Work*, const int*, int, const PState<double>&,

@@ -178,6 +178,18 @@ class Solver:
             np.ascontiguousarray(ckpt, dtype=np.uint8)
         self._check(self._lib.mpm_checkpoint_load(self.h, int(inst), buf.ctypes.data, buf.nbytes))
 
+    def launch_config(self) -> dict:
+        c = A.MpmLaunchConfig()
+        self._check(self._lib.mpm_get_launch_config(self.h, C.byref(c)))
+        return c.as_dict()
+
+    def set_launch_config(self, ctas_per_sm: int = 4, sort_every: int = 16, use_graph: bool = False,
+                          deterministic: bool = False) -> None:
+        """Launch shape; deterministic=True gives the same results bit for bit
+        on every run and launch shape (mpm_launch_config.deterministic)."""
+        c = A.MpmLaunchConfig(int(ctas_per_sm), int(sort_every), 1 if use_graph else 0, 1 if deterministic else 0)
+        self._check(self._lib.mpm_set_launch_config(self.h, C.byref(c)))
+
     def _check_state(self, status: int, strict: bool) -> None:
         if strict or status != A.MPM_NUMERIC:
             self._check(status)
@@ -356,14 +368,6 @@ class Batch(Solver):
         self.params = [p for k, p in enumerate(self.params) if k not in set(remove)] + list(add_params)
         return first.value
 
-    def launch_config(self) -> dict:
-        c = A.MpmLaunchConfig()
-        self._check(self._lib.mpm_get_launch_config(self.h, C.byref(c)))
-        return c.as_dict()
-
-    def set_launch_config(self, ctas_per_sm: int = 4, sort_every: int = 16, use_graph: bool = False) -> None:
-        c = A.MpmLaunchConfig(int(ctas_per_sm), int(sort_every), 1 if use_graph else 0, 0)
-        self._check(self._lib.mpm_set_launch_config(self.h, C.byref(c)))
 
     def autotune(self, dts) -> dict:
         d = np.ascontiguousarray(dts, dtype=np.float64)

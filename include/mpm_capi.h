@@ -387,7 +387,17 @@ typedef struct mpm_launch_config {
     int32_t ctas_per_sm;   /* persistent CTAs per SM of the step kernel, 1..8 (default 4) */
     int32_t sort_every;    /* re-bin every n steps, 1..1024 (default mpm_params.sort_every) */
     int32_t use_graph;     /* replay each step call's launches from a captured CUDA graph */
-    int32_t _pad;
+    /* 1: deterministic mode (no counterpart in the reference, whose P2G sums
+     * with FP64 atomics in arrival order).  The results are the same bit for
+     * bit on every run and every launch shape: the particles are re-binned
+     * before every P2G with ranks from a stable sort, each particle's scatter
+     * payload goes to device memory, and one thread per grid node sums the
+     * payloads of its 27 cells in a fixed order, without atomics.  Runs the
+     * split schedule, re-bins every step, ignores use_graph and sort_every,
+     * and holds 24 reals per particle slot more; several times slower than the
+     * default.  Not available with the adiabatic shear model, heat conduction
+     * or a voxel tool SDF (MPM_NOT_SUPPORTED at the step). */
+    int32_t deterministic;
 } mpm_launch_config;
 mpm_status mpm_get_launch_config(const mpm_handle *h, mpm_launch_config *out);
 mpm_status mpm_set_launch_config(mpm_handle *h, const mpm_launch_config *cfg);

@@ -1,0 +1,127 @@
+"""Deterministic mode (mpm_launch_config.deterministic): the same workpiece
+gives the same state bit for bit on every run, at every launch shape, and
+alone or inside a batch; and it still matches the oracle.
+
+Tolerances against the oracle (as tests/test_gpu_parity.py):
+  FP64: 1e-9 of each field's scale, status identical
+  FP32: positions 2e-4 cell, velocities 1e-3, other fields 2e-3; status equal
+        for >= 99.9 % of the particles
+Between deterministic runs: exact equality of every downloaded field.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+from scenarios import SCENARIOS  # noqa: E402
+from mpm_b200 import Batch, Solver, capi as A, workpiece as W  # noqa: E402
+from test_gpu_batch import assert_same, cap_of, init_i, small_cases  # noqa: E402
+from test_gpu_parity import field_errors  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+STATE = ("x", "y", "z", "vx", "vy", "vz", "F", "Fp", "C", "stress", "plastic_strain", "strain_rate",
+         "temperature", "damage", "residual_stress", "status", "id")
+
+
+def run_det(case, st, n, prec, ctas=4, splits=None):
+    s = Solver(W.to_mpm_params(case, precision=prec), len(st["x"]) + 64)
+    try:
+        s.set_launch_config(ctas_per_sm=ctas, deterministic=True)
+        assert s.launch_config()["deterministic"] == 1
+        s.set_tool(case["tool"])
+        s.upload(st)
+        if "ext" in case:
+            e = case["ext"]
+            s.apply_external_force(e["center"], e["radius"], e["force"])
+        for k in (splits or [n]):
+            s.step(case["dt"], k)
+        out = s.download()
+        out["metrics"] = s.metrics()
+    finally:
+        s.close()
+    return out
+
+
+def identical(a, b):
+    for k in STATE:
+        assert np.array_equal(a[k], b[k], equal_nan=True), k
+
+
+@pytest.mark.parametrize("name", ["plastic_damage_chip", "boundary_mix"])
+def test_runs_are_identical_bit_for_bit(name):
+    """FP32, where the default mode's atomic sums differ from run to run: two
+    runs, a third with another CTA count and a fourth split into two step
+    calls give the same bits."""
+    case, st, n, _ = SCENARIOS[name]()
+    a = run_det(case, st, n, A.PREC_F32)
+    b = run_det(case, st, n, A.PREC_F32)
+    c = run_det(case, st, n, A.PREC_F32, ctas=2)
+    d = run_det(case, st, n, A.PREC_F32, splits=[n // 2, n - n // 2])
+    for o in (b, c, d):
+        identical(a, o)
+    assert a["metrics"]["n_escaped"] == 0
+
+
+@pytest.mark.parametrize("name", ["elastic_raster", "plastic_damage_chip", "boundary_mix", "lod_kinematic_extf"])
+def test_matches_the_oracle_fp64(oracle, name):
+    case, st, n, extf = SCENARIOS[name]()
+    ref, rc = oracle.step(case, st, n, extf=extf)
+    assert rc == 0
+    out = run_det(case, st, n, A.PREC_F64)
+    assert (out["status"] == ref["status"]).all()
+    err = field_errors(out, ref, case)
+    assert max(err.values()) < 1e-9, err
+
+
+def test_matches_the_oracle_fp32(oracle):
+    case, st, n, extf = SCENARIOS["plastic_damage_chip"]()
+    ref, rc = oracle.step(case, st, n, extf=extf)
+    assert rc == 0
+    assert_same(run_det(case, st, n, A.PREC_F32), ref, case, A.PREC_F32)
+
+
+def test_batched_instance_is_identical_to_its_run_alone():
+    """The sums of an instance's nodes run over its own particles in its own
+    slot order, so a workpiece in a batch gives the bits it gives alone."""
+    prec = A.PREC_F32
+    cases = small_cases(3, seed=21, precision=prec)
+    n = 8
+    bt = Batch([W.to_mpm_params(c, precision=prec) for c in cases], [cap_of(c) for c in cases])
+    try:
+        bt.set_launch_config(deterministic=True)
+        for i, c in enumerate(cases):
+            init_i(bt, i, c)
+        bt.step_all([c["dt"] for c in cases], n)
+        outs = [bt.download_i(i) for i in range(3)]
+    finally:
+        bt.close()
+    for i, c in enumerate(cases):
+        s = Solver(W.to_mpm_params(c, precision=prec), cap_of(c))
+        try:
+            s.set_launch_config(deterministic=True)
+            b = c["box"]
+            s.init_box(b["c0"], b["c1"], b["ppc"], b["seed"], b["instance"], b["fixed_layers"], b["T0"],
+                       tool=c["tool"])
+            s.step(c["dt"], n)
+            identical(outs[i], s.download())
+        finally:
+            s.close()
+
+
+def test_extensions_are_refused():
+    case, st, n, _ = SCENARIOS["adiabatic_shear"]()
+    s = Solver(W.to_mpm_params(case, precision=A.PREC_F32), len(st["x"]) + 64)
+    try:
+        s.set_launch_config(deterministic=True)
+        s.set_tool(case["tool"])
+        s.upload(st)
+        with pytest.raises(A.MpmError) as e:
+            s.step(case["dt"], 1)
+        assert e.value.status == A.MPM_NOT_SUPPORTED
+    finally:
+        s.close()
