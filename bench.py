@@ -228,6 +228,8 @@ def run_ours(args):
         p.heat_conduction = 1
     cap = int(np.prod([box["c1"][i] - box["c0"][i] for i in range(3)]) * box["ppc"])
     s = Solver(p, cap, stream=stream.cuda_stream)
+    if args.deterministic:
+        s.set_launch_config(deterministic=True)
     n = s.init_box(box["c0"], box["c1"], box["ppc"], box["seed"] + rank, box["instance"], box["fixed_layers"],
                    T0, tool=case["tool"])
     m0 = s.metrics()
@@ -298,7 +300,9 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": desc, "particles_per_gpu": int(n_live), "cells": list(case["cells"]),
                        "dx_m": case["params"]["dx"], "dt_s": dt, "ppc": box["ppc"],
-                       "schedule": "fused G2P->P2G, one kernel per step", "parallelism": f"replicas{world}",
+                       "schedule": ("deterministic: split schedule, re-bin and atomic-free node gather every step"
+                                    if args.deterministic else "fused G2P->P2G, one kernel per step"),
+                       "parallelism": f"replicas{world}",
                        "l2": "working set >> L2 (no flush needed)", "yield_fraction": f_yield,
                        "escaped_updates": int(m1["n_escaped"]), "rebins": int(m1["n_sorts"]),
                        "contact_every": int(args.contact_every), "contacts": int(m1["n_contacts"]),
@@ -516,6 +520,8 @@ def run_precision_study(args):
 
     def run(prec):
         s = Solver(W.to_mpm_params(case, precision=prec), cap)
+        if args.deterministic:
+            s.set_launch_config(deterministic=True)
         n = _init(s, case, rank=rank)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -584,7 +590,7 @@ def run_precision_study(args):
             "config": {"workload": "precision study: 128x64x64 cells, dx 0.02 mm, 8 ppc, Ti-6Al-4V, rounded wedge "
                                    "r_e 0.3 mm at 2.5 m/s, doc 0.05 mm; the Johnson-Cook Newton solve and the "
                                    "conservation reductions are FP64 in both runs",
-                       "particles": int(n), "fp32_runs": len(runs),
+                       "particles": int(n), "fp32_runs": len(runs), "deterministic": bool(args.deterministic),
                        "target": "momentum and kinetic+internal energy within 1e-4"},
             "errors_median": med, "errors_worst": worst, "runs_within_1e-4": within,
             "particle_errors_median": part, "particle_error_scales": scales, "runs": runs,
@@ -734,6 +740,8 @@ def main():
     ap.add_argument("--chunk", type=int, default=50, help="serving: steps per tick at most")
     ap.add_argument("--resident-particles", type=float, default=0,
                     help="serving: admission cap on resident particles (0: the HBM budget alone)")
+    ap.add_argument("--deterministic", action="store_true",
+                    help="plain configs and precision_study: deterministic mode (bit-identical runs)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()

@@ -289,6 +289,37 @@ __global__ void k_bin_scatter(PState<R> src, PState<R> dst, const Inst<R>* insts
             a0.z += (R)((obv[2] - nbv[2]) * kBin);
         }
     }
+    if (det && kk - key_base[ii] < P.nbins * kCellsPerBin) {
+        // deterministic mode: the stencil base of the stored position must be the
+        // key's cell, which the rounding of a re-expressed position can miss by
+        // one; such a coordinate is set onto the cell's edge (FP32: the low part
+        // takes the difference, so hi + lo stays the same).  Only rounding-sized
+        // misses are moved: a particle outside the bins (base below 0 at the
+        // domain edge) keeps its position, and the kill zone deactivates it.
+        const int cl = kk - key_base[ii] - nbn * kCellsPerBin;
+        const int c3[3] = {cl % kBin, (cl / kBin) % kBin, cl / (kBin * kBin)};
+        R v[3] = {a0.x, a0.y, a0.z}, sh[3] = {R(0), R(0), R(0)};
+        bool moved = false;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const R f = floor(v[c] - R(0.5));
+            R nv = v[c];
+            if (f < R(c3[c])) nv = R(c3[c]) + R(0.5);
+            else if (f > R(c3[c])) nv = nextafter(R(c3[c]) + R(1.5), R(0));
+            if (fabs(nv - v[c]) > R(1e-3)) nv = v[c];
+            sh[c] = v[c] - nv;
+            moved = moved || nv != v[c];
+            v[c] = nv;
+        }
+        if (moved) {
+            a0.x = v[0]; a0.y = v[1]; a0.z = v[2];
+            if (dst.X) {
+                V4<R> lo = dst.X[d];
+                lo.x += sh[0]; lo.y += sh[1]; lo.z += sh[2];
+                dst.X[d] = lo;
+            }
+        }
+    }
     dst.A[0][d] = a0;
 #pragma unroll
     for (int q = 1; q < 6; ++q) dst.A[q][d] = src.A[q][pi];

@@ -159,9 +159,10 @@ struct StepArgs {
     int p2g_step;       // step index of the P2G part
     int ext;            // some instance runs the adiabatic shear model or heat conduction: launches
                         // take the kernel variant that has them (the others carry none of their code)
-    int det;            // deterministic mode: the P2G-only launch writes each particle's scatter
-                        // payload to det_pay (24 rows of det_stride reals) for k_p2g_det to sum
-    void* det_pay;
+    int det;            // deterministic mode: the P2G-only launch writes each particle's 27 node
+                        // contributions (m, p) to det_contrib (27 rows of det_stride V4s) for
+                        // k_p2g_det to sum
+    void* det_contrib;
     int64_t det_stride;
 };
 

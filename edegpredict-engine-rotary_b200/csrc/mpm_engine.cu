@@ -134,11 +134,11 @@ class Engine final : public EngineBase {
     int sort_every = 16, threads = 128, ctas_per_sm = 4, prec_ = MPM_PREC_F32;
     bool use_graph = false;
     int rbuf = 0;
-    // deterministic mode (mpm_launch_config.deterministic): the scatter payload
-    // (24 rows of cap_total reals) and the stable-sort scratch of the re-bin
+    // deterministic mode (mpm_launch_config.deterministic): the particles' node
+    // contributions and the stable-sort scratch of the re-bin
     bool det = false;
-    R* d_det_pay = nullptr;
-    int64_t det_pay_alloc = 0;
+    V4<R>* d_det_contrib = nullptr;   // 27 rows of cap_total node contributions
+    int64_t det_contrib_alloc = 0;
     int32_t* d_det_i32[4] = {nullptr, nullptr, nullptr, nullptr};
     int64_t det_i32_alloc[4] = {0, 0, 0, 0};
     unsigned char* d_det_tmp = nullptr;
@@ -190,7 +190,7 @@ class Engine final : public EngineBase {
                         d_bin_local,
                         d_inst_pbase, d_key, d_rank, d_newbin, d_count, d_offset, d_flag, d_flag_scan, d_scan_tmp,
                         d_pos, d_work, d_nwork, d_err, d_ierr, d_ctr, d_stat_part, d_stat_out, d_stage, d_gen,
-                        d_map, d_det_pay, d_det_i32[0], d_det_i32[1], d_det_i32[2], d_det_i32[3], d_det_tmp};
+                        d_map, d_det_contrib, d_det_i32[0], d_det_i32[1], d_det_i32[2], d_det_i32[3], d_det_tmp};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         for (auto& x : I)
@@ -713,15 +713,15 @@ class Engine final : public EngineBase {
 
     // ---------------------------------------------------------------- binning
 
-    // Deterministic mode: scratch for the payload and the stable sort (grown
+    // Deterministic mode: scratch for the node contributions and the stable sort (grown
     // outside any graph capture: the mode runs without graphs).
     mpm_status det_scratch() {
         const int64_t tmp = (int64_t)det_rank_tmp_bytes(cap_total, nkeys);
-        bool more = det_pay_alloc < 24 * std::max<int64_t>(cap_total, 1) || det_tmp_alloc < std::max<int64_t>(tmp, 1);
+        bool more = det_contrib_alloc < 27 * std::max<int64_t>(cap_total, 1) || det_tmp_alloc < std::max<int64_t>(tmp, 1);
         for (int k = 0; k < 4; ++k) more = more || det_i32_alloc[k] < std::max<int64_t>(cap_total, 1);
         if (!more) return MPM_OK;
         CK(cudaStreamSynchronize(st));   // nothing in flight uses the old buffers
-        MS(grow(d_det_pay, det_pay_alloc, 24 * std::max<int64_t>(cap_total, 1), false));
+        MS(grow(d_det_contrib, det_contrib_alloc, 27 * std::max<int64_t>(cap_total, 1), false));
         for (int k = 0; k < 4; ++k) MS(grow(d_det_i32[k], det_i32_alloc[k], cap_total));
         MS(grow(d_det_tmp, det_tmp_alloc, tmp));
         return MPM_OK;
@@ -1169,14 +1169,14 @@ class Engine final : public EngineBase {
                 if ((s = clear(w)) != MPM_OK) return s;
                 StepArgs a{k, 0, 1, (ext && k == 0) ? 1 : 0, k, xk};
                 a.det = det ? 1 : 0;
-                a.det_pay = d_det_pay;
+                a.det_contrib = d_det_contrib;
                 a.det_stride = cap_total;
                 prof_begin();
                 launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], a, w, false, true, threads, cps, d_err,
                                d_ctr, st);
                 prof_end();
                 if (det)
-                    launch_p2g_det<R>(d_inst, (int)I.size(), ps[cur], d_det_pay, cap_total, d_key_base, d_offset, w,
+                    launch_p2g_det<R>(d_inst, (int)I.size(), d_det_contrib, cap_total, d_key_base, d_offset, w,
                                       nn_total, st);
                 raster_all(k);
                 diffuse(w);

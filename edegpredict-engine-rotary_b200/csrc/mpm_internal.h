@@ -70,11 +70,11 @@ void launch_step(const Inst<R>* insts, const Work* work, const int* n_work, int 
                  const StepArgs& a, int rbuf, bool g2p, bool p2g, int threads, int ctas_per_sm, int* err,
                  unsigned long long* counters, cudaStream_t st);
 
-// Deterministic mode: the grid of every instance from the payloads of a
-// P2G-only launch (k_p2g_det), into grid buffer rbuf.
+// Deterministic mode: the grid of every instance from the node contributions
+// of a P2G-only launch (27 rows of `stride` V4<R>), into grid buffer rbuf.
 template <typename R>
-void launch_p2g_det(const Inst<R>* insts, int n_inst, const PState<R>& ps, const R* pay, int64_t stride,
-                    const int32_t* key_base, const int32_t* offset, int rbuf, int64_t nn_total, cudaStream_t st);
+void launch_p2g_det(const Inst<R>* insts, int n_inst, const void* contrib, int64_t stride, const int32_t* key_base,
+                    const int32_t* offset, int rbuf, int64_t nn_total, cudaStream_t st);
 
 // Deterministic mode, the re-bin: replaces the arrival-order ranks of
 // launch_bin_count by ranks in slot order within each key (a stable radix

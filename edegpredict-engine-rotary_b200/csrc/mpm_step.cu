@@ -949,6 +949,35 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT>& Sm, int cell, 
     }
 }
 
+// Deterministic mode: the 27 node contributions of one particle to det_contrib
+// (row o = i + 3j + 9k of the stencil, relative to the particle's base node):
+// (m w_ijk, w_ijk (Q + R (i,j,k)) + S grad w_ijk).  Q = NULL writes zeros (a
+// particle that contributes nothing).
+template <typename R>
+__device__ __noinline__ void det_contrib(const StepArgs& sa, int64_t pi, R m, const R* xi, const R* Q, const R* Rm,
+                                         const R* S) {
+    V4<R>* c = static_cast<V4<R>*>(sa.det_contrib) + pi;
+    const int64_t ds = sa.det_stride;
+    if (!Q) {
+        for (int o = 0; o < 27; ++o) c[o * ds] = mk4<R>(R(0), R(0), R(0), R(0));
+        return;
+    }
+    R w[3][3], dw[3][3];
+    for (int a = 0; a < 3; ++a) (void)bspline(xi[a], w[a], dw[a]);
+    for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) {
+                const R wijk = w[0][i] * w[1][j] * w[2][k];
+                const R gx = dw[0][i] * w[1][j] * w[2][k], gy = w[0][i] * dw[1][j] * w[2][k],
+                        gz = w[0][i] * w[1][j] * dw[2][k];
+                R p[3];
+                for (int a = 0; a < 3; ++a)
+                    p[a] = wijk * (Q[a] + Rm[3 * a] * R(i) + Rm[3 * a + 1] * R(j) + Rm[3 * a + 2] * R(k)) +
+                           S[3 * a] * gx + S[3 * a + 1] * gy + S[3 * a + 2] * gz;
+                c[(i + 3 * j + 9 * k) * ds] = mk4<R>(m * wijk, p[0], p[1], p[2]);
+            }
+}
+
 template <typename R, bool G2P, bool P2G, bool EXT, bool DET = false>
 __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __restrict__ insts, const Work* __restrict__ work,
                                               const int* __restrict__ n_work, PState<R> ps, StepArgs sa, int rbuf,
@@ -1255,6 +1284,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                         if (!(f0 >= R(1 - g0x) && f0 < R(P.nx - 2 - g0x) && f1 >= R(1 - g0y) &&
                               f1 < R(P.ny - 2 - g0y) && f2 >= R(1 - g0z) && f2 < R(P.nz - 2 - g0z))) {
                             if (!isfinite(f0 + f1 + f2)) reinterpret_cast<unsigned char*>(P.ierr)[0] = 1;
+                            if (DET) det_contrib<R>(sa, pi, R(0), xi, nullptr, nullptr, nullptr);
                             st = ST_INACTIVE;
                             if (G2P) {
                                 // no later G2P writes this particle: store this step's v, strain rate and C
@@ -1366,15 +1396,13 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                 S[5] = sf * sig[5]; S[7] = sf * sl[2];
                             }
                             if (DET) {
-                                // deterministic mode: the payload goes to global memory and
-                                // k_p2g_det sums it per node in a fixed order (no atomics)
-                                R* dp = static_cast<R*>(sa.det_pay) + pi;
-                                const int64_t ds = sa.det_stride;
-#pragma unroll
-                                for (int a = 0; a < 3; ++a) { dp[a * ds] = xi[a]; dp[(3 + a) * ds] = Q[a]; }
-#pragma unroll
-                                for (int q = 0; q < 9; ++q) { dp[(6 + q) * ds] = Rm[q]; dp[(15 + q) * ds] = S[q]; }
-                                // binned just before this launch, so the base lies in the bin
+                                // deterministic mode: the particle's 27 node contributions
+                                // (m, p) go to global memory, and k_p2g_det sums each node's
+                                // in a fixed order (no atomics).  w_ijk (Q + R (i,j,k)) +
+                                // S grad(w_ijk), the sum that cell_accumulate forms per cell.
+                                det_contrib<R>(sa, pi, m, xi, Q, Rm, S);
+                                // binned just before this launch (the re-bin puts every
+                                // base in its bin), so this counts nothing
                                 if (!(bb[0] >= 0 && bb[0] < kBin && bb[1] >= 0 && bb[1] < kBin && bb[2] >= 0 &&
                                       bb[2] < kBin))
                                     ++c_esc;
@@ -1499,14 +1527,15 @@ template <typename R, bool G2P, bool P2G, bool EXT, bool DET = false> static voi
     }
 }
 
-// Deterministic mode, the P2G sums: one thread per grid node adds the payloads
-// (written by the P2G-only step launch) of the particles in the 27 cells whose
-// stencil covers the node, cells in z-y-x order and particles in their binned
-// order, which the deterministic re-bin fixes.  No atomics, so the grid is the
-// same bit for bit on every run and launch shape.  Every node is written (zero
-// where no particle reaches it).
+// Deterministic mode, the P2G sums: one thread per grid node adds the
+// contributions (written by the P2G-only step launch) of the particles in the
+// 27 cells whose stencil covers the node, cells in z-y-x order and particles
+// in their binned order, which the deterministic re-bin fixes.  Particles
+// killed in that launch contribute zeros.  No atomics, so the grid is the same
+// bit for bit on every run and launch shape.  Every node is written (zero where
+// no particle reaches it).
 template <typename R>
-__global__ void k_p2g_det(const Inst<R>* __restrict__ insts, int n_inst, PState<R> ps, const R* __restrict__ pay,
+__global__ void k_p2g_det(const Inst<R>* __restrict__ insts, int n_inst, const void* __restrict__ contrib,
                           int64_t stride, const int32_t* __restrict__ key_base, const int32_t* __restrict__ offset,
                           int rbuf, int64_t nn_total) {
     const int64_t gn = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1520,7 +1549,7 @@ __global__ void k_p2g_det(const Inst<R>* __restrict__ insts, int n_inst, PState<
     const int64_t ln = gn - P.gbase;
     if (ln < 0 || ln >= P.nn) return;
     const int gx = (int)(ln % P.nx), gy = (int)((ln / P.nx) % P.ny), gz = (int)(ln / ((int64_t)P.nx * P.ny));
-    const R pm = P.pmass;
+    const V4<R>* __restrict__ c = static_cast<const V4<R>*>(contrib);
     R m = R(0), p[3] = {R(0), R(0), R(0)};
     for (int cz = max(gz - 2, 0); cz <= gz; ++cz)
         for (int cy = max(gy - 2, 0); cy <= gy; ++cy)
@@ -1530,36 +1559,23 @@ __global__ void k_p2g_det(const Inst<R>* __restrict__ insts, int n_inst, PState<
                 const int bin = bx + P.nbx * (by + P.nby * bz);
                 const int cell = (cx - bx * kBin) + kBin * ((cy - by * kBin) + kBin * (cz - bz * kBin));
                 const int key = key_base[lo] + bin * kCellsPerBin + cell;
+                // every particle of the cell has its base at the cell (deterministic re-bin)
+                const V4<R>* __restrict__ row = c + (int64_t)((gx - cx) + 3 * (gy - cy) + 9 * (gz - cz)) * stride;
                 const int64_t s1 = offset[key + 1];
                 for (int64_t s = offset[key]; s < s1; ++s) {
-                    if (ps.status[s] == ST_INACTIVE) continue;   // killed in the P2G launch
-                    R w[3][3], dw[3][3];
-                    const int i = gx - (bx * kBin + bspline(pay[s], w[0], dw[0]));
-                    const int j = gy - (by * kBin + bspline(pay[stride + s], w[1], dw[1]));
-                    const int k = gz - (bz * kBin + bspline(pay[2 * stride + s], w[2], dw[2]));
-                    if ((unsigned)i > 2u || (unsigned)j > 2u || (unsigned)k > 2u) continue;
-                    const R wijk = w[0][i] * w[1][j] * w[2][k];
-                    const R gxw = dw[0][i] * w[1][j] * w[2][k], gyw = w[0][i] * dw[1][j] * w[2][k],
-                            gzw = w[0][i] * w[1][j] * dw[2][k];
-                    m += pm * wijk;
-#pragma unroll
-                    for (int a = 0; a < 3; ++a) {
-                        const R q = pay[(3 + a) * stride + s] + pay[(6 + 3 * a) * stride + s] * R(i) +
-                                    pay[(7 + 3 * a) * stride + s] * R(j) + pay[(8 + 3 * a) * stride + s] * R(k);
-                        p[a] += wijk * q + pay[(15 + 3 * a) * stride + s] * gxw +
-                                pay[(16 + 3 * a) * stride + s] * gyw + pay[(17 + 3 * a) * stride + s] * gzw;
-                    }
+                    const V4<R> v = row[s];
+                    m += v.x; p[0] += v.y; p[1] += v.z; p[2] += v.w;
                 }
             }
     P.grid[rbuf][ln] = mk4<R>(m, p[0], p[1], p[2]);
 }
 
 template <typename R>
-void launch_p2g_det(const Inst<R>* insts, int n_inst, const PState<R>& ps, const R* pay, int64_t stride,
-                    const int32_t* key_base, const int32_t* offset, int rbuf, int64_t nn_total, cudaStream_t st) {
+void launch_p2g_det(const Inst<R>* insts, int n_inst, const void* contrib, int64_t stride, const int32_t* key_base,
+                    const int32_t* offset, int rbuf, int64_t nn_total, cudaStream_t st) {
     if (nn_total <= 0 || n_inst <= 0) return;
     Range nvtx_range("mpm.p2g_det");
-    k_p2g_det<R><<<(int)((nn_total + 127) / 128), 128, 0, st>>>(insts, n_inst, ps, pay, stride, key_base, offset,
+    k_p2g_det<R><<<(int)((nn_total + 127) / 128), 128, 0, st>>>(insts, n_inst, contrib, stride, key_base, offset,
                                                                 rbuf, nn_total);
     ++launch_counter();
 }
@@ -1606,10 +1622,10 @@ void launch_step(const Inst<R>* insts, const Work* work, const int* n_work, int 
     ++launch_counter();
 }
 
-template void launch_p2g_det<float>(const Inst<float>*, int, const PState<float>&, const float*, int64_t,
-                                    const int32_t*, const int32_t*, int, int64_t, cudaStream_t);
-template void launch_p2g_det<double>(const Inst<double>*, int, const PState<double>&, const double*, int64_t,
-                                     const int32_t*, const int32_t*, int, int64_t, cudaStream_t);
+template void launch_p2g_det<float>(const Inst<float>*, int, const void*, int64_t, const int32_t*, const int32_t*,
+                                    int, int64_t, cudaStream_t);
+template void launch_p2g_det<double>(const Inst<double>*, int, const void*, int64_t, const int32_t*, const int32_t*,
+                                     int, int64_t, cudaStream_t);
 template void launch_step<float>(const Inst<float>*, const Work*, const int*, int, const PState<float>&,
                                  const StepArgs&, int, bool, bool, int, int, int*, unsigned long long*, cudaStream_t);
 template void launch_step<double>(const Inst<double>*, const Work*, const int*, int, const PState<double>&,

@@ -390,12 +390,14 @@ typedef struct mpm_launch_config {
     /* 1: deterministic mode (no counterpart in the reference, whose P2G sums
      * with FP64 atomics in arrival order).  The results are the same bit for
      * bit on every run and every launch shape: the particles are re-binned
-     * before every P2G with ranks from a stable sort, each particle's scatter
-     * payload goes to device memory, and one thread per grid node sums the
-     * payloads of its 27 cells in a fixed order, without atomics.  Runs the
-     * split schedule, re-bins every step, ignores use_graph and sort_every,
-     * and holds 24 reals per particle slot more; several times slower than the
-     * default.  Not available with the adiabatic shear model, heat conduction
+     * before every P2G with ranks from a stable sort, each particle writes its
+     * 27 node contributions (m, p) to device memory, and one thread per grid
+     * node sums those of its 27 cells in a fixed order, without atomics.  A
+     * position that rounding at the re-bin would put one cell off its key is
+     * set onto the key cell's edge (FP32: the low part takes the difference).
+     * Runs the split schedule, re-bins every step, ignores use_graph and
+     * sort_every, and holds 27 x 4 reals per particle slot more; several times
+     * slower than the default.  Not available with the adiabatic shear model, heat conduction
      * or a voxel tool SDF (MPM_NOT_SUPPORTED at the step). */
     int32_t deterministic;
 } mpm_launch_config;
