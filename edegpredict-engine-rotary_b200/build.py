@@ -1,11 +1,13 @@
 """Build recipe of libmpm_b200.so (sm_100a) -- in-tree, no JIT cache.
 
-    python edegpredict-engine-rotary_b200/build.py [--force]
+    python edegpredict-engine-rotary_b200/build.py [--force] [--checked]
 
 Compiles every .cu under csrc/ with nvcc for sm_100a and links one shared
 library next to the Python package (mpm_b200/libmpm_b200.so).  Objects go to
 _build/ (git-ignored).  Incremental: a source newer than its object, or any
-header newer than the library, triggers a rebuild.
+header newer than the library, triggers a rebuild.  --checked builds the
+bounds-checked variant (-DMPMB_CHECKED, mpm_b200/libmpm_b200_checked.so,
+objects in _build_checked/) instead.
 """
 from __future__ import annotations
 
@@ -20,6 +22,7 @@ CSRC = HERE / "csrc"
 INCLUDE = HERE.parent / "include"
 BUILD = HERE / "_build"
 LIB = HERE / "mpm_b200" / "libmpm_b200.so"
+LIB_CHECKED = HERE / "mpm_b200" / "libmpm_b200_checked.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3"]
@@ -36,28 +39,30 @@ def _newest(paths) -> float:
     return max((p.stat().st_mtime for p in paths), default=0.0)
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
+def build(force: bool = False, verbose: bool = False, checked: bool = False) -> Path:
+    out_dir = HERE / "_build_checked" if checked else BUILD
+    lib = LIB_CHECKED if checked else LIB
+    extra = ["-DMPMB_CHECKED"] if checked else []
+    out_dir.mkdir(exist_ok=True)
     sources = sorted(CSRC.glob("*.cu"))
     headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h"))
     hdr_time = _newest(headers)
     objs = []
     for src in sources:
-        obj = BUILD / (src.stem + ".o")
+        obj = out_dir / (src.stem + ".o")
         objs.append(obj)
         if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, hdr_time):
-            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)
-    if force or not LIB.exists() or LIB.stat().st_mtime < _newest(objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart"]
+    if force or not lib.exists() or lib.stat().st_mtime < _newest(objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-lcudart"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True)
-    print(LIB)
+    print(build(force="--force" in sys.argv, verbose=True, checked="--checked" in sys.argv))

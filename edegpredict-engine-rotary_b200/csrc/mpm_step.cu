@@ -26,6 +26,32 @@
 
 namespace mpmb {
 
+// Bounds-checked builds (-DMPMB_CHECKED, libmpm_b200_checked.so): every index
+// the step kernels derive from data is checked before it is used; a failed
+// check counts, records the first site and index (mpm_check_report) and skips
+// the access, so no check traps.  Default builds compile every check away.
+enum : int { kSiteParticle = 1, kSiteFlush = 2, kSiteScatter = 3, kSiteGather = 4, kSiteHeat = 5, kSiteBin = 6,
+             kSiteDetCell = 7, kSiteDetRow = 8 };
+#ifdef MPMB_CHECKED
+struct CheckRecord {
+    unsigned long long count;
+    long long index;
+    int site;
+    int pad;
+};
+static __device__ CheckRecord g_check;
+__device__ __noinline__ bool check_fail(int site, long long index) {
+    if (atomicAdd(&g_check.count, 1ull) == 0ull) {
+        g_check.site = site;
+        g_check.index = index;
+    }
+    return false;
+}
+#define MPMB_CHECK(cond, site, index) ((cond) ? true : check_fail((site), (long long)(index)))
+#else
+#define MPMB_CHECK(cond, site, index) true
+#endif
+
 // ------------------------------------------------------------------ PTX helpers
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -268,7 +294,9 @@ __device__ __noinline__ GatherOut<R> gather_global(const Inst<R>& P, const V4<R>
             for (int k = 0; k < 3; ++k) {
                 const int gz = gb[2] + k;
                 if (gz < 0 || gz >= P.nz) continue;
-                const NV<R> nv = node_vel(P, grid[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], gx, gy, gz, pr0, pr2);
+                const int64_t gi = gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz);
+                if (!MPMB_CHECK(gi >= 0 && gi < P.nn, kSiteGather, gi)) continue;
+                const NV<R> nv = node_vel(P, grid[gi], gx, gy, gz, pr0, pr2);
                 const R vv[3] = {nv.x, nv.y, nv.z};
                 const R ww = w[0][i] * w[1][j] * w[2][k];
                 const R g0 = dw[0][i] * w[1][j] * w[2][k], g1 = w[0][i] * dw[1][j] * w[2][k],
@@ -321,7 +349,9 @@ __device__ __noinline__ void scatter_global(const Inst<R>& P, V4<R>* __restrict_
                 for (int a = 0; a < 3; ++a)
                     p[a] = ww * (in.Q[a] + in.Rm[a * 3] * R(i) + in.Rm[a * 3 + 1] * R(j) + in.Rm[a * 3 + 2] * R(k)) +
                            in.S[a * 3] * g0 + in.S[a * 3 + 1] * g1 + in.S[a * 3 + 2] * g2;
-                vec_atomic_add<R>(&grid[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], ww * m, p[0], p[1], p[2]);
+                const int64_t gi = gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz);
+                if (!MPMB_CHECK(gi >= 0 && gi < P.nn, kSiteScatter, gi)) continue;
+                vec_atomic_add<R>(&grid[gi], ww * m, p[0], p[1], p[2]);
             }
         }
     }
@@ -347,7 +377,9 @@ __device__ __noinline__ void scatter_T_global(const Inst<R>& P, R* __restrict__ 
             for (int k = 0; k < 3; ++k) {
                 const int gz = gb[2] + k;
                 if (gz < 0 || gz >= P.nz) continue;
-                atomicAdd(&tw[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], w[0][i] * w[1][j] * w[2][k] * mT);
+                const int64_t gi = gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz);
+                if (!MPMB_CHECK(gi >= 0 && gi < P.nn, kSiteHeat, gi)) continue;
+                atomicAdd(&tw[gi], w[0][i] * w[1][j] * w[2][k] * mT);
             }
         }
     }
@@ -956,6 +988,7 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT>& Sm, int cell, 
 template <typename R>
 __device__ __noinline__ void det_contrib(const StepArgs& sa, int64_t pi, R m, const R* xi, const R* Q, const R* Rm,
                                          const R* S) {
+    if (!MPMB_CHECK(pi >= 0 && pi < sa.det_stride, kSiteDetRow, pi)) return;
     V4<R>* c = static_cast<V4<R>*>(sa.det_contrib) + pi;
     const int64_t ds = sa.det_stride;
     if (!Q) {
@@ -1009,6 +1042,11 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
         const Inst<R>& P = insts[wk.inst];
         const int bx = wk.bin % P.nbx, by = (wk.bin / P.nbx) % P.nby, bz = wk.bin / (P.nbx * P.nby);
         const int g0x = bx * kBin, g0y = by * kBin, g0z = bz * kBin;
+        // (uniform across the CTA: a skipped work item skips for every thread)
+        if (!MPMB_CHECK(wk.bin >= 0 && wk.bin < P.nbins && wk.start >= 0 && wk.count >= 0 &&
+                            (int64_t)wk.start + wk.count <= P.np,
+                        kSiteBin, wi))
+            continue;
         const double tg = da(P.t0, dm((double)sa.k, P.dt));         // time of the G2P step
         const double tp = da(P.t0, dm((double)sa.p2g_step, P.dt));  // time of the P2G step
         const double prg0 = da(P.tool_p0[0], dm(P.tool_v[0], ds(tg, P.tool_t0)));
@@ -1067,8 +1105,17 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                 // every load of the particle is issued here, before any branch on its
                 // state: one memory round trip.  Slots past the bin's end read the
                 // bin's first particle (bins are never empty) and are discarded.
+#ifdef MPMB_CHECKED
+                bool valid = pl < wk.count;
+                int64_t pi = P.pbase + wk.start + (valid ? pl : 0);
+                if (!MPMB_CHECK(pi >= P.pbase && pi < P.pbase + P.pcap, kSiteParticle, pi)) {
+                    valid = false;
+                    pi = P.pbase;
+                }
+#else
                 const bool valid = pl < wk.count;
                 const int64_t pi = P.pbase + wk.start + (valid ? pl : 0);
+#endif
                 const uint8_t st_ld = ps.status[pi];
                 const V4<R> a0 = ps.A[0][pi], a1 = ps.A[1][pi], a2 = ps.A[2][pi], a3 = ps.A[3][pi];
                 const V4<R> xl = (G2P && ps.X) ? ps.X[pi] : mk4<R>(0, 0, 0, 0);
@@ -1486,9 +1533,10 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                 if (m == R(0)) continue;
                 const int gx = g0x + X, gy = g0y + Y, gz = g0z + Z;
                 if (gx >= P.nx || gy >= P.ny || gz >= P.nz) continue;
-                vec_atomic_add<R>(&gw[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], m, px, py, pz);
-                if (EXT && P.heat_on)
-                    atomicAdd(&P.tm[rbuf ^ (G2P ? 1 : 0)][gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)], mT);
+                const int64_t gi = gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz);
+                if (!MPMB_CHECK(gi >= 0 && gi < P.nn, kSiteFlush, gi)) continue;
+                vec_atomic_add<R>(&gw[gi], m, px, py, pz);
+                if (EXT && P.heat_on) atomicAdd(&P.tm[rbuf ^ (G2P ? 1 : 0)][gi], mT);
             }
         }
         __syncthreads();
@@ -1562,6 +1610,7 @@ __global__ void k_p2g_det(const Inst<R>* __restrict__ insts, int n_inst, const v
                 // every particle of the cell has its base at the cell (deterministic re-bin)
                 const V4<R>* __restrict__ row = c + (int64_t)((gx - cx) + 3 * (gy - cy) + 9 * (gz - cz)) * stride;
                 const int64_t s1 = offset[key + 1];
+                if (!MPMB_CHECK(offset[key] >= P.pbase && s1 <= P.pbase + P.pcap, kSiteDetCell, key)) continue;
                 for (int64_t s = offset[key]; s < s1; ++s) {
                     const V4<R> v = row[s];
                     m += v.x; p[0] += v.y; p[1] += v.z; p[2] += v.w;
@@ -1632,3 +1681,35 @@ template void launch_step<double>(const Inst<double>*, const Work*, const int*, 
                                   const StepArgs&, int, bool, bool, int, int, int*, unsigned long long*, cudaStream_t);
 
 }  // namespace mpmb
+
+extern "C" mpm_status mpm_check_report(int64_t* violations, int32_t* site, int64_t* index, int32_t reset) {
+#ifdef MPMB_CHECKED
+    using mpmb::CheckRecord;
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        cudaGetLastError();
+        return MPM_CUDA_ERROR;
+    }
+    CheckRecord r{};
+    if (cudaMemcpyFromSymbol(&r, mpmb::g_check, sizeof(r)) != cudaSuccess) {
+        cudaGetLastError();
+        return MPM_CUDA_ERROR;
+    }
+    if (violations) *violations = (int64_t)r.count;
+    if (site) *site = r.site;
+    if (index) *index = r.index;
+    if (reset) {
+        const CheckRecord z{};
+        if (cudaMemcpyToSymbol(mpmb::g_check, &z, sizeof(z)) != cudaSuccess) {
+            cudaGetLastError();
+            return MPM_CUDA_ERROR;
+        }
+    }
+    return MPM_OK;
+#else
+    (void)reset;
+    if (violations) *violations = 0;
+    if (site) *site = 0;
+    if (index) *index = 0;
+    return MPM_NOT_SUPPORTED;
+#endif
+}

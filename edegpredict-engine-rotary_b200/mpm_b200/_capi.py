@@ -7,9 +7,12 @@ there is no fallback implementation.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "libmpm_b200.so"
+# MPM_B200_LIB selects another build of the library (the bounds-checked
+# libmpm_b200_checked.so) before the first call of lib().
+LIB_PATH = Path(os.environ.get("MPM_B200_LIB") or Path(__file__).resolve().parent / "libmpm_b200.so")
 
 MPM_ABI_VERSION = 1
 MPM_OK, MPM_INVALID_ARG, MPM_OOM, MPM_CUDA_ERROR, MPM_NUMERIC, MPM_OUT_OF_GRID, MPM_TIMEOUT, \
@@ -178,6 +181,7 @@ def lib() -> C.CDLL:
             "mpm_server_tick": (_i32, [_vp, P(_i32)]),
             "mpm_server_poll": (_i32, [_vp, _i64, P(MpmResult)]),
             "mpm_server_cancel": (_i32, [_vp, _i64]),
+            "mpm_check_report": (_i32, [P(_i64), P(_i32), P(_i64), _i32]),
             "mpm_server_stats_get": (_i32, [_vp, P(MpmServerStats)]),
             "mpm_server_footprint": (_i32, [P(MpmServerConfig), P(MpmRequest), P(_i64)]),
             "mpm_get_launch_config": (_i32, [_vp, P(MpmLaunchConfig)]),

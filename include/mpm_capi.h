@@ -496,6 +496,19 @@ mpm_status mpm_server_footprint(const mpm_server_config *cfg, const mpm_request 
  * the stream (NULL: legacy default stream). */
 mpm_status mpm_selftest_bounded_wait(int64_t limit_ns, void *stream);
 
+/* Bounds-checked build report (no counterpart in the reference, which has
+ * no sanitizer runs).  libmpm_b200_checked.so, built with -DMPMB_CHECKED,
+ * checks every index its step kernels derive from data (particle slots of a
+ * work item, grid nodes of the tile flush and of the off-tile scatter and
+ * gather, heat-conduction nodes, deterministic-mode cells and rows) before
+ * using it; a failed check is counted, the first one's site (1 particle slot,
+ * 2 tile flush, 3 scatter, 4 gather, 5 heat scatter, 6 work item, 7 and 8
+ * deterministic cell range and row) and index are kept, and the access is
+ * skipped rather than trapped.  This reads the record after synchronising the
+ * device, and clears it when reset != 0.  The default library has no checks
+ * and returns MPM_NOT_SUPPORTED with zeros. */
+mpm_status mpm_check_report(int64_t *violations, int32_t *site, int64_t *index, int32_t reset);
+
 /* Record CUDA events around every launch of the step kernel (enable != 0),
  * for timing the dominant kernel inside a longer run.  mpm_profile_read
  * synchronises, returns the summed device time (ms) and count of the fused

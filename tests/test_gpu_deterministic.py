@@ -125,3 +125,16 @@ def test_extensions_are_refused():
         assert e.value.status == A.MPM_NOT_SUPPORTED
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("name", ["plastic_damage_chip", "lod_kinematic_extf"])
+def test_matches_the_atomic_path_fp64(name):
+    """The deterministic sums against the default atomic path (fused
+    schedule): FP64 within 1e-9, status identical."""
+    from test_gpu_parity import run_ours
+    case, st, n, _ = SCENARIOS[name]()
+    atomic = run_ours(case, st, n, prec=A.PREC_F64)
+    det = run_det(case, st, n, A.PREC_F64)
+    assert (det["status"] == atomic["status"]).all()
+    err = field_errors(det, atomic, case)
+    assert max(err.values()) < 1e-9, err
