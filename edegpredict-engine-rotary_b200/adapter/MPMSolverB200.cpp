@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstddef>
 #include <iostream>
+#include <limits>
 
 #include "Config.h"
 
@@ -271,7 +272,23 @@ void MPMSolverB200::getBounds(double& minX, double& minY, double& minZ, double& 
 void MPMSolverB200::syncMetrics() {
     if (!m_h || m_numParticles == 0) return;
     mpm_metrics m{};
-    if (check(mpm_sync_metrics(m_h, &m))) m_metrics = m;
+    const mpm_status s = mpm_sync_metrics(m_h, &m);
+    if (s == MPM_NUMERIC) {
+        // The workpiece's error word is set (a NaN or Inf state, or a Newton
+        // return that did not converge).  The kill zone has taken the NaN
+        // particles out of the reductions, so the peaks alone would look
+        // healthy: report them as NaN, which SimulationHealthMonitor::check
+        // turns into its NAN_CORRUPTION halt
+        // (include/SimulationHealthMonitor.h:321-328), as a NaN would in the
+        // reference.  Not run by the tests (they compile against the
+        // reference's headers, which only this container has).
+        m.ref_max_stress = std::numeric_limits<double>::quiet_NaN();
+        m.ref_max_temperature = std::numeric_limits<double>::quiet_NaN();
+        m_metrics = m;
+        check(s);
+        return;
+    }
+    if (check(s)) m_metrics = m;
 }
 
 void MPMSolverB200::applyHeatFlux(double, double, double, double) {}
