@@ -245,30 +245,52 @@ __device__ __forceinline__ int64_t in_bin_slot(int r, int n) {
     return ((int64_t)r * inv_mod(s, n)) % n;
 }
 
+// Destination slot of source slot pi in the new layout (-1: an unused slot).
 template <typename R>
-__global__ void k_bin_scatter(PState<R> src, PState<R> dst, const Inst<R>* insts, int n_inst, const int32_t* key,
-                              const int32_t* rank, const int32_t* offset, const int32_t* key_base,
-                              const int32_t* newbin, bool initial, const double* pos_scratch, bool has_K,
-                              int64_t np, bool det) {
+__device__ __forceinline__ int64_t bin_dest(const Inst<R>& P, int ii, int64_t pi, const int32_t* key,
+                                            const int32_t* rank, const int32_t* offset, const int32_t* key_base,
+                                            const int32_t* newbin, bool det) {
+    if (pi >= P.pbase + P.np) return -1;
+    const int32_t kk = key[pi];
+    if (kk - key_base[ii] >= P.nbins * kCellsPerBin) return offset[kk] + rank[pi];  // INACTIVE: after the bins
+    const int32_t fk = key_base[ii] + newbin[pi] * kCellsPerBin;
+    const int64_t b0 = offset[fk];
+    const int n = offset[fk + kCellsPerBin] - (int)b0;
+    const int r = (int)(offset[kk] - b0) + rank[pi];
+    // deterministic mode keeps each cell's particles together, in rank order
+    return b0 + (det ? (int64_t)r : in_bin_slot(r, n));
+}
+
+// The re-bin's move, in two launches so that the writes are coalesced: the
+// first records for every destination slot its source (perm[d] = pi), the
+// second runs one thread per destination slot and copies the particle from
+// its source, which lies in the same bin's window of the old layout (read
+// through L2) -- a scatter by source slot wrote every 16-, 4- and 1-byte field
+// to a permuted slot and moved about twice the bytes through DRAM.
+template <typename R>
+__global__ void k_bin_perm(const Inst<R>* insts, int n_inst, const int32_t* key, const int32_t* rank,
+                           const int32_t* offset, const int32_t* key_base, const int32_t* newbin, int32_t* perm,
+                           int64_t np, bool det) {
     const int64_t pi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pi >= np) return;
     const int ii = find_inst(insts, n_inst, pi);
+    const int64_t d = bin_dest(insts[ii], ii, pi, key, rank, offset, key_base, newbin, det);
+    if (d >= 0) perm[d] = (int32_t)pi;
+}
+
+template <typename R>
+__global__ void k_bin_gather(PState<R> src, PState<R> dst, const Inst<R>* insts, int n_inst, const int32_t* key,
+                             const int32_t* key_base, const int32_t* newbin, const int32_t* perm, bool initial,
+                             const double* pos_scratch, bool has_K, int64_t np, bool det) {
+    const int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= np) return;
+    const int64_t pi = perm[d];
+    if (pi < 0) return;
+    const int ii = find_inst(insts, n_inst, pi);
     const Inst<R>& P = insts[ii];
-    if (pi >= P.pbase + P.np) return;
     const bool fresh = initial && P.fresh;
     const int32_t kk = key[pi];
     const int nbn = newbin[pi];
-    int64_t d;
-    if (kk - key_base[ii] >= P.nbins * kCellsPerBin) {
-        d = offset[kk] + rank[pi];  // INACTIVE: after the bins, in arrival order
-    } else {
-        const int32_t fk = key_base[ii] + nbn * kCellsPerBin;
-        const int64_t b0 = offset[fk];
-        const int n = offset[fk + kCellsPerBin] - (int)b0;
-        const int r = (int)(offset[kk] - b0) + rank[pi];
-        // deterministic mode keeps each cell's particles together, in rank order
-        d = b0 + (det ? (int64_t)r : in_bin_slot(r, n));
-    }
     const int nbv[3] = {nbn % P.nbx, (nbn / P.nbx) % P.nby, nbn / (P.nbx * P.nby)};
     V4<R> a0 = src.A[0][pi];
     if (fresh) {
@@ -806,12 +828,14 @@ template <typename R>
 void launch_bin_scatter(const PState<R>& src, const PState<R>& dst, const Inst<R>* insts, int n_inst,
                         const int32_t* key, const int32_t* rank, const int32_t* offset, const int32_t* key_base,
                         const int32_t* newbin, bool initial, const double* pos_scratch, bool has_K, int64_t np,
-                        cudaStream_t st, bool det) {
+                        int32_t* perm, cudaStream_t st, bool det) {
     if (np <= 0) return;
-    k_bin_scatter<R><<<(int)((np + kT - 1) / kT), kT, 0, st>>>(src, dst, insts, n_inst, key, rank, offset,
-                                                               key_base, newbin, initial, pos_scratch, has_K, np,
-                                                               det);
-    ++launch_counter();
+    const int blocks = (int)((np + kT - 1) / kT);
+    cudaMemsetAsync(perm, 0xff, sizeof(int32_t) * np, st);
+    k_bin_perm<R><<<blocks, kT, 0, st>>>(insts, n_inst, key, rank, offset, key_base, newbin, perm, np, det);
+    k_bin_gather<R><<<blocks, kT, 0, st>>>(src, dst, insts, n_inst, key, key_base, newbin, perm, initial,
+                                           pos_scratch, has_K, np, det);
+    launch_counter() += 2;
 }
 
 void launch_raster(const double* sx, const double* sy, const double* sz, int ns, double px, double py, double pz,
@@ -981,7 +1005,7 @@ void launch_heat_diffuse(const Inst<R>* insts, int n_inst, int b, int64_t total,
                                       int32_t*, int32_t*, int32_t*, int32_t*, int64_t, cudaStream_t);               \
     template void launch_bin_scatter<R>(const PState<R>&, const PState<R>&, const Inst<R>*, int, const int32_t*,    \
                                         const int32_t*, const int32_t*, const int32_t*, const int32_t*, bool,       \
-                                        const double*, bool, int64_t, cudaStream_t, bool);                           \
+                                        const double*, bool, int64_t, int32_t*, cudaStream_t, bool);                 \
     template void launch_import<R>(const DevSoA&, int64_t, double, double, double, double, double, const PState<R>&, \
                                    int64_t, double*, cudaStream_t);                                                  \
     template void launch_gen<R>(const Inst<R>&, const int32_t*, const int32_t*, int, uint64_t, uint32_t, int, double, \

@@ -112,6 +112,8 @@ class Engine final : public EngineBase {
     int32_t *d_key_base = nullptr, *d_bin_key = nullptr, *d_bin_inst = nullptr, *d_bin_local = nullptr;
     int64_t* d_inst_pbase = nullptr;
     int32_t *d_key = nullptr, *d_rank = nullptr, *d_newbin = nullptr, *d_count = nullptr, *d_offset = nullptr;
+    int32_t* d_perm = nullptr;     // re-bin: source slot of every destination slot
+    int64_t perm_alloc = 0;
     int32_t *d_flag = nullptr, *d_flag_scan = nullptr, *d_scan_tmp = nullptr;
     double* d_pos = nullptr;
     Work* d_work = nullptr;
@@ -190,7 +192,7 @@ class Engine final : public EngineBase {
                         d_bin_local,
                         d_inst_pbase, d_key, d_rank, d_newbin, d_count, d_offset, d_flag, d_flag_scan, d_scan_tmp,
                         d_pos, d_work, d_nwork, d_err, d_ierr, d_ctr, d_stat_part, d_stat_out, d_stage, d_gen,
-                        d_map, d_det_contrib, d_det_i32[0], d_det_i32[1], d_det_i32[2], d_det_i32[3], d_det_tmp};
+                        d_map, d_perm, d_det_contrib, d_det_i32[0], d_det_i32[1], d_det_i32[2], d_det_i32[3], d_det_tmp};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         for (auto& x : I)
@@ -448,6 +450,7 @@ class Engine final : public EngineBase {
         MS(grow(d_key, slot_alloc[0], cp));
         MS(grow(d_rank, slot_alloc[1], cp));
         MS(grow(d_newbin, slot_alloc[2], cp));
+        MS(grow(d_perm, perm_alloc, cp));
         MS(grow(d_pos, slot_alloc[3], 3 * cp));
         MS(grow(d_count, key_alloc[0], nkeys + 1));
         MS(grow(d_offset, key_alloc[1], nkeys + 1));
@@ -535,6 +538,7 @@ class Engine final : public EngineBase {
         MS(grow(d_key, slot_alloc[0], particles, false));
         MS(grow(d_rank, slot_alloc[1], particles, false));
         MS(grow(d_newbin, slot_alloc[2], particles, false));
+        MS(grow(d_perm, perm_alloc, particles, false));
         MS(grow(d_pos, slot_alloc[3], 3 * particles, false));
         MS(grow(d_count, key_alloc[0], keys + 1, false));
         MS(grow(d_offset, key_alloc[1], keys + 1, false));
@@ -746,7 +750,7 @@ class Engine final : public EngineBase {
         exclusive_scan(d_count, d_offset, nkeys, d_scan_tmp, st);
         MS(det_ranks());
         launch_bin_scatter<R>(ps[cur], ps[cur ^ 1], d_inst, (int)I.size(), d_key, d_rank, d_offset, d_key_base,
-                              d_newbin, true, d_pos, has_K, cap_total, st, det);
+                              d_newbin, true, d_pos, has_K, cap_total, d_perm, st, det);
         build_work(d_offset, d_bin_key, d_bin_inst, d_bin_local, d_inst_pbase, max_work, d_flag, d_flag_scan,
                    d_scan_tmp, d_work, d_nwork, st);
         cur ^= 1;
@@ -1355,7 +1359,7 @@ class Engine final : public EngineBase {
         exclusive_scan(d_count, d_offset, nkeys, d_scan_tmp, st);
         MS(det_ranks());
         launch_bin_scatter<R>(ps[cur], ps[cur ^ 1], d_inst, (int)I.size(), d_key, d_rank, d_offset, d_key_base,
-                              d_newbin, false, d_pos, has_K, cap_total, st, det);
+                              d_newbin, false, d_pos, has_K, cap_total, d_perm, st, det);
         build_work(d_offset, d_bin_key, d_bin_inst, d_bin_local, d_inst_pbase, max_work, d_flag, d_flag_scan,
                    d_scan_tmp, d_work, d_nwork, st);
         cur ^= 1;
