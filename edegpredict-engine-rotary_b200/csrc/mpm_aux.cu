@@ -715,10 +715,14 @@ __global__ void k_stats(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64_
                         double cp, double Tamb, double* partial) {
     __shared__ double sh[kStatSlots][kT / 32];
     const Inst<R>& P = *inst;
+    // the accumulators stay in registers: every loop over them is unrolled
     double acc[kStatSlots];
+#pragma unroll
     for (int q = 0; q < kStatSlots; ++q) acc[q] = 0.0;
     acc[7] = -INFINITY; acc[8] = 0.0; acc[9] = -INFINITY; acc[11] = 0.0; acc[12] = 0.0;
+#pragma unroll
     for (int q = 19; q < 22; ++q) acc[q] = INFINITY;
+#pragma unroll
     for (int q = 22; q < 25; ++q) acc[q] = -INFINITY;
     const double m = (double)P.pmass, V = (double)P.pvol;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
@@ -753,6 +757,7 @@ __global__ void k_stats(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64_
             acc[14] += (vm * vm * m) / (6.0 * 80e9) + V * eps * vm;
             double xw[3];
             world_pos(P, ps, pi, a0, xw);
+#pragma unroll
             for (int q = 0; q < 3; ++q) {
                 acc[19 + q] = fmin(acc[19 + q], xw[q]);
                 acc[22 + q] = fmax(acc[22 + q], xw[q]);
@@ -760,6 +765,7 @@ __global__ void k_stats(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64_
         }
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
     for (int q = 0; q < kStatSlots; ++q) {
         double v = acc[q];
         const bool isMin = (q >= 19 && q < 22);
