@@ -33,6 +33,18 @@ struct GpuOps {
     mpm_status step(int k, const std::vector<double>& dts) { return e->step(k, dts.data()); }
     mpm_status metrics(int inst, mpm_metrics* m) { return e->metrics(inst, m); }
     mpm_status health(std::vector<int32_t>& st) { return e->inst_statuses(st.data(), (int)st.size()); }
+    mpm_status save(int inst, std::vector<unsigned char>* buf) {
+        int64_t n = 0;
+        mpm_status s = e->checkpoint_bytes(inst, &n);
+        if (s != MPM_OK) return s;
+        buf->resize((size_t)n);
+        return e->checkpoint_save(inst, buf->data(), n);
+    }
+    mpm_status restore(int inst, const std::vector<unsigned char>& buf, int64_t* np) {
+        const mpm_status s = e->checkpoint_load(inst, buf.data(), (int64_t)buf.size());
+        *np = e->inst(inst).np;
+        return s;
+    }
 };
 
 mpm_status fail(mpm_status s, const std::string& m) {
@@ -150,6 +162,13 @@ mpm_status mpm_server_cancel(mpm_server* s, int64_t id) {
     if (!s) return mpmb::fail(MPM_INVALID_ARG, "server is NULL");
     const mpm_status st = s->sched->cancel(id);
     if (st != MPM_OK) return mpmb::fail(st, "unknown request id");
+    return MPM_OK;
+}
+
+mpm_status mpm_server_preempt(mpm_server* s, int64_t id) {
+    if (!s) return mpmb::fail(MPM_INVALID_ARG, "server is NULL");
+    const mpm_status st = s->sched->preempt(id);
+    if (st != MPM_OK) return mpmb::fail(st, "unknown request id or the request is not running");
     return MPM_OK;
 }
 

@@ -16,9 +16,13 @@
 //      step 1, while the others run on;
 //   6. records the metrics of every request that reached its step count.
 // cancel() ends a queued request at once and marks a running one, which the
-// next tick's step 1 drops.  The engine is a template parameter: the GPU
-// engine in the library, a fake in the host tests.  submit(), poll() and
-// cancel() may run on other threads than tick().
+// next tick's step 1 drops.  preempt() marks a running request: the next
+// tick's step 1 saves its workpiece to host memory (a checkpoint), drops it
+// from the device and queues it again at the back; when it is admitted again
+// its checkpoint is loaded in place of a new workpiece, so it resumes where
+// it stopped.  The engine is a template parameter: the GPU engine in the
+// library, a fake in the host tests.  submit(), poll(), cancel() and
+// preempt() may run on other threads than tick().
 #pragma once
 
 #include <algorithm>
@@ -98,6 +102,8 @@ class Scheduler {
         Footprint f;
         mpm_result res{};
         bool cancel = false;   // cancelled while resident: dropped by the next tick
+        bool preempt = false;  // preempted while resident: saved and requeued by the next tick
+        std::vector<unsigned char> ckpt;   // the saved workpiece of a preempted request
     };
 
     Scheduler(Engine* eng, Pools pools, int max_chunk, int max_resident, std::function<double()> clock,
@@ -150,6 +156,16 @@ class Scheduler {
         return MPM_OK;
     }
 
+    // Preempts a running request (see the file comment); MPM_INVALID_ARG for
+    // an unknown id or a request that is not running.
+    mpm_status preempt(int64_t id) {
+        std::lock_guard<std::mutex> lock(mu_);
+        auto it = all_.find(id);
+        if (it == all_.end() || it->second.res.state != MPM_REQ_RUNNING) return MPM_INVALID_ARG;
+        it->second.preempt = true;
+        return MPM_OK;
+    }
+
     mpm_server_stats stats() {
         std::lock_guard<std::mutex> lock(mu_);
         mpm_server_stats s = stats_;
@@ -168,6 +184,25 @@ class Scheduler {
         std::vector<int32_t> remove;
         std::vector<int64_t> keep;
         Footprint used = used_;
+        // preempted requests: save the workpiece while it is still resident
+        for (size_t i = 0; i < resident_.size(); ++i) {
+            Req& q = ref(resident_[i]);
+            bool pre;
+            {
+                std::lock_guard<std::mutex> lock(mu_);
+                pre = q.res.state == MPM_REQ_RUNNING && q.preempt && !q.cancel;
+            }
+            if (!pre) continue;
+            std::vector<unsigned char> buf;
+            const mpm_status s = eng_->save((int)i, &buf);
+            std::lock_guard<std::mutex> lock(mu_);
+            q.preempt = false;
+            if (s != MPM_OK) continue;   // stays resident; a later preempt may retry
+            q.ckpt = std::move(buf);
+            q.res.state = MPM_REQ_QUEUED;
+            queue_.push_back(q.id);
+            ++stats_.preempted;
+        }
         {
             std::lock_guard<std::mutex> lock(mu_);
             for (size_t i = 0; i < resident_.size(); ++i) {
@@ -218,9 +253,15 @@ class Scheduler {
                 Req& q = ref(add[k]);
                 resident_.push_back(q.id);
                 int64_t np = 0;
-                mpm_status si = eng_->init(first + (int)k, q.r, &np);
+                const bool resume = !q.ckpt.empty();
+                mpm_status si = resume ? eng_->restore(first + (int)k, q.ckpt, &np)
+                                       : eng_->init(first + (int)k, q.r, &np);
                 std::lock_guard<std::mutex> lock(mu_);
-                q.res.t_admit = clock_();
+                if (resume) {
+                    std::vector<unsigned char>().swap(q.ckpt);   // the host copy is no longer needed
+                } else {
+                    q.res.t_admit = clock_();
+                }
                 q.res.n_particles = np;
                 if (si != MPM_OK) {
                     q.res.state = MPM_REQ_FAILED;
@@ -296,6 +337,7 @@ class Scheduler {
         q.res.state = MPM_REQ_CANCELLED;
         q.res.status = MPM_CANCELLED;
         q.res.t_done = clock_();
+        std::vector<unsigned char>().swap(q.ckpt);
         ++stats_.cancelled;
     }
     Req& ref(int64_t id) {

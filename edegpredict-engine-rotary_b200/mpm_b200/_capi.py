@@ -118,7 +118,7 @@ class MpmServerConfig(C.Structure):
 class MpmServerStats(C.Structure):
     _fields_ = [("offered", _i64), ("admitted", _i64), ("completed", _i64), ("failed", _i64), ("queued", _i64),
                 ("resident", _i64), ("particle_updates", _i64), ("resident_particles", _i64), ("ticks", _i64),
-                ("busy_seconds", _d), ("cancelled", _i64)]
+                ("busy_seconds", _d), ("cancelled", _i64), ("preempted", _i64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -181,6 +181,7 @@ def lib() -> C.CDLL:
             "mpm_server_tick": (_i32, [_vp, P(_i32)]),
             "mpm_server_poll": (_i32, [_vp, _i64, P(MpmResult)]),
             "mpm_server_cancel": (_i32, [_vp, _i64]),
+            "mpm_server_preempt": (_i32, [_vp, _i64]),
             "mpm_check_report": (_i32, [P(_i64), P(_i32), P(_i64), _i32]),
             "mpm_server_stats_get": (_i32, [_vp, P(MpmServerStats)]),
             "mpm_server_footprint": (_i32, [P(MpmServerConfig), P(MpmRequest), P(_i64)]),

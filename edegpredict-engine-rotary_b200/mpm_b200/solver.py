@@ -434,6 +434,11 @@ class Server:
         """Cancels a queued request at once, a running one at the next tick."""
         A.check(self._lib.mpm_server_cancel(self.h, int(rid)))
 
+    def preempt(self, rid: int) -> None:
+        """Saves a running request's workpiece at the next tick and queues it
+        again; it resumes where it stopped when it is admitted again."""
+        A.check(self._lib.mpm_server_preempt(self.h, int(rid)))
+
     def tick(self) -> int:
         n = C.c_int32()
         A.check(self._lib.mpm_server_tick(self.h, C.byref(n)))

@@ -465,6 +465,7 @@ typedef struct mpm_server_stats {
     int64_t ticks;
     double busy_seconds;       /* time spent inside mpm_server_tick */
     int64_t cancelled;
+    int64_t preempted;         /* preemptions carried out (a request may count more than once) */
 } mpm_server_stats;
 
 typedef struct mpm_server mpm_server;
@@ -484,6 +485,15 @@ mpm_status mpm_server_poll(mpm_server *s, int64_t id, mpm_result *out);
  * MPM_NUMERIC at the tick that stepped it and is dropped at the next one;
  * the other requests run on. */
 mpm_status mpm_server_cancel(mpm_server *s, int64_t id);
+/* Preempts a running request (no counterpart in the reference): the next
+ * tick saves its workpiece to host memory as a checkpoint (see
+ * mpm_checkpoint_save), drops it from the device, which frees its share of
+ * the pools, and queues the request again at the back.  When it is admitted
+ * again the checkpoint is loaded in place of a new workpiece, so it resumes
+ * at the step it reached, with the same results as an uninterrupted run to
+ * summation order.  MPM_INVALID_ARG for an unknown id or a request that is
+ * not running.  May be called from another thread than tick. */
+mpm_status mpm_server_preempt(mpm_server *s, int64_t id);
 mpm_status mpm_server_stats_get(mpm_server *s, mpm_server_stats *out);
 /* Device bytes a request holds while resident (host-only arithmetic). */
 mpm_status mpm_server_footprint(const mpm_server_config *cfg, const mpm_request *req, int64_t *bytes);

@@ -128,3 +128,33 @@ def test_zero_step_request_and_capacity_refusal():
         assert e.value.status == A.MPM_CAPACITY
     finally:
         srv.close()
+
+
+def test_preempted_request_resumes_where_it_stopped():
+    """A request preempted after 10 of its 30 steps is saved, dropped from the
+    device, admitted again from its checkpoint and finished; its completion
+    metrics equal those of its run alone (FP64: 1e-9 relative, counts exact)."""
+    case = W.config1(cells=(12, 8, 8), speed=20.0)
+    n = 30
+    alone = run_alone(case, n, A.PREC_F64)
+    srv = Server(precision=A.PREC_F64, hbm_budget_bytes=BUDGET, max_chunk=5)
+    try:
+        rid = srv.submit(case, n)
+        srv.tick()
+        srv.tick()                               # 10 steps
+        srv.preempt(rid)
+        srv.tick()                               # saved, dropped and admitted again from the checkpoint
+        assert srv.stats()["preempted"] == 1
+        for _ in range(100):
+            if srv.poll(rid)["state"] == A.REQ_DONE:
+                break
+            srv.tick()
+        res = srv.poll(rid)
+    finally:
+        srv.close()
+    assert res["state"] == A.REQ_DONE and res["steps_done"] == n
+    for k in ("mass", "kinetic", "internal_elastic", "max_plastic_strain", "max_von_mises"):
+        a, b = res["metrics"][k], alone["metrics"][k]
+        assert rel(a, b, abs(b)) <= 1e-9, (k, a, b)
+    for k in ("n_active", "n_chip", "n_inactive"):
+        assert res["metrics"][k] == alone["metrics"][k], k

@@ -60,6 +60,8 @@ struct FakeOps {
         assert(st.size() == caps.size());
         return MPM_OK;
     }
+    mpm_status save(int, std::vector<unsigned char>*) { return MPM_NOT_SUPPORTED; }
+    mpm_status restore(int, const std::vector<unsigned char>&, int64_t*) { return MPM_NOT_SUPPORTED; }
 };
 
 static mpm_request req(int cells_x, int nsteps) {
@@ -205,6 +207,24 @@ struct FaultyOps {
         for (size_t i = 0; i < caps.size(); ++i) st[i] = caps[i] == bad_tag ? MPM_NUMERIC : MPM_OK;
         return MPM_OK;
     }
+    // a checkpoint of the fake: the instance's tag and step count
+    mpm_status save(int inst, std::vector<unsigned char>* buf) {
+        const int64_t v[2] = {caps[inst], steps[inst]};
+        buf->assign((const unsigned char*)v, (const unsigned char*)v + sizeof(v));
+        ++saves;
+        return MPM_OK;
+    }
+    mpm_status restore(int inst, const std::vector<unsigned char>& buf, int64_t* np) {
+        int64_t v[2];
+        assert(buf.size() == sizeof(v));
+        std::memcpy(v, buf.data(), sizeof(v));
+        assert(v[0] == caps[inst]);
+        steps[inst] = (int)v[1];
+        *np = caps[inst];
+        ++restores;
+        return MPM_OK;
+    }
+    int saves = 0, restores = 0;
 };
 
 static mpm_request req(int cells_x, int nsteps) {
@@ -294,6 +314,34 @@ int main() {
         s.poll(b, &r);
         assert(r.state == MPM_REQ_DONE && r.metrics.mass == 10);
     }
+    // 4. preemption: the workpiece is saved, dropped and queued behind the
+    //    others, then restored and run to its full step count
+    {
+        FaultyOps ops;
+        pools.particles = 35;     // 20 + 10 fit; 20 + 10 + 15 do not
+        Scheduler<FaultyOps> s(&ops, pools, 10, 8, [&]() { now += 1.0; return now; });
+        int64_t a, b, c;
+        s.submit(req(20, 30), &a);
+        s.submit(req(10, 30), &b);
+        assert(s.tick(&nres) == MPM_OK && nres == 2);
+        s.submit(req(15, 20), &c);                      // waits: 45 > 35
+        assert(s.preempt(c) == MPM_INVALID_ARG);         // not running
+        assert(s.preempt(a) == MPM_OK);
+        assert(s.tick(&nres) == MPM_OK);                 // a saved (10 steps) and queued behind c
+        assert(ops.saves == 1);
+        s.poll(a, &r);
+        assert(r.state == MPM_REQ_QUEUED && r.steps_done == 10);
+        s.poll(c, &r);
+        assert(r.state == MPM_REQ_RUNNING);
+        for (int t = 0; t < 10; ++t) s.tick(&nres);
+        s.poll(a, &r);
+        assert(r.state == MPM_REQ_DONE && r.steps_done == 30 && r.metrics.mass == 30 && ops.restores == 1);
+        s.poll(b, &r);
+        assert(r.state == MPM_REQ_DONE && r.metrics.mass == 30);
+        s.poll(c, &r);
+        assert(r.state == MPM_REQ_DONE && r.metrics.mass == 20);
+        assert(s.stats().preempted == 1 && s.stats().completed == 3);
+    }
     std::printf("OK\n");
     return 0;
 }
@@ -307,7 +355,8 @@ def test_scheduler_faults_on_the_host(tmp_path):
     step counts; cancel ends a queued request at once and a running one at the
     next tick; a request with a NaN initial temperature is refused; an instance
     change that fails like an out-of-memory allocator leaves the queue intact
-    for the next tick."""
+    for the next tick; a preempted request is saved, queued behind the waiting
+    ones and resumed from its checkpoint to its full step count."""
     src = tmp_path / "faults.cpp"
     src.write_text(FAULTS)
     exe = tmp_path / "faults"
