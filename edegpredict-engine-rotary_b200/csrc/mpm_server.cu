@@ -68,7 +68,7 @@ extern "C" {
 mpm_status mpm_server_footprint(const mpm_server_config* cfg, const mpm_request* req, int64_t* bytes) {
     if (!cfg || !req || !bytes) return mpmb::fail(MPM_INVALID_ARG, "NULL argument");
     const mpmb::Footprint f = mpmb::request_footprint(*req);
-    const mpmb::PoolBytes b = mpmb::pool_bytes(cfg->precision, cfg->backstress != 0);
+    const mpmb::PoolBytes b = mpmb::pool_bytes(cfg->precision, cfg->backstress != 0, cfg->deterministic != 0);
     *bytes = (int64_t)(f.particles * b.particle + f.nodes * b.node + f.keys * b.key + f.bins * b.bin);
     return MPM_OK;
 }
@@ -99,13 +99,15 @@ mpm_status mpm_server_create(const mpm_server_config* cfg, void* stream, mpm_ser
     std::string e;
     auto eng = make_engine(&tmpl, nullptr, 0, (cudaStream_t)stream, &s, &e);
     if (!eng) return fail(s, e);
-    const Pools pools = pools_for_budget(cfg->hbm_budget_bytes, cfg->precision, cfg->backstress != 0);
+    const Pools pools =
+        pools_for_budget(cfg->hbm_budget_bytes, cfg->precision, cfg->backstress != 0, cfg->deterministic != 0);
     const int max_res = cfg->max_resident > 0 ? cfg->max_resident : 4096;
     s = eng->reserve(pools.particles, pools.nodes, pools.keys, pools.bins, max_res, cfg->backstress != 0);
     if (s != MPM_OK) return fail(s, "reserving the pools: " + eng->err);
     mpm_launch_config lc;
     eng->get_config(&lc);
     lc.use_graph = cfg->use_graph ? 1 : 0;
+    lc.deterministic = cfg->deterministic ? 1 : 0;
     eng->set_config(&lc);
     auto* srv = new mpm_server;
     srv->cfg = *cfg;

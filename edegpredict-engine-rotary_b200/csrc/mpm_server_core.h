@@ -60,14 +60,17 @@ struct PoolBytes {
     double particle, node, key, bin;
 };
 
-inline PoolBytes pool_bytes(int precision, bool backstress) {
+inline PoolBytes pool_bytes(int precision, bool backstress, bool deterministic = false) {
     const double v4 = precision == MPM_PREC_F64 ? 32.0 : 16.0, r = precision == MPM_PREC_F64 ? 8.0 : 4.0;
     PoolBytes b;
     // A0-A5, B0-B3, S0-S1 (+K0-K1), X (FP32 only), sres, status, shear
     // counter, id, bin, orig; two buffers; sort key, rank, new bin (int32) and
     // the FP64 position scratch
     const double nv4 = 12.0 + (backstress ? 2.0 : 0.0) + (precision == MPM_PREC_F64 ? 0.0 : 1.0);
-    b.particle = 2.0 * (nv4 * v4 + r + 2.0 + 12.0) + 12.0 + 24.0;
+    b.particle = 2.0 * (nv4 * v4 + r + 2.0 + 12.0) + 12.0 + 24.0 + 4.0;   // + the re-bin permutation
+    // deterministic mode: 27 node contributions (4 reals each), four int32 sort
+    // arrays and the radix sort's double buffers
+    if (deterministic) b.particle += 27.0 * v4 + 16.0 + 16.0;
     b.node = 2.0 * v4 + 3.0 * r + 1.0;   // two grid buffers, three heat-conduction arrays, tool mask
     b.key = 8.0;                 // count and offset
     b.bin = 40.0;                // bin tables, flags and the work item
@@ -83,8 +86,8 @@ struct Pools {
     }
 };
 
-inline Pools pools_for_budget(int64_t budget, int precision, bool backstress) {
-    const PoolBytes b = pool_bytes(precision, backstress);
+inline Pools pools_for_budget(int64_t budget, int precision, bool backstress, bool deterministic = false) {
+    const PoolBytes b = pool_bytes(precision, backstress, deterministic);
     Pools p;
     p.particles = (int64_t)(0.88 * (double)budget / b.particle);
     p.nodes = (int64_t)(0.08 * (double)budget / b.node);

@@ -112,7 +112,7 @@ class MpmResult(C.Structure):
 
 class MpmServerConfig(C.Structure):
     _fields_ = [("precision", _i32), ("max_chunk", _i32), ("hbm_budget_bytes", _i64), ("max_resident", _i32),
-                ("use_graph", _i32), ("backstress", _i32), ("_pad", _i32), ("max_resident_particles", _i64)]
+                ("use_graph", _i32), ("backstress", _i32), ("deterministic", _i32), ("max_resident_particles", _i64)]
 
 
 class MpmServerStats(C.Structure):

@@ -402,11 +402,12 @@ class Server:
 
     def __init__(self, precision: int = A.PREC_F32, hbm_budget_bytes: int = 8 << 30, max_chunk: int = 50,
                  max_resident: int = 0, use_graph: bool = True, backstress: bool = False, stream: int = 0,
-                 max_resident_particles: int = 0):
+                 max_resident_particles: int = 0, deterministic: bool = False):
         self._lib = A.lib()
         self.precision = precision
         self.cfg = A.MpmServerConfig(int(precision), int(max_chunk), int(hbm_budget_bytes), int(max_resident),
-                                     1 if use_graph else 0, 1 if backstress else 0, 0, int(max_resident_particles))
+                                     1 if use_graph else 0, 1 if backstress else 0, 1 if deterministic else 0,
+                                     int(max_resident_particles))
         h = C.c_void_p()
         A.check(self._lib.mpm_server_create(C.byref(self.cfg), C.c_void_p(stream or None), C.byref(h)))
         self.h = h

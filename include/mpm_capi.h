@@ -451,7 +451,9 @@ typedef struct mpm_server_config {
     int32_t max_resident;      /* requests resident at once at most (0: 4096) */
     int32_t use_graph;         /* replay the tick's step calls from captured CUDA graphs */
     int32_t backstress;        /* also reserve backstress state (requests with H_kin > 0) */
-    int32_t _pad;
+    int32_t deterministic;     /* 1: step in deterministic mode (mpm_launch_config.deterministic), so a
+                                  request's result is the same bit for bit alone and in any mix; the
+                                  mode's per-slot scratch is taken from the budget */
     /* admission also stops at this many resident particles (0: the budget
      * alone); fewer resident particles step faster, so requests finish
      * sooner, at the same throughput once the GPU is full */

@@ -26,8 +26,8 @@ def cases():
     return [W.config3_case(rng, i, cells_lo=6, cells_hi=12) for i in range(len(NSTEPS))]
 
 
-def run_alone(case, n, precision):
-    srv = Server(precision=precision, hbm_budget_bytes=BUDGET, max_chunk=5)
+def run_alone(case, n, precision, det=False):
+    srv = Server(precision=precision, hbm_budget_bytes=BUDGET, max_chunk=5, deterministic=det)
     try:
         rid = srv.submit(case, n)
         while srv.poll(rid)["state"] not in (A.REQ_DONE, A.REQ_FAILED):
@@ -37,8 +37,8 @@ def run_alone(case, n, precision):
         srv.close()
 
 
-def run_mix(cs, precision):
-    srv = Server(precision=precision, hbm_budget_bytes=BUDGET, max_chunk=5)
+def run_mix(cs, precision, det=False):
+    srv = Server(precision=precision, hbm_budget_bytes=BUDGET, max_chunk=5, deterministic=det)
     try:
         ids = [srv.submit(cs[k], NSTEPS[k]) for k in range(3)]
         srv.tick()                      # the first three are on the GPU
@@ -158,3 +158,22 @@ def test_preempted_request_resumes_where_it_stopped():
         assert rel(a, b, abs(b)) <= 1e-9, (k, a, b)
     for k in ("n_active", "n_chip", "n_inactive"):
         assert res["metrics"][k] == alone["metrics"][k], k
+
+
+def test_deterministic_mix_equals_alone_bit_for_bit():
+    """With the server's deterministic option, FP32 results are the same bits
+    alone and in the mix: every per-workpiece metric is equal exactly (the
+    cumulative counters of the whole handle are not per workpiece)."""
+    cs = cases()
+    mix, st = run_mix(cs, A.PREC_F32, det=True)
+    assert st["completed"] == 5 and st["failed"] == 0
+    handle_wide = {"n_escaped", "n_sorts", "n_yielded", "n_contacts", "contact_work", "contact_force",
+                   "n_asb_heated"}
+    for k, c in enumerate(cs):
+        a = run_alone(c, NSTEPS[k], A.PREC_F32, det=True)
+        assert mix[k]["state"] == a["state"] == A.REQ_DONE
+        mm, am = mix[k]["metrics"], a["metrics"]
+        for key in mm:
+            if key not in handle_wide:
+                assert mm[key] == am[key], (k, key, mm[key], am[key])
+

@@ -395,6 +395,22 @@ def test_footprint_is_host_arithmetic():
     nodes = p["nx"] * p["ny"] * p["nz"]
     bins = ((p["nx"] + 3) // 4) * ((p["ny"] + 3) // 4) * ((p["nz"] + 3) // 4)
     particles = 16 ** 3 * 8
-    per_particle = 2 * (13 * 16 + 4 + 2 + 12) + 36   # 12 state vectors + the position low parts
+    per_particle = 2 * (13 * 16 + 4 + 2 + 12) + 36 + 4   # 12 state vectors + the position low parts, permutation
     want = particles * per_particle + nodes * (33 + 12) + (bins * 64 + 2) * 8 + bins * 40   # + 3 FP32 heat arrays
     assert abs(b.value - want) <= 1
+
+
+def test_deterministic_footprint_counts_the_mode_scratch():
+    """A deterministic server counts, per particle slot, the mode's 27 node
+    contributions (16 B each in FP32) and its 32 B of sort scratch."""
+    from mpm_b200 import workpiece as W
+    from mpm_b200.solver import make_request
+    case = W.config1(cells=(16, 16, 16))
+    r = make_request(case, 100)
+    got = []
+    for det in (0, 1):
+        cfg = A.MpmServerConfig(A.PREC_F32, 50, 1 << 30, 0, 0, 0, det, 0)
+        b = C.c_int64()
+        assert A.lib().mpm_server_footprint(C.byref(cfg), C.byref(r), C.byref(b)) == A.MPM_OK
+        got.append(b.value)
+    assert abs(got[1] - got[0] - 16 ** 3 * 8 * (27 * 16 + 32)) <= 1
