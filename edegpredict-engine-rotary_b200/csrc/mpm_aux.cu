@@ -379,9 +379,8 @@ __global__ void k_det_keys(const Inst<R>* insts, int n_inst, const int32_t* key_
 
 // The rank of each live slot within its key: its place in the stably sorted
 // order less the key's first place.
-template <typename R>
-__global__ void k_det_rank(const Inst<R>* insts, int n_inst, const int32_t* sorted_keys, const int32_t* perm,
-                           const int32_t* offset, int32_t* rank, int64_t np) {
+__global__ void k_det_rank(const int32_t* sorted_keys, const int32_t* perm, const int32_t* offset, int32_t* rank,
+                           int64_t np) {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= np) return;
     const int32_t pi = perm[j];
@@ -411,7 +410,7 @@ void launch_det_ranks(const Inst<R>* insts, int n_inst, const int32_t* key_base,
     // the radix sort is stable: slots with equal keys keep their order
     size_t bytes = tmp_bytes;
     cub::DeviceRadixSort::SortPairs(tmp, bytes, keys2, sorted, slots, perm, (int)np, 0, key_bits(nkeys), st);
-    k_det_rank<R><<<blocks, kT, 0, st>>>(insts, n_inst, sorted, perm, offset, rank, np);
+    k_det_rank<<<blocks, kT, 0, st>>>(sorted, perm, offset, rank, np);
     launch_counter() += 2;
 }
 template void launch_det_ranks<float>(const Inst<float>*, int, const int32_t*, int32_t*, const int32_t*, int32_t*,

@@ -159,11 +159,11 @@ struct StepArgs {
     int p2g_step;       // step index of the P2G part
     int ext;            // some instance runs the adiabatic shear model or heat conduction: launches
                         // take the kernel variant that has them (the others carry none of their code)
-    int det;            // deterministic mode: the P2G-only launch writes each particle's 27 node
+    int det = 0;        // deterministic mode: the P2G-only launch writes each particle's 27 node
                         // contributions (m, p) to det_contrib (27 rows of det_stride V4s) for
                         // k_p2g_det to sum
-    void* det_contrib;
-    int64_t det_stride;
+    void* det_contrib = nullptr;
+    int64_t det_stride = 0;
 };
 
 // ------------------------------------------------------------------ weights
