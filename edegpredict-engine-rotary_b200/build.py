@@ -26,6 +26,12 @@ LIB_CHECKED = HERE / "mpm_b200" / "libmpm_b200_checked.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3"]
+# Per-file flags.  The step kernel's FP32 divisions and square roots use the
+# compiler's approximate forms (the reference builds everything with
+# --use_fast_math): 4 % off the fused step on the 33.5M-particle workload, and
+# within the FP32 tolerances of the parity tests.  FP64 arithmetic and the
+# explicitly rounded intrinsics are unaffected; every other file stays IEEE.
+FILE_FLAGS = {"mpm_step.cu": ["-prec-div=false", "-prec-sqrt=false"]}
 
 
 def nvcc() -> str:
@@ -52,7 +58,8 @@ def build(force: bool = False, verbose: bool = False, checked: bool = False) -> 
         obj = out_dir / (src.stem + ".o")
         objs.append(obj)
         if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, hdr_time):
-            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *extra, "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
+            cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *FILE_FLAGS.get(src.name, []), *extra, "-I", str(INCLUDE), "-c",
+                   str(src), "-o", str(obj)]
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)
