@@ -814,8 +814,8 @@ __global__ void k_set_temps(PState<R> ps, int64_t pbase, int64_t n, const double
 
 // ------------------------------------------------------------------ launchers
 
-int64_t& launch_counter() {
-    static int64_t c = 0;
+std::atomic<int64_t>& launch_counter() {
+    static std::atomic<int64_t> c{0};
     return c;
 }
 

@@ -822,6 +822,7 @@ class Engine final : public EngineBase {
         cudaFree(tmp);
         x.np = (int64_t)lasti + lastf;
         x.fresh = 1;
+        x.broken = false;
         CK(cudaMemsetAsync(d_ierr + i, 0, sizeof(int), st));   // a new state starts without errors
         CK(cudaGetLastError());
         return push_insts();  // binned by the next call that needs it
@@ -885,6 +886,7 @@ class Engine final : public EngineBase {
                          st);
         x.np = n;
         x.fresh = 1;
+        x.broken = false;
         CK(cudaMemsetAsync(d_ierr + i, 0, sizeof(int), st));   // a new state starts without errors
         CK(cudaGetLastError());
         return push_insts();  // binned by the next call that needs it
@@ -1077,6 +1079,11 @@ class Engine final : public EngineBase {
         for (int i = 0; i < (int)I.size(); ++i) {
             if (!(dts[i] > 0.0) || !std::isfinite(dts[i])) {
                 err = "dt must be positive";
+                return MPM_INVALID_ARG;
+            }
+            if (I[i].broken) {
+                err = "workpiece " + std::to_string(i) + " was left part-loaded by a failed checkpoint load; "
+                      "upload, generate or load it again";
                 return MPM_INVALID_ARG;
             }
             I[i].dt = dts[i];
@@ -1604,32 +1611,43 @@ class Engine final : public EngineBase {
             return MPM_NOT_SUPPORTED;
         }
         CK(cudaStreamSynchronize(st));   // nothing in flight uses the instance's slots
+        // The one allocation (the raster samples) comes before anything of the
+        // instance is overwritten: a refusal here leaves the old state whole.
+        double* samples = nullptr;
+        if (h.n_samples > 0) CK(cudaMalloc(&samples, 24 * (size_t)h.n_samples));
+        // From here on a failure leaves the particle arrays part old, part new:
+        // the instance is marked broken, and steps refuse it until a complete
+        // state replaces it.
+        x.broken = true;
         const unsigned char* q = static_cast<const unsigned char*>(buf) + sizeof(CkptHeader);
         const int64_t n = h.np;
-        for (const auto& a : ckpt_arrays(ps[cur], x.pbase)) {
-            const bool is_K = has_K && !h.has_K && (a.first == (char*)(ps[cur].K[0] + x.pbase) ||
-                                                    a.first == (char*)(ps[cur].K[1] + x.pbase));
-            if (is_K) {
-                // a checkpoint without backstress into a handle that has it: zero
-                if (n > 0) CK(cudaMemsetAsync(a.first, 0, a.second * n, st));
-                continue;
+        auto copy_in = [&]() -> mpm_status {
+            for (const auto& a : ckpt_arrays(ps[cur], x.pbase)) {
+                const bool is_K = has_K && !h.has_K && (a.first == (char*)(ps[cur].K[0] + x.pbase) ||
+                                                        a.first == (char*)(ps[cur].K[1] + x.pbase));
+                if (is_K) {
+                    // a checkpoint without backstress into a handle that has it: zero
+                    if (n > 0) CK(cudaMemsetAsync(a.first, 0, a.second * n, st));
+                    continue;
+                }
+                if (n > 0) CK(cudaMemcpyAsync(a.first, q, a.second * n, cudaMemcpyHostToDevice, st));
+                q += a.second * n;
             }
-            if (n > 0) CK(cudaMemcpyAsync(a.first, q, a.second * n, cudaMemcpyHostToDevice, st));
-            q += a.second * n;
-        }
-        if (x.d_samples) {
+            if (h.n_samples > 0)
+                CK(cudaMemcpyAsync(samples, q, 24 * (size_t)h.n_samples, cudaMemcpyHostToDevice, st));
+            CK(cudaMemsetAsync(d_ierr + i, 0, sizeof(int), st));
             CK(cudaStreamSynchronize(st));
-            cudaFree(x.d_samples);
-            x.d_samples = nullptr;
+            return MPM_OK;
+        };
+        if ((s = copy_in()) != MPM_OK) {
+            if (samples) cudaFree(samples);
+            err = "checkpoint load failed part-way; the workpiece must be uploaded or loaded again (" + err + ")";
+            return s;
         }
-        x.n_samples = 0;
-        if (h.n_samples > 0) {
-            CK(cudaMalloc(&x.d_samples, 24 * (size_t)h.n_samples));
-            CK(cudaMemcpyAsync(x.d_samples, q, 24 * (size_t)h.n_samples, cudaMemcpyHostToDevice, st));
-            x.n_samples = h.n_samples;
-        }
-        CK(cudaMemsetAsync(d_ierr + i, 0, sizeof(int), st));
-        CK(cudaStreamSynchronize(st));
+        if (x.d_samples) cudaFree(x.d_samples);   // the stream is idle (synchronised above)
+        x.d_samples = samples;
+        x.n_samples = h.n_samples > 0 ? h.n_samples : 0;
+        x.broken = false;
         x.p = h.params;
         x.tool = h.tool;
         x.np = n;

@@ -46,6 +46,10 @@ struct InstHost {
     double tool_t0 = 0.0;   // time at which the tool descriptor was set
     std::shared_ptr<ToolSdfTex> sdf;   // voxel tool SDF for the contact (null: analytic SDF)
     int fresh = 0;          // particles uploaded or generated, not yet binned
+    // A checkpoint load failed after it began to overwrite the particle
+    // arrays: the state is part old, part new.  Steps refuse the handle until
+    // an upload, a generated box or a complete checkpoint load replaces it.
+    bool broken = false;
 };
 
 class EngineBase {

@@ -7,6 +7,7 @@
 
 #include <nvtx3/nvToolsExt.h>
 
+#include <atomic>
 #include <string>
 
 #include "../../include/mpm_capi.h"
@@ -148,8 +149,9 @@ void build_work(const int32_t* offset, const int32_t* bin_key, const int32_t* bi
                 Work* work, int* n_work, cudaStream_t st);
 void fill_i32(int32_t* p, int32_t v, int64_t n, cudaStream_t st);
 
-// Kernel launches issued by this process (all handles).
-int64_t& launch_counter();
+// Kernel launches issued by this process (all handles and the handle-free
+// entry points), counted atomically: any host thread may launch.
+std::atomic<int64_t>& launch_counter();
 
 // The calling thread's error string, returned by mpm_last_error(NULL).
 void set_lib_error(const std::string& m);

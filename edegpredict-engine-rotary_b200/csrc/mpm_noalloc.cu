@@ -21,18 +21,20 @@
 // the result row before it reads them.  Because the ranges are fixed, the
 // summation order -- and so the result -- depends only on n and the data.
 //
-// The first call on a device looks up the scratch's device address there
-// (cudaGetSymbolAddress, which also loads this library's kernels onto that
-// device); later calls reuse it.  Make that first call before any stream
-// capture.  The scratch is shared by every caller on a device, so calls on
-// one device must not overlap: two calls in flight at once (from two host
-// threads, or on two streams) race on it and both results are wrong.  Each
-// call waits for its own result before returning.
+// Every call looks up the scratch's device address on the current device
+// (cudaGetSymbolAddress, which on the first call also loads this library's
+// kernels onto that device) and checks the lookup; nothing is cached, so a
+// cudaDeviceReset, a torn-down primary context or another current context
+// gets the address that is valid in it.  The call synchronises its stream,
+// so it cannot be made while that stream is being captured.  The scratch is
+// shared by every caller on a device, so calls on one device must not
+// overlap: two calls in flight at once (from two host threads, or on two
+// streams) race on it and both results are wrong.  Each call waits for its
+// own result before returning.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "../../include/mpm_capi.h"
@@ -45,7 +47,6 @@ constexpr int kNoAllocThreads = 256;
 constexpr int64_t kRecordsPerBlock = 16384;
 constexpr int kMaxBlocks = 4096;
 constexpr int64_t kMaxRecords = kMaxBlocks * kRecordsPerBlock;  // 67,108,864
-constexpr int kMaxDevices = 64;
 
 // kMaxBlocks partial rows, then the result row.
 __device__ __align__(256) double g_metrics_scratch[(kMaxBlocks + 1) * kStatSlots];
@@ -142,30 +143,27 @@ __global__ void k_aos_stats_final(const double* __restrict__ partial, int nb, do
     out[q] = v;
 }
 
-std::mutex g_setup_mu;
-double* g_scratch_dev[kMaxDevices] = {};
-
 mpm_status fail(mpm_status s, const std::string& m) {
     set_lib_error("mpm_metrics_aos_noalloc: " + m);
     return s;
 }
 
-// Device address of g_metrics_scratch on the current device, looked up once.
+// Device address of g_metrics_scratch in the current context of the current
+// device.  Looked up on every call rather than cached per device ordinal: a
+// cached address would outlive a cudaDeviceReset or a primary-context
+// teardown, and would belong to another context when the caller makes a
+// non-primary context current, and a kernel given it would write through a
+// stale or foreign pointer.
 mpm_status scratch_on_current_device(double** out) {
     int dev = -1;
     cudaError_t rc = cudaGetDevice(&dev);
     if (rc != cudaSuccess) return fail(MPM_CUDA_ERROR, std::string("cudaGetDevice: ") + cudaGetErrorString(rc));
-    if (dev < 0 || dev >= kMaxDevices) return fail(MPM_NOT_SUPPORTED, "device ordinal above 63");
-    std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_dev[dev]) {
-        void* p = nullptr;
-        rc = cudaGetSymbolAddress(&p, g_metrics_scratch);
-        if (rc != cudaSuccess || !p)
-            return fail(MPM_CUDA_ERROR, std::string("cudaGetSymbolAddress(g_metrics_scratch): ") +
-                                            cudaGetErrorString(rc));
-        g_scratch_dev[dev] = static_cast<double*>(p);
-    }
-    *out = g_scratch_dev[dev];
+    void* p = nullptr;
+    rc = cudaGetSymbolAddress(&p, g_metrics_scratch);
+    if (rc != cudaSuccess || !p)
+        return fail(MPM_CUDA_ERROR, std::string("cudaGetSymbolAddress(g_metrics_scratch) on device ") +
+                                        std::to_string(dev) + ": " + cudaGetErrorString(rc));
+    *out = static_cast<double*>(p);
     return MPM_OK;
 }
 

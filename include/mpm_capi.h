@@ -288,8 +288,10 @@ mpm_status mpm_sync_metrics(mpm_handle *h, mpm_metrics *out);
  * n_escaped, n_sorts and n_yielded are 0.
  *   - Scratch is a 1 MiB static device array inside the library; n above
  *     67,108,864 is refused with MPM_CAPACITY.  Nothing has to be zeroed first.
- *   - The first call on a device sets the scratch up there (and loads the
- *     library's kernels on it): make it before any stream capture.
+ *   - Every call looks up the scratch's address in the current context of
+ *     the current device (the first call there also loads the library's
+ *     kernels), so a device reset or another current context is followed.
+ *     The call synchronises its stream: make it outside stream capture.
  *   - Calls on one device must not overlap (two host threads, or two streams
  *     in flight at once): they share the scratch and race.
  *   - stream: a cudaStream_t or NULL (legacy default stream).  Synchronises

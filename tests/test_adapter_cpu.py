@@ -2,7 +2,7 @@
 compiles against the reference's own headers (IPhysicsSolver.h, Types.h,
 Config.h): every `override` matches the reference interface.  A small program
 links it with libmpm_b200.so and runs the calls that need no GPU.  Skipped
-where the reference sources are not present."""
+unless MPM_REFERENCE_SRC names the reference source tree."""
 from __future__ import annotations
 
 import os
@@ -15,12 +15,12 @@ import pytest
 from conftest import ROOT
 from mpm_b200 import capi as A
 
-REF = Path(os.environ.get("MPM_REFERENCE_SRC", "/root/reference"))
+REF = Path(os.environ.get("MPM_REFERENCE_SRC", "") or "/nonexistent")
 ADAPTER = ROOT / "edegpredict-engine-rotary_b200" / "adapter"
 CUDA = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 
 pytestmark = pytest.mark.skipif(not (REF / "include" / "IPhysicsSolver.h").exists() or shutil.which("g++") is None,
-                                reason="reference headers or g++ not available")
+                                reason="MPM_REFERENCE_SRC does not name the reference source tree, or g++ is missing")
 
 MAIN = r"""
 #include <cstdio>

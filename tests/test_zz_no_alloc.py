@@ -81,3 +81,60 @@ def test_noalloc_refuses_counts_above_scratch_limit():
     assert A.lib().mpm_metrics_aos_noalloc(None, None, 0, None, C.byref(m)) == A.MPM_INVALID_ARG
     assert A.lib().mpm_metrics_aos_noalloc(C.byref(p), None, -1, None, C.byref(m)) == A.MPM_INVALID_ARG
     assert A.lib().mpm_metrics_aos_noalloc(C.byref(p), None, 10, None, C.byref(m)) == A.MPM_INVALID_ARG
+
+
+@pytest.mark.gpu
+def test_noalloc_metrics_across_reduction_blocks():
+    """Each reduction block takes 16,384 records; the records of one workpiece
+    repeated six times (36,390 records: two full blocks and a partial third)
+    make the final combine join several partial rows: sums and counts come
+    out six times the handle's, maxima and bounds the same."""
+    import torch
+
+    case, st, n, extf = SCENARIOS["plastic_damage_chip"]()
+    p = W.to_mpm_params(case, precision=A.PREC_F32)
+    s = Solver(p, len(st["x"]) + 64)
+    try:
+        s.set_tool(case["tool"])
+        s.upload(st)
+        s.step(case["dt"], n)
+        count = s.counts()[0]
+        ref = s.metrics()
+        one = torch.empty(count * 504, dtype=torch.uint8, device="cuda")
+        s._check(s._lib.mpm_export_aos(s.h, C.c_void_p(one.data_ptr()), one.numel()))
+        k = 2 * 16384 // count + 1
+        assert count * k > 2 * 16384 and (count * k) % 16384 != 0
+        tiled = one.repeat(k)
+        heat_capacity = p.rho_phys * p.cp * p.particle_volume * count * k
+        scaled = dict(ref)
+        for key in ("mass", "kinetic", "internal_elastic", "thermal", "ref_kinetic", "ref_internal",
+                    "n_active", "n_chip", "n_fixed", "n_inactive"):
+            scaled[key] = ref[key] * k
+        scaled["momentum"] = [v * k for v in ref["momentum"]]
+        scaled["n_escaped"] = scaled["n_sorts"] = scaled["n_yielded"] = 0
+        for _ in range(2):
+            got = metrics_aos_noalloc(p, tiled.data_ptr(), count * k)
+            assert_metrics_match(got, scaled, heat_capacity)
+    finally:
+        s.close()
+
+
+@pytest.mark.gpu
+def test_noalloc_metrics_of_no_particles():
+    """n = 0 (no pointer needed): the same result as a handle holding no
+    particles -- zero sums and counts, the reductions' empty seeds."""
+    case, st, n, extf = SCENARIOS["plastic_damage_chip"]()
+    p = W.to_mpm_params(case, precision=A.PREC_F32)
+    s = Solver(p, 64)
+    try:
+        empty = {k: v[:0] for k, v in st.items()}
+        s.upload(empty)
+        ref = s.metrics()
+    finally:
+        s.close()
+    got = metrics_aos_noalloc(p, 0, 0)
+    for key in SUMS + ("thermal",) + COUNTS:
+        assert got[key] == 0, (key, got[key])
+    assert got["momentum"] == [0.0, 0.0, 0.0]
+    for key in MAXES + COUNTS + SUMS + ("thermal", "momentum", "bounds_min", "bounds_max"):
+        assert got[key] == ref[key], (key, got[key], ref[key])
