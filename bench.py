@@ -168,6 +168,13 @@ def make_case(name: str):
         return W.config1(), "plain small: 64x32x32 cells, dx 0.05 mm, 8 ppc, AISI 4340, cylinder R 0.5 mm"
     if name == "precision":
         return W.config4(), "precision study geometry: 128x64x64 cells, dx 0.02 mm, 8 ppc, Ti-6Al-4V, wedge"
+    if name == "cutting_precision":
+        return W.config4(), ("cutting regime on the precision study geometry: 128x64x64 cells, dx 0.02 mm, 8 ppc, "
+                             "Ti-6Al-4V, wedge at 2.5 m/s, timed after the engagement steps")
+    if name == "cutting":
+        return W.config2(), ("cutting regime on the plain large workload: 256x128x128 cells, dx 0.02 mm, 8 ppc "
+                             "(~33.5M particles), Ti-6Al-4V, rounded wedge at 2.5 m/s, timed after the engagement "
+                             "steps")
     return W.config2(), ("plain large single instance: 256x128x128 cells, dx 0.02 mm, 8 ppc (~33.5M particles), "
                          "Ti-6Al-4V, rounded wedge r_e 0.3 mm at 2.5 m/s, doc 0.05 mm, CFL 0.3")
 
@@ -235,6 +242,12 @@ def run_ours(args):
     m0 = s.metrics()
     n_live = n - m0["n_inactive"]
     dt = case["dt"]
+    engage = args.engage_steps if args.config.startswith("cutting") else 0
+    if engage:
+        # the tool engages and chips form before the timed region (untimed)
+        s.step(dt, engage)
+        m0 = s.metrics()
+        n_live = n - m0["n_inactive"]
     # warm-up (untimed)
     s.step(dt, args.warmup)
     torch.cuda.synchronize(dev)
@@ -274,6 +287,7 @@ def run_ours(args):
         ms_max, live_tot = ms, float(n_live)
     value = live_tot * args.steps / (ms_max / 1e3)
 
+    peak, peak_kind = load_peaks()
     # end to end through the C ABI with host buffers (per replica)
     e2e = run_e2e(s, case, args, n, dev, stream)
     if dist:
@@ -283,7 +297,6 @@ def run_ours(args):
     else:
         e2e_val = float(n_live) * args.steps / e2e["seconds"]
 
-    peak, peak_kind = load_peaks()
     b_alg = B_ALG_BASE + B_ALG_YIELD * f_yield + B_ALG_GRID / box["ppc"]
     avg_launch_s = (k_ms / max(k_n, 1)) / 1e3
     achieved = b_alg * n_live / avg_launch_s / 1e9 if k_n else None
@@ -293,7 +306,13 @@ def run_ours(args):
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu:
-            cpu = cpu_baseline(args.config, args.cpu_seconds)
+            cpu = cpu_baseline("large" if args.config == "cutting" else
+                               ("precision" if args.config == "cutting_precision" else args.config), args.cpu_seconds)
+        variants = None
+        plugin = None
+        if world == 1 and args.config == "large" and not args.no_variants and not args.deterministic:
+            variants = like_for_like(case, args, dev, stream, peak)
+            plugin = plugin_leg(case, args, dev)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -321,12 +340,135 @@ def run_ours(args):
                     "path": e2e["path"]},
             "clocks": clocks,
         }
+        if engage:
+            out["config"]["engagement_steps"] = int(engage)
+            out["config"]["chips"] = int(m1["n_chip"])
+        if variants:
+            out["like_for_like"] = variants
+        if plugin:
+            out["plugin"] = plugin
         if cpu:
             out["cpu_baseline"] = cpu
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return out
+
+
+def like_for_like(case, args, dev, stream, peak) -> dict:
+    """The same workload with the reference's boundary and precision: the
+    rasterised tool (surface samples of the wedge at half a cell, the
+    reference's only grid boundary) in FP32, and in FP64 as the reference
+    kernels compute.  Each line: particle-updates/s of one step call, the
+    fused launch's average time and its fraction of the measured HBM peak
+    (algorithmic bytes doubled in FP64)."""
+    import torch
+    from mpm_b200 import Solver, capi as A, workpiece as W
+    box = case["box"]
+    cap = int(np.prod([box["c1"][i] - box["c0"][i] for i in range(3)]) * box["ppc"])
+    steps = max(10, min(args.steps, 60))
+    out = {}
+    for name, prec in (("raster_f32", A.PREC_F32), ("raster_f64", A.PREC_F64)):
+        rc = dict(case)
+        rc["tool"] = dict(case["tool"], mode=A.TOOL_RASTER)
+        rc["tool"]["samples"] = W.tool_samples(rc)
+        s = Solver(W.to_mpm_params(rc, precision=prec), cap, stream=stream.cuda_stream)
+        try:
+            s.set_tool(rc["tool"])
+            n = s.init_box(box["c0"], box["c1"], box["ppc"], box["seed"], box["instance"], box["fixed_layers"],
+                           box["T0"], tool=case["tool"])
+            n_live = n - s.metrics()["n_inactive"]
+            s.set_tool(rc["tool"])
+            s.step(case["dt"], args.warmup)
+            torch.cuda.synchronize(dev)
+            y0 = s.metrics()["n_yielded"]
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            s.profile(True)
+            s.profile_read()
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                s.step(case["dt"], steps)
+                e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ms = e0.elapsed_time(e1)
+            k_ms, k_n = s.profile_read()
+            s.profile(False)
+            f_yield = (s.metrics()["n_yielded"] - y0) / max(1, n_live * steps)
+        finally:
+            s.close()
+        b_alg = (B_ALG_BASE + B_ALG_YIELD * f_yield + B_ALG_GRID / box["ppc"]) * (2.0 if prec == A.PREC_F64 else 1.0)
+        kms = k_ms / max(k_n, 1)
+        achieved = b_alg * n_live / (kms / 1e3) / 1e9 if k_n else None
+        out[name] = {"value": n_live * steps / (ms / 1e3), "unit": UNIT, "steps": steps,
+                     "ms_per_step": ms / steps, "kernel_ms_avg": kms, "bytes_alg_per_update": b_alg,
+                     "roofline_frac": (achieved / peak) if achieved else None, "samples": len(rc["tool"]["samples"]),
+                     "tool": "raster (wedge surface samples at 0.5 cell)",
+                     "dtype": "f64" if prec == A.PREC_F64 else "f32"}
+    return out
+
+
+def plugin_leg(case, args, dev) -> dict:
+    """The same workload through the drop-in plugin (MPMSolverB200 via
+    adapter/adapter_driver.cpp) in SimulationEngine's call pattern
+    (src/SimulationEngine.cpp:495-536): per macro step setToolPosition,
+    beginInterpolatedToolMotion on the FEM tool's device nodes (the wedge's
+    surface samples at half a cell as FEMNodeGPU records, moving at the tool
+    speed), eight interpolateToolForSubStep + step(dt), endInterpolatedToolMotion
+    and syncMetrics (the metrics read back to the host).  Host-timed over the
+    macro steps: every syncMetrics already waits for the device."""
+    import torch
+    from mpm_b200 import adapter as AD, capi as A, workpiece as W
+    if not AD.available():
+        return {"unavailable": "adapter driver not built (build.py --adapter with MPM_REFERENCE_SRC)"}
+    box, tool = case["box"], case["tool"]
+    cap = int(np.prod([box["c1"][i] - box["c0"][i] for i in range(3)]) * box["ppc"])
+    sub = 8
+    warm_m = max(1, -(-args.warmup // sub))
+    timed_m = max(2, min(8, -(-args.steps // sub)))
+    dt = case["dt"]
+    smp = W.tool_samples(case)
+
+    def pose(t):
+        return [tool["position"][a] + tool["velocity"][a] * t for a in range(3)]
+
+    nodes = [torch.from_numpy(AD.fem_node_records(smp + np.asarray(pose(m * sub * dt)), tool["velocity"]).copy())
+             .to(dev) for m in range(warm_m + timed_m + 1)]
+    ad = AD.Adapter(cap)
+    try:
+        ad.initialize(W.to_mpm_params(case))
+        n = ad.seeded_box(box["c0"], box["c1"], box["ppc"], box["seed"], box["fixed_layers"], box["T0"], tool=tool)
+        n_live = n - int(ad.sync_metrics()[1].n_inactive)
+
+        def macro(m):
+            ad.set_tool_position(pose(m * sub * dt))
+            ad.begin_interp(nodes[m].data_ptr(), len(smp))
+            for k in range(sub):
+                ad.interp_substep(nodes[m + 1].data_ptr(), k / sub)
+                ad.step(dt)
+            ad.end_interp(nodes[m + 1].data_ptr())
+            ad.sync_metrics()
+
+        for m in range(warm_m):
+            macro(m)
+        ad.ok()
+        torch.cuda.synchronize(dev)
+        l0 = ad.launches()
+        t0 = time.perf_counter()
+        for m in range(warm_m, warm_m + timed_m):
+            macro(m)
+        sec = time.perf_counter() - t0
+        ad.ok()
+        launches = ad.launches() - l0
+    finally:
+        ad.close()
+    steps = timed_m * sub
+    return {"value": n_live * steps / sec, "unit": UNIT, "steps": steps, "ms_per_step": sec * 1e3 / steps,
+            "launches_per_macro_step": launches / timed_m, "fem_nodes": len(smp),
+            "d2h_bytes_per_macro_step": ctypes.sizeof(A.MpmMetrics) + 4 * 8,
+            "dtype": "f32", "path": "MPMSolverB200 (IPhysicsSolver / IMetricsProvider drop-in): setToolPosition, "
+                                    "beginInterpolatedToolMotion, 8 x (interpolateToolForSubStep + step), "
+                                    "endInterpolatedToolMotion, syncMetrics"}
 
 
 def run_e2e(s, case, args, n, dev, stream) -> dict:
@@ -698,6 +840,10 @@ def run_reference(args):
         return {"impl": "reference", "unavailable": f"reference kernels not built: {exc}"}
     import torch
     torch.cuda.set_device(0)
+    if args.config == "batched":
+        return run_reference_batched(args, rk)
+    if args.config == "serving":
+        return run_reference_serving(args, rk)
     case, desc = make_case(args.config)
     x, y, z, status = W.generate_box_chunked(case)
     samples = W.tool_samples(case)
@@ -716,6 +862,97 @@ def run_reference(args):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def _ref_line(value, desc, extra, sample):
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": None,
+            "warmup": None, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": dict({"workload": desc}, **extra),
+            "cpu_baseline": {"value": value, "unit": UNIT, "kind": "reference", "cores": 0, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def _ref_instance(rk, case, warmup, steps):
+    """One workpiece alone through the reference kernels (FP64 AoS, a CUDA
+    graph per step as MPMSolver::step, the rasterised tool): device ms of
+    `steps` steps and live particles."""
+    from mpm_b200 import workpiece as W
+    x, y, z, status = W.generate_box_chunked(case)
+    ms, live = rk.bench_positions(case, x, y, z, status, warmup, steps, samples=W.tool_samples(case))
+    return ms, int((status != 1).sum())
+
+
+def run_reference_batched(args, rk):
+    """The config-3 sweep as the reference runs it: one MPMSolver per
+    workpiece, one after another (it has no batched form).  A bounded sample:
+    workpieces in sweep order, 20 timed steps each, until about 60 s of work;
+    value = their particle updates / their summed device time."""
+    from mpm_b200 import workpiece as W
+    cases = W.config3(args.instances, seed=7)
+    steps = min(args.steps, 20)
+    t_start = time.perf_counter()
+    pu, ms_tot, k = 0.0, 0.0, 0
+    for c in cases:
+        ms, live = _ref_instance(rk, c, 2, steps)
+        pu += live * steps
+        ms_tot += ms
+        k += 1
+        if time.perf_counter() - t_start > 60.0:
+            break
+    value = pu / (ms_tot / 1e3)
+    return _ref_line(value, "batched: the config-3 sweep (512 workpieces, cells log-uniform 16^3..64^3, aspect 1-4, "
+                            "4-8 ppc, per-instance Johnson-Cook, speed and depth of cut, rounded-wedge tool), each "
+                            "workpiece alone through the reference kernels, one after another",
+                     {"instances": len(cases), "instances_timed": k, "steps_per_instance": steps},
+                     f"the reference has no CPU implementation of this path; its own CUDA kernels (src/MPMSolver.cu, "
+                     f"FP64 AoS, CUDA graph per step) on the B200: the first {k} workpieces of the sweep, "
+                     f"{steps} timed steps each")
+
+
+def run_reference_serving(args, rk):
+    """The serving workload as the reference would serve it: requests in
+    arrival order (FIFO), one MPMSolver at a time.  Each request's service
+    time is the reference kernels' device time for its steps, measured on
+    min(steps, 50) steps and scaled to its step count; the queue is then
+    played over the window with the same Poisson arrivals as our arm:
+    throughput = particle updates done in the window / the window,
+    latency = completion - arrival of the requests completed in it."""
+    from mpm_b200 import workpiece as W
+    rng = np.random.default_rng(17)
+    n_arr = int(args.rate * args.duration * 1.5) + 16
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, n_arr))
+    arrivals = arrivals[arrivals < args.duration]
+    reqs = []
+    for i in range(len(arrivals)):
+        c = W.config3_case(rng, i, cells_lo=16, cells_hi=96, ppc=8)
+        reqs.append((c, int(rng.integers(200, 2001))))
+    clock, done_pu, lat, k = 0.0, 0.0, [], 0
+    t_start = time.perf_counter()
+    for (c, n), t_arr in zip(reqs, arrivals):
+        if clock >= args.duration or time.perf_counter() - t_start > 120.0:
+            break
+        meas = min(n, 50)
+        ms, live = _ref_instance(rk, c, 2, meas)
+        service = ms / 1e3 * n / meas
+        start = max(clock, t_arr)
+        end = start + service
+        frac = min(1.0, max(0.0, (args.duration - start) / service))
+        done_pu += live * n * frac
+        if end <= args.duration:
+            lat.append(end - t_arr)
+        clock = end
+        k += 1
+    q = (lambda p: float(np.percentile(lat, p))) if lat else (lambda p: None)
+    out = _ref_line(done_pu / args.duration,
+                    f"serving: Poisson arrivals at {args.rate:g} requests/s for {args.duration:g} s, requests of "
+                    "16^3..96^3 cells at 8 ppc, 200-2000 steps, served first come first served by the reference "
+                    "kernels one request at a time",
+                    {"requests_offered": len(reqs), "requests_started": k, "completed_in_window": len(lat)},
+                    "the reference has no CPU implementation of this path; its own CUDA kernels (src/MPMSolver.cu, "
+                    "FP64 AoS, CUDA graph per step) on the B200: each request's service time measured on "
+                    "min(steps, 50) steps and scaled to its steps, played in arrival order over the window")
+    out["latency_s"] = {"p50": q(50), "p99": q(99), "p999": q(99.9), "of": "requests completed in the window"}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -723,7 +960,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="large", choices=["large", "small", "precision", "batched", "serving",
-                                                           "precision_study"])
+                                                           "precision_study", "cutting", "cutting_precision"])
+    ap.add_argument("--engage-steps", type=int, default=1000,
+                    help="cutting configs: untimed steps before the timed region (the tool engages, chips form)")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="large config: skip the like-for-like lines (raster tool FP32, raster tool FP64)")
     ap.add_argument("--instances", type=int, default=512)
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--contact-every", type=int, default=0,

@@ -19,7 +19,9 @@ MPMSolverB200::MPMSolverB200(int maxParticles) : m_maxParticles(maxParticles) {
 }
 
 MPMSolverB200::~MPMSolverB200() {
+    flush();   // the reference would have run the steps it was given
     if (m_deviceMirror) cudaFree(m_deviceMirror);
+    if (m_startNodes) cudaFree(m_startNodes);
     if (m_h) mpm_destroy(m_h);
 }
 
@@ -37,6 +39,7 @@ bool MPMSolverB200::check(mpm_status s) {
 // is taken when the workpiece is created (particle mass and volume depend on
 // its spacing).
 bool MPMSolverB200::initialize(const Config& config) {
+    flush();
     const auto& sph = config.getSPH();
     const auto& mat = config.getMaterial();
     const int precision = m_params.precision;
@@ -79,6 +82,7 @@ bool MPMSolverB200::initialize(const Config& config) {
 
 bool MPMSolverB200::ensureHandle(double spacing) {
     if (!m_initialized) return false;
+    flush();
     if (m_h) {
         mpm_destroy(m_h);
         m_h = nullptr;
@@ -86,6 +90,35 @@ bool MPMSolverB200::ensureHandle(double spacing) {
     m_params.particle_volume = spacing * spacing * spacing;
     m_params.particle_mass = m_density * m_params.particle_volume;
     return check(mpm_create(&m_params, m_maxParticles, nullptr, &m_h));
+}
+
+// The library's own parameters (any grid), for workpieces the reference's
+// initialize cannot express; the inertial density is params.rho_phys.
+bool MPMSolverB200::initializeWithParams(const mpm_params& params) {
+    flush();
+    if (m_h) {
+        mpm_destroy(m_h);
+        m_h = nullptr;
+    }
+    m_numParticles = 0;
+    m_params = params;
+    m_density = params.rho_phys;
+    m_domainMin = Vec3(params.origin[0], params.origin[1], params.origin[2]);
+    m_initialized = check(mpm_create(&m_params, m_maxParticles, nullptr, &m_h));
+    return m_initialized;
+}
+
+bool MPMSolverB200::initializeSeededBox(const int32_t c0[3], const int32_t c1[3], int ppc, uint64_t seed,
+                                        int fixedLayers, double T0, const mpm_tool_desc* removeInside) {
+    flush();
+    if (!m_h) return false;
+    int64_t n = 0;
+    if (!check(mpm_init_box(m_h, c0, c1, ppc, seed, 0, fixedLayers, T0, removeInside))) return false;
+    if (!check(mpm_get_counts(m_h, &n, nullptr, nullptr))) return false;
+    m_numParticles = (int)n;
+    m_time = 0.0;
+    push();
+    return true;
 }
 
 bool MPMSolverB200::uploadLattice(const std::vector<double>& x, const std::vector<double>& y,
@@ -101,6 +134,7 @@ bool MPMSolverB200::uploadLattice(const std::vector<double>& x, const std::vecto
     soa.status = const_cast<int32_t*>(status.data());
     if (!check(mpm_upload(m_h, &soa, n))) return false;
     m_numParticles = (int)n;
+    push();
     return true;
 }
 
@@ -153,93 +187,171 @@ void MPMSolverB200::initializeCylindricalWorkpiece(const Vec3& center, double ra
     m_metrics.bounds_max[2] = center.z;
 }
 
-bool MPMSolverB200::readToolNodes(const FEMNodeGPU* nodes, int n, std::vector<double>& px, std::vector<double>& py,
-                                  std::vector<double>& pz, double vel[3]) {
-    std::vector<FEMNodeGPU> h((size_t)n);
-    cudaError_t e = cudaMemcpy(h.data(), nodes, sizeof(FEMNodeGPU) * (size_t)n, cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) {
-        m_status = MPM_CUDA_ERROR;
-        m_error = std::string("tool nodes: ") + cudaGetErrorString(e);
-        return false;
+// The tool source the next sub-step reads: the blended FEM nodes while a
+// blended motion is on (interpolateToolForSubStep's alpha), else the nodes
+// of setToolNodes (or none).
+MPMSolverB200::ToolSource MPMSolverB200::currentSource() const {
+    ToolSource t;
+    t.end = m_toolNodes;
+    if (m_interpActive && m_startNodes) {
+        t.start = m_startNodes;
+        t.alpha = m_interpAlpha;
     }
-    px.resize((size_t)n); py.resize((size_t)n); pz.resize((size_t)n);
-    vel[0] = vel[1] = vel[2] = 0.0;
-    for (int i = 0; i < n; ++i) {
-        px[i] = h[i].x; py[i] = h[i].y; pz[i] = h[i].z;
-        vel[0] += h[i].vx; vel[1] += h[i].vy; vel[2] += h[i].vz;
-    }
-    if (n > 0) for (int a = 0; a < 3; ++a) vel[a] /= n;
-    return true;
+    return t;
 }
 
-// rasterizeToolKernel + applyGridCollisionKernel (src/MPMSolver.cu:444-492):
-// the tool nodes as raster samples about the tool tip; the grid takes the
-// tool's mean node velocity (equal to every node's for a translating tool).
-bool MPMSolverB200::pushToolSamples(const std::vector<double>& px, const std::vector<double>& py,
-                                    const std::vector<double>& pz, const double vel[3]) {
-    const size_t n = px.size();
-    std::vector<double> ox(n), oy(n), oz(n);
-    for (size_t i = 0; i < n; ++i) {
-        ox[i] = px[i] - m_toolPosition.x;
-        oy[i] = py[i] - m_toolPosition.y;
-        oz[i] = pz[i] - m_toolPosition.z;
-    }
-    mpm_tool_desc t{};
-    t.mode = MPM_TOOL_RASTER;
-    t.shape = MPM_SHAPE_CYLINDER_Y;
-    t.position[0] = m_toolPosition.x; t.position[1] = m_toolPosition.y; t.position[2] = m_toolPosition.z;
-    t.velocity[0] = vel[0]; t.velocity[1] = vel[1]; t.velocity[2] = vel[2];
-    t.tip_dz = 0.0;
-    t.n_samples = (int32_t)n;
-    t.sample_dx = ox.data(); t.sample_dy = oy.data(); t.sample_dz = oz.data();
-    return check(mpm_set_tool(m_h, &t));
-}
-
+// rasterizeToolKernel + applyGridCollisionKernel (src/MPMSolver.cu:444-492)
+// read the FEM tool's device nodes on every step: the library does the same
+// from the node records (mpm_set_tool_nodes), with no host copy.
 void MPMSolverB200::setToolNodes(FEMNodeGPU* nodes, int numNodes) {
+    flush();
     m_toolNodes = nodes;
     m_numToolNodes = numNodes;
 }
 
 // beginInterpolatedToolMotion / interpolateToolForSubStep /
-// endInterpolatedToolMotion (include/MPMSolver.cuh:91-110): positions blend
-// linearly between the snapshot and the current FEM nodes over a macro step.
+// endInterpolatedToolMotion (src/MPMSolver.cu:976-1000): the nodes of each
+// sub-step blend linearly from a snapshot taken here (a device-to-device
+// copy, as the reference takes it) to the current FEM nodes; the blend itself
+// runs on the device inside the raster launch of every step.
 void MPMSolverB200::beginInterpolatedToolMotion(FEMNodeGPU* femNodes, int numNodes) {
-    double v[3];
-    m_interpActive = readToolNodes(femNodes, numNodes, m_interpStart[0], m_interpStart[1], m_interpStart[2], v);
+    flush();
+    const size_t bytes = sizeof(FEMNodeGPU) * (size_t)std::max(numNodes, 0);
+    if (bytes > m_startNodesBytes) {
+        if (m_startNodes) cudaFree(m_startNodes);
+        m_startNodes = nullptr;
+        m_startNodesBytes = 0;
+        if (cudaMalloc(&m_startNodes, bytes) != cudaSuccess) {
+            m_status = MPM_OOM;
+            m_error = "tool node snapshot: out of memory";
+            m_interpActive = false;
+            return;
+        }
+        m_startNodesBytes = bytes;
+    }
+    cudaStream_t st = getComputeStream();
+    cudaError_t e = bytes ? cudaMemcpyAsync(m_startNodes, femNodes, bytes, cudaMemcpyDeviceToDevice, st)
+                          : cudaSuccess;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        m_status = MPM_CUDA_ERROR;
+        m_error = std::string("tool node snapshot: ") + cudaGetErrorString(e);
+        m_interpActive = false;
+        return;
+    }
     m_toolNodes = femNodes;
     m_numToolNodes = numNodes;
+    m_interpActive = true;
+    m_interpAlpha = 0.0;
 }
 
 void MPMSolverB200::interpolateToolForSubStep(FEMNodeGPU* femNodes, double alpha) {
+    // part of the sub-step sequence: no flush unless the node array changes
+    if (femNodes != m_toolNodes) flush();
     m_toolNodes = femNodes;
-    m_interpAlpha = std::min(std::max(alpha, 0.0), 1.0);
+    m_interpAlpha = alpha;
 }
 
 void MPMSolverB200::endInterpolatedToolMotion(FEMNodeGPU* femNodes) {
+    flush();
     m_toolNodes = femNodes;
     m_interpActive = false;
-    m_interpAlpha = 1.0;
+    m_interpAlpha = 0.0;
 }
 
 // MPMSolver::step (src/MPMSolver.cu:1062-1168): one step of dt; nothing
-// before a workpiece exists.
+// before a workpiece exists.  Queued: a sub-step joins the queue when it has
+// the queue's dt and its tool source continues the queue's (the same node
+// arrays, and a blend weight one per-step increment further); otherwise the
+// queue runs first.
 void MPMSolverB200::step(double dt) {
     if (!m_initialized || !m_h || m_numParticles == 0) return;
-    if (m_toolNodes && m_numToolNodes > 0) {
-        std::vector<double> px, py, pz;
-        double vel[3];
-        if (!readToolNodes(m_toolNodes, m_numToolNodes, px, py, pz, vel)) return;
-        if (m_interpActive && m_interpStart[0].size() == px.size()) {
-            const double a = m_interpAlpha;
-            for (size_t i = 0; i < px.size(); ++i) {
-                px[i] = m_interpStart[0][i] + a * (px[i] - m_interpStart[0][i]);
-                py[i] = m_interpStart[1][i] + a * (py[i] - m_interpStart[1][i]);
-                pz[i] = m_interpStart[2][i] + a * (pz[i] - m_interpStart[2][i]);
-            }
+    const ToolSource t = currentSource();
+    if (m_pendingSteps > 0) {
+        bool join = dt == m_pendingDt && t.start == m_runSource.start && t.end == m_runSource.end;
+        if (join && t.start) {
+            const double want = m_pendingSteps == 1 ? t.alpha
+                                                    : m_runSource.alpha + m_pendingSteps * m_runDalpha;
+            join = std::fabs(t.alpha - want) <= 1e-12 * std::max(1.0, std::fabs(want));
+            if (join && m_pendingSteps == 1) m_runDalpha = t.alpha - m_runSource.alpha;
         }
-        if (!pushToolSamples(px, py, pz, vel)) return;
+        if (!join || m_pendingSteps >= kMaxQueuedSteps) flush();
     }
-    if (check(mpm_step(m_h, dt, 1))) m_time += dt;
+    if (m_pendingSteps == 0) {
+        m_pendingDt = dt;
+        m_runSource = t;
+        m_runDalpha = 0.0;
+    }
+    ++m_pendingSteps;
+    m_time += dt;
+}
+
+// The queued sub-steps as one library call: the tool pose (chip separation
+// and LOD read its tip, src/MPMSolver.cu:1160-1162), the node source of the
+// first queued sub-step with the per-step blend increment, then the steps.
+bool MPMSolverB200::runQueue() {
+    const int n = m_pendingSteps;
+    m_pendingSteps = 0;
+    mpm_tool_desc t{};
+    t.mode = m_runSource.end ? MPM_TOOL_RASTER : MPM_TOOL_NONE;
+    t.shape = MPM_SHAPE_CYLINDER_Y;
+    t.position[0] = m_toolPosition.x; t.position[1] = m_toolPosition.y; t.position[2] = m_toolPosition.z;
+    if (!check(mpm_set_tool(m_h, &t))) return false;
+    if (m_runSource.end) {
+        mpm_tool_nodes tn{};
+        tn.start = m_runSource.start;
+        tn.end = m_runSource.end;
+        tn.n = m_numToolNodes;
+        tn.stride = (int32_t)sizeof(FEMNodeGPU);
+        tn.off_pos[0] = (int32_t)offsetof(FEMNodeGPU, x);
+        tn.off_pos[1] = (int32_t)offsetof(FEMNodeGPU, y);
+        tn.off_pos[2] = (int32_t)offsetof(FEMNodeGPU, z);
+        tn.off_vel[0] = (int32_t)offsetof(FEMNodeGPU, vx);
+        tn.off_vel[1] = (int32_t)offsetof(FEMNodeGPU, vy);
+        tn.off_vel[2] = (int32_t)offsetof(FEMNodeGPU, vz);
+        tn.alpha0 = m_runSource.alpha;
+        tn.dalpha = m_runDalpha;
+        if (!check(mpm_set_tool_nodes(m_h, &tn))) return false;
+    }
+    return check(mpm_step(m_h, m_pendingDt, n));
+}
+
+void MPMSolverB200::flush() {
+    if (m_pendingSteps == 0 || !m_h) {
+        m_pendingSteps = 0;
+        return;
+    }
+    pull();
+    runQueue();
+    push();
+}
+
+// The live mirror: writes of the reference's consumers come in before a step
+// or a read (pull), the state goes out after steps (push).
+void MPMSolverB200::pull() {
+    if (!m_mirrorLive || !m_h || !m_deviceMirror || m_numParticles == 0) return;
+    check(mpm_import_aos(m_h, m_deviceMirror, (int64_t)m_deviceMirrorBytes, MPM_AOS_WRITABLE));
+}
+
+void MPMSolverB200::push() {
+    if (!m_mirrorLive || !m_h || m_numParticles == 0 || !ensureMirror()) return;
+    check(mpm_export_aos(m_h, m_deviceMirror, (int64_t)((size_t)m_numParticles * sizeof(MPMParticle))));
+}
+
+bool MPMSolverB200::ensureMirror() {
+    const size_t bytes = (size_t)m_numParticles * sizeof(MPMParticle);
+    if (bytes <= m_deviceMirrorBytes && m_deviceMirror) return true;
+    if (m_deviceMirror) cudaFree(m_deviceMirror);
+    m_deviceMirror = nullptr;
+    m_deviceMirrorBytes = 0;
+    if (cudaMalloc(&m_deviceMirror, bytes) != cudaSuccess) {
+        m_status = MPM_OOM;
+        m_error = "device particle mirror: out of memory";
+        m_mirrorLive = false;
+        return false;
+    }
+    m_deviceMirrorBytes = bytes;
+    return true;
 }
 
 // getStableTimeStep (src/MPMSolver.cu:1170-1178): CFL * dx / max(c, 1) with
@@ -258,6 +370,7 @@ double MPMSolverB200::getHighestFrequency() const {
 }
 
 void MPMSolverB200::reset() {
+    flush();
     m_time = 0.0;
     if (m_h) check(mpm_reset_clock(m_h));
 }
@@ -271,6 +384,8 @@ void MPMSolverB200::getBounds(double& minX, double& minY, double& minZ, double& 
 // syncMetrics (src/MPMSolver.cu:1239-1259) and the cached bounds.
 void MPMSolverB200::syncMetrics() {
     if (!m_h || m_numParticles == 0) return;
+    flush();
+    pull();
     mpm_metrics m{};
     const mpm_status s = mpm_sync_metrics(m_h, &m);
     if (s == MPM_NUMERIC) {
@@ -309,10 +424,14 @@ double MPMSolverB200::getTemperatureAt(double x, double y, double z) const {
 // setParticleTemperatures (src/MPMSolver.cu:1267-1277): count <= particles.
 void MPMSolverB200::setParticleTemperatures(const double* temperatures, int count) {
     if (!m_h || !temperatures || count <= 0 || count > m_numParticles) return;
-    check(mpm_set_temperatures(m_h, temperatures, count));
+    flush();
+    pull();
+    if (check(mpm_set_temperatures(m_h, temperatures, count))) push();
 }
 
 std::vector<MPMParticle> MPMSolverB200::getParticles() {
+    flush();
+    pull();
     m_hostParticles.assign((size_t)m_numParticles, MPMParticle());
     if (m_h && m_numParticles > 0 &&
         !check(mpm_export_aos(m_h, m_hostParticles.data(), (int64_t)m_hostParticles.size() * 504)))
@@ -320,25 +439,23 @@ std::vector<MPMParticle> MPMSolverB200::getParticles() {
     return m_hostParticles;
 }
 
+// The reference hands out its own particle array (include/MPMSolver.cuh:
+// 143, used by ContactSolver at src/ContactSolver.cu:1131 and by CFD chip
+// coupling at src/SimulationEngine.cpp:1012): here the live mirror.
 MPMParticle* MPMSolverB200::getDeviceParticles() {
     if (!m_h || m_numParticles == 0) return nullptr;
-    const size_t bytes = (size_t)m_numParticles * sizeof(MPMParticle);
-    if (bytes > m_deviceMirrorBytes) {
-        if (m_deviceMirror) cudaFree(m_deviceMirror);
-        m_deviceMirror = nullptr;
-        m_deviceMirrorBytes = 0;
-        if (cudaMalloc(&m_deviceMirror, bytes) != cudaSuccess) {
-            m_status = MPM_OOM;
-            m_error = "device particle mirror: out of memory";
-            return nullptr;
-        }
-        m_deviceMirrorBytes = bytes;
-    }
-    if (!check(mpm_export_aos(m_h, m_deviceMirror, (int64_t)bytes))) return nullptr;
+    flush();
+    pull();   // writes since the last export, when the mirror is already out
+    if (!ensureMirror()) return nullptr;
+    m_mirrorLive = true;
+    if (!check(mpm_export_aos(m_h, m_deviceMirror, (int64_t)((size_t)m_numParticles * sizeof(MPMParticle)))))
+        return nullptr;
     return m_deviceMirror;
 }
 
+// The handle's stream, after the queued sub-steps are issued on it.
 cudaStream_t MPMSolverB200::getComputeStream() const {
+    const_cast<MPMSolverB200*>(this)->flush();
     void* s = nullptr;
     if (m_h) mpm_get_stream(m_h, &s);
     return static_cast<cudaStream_t>(s);
@@ -346,6 +463,7 @@ cudaStream_t MPMSolverB200::getComputeStream() const {
 
 void MPMSolverB200::applyExternalForce(const Vec3& center, double radius, const Vec3& force) {
     if (!m_h) return;
+    flush();
     const double c[3] = {center.x, center.y, center.z}, f[3] = {force.x, force.y, force.z};
     check(mpm_apply_external_force(m_h, c, radius, f));
 }
@@ -354,6 +472,7 @@ void MPMSolverB200::applyExternalForce(const Vec3& center, double radius, const 
 // max(physical * factor, physical); thermal terms keep the physical density.
 void MPMSolverB200::setDynamicMassScaling(double factor) {
     if (!(factor > 0.0)) return;
+    flush();
     m_density = std::max(m_params.rho_phys * factor, m_params.rho_phys);
     if (m_h) check(mpm_set_mass_scaling(m_h, factor));
 }

@@ -9,6 +9,24 @@
 // and meanings.  Where the reference returns void/bool and swallows errors,
 // so does this class; the last C-ABI status and message are kept
 // (lastStatus(), lastError()).
+//
+// Sub-stepping.  SimulationEngine calls step(microDt) once per sub-step with
+// only interpolateToolForSubStep between the calls (src/SimulationEngine.cpp:
+// 515-524).  step() queues the sub-step; the queue runs as ONE multi-step
+// call of the library (one fused launch per step, replayable from a CUDA
+// graph) at the next call of any other member, or when dt or the tool
+// source changes.  The FEM tool nodes are rasterised on the device from
+// their own device records with the sub-step blend done there
+// (mpm_set_tool_nodes): no host copy of the nodes and no synchronisation per
+// sub-step.  getComputeStream() runs the queue first, so work that the
+// caller orders after it on that stream sees every step.
+//
+// The device mirror.  getDeviceParticles() hands out an MPMParticle array,
+// as the reference hands out its own d_particles, which ContactSolver and CFD
+// chip coupling write in place.  Once handed out it stays live: before every
+// step and every read the writes in it are imported (mpm_import_aos:
+// positions, velocities, temperatures, statuses and ext_f), and after every
+// batch of steps it is exported again.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -64,8 +82,10 @@ public:
     void initializeCylindricalWorkpiece(const Vec3& center, double radius, double length, double spacing,
                                         int axis = 2);
     std::vector<MPMParticle> getParticles();
-    // Device copy of the particles in the MPMParticle layout, refreshed on
-    // every call (read-only: writes to it do not reach the solver).
+    // The particles in the MPMParticle layout in device memory, writable in
+    // place: writes reach the solver before its next step or read (positions,
+    // velocities, temperatures, statuses, ext_f).  The pointer stays valid
+    // until a larger workpiece is initialised.
     MPMParticle* getDeviceParticles();
     cudaStream_t getComputeStream() const;
     const Vec3& getDomainMin() const { return m_domainMin; }
@@ -95,19 +115,41 @@ public:
     // Arithmetic of the bulk state: MPM_PREC_F32 (default) or MPM_PREC_F64.
     // Takes effect at the next workpiece initialisation.
     void setPrecision(int precision) { m_params.precision = precision; }
+    // A workpiece on a grid the reference's initialize(Config) cannot express
+    // (its domain is the 0.2 m cube with dx >= 0.5 mm, src/MPMSolver.cu:
+    // 840-846): the library's parameters as given, then a seeded box of
+    // cells [c0, c1) with ppc particles per cell (mpm_init_box), leaving out
+    // the candidates inside removeInside's analytic shape when it is given.
+    bool initializeWithParams(const mpm_params& params);
+    bool initializeSeededBox(const int32_t c0[3], const int32_t c1[3], int ppc, uint64_t seed, int fixedLayers,
+                             double T0, const mpm_tool_desc* removeInside = nullptr);
+    // Runs the queued sub-steps now (every other member does this first).
+    void flush();
+    int pendingSteps() const { return m_pendingSteps; }
+    mpm_handle* handle() { return m_h; }
     const mpm_metrics& getMetrics() const { return m_metrics; }
     mpm_status lastStatus() const { return m_status; }
     std::string lastError() const { return m_error; }
 
 private:
+    // The tool source of one sub-step: FEM records end (blended from start by
+    // alpha when start is set).
+    struct ToolSource {
+        const FEMNodeGPU* start = nullptr;
+        const FEMNodeGPU* end = nullptr;
+        double alpha = 0.0;
+    };
     bool check(mpm_status s);
     bool ensureHandle(double spacing);
     bool uploadLattice(const std::vector<double>& x, const std::vector<double>& y, const std::vector<double>& z,
                        const std::vector<int32_t>& status);
-    bool pushToolSamples(const std::vector<double>& px, const std::vector<double>& py,
-                         const std::vector<double>& pz, const double vel[3]);
-    bool readToolNodes(const FEMNodeGPU* nodes, int n, std::vector<double>& px, std::vector<double>& py,
-                       std::vector<double>& pz, double vel[3]);
+    ToolSource currentSource() const;
+    bool runQueue();
+    void pull();
+    void push();
+    bool ensureMirror();
+    // A queue longer than this runs without waiting for an observation.
+    static constexpr int kMaxQueuedSteps = 64;
 
     mpm_params m_params{};
     mpm_handle* m_h = nullptr;
@@ -119,15 +161,23 @@ private:
     double m_density = 7850.0;       // inertial density (physical x mass scaling)
     Vec3 m_domainMin;
     Vec3 m_toolPosition;
-    FEMNodeGPU* m_toolNodes = nullptr;
+    FEMNodeGPU* m_toolNodes = nullptr;       // the nodes a step reads (setToolNodes / the blend's end)
     int m_numToolNodes = 0;
-    std::vector<double> m_interpStart[3];
+    FEMNodeGPU* m_startNodes = nullptr;      // the blend's start snapshot (device, owned)
+    size_t m_startNodesBytes = 0;
     bool m_interpActive = false;
-    double m_interpAlpha = 1.0;
+    double m_interpAlpha = 0.0;
+    // queued sub-steps: count, their dt, the first one's tool source and the
+    // blend weight added per sub-step
+    int m_pendingSteps = 0;
+    double m_pendingDt = 0.0;
+    ToolSource m_runSource;
+    double m_runDalpha = 0.0;
     mpm_metrics m_metrics{};
     std::vector<MPMParticle> m_hostParticles;
     MPMParticle* m_deviceMirror = nullptr;
     size_t m_deviceMirrorBytes = 0;
+    bool m_mirrorLive = false;
     mpm_status m_status = MPM_OK;
     std::string m_error;
 };

@@ -210,39 +210,35 @@ __global__ void k_bin_count(const Inst<R>* insts, int n_inst, PState<R> ps, cons
     rank[pi] = atomicAdd(&count[kk], 1);
 }
 
-__device__ __forceinline__ int gcd_i(int a, int b) {
-    while (b) {
-        const int t = a % b;
-        a = b;
-        b = t;
+// Position in its bin of the particle of cell c (0..63) with rank r among
+// that cell's particles; cs points at the bin's 65 cell offsets in the new
+// layout (cell q holds cs[q+1] - cs[q] particles, n = cs[64] - cs[0]).
+// The bin is a table of 64 columns, column c for cell c: with R = n / 64
+// full rows, particle (c, r < R) sits at r*64 + c.  The particles of cells
+// holding more than R (the overflow, in cell then rank order) fill first
+// the holes the smaller cells leave in the full rows (row m..R-1 of a cell
+// with m < R particles, in cell then row order), then the tail [64R, n).
+// A warp of the step kernel takes 32 consecutive positions: mostly 32
+// distinct cells of one half of the bin (x, y and two z layers), which is
+// what makes its velocity-tile gathers and node-tile adds conflict-free,
+// and a 256-particle pass holds at most four particles of a cell outside
+// the overflow.
+__device__ __forceinline__ int64_t column_slot(const int32_t* __restrict__ cs, int c, int r) {
+    const int n = cs[kCellsPerBin] - cs[0];
+    const int R = n / kCellsPerBin;
+    if (r < R) return (int64_t)r * kCellsPerBin + c;
+    int k = r - R;   // k-th overflow particle of the bin
+    for (int q = 0; q < c; ++q) {
+        const int m = cs[q + 1] - cs[q];
+        if (m > R) k += m - R;
     }
-    return a;
-}
-
-// x with (s * x) mod n == 1, for gcd(s, n) == 1 (extended Euclid).
-__device__ __forceinline__ int64_t inv_mod(int64_t s, int64_t n) {
-    int64_t t = 0, nt = 1, r = n, nr = s % n;
-    while (nr != 0) {
-        const int64_t q = r / nr;
-        int64_t tmp = t - q * nt;
-        t = nt;
-        nt = tmp;
-        tmp = r - q * nr;
-        r = nr;
-        nr = tmp;
+    for (int q = 0; q < kCellsPerBin; ++q) {
+        const int m = cs[q + 1] - cs[q];
+        const int holes = m < R ? R - m : 0;
+        if (k < holes) return (int64_t)(m + k) * kCellsPerBin + q;
+        k -= holes;
     }
-    return t < 0 ? t + n : t;
-}
-
-// Position in the bin of the particle of (cell-major) rank r among n: the
-// bin is laid out so that position p holds rank (p * s) mod n, s coprime to n
-// and about n/8 (a cell holds ~8 of a bin's ~512 particles).  Consecutive
-// positions -- the lanes of a warp -- then hold particles ~8 cells apart.
-__device__ __forceinline__ int64_t in_bin_slot(int r, int n) {
-    if (n <= 2) return r;
-    int s = (n >> 3) | 1;
-    while (gcd_i(s, n) != 1) s += 2;
-    return ((int64_t)r * inv_mod(s, n)) % n;
+    return (int64_t)R * kCellsPerBin + k;
 }
 
 // Destination slot of source slot pi in the new layout (-1: an unused slot).
@@ -255,10 +251,9 @@ __device__ __forceinline__ int64_t bin_dest(const Inst<R>& P, int ii, int64_t pi
     if (kk - key_base[ii] >= P.nbins * kCellsPerBin) return offset[kk] + rank[pi];  // INACTIVE: after the bins
     const int32_t fk = key_base[ii] + newbin[pi] * kCellsPerBin;
     const int64_t b0 = offset[fk];
-    const int n = offset[fk + kCellsPerBin] - (int)b0;
-    const int r = (int)(offset[kk] - b0) + rank[pi];
     // deterministic mode keeps each cell's particles together, in rank order
-    return b0 + (det ? (int64_t)r : in_bin_slot(r, n));
+    if (det) return b0 + (int64_t)(offset[kk] - b0) + rank[pi];
+    return b0 + column_slot(offset + fk, kk - fk, rank[pi]);
 }
 
 // The re-bin's move, in two launches so that the writes are coalesced: the
@@ -439,24 +434,59 @@ template void launch_pad_counts<double>(const Inst<double>*, int, const int32_t*
 
 // rasterizeToolKernel (reference src/MPMSolver.cu:444-473): each tool sample
 // marks the 2x2x2 nodes from round((x - min)/dx).
-__global__ void k_raster(const double* sx, const double* sy, const double* sz, int ns, double px, double py,
-                         double pz, double ox, double oy, double oz, double inv_dx, int nx, int ny, int nz,
-                         uint8_t* mask) {
+// The raster tool of instance i at step k of the current call, restating
+// rasterizeToolKernel (src/MPMSolver.cu:444-473): each point marks the 2x2x2
+// grid nodes from g = round((p - origin) / dx).  The pose comes from the
+// instance record (time t0 + k dt, as the step kernel computes it), so the
+// launch has the same arguments in every call and replays from a CUDA graph.
+// Samples: p = pose + offset, mark 1.  FEM nodes: p = start + a (end -
+// start) with the blend weight a of this step (fused multiply-add, as the
+// reference's compiled blend kernel, src/MPMSolver.cu:494-504, rounds it), or
+// end when there is no blend; the mark is the node's index + 1, the highest
+// winning, so a marked grid node's velocity is one node's, whatever the
+// thread order.
+template <typename R>
+__global__ void k_raster(const Inst<R>* __restrict__ insts, int i, int k) {
+    const Inst<R>& P = insts[i];
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ns) return;
-    const int gx = (int)round(((px + sx[t]) - ox) * inv_dx);
-    const int gy = (int)round(((py + sy[t]) - oy) * inv_dx);
-    const int gz = (int)round(((pz + sz[t]) - oz) * inv_dx);
+    double p[3];
+    int32_t mark;
+    if (P.tn_end) {
+        if (t >= P.tn_n) return;
+        const unsigned char* e = P.tn_end + (int64_t)t * P.tn_stride;
+        for (int a = 0; a < 3; ++a) p[a] = *reinterpret_cast<const double*>(e + P.tn_off[a]);
+        if (P.tn_start) {
+            const unsigned char* s0 = P.tn_start + (int64_t)t * P.tn_stride;
+            const double al = P.tn_a0 + (double)(P.step0 + k - P.tn_step0) * P.tn_da;
+            for (int a = 0; a < 3; ++a) {
+                const double q0 = *reinterpret_cast<const double*>(s0 + P.tn_off[a]);
+                p[a] = fma(al, p[a] - q0, q0);
+            }
+        }
+        mark = t + 1;
+    } else {
+        if (t >= P.n_samples) return;
+        const double tk = da(P.t0, dm((double)k, P.dt));
+        for (int a = 0; a < 3; ++a)
+            p[a] = da(da(P.tool_p0[a], dm(P.tool_v[a], ds(tk, P.tool_t0))), P.samples[a * P.n_samples + t]);
+        mark = 1;
+    }
+    const double inv_dx = 1.0 / P.dx;
+    const int gx = (int)round(ds(p[0], P.ox) * inv_dx);
+    const int gy = (int)round(ds(p[1], P.oy) * inv_dx);
+    const int gz = (int)round(ds(p[2], P.oz) * inv_dx);
     for (int a = 0; a < 2; ++a) {
         const int cx = gx + a;
-        if (cx < 0 || cx >= nx) continue;
+        if (cx < 0 || cx >= P.nx) continue;
         for (int b = 0; b < 2; ++b) {
             const int cy = gy + b;
-            if (cy < 0 || cy >= ny) continue;
+            if (cy < 0 || cy >= P.ny) continue;
             for (int c = 0; c < 2; ++c) {
                 const int cz = gz + c;
-                if (cz < 0 || cz >= nz) continue;
-                mask[cx + (int64_t)nx * (cy + (int64_t)ny * cz)] = 1;
+                if (cz < 0 || cz >= P.nz) continue;
+                int32_t* m = &P.tool_mask[cx + (int64_t)P.nx * (cy + (int64_t)P.ny * cz)];
+                if (mark == 1) *m = 1;
+                else atomicMax(m, mark);
             }
         }
     }
@@ -709,6 +739,64 @@ __global__ void k_export_aos(const Inst<R>* inst, PState<R> ps, int64_t pbase, i
 //  0 mass 1-3 momentum 4 kinetic 5 elastic 6 thermal 7 max dT 8 max vm 9 max eps
 //  10 sum eps 11 ref max stress 12 ref max T 13 ref kinetic 14 ref internal
 //  15 n active 16 n chip 17 n fixed 18 n inactive 19-21 bmin 22-24 bmax
+// The way back from k_export_aos for the fields the reference's consumers of
+// the particle array write in place (ContactSolver: x, v, T; CFD coupling:
+// ext_f, T).  Slot pi reads record orig[pi] (upload order, as exported).  A
+// position or temperature equal to what the export writes now is left as it
+// is, so an unmodified array imports bit for bit; a moved particle is
+// re-expressed in its current bin (hi + lo in FP32 state) and flags[0] asks
+// the host to re-bin.  The external force goes to pext in upload order (the
+// next step's first P2G reads it there, whatever the re-bin does).  A status
+// outside 0..4 is left as it was and counted in flags[1].
+template <typename R>
+__global__ void k_import_aos(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64_t n, double Tamb, uint32_t fields,
+                             const AosParticle* __restrict__ in, V4<R>* __restrict__ pext, int* __restrict__ flags) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const Inst<R>& P = *inst;
+    const int64_t pi = pbase + s;
+    const int32_t o = ps.orig[pi];
+    const AosParticle& q = in[o];
+    if (fields & MPM_AOS_POSITION) {
+        const V4<R> a0 = ps.A[0][pi];
+        double xw[3];
+        world_pos(P, ps, pi, a0, xw);
+        const double nw[3] = {q.x, q.y, q.z};
+        if (nw[0] != xw[0] || nw[1] != xw[1] || nw[2] != xw[2]) {
+            const int bin = ps.bin[pi];
+            const int bo[3] = {(bin % P.nbx) * kBin, ((bin / P.nbx) % P.nby) * kBin, (bin / (P.nbx * P.nby)) * kBin};
+            const double org[3] = {P.ox, P.oy, P.oz};
+            double l[3];
+            R hi[3];
+            for (int a = 0; a < 3; ++a) {
+                l[a] = (nw[a] - org[a]) / P.dx - (double)bo[a];
+                hi[a] = (R)l[a];
+            }
+            ps.A[0][pi] = mk4<R>(hi[0], hi[1], hi[2], a0.w);
+            if (ps.X) ps.X[pi] = mk4<R>((R)(l[0] - (double)hi[0]), (R)(l[1] - (double)hi[1]), (R)(l[2] - (double)hi[2]),
+                                        R(0));
+            flags[0] = 1;
+        }
+    }
+    if (fields & MPM_AOS_VELOCITY) {
+        const V4<R> b0 = ps.B[0][pi];
+        ps.B[0][pi] = mk4<R>((R)q.vx, (R)q.vy, (R)q.vz, b0.w);
+    }
+    if (fields & MPM_AOS_TEMPERATURE) {
+        V4<R> a3 = ps.A[3][pi];
+        if (q.temperature != Tamb + (double)a3.z) {
+            a3.z = (R)(q.temperature - Tamb);
+            ps.A[3][pi] = a3;
+        }
+    }
+    if (fields & MPM_AOS_STATUS) {
+        const int32_t st = q.status;
+        if (st >= (int32_t)ST_ACTIVE && st <= (int32_t)ST_FIXED) ps.status[pi] = (uint8_t)st;
+        else atomicAdd(&flags[1], 1);
+    }
+    if (fields & MPM_AOS_EXT_FORCE) pext[pbase + o] = mk4<R>((R)q.ext_fx, (R)q.ext_fy, (R)q.ext_fz, R(0));
+}
+
 template <typename R>
 __global__ void k_stats(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64_t n, double mu, double K, double rho,
                         double cp, double Tamb, double* partial) {
@@ -843,10 +931,10 @@ void launch_bin_scatter(const PState<R>& src, const PState<R>& dst, const Inst<R
     launch_counter() += 2;
 }
 
-void launch_raster(const double* sx, const double* sy, const double* sz, int ns, double px, double py, double pz,
-                   double ox, double oy, double oz, double dx, int nx, int ny, int nz, uint8_t* mask, cudaStream_t st) {
-    if (ns <= 0) return;
-    k_raster<<<(ns + kT - 1) / kT, kT, 0, st>>>(sx, sy, sz, ns, px, py, pz, ox, oy, oz, 1.0 / dx, nx, ny, nz, mask);
+template <typename R>
+void launch_raster(const Inst<R>* insts, int i, int k, int npoints, cudaStream_t st) {
+    if (npoints <= 0) return;
+    k_raster<R><<<(npoints + kT - 1) / kT, kT, 0, st>>>(insts, i, k);
     ++launch_counter();
 }
 
@@ -887,6 +975,16 @@ void launch_export_aos(const Inst<R>* inst_dev, const PState<R>& ps, int64_t pba
                        double rho, void* out, cudaStream_t st) {
     if (n <= 0) return;
     k_export_aos<R><<<(int)((n + kT - 1) / kT), kT, 0, st>>>(inst_dev, ps, pbase, n, Tamb, rho, (AosParticle*)out);
+    ++launch_counter();
+}
+
+template <typename R>
+void launch_import_aos(const Inst<R>* inst_dev, const PState<R>& ps, int64_t pbase, int64_t n, double Tamb,
+                       uint32_t fields, const void* in, V4<R>* pext, int* flags, cudaStream_t st) {
+    if (n <= 0) return;
+    Range nvtx_range("mpm.import_aos");
+    k_import_aos<R><<<(int)((n + kT - 1) / kT), kT, 0, st>>>(inst_dev, ps, pbase, n, Tamb, fields,
+                                                             (const AosParticle*)in, pext, flags);
     ++launch_counter();
 }
 
@@ -1019,11 +1117,14 @@ void launch_heat_diffuse(const Inst<R>* insts, int n_inst, int b, int64_t total,
                                    cudaStream_t);                                                                    \
     template void launch_export_aos<R>(const Inst<R>*, const PState<R>&, int64_t, int64_t, double, double, void*,    \
                                        cudaStream_t);                                                                \
+    template void launch_import_aos<R>(const Inst<R>*, const PState<R>&, int64_t, int64_t, double, uint32_t,         \
+                                       const void*, V4<R>*, int*, cudaStream_t);                                     \
     template void launch_stats<R>(const Inst<R>*, const PState<R>&, int64_t, int64_t, double, double, double, double, \
                                   double, double*, int, double*, cudaStream_t);                                      \
     template void launch_set_temps<R>(const PState<R>&, int64_t, int64_t, const double*, int64_t, double, cudaStream_t); \
     template void launch_relayout<R>(const PState<R>&, const PState<R>&, const RelayoutMap*, int, int64_t, cudaStream_t); \
-    template void launch_heat_diffuse<R>(const Inst<R>*, int, int, int64_t, cudaStream_t);
+    template void launch_heat_diffuse<R>(const Inst<R>*, int, int, int64_t, cudaStream_t);                      \
+    template void launch_raster<R>(const Inst<R>*, int, int, int, cudaStream_t);
 
 MPMB_INST(float)
 MPMB_INST(double)

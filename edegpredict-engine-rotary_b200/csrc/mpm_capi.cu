@@ -137,9 +137,24 @@ mpm_status mpm_export_aos(mpm_handle* h, void* dst, int64_t dst_bytes) {
     return ret(h, h->eng->export_aos(0, dst, dst_bytes));
 }
 
+mpm_status mpm_import_aos(mpm_handle* h, const void* src, int64_t src_bytes, uint32_t fields) {
+    NEED_H(h);
+    return ret(h, h->eng->import_aos(0, src, src_bytes, fields));
+}
+
 mpm_status mpm_set_tool(mpm_handle* h, const mpm_tool_desc* tool) {
     NEED_H(h);
     return ret(h, h->eng->set_tool(0, tool));
+}
+
+mpm_status mpm_set_tool_nodes(mpm_handle* h, const mpm_tool_nodes* nodes) {
+    NEED_H(h);
+    return ret(h, h->eng->set_tool_nodes(0, nodes));
+}
+
+mpm_status mpm_set_workpiece_semantics(mpm_handle* h, const mpm_workpiece_params* params) {
+    NEED_H(h);
+    return ret(h, h->eng->set_workpiece_semantics(params));
 }
 
 mpm_status mpm_step(mpm_handle* h, double dt, int32_t nsteps) {
@@ -244,9 +259,24 @@ mpm_status mpm_batch_download(mpm_handle* h, int32_t inst, mpm_particles_soa* ho
     return ret(h, h->eng->download(inst, host));
 }
 
+mpm_status mpm_batch_export_aos(mpm_handle* h, int32_t inst, void* dst, int64_t dst_bytes) {
+    NEED_I(h, inst);
+    return ret(h, h->eng->export_aos(inst, dst, dst_bytes));
+}
+
+mpm_status mpm_batch_import_aos(mpm_handle* h, int32_t inst, const void* src, int64_t src_bytes, uint32_t fields) {
+    NEED_I(h, inst);
+    return ret(h, h->eng->import_aos(inst, src, src_bytes, fields));
+}
+
 mpm_status mpm_set_tool_sdf(mpm_handle* h, const mpm_tool_sdf* sdf) {
     NEED_H(h);
     return ret(h, h->eng->set_tool_sdf(0, sdf));
+}
+
+mpm_status mpm_batch_set_tool_nodes(mpm_handle* h, int32_t inst, const mpm_tool_nodes* nodes) {
+    NEED_I(h, inst);
+    return ret(h, h->eng->set_tool_nodes(inst, nodes));
 }
 
 mpm_status mpm_batch_set_tool_sdf(mpm_handle* h, int32_t inst, const mpm_tool_sdf* sdf) {

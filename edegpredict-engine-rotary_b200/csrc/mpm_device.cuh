@@ -76,7 +76,9 @@ template <typename R> struct PState {
 template <typename R> struct alignas(128) Inst {
     CUtensorMap tmap[2];           // TMA descriptors of grid buffers 0 and 1
     V4<R>* grid[2];
-    uint8_t* tool_mask;            // raster mode: 1 where a tool sample marked the node
+    // raster mode, per grid node: 0 unmarked, 1 marked by a sample (the tool's
+    // velocity), q + 1 marked last by tool node q (that node's velocity)
+    int32_t* tool_mask;
     int nx, ny, nz;
     int nbx, nby, nbz;
     int64_t nn;
@@ -104,6 +106,18 @@ template <typename R> struct alignas(128) Inst {
     double tool_p0[3], tool_v[3], tool_t0;
     double tool_r, tool_rake, tool_clear, tool_tip_dz;
     double tool_sg, tool_cg, tool_sa, tool_ca;   // sin/cos of rake and clearance, computed on the host
+    // raster samples (offsets from the tool pose: x..., y..., z...), rasterised
+    // at the pose of each step; or, when tn_end is set, the FEM tool's node
+    // records: node q at tn_start_q + a (tn_end_q - tn_start_q), a = tn_a0 +
+    // (steps since tn_step0) tn_da (tn_end_q when tn_start is NULL)
+    const double* samples;
+    int n_samples;
+    int tn_n, tn_stride;
+    int tn_off[6];                 // byte offsets of x, y, z, vx, vy, vz
+    const unsigned char* tn_start;
+    const unsigned char* tn_end;
+    double tn_a0, tn_da;
+    int64_t tn_step0;
     // particle-side tool contact after every contact_every-th step (0: off)
     int contact_every;
     double contact_r, contact_mu, contact_hp;
@@ -129,6 +143,18 @@ template <typename R> struct alignas(128) Inst {
     float sdf_o[3], sdf_vox, sdf_cos, sdf_sin;
     // external force for one step (radius 0: none)
     double ext_c[3], ext_r, ext_f[3];
+    // per-particle external force for one step, indexed pbase + upload order
+    // (written by an AoS import; NULL: none)
+    const V4<R>* pext;
+    // MPMWorkpieceSolver's semantics (mpm_set_workpiece_semantics): its shear
+    // and bulk moduli, damage rate divisor, CHIP thresholds (plastic strain,
+    // fraction of Tm), tool contact radius, contact heating damping, per-step
+    // heating cap with its switch, and the tool samples' offset box (x, y, z
+    // min then max) that bounds the nearest-sample search
+    R ws_shear, ws_bulk, ws_fail, ws_crit_eps, ws_chip_ratio, ws_damping, ws_max_rise;
+    int ws_clamp;
+    double ws_contact_r;
+    double ws_sbox[6];
     int64_t pbase;                 // first particle slot of this instance in the batch arrays
     int64_t np;                    // live particles of this instance, at [pbase, pbase + np)
     int64_t pcap;                  // particle slots of this instance

@@ -106,7 +106,7 @@ class Engine final : public EngineBase {
     // heat conduction node arrays, beside the grids: T m scatter (two buffers, paired with
     // gpool) and the node temperatures after the diffusion step
     R* tpool[3] = {nullptr, nullptr, nullptr};
-    uint8_t* mask_pool = nullptr;
+    int32_t* mask_pool = nullptr;     // raster marks per grid node (Inst::tool_mask)
     Inst<R>* d_inst = nullptr;
     std::vector<Inst<R>> h_inst;
     int32_t *d_key_base = nullptr, *d_bin_key = nullptr, *d_bin_inst = nullptr, *d_bin_local = nullptr;
@@ -128,6 +128,11 @@ class Engine final : public EngineBase {
     int stat_blocks = 0;
     void* d_stage = nullptr;
     size_t stage_bytes = 0;
+    V4<R>* d_pext = nullptr;       // per-particle external force of an AoS import (pbase + upload order)
+    int64_t pext_alloc = 0;
+    int* d_flags = nullptr;        // AoS import: [0] a particle moved, [1] records with an invalid status
+    bool ws_on = false;            // MPMWorkpieceSolver's step semantics
+    mpm_workpiece_params ws{};
     int32_t* d_gen = nullptr;
     size_t gen_bytes = 0;
     bool binned = false;
@@ -192,7 +197,8 @@ class Engine final : public EngineBase {
                         d_bin_local,
                         d_inst_pbase, d_key, d_rank, d_newbin, d_count, d_offset, d_flag, d_flag_scan, d_scan_tmp,
                         d_pos, d_work, d_nwork, d_err, d_ierr, d_ctr, d_stat_part, d_stat_out, d_stage, d_gen,
-                        d_map, d_perm, d_det_contrib, d_det_i32[0], d_det_i32[1], d_det_i32[2], d_det_i32[3], d_det_tmp};
+                        d_map, d_perm, d_det_contrib, d_det_i32[0], d_det_i32[1], d_det_i32[2], d_det_i32[3], d_det_tmp,
+                        d_pext, d_flags};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         for (auto& x : I)
@@ -347,6 +353,9 @@ class Engine final : public EngineBase {
         std::vector<int64_t> inst_pbase(n);
         for (int i = 0; i < n; ++i) {
             InstHost& x = I[i];
+            // a pending imported per-particle force is indexed by the old slot
+            // range: an instance change drops it
+            x.pext_pending = false;
             x.pbase = pb;
             pb += x.cap;
             x.nn = (int64_t)x.p.nx * x.p.ny * x.p.nz;
@@ -436,14 +445,14 @@ class Engine final : public EngineBase {
             const int64_t nn = std::max<int64_t>(nn_total + nn_total / 4, 1);
             for (int b = 0; b < 2; ++b) CK(cudaMalloc(&gpool[b], sizeof(V4<R>) * nn));
             for (int b = 0; b < 3; ++b) CK(cudaMalloc(&tpool[b], sizeof(R) * nn));
-            CK(cudaMalloc(&mask_pool, nn));
+            CK(cudaMalloc(&mask_pool, sizeof(int32_t) * nn));
             nn_alloc = nn;
         }
         if (nn_total > 0) {
             CK(cudaMemsetAsync(gpool[0], 0, sizeof(V4<R>) * nn_total, st));
             CK(cudaMemsetAsync(gpool[1], 0, sizeof(V4<R>) * nn_total, st));
             for (int b = 0; b < 3; ++b) CK(cudaMemsetAsync(tpool[b], 0, sizeof(R) * nn_total, st));
-            CK(cudaMemsetAsync(mask_pool, 0, nn_total, st));
+            CK(cudaMemsetAsync(mask_pool, 0, sizeof(int32_t) * nn_total, st));
         }
         rbuf = 0;
         // sort scratch, key and bin tables
@@ -533,7 +542,7 @@ class Engine final : public EngineBase {
         }
         if (mask_pool) cudaFree(mask_pool);
         mask_pool = nullptr;
-        CK(cudaMalloc(&mask_pool, nodes));
+        CK(cudaMalloc(&mask_pool, sizeof(int32_t) * nodes));
         nn_alloc = nodes;
         MS(grow(d_key, slot_alloc[0], particles, false));
         MS(grow(d_rank, slot_alloc[1], particles, false));
@@ -631,6 +640,19 @@ class Engine final : public EngineBase {
         const mpm_params& p = x.p;
         Inst<R>& d = h_inst[i];
         d.tool_mask = mask_pool + x.grid_off;
+        d.samples = x.d_samples;
+        d.n_samples = x.n_samples;
+        d.tn_start = x.has_nodes ? static_cast<const unsigned char*>(x.nodes.start) : nullptr;
+        d.tn_end = x.has_nodes ? static_cast<const unsigned char*>(x.nodes.end) : nullptr;
+        d.tn_n = x.has_nodes ? x.nodes.n : 0;
+        d.tn_stride = x.nodes.stride;
+        for (int a = 0; a < 3; ++a) {
+            d.tn_off[a] = x.nodes.off_pos[a];
+            d.tn_off[3 + a] = x.nodes.off_vel[a];
+        }
+        d.tn_a0 = x.nodes.alpha0;
+        d.tn_da = x.nodes.dalpha;
+        d.tn_step0 = x.nodes_step0;
         d.ierr = d_ierr + i;
         d.tm[0] = tpool[0] + x.grid_off;
         d.tm[1] = tpool[1] + x.grid_off;
@@ -683,7 +705,19 @@ class Engine final : public EngineBase {
             for (int a = 0; a < 3; ++a) { d.sdf_n[a] = x.sdf->n[a]; d.sdf_o[a] = x.sdf->origin[a]; }
             d.sdf_vox = x.sdf->voxel; d.sdf_cos = x.sdf->cos_a; d.sdf_sin = x.sdf->sin_a;
         }
-        d.heat_on = p.heat_conduction ? 1 : 0;
+        // MPMWorkpieceSolver diffuses whenever k / (rho cp) > 0 (src/MPMWorkpieceSolver.cu:750-760)
+        d.heat_on = (ws_on ? (p.thermal_conductivity > 0.0 && p.cp > 0.0 && p.rho_phys > 0.0) : p.heat_conduction != 0)
+                        ? 1 : 0;
+        d.ws_shear = (R)(p.E / (2.0 * (1.0 + p.nu)));
+        d.ws_bulk = (R)(p.E / (3.0 * (1.0 - 2.0 * p.nu)));
+        d.ws_fail = (R)ws.failure_strain;
+        d.ws_crit_eps = (R)ws.critical_plastic_strain;
+        d.ws_chip_ratio = (R)ws.thermal_chip_ratio;
+        d.ws_damping = (R)ws.contact_damping;
+        d.ws_max_rise = (R)ws.max_contact_temp_rise;
+        d.ws_clamp = ws.thermal_clamp ? 1 : 0;
+        d.ws_contact_r = ws.tool_contact_radius;
+        for (int a = 0; a < 6; ++a) d.ws_sbox[a] = x.sbox[a];
         d.heat_c = p.thermal_conductivity / (p.rho_phys * p.cp) * x.dt / (p.dx * p.dx);
         d.Tamb = (R)p.Tamb;
         d.cp = p.cp;
@@ -705,6 +739,7 @@ class Engine final : public EngineBase {
         d.tool_sa = std::sin(t.clearance); d.tool_ca = std::cos(t.clearance);
         for (int a = 0; a < 3; ++a) { d.ext_c[a] = x.ext_c[a]; d.ext_f[a] = x.ext_f[a]; }
         d.ext_r = x.ext_pending ? x.ext_r : 0.0;
+        d.pext = x.pext_pending ? d_pext : nullptr;
         d.pbase = x.pbase; d.np = x.np; d.pcap = x.cap;
         d.fresh = x.fresh;
     }
@@ -823,6 +858,7 @@ class Engine final : public EngineBase {
         x.np = (int64_t)lasti + lastf;
         x.fresh = 1;
         x.broken = false;
+        x.pext_pending = false;
         CK(cudaMemsetAsync(d_ierr + i, 0, sizeof(int), st));   // a new state starts without errors
         CK(cudaGetLastError());
         return push_insts();  // binned by the next call that needs it
@@ -887,6 +923,7 @@ class Engine final : public EngineBase {
         x.np = n;
         x.fresh = 1;
         x.broken = false;
+        x.pext_pending = false;
         CK(cudaMemsetAsync(d_ierr + i, 0, sizeof(int), st));   // a new state starts without errors
         CK(cudaGetLastError());
         return push_insts();  // binned by the next call that needs it
@@ -971,6 +1008,59 @@ class Engine final : public EngineBase {
         return inst_status(i);
     }
 
+    mpm_status import_aos(int i, const void* src, int64_t bytes, uint32_t fields) override {
+        Range nvtx_range("mpm.import_aos");
+        InstHost& x = I[i];
+        if (!src || bytes < x.np * 504) {
+            err = "source smaller than np * sizeof(MPMParticle) (504 bytes)";
+            return MPM_INVALID_ARG;
+        }
+        if (fields & ~(uint32_t)MPM_AOS_WRITABLE) {
+            err = "unknown MPM_AOS_* field bits";
+            return MPM_INVALID_ARG;
+        }
+        if (fields == 0 || x.np == 0) return MPM_OK;
+        // positions are re-expressed in the bins the export was taken from
+        MS(ensure_binned());
+        cudaPointerAttributes at{};
+        const bool dev = cudaPointerGetAttributes(&at, src) == cudaSuccess &&
+                         (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged);
+        cudaGetLastError();
+        const void* in = src;
+        if (!dev) {
+            const size_t need = (size_t)504 * x.np;
+            if (stage_bytes < need) {
+                CK(cudaStreamSynchronize(st));
+                if (d_stage) cudaFree(d_stage);
+                d_stage = nullptr;
+                CK(cudaMalloc(&d_stage, need));
+                stage_bytes = need;
+            }
+            CK(cudaMemcpyAsync(d_stage, src, need, cudaMemcpyHostToDevice, st));
+            in = d_stage;
+        }
+        if (!d_flags) CK(cudaMalloc(&d_flags, 2 * sizeof(int)));
+        if ((fields & MPM_AOS_EXT_FORCE) && pext_alloc < cap_total) {
+            CK(cudaStreamSynchronize(st));
+            MS(grow(d_pext, pext_alloc, cap_total, false));
+        }
+        CK(cudaMemsetAsync(d_flags, 0, 2 * sizeof(int), st));
+        launch_import_aos<R>(d_inst + i, ps[cur], x.pbase, x.np, x.p.Tamb, fields,
+                             in, (fields & MPM_AOS_EXT_FORCE) ? d_pext : nullptr, d_flags, st);
+        int h[2] = {0, 0};
+        CK(cudaMemcpyAsync(h, d_flags, sizeof(h), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        CK(cudaGetLastError());
+        if (h[0]) binned = false;   // moved particles: re-bin before the next step
+        if (fields & MPM_AOS_EXT_FORCE) x.pext_pending = true;
+        MS(push_insts());
+        if (h[1]) {
+            err = std::to_string(h[1]) + " records have a status outside 0..4 (kept their status)";
+            return MPM_INVALID_ARG;
+        }
+        return MPM_OK;
+    }
+
     // ---------------------------------------------------------------- tool
 
     // The voxel tool SDF as a 3D texture set up as ToolSDF::createTexture does
@@ -1032,40 +1122,95 @@ class Engine final : public EngineBase {
         x.tool_t0 = x.time;
         if (t->mode == MPM_TOOL_RASTER) {
             const int ns = std::max(t->n_samples, 0);
-            if (x.d_samples) {
-                CK(cudaStreamSynchronize(st));
-                cudaFree(x.d_samples);
+            // the samples live in one device buffer, reused while it is large
+            // enough: a captured step graph reads them through the instance
+            // record and stays valid
+            if (ns > x.samples_cap) {
+                CK(cudaStreamSynchronize(st));   // nothing in flight reads the old buffer
+                if (x.d_samples) cudaFree(x.d_samples);
                 x.d_samples = nullptr;
+                x.samples_cap = 0;
+                CK(cudaMalloc(&x.d_samples, 3 * sizeof(double) * ns));
+                x.samples_cap = ns;
             }
             x.n_samples = ns;
+            for (int a = 0; a < 3; ++a) { x.sbox[a] = 0.0; x.sbox[3 + a] = 0.0; }
             if (ns > 0) {
-                CK(cudaMalloc(&x.d_samples, 3 * sizeof(double) * ns));
+                const double* c[3] = {t->sample_dx, t->sample_dy, t->sample_dz};
+                for (int a = 0; a < 3; ++a) {
+                    x.sbox[a] = x.sbox[3 + a] = c[a][0];
+                    for (int q = 1; q < ns; ++q) {
+                        x.sbox[a] = std::min(x.sbox[a], c[a][q]);
+                        x.sbox[3 + a] = std::max(x.sbox[3 + a], c[a][q]);
+                    }
+                }
                 CK(cudaMemcpyAsync(x.d_samples, t->sample_dx, 8 * ns, cudaMemcpyHostToDevice, st));
                 CK(cudaMemcpyAsync(x.d_samples + ns, t->sample_dy, 8 * ns, cudaMemcpyHostToDevice, st));
                 CK(cudaMemcpyAsync(x.d_samples + 2 * ns, t->sample_dz, 8 * ns, cudaMemcpyHostToDevice, st));
                 CK(cudaStreamSynchronize(st));
             }
+        } else {
+            x.has_nodes = false;
         }
+        return push_insts();
+    }
+
+    // The raster tool from FEM node records in device memory (mpm_tool_nodes).
+    mpm_status set_tool_nodes(int i, const mpm_tool_nodes* n) override {
+        InstHost& x = I[i];
+        if (!n) {
+            x.has_nodes = false;
+            return push_insts();
+        }
+        if (!n->end || n->n <= 0 || n->stride < 24) {
+            err = "tool nodes: end records, n > 0 and a stride of at least 24 bytes required";
+            return MPM_INVALID_ARG;
+        }
+        for (int a = 0; a < 3; ++a)
+            if (n->off_pos[a] < 0 || n->off_pos[a] + 8 > n->stride || n->off_vel[a] < 0 ||
+                n->off_vel[a] + 8 > n->stride || (n->off_pos[a] % 8) != 0 || (n->off_vel[a] % 8) != 0) {
+                err = "tool nodes: field offsets must be 8-byte aligned and inside a record";
+                return MPM_INVALID_ARG;
+            }
+        if ((n->stride % 8) != 0 || (reinterpret_cast<uintptr_t>(n->end) % 8) != 0 ||
+            (reinterpret_cast<uintptr_t>(n->start) % 8) != 0) {
+            err = "tool nodes: records must be 8-byte aligned";
+            return MPM_INVALID_ARG;
+        }
+        if (!std::isfinite(n->alpha0) || !std::isfinite(n->dalpha)) {
+            err = "tool nodes: alpha0 and dalpha must be finite";
+            return MPM_INVALID_ARG;
+        }
+        x.nodes = *n;
+        x.has_nodes = true;
+        x.nodes_step0 = x.step;
+        x.tool.mode = MPM_TOOL_RASTER;
         return push_insts();
     }
 
     // ---------------------------------------------------------------- step
 
+    // Points the raster tool of an instance marks per step (samples or FEM
+    // nodes; 0: no raster tool).
+    static int raster_points(const InstHost& x) {
+        if (x.tool.mode != MPM_TOOL_RASTER) return 0;
+        return x.has_nodes ? x.nodes.n : x.n_samples;
+    }
+
+    // The tool masks of step k of the call: cleared, then marked by the
+    // raster kernel, which reads the pose (or the node records and their
+    // blend) from the instance record, so the sequence replays from a graph.
     void raster_all(int k) {
         bool any = false;
-        for (const auto& x : I) any |= (x.tool.mode == MPM_TOOL_RASTER && x.n_samples > 0);
+        for (const auto& x : I) any |= raster_points(x) > 0;
         if (!any) return;
         Range nvtx_range("mpm.tool_raster");
-        for (auto& x : I) {
-            if (x.tool.mode != MPM_TOOL_RASTER || x.n_samples <= 0) continue;
-            const double t = x.time + (double)k * x.dt;
-            const double px = x.tool.position[0] + x.tool.velocity[0] * (t - x.tool_t0);
-            const double py = x.tool.position[1] + x.tool.velocity[1] * (t - x.tool_t0);
-            const double pz = x.tool.position[2] + x.tool.velocity[2] * (t - x.tool_t0);
-            cudaMemsetAsync(mask_pool + x.grid_off, 0, x.nn, st);
-            launch_raster(x.d_samples, x.d_samples + x.n_samples, x.d_samples + 2 * x.n_samples, x.n_samples, px, py,
-                          pz, x.p.origin[0], x.p.origin[1], x.p.origin[2], x.p.dx, x.p.nx, x.p.ny, x.p.nz,
-                          mask_pool + x.grid_off, st);
+        for (int i = 0; i < (int)I.size(); ++i) {
+            const InstHost& x = I[i];
+            const int np = raster_points(x);
+            if (np <= 0) continue;
+            cudaMemsetAsync(mask_pool + x.grid_off, 0, sizeof(int32_t) * x.nn, st);
+            launch_raster<R>(d_inst, i, k, np, st);
         }
     }
 
@@ -1092,10 +1237,11 @@ class Engine final : public EngineBase {
         if (s != MPM_OK) return s;
         s = push_insts();
         if (s != MPM_OK) return s;
-        bool ext = false, raster = false;
-        for (auto& x : I) {
-            ext |= x.ext_pending;
-            raster |= (x.tool.mode == MPM_TOOL_RASTER && x.n_samples > 0);
+        bool ext = false;
+        for (auto& x : I) ext |= x.ext_pending || x.pext_pending;
+        if (det && ws_on) {
+            err = "the deterministic mode covers MPMSolver's semantics only";
+            return MPM_NOT_SUPPORTED;
         }
         if (det) {
             for (const auto& x : I)
@@ -1106,7 +1252,16 @@ class Engine final : public EngineBase {
                 }
             MS(det_scratch());
         }
-        if (use_graph && !raster && !prof && max_work > 0 && !det)
+        // the raster launches' sizes are part of a captured graph
+        std::vector<int> rsig(I.size());
+        for (size_t q = 0; q < I.size(); ++q) rsig[q] = raster_points(I[q]);
+        if (rsig != raster_sig) {
+            drop_graphs();
+            raster_sig = rsig;
+        }
+        if (ws_on)
+            s = issue_ws_steps(N, ext);
+        else if (use_graph && !prof && max_work > 0 && !det)
             s = step_graph(N, ext);
         else
             s = issue_steps(N, ext);
@@ -1115,6 +1270,7 @@ class Engine final : public EngineBase {
             x.time += (double)N * x.dt;
             x.step += N;
             x.ext_pending = false;
+            x.pext_pending = false;
         }
         CK(cudaGetLastError());
         return MPM_OK;
@@ -1203,6 +1359,48 @@ class Engine final : public EngineBase {
         return MPM_OK;
     }
 
+    // MPMWorkpieceSolver's step, N times: clear grid buffer 0 and its T m, then
+    // P2G, the grid update (contact force of the step into the metrics'
+    // contact-force slot), the diffusion step, G2P and chip separation.
+    mpm_status issue_ws_steps(int32_t N, bool ext) {
+        std::vector<int64_t> np(I.size()), nn(I.size());
+        for (size_t i = 0; i < I.size(); ++i) {
+            np[i] = I[i].np;
+            nn[i] = I[i].nn;
+        }
+        int diffuse = 0;
+        for (const auto& h : h_inst) diffuse |= h.heat_on;
+        double* fsum = reinterpret_cast<double*>(d_ctr + 4) + 1;
+        for (int k = 0; k < N; ++k) {
+            CK(cudaMemsetAsync(gpool[0], 0, sizeof(V4<R>) * nn_total, st));
+            CK(cudaMemsetAsync(tpool[0], 0, sizeof(R) * nn_total, st));
+            CK(cudaMemsetAsync(fsum, 0, sizeof(double), st));
+            launch_ws_step<R>(d_inst, np, nn, ps[cur], k, (ext && k == 0) ? 1 : 0, diffuse, fsum, st,
+                              &launch_heat_diffuse<R>, nn_total);
+        }
+        rbuf = 0;
+        return MPM_OK;
+    }
+
+    mpm_status set_workpiece_semantics(const mpm_workpiece_params* p) override {
+        CK(cudaStreamSynchronize(st));
+        drop_graphs();
+        if (!p) {
+            if (ws_on) binned = false;   // positions drifted from their bins: re-bin for the fused kernel
+            ws_on = false;
+            return push_insts();
+        }
+        if (!(p->tool_contact_radius >= 0.0) || !std::isfinite(p->failure_strain) ||
+            !std::isfinite(p->critical_plastic_strain) || !std::isfinite(p->thermal_chip_ratio) ||
+            !(p->contact_damping >= 0.0) || !(p->max_contact_temp_rise >= 0.0)) {
+            err = "workpiece semantics: finite constants, non-negative radius, damping and cap required";
+            return MPM_INVALID_ARG;
+        }
+        ws = *p;
+        ws_on = true;
+        return push_insts();
+    }
+
     // ---------------------------------------------------------------- graphs
 
     // A captured step call, valid for one layout and launch configuration; the
@@ -1217,6 +1415,7 @@ class Engine final : public EngineBase {
         uint64_t use;
     };
     std::vector<GraphEntry> graphs;
+    std::vector<int> raster_sig;   // raster points per instance when the graphs were captured
     uint64_t graph_clock = 0;
     static constexpr size_t kMaxGraphs = 32;
 
@@ -1647,6 +1846,8 @@ class Engine final : public EngineBase {
         if (x.d_samples) cudaFree(x.d_samples);   // the stream is idle (synchronised above)
         x.d_samples = samples;
         x.n_samples = h.n_samples > 0 ? h.n_samples : 0;
+        x.samples_cap = x.n_samples;
+        x.has_nodes = false;   // a node source (device pointers) is not part of a checkpoint
         x.broken = false;
         x.p = h.params;
         x.tool = h.tool;
@@ -1657,6 +1858,7 @@ class Engine final : public EngineBase {
         x.dt = h.dt;
         x.fresh = 0;
         x.ext_pending = false;
+        x.pext_pending = false;
         binned = false;   // the next call that needs bins re-bins from the loaded bins
         return push_insts();
     }

@@ -41,6 +41,12 @@ struct InstHost {
     int64_t step = 0;
     double* d_samples = nullptr;
     int n_samples = 0;
+    int samples_cap = 0;    // samples d_samples holds room for (set_tool reuses it)
+    double sbox[6] = {0, 0, 0, 0, 0, 0};   // the samples' offset box: x, y, z min, then max
+    // raster from FEM node records in device memory (mpm_set_tool_nodes)
+    bool has_nodes = false;
+    mpm_tool_nodes nodes{};
+    int64_t nodes_step0 = 0;  // step counter when the node source was set
     double ext_c[3] = {0, 0, 0}, ext_r = 0.0, ext_f[3] = {0, 0, 0};
     bool ext_pending = false;
     double tool_t0 = 0.0;   // time at which the tool descriptor was set
@@ -50,6 +56,9 @@ struct InstHost {
     // arrays: the state is part old, part new.  Steps refuse the handle until
     // an upload, a generated box or a complete checkpoint load replaces it.
     bool broken = false;
+    // An AoS import brought per-particle external forces for the next step
+    // (device array indexed pbase + upload order).
+    bool pext_pending = false;
 };
 
 class EngineBase {
@@ -61,8 +70,13 @@ class EngineBase {
     virtual mpm_status upload(int inst, const mpm_particles_soa* host, int64_t n) = 0;
     virtual mpm_status download(int inst, mpm_particles_soa* host) = 0;
     virtual mpm_status export_aos(int inst, void* dst, int64_t bytes) = 0;
+    virtual mpm_status import_aos(int inst, const void* src, int64_t bytes, uint32_t fields) = 0;
     virtual mpm_status set_tool(int inst, const mpm_tool_desc* t) = 0;
     virtual mpm_status set_tool_sdf(int inst, const mpm_tool_sdf* s) = 0;
+    virtual mpm_status set_tool_nodes(int inst, const mpm_tool_nodes* n) = 0;
+    // MPMWorkpieceSolver's step semantics for the whole handle (NULL: back to
+    // MPMSolver's).
+    virtual mpm_status set_workpiece_semantics(const mpm_workpiece_params* p) = 0;
     virtual mpm_status step(int32_t nsteps, const double* dt_per_inst) = 0;
     virtual mpm_status metrics(int inst, mpm_metrics* out) = 0;
     virtual mpm_status set_mass_scaling(int inst, double f) = 0;

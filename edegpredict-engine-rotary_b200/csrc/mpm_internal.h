@@ -9,6 +9,7 @@
 
 #include <atomic>
 #include <string>
+#include <vector>
 
 #include "../../include/mpm_capi.h"
 #include "mpm_device.cuh"
@@ -102,8 +103,11 @@ void launch_bin_scatter(const PState<R>& src, const PState<R>& dst, const Inst<R
 template <typename R>
 void launch_pad_counts(const Inst<R>* insts, int n_inst, const int32_t* key_base, int32_t* count, cudaStream_t st);
 
-void launch_raster(const double* sx, const double* sy, const double* sz, int ns, double px, double py, double pz,
-                   double ox, double oy, double oz, double dx, int nx, int ny, int nz, uint8_t* mask, cudaStream_t st);
+// The raster tool of instance i at step k of the current call (samples or FEM
+// node records, pose and blend from the instance record) into its tool mask;
+// npoints = samples or nodes.
+template <typename R>
+void launch_raster(const Inst<R>* insts, int i, int k, int npoints, cudaStream_t st);
 
 template <typename R>
 void launch_import(const DevSoA& in, int64_t n, double ox, double oy, double oz, double dx, double Tamb,
@@ -123,6 +127,23 @@ void launch_export(const Inst<R>* inst_dev, const PState<R>& ps, int64_t pbase, 
 template <typename R>
 void launch_export_aos(const Inst<R>* inst_dev, const PState<R>& ps, int64_t pbase, int64_t n, double Tamb,
                        double rho, void* out, cudaStream_t st);
+
+// Reads `fields` (MPM_AOS_*) of n MPMParticle records (device memory, upload
+// order) back into the particle state; the external force goes to pext
+// (indexed pbase + upload order).  flags[0]: a particle moved (re-bin);
+// flags[1]: records whose status is outside 0..4.
+template <typename R>
+void launch_import_aos(const Inst<R>* inst_dev, const PState<R>& ps, int64_t pbase, int64_t n, double Tamb,
+                       uint32_t fields, const void* in, V4<R>* pext, int* flags, cudaStream_t st);
+
+// One step of MPMWorkpieceSolver's semantics for every instance (np, nn:
+// particles and nodes of each): P2G into grid buffer 0 and tm[0], the grid
+// update (contact force into *fsum), diffuse_fn when diffuse, G2P and chip
+// separation.  use_ext: the first step of a call (pending external forces).
+template <typename R>
+void launch_ws_step(const Inst<R>* insts, const std::vector<int64_t>& np, const std::vector<int64_t>& nn,
+                    const PState<R>& ps, int k, int use_ext, int diffuse, double* fsum, cudaStream_t st,
+                    void (*diffuse_fn)(const Inst<R>*, int, int, int64_t, cudaStream_t), int64_t nn_total);
 
 template <typename R>
 void launch_stats(const Inst<R>* inst_dev, const PState<R>& ps, int64_t pbase, int64_t n, double mu, double K,

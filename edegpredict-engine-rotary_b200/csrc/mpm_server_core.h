@@ -71,7 +71,7 @@ inline PoolBytes pool_bytes(int precision, bool backstress, bool deterministic =
     // deterministic mode: 27 node contributions (4 reals each), four int32 sort
     // arrays and the radix sort's double buffers
     if (deterministic) b.particle += 27.0 * v4 + 16.0 + 16.0;
-    b.node = 2.0 * v4 + 3.0 * r + 1.0;   // two grid buffers, three heat-conduction arrays, tool mask
+    b.node = 2.0 * v4 + 3.0 * r + 4.0;   // two grid buffers, three heat-conduction arrays, tool mask (int32)
     b.key = 8.0;                 // count and offset
     b.bin = 40.0;                // bin tables, flags and the work item
     return b;

@@ -177,8 +177,17 @@ __device__ __forceinline__ NV<R> node_vel_inl(const Inst<R>& P, const V4<R> g, i
         }
     }
     if (P.tool_mode == TOOL_RASTER) {
-        if (P.tool_mask[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)]) {
-            vx = (R)P.tool_v[0]; vy = (R)P.tool_v[1]; vz = (R)P.tool_v[2];
+        const int32_t mk = P.tool_mask[gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz)];
+        if (mk) {
+            if (P.tn_end) {
+                // the velocity of the tool node that marked it
+                const unsigned char* r = P.tn_end + (int64_t)(mk - 1) * P.tn_stride;
+                vx = (R)*reinterpret_cast<const double*>(r + P.tn_off[3]);
+                vy = (R)*reinterpret_cast<const double*>(r + P.tn_off[4]);
+                vz = (R)*reinterpret_cast<const double*>(r + P.tn_off[5]);
+            } else {
+                vx = (R)P.tool_v[0]; vy = (R)P.tool_v[1]; vz = (R)P.tool_v[2];
+            }
         }
     } else if ((P.tool_mode == TOOL_SDF_STICKY || P.tool_mode == TOOL_SDF_SLIP) &&
                !tool_far(P, node_coord(gx, P.dx, P.ox), node_coord(gz, P.dx, P.oz), pr0, pr2)) {
@@ -851,9 +860,13 @@ template <typename R, bool EXT> struct StepSmem {
         R pay[EXT ? kPay + 1 : kPay][StepCfg<R>::kChunk];  // scatter payload of the staged particles
     };
     R vel[3][kPlane];                      // node velocities after the grid update
-    R nacc[EXT ? 5 : 4][kPlane];           // the bin's node sums m, p_x, p_y, p_z (, T m) (tidx layout)
+    // the bin's node sums m, p_x, p_y, p_z (, T m) (tidx layout), one copy per
+    // half of the bin's cells: each warp adds only to its own copy, so the
+    // adds need no atomics (the flush sums the two)
+    R nacc[2][EXT ? 5 : 4][kPlane];
     R ttile[EXT ? 2 : 1][EXT ? kPlane : 1];  // node temperatures and their m > 1e-18 mask
-    short slot[kCellsPerBin][kCellCap];    // staged particles of each base cell
+    short slot[kCellCap][kCellsPerBin];    // staged particles of each base cell, by rank (the cells of a warp
+                                           // read consecutive entries)
     int cnt[2][kCellsPerBin];              // staged particles per cell (atomic ranks), by pass parity
     uint64_t mbar;
     int fail;
@@ -896,13 +909,18 @@ __device__ __forceinline__ void channel_add(const R (&w)[3][3], const R (&dw)[3]
 
 // Accumulation of one cell's staged particles (thread pair per cell: h = 0
 // takes m and p_x, h = 1 takes p_y and p_z) in registers, then added to the
-// 27 nodes of the cell's stencil in the bin's node tile with shared-memory
-// atomics.  For one stencil offset the 32 cells of a warp (cz in {0,1} or
-// {2,3}) address 32 distinct nodes, and tidx's z stride of 68 (4 mod 32)
-// puts them in 32 distinct banks: the adds neither collide nor conflict.
-// par: parity of the staging pass.
+// 27 nodes of the cell's stencil in the warp's own copy of the node tile
+// (half = the warp's half of the cells).  The adds run in 27 phases, one
+// stencil offset each, separated by __syncwarp: within a phase the 32 cells
+// of the warp (cz in {0,1} or {2,3}) address 32 distinct nodes, and tidx's z
+// stride of 68 (4 mod 32) puts them in 32 distinct banks, so plain
+// load-add-stores neither collide nor conflict (a shared-memory FP32 atomic
+// costs several times a plain add on this part).  Every lane takes part in
+// every phase (a cell without particles adds zeros), so the warp stays
+// converged at each __syncwarp.  par: parity of the staging pass.
 template <typename R, bool EXT>
-__device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT>& Sm, int cell, int h, R pm, int par, bool heat) {
+__device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT>& Sm, int cell, int h, int half, R pm, int par,
+                                                bool heat) {
     R a0[kOff], a1[kOff];
 #pragma unroll
     for (int o = 0; o < kOff; ++o) { a0[o] = R(0); a1[o] = R(0); }
@@ -911,7 +929,7 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT>& Sm, int cell, 
     // them for the next one
     if (h == 0) Sm.cnt[par ^ 1][cell] = 0;
     for (int q = 0; q < n; ++q) {
-        const int e = Sm.slot[cell][q];
+        const int e = Sm.slot[q][cell];
         R w[3][3], dw[3][3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) (void)bspline(Sm.pay[a][e], w[a], dw[a]);
@@ -935,8 +953,10 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT>& Sm, int cell, 
                            Sm.pay[22][e], Sm.pay[23][e], a1);
         }
     }
-    if (n > 0) {
+    {
         const int base = tidx(cell & (kBin - 1), (cell / kBin) & (kBin - 1), cell / (kBin * kBin));
+        R* __restrict__ t0 = Sm.nacc[half][2 * h];
+        R* __restrict__ t1 = Sm.nacc[half][2 * h + 1];
 #pragma unroll
         for (int k = 0; k < 3; ++k)
 #pragma unroll
@@ -944,17 +964,19 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT>& Sm, int cell, 
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
                     const int o = i + 3 * j + 9 * k, t = base + i + kSY * j + kSZ * k;
-                    atomicAdd(&Sm.nacc[2 * h][t], a0[o]);
-                    atomicAdd(&Sm.nacc[2 * h + 1][t], a1[o]);
+                    __syncwarp();
+                    t0[t] += a0[o];
+                    t1[t] += a1[o];
                 }
+        __syncwarp();
     }
-    if (EXT && heat && h == 0 && n > 0) {
+    if (EXT && heat && h == 0) {
         // heat conduction: the T m channel, w m T over the cell's particles (the
         // lighter half of the pair takes it)
 #pragma unroll
         for (int o = 0; o < kOff; ++o) a0[o] = R(0);
         for (int q = 0; q < n; ++q) {
-            const int e = Sm.slot[cell][q];
+            const int e = Sm.slot[q][cell];
             R w[3][3], dw[3][3];
 #pragma unroll
             for (int a = 0; a < 3; ++a) (void)bspline(Sm.pay[a][e], w[a], dw[a]);
@@ -971,13 +993,17 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT>& Sm, int cell, 
             }
         }
         const int base = tidx(cell & (kBin - 1), (cell / kBin) & (kBin - 1), cell / (kBin * kBin));
+        R* __restrict__ t4 = Sm.nacc[half][EXT ? 4 : 0];
 #pragma unroll
         for (int k = 0; k < 3; ++k)
 #pragma unroll
             for (int j = 0; j < 3; ++j)
 #pragma unroll
-                for (int i = 0; i < 3; ++i)
-                    atomicAdd(&Sm.nacc[4][base + i + kSY * j + kSZ * k], a0[i + 3 * j + 9 * k]);
+                for (int i = 0; i < 3; ++i) {
+                    __syncwarp();
+                    t4[base + i + kSY * j + kSZ * k] += a0[i + 3 * j + 9 * k];
+                }
+        __syncwarp();
     }
 }
 
@@ -1032,7 +1058,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
     if (tid < 2 * kCellsPerBin) (&Sm.cnt[0][0])[tid] = 0;
     // node sums start at zero; the end-of-bin flush clears what it reads
     if (P2G)
-        for (int q = tid; q < (EXT ? 5 : 4) * kPlane; q += kNT) (&Sm.nacc[0][0])[q] = R(0);
+        for (int q = tid; q < 2 * (EXT ? 5 : 4) * kPlane; q += kNT) (&Sm.nacc[0][0][0])[q] = R(0);
     __syncthreads();
     int par = 0;  // parity of the staging pass (counts double-buffered across passes)
     int last_inst = -1;
@@ -1414,10 +1440,19 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                             R Q[3] = {0, 0, 0}, Rm[9], S[9];
 #pragma unroll
                             for (int q = 0; q < 9; ++q) { Rm[q] = R(0); S[q] = R(0); }
+                            R ef[3] = {0, 0, 0};
+                            if (sa.use_ext && P.pext) {
+                                // an imported per-particle force (MPMParticle::ext_f) acts on every
+                                // particle the step scatters, FIXED included: p2gKernel adds
+                                // w * ext_f to the node force (src/MPMSolver.cu:410-417)
+                                const V4<R> e = P.pext[P.pbase + ps.orig[pi]];
+                                const R fdt = (R)P.dt;
+                                ef[0] = e.x * fdt; ef[1] = e.y * fdt; ef[2] = e.z * fdt;
+                                if (fixed) { Q[0] = ef[0]; Q[1] = ef[1]; Q[2] = ef[2]; }
+                            }
                             if (!fixed) {
                                 const R d[3] = {xi[0] - R(bb[0]), xi[1] - R(bb[1]), xi[2] - R(bb[2])};
                                 const R mdx = m * (R)P.dx;
-                                R ef[3] = {0, 0, 0};
                                 if (sa.use_ext && P.ext_r > 0.0 && (st == ST_ACTIVE || st == ST_CHIP)) {
                                     const double ex = P.ox + ((double)g0x + ((double)xi[0] + (double)lo[0])) * P.dx - P.ext_c[0];
                                     const double ey = P.oy + ((double)g0y + ((double)xi[1] + (double)lo[1])) * P.dx - P.ext_c[1];
@@ -1425,8 +1460,8 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                     const double dist = sqrt(ex * ex + ey * ey + ez * ez);
                                     if (dist < P.ext_r) {
                                         const double fw = (1.0 - dist / P.ext_r) * P.dt;
-                                        ef[0] = (R)(P.ext_f[0] * fw); ef[1] = (R)(P.ext_f[1] * fw);
-                                        ef[2] = (R)(P.ext_f[2] * fw);
+                                        ef[0] += (R)(P.ext_f[0] * fw); ef[1] += (R)(P.ext_f[1] * fw);
+                                        ef[2] += (R)(P.ext_f[2] * fw);
                                     }
                                 }
 #pragma unroll
@@ -1459,7 +1494,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                 bb[2] < kBin) {
                                 const int scell = bb[0] + kBin * (bb[1] + kBin * bb[2]);
                                 rank = atomicAdd(&Sm.cnt[par][scell], 1);
-                                if (rank < kCellCap) Sm.slot[scell][rank] = (short)slot;
+                                if (rank < kCellCap) Sm.slot[rank][scell] = (short)slot;
                             }
                             if (rank < kCellCap) {
                                 if (EXT) Sm.pay[EXT ? kPay : 0][slot] = P.Tamb + dT;   // absolute T (heat conduction)
@@ -1512,7 +1547,8 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
             }
             if (P2G && !DET) {
                 __syncthreads();
-                cell_accumulate<R, EXT>(Sm, tid & (kCellsPerBin - 1), tid >> 6, P.pmass, par, P.heat_on != 0);
+                cell_accumulate<R, EXT>(Sm, tid & (kCellsPerBin - 1), tid >> 6, (tid >> 5) & 1, P.pmass, par,
+                                        P.heat_on != 0);
                 par ^= 1;
                 __syncthreads();
             }
@@ -1523,13 +1559,15 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
             for (int nidx = tid; nidx < kTileNodes; nidx += kNT) {
                 const int X = nidx % kTile, Y = (nidx / kTile) % kTile, Z = nidx / (kTile * kTile);
                 const int t = tidx(X, Y, Z);
-                const R m = Sm.nacc[0][t], px = Sm.nacc[1][t], py = Sm.nacc[2][t], pz = Sm.nacc[3][t];
-                Sm.nacc[0][t] = R(0); Sm.nacc[1][t] = R(0); Sm.nacc[2][t] = R(0); Sm.nacc[3][t] = R(0);
-                R mT = R(0);
-                if (EXT) {
-                    mT = Sm.nacc[EXT ? 4 : 0][t];
-                    Sm.nacc[EXT ? 4 : 0][t] = R(0);
+                R c[EXT ? 5 : 4];
+#pragma unroll
+                for (int q = 0; q < (EXT ? 5 : 4); ++q) {
+                    c[q] = Sm.nacc[0][q][t] + Sm.nacc[1][q][t];
+                    Sm.nacc[0][q][t] = R(0);
+                    Sm.nacc[1][q][t] = R(0);
                 }
+                const R m = c[0], px = c[1], py = c[2], pz = c[3];
+                const R mT = EXT ? c[EXT ? 4 : 0] : R(0);
                 if (m == R(0)) continue;
                 const int gx = g0x + X, gy = g0y + Y, gz = g0z + Z;
                 if (gx >= P.nx || gy >= P.ny || gz >= P.nz) continue;

@@ -10,6 +10,8 @@ import ctypes as C
 import os
 from pathlib import Path
 
+import numpy as np
+
 # MPM_B200_LIB selects another build of the library (the bounds-checked
 # libmpm_b200_checked.so) before the first call of lib().
 LIB_PATH = Path(os.environ.get("MPM_B200_LIB") or Path(__file__).resolve().parent / "libmpm_b200.so")
@@ -23,6 +25,20 @@ TOOL_NONE, TOOL_RASTER, TOOL_SDF_STICKY, TOOL_SDF_SLIP = 0, 1, 2, 3
 SHAPE_CYLINDER_Y, SHAPE_WEDGE_Y = 0, 1
 PLAST_EXPLICIT, PLAST_NEWTON = 0, 1
 SCHED_SPLIT, SCHED_FUSED = 0, 1
+
+# fields of mpm_import_aos
+AOS_POSITION, AOS_VELOCITY, AOS_TEMPERATURE, AOS_STATUS, AOS_EXT_FORCE = 1, 2, 4, 8, 16
+AOS_WRITABLE = 31
+
+# MPMParticle (the reference's include/Types.h:199-266) as a numpy record, 504 bytes
+MPM_PARTICLE = np.dtype([
+    ("x", "f8"), ("y", "f8"), ("z", "f8"), ("vx", "f8"), ("vy", "f8"), ("vz", "f8"), ("fx", "f8"), ("fy", "f8"),
+    ("fz", "f8"), ("ext_fx", "f8"), ("ext_fy", "f8"), ("ext_fz", "f8"), ("density", "f8"), ("pressure", "f8"),
+    ("volume", "f8"), ("mass", "f8"), ("temperature", "f8"), ("F", "f8", 9), ("F_p", "f8", 9), ("C", "f8", 9),
+    ("stress", "f8", 6), ("backstress", "f8", 6), ("plasticStrain", "f8"), ("strainRate", "f8"), ("damage", "f8"),
+    ("residualStress", "f8"), ("id", "i4"), ("status", "i4"), ("cellHash", "i4"), ("lodZone", "i4"),
+    ("lastUpdateStep", "i4"), ("asbCounter", "u1"), ("_pad", "u1", 3)])
+assert MPM_PARTICLE.itemsize == 504
 
 _d, _i32, _i64, _vp = C.c_double, C.c_int32, C.c_int64, C.c_void_p
 
@@ -57,6 +73,19 @@ class MpmToolDesc(C.Structure):
         ("rake", _d), ("clearance", _d), ("tip_dz", _d), ("n_samples", _i32), ("_pad", _i32),
         ("sample_dx", _vp), ("sample_dy", _vp), ("sample_dz", _vp),
     ]
+
+
+class MpmToolNodes(C.Structure):
+    """mpm_tool_nodes: the raster tool from FEM node records in device memory."""
+    _fields_ = [("start", _vp), ("end", _vp), ("n", _i32), ("stride", _i32), ("off_pos", _i32 * 3),
+                ("off_vel", _i32 * 3), ("alpha0", _d), ("dalpha", _d)]
+
+
+class MpmWorkpieceParams(C.Structure):
+    """mpm_workpiece_params: MPMWorkpieceSolver's own constants."""
+    _fields_ = [("failure_strain", _d), ("critical_plastic_strain", _d), ("thermal_chip_ratio", _d),
+                ("tool_contact_radius", _d), ("contact_damping", _d), ("max_contact_temp_rise", _d),
+                ("thermal_clamp", _i32), ("_pad", _i32)]
 
 
 class MpmParticlesSoa(C.Structure):
@@ -152,6 +181,12 @@ def lib() -> C.CDLL:
             "mpm_upload": (_i32, [_vp, P(MpmParticlesSoa), _i64]),
             "mpm_download": (_i32, [_vp, P(MpmParticlesSoa)]),
             "mpm_export_aos": (_i32, [_vp, _vp, _i64]),
+            "mpm_import_aos": (_i32, [_vp, _vp, _i64, C.c_uint32]),
+            "mpm_set_tool_nodes": (_i32, [_vp, _vp]),
+            "mpm_set_workpiece_semantics": (_i32, [_vp, _vp]),
+            "mpm_batch_set_tool_nodes": (_i32, [_vp, _i32, _vp]),
+            "mpm_batch_export_aos": (_i32, [_vp, _i32, _vp, _i64]),
+            "mpm_batch_import_aos": (_i32, [_vp, _i32, _vp, _i64, C.c_uint32]),
             "mpm_set_tool": (_i32, [_vp, P(MpmToolDesc)]),
             "mpm_set_tool_sdf": (_i32, [_vp, P(MpmToolSdf)]),
             "mpm_batch_set_tool_sdf": (_i32, [_vp, _i32, P(MpmToolSdf)]),
@@ -201,7 +236,13 @@ def lib() -> C.CDLL:
             "mpm_last_error": (C.c_char_p, [_vp]),
             "mpm_status_string": (C.c_char_p, [_i32]),
         }
+        # entry points a library built before them lacks: it still loads, and a
+        # call of one of them raises AttributeError
+        later = {"mpm_import_aos", "mpm_batch_export_aos", "mpm_batch_import_aos", "mpm_set_tool_nodes",
+                 "mpm_batch_set_tool_nodes", "mpm_set_workpiece_semantics"}
         for name, (res, args) in sig.items():
+            if name in later and not hasattr(L, name):
+                continue
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args

@@ -208,6 +208,35 @@ class Solver:
         self._check(self._lib.mpm_export_aos(self.h, buf.ctypes.data_as(C.c_void_p), buf.nbytes))
         return buf[: n * 504]
 
+    def set_workpiece_semantics(self, ws: Optional[dict]) -> None:
+        """mpm_set_workpiece_semantics: MPMWorkpieceSolver's step with its
+        constants (failure_strain, critical_plastic_strain, thermal_chip_ratio,
+        tool_contact_radius, contact_damping, max_contact_temp_rise,
+        thermal_clamp); None returns to MPMSolver's."""
+        if ws is None:
+            self._check(self._lib.mpm_set_workpiece_semantics(self.h, None))
+            return
+        w = A.MpmWorkpieceParams()
+        for k in ("failure_strain", "critical_plastic_strain", "thermal_chip_ratio", "tool_contact_radius",
+                  "contact_damping", "max_contact_temp_rise"):
+            setattr(w, k, float(ws[k]))
+        w.thermal_clamp = int(ws.get("thermal_clamp", 1))
+        self._check(self._lib.mpm_set_workpiece_semantics(self.h, C.byref(w)))
+
+    def export_aos_device(self, ptr: int, nbytes: int) -> None:
+        """mpm_export_aos into device memory at ptr (nbytes >= 504 per particle)."""
+        self._check(self._lib.mpm_export_aos(self.h, C.c_void_p(ptr), int(nbytes)))
+
+    def import_aos(self, src, fields: int = A.AOS_WRITABLE, nbytes: Optional[int] = None) -> None:
+        """mpm_import_aos: reads `fields` (A.AOS_*) of MPMParticle records back
+        into the workpiece.  src: a host uint8/record array, or an int device
+        address with nbytes."""
+        if isinstance(src, np.ndarray):
+            buf = np.ascontiguousarray(src)
+            self._check(self._lib.mpm_import_aos(self.h, buf.ctypes.data_as(C.c_void_p), buf.nbytes, int(fields)))
+        else:
+            self._check(self._lib.mpm_import_aos(self.h, C.c_void_p(int(src)), int(nbytes), int(fields)))
+
     # ---------------------------------------------------------------- stepping
     def step(self, dt: float, nsteps: int = 1) -> None:
         self._check(self._lib.mpm_step(self.h, float(dt), int(nsteps)))

@@ -220,8 +220,70 @@ mpm_status mpm_download(mpm_handle *h, mpm_particles_soa *host);
  * CFD and the exporters.  dst is host or device memory. Synchronises. */
 mpm_status mpm_export_aos(mpm_handle *h, void *dst, int64_t dst_bytes);
 
+/* Fields of an MPMParticle array that mpm_import_aos reads back. */
+enum {
+    MPM_AOS_POSITION = 1,     /* x, y, z */
+    MPM_AOS_VELOCITY = 2,     /* vx, vy, vz */
+    MPM_AOS_TEMPERATURE = 4,  /* temperature */
+    MPM_AOS_STATUS = 8,       /* status (0..4; a record outside that range keeps its status) */
+    MPM_AOS_EXT_FORCE = 16,   /* ext_fx, ext_fy, ext_fz: a body force for the next step only */
+    MPM_AOS_WRITABLE = 31     /* all of the above */
+};
+
+/* The way back from mpm_export_aos.  The reference's consumers of the
+ * particle array write the solver's own d_particles in place:
+ * ContactSolver::resolveContacts (xpbdContactSDFKernel, src/ContactSolver.cu:
+ * 797-923, launched at :1130-1147) moves positions, velocities and
+ * temperatures; CFD chip coupling adds drag to ext_f and cooling to the
+ * temperature (src/CFDSolverGPU.cu:1347-1400, registered at
+ * src/SimulationEngine.cpp:1008-1013).  This reads the `fields` of an array
+ * of n records (n = the workpiece's particles, in upload order, as
+ * mpm_export_aos wrote it; src is host or device memory of at least
+ * n * 504 bytes) back into the workpiece:
+ *   - a position, velocity or temperature equal to what mpm_export_aos would
+ *     write now is left as it is (an unmodified array imports as a no-op, bit
+ *     for bit); moved particles are re-binned before the next step;
+ *   - the external force acts in the next step's P2G on every particle that
+ *     is not INACTIVE, as the reference's p2gKernel adds w * ext_f to the
+ *     node force (src/MPMSolver.cu:410-417), and is then cleared
+ *     (resetExternalForceKernel, :682-688).
+ * Synchronises; MPM_INVALID_ARG when a record's status is outside 0..4
+ * (those records keep their status, the other fields are imported). */
+mpm_status mpm_import_aos(mpm_handle *h, const void *src, int64_t src_bytes, uint32_t fields);
+
 /* Replaces setToolNodes / setToolPosition (include/MPMSolver.cuh:86-89, :171). */
 mpm_status mpm_set_tool(mpm_handle *h, const mpm_tool_desc *tool);
+
+/* The raster tool read straight from the FEM tool's node records in device
+ * memory (the reference's FEMNodeGPU, include/Types.h:316-379, or any record
+ * with double x, y, z and vx, vy, vz fields), as rasterizeToolKernel reads
+ * them (src/MPMSolver.cu:444-473), with the sub-step blend of
+ * interpolateToolNodesKernel (:494-504) done on the device: no host copy of
+ * the nodes and no synchronisation per step. */
+typedef struct mpm_tool_nodes {
+    const void *start;    /* device records at the start of the blended motion, or NULL (no blend) */
+    const void *end;      /* device records the step reads (the current FEM nodes) */
+    int32_t n;            /* records */
+    int32_t stride;       /* bytes from one record to the next (sizeof(FEMNodeGPU)) */
+    int32_t off_pos[3];   /* byte offsets of x, y, z (double) in a record */
+    int32_t off_vel[3];   /* byte offsets of vx, vy, vz (double) */
+    double alpha0;        /* blend weight of the first step after this call */
+    double dalpha;        /* added per step */
+} mpm_tool_nodes;
+
+/* The grid boundary of raster mode from device node records (mode becomes
+ * MPM_TOOL_RASTER; the tool descriptor's pose still drives chip separation
+ * and LOD).  At the j-th step after the call (counted across step calls),
+ * node q sits at end_q when start is NULL, else at start_q + a (end_q -
+ * start_q) with a = alpha0 + j * dalpha; it marks the 2x2x2 grid nodes from
+ * round((x - origin) / dx), and a marked grid node takes the velocity of the
+ * highest-indexed tool node that marks it (the reference's last writer is
+ * whichever thread ran last).  The velocity is end_q's: the reference reads
+ * it from its blend buffer, whose velocity fields interpolateToolNodesKernel
+ * never writes (:494-504).  Both arrays must stay valid and unchanged while
+ * the steps that read them run.  nodes = NULL returns to the descriptor's
+ * sample offsets. */
+mpm_status mpm_set_tool_nodes(mpm_handle *h, const mpm_tool_nodes *nodes);
 
 /*
  * Voxel signed-distance field of the tool for the particle-side contact
@@ -269,6 +331,41 @@ mpm_status mpm_tool_sdf_build(const float *verts, int32_t n_verts, const int32_t
 /* Replaces MPMSolver::step (src/MPMSolver.cu:1062-1168): nsteps steps of dt.
  * Asynchronous on the handle's stream. */
 mpm_status mpm_step(mpm_handle *h, double dt, int32_t nsteps);
+
+/* The constants of the reference's other MPM solver, MPMWorkpieceSolver
+ * (MPMMaterialParams, include/MPMWorkpieceSolver.cuh:60-83), that mpm_params
+ * does not carry. */
+typedef struct mpm_workpiece_params {
+    double failure_strain;           /* damage += rate dt / max(failure_strain, 1e-3) */
+    double critical_plastic_strain;  /* ACTIVE -> CHIP at this plastic strain */
+    double thermal_chip_ratio;       /* ACTIVE -> CHIP at T >= ratio * Tm */
+    double tool_contact_radius;      /* a grid node within this of a tool sample is in contact */
+    double contact_damping;          /* contact heating 0.5 m vn^2 * damping */
+    double max_contact_temp_rise;    /* per-step cap of contact and plastic heating */
+    int32_t thermal_clamp;           /* the cap on (1) or off (0) */
+    int32_t _pad;
+} mpm_workpiece_params;
+
+/* Switches the handle's step to MPMWorkpieceSolver::step
+ * (src/MPMWorkpieceSolver.cu:727-781), the reference's other MPM solver,
+ * which its engine never constructs: trilinear PIC transfers (:52-134,
+ * :264-306), the grid update with the fixture and the nearest-tool-sample
+ * normal projection and contact heating (:136-192), the grid diffusion step
+ * when thermal_conductivity > 0 (:208-262), a hypoelastic stress rate with
+ * the Johnson-Cook radial return at the old plastic strain, kinematic
+ * hardening, strain-rate damage and the CHIP criteria (:308-395), and its
+ * chip separation on even steps (:667-725).  mpm_params supplies the grid,
+ * E and nu, rho_phys (its density), cp, Tm, Tamb (its reference
+ * temperature), the Johnson-Cook constants, edot0, D_th, H_kin, the fixture
+ * thickness and the conductivity; the tool samples of an MPM_TOOL_RASTER
+ * descriptor are its tool samples, at the tool's pose each step; the tool tip
+ * for the chip separation is pose z + tip_dz.  mpm_apply_external_force
+ * takes its form (the whole force on ACTIVE particles within the radius,
+ * :402-413).  The grid stays the handle's (the solver's rebuild of its grid
+ * from the particle bounds is host-side domain management).  NULL returns to
+ * MPMSolver's semantics.  Not with the deterministic mode or a batch of more
+ * than one workpiece. */
+mpm_status mpm_set_workpiece_semantics(mpm_handle *h, const mpm_workpiece_params *params);
 
 /* Replaces getStableTimeStep (src/MPMSolver.cu:1170-1178): cfl*dx/sqrt(E/rho). */
 mpm_status mpm_stable_dt(const mpm_handle *h, double cfl, double *dt);
@@ -332,8 +429,11 @@ mpm_status mpm_batch_init_box(mpm_handle *h, int32_t inst, const int32_t c0[3], 
                               const mpm_tool_desc *tool_at_t0);
 mpm_status mpm_batch_upload(mpm_handle *h, int32_t inst, const mpm_particles_soa *host, int64_t n);
 mpm_status mpm_batch_download(mpm_handle *h, int32_t inst, mpm_particles_soa *host);
+mpm_status mpm_batch_export_aos(mpm_handle *h, int32_t inst, void *dst, int64_t dst_bytes);
+mpm_status mpm_batch_import_aos(mpm_handle *h, int32_t inst, const void *src, int64_t src_bytes, uint32_t fields);
 mpm_status mpm_batch_set_tool(mpm_handle *h, int32_t inst, const mpm_tool_desc *tool);
 mpm_status mpm_batch_set_tool_sdf(mpm_handle *h, int32_t inst, const mpm_tool_sdf *sdf);
+mpm_status mpm_batch_set_tool_nodes(mpm_handle *h, int32_t inst, const mpm_tool_nodes *nodes);
 /* nsteps steps of every instance; dt[i] is instance i's step (n_instances values). */
 mpm_status mpm_batch_step(mpm_handle *h, const double *dt, int32_t nsteps);
 mpm_status mpm_batch_sync_metrics(mpm_handle *h, int32_t inst, mpm_metrics *out);

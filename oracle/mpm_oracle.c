@@ -1020,6 +1020,304 @@ int orc_step(const orc_params *p, orc_state *s, const orc_tool_samples *tool, do
     return err;
 }
 
+/* ------------------------------------------------ MPMWorkpieceSolver semantics */
+
+/* Node channels of the workpiece solver's grid (MPMGridNodeGPU,
+ * include/MPMWorkpieceSolver.cuh:44-55): mass, momentum then velocity,
+ * force, T m, and the node temperature after diffusion. */
+enum { WS_M, WS_VX, WS_VY, WS_VZ, WS_FX, WS_FY, WS_FZ, WS_TM, WS_TN, WS_N };
+
+int64_t orc_ws_grid_doubles(const orc_params *p) { return nnodes(p) * WS_N; }
+
+/* computeWeights (src/MPMWorkpieceSolver.cu:52-90): the 8 trilinear nodes in
+ * dz, dy, dx order; a node outside the grid has index -1 and weight 0. */
+static void ws_weights(const orc_params *p, double x, double y, double z, int64_t id[8], double w[8],
+                       double g[8][3]) {
+    const double rx = (x - p->ox) / p->dx, ry = (y - p->oy) / p->dx, rz = (z - p->oz) / p->dx;
+    const int bx = (int)floor(rx), by = (int)floor(ry), bz = (int)floor(rz);
+    const double fx = rx - bx, fy = ry - by, fz = rz - bz;
+    int n = 0;
+    for (int dz = 0; dz <= 1; ++dz)
+        for (int dy = 0; dy <= 1; ++dy)
+            for (int dx = 0; dx <= 1; ++dx, ++n) {
+                const int i = bx + dx, j = by + dy, k = bz + dz;
+                if (i < 0 || j < 0 || k < 0 || i >= p->nx || j >= p->ny || k >= p->nz) {
+                    id[n] = -1;
+                    w[n] = 0.0;
+                    g[n][0] = g[n][1] = g[n][2] = 0.0;
+                    continue;
+                }
+                const double wx = dx ? fx : 1.0 - fx, wy = dy ? fy : 1.0 - fy, wz = dz ? fz : 1.0 - fz;
+                const double dwx = dx ? 1.0 / p->dx : -1.0 / p->dx;
+                const double dwy = dy ? 1.0 / p->dx : -1.0 / p->dx;
+                const double dwz = dz ? 1.0 / p->dx : -1.0 / p->dx;
+                id[n] = ((int64_t)k * p->ny + j) * p->nx + i;
+                w[n] = wx * wy * wz;
+                g[n][0] = dwx * wy * wz;
+                g[n][1] = wx * dwy * wz;
+                g[n][2] = wx * wy * dwz;
+            }
+}
+
+/* equivalentStress (:19-25). */
+static double ws_eq(double xx, double yy, double zz, double xy, double xz, double yz) {
+    const double s1 = xx - yy, s2 = yy - zz, s3 = zz - xx;
+    return sqrt(0.5 * (s1 * s1 + s2 * s2 + s3 * s3 + 6.0 * (xy * xy + xz * xz + yz * yz)));
+}
+
+/* johnsonCookStress (:43-50): rate term floored at 1, thermal term at 0.01. */
+static double ws_flow(const orc_params *p, double eps, double edot, double T) {
+    const double strain = p->A + p->B * pow(fmax(eps, 0.0), p->n);
+    const double ratio = fmax(edot / fmax(p->edot0, 1e-9), 1.0);
+    const double rate = 1.0 + p->C * log(ratio);
+    const double ts = fmax(0.0, fmin(1.0, (T - p->Tamb) / fmax(p->Tm - p->Tamb, 1.0)));
+    return strain * rate * fmax(0.01, 1.0 - pow(ts, p->m));
+}
+
+/* mpmP2GKernel (:98-134): mass, momentum and T m of every particle that is
+ * not INACTIVE; the stress force (and the particle force) of ACTIVE and
+ * FIXED particles, the particle force alone of CHIP ones. */
+static void ws_p2g(const orc_params *p, const orc_state *s, double *g) {
+    const int64_t nn = nnodes(p);
+    for (int32_t ip = 0; ip < s->n; ++ip) {
+        const int st = s->status[ip];
+        if (st == ORC_INACTIVE) continue;
+        int64_t id[8];
+        double w[8], gr[8][3];
+        ws_weights(p, s->x[ip], s->y[ip], s->z[ip], id, w, gr);
+        const double *sg = s->sig + 6 * (int64_t)ip;
+        const double fp[3] = {s->extf ? s->extf[3 * (int64_t)ip] : 0.0, s->extf ? s->extf[3 * (int64_t)ip + 1] : 0.0,
+                              s->extf ? s->extf[3 * (int64_t)ip + 2] : 0.0};
+        for (int n = 0; n < 8; ++n) {
+            const int64_t gi = id[n];
+            if (gi < 0 || w[n] <= 0.0) continue;
+            const double m = s->mass[ip] * w[n];
+            g[WS_M * nn + gi] += m;
+            g[WS_VX * nn + gi] += s->vx[ip] * m;
+            g[WS_VY * nn + gi] += s->vy[ip] * m;
+            g[WS_VZ * nn + gi] += s->vz[ip] * m;
+            g[WS_TM * nn + gi] += s->T[ip] * m;
+            if (st == ORC_ACTIVE || st == ORC_FIXED) {
+                const double fX = -(sg[0] * gr[n][0] + sg[3] * gr[n][1] + sg[4] * gr[n][2]) * s->vol[ip];
+                const double fY = -(sg[3] * gr[n][0] + sg[1] * gr[n][1] + sg[5] * gr[n][2]) * s->vol[ip];
+                const double fZ = -(sg[4] * gr[n][0] + sg[5] * gr[n][1] + sg[2] * gr[n][2]) * s->vol[ip];
+                g[WS_FX * nn + gi] += fX + fp[0] * w[n];
+                g[WS_FY * nn + gi] += fY + fp[1] * w[n];
+                g[WS_FZ * nn + gi] += fZ + fp[2] * w[n];
+            } else if (st == ORC_CHIP) {
+                g[WS_FX * nn + gi] += fp[0] * w[n];
+                g[WS_FY * nn + gi] += fp[1] * w[n];
+                g[WS_FZ * nn + gi] += fp[2] * w[n];
+            }
+        }
+    }
+}
+
+/* mpmGridUpdateKernel (:136-192): velocity = momentum / mass; nodes at or
+ * below the fixture (z <= min z + thickness + dx) stop; then the force
+ * impulse; then the tool: the nearest sample within the contact radius (the
+ * first of equal ones) gives the normal n = (node - sample) / |.|, and an
+ * approaching normal velocity (v.n < 0) is removed, heating the node by
+ * 0.5 m vn^2 damping / (m cp) (capped with the thermal clamp) and adding
+ * |m vn / dt| to the contact force. */
+static void ws_grid(const orc_params *p, const orc_ws_params *wp, double *g, double dt, const orc_tool_samples *tool,
+                    const double pr[3], double *force) {
+    const int64_t nn = nnodes(p);
+    double fsum = 0.0;
+    for (int64_t idx = 0; idx < nn; ++idx) {
+        const double m = g[WS_M * nn + idx];
+        if (m <= 1e-18) continue;
+        double v[3] = {g[WS_VX * nn + idx] / m, g[WS_VY * nn + idx] / m, g[WS_VZ * nn + idx] / m};
+        const int i = (int)(idx % p->nx);
+        const int64_t t = idx / p->nx;
+        const int j = (int)(t % p->ny), k = (int)(t / p->ny);
+        const double pos[3] = {p->ox + i * p->dx, p->oy + j * p->dx, p->oz + k * p->dx};
+        if (pos[2] <= p->oz + p->fixture_thickness + p->dx) {
+            g[WS_VX * nn + idx] = g[WS_VY * nn + idx] = g[WS_VZ * nn + idx] = 0.0;
+            continue;
+        }
+        v[0] += (g[WS_FX * nn + idx] / m) * dt;
+        v[1] += (g[WS_FY * nn + idx] / m) * dt;
+        v[2] += (g[WS_FZ * nn + idx] / m) * dt;
+        if (tool && tool->n > 0) {
+            double r2 = wp->tool_contact_radius * wp->tool_contact_radius, bn[3] = {0.0, 0.0, 0.0};
+            int hit = 0;
+            for (int q = 0; q < tool->n; ++q) {
+                const double d[3] = {pos[0] - (pr[0] + tool->ox[q]), pos[1] - (pr[1] + tool->oy[q]),
+                                     pos[2] - (pr[2] + tool->oz[q])};
+                const double d2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+                if (d2 < r2 && d2 > 1e-20) {
+                    r2 = d2;
+                    const double len = sqrt(d2);
+                    if (len > 1e-12) { bn[0] = d[0] / len; bn[1] = d[1] / len; bn[2] = d[2] / len; }
+                    else { bn[0] = bn[1] = bn[2] = 0.0; }
+                    hit = 1;
+                }
+            }
+            if (hit) {
+                const double vn = v[0] * bn[0] + v[1] * bn[1] + v[2] * bn[2];
+                if (vn < 0.0) {
+                    fsum += fabs(m * vn / fmax(dt, 1e-15));
+                    for (int a = 0; a < 3; ++a) v[a] -= vn * bn[a];
+                    const double heat = 0.5 * m * vn * vn * wp->contact_damping;
+                    double dT = heat / fmax(m * p->cp, 1e-12);
+                    if (wp->thermal_clamp) dT = fmin(dT, wp->max_contact_temp_rise);
+                    g[WS_TM * nn + idx] += dT * m;
+                }
+            }
+        }
+        g[WS_VX * nn + idx] = v[0];
+        g[WS_VY * nn + idx] = v[1];
+        g[WS_VZ * nn + idx] = v[2];
+    }
+    if (force) *force = fsum;
+}
+
+/* mpmG2PKernel (:264-400) on every particle that is not INACTIVE. */
+static void ws_g2p(const orc_params *p, const orc_ws_params *wp, orc_state *s, const double *g, double dt,
+                   int diffused) {
+    const int64_t nn = nnodes(p);
+    const double G = p->E / (2.0 * (1.0 + p->nu)), K = p->E / (3.0 * (1.0 - 2.0 * p->nu));
+    for (int32_t ip = 0; ip < s->n; ++ip) {
+        const int st = s->status[ip];
+        if (st == ORC_INACTIVE) continue;
+        int64_t id[8];
+        double w[8], gr[8][3];
+        ws_weights(p, s->x[ip], s->y[ip], s->z[ip], id, w, gr);
+        double v[3] = {0.0, 0.0, 0.0}, temp = 0.0, wsum = 0.0, L[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        for (int n = 0; n < 8; ++n) {
+            const int64_t gi = id[n];
+            if (gi < 0 || w[n] <= 0.0) continue;
+            const double m = g[WS_M * nn + gi];
+            if (m <= 1e-18) continue;
+            const double nv[3] = {g[WS_VX * nn + gi], g[WS_VY * nn + gi], g[WS_VZ * nn + gi]};
+            for (int a = 0; a < 3; ++a) v[a] += nv[a] * w[n];
+            temp += (diffused ? g[WS_TN * nn + gi] : g[WS_TM * nn + gi] / m) * w[n];
+            wsum += w[n];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) L[a][b] += nv[a] * gr[n][b];
+        }
+        double *ext = s->extf ? s->extf + 3 * (int64_t)ip : NULL;
+        if (st == ORC_FIXED) {
+            s->vx[ip] = s->vy[ip] = s->vz[ip] = 0.0;
+            if (ext) ext[0] = ext[1] = ext[2] = 0.0;
+            continue;
+        }
+        s->vx[ip] = v[0]; s->vy[ip] = v[1]; s->vz[ip] = v[2];
+        s->x[ip] += v[0] * dt;
+        s->y[ip] += v[1] * dt;
+        s->z[ip] += v[2] * dt;
+        if (wsum > 1e-8) s->T[ip] = fmin(fmax(temp / wsum, p->Tamb), p->Tm);
+        double *sg = s->sig + 6 * (int64_t)ip, *bs = s->bs + 6 * (int64_t)ip;
+        if (st == ORC_ACTIVE) {
+            const double Dxx = L[0][0], Dyy = L[1][1], Dzz = L[2][2];
+            const double Dxy = 0.5 * (L[0][1] + L[1][0]), Dxz = 0.5 * (L[0][2] + L[2][0]),
+                         Dyz = 0.5 * (L[1][2] + L[2][1]);
+            const double tr = Dxx + Dyy + Dzz;
+            const double dxx = Dxx - tr / 3.0, dyy = Dyy - tr / 3.0, dzz = Dzz - tr / 3.0;
+            const double rate = sqrt(2.0 / 3.0 * (dxx * dxx + dyy * dyy + dzz * dzz +
+                                                   2.0 * (Dxy * Dxy + Dxz * Dxz + Dyz * Dyz)));
+            s->edot[ip] = rate;
+            const double pinc = K * tr * dt;
+            sg[0] += (2.0 * G * dxx) * dt + pinc;
+            sg[1] += (2.0 * G * dyy) * dt + pinc;
+            sg[2] += (2.0 * G * dzz) * dt + pinc;
+            sg[3] += 2.0 * G * Dxy * dt;
+            sg[4] += 2.0 * G * Dxz * dt;
+            sg[5] += 2.0 * G * Dyz * dt;
+            const double sh[6] = {sg[0] - bs[0], sg[1] - bs[1], sg[2] - bs[2], sg[3] - bs[3], sg[4] - bs[4],
+                                  sg[5] - bs[5]};
+            const double seq = ws_eq(sh[0], sh[1], sh[2], sh[3], sh[4], sh[5]);
+            const double flow = ws_flow(p, s->eps[ip], s->edot[ip], s->T[ip]);
+            if (seq > flow && seq > 1e-9) {
+                const double sc = flow / seq;
+                for (int q = 0; q < 6; ++q) sg[q] = bs[q] + sc * sh[q];
+                const double dp = (seq - flow) / fmax(3.0 * G, 1.0);
+                if (p->Hkin > 0.0 && dp > 0.0) {
+                    const double ns = p->Hkin * dp / seq;
+                    for (int q = 0; q < 6; ++q) bs[q] += ns * sh[q];
+                }
+                s->eps[ip] += dp;
+                double dT = 0.9 * flow * dp / fmax(p->rho_phys * p->cp, 1.0);
+                if (wp->thermal_clamp) dT = fmin(dT, wp->max_contact_temp_rise);
+                s->T[ip] = fmin(s->T[ip] + dT, p->Tm);
+            }
+            if (rate > 0.0) s->D[ip] += (rate * dt) / fmax(wp->failure_strain, 1e-3);
+            if (s->D[ip] > 0.7 * p->Dth && s->D[ip] < p->Dth) {
+                const double dg = fmax(0.0, (p->Dth - s->D[ip]) / (p->Dth * 0.3));
+                for (int q = 0; q < 6; ++q) { sg[q] *= dg; bs[q] *= dg; }
+                s->sres[ip] = fmax(s->sres[ip], ws_eq(sg[0], sg[1], sg[2], sg[3], sg[4], sg[5]));
+            }
+        }
+        if (st == ORC_ACTIVE && (s->D[ip] >= p->Dth || s->eps[ip] >= wp->critical_plastic_strain ||
+                                 s->T[ip] >= p->Tm * wp->thermal_chip_ratio)) {
+            s->status[ip] = ORC_CHIP;
+            s->sres[ip] = fmax(s->sres[ip], ws_eq(sg[0], sg[1], sg[2], sg[3], sg[4], sg[5]));
+            for (int q = 0; q < 6; ++q) { sg[q] = 0.0; bs[q] = 0.0; }
+            s->D[ip] = fmax(s->D[ip], p->Dth);
+        }
+        if (ext) ext[0] = ext[1] = ext[2] = 0.0;
+    }
+}
+
+/* The workpiece solver's chipFractureAndSeparationKernel (:667-725):
+ * ACTIVE particles below tip z - 1.5 dx with any plastic strain become
+ * CHIP; CHIP particles at 1.5 Dth of damage get the id-seeded push and
+ * damage 0.5 Dth. */
+static void ws_chip(const orc_params *p, orc_state *s, double tipZ) {
+    for (int32_t ip = 0; ip < s->n; ++ip) {
+        const int st = s->status[ip];
+        if (st == ORC_INACTIVE) continue;
+        double *sg = s->sig + 6 * (int64_t)ip, *bs = s->bs + 6 * (int64_t)ip;
+        if (st == ORC_ACTIVE) {
+            if (s->z[ip] < tipZ - p->dx * 1.5 && s->eps[ip] > 1e-6) {
+                s->status[ip] = ORC_CHIP;
+                s->sres[ip] = fmax(s->sres[ip], sqrt(sg[0] * sg[0] + sg[1] * sg[1] + sg[2] * sg[2]));
+                for (int q = 0; q < 6; ++q) { sg[q] = 0.0; bs[q] = 0.0; }
+                s->D[ip] = fmax(s->D[ip], p->Dth);
+            }
+            continue;
+        }
+        if (st == ORC_CHIP) {
+            if (s->D[ip] < p->Dth * 1.5) continue;
+            const uint32_t seed = (uint32_t)s->id[ip] * 2654435761u;
+            const double rx = (double)((seed >> 16) & 0xFF) / 255.0 - 0.5;
+            const double ry = (double)((seed >> 8) & 0xFF) / 255.0 - 0.5;
+            const double rz = (double)(seed & 0xFF) / 255.0 - 0.5;
+            const double sp = sqrt(s->vx[ip] * s->vx[ip] + s->vy[ip] * s->vy[ip] + s->vz[ip] * s->vz[ip]);
+            const double pm = sp * 0.3 + 0.5;
+            s->vx[ip] += rx * pm;
+            s->vy[ip] += ry * pm;
+            s->vz[ip] += rz * pm;
+            s->D[ip] = p->Dth * 0.5;
+        }
+    }
+}
+
+/* The node-temperature step of the workpiece solver: diffusion (WS_TM ->
+ * WS_TN) through the common restatement. */
+static void ws_diffuse(const orc_params *p, double *g, double dt) {
+    const int64_t nn = nnodes(p);
+    orc_heat_diffuse(p, g + WS_M * nn, g + WS_TM * nn, g + WS_TN * nn, dt);
+}
+
+void orc_ws_step(const orc_params *p, const orc_ws_params *w, orc_state *s, const orc_tool_samples *tool, double *grid,
+                 double dt, int32_t nsteps, int64_t step0, double t0, double *contact_force) {
+    const int64_t ng = orc_ws_grid_doubles(p);
+    const int diffuse = p->cp > 0.0 && p->thermal_conductivity / (p->rho_phys * p->cp) > 0.0;
+    for (int32_t k = 0; k < nsteps; ++k) {
+        const double t = t0 + (double)k * dt;
+        double pr[3];
+        for (int d = 0; d < 3; ++d) pr[d] = p->tool_p0[d] + p->tool_v[d] * t;
+        memset(grid, 0, sizeof(double) * (size_t)ng);
+        ws_p2g(p, s, grid);
+        ws_grid(p, w, grid, dt, tool, pr, contact_force);
+        if (diffuse) ws_diffuse(p, grid, dt);
+        ws_g2p(p, w, s, grid, dt, diffuse);
+        if (((step0 + k) % 2) == 0) ws_chip(p, s, pr[2] + p->tool_tip_dz);
+    }
+}
+
 /* ---------------------------------------------------------------- metrics */
 
 /* Reference-compatible stats: computeParticleStatsKernel (:729-788) over

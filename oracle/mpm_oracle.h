@@ -193,6 +193,42 @@ int orc_step(const orc_params *p, orc_state *s, const orc_tool_samples *tool,
              double *grid, double dt, int32_t nsteps, int64_t step0, double t0,
              int32_t nthreads);
 
+/* The other MPM solver of the reference, MPMWorkpieceSolver
+ * (src/MPMWorkpieceSolver.cu), which the engine never constructs: trilinear
+ * PIC transfers, a hypoelastic stress rate with a Johnson-Cook radial return
+ * at the old plastic strain, and a tool boundary that projects out the
+ * approaching normal velocity at the nearest tool sample.  Its own constants
+ * (MPMMaterialParams, include/MPMWorkpieceSolver.cuh:60-83) beside orc_params,
+ * which gives the grid, E and nu (shear and bulk moduli), rho_phys (its
+ * density), cp, Tm, Tamb (its reference temperature), A, B, n, C, m, edot0,
+ * Dth, Hkin, the fixture thickness and the thermal conductivity. */
+typedef struct orc_ws_params {
+    double failure_strain;           /* damage += eqRate dt / max(failure_strain, 1e-3) */
+    double critical_plastic_strain;  /* ACTIVE -> CHIP at eps >= this */
+    double thermal_chip_ratio;       /* ACTIVE -> CHIP at T >= ratio * Tm */
+    double tool_contact_radius;      /* a node within this of a tool sample is in contact */
+    double contact_damping;          /* heating of a contact: 0.5 m vn^2 * damping */
+    double max_contact_temp_rise;    /* per-step cap of contact and plastic heating (thermal clamp) */
+    int32_t thermal_clamp;
+    int32_t _pad;
+} orc_ws_params;
+
+/* Node arrays of one MPMWorkpieceSolver step, for the contact force it sums:
+ * *contact_force (may be NULL) receives the last step's sum of
+ * |m vn / dt| over the contact nodes (mpmGridUpdateKernel's totalContactForce). */
+int64_t orc_ws_grid_doubles(const orc_params *p);
+
+/* Advance nsteps steps of MPMWorkpieceSolver::step (src/MPMWorkpieceSolver.cu:
+ * 727-781) on the fixed grid of p: clear, mpmP2GKernel, mpmGridUpdateKernel
+ * with the tool samples at pose p0 + v t (offsets in tool), the diffusion
+ * step when k / (rho cp) > 0 (Jacobi, as orc_heat_diffuse), mpmG2PKernel, and
+ * on even step counts its chipFractureAndSeparationKernel with the tool tip
+ * z = pose z + tool_tip_dz.  s->extf, when set, is the particles' force
+ * (MPMParticleGPU::f), applied in the first step and then zeroed as
+ * mpmG2PKernel does; s->bs is the backstress. */
+void orc_ws_step(const orc_params *p, const orc_ws_params *w, orc_state *s, const orc_tool_samples *tool, double *grid,
+                 double dt, int32_t nsteps, int64_t step0, double t0, double *contact_force);
+
 /* Tool SDF at a world point for the tool reference point pr. */
 double orc_tool_sdf(const orc_params *p, const double pr[3], double x, double y, double z);
 

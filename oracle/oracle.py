@@ -83,6 +83,22 @@ def contact_args(a: dict) -> OrcContactArgs:
     return o
 
 
+class OrcWsParams(C.Structure):
+    """orc_ws_params: MPMWorkpieceSolver's own constants."""
+    _fields_ = [("failure_strain", _d), ("critical_plastic_strain", _d), ("thermal_chip_ratio", _d),
+                ("tool_contact_radius", _d), ("contact_damping", _d), ("max_contact_temp_rise", _d),
+                ("thermal_clamp", _i32), ("_pad", _i32)]
+
+
+def ws_params(w: dict) -> OrcWsParams:
+    o = OrcWsParams()
+    for k in ("failure_strain", "critical_plastic_strain", "thermal_chip_ratio", "tool_contact_radius",
+              "contact_damping", "max_contact_temp_rise"):
+        setattr(o, k, float(w[k]))
+    o.thermal_clamp = int(w.get("thermal_clamp", 1))
+    return o
+
+
 class OrcTool(C.Structure):
     _fields_ = [("n", _i32), ("_pad", _i32), ("ox", _vp), ("oy", _vp), ("oz", _vp)]
 
@@ -223,6 +239,11 @@ class Oracle:
         L.orc_tool_sdf_build.restype = _i32
         L.orc_tool_sdf_build.argtypes = [_vp, _i32, _vp, _i32, _vp, _d, _i32, C.POINTER(_i32 * 3),
                                          C.POINTER(C.c_float * 3), C.POINTER(C.c_float), _vp]
+        L.orc_ws_grid_doubles.restype = _i64
+        L.orc_ws_grid_doubles.argtypes = [C.POINTER(OrcParams)]
+        L.orc_ws_step.restype = None
+        L.orc_ws_step.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcWsParams), C.POINTER(OrcState),
+                                  C.POINTER(OrcTool), C.POINTER(_d), _d, _i32, _i64, _d, C.POINTER(_d)]
         L.orc_contact_sdf.restype = None
         L.orc_contact_sdf.argtypes = [C.POINTER(OrcSdfGrid), C.POINTER(OrcContactArgs), C.POINTER(OrcState),
                                       C.POINTER(_i64), C.POINTER(_d), C.POINTER(_d)]
@@ -237,6 +258,23 @@ class Oracle:
                              grid.ctypes.data_as(C.POINTER(_d)), float(dt if dt is not None else case["dt"]),
                              int(nsteps), int(step0), float(t0), int(nthreads))
         return b.result(), rc
+
+    def ws_step(self, case: dict, state: Dict[str, np.ndarray], nsteps: int, step0: int = 0, t0: float = 0.0,
+                extf: Optional[np.ndarray] = None):
+        """nsteps of MPMWorkpieceSolver's step (case["ws"]: its constants):
+        (state after, contact force of the last step)."""
+        p = orc_params(case)
+        w = ws_params(case["ws"])
+        b = _Bound(case, state, extf)
+        grid = np.zeros(int(self.L.orc_ws_grid_doubles(C.byref(p))), dtype=np.float64)
+        f = _d()
+        self.L.orc_ws_step(C.byref(p), C.byref(w), C.byref(b.state), C.byref(b.tool),
+                           grid.ctypes.data_as(C.POINTER(_d)), float(case["dt"]), int(nsteps), int(step0), float(t0),
+                           C.byref(f))
+        out = b.result()
+        if extf is not None:
+            out["extf"] = b.arrs["extf"]
+        return out, f.value
 
     def asb_heat(self, case: dict, state: Dict[str, np.ndarray], dt: float) -> Dict[str, np.ndarray]:
         """One adiabatic shear heating pass (no grid step)."""
@@ -321,12 +359,18 @@ class RefKern:
         L.ref_heat_diffuse.restype = _i32
         L.ref_heat_diffuse.argtypes = [C.POINTER(OrcParams), C.POINTER(_d), C.POINTER(_d), _d]
         L.ref_heat_last_error.restype = C.c_char_p
+        L.ref_ws_run.restype = _i32
+        L.ref_ws_run.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcWsParams), C.POINTER(OrcState),
+                                 C.POINTER(OrcTool), _d, _i32, C.c_longlong, _d, C.POINTER(_d)]
         L.ref_contact_last_error.restype = C.c_char_p
         L.ref_tex_probe.restype = _i32
         L.ref_tex_probe.argtypes = [C.POINTER(OrcSdfGrid), _vp, _i32, _vp]
         L.ref_contact_sdf.restype = _i32
         L.ref_contact_sdf.argtypes = [C.POINTER(OrcSdfGrid), C.POINTER(OrcContactArgs), C.POINTER(OrcState),
                                       C.POINTER(_i64), C.POINTER(_d), C.POINTER(_d)]
+        L.ref_contact_sdf_device.restype = _i32
+        L.ref_contact_sdf_device.argtypes = [C.POINTER(OrcSdfGrid), C.POINTER(OrcContactArgs), _vp, _i32,
+                                             C.POINTER(_i64), C.POINTER(_d), C.POINTER(_d)]
         L.ref_bench.restype = _i32
         L.ref_bench.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcState), C.POINTER(OrcTool), _d, _i32, _i32,
                                 C.POINTER(_d)]
@@ -353,6 +397,23 @@ class RefKern:
         if rc != 0:
             raise RuntimeError(f"reference shear pass failed ({rc}): {self.L.ref_last_error().decode()}")
         return b.result()
+
+    def ws_step(self, case: dict, state: Dict[str, np.ndarray], nsteps: int, step0: int = 0, t0: float = 0.0,
+                extf: Optional[np.ndarray] = None):
+        """The reference's MPMWorkpieceSolver kernels for nsteps steps:
+        (state after, contact force of the last step)."""
+        p = orc_params(case)
+        w = ws_params(case["ws"])
+        b = _Bound(case, state, extf)
+        f = _d()
+        rc = self.L.ref_ws_run(C.byref(p), C.byref(w), C.byref(b.state), C.byref(b.tool), float(case["dt"]),
+                               int(nsteps), int(step0), float(t0), C.byref(f))
+        if rc != 0:
+            raise RuntimeError(f"reference workpiece-solver run failed: {self.L.ref_heat_last_error().decode()}")
+        out = b.result()
+        if extf is not None:
+            out["extf"] = b.arrs["extf"]
+        return out, f.value
 
     def heat_diffuse(self, case: dict, mass: np.ndarray, tm: np.ndarray, dt: float) -> np.ndarray:
         """The reference's mpmDiffuseTemperatureKernel once: returns its new T m."""
@@ -386,6 +447,18 @@ class RefKern:
         if rc != 0:
             raise RuntimeError(self.L.ref_contact_last_error().decode())
         return b.result(), (cnt.value, heat.value, force.value)
+
+    def contact_sdf_device(self, sdf: dict, args: dict, d_particles: int, n: int):
+        """The reference's xpbdContactSDFKernel once, in place on n MPMParticle
+        records at device address d_particles: (count, friction work, normal force)."""
+        g, keep = sdf_grid(sdf)
+        a = contact_args(args)
+        cnt, heat, force = _i64(), _d(), _d()
+        rc = self.L.ref_contact_sdf_device(C.byref(g), C.byref(a), C.c_void_p(int(d_particles)), int(n),
+                                           C.byref(cnt), C.byref(heat), C.byref(force))
+        if rc != 0:
+            raise RuntimeError(self.L.ref_contact_last_error().decode())
+        return cnt.value, heat.value, force.value
 
     def stats(self, case: dict, state: Dict[str, np.ndarray]) -> np.ndarray:
         b = _Bound(case, state)

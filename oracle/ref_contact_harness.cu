@@ -140,4 +140,43 @@ int ref_contact_sdf(const orc_sdf_grid* g, const orc_contact_sdf_args* a, orc_st
     return 0;
 }
 
+// One launch of xpbdContactSDFKernel on n MPMParticle records already in
+// device memory (d_particles), updated in place: the reference's contact
+// pass run on an array another solver handed out (ContactSolver::
+// resolveContacts launches it on MPMSolver::getDeviceParticles(),
+// src/ContactSolver.cu:1130-1147).
+int ref_contact_sdf_device(const orc_sdf_grid* g, const orc_contact_sdf_args* a, void* d_particles, int n,
+                           int64_t* count, double* heat, double* force) {
+    using namespace edgepredict;
+    SdfTexture t;
+    cudaError_t e = t.create(g);
+    if (e != cudaSuccess) return fail("texture", e);
+    int* d_cnt = nullptr;
+    double* d_sum = nullptr;
+    e = cudaMalloc(&d_cnt, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&d_sum, 2 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(d_cnt, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(d_sum, 0, 2 * sizeof(double));
+    if (e == cudaSuccess && n > 0) {
+        xpbdContactSDFKernel<<<(n + 255) / 256, 256>>>(
+            static_cast<MPMParticle*>(d_particles), n, t.tex, make_float3(g->ox, g->oy, g->oz), g->voxel,
+            make_int3(g->nx, g->ny, g->nz), a->cx, a->cy, a->cz, a->cos_a, a->sin_a, a->radius, a->friction,
+            a->heat_partition, a->dt, a->cp, a->rho_phys, a->Tm, 0.0, false, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 1.0,
+            d_cnt, d_sum, d_sum + 1);
+        e = cudaGetLastError();
+    }
+    int cnt = 0;
+    double sums[2] = {0.0, 0.0};
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(&cnt, d_cnt, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(sums, d_sum, 2 * sizeof(double), cudaMemcpyDeviceToHost);
+    if (d_cnt) cudaFree(d_cnt);
+    if (d_sum) cudaFree(d_sum);
+    if (e != cudaSuccess) return fail("contact (device array)", e);
+    *count = cnt;
+    *heat = sums[0];
+    *force = sums[1];
+    return 0;
+}
+
 }  // extern "C"

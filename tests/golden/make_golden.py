@@ -28,6 +28,10 @@ crafted grid (heat_pass_inputs); written when no scenario is named or when
 "heat_pass" is.  The kernel updates the grid in place, so in general its result
 depends on the thread schedule; on this grid every node it updates (mass >=
 1e-15) has only neighbours it never updates, so the result is deterministic.
+
+workpiece_solver.npz holds the reference's MPMWorkpieceSolver kernels
+(src/MPMWorkpieceSolver.cu) stepped on the scenario of that name
+(scenarios.WS_SCENARIOS); written when no scenario is named or when it is.
 """
 from __future__ import annotations
 
@@ -43,7 +47,7 @@ sys.path.insert(0, str(HERE.parents[1]))
 sys.path.insert(0, str(HERE))
 
 from oracle.oracle import RefKern  # noqa: E402
-from scenarios import SCENARIOS  # noqa: E402
+from scenarios import SCENARIOS, WS_SCENARIOS  # noqa: E402
 
 FIELDS = ("x", "y", "z", "vx", "vy", "vz", "F", "Fp", "C", "stress", "backstress", "plastic_strain", "strain_rate",
           "temperature", "damage", "residual_stress", "status", "id", "asb")
@@ -200,6 +204,30 @@ def write_asb_pass(rk, outdir: Path) -> None:
     print(f"asb_pass: n={len(st['status'])} heated={moved} counters changed={int((out['asb'] != st['asb']).sum())}")
 
 
+WS_FIELDS = ("x", "y", "z", "vx", "vy", "vz", "stress", "backstress", "plastic_strain", "strain_rate", "temperature",
+             "damage", "residual_stress", "status", "id")
+
+
+def write_ws(rk, outdir: Path, name: str, fn) -> None:
+    """The reference's MPMWorkpieceSolver kernels on a scenario: input and
+    output state, the last step's contact force, the run-to-run spread."""
+    case, st, n, extf = fn()
+    out1, f1 = rk.ws_step(case, st, n, extf=extf.copy())
+    out2, f2 = rk.ws_step(case, st, n, extf=extf.copy())
+    spread = {k: float(np.abs(out1[k].astype(float) - out2[k].astype(float)).max()) for k in WS_FIELDS}
+    arrays = {f"in_{k}": np.asarray(st[k]) for k in WS_FIELDS}
+    arrays.update({f"out_{k}": np.asarray(out1[k]) for k in WS_FIELDS})
+    arrays["extf"] = extf
+    arrays["contact_force"] = np.array([f1, f2])
+    meta = {"nsteps": n, "spread": spread}
+    arrays["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
+    (outdir / "workpiece").mkdir(parents=True, exist_ok=True)
+    np.savez_compressed(outdir / "workpiece" / f"{name}.npz", **arrays)
+    print(f"{name}: n={len(st['x'])} steps={n} chips={int((out1['status'] == 2).sum())} "
+          f"max_eps={out1['plastic_strain'].max():.3e} max_D={out1['damage'].max():.3e} "
+          f"contact_force={f1:.3e} spread_x={spread['x']:.2e}")
+
+
 def main(outdir: Path, names=None) -> None:
     rk = RefKern()
     outdir.mkdir(parents=True, exist_ok=True)
@@ -209,6 +237,9 @@ def main(outdir: Path, names=None) -> None:
         write_heat_pass(rk, outdir)
     if not names or "contact_pass" in names:
         write_contact_pass(rk, outdir)
+    for name, fn in WS_SCENARIOS.items():
+        if not names or name in names:
+            write_ws(rk, outdir, name, fn)
     for name, fn in SCENARIOS.items():
         if names and name not in names:
             continue

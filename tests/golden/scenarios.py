@@ -139,6 +139,40 @@ def heat_conduction():
     return case, st, n, None
 
 
+def workpiece_solver():
+    """MPMWorkpieceSolver's semantics (src/MPMWorkpieceSolver.cu:98-400,
+    :667-725): trilinear PIC, hypoelastic stress with the Johnson-Cook return
+    at the old plastic strain, nearest-sample normal projection with contact
+    heating.  The soft plastic_damage_chip workpiece flies at -30 m/s in x
+    (with noise) into the cylinder's surface samples, so that nodes meet the
+    tool with an approaching normal velocity; kinematic hardening; a particle
+    force on a tenth of the particles; damage from the strain rate (failure
+    strain 0.005, threshold 1) reaching degradation and CHIP, and chip
+    separation on even steps.  Conduction off (k = 0): the reference's diffusion updates its grid
+    in place, so its result depends on the thread schedule; the diffusion is
+    pinned on its own (kernels/heat_diffusion.npz)."""
+    case, st, n, _ = plastic_damage_chip()
+    p = case["params"]
+    p.update(H_kin=2e9, thermal_conductivity=0.0, D_th=1.0)
+    case["ws"] = dict(failure_strain=0.005, critical_plastic_strain=0.3, thermal_chip_ratio=0.98,
+                      tool_contact_radius=1.5 * p["dx"], contact_damping=0.15, max_contact_temp_rise=25.0,
+                      thermal_clamp=1)
+    rng = np.random.default_rng(29)
+    nn = len(st["x"])
+    st["vx"] = -30.0 + rng.normal(0.0, 2.0, nn)
+    st["vy"] = rng.normal(0.0, 2.0, nn)
+    st["vz"] = rng.normal(0.0, 2.0, nn)
+    pick = rng.uniform(0, 1, nn) < 0.1
+    extf = np.zeros((nn, 3))
+    extf[pick] = rng.normal(0.0, 2e-4, (int(pick.sum()), 3))
+    return case, st, 16, extf
+
+
+# MPMWorkpieceSolver's semantics (the reference's other MPM solver).
+WS_SCENARIOS = {
+    "workpiece_solver": workpiece_solver,
+}
+
 SCENARIOS = {
     "elastic_raster": elastic_raster,
     "plastic_damage_chip": plastic_damage_chip,

@@ -12,14 +12,7 @@ from mpm_b200 import Solver, capi as A, workpiece as W
 pytestmark = pytest.mark.gpu
 
 # MPMParticle (include/Types.h:199-266) as a numpy record, 504 bytes
-AOS = np.dtype([
-    ("x", "f8"), ("y", "f8"), ("z", "f8"), ("vx", "f8"), ("vy", "f8"), ("vz", "f8"), ("fx", "f8"), ("fy", "f8"),
-    ("fz", "f8"), ("ext_fx", "f8"), ("ext_fy", "f8"), ("ext_fz", "f8"), ("density", "f8"), ("pressure", "f8"),
-    ("volume", "f8"), ("mass", "f8"), ("temperature", "f8"), ("F", "f8", 9), ("F_p", "f8", 9), ("C", "f8", 9),
-    ("stress", "f8", 6), ("backstress", "f8", 6), ("plasticStrain", "f8"), ("strainRate", "f8"), ("damage", "f8"),
-    ("residualStress", "f8"), ("id", "i4"), ("status", "i4"), ("cellHash", "i4"), ("lodZone", "i4"),
-    ("lastUpdateStep", "i4"), ("asbCounter", "u1"), ("_pad", "u1", 3)])
-assert AOS.itemsize == 504
+AOS = A.MPM_PARTICLE
 
 
 def small_case(**kw):
