@@ -6,8 +6,6 @@
 #include <algorithm>
 #include <cuda_runtime.h>
 
-#include <cub/device/device_radix_sort.cuh>
-
 #include "mpm_device.cuh"
 #include "mpm_internal.h"
 
@@ -166,16 +164,28 @@ void build_work(const int32_t* offset, const int32_t* bin_key, const int32_t* bi
 // Key of every particle: instance key base + bin*64 + cell within the bin,
 // where the cell is the stencil base node; INACTIVE particles take the
 // instance's sentinel key (after all bins).  rank = arrival order in the key.
+// An instance that keeps its layout at this re-bin (keep_all, or not due at
+// point kpt of its re-bin phase) takes the keys its particles were placed
+// under (skey), so that the move leaves every particle of it in its slot.
 template <typename R>
 __global__ void k_bin_count(const Inst<R>* insts, int n_inst, PState<R> ps, const int32_t* key_base, bool initial,
                             const double* pos_scratch, int32_t* key, int32_t* rank, int32_t* count, int32_t* newbin,
-                            int64_t np) {
+                            int64_t np, int kpt, int sort_every, bool keep_all) {
     const int64_t pi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pi >= np) return;
     const int ii = find_inst(insts, n_inst, pi);
     const Inst<R>& P = insts[ii];
     if (pi >= P.pbase + P.np) return;  // unused slot of the instance
     const bool fresh = initial && P.fresh;
+    const bool due = kpt < 0 || (kpt >= P.rebin_first && (kpt - P.rebin_first) % sort_every == 0);
+    const int32_t sk = ps.skey[pi];
+    if (!fresh && !P.rebin_now && (keep_all || !due) && sk >= 0) {
+        const int32_t kk = key_base[ii] + sk;
+        key[pi] = kk;
+        newbin[pi] = sk < P.nbins * kCellsPerBin ? sk / kCellsPerBin : ps.bin[pi];
+        rank[pi] = atomicAdd(&count[kk], 1);
+        return;
+    }
     int b[3];
     if (fresh) {
         for (int a = 0; a < 3; ++a) {
@@ -245,15 +255,12 @@ __device__ __forceinline__ int64_t column_slot(const int32_t* __restrict__ cs, i
 template <typename R>
 __device__ __forceinline__ int64_t bin_dest(const Inst<R>& P, int ii, int64_t pi, const int32_t* key,
                                             const int32_t* rank, const int32_t* offset, const int32_t* key_base,
-                                            const int32_t* newbin, bool det) {
+                                            const int32_t* newbin) {
     if (pi >= P.pbase + P.np) return -1;
     const int32_t kk = key[pi];
     if (kk - key_base[ii] >= P.nbins * kCellsPerBin) return offset[kk] + rank[pi];  // INACTIVE: after the bins
     const int32_t fk = key_base[ii] + newbin[pi] * kCellsPerBin;
-    const int64_t b0 = offset[fk];
-    // deterministic mode keeps each cell's particles together, in rank order
-    if (det) return b0 + (int64_t)(offset[kk] - b0) + rank[pi];
-    return b0 + column_slot(offset + fk, kk - fk, rank[pi]);
+    return offset[fk] + column_slot(offset + fk, kk - fk, rank[pi]);
 }
 
 // The re-bin's move, in two launches so that the writes are coalesced: the
@@ -265,18 +272,86 @@ __device__ __forceinline__ int64_t bin_dest(const Inst<R>& P, int ii, int64_t pi
 template <typename R>
 __global__ void k_bin_perm(const Inst<R>* insts, int n_inst, const int32_t* key, const int32_t* rank,
                            const int32_t* offset, const int32_t* key_base, const int32_t* newbin, int32_t* perm,
-                           int64_t np, bool det) {
+                           int64_t np) {
     const int64_t pi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pi >= np) return;
     const int ii = find_inst(insts, n_inst, pi);
-    const int64_t d = bin_dest(insts[ii], ii, pi, key, rank, offset, key_base, newbin, det);
+    const int64_t d = bin_dest(insts[ii], ii, pi, key, rank, offset, key_base, newbin);
     if (d >= 0) perm[d] = (int32_t)pi;
+}
+
+// The ranks of k_bin_count follow the atomics' arrival order.  One CTA per
+// bin of the bin table puts each cell's particles in the order of their
+// upload positions (orig): thread c takes the destinations of cell c (rank
+// order) and hands them the cell's sources sorted by orig.  The layout -- and
+// with it the order of every sum the step kernel forms -- then depends on the
+// particles' positions and upload order alone, not on the thread schedule or
+// the layout before (so re-binning a freshly binned state changes nothing).
+// Cells of up to kOrderLocal particles sort in registers and local memory; a
+// larger one (a cell packed several times over its particles per cell) takes
+// a selection sort through global memory.
+constexpr int kOrderLocal = 48;
+
+__device__ __forceinline__ int64_t order_dest(const int32_t* cs, int c, int r, int64_t b0) {
+    return b0 + column_slot(cs, c, r);
+}
+
+__global__ void __launch_bounds__(kCellsPerBin) k_bin_order(const int32_t* __restrict__ bin_key,
+                                                            const int32_t* __restrict__ offset,
+                                                            const int32_t* __restrict__ orig, int32_t* perm) {
+    __shared__ int32_t cs[kCellsPerBin + 1];
+    const int32_t fk = bin_key[blockIdx.x];
+    const int c = threadIdx.x;
+    cs[c] = offset[fk + c];
+    if (c == 0) cs[kCellsPerBin] = offset[fk + kCellsPerBin];
+    __syncthreads();
+    const int m = cs[c + 1] - cs[c];
+    if (m <= 1) return;
+    const int64_t b0 = cs[0];
+    if (m <= kOrderLocal) {
+        int32_t src[kOrderLocal], key[kOrderLocal];
+        int64_t dst[kOrderLocal];
+        for (int r = 0; r < m; ++r) {
+            dst[r] = order_dest(cs, c, r, b0);
+            src[r] = perm[dst[r]];
+            key[r] = orig[src[r]];
+        }
+        // insertion sort by orig (distinct within an instance)
+        for (int r = 1; r < m; ++r) {
+            const int32_t v = src[r], k = key[r];
+            int q = r - 1;
+            while (q >= 0 && key[q] > k) {
+                src[q + 1] = src[q];
+                key[q + 1] = key[q];
+                --q;
+            }
+            src[q + 1] = v;
+            key[q + 1] = k;
+        }
+        for (int r = 0; r < m; ++r) perm[dst[r]] = src[r];
+    } else {
+        // selection sort in place: rank r takes the smallest orig among ranks r..m-1
+        for (int r = 0; r < m - 1; ++r) {
+            const int64_t dr = order_dest(cs, c, r, b0);
+            int64_t best = dr;
+            int32_t bv = perm[dr], bk = orig[bv];
+            for (int q = r + 1; q < m; ++q) {
+                const int64_t dq = order_dest(cs, c, q, b0);
+                const int32_t v = perm[dq], k = orig[v];
+                if (k < bk) { bv = v; bk = k; best = dq; }
+            }
+            if (best != dr) {
+                perm[best] = perm[dr];
+                perm[dr] = bv;
+            }
+        }
+    }
 }
 
 template <typename R>
 __global__ void k_bin_gather(PState<R> src, PState<R> dst, const Inst<R>* insts, int n_inst, const int32_t* key,
                              const int32_t* key_base, const int32_t* newbin, const int32_t* perm, bool initial,
-                             const double* pos_scratch, bool has_K, int64_t np, bool det) {
+                             const double* pos_scratch, bool has_K, int64_t np) {
     const int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= np) return;
     const int64_t pi = perm[d];
@@ -284,7 +359,6 @@ __global__ void k_bin_gather(PState<R> src, PState<R> dst, const Inst<R>* insts,
     const int ii = find_inst(insts, n_inst, pi);
     const Inst<R>& P = insts[ii];
     const bool fresh = initial && P.fresh;
-    const int32_t kk = key[pi];
     const int nbn = newbin[pi];
     const int nbv[3] = {nbn % P.nbx, (nbn / P.nbx) % P.nby, nbn / (P.nbx * P.nby)};
     V4<R> a0 = src.A[0][pi];
@@ -306,38 +380,8 @@ __global__ void k_bin_gather(PState<R> src, PState<R> dst, const Inst<R>* insts,
             a0.z += (R)((obv[2] - nbv[2]) * kBin);
         }
     }
-    if (det && kk - key_base[ii] < P.nbins * kCellsPerBin) {
-        // deterministic mode: the stencil base of the stored position must be the
-        // key's cell, which the rounding of a re-expressed position can miss by
-        // one; such a coordinate is set onto the cell's edge (FP32: the low part
-        // takes the difference, so hi + lo stays the same).  Only rounding-sized
-        // misses are moved: a particle outside the bins (base below 0 at the
-        // domain edge) keeps its position, and the kill zone deactivates it.
-        const int cl = kk - key_base[ii] - nbn * kCellsPerBin;
-        const int c3[3] = {cl % kBin, (cl / kBin) % kBin, cl / (kBin * kBin)};
-        R v[3] = {a0.x, a0.y, a0.z}, sh[3] = {R(0), R(0), R(0)};
-        bool moved = false;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const R f = floor(v[c] - R(0.5));
-            R nv = v[c];
-            if (f < R(c3[c])) nv = R(c3[c]) + R(0.5);
-            else if (f > R(c3[c])) nv = nextafter(R(c3[c]) + R(1.5), R(0));
-            if (fabs(nv - v[c]) > R(1e-3)) nv = v[c];
-            sh[c] = v[c] - nv;
-            moved = moved || nv != v[c];
-            v[c] = nv;
-        }
-        if (moved) {
-            a0.x = v[0]; a0.y = v[1]; a0.z = v[2];
-            if (dst.X) {
-                V4<R> lo = dst.X[d];
-                lo.x += sh[0]; lo.y += sh[1]; lo.z += sh[2];
-                dst.X[d] = lo;
-            }
-        }
-    }
     dst.A[0][d] = a0;
+    dst.skey[d] = key[pi] - key_base[ii];
 #pragma unroll
     for (int q = 1; q < 6; ++q) dst.A[q][d] = src.A[q][pi];
 #pragma unroll
@@ -358,63 +402,6 @@ __global__ void k_bin_gather(PState<R> src, PState<R> dst, const Inst<R>* insts,
 
 // Unused slots of each instance are counted into the instance's last key so
 // that the global scan keeps every instance at its own slot range.
-// ------------------------------------------------------------------ deterministic ranks
-
-// Every slot's sort key (unused slots: their instance's pad key) and its index.
-template <typename R>
-__global__ void k_det_keys(const Inst<R>* insts, int n_inst, const int32_t* key_base, const int32_t* key,
-                           int32_t* keys2, int32_t* slots, int64_t np) {
-    const int64_t pi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (pi >= np) return;
-    const int ii = find_inst(insts, n_inst, pi);
-    const Inst<R>& P = insts[ii];
-    keys2[pi] = pi < P.pbase + P.np ? key[pi] : key_base[ii] + P.nbins * kCellsPerBin + 1;
-    slots[pi] = (int32_t)pi;
-}
-
-// The rank of each live slot within its key: its place in the stably sorted
-// order less the key's first place.
-__global__ void k_det_rank(const int32_t* sorted_keys, const int32_t* perm, const int32_t* offset, int32_t* rank,
-                           int64_t np) {
-    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= np) return;
-    const int32_t pi = perm[j];
-    rank[pi] = (int32_t)(j - offset[sorted_keys[j]]);
-}
-
-static int key_bits(int64_t nkeys) {
-    int b = 1;
-    while (b < 31 && ((int64_t)1 << b) <= nkeys) ++b;
-    return b;
-}
-
-size_t det_rank_tmp_bytes(int64_t np, int64_t nkeys) {
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const int32_t*)nullptr, (int32_t*)nullptr,
-                                    (const int32_t*)nullptr, (int32_t*)nullptr, (int)np, 0, key_bits(nkeys));
-    return bytes;
-}
-
-template <typename R>
-void launch_det_ranks(const Inst<R>* insts, int n_inst, const int32_t* key_base, int32_t* key, const int32_t* offset,
-                      int32_t* rank, int64_t np, int64_t nkeys, int32_t* keys2, int32_t* slots, int32_t* perm,
-                      int32_t* sorted, void* tmp, size_t tmp_bytes, cudaStream_t st) {
-    if (np <= 0) return;
-    const int blocks = (int)((np + kT - 1) / kT);
-    k_det_keys<R><<<blocks, kT, 0, st>>>(insts, n_inst, key_base, key, keys2, slots, np);
-    // the radix sort is stable: slots with equal keys keep their order
-    size_t bytes = tmp_bytes;
-    cub::DeviceRadixSort::SortPairs(tmp, bytes, keys2, sorted, slots, perm, (int)np, 0, key_bits(nkeys), st);
-    k_det_rank<<<blocks, kT, 0, st>>>(sorted, perm, offset, rank, np);
-    launch_counter() += 2;
-}
-template void launch_det_ranks<float>(const Inst<float>*, int, const int32_t*, int32_t*, const int32_t*, int32_t*,
-                                      int64_t, int64_t, int32_t*, int32_t*, int32_t*, int32_t*, void*, size_t,
-                                      cudaStream_t);
-template void launch_det_ranks<double>(const Inst<double>*, int, const int32_t*, int32_t*, const int32_t*, int32_t*,
-                                       int64_t, int64_t, int32_t*, int32_t*, int32_t*, int32_t*, void*, size_t,
-                                       cudaStream_t);
-
 template <typename R>
 __global__ void k_pad_counts(const Inst<R>* insts, int n_inst, const int32_t* key_base, int32_t* count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -545,6 +532,7 @@ __global__ void k_import(DevSoA in, int64_t n, double ox, double oy, double oz, 
     ps.id[d] = in.id ? in.id[i] : (int32_t)i;
     ps.orig[d] = (int32_t)i;
     ps.bin[d] = 0;
+    ps.skey[d] = -1;
 }
 
 // ------------------------------------------------------------------ generator
@@ -608,6 +596,7 @@ __global__ void k_gen_write(Inst<R> P, int c0x, int c0y, int c0z, int wx, int wy
     ps.id[d] = (int32_t)i;
     ps.orig[d] = (int32_t)i;
     ps.bin[d] = 0;
+    ps.skey[d] = -1;
     (void)wz;
     (void)P;
 }
@@ -910,10 +899,10 @@ std::atomic<int64_t>& launch_counter() {
 template <typename R>
 void launch_bin_count(const Inst<R>* insts, int n_inst, const PState<R>& ps, const int32_t* key_base, bool initial,
                       const double* pos_scratch, int32_t* key, int32_t* rank, int32_t* count, int32_t* newbin,
-                      int64_t np, cudaStream_t st) {
+                      int64_t np, int kpt, int sort_every, bool keep_all, cudaStream_t st) {
     if (np <= 0) return;
     k_bin_count<R><<<(int)((np + kT - 1) / kT), kT, 0, st>>>(insts, n_inst, ps, key_base, initial, pos_scratch, key,
-                                                             rank, count, newbin, np);
+                                                             rank, count, newbin, np, kpt, sort_every, keep_all);
     ++launch_counter();
 }
 
@@ -921,14 +910,15 @@ template <typename R>
 void launch_bin_scatter(const PState<R>& src, const PState<R>& dst, const Inst<R>* insts, int n_inst,
                         const int32_t* key, const int32_t* rank, const int32_t* offset, const int32_t* key_base,
                         const int32_t* newbin, bool initial, const double* pos_scratch, bool has_K, int64_t np,
-                        int32_t* perm, cudaStream_t st, bool det) {
+                        int32_t* perm, const int32_t* bin_key, int nbins_total, cudaStream_t st) {
     if (np <= 0) return;
     const int blocks = (int)((np + kT - 1) / kT);
     cudaMemsetAsync(perm, 0xff, sizeof(int32_t) * np, st);
-    k_bin_perm<R><<<blocks, kT, 0, st>>>(insts, n_inst, key, rank, offset, key_base, newbin, perm, np, det);
+    k_bin_perm<R><<<blocks, kT, 0, st>>>(insts, n_inst, key, rank, offset, key_base, newbin, perm, np);
+    if (nbins_total > 0) k_bin_order<<<nbins_total, kCellsPerBin, 0, st>>>(bin_key, offset, src.orig, perm);
     k_bin_gather<R><<<blocks, kT, 0, st>>>(src, dst, insts, n_inst, key, key_base, newbin, perm, initial,
-                                           pos_scratch, has_K, np, det);
-    launch_counter() += 2;
+                                           pos_scratch, has_K, np);
+    launch_counter() += nbins_total > 0 ? 3 : 2;
 }
 
 template <typename R>
@@ -1037,6 +1027,7 @@ __global__ void k_relayout(PState<R> src, PState<R> dst, const RelayoutMap* __re
     if (src.X && dst.X) dst.X[s] = src.X[o];
     dst.orig[s] = src.orig[o];
     dst.bin[s] = src.bin[o];
+    dst.skey[s] = src.skey[o];
 }
 
 template <typename R>
@@ -1105,10 +1096,10 @@ void launch_heat_diffuse(const Inst<R>* insts, int n_inst, int b, int64_t total,
 
 #define MPMB_INST(R)                                                                                                  \
     template void launch_bin_count<R>(const Inst<R>*, int, const PState<R>&, const int32_t*, bool, const double*,   \
-                                      int32_t*, int32_t*, int32_t*, int32_t*, int64_t, cudaStream_t);               \
+                                      int32_t*, int32_t*, int32_t*, int32_t*, int64_t, int, int, bool, cudaStream_t); \
     template void launch_bin_scatter<R>(const PState<R>&, const PState<R>&, const Inst<R>*, int, const int32_t*,    \
                                         const int32_t*, const int32_t*, const int32_t*, const int32_t*, bool,       \
-                                        const double*, bool, int64_t, int32_t*, cudaStream_t, bool);                 \
+                                        const double*, bool, int64_t, int32_t*, const int32_t*, int, cudaStream_t);  \
     template void launch_import<R>(const DevSoA&, int64_t, double, double, double, double, double, const PState<R>&, \
                                    int64_t, double*, cudaStream_t);                                                  \
     template void launch_gen<R>(const Inst<R>&, const int32_t*, const int32_t*, int, uint64_t, uint32_t, int, double, \

@@ -24,7 +24,7 @@
 namespace mpmb {
 
 constexpr char kCkptMagic[8] = {'M', 'P', 'M', 'C', 'K', 'P', 'T', '\0'};
-constexpr uint32_t kCkptVersion = 1;
+constexpr uint32_t kCkptVersion = 2;
 
 struct CkptHeader {
     char magic[8];
@@ -33,7 +33,7 @@ struct CkptHeader {
     int32_t precision;      // MPM_PREC_F32 or MPM_PREC_F64
     int32_t has_K;          // backstress arrays present
     int32_t n_samples;      // raster tool samples after the arrays
-    int32_t _pad;
+    int32_t since_rebin;    // steps since the instance's last re-bin (its re-bin phase)
     int64_t np;             // particles
     int64_t step;           // steps taken
     double time, tool_t0, dt;
@@ -52,6 +52,7 @@ inline std::vector<size_t> ckpt_array_elem(int precision, bool has_K) {
     e.push_back(r);                           // sres
     e.push_back(1); e.push_back(1);           // status, shear counter
     e.push_back(4); e.push_back(4); e.push_back(4);   // id, bin, orig
+    e.push_back(4);                           // the re-bin key (layout)
     return e;
 }
 

@@ -69,6 +69,8 @@ template <typename R> struct PState {
     int32_t* id;
     int32_t* bin;       // bin (block) index the particle is filed under, written by the re-bin
     int32_t* orig;      // position of the particle in upload order
+    int32_t* skey;      // the particle's key at the re-bin that placed it, relative to its
+                        // instance (bin*64 + cell; nbins*64 when INACTIVE; -1 before any)
 };
 
 // Per-instance constants, built on the host.  Lives in a device array (the
@@ -161,7 +163,29 @@ template <typename R> struct alignas(128) Inst {
     int fresh;                     // positions still in the upload scratch (not yet binned)
     int nbins;                     // nbx * nby * nbz
     int* ierr;                     // this instance's error word: byte 0 NaN/Inf, byte 1 Newton
+    int bin0;                      // first bin of this instance in the batch bin tables
+    // re-bin phase: this instance is re-binned before the step launches of
+    // points k = rebin_first, rebin_first + sort_every, ... of the current
+    // call (point k: before the launch that holds G2P of step k, fused
+    // schedule; before the P2G of step k, split schedule); at other re-bins
+    // of the handle it keeps its layout
+    int rebin_first;
+    int rebin_now;                 // binned from its positions at the next re-bin whatever its phase
+    // deterministic mode: the node sums of particles whose stencil left their
+    // bin's tile, in fixed point (value x esc_scale rounded to an integer and
+    // added with integer atomics, so that the order of the adds cannot change
+    // the sum), channel c (m, p_x, p_y, p_z, T m) of node li at
+    // esc[c * esc_stride + li]; esc_flag[b] is set for each bin b whose core
+    // holds such a node.  NULL: the default mode's float atomics on the grid.
+    unsigned long long* esc;
+    int64_t esc_stride;
+    int* esc_flag;
+    double esc_scale;
 };
+
+// Deterministic mode: node-tile values stored per work item (channels m,
+// p_x, p_y, p_z, T m; kTileNodes nodes each, in tile order x + 6y + 36z).
+constexpr int kPartCh = 5;
 
 // Threads per CTA of the step kernel (four warps, each with its own P2G tile).
 constexpr int kNT = 128;
@@ -185,11 +209,10 @@ struct StepArgs {
     int p2g_step;       // step index of the P2G part
     int ext;            // some instance runs the adiabatic shear model or heat conduction: launches
                         // take the kernel variant that has them (the others carry none of their code)
-    int det = 0;        // deterministic mode: the P2G-only launch writes each particle's 27 node
-                        // contributions (m, p) to det_contrib (27 rows of det_stride V4s) for
-                        // k_p2g_det to sum
-    void* det_contrib = nullptr;
-    int64_t det_stride = 0;
+    int chunk = 2;         // FP32 particles per pass / 128 (1, 2 or 4): the launch config's pass size
+    void* part = nullptr;  // deterministic mode: each work item's node tile is stored at
+                           // part + wi * kPartCh * kTileNodes (R values) for k_node_sum to add
+                           // up in a fixed order, instead of added to the grid with atomics
 };
 
 // ------------------------------------------------------------------ weights

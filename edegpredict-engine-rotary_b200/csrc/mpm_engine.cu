@@ -136,20 +136,23 @@ class Engine final : public EngineBase {
     int32_t* d_gen = nullptr;
     size_t gen_bytes = 0;
     bool binned = false;
-    int64_t since_sort = 0, n_sorts = 0;
+    int64_t n_sorts = 0;
     int64_t launch_base = 0;
     int sort_every = 16, threads = 128, ctas_per_sm = 4, prec_ = MPM_PREC_F32;
+    static constexpr int kDefaultPassChunk = 2;
+    int pass_chunk = kDefaultPassChunk;   // FP32 particles per pass of the step kernel / 128
     bool use_graph = false;
     int rbuf = 0;
-    // deterministic mode (mpm_launch_config.deterministic): the particles' node
-    // contributions and the stable-sort scratch of the re-bin
+    // deterministic mode (mpm_launch_config.deterministic): every work item's
+    // node tile (kPartCh x kTileNodes values), the escaped fixed-point node
+    // sums (kPartCh x nn_total) and their per-bin marks
     bool det = false;
-    V4<R>* d_det_contrib = nullptr;   // 27 rows of cap_total node contributions
-    int64_t det_contrib_alloc = 0;
-    int32_t* d_det_i32[4] = {nullptr, nullptr, nullptr, nullptr};
-    int64_t det_i32_alloc[4] = {0, 0, 0, 0};
-    unsigned char* d_det_tmp = nullptr;
-    int64_t det_tmp_alloc = 0;
+    R* d_part = nullptr;
+    int64_t part_alloc = 0;
+    unsigned long long* d_esc = nullptr;
+    int64_t esc_alloc = 0;
+    int32_t* d_esc_flag = nullptr;
+    int64_t esc_flag_alloc = 0;
     // step-kernel timing (mpm_profile_enable)
     bool prof = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -197,8 +200,7 @@ class Engine final : public EngineBase {
                         d_bin_local,
                         d_inst_pbase, d_key, d_rank, d_newbin, d_count, d_offset, d_flag, d_flag_scan, d_scan_tmp,
                         d_pos, d_work, d_nwork, d_err, d_ierr, d_ctr, d_stat_part, d_stat_out, d_stage, d_gen,
-                        d_map, d_perm, d_det_contrib, d_det_i32[0], d_det_i32[1], d_det_i32[2], d_det_i32[3], d_det_tmp,
-                        d_pext, d_flags};
+                        d_map, d_perm, d_part, d_esc, d_esc_flag, d_pext, d_flags};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         for (auto& x : I)
@@ -285,7 +287,7 @@ class Engine final : public EngineBase {
     static size_t pstate_bytes(int64_t cp, bool withK) {
         const size_t v4 = sizeof(V4<R>);
         return (12 + (kPosLo ? 1 : 0)) * al256(v4 * cp) + (withK ? 2 * al256(v4 * cp) : 0) + al256(sizeof(R) * cp) +
-               2 * al256(cp) + 3 * al256(4 * cp);
+               2 * al256(cp) + 4 * al256(4 * cp);
     }
     static void carve(void* base, int64_t cp, bool withK, PState<R>& s) {
         char* q = (char*)base;
@@ -306,6 +308,7 @@ class Engine final : public EngineBase {
         s.id = (int32_t*)take(4 * cp);
         s.bin = (int32_t*)take(4 * cp);
         s.orig = (int32_t*)take(4 * cp);
+        s.skey = (int32_t*)take(4 * cp);
     }
 
     // Replaces the instance set by nI; from[j] is the old index of new
@@ -365,6 +368,7 @@ class Engine final : public EngineBase {
             x.nby = (x.p.ny + kBin - 1) / kBin;
             x.nbz = (x.p.nz + kBin - 1) / kBin;
             const int64_t nbins = (int64_t)x.nbx * x.nby * x.nbz;
+            x.bin0 = (int)bin_key.size();
             key_base[i] = (int32_t)kb;
             for (int64_t b = 0; b < nbins; ++b) {
                 bin_key.push_back((int32_t)(kb + b * kCellsPerBin));
@@ -495,7 +499,6 @@ class Engine final : public EngineBase {
         if (n > 0) CK(cudaMemcpyAsync(d_inst, h_inst.data(), sizeof(Inst<R>) * n, cudaMemcpyHostToDevice, st));
         CK(cudaStreamSynchronize(st));
         binned = false;
-        since_sort = 0;
         return MPM_OK;
     }
 
@@ -661,7 +664,19 @@ class Engine final : public EngineBase {
         d.nx = p.nx; d.ny = p.ny; d.nz = p.nz;
         d.nbx = x.nbx; d.nby = x.nby; d.nbz = x.nbz;
         d.nbins = x.nbx * x.nby * x.nbz;
+        d.bin0 = x.bin0;
+        d.rebin_first = std::max(sort_every - x.since, 0);
+        d.rebin_now = x.rebin_now ? 1 : 0;
         d.nn = x.nn;
+        if (det && d_esc) {
+            d.esc = d_esc + x.grid_off;
+            d.esc_stride = std::max<int64_t>(nn_total, 1);
+            d.esc_flag = d_esc_flag + x.bin0;
+            d.esc_scale = std::ldexp(1.0, 40) / std::max(p.particle_mass, 1e-300);
+        } else {
+            d.esc = nullptr;
+            d.esc_flag = nullptr;
+        }
         d.dx = p.dx; d.ox = p.origin[0]; d.oy = p.origin[1]; d.oz = p.origin[2];
         d.dt = x.dt; d.t0 = x.time; d.step0 = x.step;
         const double mu = p.E / (2.0 * (1.0 + p.nu));
@@ -752,48 +767,52 @@ class Engine final : public EngineBase {
 
     // ---------------------------------------------------------------- binning
 
-    // Deterministic mode: scratch for the node contributions and the stable sort (grown
-    // outside any graph capture: the mode runs without graphs).
+    // Deterministic mode: the stored node tiles and the escaped sums, grown
+    // outside any graph capture and zeroed when grown (k_node_sum clears what
+    // it reads).  fill_mutable points the instances into them.
     mpm_status det_scratch() {
-        const int64_t tmp = (int64_t)det_rank_tmp_bytes(cap_total, nkeys);
-        bool more = det_contrib_alloc < 27 * std::max<int64_t>(cap_total, 1) || det_tmp_alloc < std::max<int64_t>(tmp, 1);
-        for (int k = 0; k < 4; ++k) more = more || det_i32_alloc[k] < std::max<int64_t>(cap_total, 1);
-        if (!more) return MPM_OK;
+        const int64_t items = std::max<int64_t>(max_work, 1);
+        const int64_t nodes = std::max<int64_t>(nn_total, 1);
+        if (part_alloc >= items * kPartCh * kTileNodes && esc_alloc >= kPartCh * nodes && esc_flag_alloc >= items)
+            return MPM_OK;
         CK(cudaStreamSynchronize(st));   // nothing in flight uses the old buffers
-        MS(grow(d_det_contrib, det_contrib_alloc, 27 * std::max<int64_t>(cap_total, 1), false));
-        for (int k = 0; k < 4; ++k) MS(grow(d_det_i32[k], det_i32_alloc[k], cap_total));
-        MS(grow(d_det_tmp, det_tmp_alloc, tmp));
-        return MPM_OK;
-    }
-    // Deterministic mode: ranks within each key in slot order (the scatter then
-    // keeps every cell's particles together in that order).
-    mpm_status det_ranks() {
-        if (!det) return MPM_OK;
-        MS(det_scratch());
-        launch_det_ranks<R>(d_inst, (int)I.size(), d_key_base, d_key, d_offset, d_rank, cap_total, nkeys,
-                            d_det_i32[0], d_det_i32[1], d_det_i32[2], d_det_i32[3], d_det_tmp,
-                            (size_t)det_tmp_alloc, st);
+        MS(grow(d_part, part_alloc, items * kPartCh * kTileNodes, false));
+        MS(grow(d_esc, esc_alloc, kPartCh * nodes, false));
+        MS(grow(d_esc_flag, esc_flag_alloc, items, false));
+        CK(cudaMemsetAsync(d_esc, 0, sizeof(unsigned long long) * esc_alloc, st));
+        CK(cudaMemsetAsync(d_esc_flag, 0, sizeof(int32_t) * esc_flag_alloc, st));
         return MPM_OK;
     }
 
+    // The re-bin before a step call after an upload, a generation, a load or
+    // a change of the instance set: fresh instances are binned from their
+    // positions, every other instance keeps the layout its last re-bin gave
+    // it (so an instance's layout, and with it every sum of its steps, does
+    // not depend on when other instances arrive or on a checkpoint reload).
     mpm_status rebin() {
         Range nvtx_range("mpm.rebin");
         CK(cudaMemsetAsync(d_count, 0, 4 * (nkeys + 1), st));
         launch_pad_counts<R>(d_inst, (int)I.size(), d_key_base, d_count, st);
         launch_bin_count<R>(d_inst, (int)I.size(), ps[cur], d_key_base, true, d_pos, d_key, d_rank, d_count, d_newbin,
-                            cap_total, st);
+                            cap_total, 0, sort_every, true, st);
         exclusive_scan(d_count, d_offset, nkeys, d_scan_tmp, st);
-        MS(det_ranks());
         launch_bin_scatter<R>(ps[cur], ps[cur ^ 1], d_inst, (int)I.size(), d_key, d_rank, d_offset, d_key_base,
-                              d_newbin, true, d_pos, has_K, cap_total, d_perm, st, det);
+                              d_newbin, true, d_pos, has_K, cap_total, d_perm, d_bin_key, max_work, st);
         build_work(d_offset, d_bin_key, d_bin_inst, d_bin_local, d_inst_pbase, max_work, d_flag, d_flag_scan,
                    d_scan_tmp, d_work, d_nwork, st);
         cur ^= 1;
-        since_sort = 0;
         ++n_sorts;
         binned = true;
         bool any_fresh = false;
-        for (auto& x : I) { any_fresh |= (x.fresh != 0); x.fresh = 0; }
+        bool any_now = false;
+        for (auto& x : I) {
+            any_fresh |= (x.fresh != 0);
+            any_now |= x.rebin_now;
+            if (x.fresh || x.rebin_now) x.since = 0;
+            x.fresh = 0;
+            x.rebin_now = false;
+        }
+        any_fresh |= any_now;
         if (any_fresh) return push_insts();
         return MPM_OK;
     }
@@ -1051,7 +1070,10 @@ class Engine final : public EngineBase {
         CK(cudaMemcpyAsync(h, d_flags, sizeof(h), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         CK(cudaGetLastError());
-        if (h[0]) binned = false;   // moved particles: re-bin before the next step
+        if (h[0]) {   // moved particles: re-bin the instance from its positions before the next step
+            binned = false;
+            I[i].rebin_now = true;
+        }
         if (fields & MPM_AOS_EXT_FORCE) x.pext_pending = true;
         MS(push_insts());
         if (h[1]) {
@@ -1233,25 +1255,17 @@ class Engine final : public EngineBase {
             }
             I[i].dt = dts[i];
         }
-        mpm_status s = ensure_binned();
-        if (s != MPM_OK) return s;
-        s = push_insts();
-        if (s != MPM_OK) return s;
-        bool ext = false;
-        for (auto& x : I) ext |= x.ext_pending || x.pext_pending;
         if (det && ws_on) {
             err = "the deterministic mode covers MPMSolver's semantics only";
             return MPM_NOT_SUPPORTED;
         }
-        if (det) {
-            for (const auto& x : I)
-                if (x.p.asb_enabled || x.p.heat_conduction || (x.sdf && x.p.contact_every > 0)) {
-                    err = "deterministic mode does not cover the adiabatic shear model, heat conduction or the "
-                          "voxel tool SDF contact";
-                    return MPM_NOT_SUPPORTED;
-                }
-            MS(det_scratch());
-        }
+        mpm_status s = ensure_binned();
+        if (s != MPM_OK) return s;
+        if (det) MS(det_scratch());
+        s = push_insts();
+        if (s != MPM_OK) return s;
+        bool ext = false;
+        for (auto& x : I) ext |= x.ext_pending || x.pext_pending;
         // the raster launches' sizes are part of a captured graph
         std::vector<int> rsig(I.size());
         for (size_t q = 0; q < I.size(); ++q) rsig[q] = raster_points(I[q]);
@@ -1261,7 +1275,7 @@ class Engine final : public EngineBase {
         }
         if (ws_on)
             s = issue_ws_steps(N, ext);
-        else if (use_graph && !prof && max_work > 0 && !det)
+        else if (use_graph && !prof && max_work > 0)
             s = step_graph(N, ext);
         else
             s = issue_steps(N, ext);
@@ -1283,12 +1297,22 @@ class Engine final : public EngineBase {
     mpm_status issue_steps(int32_t N, bool ext) {
         mpm_status s = MPM_OK;
         const size_t gbytes = sizeof(V4<R>) * nn_total;
-        // deterministic mode: split schedule, re-binned before every P2G
-        const bool fused = I[0].p.schedule == MPM_SCHED_FUSED && !det;
+        const bool fused = I[0].p.schedule == MPM_SCHED_FUSED;
         int w = rbuf;
-        auto maybe_sort = [&]() -> mpm_status {
-            if (since_sort >= sort_every || (det && since_sort > 0)) return rebin_regular();
-            return MPM_OK;
+        // point k of the call: the instances whose re-bin phase falls on k are
+        // re-binned (the others keep their layout); last[i] = the call's last
+        // such point of instance i
+        std::vector<int> last(I.size(), -1);
+        auto maybe_sort = [&](int k) -> mpm_status {
+            bool any = false;
+            for (size_t i = 0; i < I.size(); ++i) {
+                const int f = std::max(sort_every - I[i].since, 0);
+                if (k >= f && (k - f) % sort_every == 0) {
+                    any = true;
+                    last[i] = k;
+                }
+            }
+            return any ? rebin_regular(k) : MPM_OK;
         };
         const int cps = ctas_per_sm;
         int xk = 0, heat = 0;
@@ -1296,11 +1320,26 @@ class Engine final : public EngineBase {
             xk |= (x.p.asb_enabled || x.p.heat_conduction || (x.sdf && x.p.contact_every > 0)) ? 1 : 0;
             heat |= x.p.heat_conduction ? 1 : 0;
         }
-        // the grid buffer a P2G launch writes starts at zero, and so does its T m buffer
+        // Default mode: the grid buffer a P2G launch writes starts at zero, and
+        // so does its T m buffer; the launch adds its tiles with atomics.
+        // Deterministic mode: the launch stores its tiles and k_node_sum writes
+        // every node of the buffer from them.
         auto clear = [&](int b) -> mpm_status {
+            if (det) return MPM_OK;
             CK(cudaMemsetAsync(gpool[b], 0, gbytes, st));
             if (heat) CK(cudaMemsetAsync(tpool[b], 0, sizeof(R) * nn_total, st));
             return MPM_OK;
+        };
+        const int64_t part_items = part_alloc / (kPartCh * kTileNodes);
+        auto node_sum = [&](int b) {
+            if (det)
+                launch_node_sum<R>(d_inst, d_bin_inst, d_bin_local, d_flag, d_flag_scan, d_part, part_items, b,
+                                   max_work, st);
+        };
+        auto p2g_args = [&](StepArgs a) {
+            a.part = det ? d_part : nullptr;
+            a.chunk = pass_chunk;
+            return a;
         };
         // heat conduction: the diffusion step on grid buffer b before the G2P that reads it
         auto diffuse = [&](int b) {
@@ -1308,53 +1347,54 @@ class Engine final : public EngineBase {
         };
         if (fused) {
             if ((s = clear(w)) != MPM_OK) return s;
-            StepArgs a{0, 0, N == 1 ? 1 : 0, ext ? 1 : 0, 0, xk};
+            const StepArgs a = p2g_args(StepArgs{0, 0, N == 1 ? 1 : 0, ext ? 1 : 0, 0, xk});
             launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], a, w, false, true, threads, cps, d_err, d_ctr,
                            st);
+            node_sum(w);
             for (int k = 0; k + 1 < N; ++k) {
-                if ((s = maybe_sort()) != MPM_OK) return s;
+                if ((s = maybe_sort(k)) != MPM_OK) return s;
                 if ((s = clear(w ^ 1)) != MPM_OK) return s;
                 raster_all(k);
                 diffuse(w);
-                StepArgs b{k, 0, (k + 2 == N) ? 1 : 0, 0, k + 1, xk};
+                const StepArgs b = p2g_args(StepArgs{k, 0, (k + 2 == N) ? 1 : 0, 0, k + 1, xk});
                 prof_begin();
                 launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], b, w, true, true, threads, cps, d_err,
                                d_ctr, st);
                 prof_end();
+                node_sum(w ^ 1);
                 w ^= 1;
-                ++since_sort;
             }
+            // the last point: a split of these steps into several calls re-bins
+            // at the same steps as one call
+            if ((s = maybe_sort(N - 1)) != MPM_OK) return s;
             raster_all(N - 1);
             diffuse(w);
             StepArgs c{N - 1, 1, 0, 0, N - 1, xk};
+            c.chunk = pass_chunk;
             launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], c, w, true, false, threads, cps, d_err, d_ctr,
                            st);
-            ++since_sort;
         } else {
             for (int k = 0; k < N; ++k) {
-                if ((s = maybe_sort()) != MPM_OK) return s;
+                if ((s = maybe_sort(k)) != MPM_OK) return s;
                 if ((s = clear(w)) != MPM_OK) return s;
-                StepArgs a{k, 0, 1, (ext && k == 0) ? 1 : 0, k, xk};
-                a.det = det ? 1 : 0;
-                a.det_contrib = d_det_contrib;
-                a.det_stride = cap_total;
+                const StepArgs a = p2g_args(StepArgs{k, 0, 1, (ext && k == 0) ? 1 : 0, k, xk});
                 prof_begin();
                 launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], a, w, false, true, threads, cps, d_err,
                                d_ctr, st);
                 prof_end();
-                if (det)
-                    launch_p2g_det<R>(d_inst, (int)I.size(), d_det_contrib, cap_total, d_key_base, d_offset, w,
-                                      nn_total, st);
+                node_sum(w);
                 raster_all(k);
                 diffuse(w);
                 StepArgs c{k, 1, 0, 0, k, xk};
+                c.chunk = pass_chunk;
                 prof_begin();
                 launch_step<R>(d_inst, d_work, d_nwork, max_work, ps[cur], c, w, true, false, threads, cps, d_err,
                                d_ctr, st);
                 prof_end();
-                ++since_sort;
             }
         }
+        // G2P steps since each instance's last re-bin
+        for (size_t i = 0; i < I.size(); ++i) I[i].since = last[i] >= 0 ? N - last[i] : I[i].since + N;
         rbuf = w;
         return MPM_OK;
     }
@@ -1386,7 +1426,10 @@ class Engine final : public EngineBase {
         CK(cudaStreamSynchronize(st));
         drop_graphs();
         if (!p) {
-            if (ws_on) binned = false;   // positions drifted from their bins: re-bin for the fused kernel
+            if (ws_on) {   // positions drifted from their bins: re-bin for the fused kernel
+                binned = false;
+                for (auto& x : I) x.rebin_now = true;
+            }
             ws_on = false;
             return push_insts();
         }
@@ -1407,10 +1450,11 @@ class Engine final : public EngineBase {
     // host counters it leaves behind are replayed with it.
     struct GraphEntry {
         int32_t N;
-        int64_t since_sort0;
+        std::vector<int> since0;   // the instances' re-bin phases before the call
         int cur0, rbuf0, ext;
         cudaGraphExec_t exec;
-        int64_t since_sort1, sorts, launches;
+        std::vector<int> since1;   // ... and after it
+        int64_t sorts, launches;
         int cur1, rbuf1;
         uint64_t use;
     };
@@ -1426,10 +1470,12 @@ class Engine final : public EngineBase {
 
     mpm_status step_graph(int32_t N, bool ext) {
         Range nvtx_range("mpm.graph");
+        std::vector<int> since(I.size());
+        for (size_t i = 0; i < I.size(); ++i) since[i] = I[i].since;
         for (auto& g : graphs) {
-            if (g.N == N && g.since_sort0 == since_sort && g.cur0 == cur && g.rbuf0 == rbuf && g.ext == (int)ext) {
+            if (g.N == N && g.since0 == since && g.cur0 == cur && g.rbuf0 == rbuf && g.ext == (int)ext) {
                 CK(cudaGraphLaunch(g.exec, st));
-                since_sort = g.since_sort1;
+                for (size_t i = 0; i < I.size(); ++i) I[i].since = g.since1[i];
                 n_sorts += g.sorts;
                 cur = g.cur1;
                 rbuf = g.rbuf1;
@@ -1440,7 +1486,7 @@ class Engine final : public EngineBase {
         }
         GraphEntry e{};
         e.N = N;
-        e.since_sort0 = since_sort;
+        e.since0 = since;
         e.cur0 = cur;
         e.rbuf0 = rbuf;
         e.ext = (int)ext;
@@ -1464,7 +1510,8 @@ class Engine final : public EngineBase {
             return MPM_CUDA_ERROR;
         }
         CK(cudaGraphLaunch(e.exec, st));
-        e.since_sort1 = since_sort;
+        e.since1.resize(I.size());
+        for (size_t i = 0; i < I.size(); ++i) e.since1[i] = I[i].since;
         e.sorts = n_sorts - sorts0;
         e.launches = launch_counter() - l0;
         e.cur1 = cur;
@@ -1488,17 +1535,23 @@ class Engine final : public EngineBase {
         c->sort_every = sort_every;
         c->use_graph = use_graph ? 1 : 0;
         c->deterministic = det ? 1 : 0;
+        c->pass_size = pass_chunk * 128;
         return MPM_OK;
     }
 
     mpm_status set_config(const mpm_launch_config* c) override {
         if (!c || c->ctas_per_sm < 1 || c->ctas_per_sm > 8 || c->sort_every < 1 || c->sort_every > 1024 ||
-            (c->deterministic != 0 && c->deterministic != 1)) {
-            err = "launch config: ctas_per_sm in [1, 8], sort_every in [1, 1024], deterministic 0 or 1";
+            (c->deterministic != 0 && c->deterministic != 1) ||
+            (c->pass_size != 0 && c->pass_size != 128 && c->pass_size != 256 && c->pass_size != 512)) {
+            err = "launch config: ctas_per_sm in [1, 8], sort_every in [1, 1024], deterministic 0 or 1, pass_size "
+                  "0, 128, 256 or 512";
             return MPM_INVALID_ARG;
         }
-        if (c->ctas_per_sm != ctas_per_sm || c->sort_every != sort_every || (c->deterministic != 0) != det)
+        const int chunk = c->pass_size ? c->pass_size / 128 : kDefaultPassChunk;
+        if (c->ctas_per_sm != ctas_per_sm || c->sort_every != sort_every || (c->deterministic != 0) != det ||
+            chunk != pass_chunk)
             drop_graphs();
+        pass_chunk = chunk;
         det = c->deterministic != 0;
         ctas_per_sm = c->ctas_per_sm;
         sort_every = c->sort_every;
@@ -1507,10 +1560,12 @@ class Engine final : public EngineBase {
         return MPM_OK;
     }
 
-    // Times each candidate (persistent CTAs per SM x re-bin cadence) over one
-    // re-bin period of real steps and keeps the fastest.  The trial steps
-    // advance the simulation like any other steps.
+    // Times the candidates over real steps and keeps the fastest: the pass
+    // size first (16 steps each at the current CTAs and cadence), then, at the
+    // fastest pass size, CTAs per SM x re-bin cadence over one re-bin period
+    // each.  The trial steps advance the simulation like any other steps.
     mpm_status autotune(const double* dts, mpm_launch_config* best) override {
+        const int cand_pass[3] = {128, 256, 512};
         const int cand_ctas[3] = {2, 3, 4};
         const int cand_sort[3] = {8, 16, 32};
         mpm_launch_config cur_cfg{};
@@ -1520,28 +1575,46 @@ class Engine final : public EngineBase {
         cudaEvent_t e0, e1;
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
+        // n steps of candidate c, then the re-bin that ends the period: ms per step
+        auto trial = [&](const mpm_launch_config& c, int n, double* per) -> mpm_status {
+            mpm_status s = set_config(&c);
+            if (s != MPM_OK) return s;
+            for (auto& x : I) x.since = 0;
+            cudaEventRecord(e0, st);
+            if ((s = step(n, dts)) != MPM_OK) return s;
+            if ((s = rebin_regular(-1)) != MPM_OK) return s;
+            for (auto& x : I) x.since = 0;
+            cudaEventRecord(e1, st);
+            if (cudaEventSynchronize(e1) != cudaSuccess) {
+                err = "autotune: event sync failed";
+                return MPM_CUDA_ERROR;
+            }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            *per = ms / n;
+            return MPM_OK;
+        };
         mpm_status s = MPM_OK;
+        for (int a = 0; a < 3 && s == MPM_OK; ++a) {
+            mpm_launch_config c = cur_cfg;
+            c.pass_size = cand_pass[a];
+            double per = 0.0;
+            if ((s = trial(c, 16, &per)) != MPM_OK) break;
+            if (per < win_ms) {
+                win_ms = per;
+                win = c;
+            }
+        }
+        const int pass = win.pass_size;
+        win_ms = 1e300;
         for (int a = 0; a < 3 && s == MPM_OK; ++a)
             for (int b = 0; b < 3 && s == MPM_OK; ++b) {
                 mpm_launch_config c = cur_cfg;
+                c.pass_size = pass;
                 c.ctas_per_sm = cand_ctas[a];
                 c.sort_every = cand_sort[b];
-                if ((s = set_config(&c)) != MPM_OK) break;
-                since_sort = 0;
-                const int n = cand_sort[b];
-                cudaEventRecord(e0, st);
-                if ((s = step(n, dts)) != MPM_OK) break;
-                // the re-bin of this period (the cadence counter is at n)
-                if ((s = rebin_regular()) != MPM_OK) break;
-                cudaEventRecord(e1, st);
-                if (cudaEventSynchronize(e1) != cudaSuccess) {
-                    s = MPM_CUDA_ERROR;
-                    err = "autotune: event sync failed";
-                    break;
-                }
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                const double per = ms / n;
+                double per = 0.0;
+                if ((s = trial(c, cand_sort[b], &per)) != MPM_OK) break;
                 if (per < win_ms) {
                     win_ms = per;
                     win = c;
@@ -1555,21 +1628,22 @@ class Engine final : public EngineBase {
         return s == MPM_OK ? device_status() : s;
     }
 
-    mpm_status rebin_regular() {
+    // The re-bin at point kpt of a step call: the instances whose re-bin
+    // phase falls on kpt are binned from their positions, the others keep
+    // their layout (kpt < 0: every instance is re-binned).
+    mpm_status rebin_regular(int kpt) {
         Range nvtx_range("mpm.rebin");
         // positions are bin-local (no instance is fresh here)
         CK(cudaMemsetAsync(d_count, 0, 4 * (nkeys + 1), st));
         launch_pad_counts<R>(d_inst, (int)I.size(), d_key_base, d_count, st);
         launch_bin_count<R>(d_inst, (int)I.size(), ps[cur], d_key_base, false, d_pos, d_key, d_rank, d_count,
-                            d_newbin, cap_total, st);
+                            d_newbin, cap_total, kpt, sort_every, false, st);
         exclusive_scan(d_count, d_offset, nkeys, d_scan_tmp, st);
-        MS(det_ranks());
         launch_bin_scatter<R>(ps[cur], ps[cur ^ 1], d_inst, (int)I.size(), d_key, d_rank, d_offset, d_key_base,
-                              d_newbin, false, d_pos, has_K, cap_total, d_perm, st, det);
+                              d_newbin, false, d_pos, has_K, cap_total, d_perm, d_bin_key, max_work, st);
         build_work(d_offset, d_bin_key, d_bin_inst, d_bin_local, d_inst_pbase, max_work, d_flag, d_flag_scan,
                    d_scan_tmp, d_work, d_nwork, st);
         cur ^= 1;
-        since_sort = 0;
         ++n_sorts;
         return MPM_OK;
     }
@@ -1749,6 +1823,7 @@ class Engine final : public EngineBase {
         a.push_back({(char*)(s.id + pbase), 4});
         a.push_back({(char*)(s.bin + pbase), 4});
         a.push_back({(char*)(s.orig + pbase), 4});
+        a.push_back({(char*)(s.skey + pbase), 4});
         return a;
     }
     int ckpt_samples(const InstHost& x) const { return x.tool.mode == MPM_TOOL_RASTER ? x.n_samples : 0; }
@@ -1785,6 +1860,7 @@ class Engine final : public EngineBase {
         h.has_K = has_K ? 1 : 0;
         h.n_samples = ns;
         h.np = x.np;
+        h.since_rebin = x.since;
         h.step = x.step;
         h.time = x.time;
         h.tool_t0 = x.tool_t0;
@@ -1852,6 +1928,8 @@ class Engine final : public EngineBase {
         x.p = h.params;
         x.tool = h.tool;
         x.np = n;
+        x.since = std::max(h.since_rebin, 0);
+        x.rebin_now = false;
         x.step = h.step;
         x.time = h.time;
         x.tool_t0 = h.tool_t0;
@@ -1859,7 +1937,7 @@ class Engine final : public EngineBase {
         x.fresh = 0;
         x.ext_pending = false;
         x.pext_pending = false;
-        binned = false;   // the next call that needs bins re-bins from the loaded bins
+        binned = false;   // the next call re-bins; the loaded instance keeps its saved layout
         return push_insts();
     }
 

@@ -37,6 +37,9 @@ struct InstHost {
     int64_t cap = 0, np = 0, pbase = 0;
     int64_t nn = 0, grid_off = 0;  // grid nodes and offset (in nodes) in the grid pools
     int nbx = 0, nby = 0, nbz = 0;
+    int bin0 = 0;                  // first bin of the instance in the engine's bin table
+    int since = 0;                 // G2P steps since the re-bin that last moved its particles
+    bool rebin_now = false;        // positions changed outside a step: bin from them at the next re-bin
     double time = 0.0, dt = 0.0;
     int64_t step = 0;
     double* d_samples = nullptr;

@@ -72,33 +72,27 @@ void launch_step(const Inst<R>* insts, const Work* work, const int* n_work, int 
                  const StepArgs& a, int rbuf, bool g2p, bool p2g, int threads, int ctas_per_sm, int* err,
                  unsigned long long* counters, cudaStream_t st);
 
-// Deterministic mode: the grid of every instance from the node contributions
-// of a P2G-only launch (27 rows of `stride` V4<R>), into grid buffer rbuf.
+// Deterministic mode: the grid buffer b of every instance from the node
+// tiles the step launch stored per work item (part, part_items items) and the
+// escaped fixed-point sums; one CTA per two bins of the batch bin table.
 template <typename R>
-void launch_p2g_det(const Inst<R>* insts, int n_inst, const void* contrib, int64_t stride, const int32_t* key_base,
-                    const int32_t* offset, int rbuf, int64_t nn_total, cudaStream_t st);
-
-// Deterministic mode, the re-bin: replaces the arrival-order ranks of
-// launch_bin_count by ranks in slot order within each key (a stable radix
-// sort of the keys; unused slots take their instance's pad key).  keys2,
-// slots, perm and sorted hold np int32 each; tmp holds
-// det_rank_tmp_bytes(np, nkeys).
-size_t det_rank_tmp_bytes(int64_t np, int64_t nkeys);
-template <typename R>
-void launch_det_ranks(const Inst<R>* insts, int n_inst, const int32_t* key_base, int32_t* key, const int32_t* offset,
-                      int32_t* rank, int64_t np, int64_t nkeys, int32_t* keys2, int32_t* slots, int32_t* perm,
-                      int32_t* sorted, void* tmp, size_t tmp_bytes, cudaStream_t st);
+void launch_node_sum(const Inst<R>* insts, const int32_t* bin_inst, const int32_t* bin_local, const int32_t* flag,
+                     const int32_t* flag_scan, const R* part, int64_t part_items, int b, int nbins_total,
+                     cudaStream_t st);
 
 template <typename R>
 void launch_bin_count(const Inst<R>* insts, int n_inst, const PState<R>& ps, const int32_t* key_base, bool initial,
                       const double* pos_scratch, int32_t* key, int32_t* rank, int32_t* count, int32_t* newbin,
-                      int64_t np, cudaStream_t st);
+                      int64_t np, int kpt, int sort_every, bool keep_all, cudaStream_t st);
 
+// The re-bin's move: every particle to its slot in the new layout, each
+// cell's particles in the order of their old slots (bin_key: the first key
+// of each of the nbins_total bins of the bin table).
 template <typename R>
 void launch_bin_scatter(const PState<R>& src, const PState<R>& dst, const Inst<R>* insts, int n_inst,
                         const int32_t* key, const int32_t* rank, const int32_t* offset, const int32_t* key_base,
                         const int32_t* newbin, bool initial, const double* pos_scratch, bool has_K, int64_t np,
-                        int32_t* perm, cudaStream_t st, bool det = false);
+                        int32_t* perm, const int32_t* bin_key, int nbins_total, cudaStream_t st);
 
 template <typename R>
 void launch_pad_counts(const Inst<R>* insts, int n_inst, const int32_t* key_base, int32_t* count, cudaStream_t st);

@@ -64,16 +64,19 @@ inline PoolBytes pool_bytes(int precision, bool backstress, bool deterministic =
     const double v4 = precision == MPM_PREC_F64 ? 32.0 : 16.0, r = precision == MPM_PREC_F64 ? 8.0 : 4.0;
     PoolBytes b;
     // A0-A5, B0-B3, S0-S1 (+K0-K1), X (FP32 only), sres, status, shear
-    // counter, id, bin, orig; two buffers; sort key, rank, new bin (int32) and
-    // the FP64 position scratch
+    // counter, id, bin, orig, re-bin key; two buffers; sort key, rank, new
+    // bin (int32) and the FP64 position scratch
     const double nv4 = 12.0 + (backstress ? 2.0 : 0.0) + (precision == MPM_PREC_F64 ? 0.0 : 1.0);
-    b.particle = 2.0 * (nv4 * v4 + r + 2.0 + 12.0) + 12.0 + 24.0 + 4.0;   // + the re-bin permutation
-    // deterministic mode: 27 node contributions (4 reals each), four int32 sort
-    // arrays and the radix sort's double buffers
-    if (deterministic) b.particle += 27.0 * v4 + 16.0 + 16.0;
+    b.particle = 2.0 * (nv4 * v4 + r + 2.0 + 16.0) + 12.0 + 24.0 + 4.0;   // + the re-bin permutation
     b.node = 2.0 * v4 + 3.0 * r + 4.0;   // two grid buffers, three heat-conduction arrays, tool mask (int32)
     b.key = 8.0;                 // count and offset
     b.bin = 40.0;                // bin tables, flags and the work item
+    // deterministic mode: the escaped fixed-point sums (5 x int64 per node),
+    // each work item's stored node tile (5 x 216 reals) and its escape mark
+    if (deterministic) {
+        b.node += 5.0 * 8.0;
+        b.bin += 5.0 * 216.0 * r + 4.0;
+    }
     return b;
 }
 

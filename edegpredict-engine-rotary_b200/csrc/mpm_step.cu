@@ -31,7 +31,7 @@ namespace mpmb {
 // check counts, records the first site and index (mpm_check_report) and skips
 // the access, so no check traps.  Default builds compile every check away.
 enum : int { kSiteParticle = 1, kSiteFlush = 2, kSiteScatter = 3, kSiteGather = 4, kSiteHeat = 5, kSiteBin = 6,
-             kSiteDetCell = 7, kSiteDetRow = 8 };
+             kSiteNodeSum = 7, kSitePart = 8 };
 #ifdef MPMB_CHECKED
 struct CheckRecord {
     unsigned long long count;
@@ -74,6 +74,23 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, u
         "[%2];" ::"r"(smem_u32(dst)),
         "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
         : "memory");
+}
+// Bulk prefetch of [p, p + bytes) into L2 (p and bytes multiples of 16).
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+    if (bytes) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+// ... of a byte range of any alignment, widened to 16-byte bounds (the
+// allocations are padded to 256 bytes).
+__device__ __forceinline__ void prefetch_l2_any(const void* p, int64_t bytes) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p) & ~(uintptr_t)15;
+    const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + (uintptr_t)bytes + 15) & ~(uintptr_t)15;
+    prefetch_l2(reinterpret_cast<const void*>(a), (uint32_t)(e - a));
+}
+// Prefetch of the tile at coordinates (c0, c1, c2, c3) of a tensor map into L2.
+__device__ __forceinline__ void tma_prefetch_4d(const CUtensorMap* map, int c0, int c1, int c2, int c3) {
+    asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(map), "r"(c0),
+                 "r"(c1), "r"(c2), "r"(c3)
+                 : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
@@ -337,6 +354,19 @@ template <typename R> struct ScatterIn {
     int g0[3];
 };
 
+// Deterministic mode: channel ch of node gi gets v in fixed point (rounded to
+// a multiple of 1/esc_scale, clamped to +-4e18 units; integer adds commute, so
+// the escaped sums do not depend on the order of the particles).
+template <typename R>
+__device__ __forceinline__ void esc_add(const Inst<R>& P, int64_t gi, int ch, R v) {
+    const double q = fmin(fmax((double)v * P.esc_scale, -4.0e18), 4.0e18);
+    atomicAdd(&P.esc[ch * P.esc_stride + gi], (unsigned long long)__double2ll_rn(q));
+}
+// ... and marks the bin whose 4x4x4 core holds node (gx, gy, gz) for k_node_sum.
+template <typename R> __device__ __forceinline__ void esc_mark(const Inst<R>& P, int gx, int gy, int gz) {
+    P.esc_flag[gx / kBin + P.nbx * (gy / kBin + P.nby * (gz / kBin))] = 1;
+}
+
 template <typename R>
 __device__ __noinline__ void scatter_global(const Inst<R>& P, V4<R>* __restrict__ grid, const ScatterIn<R> in, R m) {
     R w[3][3], dw[3][3];
@@ -360,7 +390,15 @@ __device__ __noinline__ void scatter_global(const Inst<R>& P, V4<R>* __restrict_
                            in.S[a * 3] * g0 + in.S[a * 3 + 1] * g1 + in.S[a * 3 + 2] * g2;
                 const int64_t gi = gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz);
                 if (!MPMB_CHECK(gi >= 0 && gi < P.nn, kSiteScatter, gi)) continue;
-                vec_atomic_add<R>(&grid[gi], ww * m, p[0], p[1], p[2]);
+                if (P.esc) {
+                    esc_add<R>(P, gi, 0, ww * m);
+                    esc_add<R>(P, gi, 1, p[0]);
+                    esc_add<R>(P, gi, 2, p[1]);
+                    esc_add<R>(P, gi, 3, p[2]);
+                    esc_mark<R>(P, gx, gy, gz);
+                } else {
+                    vec_atomic_add<R>(&grid[gi], ww * m, p[0], p[1], p[2]);
+                }
             }
         }
     }
@@ -388,7 +426,12 @@ __device__ __noinline__ void scatter_T_global(const Inst<R>& P, R* __restrict__ 
                 if (gz < 0 || gz >= P.nz) continue;
                 const int64_t gi = gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz);
                 if (!MPMB_CHECK(gi >= 0 && gi < P.nn, kSiteHeat, gi)) continue;
-                atomicAdd(&tw[gi], w[0][i] * w[1][j] * w[2][k] * mT);
+                if (P.esc) {
+                    esc_add<R>(P, gi, 4, w[0][i] * w[1][j] * w[2][k] * mT);
+                    esc_mark<R>(P, gx, gy, gz);
+                } else {
+                    atomicAdd(&tw[gi], w[0][i] * w[1][j] * w[2][k] * mT);
+                }
             }
         }
     }
@@ -827,37 +870,62 @@ __device__ __noinline__ ContactOut particle_contact_sdf(const Inst<R>& P, double
 // Particles staged per pass and scatter payload per particle:
 //   [0..2] xi (bin-local, after the move)  [3..5] Q = m (v - dx C d) + f_ext dt
 //   [6..14] R = m dx C (row-major)         [15..23] S = -dt V J sigma / dx (row-major)
-// FP32 passes stage 2 x 128 particles (about 4 per cell at 8 per cell):
-// half the barriers and accumulation rounds of 128-particle passes
-#ifndef MPMB_CHUNK_F32
-#define MPMB_CHUNK_F32 2
-#endif
+// FP32 passes stage CH x 128 particles, CH in {1, 2, 4} (the launch
+// config's pass size, 256 by default: about 4 per cell at 8 per cell, half
+// the barriers and accumulation rounds of 128-particle passes); FP64 passes
+// stage 128.
 #ifndef MPMB_MIN_CTAS
 #define MPMB_MIN_CTAS 4
 #endif
-template <typename R> struct StepCfg {
-    static constexpr int kChunk = sizeof(R) == 4 ? MPMB_CHUNK_F32 * kNT : kNT;
+constexpr int kDefaultChunk = 2;
+template <typename R, int CH> struct StepCfg {
+    static constexpr int kChunk = sizeof(R) == 4 ? CH * kNT : kNT;
     static constexpr int kPerThread = kChunk / kNT;
+    static constexpr int kMaskWords = kChunk / 32;   // words of a cell's slot mask
 };
 constexpr int kPay = 24;
 constexpr int kOff = 27;  // stencil offsets, off = i + 3j + 9k
 
-// Staging slots per base cell and pass; a particle beyond them scatters
-// straight to the grid (counted with the escaped updates).
-constexpr int kCellCap = 16;
+// Staged particles of a pass are recorded per base cell as bit masks, so
+// that the cell's thread pair takes them in a fixed order whatever order the
+// atomics set the bits in.  In the column layout the particle in slot s of a
+// pass is filed under cell s mod 64 (row s / 64) unless it overflowed its
+// column or has moved since the re-bin: a "home" particle (base cell = s mod
+// 64) sets bit s / 64 of its cell's home mask, any other sets bit s of the
+// cell's foreign mask (kMaskWords words of 32 slots) and bit 31 of the home
+// mask.  The cell takes its home rows in ascending order, then its foreign
+// slots in ascending order.
+template <typename R, int CH> struct SlotIter {
+    uint32_t bits;    // bits left in the current word
+    uint32_t home;    // the cell's home mask (bit 31: foreign slots present)
+    int q;            // -1: the home rows; >= 0: foreign word q
+    int cell;
+    __device__ __forceinline__ SlotIter(uint32_t h, int c) : bits(h & 0x7fffffffu), home(h), q(-1), cell(c) {}
+    // the next staged slot of the cell, or false when none is left
+    template <typename Mask> __device__ __forceinline__ bool next(const Mask& fmask, int& e) {
+        while (bits == 0u) {
+            if ((home >> 31) == 0u || ++q >= StepCfg<R, CH>::kMaskWords) return false;
+            bits = fmask[q][cell];
+        }
+        const int b = __ffs((int)bits) - 1;
+        bits &= bits - 1u;
+        e = q < 0 ? (b << 6) | cell : (q << 5) | b;
+        return true;
+    }
+};
 
 // EXT: the kernel variant with the extensions (adiabatic shear heating, heat
 // conduction), which adds the payload's absolute temperature (row kPay), the
 // T m node sums (nacc[4]) and the node temperature tile with its m > 1e-18
 // mask (ttile).
-template <typename R, bool EXT> struct StepSmem {
+template <typename R, bool EXT, int CH> struct StepSmem {
     // The TMA tile is read only by the fill at the start of a bin and the payload
     // only inside the bin's passes, with barriers between: one buffer holds both,
     // which keeps four CTAs within the 164 KB shared-memory carveout (92 KB of L1
     // left for the register spills).
     union {
         V4<R> raw[kTileNodes];                          // TMA destination (offset 0 of the 128-byte aligned block)
-        R pay[EXT ? kPay + 1 : kPay][StepCfg<R>::kChunk];  // scatter payload of the staged particles
+        R pay[EXT ? kPay + 1 : kPay][StepCfg<R, CH>::kChunk];  // scatter payload of the staged particles
     };
     R vel[3][kPlane];                      // node velocities after the grid update
     // the bin's node sums m, p_x, p_y, p_z (, T m) (tidx layout), one copy per
@@ -865,14 +933,16 @@ template <typename R, bool EXT> struct StepSmem {
     // adds need no atomics (the flush sums the two)
     R nacc[2][EXT ? 5 : 4][kPlane];
     R ttile[EXT ? 2 : 1][EXT ? kPlane : 1];  // node temperatures and their m > 1e-18 mask
-    short slot[kCellCap][kCellsPerBin];    // staged particles of each base cell, by rank (the cells of a warp
-                                           // read consecutive entries)
-    int cnt[2][kCellsPerBin];              // staged particles per cell (atomic ranks), by pass parity
+    // staged slots of each base cell, by pass parity (see SlotIter): home rows,
+    // and foreign slots with bit s of word q for slot 32 q + s (the cells of a
+    // warp read consecutive words)
+    uint32_t hmask[2][kCellsPerBin];
+    uint32_t fmask[2][StepCfg<R, CH>::kMaskWords][kCellsPerBin];
     uint64_t mbar;
     int fail;
 };
 
-template <typename R, bool EXT> constexpr size_t step_smem_bytes() { return sizeof(StepSmem<R, EXT>); }
+template <typename R, bool EXT, int CH> constexpr size_t step_smem_bytes() { return sizeof(StepSmem<R, EXT, CH>); }
 
 // Momentum + impulse of one channel a over the 27 stencil nodes (i,j,k) of a
 // particle, relative to its base node:
@@ -918,18 +988,26 @@ __device__ __forceinline__ void channel_add(const R (&w)[3][3], const R (&dw)[3]
 // costs several times a plain add on this part).  Every lane takes part in
 // every phase (a cell without particles adds zeros), so the warp stays
 // converged at each __syncwarp.  par: parity of the staging pass.
-template <typename R, bool EXT>
-__device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT>& Sm, int cell, int h, int half, R pm, int par,
+template <typename R, bool EXT, int CH>
+__device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT, CH>& Sm, int cell, int h, int half, R pm, int par,
                                                 bool heat) {
     R a0[kOff], a1[kOff];
 #pragma unroll
     for (int o = 0; o < kOff; ++o) { a0[o] = R(0); a1[o] = R(0); }
-    const int n = min(Sm.cnt[par][cell], kCellCap);
-    // the other parity's counts were last read in the previous pass: clear
+    constexpr int kW = StepCfg<R, CH>::kMaskWords;
+    // the other parity's masks were last read in the previous pass: clear
     // them for the next one
-    if (h == 0) Sm.cnt[par ^ 1][cell] = 0;
-    for (int q = 0; q < n; ++q) {
-        const int e = Sm.slot[q][cell];
+    if (h == 0) {
+        const uint32_t old = Sm.hmask[par ^ 1][cell];
+        Sm.hmask[par ^ 1][cell] = 0u;
+        if (old >> 31) {
+#pragma unroll
+            for (int q = 0; q < kW; ++q) Sm.fmask[par ^ 1][q][cell] = 0u;
+        }
+    }
+    const uint32_t home = Sm.hmask[par][cell];
+    SlotIter<R, CH> it(home, cell);
+    for (int e; it.next(Sm.fmask[par], e);) {
         R w[3][3], dw[3][3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) (void)bspline(Sm.pay[a][e], w[a], dw[a]);
@@ -975,8 +1053,8 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT>& Sm, int cell, 
         // lighter half of the pair takes it)
 #pragma unroll
         for (int o = 0; o < kOff; ++o) a0[o] = R(0);
-        for (int q = 0; q < n; ++q) {
-            const int e = Sm.slot[q][cell];
+        SlotIter<R, CH> ih(home, cell);
+        for (int e; ih.next(Sm.fmask[par], e);) {
             R w[3][3], dw[3][3];
 #pragma unroll
             for (int a = 0; a < 3; ++a) (void)bspline(Sm.pay[a][e], w[a], dw[a]);
@@ -1007,43 +1085,13 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT>& Sm, int cell, 
     }
 }
 
-// Deterministic mode: the 27 node contributions of one particle to det_contrib
-// (row o = i + 3j + 9k of the stencil, relative to the particle's base node):
-// (m w_ijk, w_ijk (Q + R (i,j,k)) + S grad w_ijk).  Q = NULL writes zeros (a
-// particle that contributes nothing).
-template <typename R>
-__device__ __noinline__ void det_contrib(const StepArgs& sa, int64_t pi, R m, const R* xi, const R* Q, const R* Rm,
-                                         const R* S) {
-    if (!MPMB_CHECK(pi >= 0 && pi < sa.det_stride, kSiteDetRow, pi)) return;
-    V4<R>* c = static_cast<V4<R>*>(sa.det_contrib) + pi;
-    const int64_t ds = sa.det_stride;
-    if (!Q) {
-        for (int o = 0; o < 27; ++o) c[o * ds] = mk4<R>(R(0), R(0), R(0), R(0));
-        return;
-    }
-    R w[3][3], dw[3][3];
-    for (int a = 0; a < 3; ++a) (void)bspline(xi[a], w[a], dw[a]);
-    for (int k = 0; k < 3; ++k)
-        for (int j = 0; j < 3; ++j)
-            for (int i = 0; i < 3; ++i) {
-                const R wijk = w[0][i] * w[1][j] * w[2][k];
-                const R gx = dw[0][i] * w[1][j] * w[2][k], gy = w[0][i] * dw[1][j] * w[2][k],
-                        gz = w[0][i] * w[1][j] * dw[2][k];
-                R p[3];
-                for (int a = 0; a < 3; ++a)
-                    p[a] = wijk * (Q[a] + Rm[3 * a] * R(i) + Rm[3 * a + 1] * R(j) + Rm[3 * a + 2] * R(k)) +
-                           S[3 * a] * gx + S[3 * a + 1] * gy + S[3 * a + 2] * gz;
-                c[(i + 3 * j + 9 * k) * ds] = mk4<R>(m * wijk, p[0], p[1], p[2]);
-            }
-}
-
-template <typename R, bool G2P, bool P2G, bool EXT, bool DET = false>
+template <typename R, bool G2P, bool P2G, bool EXT, int CH>
 __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __restrict__ insts, const Work* __restrict__ work,
                                               const int* __restrict__ n_work, PState<R> ps, StepArgs sa, int rbuf,
                                               int* __restrict__ err, unsigned long long* __restrict__ ctr) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    StepSmem<R, EXT>& Sm = *reinterpret_cast<StepSmem<R, EXT>*>(smem_raw);
-    constexpr int kChunk = StepCfg<R>::kChunk;
+    StepSmem<R, EXT, CH>& Sm = *reinterpret_cast<StepSmem<R, EXT, CH>*>(smem_raw);
+    constexpr int kChunk = StepCfg<R, CH>::kChunk;
     const int tid = threadIdx.x, lane = tid & 31;
     const int nw = *n_work;
     uint32_t phase = 0;
@@ -1055,7 +1103,8 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
         fence_async_smem();
     }
     if (tid == 0) Sm.fail = 0;
-    if (tid < 2 * kCellsPerBin) (&Sm.cnt[0][0])[tid] = 0;
+    for (int q = tid; q < 2 * kCellsPerBin; q += kNT) (&Sm.hmask[0][0])[q] = 0u;
+    for (int q = tid; q < 2 * StepCfg<R, CH>::kMaskWords * kCellsPerBin; q += kNT) (&Sm.fmask[0][0][0])[q] = 0u;
     // node sums start at zero; the end-of-bin flush clears what it reads
     if (P2G)
         for (int q = tid; q < 2 * (EXT ? 5 : 4) * kPlane; q += kNT) (&Sm.nacc[0][0][0])[q] = R(0);
@@ -1073,6 +1122,30 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                             (int64_t)wk.start + wk.count <= P.np,
                         kSiteBin, wi))
             continue;
+        if (tid == 0 && wi + (int)gridDim.x < nw) {
+            // the work item this CTA takes next: its particle state and its
+            // grid tile into L2 while this one is processed
+            const Work wn = work[wi + gridDim.x];
+            const Inst<R>& Pn = insts[wn.inst];
+            if (wn.count > 0 && wn.start >= 0 && (int64_t)wn.start + wn.count <= Pn.np) {
+                const int64_t p0 = Pn.pbase + wn.start;
+                const uint32_t vb = (uint32_t)wn.count * (uint32_t)sizeof(V4<R>);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) prefetch_l2(ps.A[q] + p0, vb);
+                if (P2G) {
+                    prefetch_l2(ps.A[4] + p0, vb);
+                    prefetch_l2(ps.A[5] + p0, vb);
+                }
+                if (G2P && ps.X) prefetch_l2(ps.X + p0, vb);
+                if (!G2P) prefetch_l2(ps.B[0] + p0, vb);
+                prefetch_l2_any(ps.status + p0, wn.count);
+                if (G2P) {
+                    const int nbx = wn.bin % Pn.nbx, nby = (wn.bin / Pn.nbx) % Pn.nby, nbz = wn.bin / (Pn.nbx * Pn.nby);
+                    if (wn.inst != wk.inst) tmap_acquire(&Pn.tmap[rbuf]);
+                    tma_prefetch_4d(&Pn.tmap[rbuf], 0, nbx * kBin, nby * kBin, nbz * kBin);
+                }
+            }
+        }
         const double tg = da(P.t0, dm((double)sa.k, P.dt));         // time of the G2P step
         const double tp = da(P.t0, dm((double)sa.p2g_step, P.dt));  // time of the P2G step
         const double prg0 = da(P.tool_p0[0], dm(P.tool_v[0], ds(tg, P.tool_t0)));
@@ -1100,6 +1173,12 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
             last_inst = wk.inst;
             __syncthreads();
             if (Sm.fail) {
+                // The tile copy has not landed after 4 s.  If it is only late
+                // rather than lost, it can still write Sm.raw after this CTA
+                // has returned, into shared memory that the SM's next CTA may
+                // own.  The error word is never cleared: every later status or
+                // metrics call on the handle returns MPM_TIMEOUT, and the
+                // caller is expected to stop using it.
                 if (tid == 0) atomicOr(err, ERR_TIMEOUT);
                 return;
             }
@@ -1125,7 +1204,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
         const bool chip_now = G2P && P.chip_every > 0 && ((P.step0 + sa.k) % P.chip_every) == 0;
         for (int base = 0; base < wk.count; base += kChunk) {
 #pragma unroll 1
-            for (int sidx = 0; sidx < StepCfg<R>::kPerThread; ++sidx) {
+            for (int sidx = 0; sidx < StepCfg<R, CH>::kPerThread; ++sidx) {
                 const int slot = tid + sidx * kNT;
                 const int pl = base + slot;
                 // every load of the particle is issued here, before any branch on its
@@ -1357,7 +1436,6 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                         if (!(f0 >= R(1 - g0x) && f0 < R(P.nx - 2 - g0x) && f1 >= R(1 - g0y) &&
                               f1 < R(P.ny - 2 - g0y) && f2 >= R(1 - g0z) && f2 < R(P.nz - 2 - g0z))) {
                             if (!isfinite(f0 + f1 + f2)) reinterpret_cast<unsigned char*>(P.ierr)[0] = 1;
-                            if (DET) det_contrib<R>(sa, pi, R(0), xi, nullptr, nullptr, nullptr);
                             st = ST_INACTIVE;
                             if (G2P) {
                                 // no later G2P writes this particle: store this step's v, strain rate and C
@@ -1477,26 +1555,15 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                 S[2] = sf * sig[4]; S[6] = sf * sl[1];
                                 S[5] = sf * sig[5]; S[7] = sf * sl[2];
                             }
-                            if (DET) {
-                                // deterministic mode: the particle's 27 node contributions
-                                // (m, p) go to global memory, and k_p2g_det sums each node's
-                                // in a fixed order (no atomics).  w_ijk (Q + R (i,j,k)) +
-                                // S grad(w_ijk), the sum that cell_accumulate forms per cell.
-                                det_contrib<R>(sa, pi, m, xi, Q, Rm, S);
-                                // binned just before this launch (the re-bin puts every
-                                // base in its bin), so this counts nothing
-                                if (!(bb[0] >= 0 && bb[0] < kBin && bb[1] >= 0 && bb[1] < kBin && bb[2] >= 0 &&
-                                      bb[2] < kBin))
-                                    ++c_esc;
-                            } else {
-                            int rank = kCellCap;
                             if (bb[0] >= 0 && bb[0] < kBin && bb[1] >= 0 && bb[1] < kBin && bb[2] >= 0 &&
                                 bb[2] < kBin) {
                                 const int scell = bb[0] + kBin * (bb[1] + kBin * bb[2]);
-                                rank = atomicAdd(&Sm.cnt[par][scell], 1);
-                                if (rank < kCellCap) Sm.slot[rank][scell] = (short)slot;
-                            }
-                            if (rank < kCellCap) {
+                                if (scell == (slot & (kCellsPerBin - 1))) {
+                                    atomicOr(&Sm.hmask[par][scell], 1u << (slot >> 6));
+                                } else {
+                                    atomicOr(&Sm.fmask[par][slot >> 5][scell], 1u << (slot & 31));
+                                    atomicOr(&Sm.hmask[par][scell], 0x80000000u);
+                                }
                                 if (EXT) Sm.pay[EXT ? kPay : 0][slot] = P.Tamb + dT;   // absolute T (heat conduction)
                                 Sm.pay[0][slot] = xi[0]; Sm.pay[1][slot] = xi[1]; Sm.pay[2][slot] = xi[2];
 #pragma unroll
@@ -1515,7 +1582,6 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                     scatter_T_global<R>(P, P.tm[rbuf ^ (G2P ? 1 : 0)], g0x, g0y, g0z, xi[0], xi[1],
                                                         xi[2], m * (P.Tamb + dT));
                                 ++c_esc;
-                            }
                             }
                         }
                     }
@@ -1545,16 +1611,30 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                     c_yield += yielded ? 1 : 0;
                 }
             }
-            if (P2G && !DET) {
+            if (P2G) {
                 __syncthreads();
-                cell_accumulate<R, EXT>(Sm, tid & (kCellsPerBin - 1), tid >> 6, (tid >> 5) & 1, P.pmass, par,
+                cell_accumulate<R, EXT, CH>(Sm, tid & (kCellsPerBin - 1), tid >> 6, (tid >> 5) & 1, P.pmass, par,
                                         P.heat_on != 0);
                 par ^= 1;
                 __syncthreads();
             }
         }
 
-        if (P2G && !DET) {
+        if (P2G && sa.part) {
+            // deterministic mode: the bin's node tile is stored for k_node_sum
+            // (every node and channel, zeros included), clearing it for the next bin
+            R* __restrict__ dst = static_cast<R*>(sa.part) + (int64_t)wi * (kPartCh * kTileNodes);
+            for (int nidx = tid; nidx < kTileNodes; nidx += kNT) {
+                const int X = nidx % kTile, Y = (nidx / kTile) % kTile, Z = nidx / (kTile * kTile);
+                const int t = tidx(X, Y, Z);
+#pragma unroll
+                for (int q = 0; q < (EXT ? 5 : 4); ++q) {
+                    dst[q * kTileNodes + nidx] = Sm.nacc[0][q][t] + Sm.nacc[1][q][t];
+                    Sm.nacc[0][q][t] = R(0);
+                    Sm.nacc[1][q][t] = R(0);
+                }
+            }
+        } else if (P2G) {
             // flush the bin's node tile to the grid, clearing it for the next bin
             for (int nidx = tid; nidx < kTileNodes; nidx += kNT) {
                 const int X = nidx % kTile, Y = (nidx / kTile) % kTile, Z = nidx / (kTile * kTile);
@@ -1604,67 +1684,132 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
     else if (errf < 0) atomicOr(err, ERR_NEWTON);
 }
 
-template <typename R, bool G2P, bool P2G, bool EXT, bool DET = false> static void set_smem_attr() {
+template <typename R, bool G2P, bool P2G, bool EXT, int CH> static void set_smem_attr() {
     static bool done = false;
     if (!done) {
-        cudaFuncSetAttribute(k_step<R, G2P, P2G, EXT, DET>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)step_smem_bytes<R, EXT>());
+        cudaFuncSetAttribute(k_step<R, G2P, P2G, EXT, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)step_smem_bytes<R, EXT, CH>());
         done = true;
     }
 }
 
-// Deterministic mode, the P2G sums: one thread per grid node adds the
-// contributions (written by the P2G-only step launch) of the particles in the
-// 27 cells whose stencil covers the node, cells in z-y-x order and particles
-// in their binned order, which the deterministic re-bin fixes.  Particles
-// killed in that launch contribute zeros.  No atomics, so the grid is the same
-// bit for bit on every run and launch shape.  Every node is written (zero where
-// no particle reaches it).
+// Deterministic mode, the grid of one P2G: one thread per node of a bin's
+// 4x4x4 core (a CTA of 128 threads takes two bins of the batch's bin table)
+// adds, in a fixed order, the node's values in the stored tiles of the bins
+// whose 6x6x6 tile holds it (per axis the bin itself and, for the first two
+// layers of its core, the bin before; z, then y, then x, lower bin first),
+// then the node's escaped fixed-point sums (cleared after reading), and
+// writes the node -- zero where nothing reached it, so no clear of the grid
+// precedes the P2G.  No float atomics anywhere: with the re-bin's order fixed,
+// the grid is the same bit for bit on every run and launch shape.
 template <typename R>
-__global__ void k_p2g_det(const Inst<R>* __restrict__ insts, int n_inst, const void* __restrict__ contrib,
-                          int64_t stride, const int32_t* __restrict__ key_base, const int32_t* __restrict__ offset,
-                          int rbuf, int64_t nn_total) {
-    const int64_t gn = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gn >= nn_total) return;
-    int lo = 0, hi = n_inst - 1;   // the instance whose grid holds node gn
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) / 2;
-        if (insts[mid].gbase <= gn) lo = mid; else hi = mid - 1;
-    }
-    const Inst<R>& P = insts[lo];
-    const int64_t ln = gn - P.gbase;
-    if (ln < 0 || ln >= P.nn) return;
-    const int gx = (int)(ln % P.nx), gy = (int)((ln / P.nx) % P.ny), gz = (int)(ln / ((int64_t)P.nx * P.ny));
-    const V4<R>* __restrict__ c = static_cast<const V4<R>*>(contrib);
-    R m = R(0), p[3] = {R(0), R(0), R(0)};
-    for (int cz = max(gz - 2, 0); cz <= gz; ++cz)
-        for (int cy = max(gy - 2, 0); cy <= gy; ++cy)
-            for (int cx = max(gx - 2, 0); cx <= gx; ++cx) {
-                const int bx = cx / kBin, by = cy / kBin, bz = cz / kBin;
-                if (bx >= P.nbx || by >= P.nby || bz >= P.nbz) continue;
-                const int bin = bx + P.nbx * (by + P.nby * bz);
-                const int cell = (cx - bx * kBin) + kBin * ((cy - by * kBin) + kBin * (cz - bz * kBin));
-                const int key = key_base[lo] + bin * kCellsPerBin + cell;
-                // every particle of the cell has its base at the cell (deterministic re-bin)
-                const V4<R>* __restrict__ row = c + (int64_t)((gx - cx) + 3 * (gy - cy) + 9 * (gz - cz)) * stride;
-                const int64_t s1 = offset[key + 1];
-                if (!MPMB_CHECK(offset[key] >= P.pbase && s1 <= P.pbase + P.pcap, kSiteDetCell, key)) continue;
-                for (int64_t s = offset[key]; s < s1; ++s) {
-                    const V4<R> v = row[s];
-                    m += v.x; p[0] += v.y; p[1] += v.z; p[2] += v.w;
+__global__ void __launch_bounds__(128) k_node_sum(const Inst<R>* __restrict__ insts, const int32_t* __restrict__ bin_inst,
+                                                  const int32_t* __restrict__ bin_local,
+                                                  const int32_t* __restrict__ flag,
+                                                  const int32_t* __restrict__ flag_scan, const R* __restrict__ part,
+                                                  int64_t part_items, int b, int nbins_total) {
+    const int gb = blockIdx.x * 2 + (threadIdx.x >> 6);
+    const int c = threadIdx.x & (kCellsPerBin - 1);
+    const bool have = gb < nbins_total;
+    const Inst<R>* P = have ? &insts[bin_inst[gb]] : insts;
+    const int lb = have ? bin_local[gb] : 0;
+    bool esc = false;
+    if (have) {
+        const int bx = lb % P->nbx, by = (lb / P->nbx) % P->nby, bz = lb / (P->nbx * P->nby);
+        const int gx = bx * kBin + (c & 3), gy = by * kBin + ((c >> 2) & 3), gz = bz * kBin + (c >> 4);
+        R acc[kPartCh] = {R(0), R(0), R(0), R(0), R(0)};
+        const int nch = P->heat_on ? 5 : 4;
+        for (int z = bz - 1; z <= bz; ++z) {
+            const int Z = gz - z * kBin;
+            if (z < 0 || Z >= kTile) continue;
+            for (int y = by - 1; y <= by; ++y) {
+                const int Y = gy - y * kBin;
+                if (y < 0 || Y >= kTile) continue;
+                for (int x = bx - 1; x <= bx; ++x) {
+                    const int X = gx - x * kBin;
+                    if (x < 0 || X >= kTile) continue;
+                    const int g = P->bin0 + x + P->nbx * (y + P->nby * z);
+                    if (!flag[g]) continue;
+                    const int64_t wi = flag_scan[g];
+                    if (!MPMB_CHECK(wi >= 0 && wi < part_items, kSitePart, wi)) continue;
+                    const R* __restrict__ t = part + wi * (kPartCh * kTileNodes) + X + kTile * (Y + kTile * Z);
+                    for (int q = 0; q < nch; ++q) acc[q] += t[q * kTileNodes];
                 }
             }
-    P.grid[rbuf][ln] = mk4<R>(m, p[0], p[1], p[2]);
+        }
+        if (gx < P->nx && gy < P->ny && gz < P->nz) {
+            const int64_t li = gx + (int64_t)P->nx * (gy + (int64_t)P->ny * gz);
+            esc = P->esc != nullptr && P->esc_flag[lb] != 0;
+            if (esc) {
+                for (int q = 0; q < nch; ++q) {
+                    unsigned long long* e = &P->esc[q * P->esc_stride + li];
+                    const long long v = (long long)*e;
+                    if (v != 0) {
+                        acc[q] += (R)((double)v / P->esc_scale);
+                        *e = 0ull;
+                    }
+                }
+            }
+            if (MPMB_CHECK(li >= 0 && li < P->nn, kSiteNodeSum, li)) {
+                P->grid[b][li] = mk4<R>(acc[0], acc[1], acc[2], acc[3]);
+                if (P->heat_on) P->tm[b][li] = acc[4];
+            }
+        }
+    }
+    // every thread of the bin has read its flag before it is cleared
+    __syncthreads();
+    if (have && c == 0 && P->esc != nullptr && P->esc_flag[lb] != 0) P->esc_flag[lb] = 0;
+    (void)esc;
 }
 
 template <typename R>
-void launch_p2g_det(const Inst<R>* insts, int n_inst, const void* contrib, int64_t stride, const int32_t* key_base,
-                    const int32_t* offset, int rbuf, int64_t nn_total, cudaStream_t st) {
-    if (nn_total <= 0 || n_inst <= 0) return;
-    Range nvtx_range("mpm.p2g_det");
-    k_p2g_det<R><<<(int)((nn_total + 127) / 128), 128, 0, st>>>(insts, n_inst, contrib, stride, key_base, offset,
-                                                                rbuf, nn_total);
+void launch_node_sum(const Inst<R>* insts, const int32_t* bin_inst, const int32_t* bin_local, const int32_t* flag,
+                     const int32_t* flag_scan, const R* part, int64_t part_items, int b, int nbins_total,
+                     cudaStream_t st) {
+    if (nbins_total <= 0) return;
+    Range nvtx_range("mpm.node_sum");
+    k_node_sum<R><<<(nbins_total + 1) / 2, 128, 0, st>>>(insts, bin_inst, bin_local, flag, flag_scan, part,
+                                                         part_items, b, nbins_total);
     ++launch_counter();
+}
+
+// One pass size: the G2P / P2G / extension variant of the launch.  (FP64
+// instantiates only the default pass size, whose kChunk is 128 like all of
+// its pass sizes.)
+template <typename R, int CH>
+static void launch_variant(const Inst<R>* insts, const Work* work, const int* n_work, const PState<R>& ps,
+                           const StepArgs& a, int rbuf, bool g2p, bool p2g, int grid, int* err,
+                           unsigned long long* counters, cudaStream_t st) {
+    if constexpr (sizeof(R) == 8 && CH != kDefaultChunk) {
+        launch_variant<R, kDefaultChunk>(insts, work, n_work, ps, a, rbuf, g2p, p2g, grid, err, counters, st);
+    } else if (a.ext) {
+        const size_t smem = step_smem_bytes<R, true, kDefaultChunk>();
+        if (g2p && p2g) {
+            set_smem_attr<R, true, true, true, kDefaultChunk>();
+            k_step<R, true, true, true, kDefaultChunk><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err,
+                                                                               counters);
+        } else if (g2p) {
+            set_smem_attr<R, true, false, true, kDefaultChunk>();
+            k_step<R, true, false, true, kDefaultChunk><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err,
+                                                                                counters);
+        } else {
+            set_smem_attr<R, false, true, true, kDefaultChunk>();
+            k_step<R, false, true, true, kDefaultChunk><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err,
+                                                                                counters);
+        }
+    } else {
+        const size_t smem = step_smem_bytes<R, false, CH>();
+        if (g2p && p2g) {
+            set_smem_attr<R, true, true, false, CH>();
+            k_step<R, true, true, false, CH><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+        } else if (g2p) {
+            set_smem_attr<R, true, false, false, CH>();
+            k_step<R, true, false, false, CH><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+        } else {
+            set_smem_attr<R, false, true, false, CH>();
+            k_step<R, false, true, false, CH><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
+        }
+    }
 }
 
 template <typename R>
@@ -1683,36 +1828,22 @@ void launch_step(const Inst<R>* insts, const Work* work, const int* n_work, int 
     if (max_work <= 0) return;
     int grid = sms * (ctas_per_sm > 0 ? ctas_per_sm : 4);
     if (grid > max_work) grid = max_work;
-    const size_t smem = a.ext ? step_smem_bytes<R, true>() : step_smem_bytes<R, false>();
-    if (a.det && !g2p && p2g && !a.ext) {
-        set_smem_attr<R, false, true, false, true>();
-        k_step<R, false, true, false, true><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
-    } else if (g2p && p2g && a.ext) {
-        set_smem_attr<R, true, true, true>();
-        k_step<R, true, true, true><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
-    } else if (g2p && p2g) {
-        set_smem_attr<R, true, true, false>();
-        k_step<R, true, true, false><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
-    } else if (g2p && a.ext) {
-        set_smem_attr<R, true, false, true>();
-        k_step<R, true, false, true><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
-    } else if (g2p) {
-        set_smem_attr<R, true, false, false>();
-        k_step<R, true, false, false><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
-    } else if (a.ext) {
-        set_smem_attr<R, false, true, true>();
-        k_step<R, false, true, true><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
-    } else {
-        set_smem_attr<R, false, true, false>();
-        k_step<R, false, true, false><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
-    }
+    // FP64 passes are 128 particles whatever the pass size; the extension
+    // variant runs the default pass size
+    const int ch = (sizeof(R) == 8 || a.ext) ? kDefaultChunk : a.chunk;
+    if (ch == 1)
+        launch_variant<R, 1>(insts, work, n_work, ps, a, rbuf, g2p, p2g, grid, err, counters, st);
+    else if (ch == 4)
+        launch_variant<R, 4>(insts, work, n_work, ps, a, rbuf, g2p, p2g, grid, err, counters, st);
+    else
+        launch_variant<R, kDefaultChunk>(insts, work, n_work, ps, a, rbuf, g2p, p2g, grid, err, counters, st);
     ++launch_counter();
 }
 
-template void launch_p2g_det<float>(const Inst<float>*, int, const void*, int64_t, const int32_t*, const int32_t*,
-                                    int, int64_t, cudaStream_t);
-template void launch_p2g_det<double>(const Inst<double>*, int, const void*, int64_t, const int32_t*, const int32_t*,
-                                     int, int64_t, cudaStream_t);
+template void launch_node_sum<float>(const Inst<float>*, const int32_t*, const int32_t*, const int32_t*,
+                                    const int32_t*, const float*, int64_t, int, int, cudaStream_t);
+template void launch_node_sum<double>(const Inst<double>*, const int32_t*, const int32_t*, const int32_t*,
+                                     const int32_t*, const double*, int64_t, int, int, cudaStream_t);
 template void launch_step<float>(const Inst<float>*, const Work*, const int*, int, const PState<float>&,
                                  const StepArgs&, int, bool, bool, int, int, int*, unsigned long long*, cudaStream_t);
 template void launch_step<double>(const Inst<double>*, const Work*, const int*, int, const PState<double>&,

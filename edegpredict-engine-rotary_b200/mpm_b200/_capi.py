@@ -155,11 +155,11 @@ class MpmServerStats(C.Structure):
 
 class MpmLaunchConfig(C.Structure):
     _fields_ = [("ctas_per_sm", C.c_int32), ("sort_every", C.c_int32), ("use_graph", C.c_int32),
-                ("deterministic", C.c_int32)]
+                ("deterministic", C.c_int32), ("pass_size", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {"ctas_per_sm": self.ctas_per_sm, "sort_every": self.sort_every, "use_graph": self.use_graph,
-                "deterministic": self.deterministic}
+                "deterministic": self.deterministic, "pass_size": self.pass_size}
 
 
 _lib = None

@@ -184,10 +184,13 @@ class Solver:
         return c.as_dict()
 
     def set_launch_config(self, ctas_per_sm: int = 4, sort_every: int = 16, use_graph: bool = False,
-                          deterministic: bool = False) -> None:
+                          deterministic: bool = False, pass_size: int = 0) -> None:
         """Launch shape; deterministic=True gives the same results bit for bit
-        on every run and launch shape (mpm_launch_config.deterministic)."""
-        c = A.MpmLaunchConfig(int(ctas_per_sm), int(sort_every), 1 if use_graph else 0, 1 if deterministic else 0)
+        on every run and launch shape (mpm_launch_config.deterministic);
+        pass_size: FP32 particles per pass of the step kernel (128, 256, 512;
+        0: the default)."""
+        c = A.MpmLaunchConfig(int(ctas_per_sm), int(sort_every), 1 if use_graph else 0, 1 if deterministic else 0,
+                              int(pass_size))
         self._check(self._lib.mpm_set_launch_config(self.h, C.byref(c)))
 
     def _check_state(self, status: int, strict: bool) -> None:

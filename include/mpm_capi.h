@@ -466,10 +466,13 @@ mpm_status mpm_batch_instance_status(mpm_handle *h, int32_t *status, int32_t n);
  * replaces the instance's parameters, tool, clock and particles, and clears
  * its error word.  A voxel tool SDF (mpm_set_tool_sdf) is not part of the
  * checkpoint: set it again after loading.  The state is written to and read
- * from caller memory (host or pinned); _bytes gives the size.  The particle
- * order within a cell after the reload's re-bin may differ, so continued
- * runs agree to summation order (FP64 1e-9), as a batch does with its
- * instances run alone.  Single-instance handles use inst 0. */
+ * from caller memory (host or pinned); _bytes gives the size.  The saved
+ * state includes the particles' layout (each one's re-bin key) and the
+ * instance's re-bin phase, so the reloaded instance keeps its layout and
+ * re-bins at the same steps: a resumed run continues the saving run's sums in
+ * the same order.  With the deterministic mode it gives the same bits; with
+ * the default atomics it agrees to summation order (FP64 1e-9), as a batch
+ * does with its instances run alone.  Single-instance handles use inst 0. */
 mpm_status mpm_checkpoint_bytes(mpm_handle *h, int32_t inst, int64_t *bytes);
 mpm_status mpm_checkpoint_save(mpm_handle *h, int32_t inst, void *buf, int64_t bytes);
 mpm_status mpm_checkpoint_load(mpm_handle *h, int32_t inst, const void *buf, int64_t bytes);
@@ -491,24 +494,34 @@ typedef struct mpm_launch_config {
     int32_t use_graph;     /* replay each step call's launches from a captured CUDA graph */
     /* 1: deterministic mode (no counterpart in the reference, whose P2G sums
      * with FP64 atomics in arrival order).  The results are the same bit for
-     * bit on every run and every launch shape: the particles are re-binned
-     * before every P2G with ranks from a stable sort, each particle writes its
-     * 27 node contributions (m, p) to device memory, and one thread per grid
-     * node sums those of its 27 cells in a fixed order, without atomics.  A
-     * position that rounding at the re-bin would put one cell off its key is
-     * set onto the key cell's edge (FP32: the low part takes the difference).
-     * Runs the split schedule, re-bins every step, ignores use_graph and
-     * sort_every, and holds 27 x 4 reals per particle slot more; several times
-     * slower than the default.  Not available with the adiabatic shear model, heat conduction
-     * or a voxel tool SDF (MPM_NOT_SUPPORTED at the step). */
+     * bit on every run, every launch shape and every split of the steps into
+     * calls, alone or in a batch.  The fused step kernel runs as in the
+     * default mode, with three changes: each work item stores its node tile
+     * and one thread per grid node adds the stored tiles of the bins that
+     * cover it in a fixed order (no float atomics; one extra launch per step);
+     * a particle whose stencil left its bin's tile adds to the grid in 2^-40
+     * particle-mass fixed point with integer atomics; and the re-bin's order
+     * within each cell (which it uses in both modes) is the order of the old
+     * slots.  Holds 5 x 216 reals per bin and 5 x 8 bytes per grid node more;
+     * every option runs in it (graphs included) except the
+     * MPMWorkpieceSolver semantics (MPM_NOT_SUPPORTED at the step). */
     int32_t deterministic;
+    /* FP32 particles staged per pass of the step kernel: 128, 256 or 512
+     * (0: the default, 256).  A larger pass halves the passes' barriers and
+     * node-tile adds and takes more shared memory per CTA (512: three CTAs
+     * per SM).  FP64 and the kernel variant with the adiabatic shear model,
+     * heat conduction or the voxel contact stage 256 (FP64: 128) whatever
+     * this says. */
+    int32_t pass_size;
 } mpm_launch_config;
 mpm_status mpm_get_launch_config(const mpm_handle *h, mpm_launch_config *out);
 mpm_status mpm_set_launch_config(mpm_handle *h, const mpm_launch_config *cfg);
-/* Times every candidate launch shape (CTAs per SM in {2,3,4} x re-bin every
- * {8,16,32} steps) over one re-bin period of real steps each (168 steps in
- * all, dt[i] per instance, counted like any other steps) and keeps the
- * fastest; *chosen (may be NULL) receives it. */
+/* Picks the launch shape by timing real steps (dt[i] per instance, counted
+ * like any other steps): first the pass size (128, 256, 512 FP32 particles,
+ * 16 steps each at the current CTAs and cadence), then, at the fastest pass
+ * size, every CTAs per SM in {2,3,4} x re-bin every {8,16,32} steps over one
+ * re-bin period each (216 steps in all).  Keeps the fastest; *chosen (may be
+ * NULL) receives it. */
 mpm_status mpm_autotune(mpm_handle *h, const double *dt, mpm_launch_config *chosen);
 
 /*
@@ -614,10 +627,11 @@ mpm_status mpm_selftest_bounded_wait(int64_t limit_ns, void *stream);
  * no sanitizer runs).  libmpm_b200_checked.so, built with -DMPMB_CHECKED,
  * checks every index its step kernels derive from data (particle slots of a
  * work item, grid nodes of the tile flush and of the off-tile scatter and
- * gather, heat-conduction nodes, deterministic-mode cells and rows) before
- * using it; a failed check is counted, the first one's site (1 particle slot,
- * 2 tile flush, 3 scatter, 4 gather, 5 heat scatter, 6 work item, 7 and 8
- * deterministic cell range and row) and index are kept, and the access is
+ * gather, heat-conduction nodes, the deterministic mode's node sums and
+ * stored tiles) before using it; a failed check is counted, the first one's
+ * site (1 particle slot, 2 tile flush, 3 scatter, 4 gather, 5 heat scatter,
+ * 6 work item, 7 node of the deterministic node sum, 8 its stored tile) and
+ * index are kept, and the access is
  * skipped rather than trapped.  This reads the record after synchronising the
  * device, and clears it when reset != 0.  The default library has no checks
  * and returns MPM_NOT_SUPPORTED with zeros. */

@@ -54,10 +54,11 @@ static mpm_status chk(const std::vector<unsigned char>& b, int prec = MPM_PREC_F
 }
 
 int main() {
-    // bytes per particle: FP32 13 vectors of 16 B + sres 4 + 2 x 1 + 3 x 4; FP64 12 x 32 + 8 + 2 + 12
-    assert(ckpt_payload_bytes(MPM_PREC_F32, false, 1, 0) == 13 * 16 + 4 + 2 + 12);
-    assert(ckpt_payload_bytes(MPM_PREC_F64, false, 1, 0) == 12 * 32 + 8 + 2 + 12);
-    assert(ckpt_payload_bytes(MPM_PREC_F64, true, 1, 0) == 14 * 32 + 8 + 2 + 12);
+    // bytes per particle: FP32 13 vectors of 16 B + sres 4 + 2 x 1 + 4 x 4 (id, bin, orig, re-bin key);
+    // FP64 12 x 32 + 8 + 2 + 16
+    assert(ckpt_payload_bytes(MPM_PREC_F32, false, 1, 0) == 13 * 16 + 4 + 2 + 16);
+    assert(ckpt_payload_bytes(MPM_PREC_F64, false, 1, 0) == 12 * 32 + 8 + 2 + 16);
+    assert(ckpt_payload_bytes(MPM_PREC_F64, true, 1, 0) == 14 * 32 + 8 + 2 + 16);
     assert(ckpt_payload_bytes(MPM_PREC_F32, false, 0, 5) == 5 * 24);
     auto good = make(MPM_PREC_F32, 0, 100, 3);
     assert(chk(good) == MPM_OK);

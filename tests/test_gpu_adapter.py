@@ -72,8 +72,8 @@ def _engine_macro_steps(ad, case, m0, m1, keep):
         pose = (C.c_double * 3)(*[tool["position"][a] + tool["velocity"][a] * t0 for a in range(3)])
         ad.L.mad_set_tool_position(ad.a, pose)
         ad.L.mad_begin_interp(ad.a, start.data_ptr(), n)
-        l0 = ad.launches()
         sorts0 = ad.sync_metrics()[1].n_sorts
+        l0 = ad.launches()
         for sub in range(SUB):
             ad.L.mad_interp_substep(ad.a, end.data_ptr(), sub / SUB)
             ad.L.mad_step(ad.a, dt)

@@ -395,15 +395,16 @@ def test_footprint_is_host_arithmetic():
     nodes = p["nx"] * p["ny"] * p["nz"]
     bins = ((p["nx"] + 3) // 4) * ((p["ny"] + 3) // 4) * ((p["nz"] + 3) // 4)
     particles = 16 ** 3 * 8
-    per_particle = 2 * (13 * 16 + 4 + 2 + 12) + 36 + 4   # 12 state vectors + the position low parts, permutation
+    per_particle = 2 * (13 * 16 + 4 + 2 + 16) + 36 + 4   # 12 state vectors + the position low parts, permutation
     # per node: two 16 B grids, an int32 tool mask, three FP32 heat-conduction arrays
     want = particles * per_particle + nodes * (36 + 12) + (bins * 64 + 2) * 8 + bins * 40
     assert abs(b.value - want) <= 1
 
 
 def test_deterministic_footprint_counts_the_mode_scratch():
-    """A deterministic server counts, per particle slot, the mode's 27 node
-    contributions (16 B each in FP32) and its 32 B of sort scratch."""
+    """A deterministic server counts the mode's escaped fixed-point sums (5 x
+    8 B per grid node) and, per bin, its stored node tile (5 x 216 FP32
+    values) and escape mark (4 B)."""
     from mpm_b200 import workpiece as W
     from mpm_b200.solver import make_request
     case = W.config1(cells=(16, 16, 16))
@@ -414,4 +415,7 @@ def test_deterministic_footprint_counts_the_mode_scratch():
         b = C.c_int64()
         assert A.lib().mpm_server_footprint(C.byref(cfg), C.byref(r), C.byref(b)) == A.MPM_OK
         got.append(b.value)
-    assert abs(got[1] - got[0] - 16 ** 3 * 8 * (27 * 16 + 32)) <= 1
+    p = r.params
+    nodes = p.nx * p.ny * p.nz
+    bins = -(-p.nx // 4) * -(-p.ny // 4) * -(-p.nz // 4)
+    assert abs(got[1] - got[0] - (nodes * 40 + bins * (5 * 216 * 4 + 4))) <= 1
