@@ -235,8 +235,9 @@ def run_ours(args):
         p.heat_conduction = 1
     cap = int(np.prod([box["c1"][i] - box["c0"][i] for i in range(3)]) * box["ppc"])
     s = Solver(p, cap, stream=stream.cuda_stream)
-    if args.deterministic:
-        s.set_launch_config(deterministic=True)
+    if args.atomic or args.pass_size:
+        s.set_launch_config(deterministic=not args.atomic, pass_size=args.pass_size)
+    launch_cfg = s.launch_config()
     n = s.init_box(box["c0"], box["c1"], box["ppc"], box["seed"] + rank, box["instance"], box["fixed_layers"],
                    T0, tool=case["tool"])
     m0 = s.metrics()
@@ -310,7 +311,7 @@ def run_ours(args):
                                ("precision" if args.config == "cutting_precision" else args.config), args.cpu_seconds)
         variants = None
         plugin = None
-        if world == 1 and args.config == "large" and not args.no_variants and not args.deterministic:
+        if world == 1 and args.config == "large" and not args.no_variants and not args.atomic:
             variants = like_for_like(case, args, dev, stream, peak)
             plugin = plugin_leg(case, args, dev)
         out = {
@@ -319,8 +320,11 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": desc, "particles_per_gpu": int(n_live), "cells": list(case["cells"]),
                        "dx_m": case["params"]["dx"], "dt_s": dt, "ppc": box["ppc"],
-                       "schedule": ("deterministic: split schedule, re-bin and atomic-free node gather every step"
-                                    if args.deterministic else "fused G2P->P2G, one kernel per step"),
+                       "schedule": ("fused G2P->P2G, one kernel per step; node tiles added to the grid with "
+                                    "FP32 atomics" if args.atomic else
+                                    "fused G2P->P2G, one kernel per step; deterministic: stored node tiles "
+                                    "summed per node in a fixed order (one node-sum launch per step)"),
+                       "pass_size": launch_cfg["pass_size"],
                        "parallelism": f"replicas{world}",
                        "l2": "working set >> L2 (no flush needed)", "yield_fraction": f_yield,
                        "escaped_updates": int(m1["n_escaped"]), "rebins": int(m1["n_sorts"]),
@@ -647,10 +651,11 @@ def run_batched(args):
 def run_precision_study(args):
     """Config 4: the same workpiece stepped in FP32 (the product) and in FP64
     (the oracle run of the same kernels) from the same seeded state; relative
-    errors of the conservation and peak quantities after K steps.  FP32 runs
-    are not bitwise reproducible (the grid sums use atomics), and the fracture
-    zone under the tool edge can branch on a ~1e-7 difference, so the FP32 run
-    is repeated and every run is reported."""
+    errors of the conservation and peak quantities after K steps.  With the
+    default deterministic node sums every FP32 run gives the same bits; with
+    --atomic they vary in the last bits, and the fracture zone under the tool
+    edge can branch on a ~1e-7 difference.  The FP32 run is repeated and every
+    run is reported."""
     import torch
     rank, world, local, dist = dist_setup(args.gpus)
     from mpm_b200 import Solver, capi as A, workpiece as W
@@ -662,8 +667,7 @@ def run_precision_study(args):
 
     def run(prec):
         s = Solver(W.to_mpm_params(case, precision=prec), cap)
-        if args.deterministic:
-            s.set_launch_config(deterministic=True)
+        s.set_launch_config(deterministic=not args.atomic)
         n = _init(s, case, rank=rank)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -732,7 +736,7 @@ def run_precision_study(args):
             "config": {"workload": "precision study: 128x64x64 cells, dx 0.02 mm, 8 ppc, Ti-6Al-4V, rounded wedge "
                                    "r_e 0.3 mm at 2.5 m/s, doc 0.05 mm; the Johnson-Cook Newton solve and the "
                                    "conservation reductions are FP64 in both runs",
-                       "particles": int(n), "fp32_runs": len(runs), "deterministic": bool(args.deterministic),
+                       "particles": int(n), "fp32_runs": len(runs), "deterministic": not args.atomic,
                        "target": "momentum and kinetic+internal energy within 1e-4"},
             "errors_median": med, "errors_worst": worst, "runs_within_1e-4": within,
             "particle_errors_median": part, "particle_error_scales": scales, "runs": runs,
@@ -973,16 +977,20 @@ def main():
                     help="plain configs: run the adiabatic shear band heating after every move")
     ap.add_argument("--heat", action="store_true",
                     help="plain configs: grid heat conduction (scatter, diffusion step, gather) every step")
-    ap.add_argument("--repeats", type=int, default=11,
-                    help="precision_study: FP32 runs (odd; about one in five branches in the fracture zone)")
+    ap.add_argument("--repeats", type=int, default=3,
+                    help="precision_study: FP32 runs (identical unless --atomic, where about one run in five "
+                         "branches in the fracture zone)")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: window in seconds")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serving: HBM budget")
     ap.add_argument("--chunk", type=int, default=50, help="serving: steps per tick at most")
     ap.add_argument("--resident-particles", type=float, default=0,
                     help="serving: admission cap on resident particles (0: the HBM budget alone)")
-    ap.add_argument("--deterministic", action="store_true",
-                    help="plain configs and precision_study: deterministic mode (bit-identical runs)")
+    ap.add_argument("--pass-size", type=int, default=0, choices=[0, 128, 256, 512],
+                    help="plain configs: FP32 particles per pass of the step kernel (0: the default)")
+    ap.add_argument("--atomic", action="store_true",
+                    help="plain configs and precision_study: add node tiles with FP32 atomics instead of the "
+                         "default deterministic node sums")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()

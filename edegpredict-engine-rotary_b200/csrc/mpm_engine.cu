@@ -146,7 +146,7 @@ class Engine final : public EngineBase {
     // deterministic mode (mpm_launch_config.deterministic): every work item's
     // node tile (kPartCh x kTileNodes values), the escaped fixed-point node
     // sums (kPartCh x nn_total) and their per-bin marks
-    bool det = false;
+    bool det = true;
     R* d_part = nullptr;
     int64_t part_alloc = 0;
     unsigned long long* d_esc = nullptr;

@@ -75,23 +75,6 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, u
         "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
         : "memory");
 }
-// Bulk prefetch of [p, p + bytes) into L2 (p and bytes multiples of 16).
-__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
-    if (bytes) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-// ... of a byte range of any alignment, widened to 16-byte bounds (the
-// allocations are padded to 256 bytes).
-__device__ __forceinline__ void prefetch_l2_any(const void* p, int64_t bytes) {
-    const uintptr_t a = reinterpret_cast<uintptr_t>(p) & ~(uintptr_t)15;
-    const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + (uintptr_t)bytes + 15) & ~(uintptr_t)15;
-    prefetch_l2(reinterpret_cast<const void*>(a), (uint32_t)(e - a));
-}
-// Prefetch of the tile at coordinates (c0, c1, c2, c3) of a tensor map into L2.
-__device__ __forceinline__ void tma_prefetch_4d(const CUtensorMap* map, int c0, int c1, int c2, int c3) {
-    asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(map), "r"(c0),
-                 "r"(c1), "r"(c2), "r"(c3)
-                 : "memory");
-}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
@@ -896,21 +879,33 @@ constexpr int kOff = 27;  // stencil offsets, off = i + 3j + 9k
 // mask.  The cell takes its home rows in ascending order, then its foreign
 // slots in ascending order.
 template <typename R, int CH> struct SlotIter {
-    uint32_t bits;    // bits left in the current word
-    uint32_t home;    // the cell's home mask (bit 31: foreign slots present)
-    int q;            // -1: the home rows; >= 0: foreign word q
+    uint32_t hb;      // home rows left
+    uint32_t fb;      // foreign slots left in word fq
+    int fq;           // current foreign word
+    int n;            // staged slots of the cell
     int cell;
-    __device__ __forceinline__ SlotIter(uint32_t h, int c) : bits(h & 0x7fffffffu), home(h), q(-1), cell(c) {}
-    // the next staged slot of the cell, or false when none is left
-    template <typename Mask> __device__ __forceinline__ bool next(const Mask& fmask, int& e) {
-        while (bits == 0u) {
-            if ((home >> 31) == 0u || ++q >= StepCfg<R, CH>::kMaskWords) return false;
-            bits = fmask[q][cell];
+    // home: the cell's home mask; fmask: its foreign words (read only when
+    // bit 31 of home says there are any)
+    template <typename Mask>
+    __device__ __forceinline__ SlotIter(uint32_t home, const Mask& fmask, int c)
+        : hb(home & 0x7fffffffu), fb(0u), fq(-1), n(0), cell(c) {
+        n = __popc(hb);
+        if (home >> 31) {
+#pragma unroll
+            for (int q = 0; q < StepCfg<R, CH>::kMaskWords; ++q) n += __popc(fmask[q][c]);
         }
-        const int b = __ffs((int)bits) - 1;
-        bits &= bits - 1u;
-        e = q < 0 ? (b << 6) | cell : (q << 5) | b;
-        return true;
+    }
+    // the next staged slot (call n times): home rows first, then foreign slots
+    template <typename Mask> __device__ __forceinline__ int next(const Mask& fmask) {
+        if (hb) {
+            const int b = __ffs((int)hb) - 1;
+            hb &= hb - 1u;
+            return (b << 6) | cell;
+        }
+        while (fb == 0u) fb = fmask[++fq][cell];
+        const int b = __ffs((int)fb) - 1;
+        fb &= fb - 1u;
+        return (fq << 5) | b;
     }
 };
 
@@ -938,6 +933,10 @@ template <typename R, bool EXT, int CH> struct StepSmem {
     // warp read consecutive words)
     uint32_t hmask[2][kCellsPerBin];
     uint32_t fmask[2][StepCfg<R, CH>::kMaskWords][kCellsPerBin];
+    // the work item's tool poses at the G2P step (x, y, z) and at the P2G step:
+    // read where used (volatile), so that no thread holds them in registers
+    // across the particle loop
+    double pose[6];
     uint64_t mbar;
     int fail;
 };
@@ -1006,8 +1005,9 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT, CH>& Sm, int ce
         }
     }
     const uint32_t home = Sm.hmask[par][cell];
-    SlotIter<R, CH> it(home, cell);
-    for (int e; it.next(Sm.fmask[par], e);) {
+    SlotIter<R, CH> it(home, Sm.fmask[par], cell);
+    for (int q = 0; q < it.n; ++q) {
+        const int e = it.next(Sm.fmask[par]);
         R w[3][3], dw[3][3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) (void)bspline(Sm.pay[a][e], w[a], dw[a]);
@@ -1031,7 +1031,10 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT, CH>& Sm, int ce
                            Sm.pay[22][e], Sm.pay[23][e], a1);
         }
     }
-    {
+    // a warp whose 32 cells staged nothing in this pass (a sparse surface
+    // bin) has only zeros to add
+    const bool warp_any = __any_sync(0xffffffffu, home != 0u);
+    if (warp_any) {
         const int base = tidx(cell & (kBin - 1), (cell / kBin) & (kBin - 1), cell / (kBin * kBin));
         R* __restrict__ t0 = Sm.nacc[half][2 * h];
         R* __restrict__ t1 = Sm.nacc[half][2 * h + 1];
@@ -1048,13 +1051,14 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT, CH>& Sm, int ce
                 }
         __syncwarp();
     }
-    if (EXT && heat && h == 0) {
+    if (EXT && heat && h == 0 && warp_any) {
         // heat conduction: the T m channel, w m T over the cell's particles (the
         // lighter half of the pair takes it)
 #pragma unroll
         for (int o = 0; o < kOff; ++o) a0[o] = R(0);
-        SlotIter<R, CH> ih(home, cell);
-        for (int e; ih.next(Sm.fmask[par], e);) {
+        SlotIter<R, CH> ih(home, Sm.fmask[par], cell);
+        for (int q = 0; q < ih.n; ++q) {
+            const int e = ih.next(Sm.fmask[par]);
             R w[3][3], dw[3][3];
 #pragma unroll
             for (int a = 0; a < 3; ++a) (void)bspline(Sm.pay[a][e], w[a], dw[a]);
@@ -1095,7 +1099,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
     const int tid = threadIdx.x, lane = tid & 31;
     const int nw = *n_work;
     uint32_t phase = 0;
-    unsigned long long c_esc = 0, c_yield = 0, c_contact = 0;
+    unsigned int c_esc = 0, c_yield = 0, c_contact = 0;   // per thread: far below 2^32
     double f_work = 0.0, f_force = 0.0;
     int errf = 0;   // Newton failures: 0 none, k > 0 instance k - 1 only, -1 several instances
     if (G2P && tid == 0) {
@@ -1122,38 +1126,16 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                             (int64_t)wk.start + wk.count <= P.np,
                         kSiteBin, wi))
             continue;
-        if (tid == 0 && wi + (int)gridDim.x < nw) {
-            // the work item this CTA takes next: its particle state and its
-            // grid tile into L2 while this one is processed
-            const Work wn = work[wi + gridDim.x];
-            const Inst<R>& Pn = insts[wn.inst];
-            if (wn.count > 0 && wn.start >= 0 && (int64_t)wn.start + wn.count <= Pn.np) {
-                const int64_t p0 = Pn.pbase + wn.start;
-                const uint32_t vb = (uint32_t)wn.count * (uint32_t)sizeof(V4<R>);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) prefetch_l2(ps.A[q] + p0, vb);
-                if (P2G) {
-                    prefetch_l2(ps.A[4] + p0, vb);
-                    prefetch_l2(ps.A[5] + p0, vb);
-                }
-                if (G2P && ps.X) prefetch_l2(ps.X + p0, vb);
-                if (!G2P) prefetch_l2(ps.B[0] + p0, vb);
-                prefetch_l2_any(ps.status + p0, wn.count);
-                if (G2P) {
-                    const int nbx = wn.bin % Pn.nbx, nby = (wn.bin / Pn.nbx) % Pn.nby, nbz = wn.bin / (Pn.nbx * Pn.nby);
-                    if (wn.inst != wk.inst) tmap_acquire(&Pn.tmap[rbuf]);
-                    tma_prefetch_4d(&Pn.tmap[rbuf], 0, nbx * kBin, nby * kBin, nbz * kBin);
-                }
-            }
-        }
         const double tg = da(P.t0, dm((double)sa.k, P.dt));         // time of the G2P step
         const double tp = da(P.t0, dm((double)sa.p2g_step, P.dt));  // time of the P2G step
-        const double prg0 = da(P.tool_p0[0], dm(P.tool_v[0], ds(tg, P.tool_t0)));
-        const double prg1 = da(P.tool_p0[1], dm(P.tool_v[1], ds(tg, P.tool_t0)));
-        const double prg2 = da(P.tool_p0[2], dm(P.tool_v[2], ds(tg, P.tool_t0)));
-        const double prp0 = da(P.tool_p0[0], dm(P.tool_v[0], ds(tp, P.tool_t0)));
-        const double prp1 = da(P.tool_p0[1], dm(P.tool_v[1], ds(tp, P.tool_t0)));
-        const double prp2 = da(P.tool_p0[2], dm(P.tool_v[2], ds(tp, P.tool_t0)));
+        if (tid == 0) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                Sm.pose[a] = da(P.tool_p0[a], dm(P.tool_v[a], ds(tg, P.tool_t0)));
+                Sm.pose[3 + a] = da(P.tool_p0[a], dm(P.tool_v[a], ds(tp, P.tool_t0)));
+            }
+        }
+        const volatile double* pose = Sm.pose;
         const V4<R>* __restrict__ gr = P.grid[rbuf];
         V4<R>* __restrict__ gw = P.grid[rbuf ^ (G2P ? 1 : 0)];
 
@@ -1184,7 +1166,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
             }
             for (int nidx = tid; nidx < kTileNodes; nidx += kNT) {
                 const int lx = nidx % kTile, ly = (nidx / kTile) % kTile, lz = nidx / (kTile * kTile);
-                const NV<R> nv = node_vel_inl(P, Sm.raw[nidx], g0x + lx, g0y + ly, g0z + lz, prg0, prg2);
+                const NV<R> nv = node_vel_inl(P, Sm.raw[nidx], g0x + lx, g0y + ly, g0z + lz, pose[0], pose[2]);
                 const int t = tidx(lx, ly, lz);
                 Sm.vel[0][t] = nv.x; Sm.vel[1][t] = nv.y; Sm.vel[2][t] = nv.z;
                 if (EXT && P.heat_on) {
@@ -1207,9 +1189,10 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
             for (int sidx = 0; sidx < StepCfg<R, CH>::kPerThread; ++sidx) {
                 const int slot = tid + sidx * kNT;
                 const int pl = base + slot;
-                // every load of the particle is issued here, before any branch on its
-                // state: one memory round trip.  Slots past the bin's end read the
-                // bin's first particle (bins are never empty) and are discarded.
+                // the loads the G2P needs are issued here, before any branch on the
+                // particle's state: one memory round trip (F_p waits for the
+                // constitutive update).  Slots past the bin's end read the bin's
+                // first particle (bins are never empty) and are discarded.
 #ifdef MPMB_CHECKED
                 bool valid = pl < wk.count;
                 int64_t pi = P.pbase + wk.start + (valid ? pl : 0);
@@ -1224,8 +1207,6 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                 const uint8_t st_ld = ps.status[pi];
                 const V4<R> a0 = ps.A[0][pi], a1 = ps.A[1][pi], a2 = ps.A[2][pi], a3 = ps.A[3][pi];
                 const V4<R> xl = (G2P && ps.X) ? ps.X[pi] : mk4<R>(0, 0, 0, 0);
-                const V4<R> a4 = P2G ? ps.A[4][pi] : mk4<R>(0, 0, 0, 0);
-                const V4<R> a5 = P2G ? ps.A[5][pi] : mk4<R>(0, 0, 0, 0);
                 const V4<R> b0_ld = G2P ? mk4<R>(0, 0, 0, 0) : ps.B[0][pi];
                 uint8_t st = valid ? st_ld : (uint8_t)ST_INACTIVE;
                 if (st != ST_INACTIVE) {
@@ -1246,10 +1227,10 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                         if (!fixed) {
                             bool far = false;
                             if (P.lod && st == ST_ACTIVE) {
-                                const double wx = P.ox + ((double)g0x + ((double)xi[0] + (double)lo[0])) * P.dx - prg0;
-                                const double wy = P.oy + ((double)g0y + ((double)xi[1] + (double)lo[1])) * P.dx - prg1;
+                                const double wx = P.ox + ((double)g0x + ((double)xi[0] + (double)lo[0])) * P.dx - pose[0];
+                                const double wy = P.oy + ((double)g0y + ((double)xi[1] + (double)lo[1])) * P.dx - pose[1];
                                 const double wz =
-                                    P.oz + ((double)g0z + ((double)xi[2] + (double)lo[2])) * P.dx - (prg2 + P.tool_tip_dz);
+                                    P.oz + ((double)g0z + ((double)xi[2] + (double)lo[2])) * P.dx - (pose[2] + P.tool_tip_dz);
                                 far = sqrt(wx * wx + wy * wy + wz * wz) > P.lod_r2;
                             }
                             R w[3][3], dw[3][3];
@@ -1278,7 +1259,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                 }
                             } else {
                                 const GatherOut<R> go = gather_global<R>(P, gr, g0x, g0y, g0z, xi[0], xi[1], xi[2],
-                                                                         prg0, prg2);
+                                                                         pose[0], pose[2]);
 #pragma unroll
                                 for (int c = 0; c < 3; ++c) {
                                     v[c] = go.v[c];
@@ -1360,7 +1341,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                         // chip separation and fracture after the move (step counter parity)
                         if (chip_now) {
                             if (st == ST_ACTIVE) {
-                                const double tipz = ds(da(prg2, P.tool_tip_dz), dm(P.dx, 1.5));
+                                const double tipz = ds(da(pose[2], P.tool_tip_dz), dm(P.dx, 1.5));
                                 const double zw = P.oz + ((double)g0z + ((double)xi[2] + (double)lo[2])) * P.dx;
                                 if (zw < tipz && Dm > R(1e-6)) {
                                     st = ST_CHIP;
@@ -1454,10 +1435,10 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                                    cz < 3 || cz >= P.nz - 4;
                             bool far = false;
                             if (P.lod && st == ST_ACTIVE) {
-                                const double wx = P.ox + ((double)g0x + ((double)xi[0] + (double)lo[0])) * P.dx - prp0;
-                                const double wy = P.oy + ((double)g0y + ((double)xi[1] + (double)lo[1])) * P.dx - prp1;
+                                const double wx = P.ox + ((double)g0x + ((double)xi[0] + (double)lo[0])) * P.dx - pose[3];
+                                const double wy = P.oy + ((double)g0y + ((double)xi[1] + (double)lo[1])) * P.dx - pose[4];
                                 const double wz =
-                                    P.oz + ((double)g0z + ((double)xi[2] + (double)lo[2])) * P.dx - (prp2 + P.tool_tip_dz);
+                                    P.oz + ((double)g0z + ((double)xi[2] + (double)lo[2])) * P.dx - (pose[5] + P.tool_tip_dz);
                                 far = sqrt(wx * wx + wy * wy + wz * wz) > P.lod_r2;
                             }
                             bool skip = far || fixed || st == ST_CHIP;
@@ -1465,6 +1446,9 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                             R sig[6] = {0, 0, 0, 0, 0, 0};
                             R sl[3] = {0, 0, 0};
                             if (!skip && st == ST_ACTIVE) {
+                                // F_p - I: loaded here, where the constitutive update needs
+                                // it, rather than held in registers through the gather
+                                const V4<R> a4 = ps.A[4][pi], a5 = ps.A[5][pi];
                                 R Hp[9] = {a4.x, a4.y, a4.z, a4.w, a5.x, a5.y, a5.z, a5.w, Hp8};
                                 R bsv[6];
                                 R* bsp = nullptr;
@@ -1669,11 +1653,11 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
         f_force += __shfl_down_sync(0xffffffffu, f_force, o);
     }
     if (lane == 0) {
-        if (c_esc) atomicAdd(&ctr[0], c_esc);
-        if (c_yield) atomicAdd(&ctr[1], c_yield);
+        if (c_esc) atomicAdd(&ctr[0], (unsigned long long)c_esc);
+        if (c_yield) atomicAdd(&ctr[1], (unsigned long long)c_yield);
         if (c_contact) {
             // ctr[2] counts contacts; two FP64 sums follow the four counters
-            atomicAdd(&ctr[2], c_contact);
+            atomicAdd(&ctr[2], (unsigned long long)c_contact);
             atomicAdd(reinterpret_cast<double*>(ctr + 4), f_work);
             atomicAdd(reinterpret_cast<double*>(ctr + 4) + 1, f_force);
         }

@@ -184,9 +184,10 @@ class Solver:
         return c.as_dict()
 
     def set_launch_config(self, ctas_per_sm: int = 4, sort_every: int = 16, use_graph: bool = False,
-                          deterministic: bool = False, pass_size: int = 0) -> None:
-        """Launch shape; deterministic=True gives the same results bit for bit
-        on every run and launch shape (mpm_launch_config.deterministic);
+                          deterministic: bool = True, pass_size: int = 0) -> None:
+        """Launch shape; deterministic=True (the default) gives the same
+        results bit for bit on every run and launch shape, False sums node
+        tiles with float atomics (mpm_launch_config.deterministic);
         pass_size: FP32 particles per pass of the step kernel (128, 256, 512;
         0: the default)."""
         c = A.MpmLaunchConfig(int(ctas_per_sm), int(sort_every), 1 if use_graph else 0, 1 if deterministic else 0,

@@ -492,11 +492,13 @@ typedef struct mpm_launch_config {
     int32_t ctas_per_sm;   /* persistent CTAs per SM of the step kernel, 1..8 (default 4) */
     int32_t sort_every;    /* re-bin every n steps, 1..1024 (default mpm_params.sort_every) */
     int32_t use_graph;     /* replay each step call's launches from a captured CUDA graph */
-    /* 1: deterministic mode (no counterpart in the reference, whose P2G sums
-     * with FP64 atomics in arrival order).  The results are the same bit for
-     * bit on every run, every launch shape and every split of the steps into
-     * calls, alone or in a batch.  The fused step kernel runs as in the
-     * default mode, with three changes: each work item stores its node tile
+    /* 1 (the default): deterministic mode (no counterpart in the reference,
+     * whose P2G sums with FP64 atomics in arrival order).  The results are
+     * the same bit for bit on every run, every launch shape and every split
+     * of the steps into calls, alone or in a batch.  0: each work item adds
+     * its node tile to the grid with FP32 atomics (about 1 % faster; the
+     * last bits vary from run to run).  The deterministic mode runs the same
+     * fused step kernel with three changes: each work item stores its node tile
      * and one thread per grid node adds the stored tiles of the bins that
      * cover it in a fixed order (no float atomics; one extra launch per step);
      * a particle whose stencil left its bin's tile adds to the grid in 2^-40

@@ -22,7 +22,7 @@ import numpy as np
 import pytest
 
 sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
-from scenarios import SCENARIOS  # noqa: E402
+from scenarios import PARITY_SCENARIOS, SCENARIOS  # noqa: E402
 from mpm_b200 import Batch, Solver, capi as A, workpiece as W  # noqa: E402
 from test_gpu_batch import assert_same, cap_of, init_i, small_cases  # noqa: E402
 from test_gpu_parity import field_errors  # noqa: E402
@@ -59,7 +59,7 @@ def identical(a, b):
 
 @pytest.mark.parametrize("name", ["plastic_damage_chip", "boundary_mix"])
 def test_runs_are_identical_bit_for_bit(name):
-    """FP32, where the default mode's atomic sums differ from run to run: two
+    """FP32, where the atomic mode's sums differ from run to run: two
     runs, a third with another CTA count and a fourth split into two step
     calls give the same bits."""
     case, st, n, _ = SCENARIOS[name]()
@@ -121,14 +121,14 @@ def test_batched_instance_is_identical_to_its_run_alone():
 def test_extensions_run_deterministically(name):
     """The adiabatic shear model and grid heat conduction (the kernel variant
     with the T m channel in its stored tiles): FP32 runs are identical, and
-    FP64 agrees with the default atomic path within 1e-9."""
+    FP64 agrees with the atomic path within 1e-9."""
     from test_gpu_parity import run_ours
-    case, st, n, _ = SCENARIOS[name]()
+    case, st, n, _ = PARITY_SCENARIOS[name]()
     a = run_det(case, st, n, A.PREC_F32)
     b = run_det(case, st, n, A.PREC_F32, ctas=2)
     identical(a, b)
     det = run_det(case, st, n, A.PREC_F64)
-    atomic = run_ours(case, st, n, prec=A.PREC_F64)
+    atomic = run_ours(case, st, n, prec=A.PREC_F64, atomic=True)
     assert (det["status"] == atomic["status"]).all()
     err = field_errors(det, atomic, case)
     assert max(err.values()) < 1e-9, err
@@ -169,7 +169,7 @@ def test_matches_the_atomic_path_fp64(name):
     schedule): FP64 within 1e-9, status identical."""
     from test_gpu_parity import run_ours
     case, st, n, _ = SCENARIOS[name]()
-    atomic = run_ours(case, st, n, prec=A.PREC_F64)
+    atomic = run_ours(case, st, n, prec=A.PREC_F64, atomic=True)
     det = run_det(case, st, n, A.PREC_F64)
     assert (det["status"] == atomic["status"]).all()
     err = field_errors(det, atomic, case)

@@ -30,10 +30,12 @@ FIELDS = ("x", "y", "z", "vx", "vy", "vz", "F", "Fp", "C", "stress", "backstress
           "strain_rate", "temperature", "damage", "residual_stress")
 
 
-def run_ours(case, st, n, *, prec=A.PREC_F64, sched=A.SCHED_FUSED, splits=None, **over):
+def run_ours(case, st, n, *, prec=A.PREC_F64, sched=A.SCHED_FUSED, splits=None, atomic=False, **over):
     p = W.to_mpm_params(case, precision=prec, schedule=sched, **over)
     s = Solver(p, len(st["x"]) + 64)
     try:
+        if atomic:   # node tiles added with FP32 atomics instead of the deterministic node sums
+            s.set_launch_config(deterministic=False)
         s.set_tool(case["tool"])
         if case["tool"].get("sdf") is not None:
             s.set_tool_sdf(case["tool"]["sdf"])
