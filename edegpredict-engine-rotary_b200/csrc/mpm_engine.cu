@@ -1255,10 +1255,6 @@ class Engine final : public EngineBase {
             }
             I[i].dt = dts[i];
         }
-        if (det && ws_on) {
-            err = "the deterministic mode covers MPMSolver's semantics only";
-            return MPM_NOT_SUPPORTED;
-        }
         mpm_status s = ensure_binned();
         if (s != MPM_OK) return s;
         if (det) MS(det_scratch());

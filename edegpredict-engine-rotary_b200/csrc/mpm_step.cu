@@ -501,88 +501,31 @@ struct JCOut {
 // The return rescales only the diagonal and upper off-diagonal entries of the
 // deviator (:239-248); the lower entries yx, zx, zy keep their trial values and
 // enter the force (:406-408) and the F_p update (:282-294).  sl[3] carries them.
+// The flow-stress part of the return (rate and thermal factors, the radial
+// return, F_p, plastic heating and damage) for a particle whose trial stress
+// can reach the flow stress.  Out of line and with its state passed by value,
+// so that the common elastic path keeps fewer registers.
+template <typename R> struct JCFlow {
+    R Hp[9], sig[6], sl[3], sd[6], bs[6], e[6];
+    R eps, dT, D, q, p3, Ts, edot;
+    int errf;
+    bool yielded, to_chip;
+};
+
 template <typename R>
-__device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[9], R& eps, R& dT, R& D, R edot,
-                                           R sig[6], R sl[3], R& J, R* sres_p, R* bsx, int& errf,
-                                           const Inst<R>* insts) {
+__device__ __noinline__ JCFlow<R> jc_flow(const Inst<R>& P, JCFlow<R> f, R* bsx, R* sres_p, const Inst<R>* insts) {
+    R(&Hp)[9] = f.Hp;
+    R(&sig)[6] = f.sig;
+    R(&sl)[3] = f.sl;
+    R(&sd)[6] = f.sd;
+    R(&bs)[6] = f.bs;
+    R& eps = f.eps;
+    R& dT = f.dT;
+    R& D = f.D;
+    int& errf = f.errf;
+    const R q = f.q, p3 = f.p3, Ts = f.Ts, edot = f.edot;
+    const R ex = f.e[0], ey = f.e[1], ez = f.e[2], exy = f.e[3], exz = f.e[4], eyz = f.e[5];
     JCOut o{true, false, false};
-    // inverse of G = I + Hp (identity when |det G| < 1e-12, inv3x3 :50-57);
-    // a particle that never yielded has Hp = 0 exactly and F_e = F
-    R E[9];
-    bool hp0 = true;
-#pragma unroll
-    for (int q = 0; q < 9; ++q) hp0 = hp0 && (Hp[q] == R(0));
-    if (hp0) {
-#pragma unroll
-        for (int q = 0; q < 9; ++q) E[q] = H[q];
-    } else {
-        const R dgm1 = detm1(Hp);
-        const R det = R(1) + dgm1;
-        R Gi[9];
-        if (fabs(det) < R(1e-12)) {
-#pragma unroll
-            for (int q = 0; q < 9; ++q) Gi[q] = (q % 4 == 0) ? R(1) : R(0);
-        } else {
-            const R g0 = R(1) + Hp[0], g4 = R(1) + Hp[4], g8 = R(1) + Hp[8];
-            const R id = R(1) / det;
-            Gi[0] = (g4 * g8 - Hp[5] * Hp[7]) * id;
-            Gi[1] = -(Hp[1] * g8 - Hp[2] * Hp[7]) * id;
-            Gi[2] = (Hp[1] * Hp[5] - Hp[2] * g4) * id;
-            Gi[3] = -(Hp[3] * g8 - Hp[5] * Hp[6]) * id;
-            Gi[4] = (g0 * g8 - Hp[2] * Hp[6]) * id;
-            Gi[5] = -(g0 * Hp[5] - Hp[2] * Hp[3]) * id;
-            Gi[6] = (Hp[3] * Hp[7] - g4 * Hp[6]) * id;
-            Gi[7] = -(g0 * Hp[7] - Hp[1] * Hp[6]) * id;
-            Gi[8] = (g0 * g4 - Hp[1] * Hp[3]) * id;
-        }
-        // F_e - I = (I + H) G^-1 - I = (H - Hp) G^-1 when G^-1 is exact; with the
-        // identity fallback F_e = F, so F_e - I = H.
-        if (fabs(det) < R(1e-12)) {
-#pragma unroll
-            for (int q = 0; q < 9; ++q) E[q] = H[q];
-        } else {
-            R Dm[9];
-#pragma unroll
-            for (int q = 0; q < 9; ++q) Dm[q] = H[q] - Hp[q];
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-                    E[r * 3 + c] = Dm[r * 3] * Gi[c] + Dm[r * 3 + 1] * Gi[3 + c] + Dm[r * 3 + 2] * Gi[6 + c];
-        }
-    }
-    R jm1 = detm1(E);
-    jm1 = fmin(fmax(jm1, R(-0.1)), R(0.1));  // J clamp [0.9, 1.1], :174-175
-    J = R(1) + jm1;
-    // B - I (symmetric)
-    R b00 = R(2) * E[0] + E[0] * E[0] + E[1] * E[1] + E[2] * E[2];
-    R b11 = R(2) * E[4] + E[3] * E[3] + E[4] * E[4] + E[5] * E[5];
-    R b22 = R(2) * E[8] + E[6] * E[6] + E[7] * E[7] + E[8] * E[8];
-    R b01 = E[1] + E[3] + E[0] * E[3] + E[1] * E[4] + E[2] * E[5];
-    R b02 = E[2] + E[6] + E[0] * E[6] + E[1] * E[7] + E[2] * E[8];
-    R b12 = E[5] + E[7] + E[3] * E[6] + E[4] * E[7] + E[5] * E[8];
-    const R muJ = P.mu / J, lj = P.lam * jm1;
-    R s[6] = {muJ * b00 + lj, muJ * b11 + lj, muJ * b22 + lj, muJ * b01, muJ * b02, muJ * b12};
-    // Johnson-Cook return, :205-360
-    const R tr = s[0] + s[1] + s[2];
-    const R p3 = tr / R(3);
-    R sd[6] = {s[0] - p3, s[1] - p3, s[2] - p3, s[3], s[4], s[5]};
-    R bs[6] = {0, 0, 0, 0, 0, 0};
-    if (bsx) {
-#pragma unroll
-        for (int q = 0; q < 6; ++q) bs[q] = bsx[q];
-    }
-    const R ex = sd[0] - bs[0], ey = sd[1] - bs[1], ez = sd[2] - bs[2], exy = sd[3] - bs[3], exz = sd[4] - bs[4],
-            eyz = sd[5] - bs[5];
-    const R q = sqrt(R(1.5) * (ex * ex + ey * ey + ez * ez + R(2) * (exy * exy + exz * exz + eyz * eyz)));
-    R Ts = dT / P.Tspan;
-    Ts = fmin(fmax(Ts, R(0)), R(1));
-#pragma unroll
-    for (int q2 = 0; q2 < 6; ++q2) sig[q2] = s[q2];
-    sl[0] = s[3]; sl[1] = s[4]; sl[2] = s[5];
-    // an unheated particle with q below the smallest flow stress the step can
-    // have (ylo) cannot yield: the flow stress itself is not needed
-    if (Ts == R(0) && q < P.ylo) return o;
     const R es = fmax(edot / P.edot0, R(1e-5));
     const R rt = R(1) + P.C * log(es);
     // pow(0, y) is +0 for y > 0: skipped for the common unheated, unyielded particle
@@ -668,6 +611,110 @@ __device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[
             }
         }
     }
+    f.yielded = o.yielded;
+    f.to_chip = o.to_chip;
+    return f;
+}
+
+template <typename R>
+__device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[9], R& eps, R& dT, R& D, R edot,
+                                           R sig[6], R sl[3], R& J, R* sres_p, R* bsx, int& errf,
+                                           const Inst<R>* insts) {
+    JCOut o{true, false, false};
+    // inverse of G = I + Hp (identity when |det G| < 1e-12, inv3x3 :50-57);
+    // a particle that never yielded has Hp = 0 exactly and F_e = F
+    R E[9];
+    bool hp0 = true;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) hp0 = hp0 && (Hp[q] == R(0));
+    if (hp0) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) E[q] = H[q];
+    } else {
+        const R dgm1 = detm1(Hp);
+        const R det = R(1) + dgm1;
+        R Gi[9];
+        if (fabs(det) < R(1e-12)) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) Gi[q] = (q % 4 == 0) ? R(1) : R(0);
+        } else {
+            const R g0 = R(1) + Hp[0], g4 = R(1) + Hp[4], g8 = R(1) + Hp[8];
+            const R id = R(1) / det;
+            Gi[0] = (g4 * g8 - Hp[5] * Hp[7]) * id;
+            Gi[1] = -(Hp[1] * g8 - Hp[2] * Hp[7]) * id;
+            Gi[2] = (Hp[1] * Hp[5] - Hp[2] * g4) * id;
+            Gi[3] = -(Hp[3] * g8 - Hp[5] * Hp[6]) * id;
+            Gi[4] = (g0 * g8 - Hp[2] * Hp[6]) * id;
+            Gi[5] = -(g0 * Hp[5] - Hp[2] * Hp[3]) * id;
+            Gi[6] = (Hp[3] * Hp[7] - g4 * Hp[6]) * id;
+            Gi[7] = -(g0 * Hp[7] - Hp[1] * Hp[6]) * id;
+            Gi[8] = (g0 * g4 - Hp[1] * Hp[3]) * id;
+        }
+        // F_e - I = (I + H) G^-1 - I = (H - Hp) G^-1 when G^-1 is exact; with the
+        // identity fallback F_e = F, so F_e - I = H.
+        if (fabs(det) < R(1e-12)) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) E[q] = H[q];
+        } else {
+            R Dm[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) Dm[q] = H[q] - Hp[q];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    E[r * 3 + c] = Dm[r * 3] * Gi[c] + Dm[r * 3 + 1] * Gi[3 + c] + Dm[r * 3 + 2] * Gi[6 + c];
+        }
+    }
+    R jm1 = detm1(E);
+    jm1 = fmin(fmax(jm1, R(-0.1)), R(0.1));  // J clamp [0.9, 1.1], :174-175
+    J = R(1) + jm1;
+    // B - I (symmetric)
+    R b00 = R(2) * E[0] + E[0] * E[0] + E[1] * E[1] + E[2] * E[2];
+    R b11 = R(2) * E[4] + E[3] * E[3] + E[4] * E[4] + E[5] * E[5];
+    R b22 = R(2) * E[8] + E[6] * E[6] + E[7] * E[7] + E[8] * E[8];
+    R b01 = E[1] + E[3] + E[0] * E[3] + E[1] * E[4] + E[2] * E[5];
+    R b02 = E[2] + E[6] + E[0] * E[6] + E[1] * E[7] + E[2] * E[8];
+    R b12 = E[5] + E[7] + E[3] * E[6] + E[4] * E[7] + E[5] * E[8];
+    const R muJ = P.mu / J, lj = P.lam * jm1;
+    R s[6] = {muJ * b00 + lj, muJ * b11 + lj, muJ * b22 + lj, muJ * b01, muJ * b02, muJ * b12};
+    // Johnson-Cook return, :205-360
+    const R tr = s[0] + s[1] + s[2];
+    const R p3 = tr / R(3);
+    R sd[6] = {s[0] - p3, s[1] - p3, s[2] - p3, s[3], s[4], s[5]};
+    R bs[6] = {0, 0, 0, 0, 0, 0};
+    if (bsx) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) bs[q] = bsx[q];
+    }
+    const R ex = sd[0] - bs[0], ey = sd[1] - bs[1], ez = sd[2] - bs[2], exy = sd[3] - bs[3], exz = sd[4] - bs[4],
+            eyz = sd[5] - bs[5];
+    const R q = sqrt(R(1.5) * (ex * ex + ey * ey + ez * ez + R(2) * (exy * exy + exz * exz + eyz * eyz)));
+    R Ts = dT / P.Tspan;
+    Ts = fmin(fmax(Ts, R(0)), R(1));
+#pragma unroll
+    for (int q2 = 0; q2 < 6; ++q2) sig[q2] = s[q2];
+    sl[0] = s[3]; sl[1] = s[4]; sl[2] = s[5];
+    // an unheated particle with q below the smallest flow stress the step can
+    // have (ylo) cannot yield: the flow stress itself is not needed
+    if (Ts == R(0) && q < P.ylo) return o;
+    JCFlow<R> f;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f.Hp[k] = Hp[k];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) { f.sig[k] = sig[k]; f.sd[k] = sd[k]; f.bs[k] = bs[k]; }
+    f.sl[0] = sl[0]; f.sl[1] = sl[1]; f.sl[2] = sl[2];
+    f.e[0] = ex; f.e[1] = ey; f.e[2] = ez; f.e[3] = exy; f.e[4] = exz; f.e[5] = eyz;
+    f.eps = eps; f.dT = dT; f.D = D; f.q = q; f.p3 = p3; f.Ts = Ts; f.edot = edot; f.errf = errf;
+    f = jc_flow<R>(P, f, bsx, sres_p, insts);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Hp[k] = f.Hp[k];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) sig[k] = f.sig[k];
+    sl[0] = f.sl[0]; sl[1] = f.sl[1]; sl[2] = f.sl[2];
+    eps = f.eps; dT = f.dT; D = f.D; errf = f.errf;
+    o.yielded = f.yielded;
+    o.to_chip = f.to_chip;
     return o;
 }
 
@@ -1668,13 +1715,28 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
     else if (errf < 0) atomicOr(err, ERR_NEWTON);
 }
 
-template <typename R, bool G2P, bool P2G, bool EXT, int CH> static void set_smem_attr() {
-    static bool done = false;
-    if (!done) {
+// Sets the variant's shared-memory size once and returns how many of its
+// CTAs fit on one SM.  The work loop hands every CTA of the grid the same
+// share of the work items, so a grid with more CTAs than fit would run its
+// last CTAs as a second wave: launches clamp the grid to this.
+template <typename R, bool G2P, bool P2G, bool EXT, int CH> static int set_smem_attr() {
+    static bool attr = false;
+    static int fit = 0;
+    if (!attr) {
         cudaFuncSetAttribute(k_step<R, G2P, P2G, EXT, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)step_smem_bytes<R, EXT, CH>());
-        done = true;
+        attr = true;
     }
+    if (!fit) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_step<R, G2P, P2G, EXT, CH>, kNT,
+                                                          step_smem_bytes<R, EXT, CH>()) == cudaSuccess &&
+            n >= 1)
+            fit = n;
+        else
+            return 8;   // not known (the query failed): no clamp this time, asked again next launch
+    }
+    return fit;
 }
 
 // Deterministic mode, the grid of one P2G: one thread per node of a bin's
@@ -1762,35 +1824,38 @@ void launch_node_sum(const Inst<R>* insts, const int32_t* bin_inst, const int32_
 // its pass sizes.)
 template <typename R, int CH>
 static void launch_variant(const Inst<R>* insts, const Work* work, const int* n_work, const PState<R>& ps,
-                           const StepArgs& a, int rbuf, bool g2p, bool p2g, int grid, int* err,
+                           const StepArgs& a, int rbuf, bool g2p, bool p2g, int sms, int cps, int max_work, int* err,
                            unsigned long long* counters, cudaStream_t st) {
+    // persistent CTAs: cps per SM, at most as many as fit, at most one per work item
+    auto grid_of = [&](int fit) { return std::max(1, std::min(sms * std::min(cps, fit), max_work)); };
     if constexpr (sizeof(R) == 8 && CH != kDefaultChunk) {
-        launch_variant<R, kDefaultChunk>(insts, work, n_work, ps, a, rbuf, g2p, p2g, grid, err, counters, st);
+        launch_variant<R, kDefaultChunk>(insts, work, n_work, ps, a, rbuf, g2p, p2g, sms, cps, max_work, err, counters,
+                                         st);
     } else if (a.ext) {
         const size_t smem = step_smem_bytes<R, true, kDefaultChunk>();
         if (g2p && p2g) {
-            set_smem_attr<R, true, true, true, kDefaultChunk>();
+            const int grid = grid_of(set_smem_attr<R, true, true, true, kDefaultChunk>());
             k_step<R, true, true, true, kDefaultChunk><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err,
                                                                                counters);
         } else if (g2p) {
-            set_smem_attr<R, true, false, true, kDefaultChunk>();
+            const int grid = grid_of(set_smem_attr<R, true, false, true, kDefaultChunk>());
             k_step<R, true, false, true, kDefaultChunk><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err,
                                                                                 counters);
         } else {
-            set_smem_attr<R, false, true, true, kDefaultChunk>();
+            const int grid = grid_of(set_smem_attr<R, false, true, true, kDefaultChunk>());
             k_step<R, false, true, true, kDefaultChunk><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err,
                                                                                 counters);
         }
     } else {
         const size_t smem = step_smem_bytes<R, false, CH>();
         if (g2p && p2g) {
-            set_smem_attr<R, true, true, false, CH>();
+            const int grid = grid_of(set_smem_attr<R, true, true, false, CH>());
             k_step<R, true, true, false, CH><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
         } else if (g2p) {
-            set_smem_attr<R, true, false, false, CH>();
+            const int grid = grid_of(set_smem_attr<R, true, false, false, CH>());
             k_step<R, true, false, false, CH><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
         } else {
-            set_smem_attr<R, false, true, false, CH>();
+            const int grid = grid_of(set_smem_attr<R, false, true, false, CH>());
             k_step<R, false, true, false, CH><<<grid, kNT, smem, st>>>(insts, work, n_work, ps, a, rbuf, err, counters);
         }
     }
@@ -1810,17 +1875,17 @@ void launch_step(const Inst<R>* insts, const Work* work, const int* n_work, int 
         if (sms <= 0) sms = 148;
     }
     if (max_work <= 0) return;
-    int grid = sms * (ctas_per_sm > 0 ? ctas_per_sm : 4);
-    if (grid > max_work) grid = max_work;
+    const int cps = ctas_per_sm > 0 ? ctas_per_sm : 4;
     // FP64 passes are 128 particles whatever the pass size; the extension
     // variant runs the default pass size
     const int ch = (sizeof(R) == 8 || a.ext) ? kDefaultChunk : a.chunk;
     if (ch == 1)
-        launch_variant<R, 1>(insts, work, n_work, ps, a, rbuf, g2p, p2g, grid, err, counters, st);
+        launch_variant<R, 1>(insts, work, n_work, ps, a, rbuf, g2p, p2g, sms, cps, max_work, err, counters, st);
     else if (ch == 4)
-        launch_variant<R, 4>(insts, work, n_work, ps, a, rbuf, g2p, p2g, grid, err, counters, st);
+        launch_variant<R, 4>(insts, work, n_work, ps, a, rbuf, g2p, p2g, sms, cps, max_work, err, counters, st);
     else
-        launch_variant<R, kDefaultChunk>(insts, work, n_work, ps, a, rbuf, g2p, p2g, grid, err, counters, st);
+        launch_variant<R, kDefaultChunk>(insts, work, n_work, ps, a, rbuf, g2p, p2g, sms, cps, max_work, err,
+                                         counters, st);
     ++launch_counter();
 }
 

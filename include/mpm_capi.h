@@ -363,8 +363,10 @@ typedef struct mpm_workpiece_params {
  * takes its form (the whole force on ACTIVE particles within the radius,
  * :402-413).  The grid stays the handle's (the solver's rebuild of its grid
  * from the particle bounds is host-side domain management).  NULL returns to
- * MPMSolver's semantics.  Not with the deterministic mode or a batch of more
- * than one workpiece. */
+ * MPMSolver's semantics.  Its kernels sum with atomics as the reference's
+ * do (FP64 runs agree to 1e-15, FP32 to summation order) whatever the
+ * launch config's deterministic flag says.  Not for a batch of more than one
+ * workpiece. */
 mpm_status mpm_set_workpiece_semantics(mpm_handle *h, const mpm_workpiece_params *params);
 
 /* Replaces getStableTimeStep (src/MPMSolver.cu:1170-1178): cfl*dx/sqrt(E/rho). */

@@ -86,11 +86,11 @@ def _engine_macro_steps(ad, case, m0, m1, keep, live=False):
         iface, full = (C.c_double * 4)(), A.MpmMetrics()
         ad.L.mad_sync_metrics(ad.a, iface, C.byref(full))
         ad.ok()
-        # 9 step launches and 8 raster launches, not 2 + 1 per sub-step, plus
-        # the launches of a re-bin when one fell due (counts, scans, scatter,
-        # work list: at most 14)
+        # 9 step launches, 8 node sums (deterministic mode) and 8 raster
+        # launches, not 2 + 1 per sub-step, plus the launches of a re-bin when
+        # one fell due (counts, scans, order, scatter, work list: at most 15)
         rebins = full.n_sorts - sorts0
-        assert steps <= SUB + 1 + SUB + 14 * rebins + (2 if live else 0), (steps, rebins)
+        assert steps <= SUB + 1 + SUB + SUB + 15 * rebins + (2 if live else 0), (steps, rebins)
 
 
 def _state_of(rec):
