@@ -139,7 +139,7 @@ class Engine final : public EngineBase {
     int64_t n_sorts = 0;
     int64_t launch_base = 0;
     int sort_every = 16, threads = 128, ctas_per_sm = 4, prec_ = MPM_PREC_F32;
-    static constexpr int kDefaultPassChunk = 2;
+    static constexpr int kDefaultPassChunk = 1;
     int pass_chunk = kDefaultPassChunk;   // FP32 particles per pass of the step kernel / 128
     bool use_graph = false;
     int rbuf = 0;

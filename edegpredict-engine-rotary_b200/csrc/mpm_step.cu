@@ -224,8 +224,15 @@ __device__ __noinline__ NV<R> node_vel(const Inst<R>& P, const V4<R> g, int gx, 
 //   v_a   = sum w v_a,  M_ab = sum w v_a o_b  (o = stencil offset 0,1,2),
 //   L_ab  = sum v_a dw_b  (cell units).
 // k (z) first: Z0 = sum wz v, Z1 = sum k wz v, Z2 = sum dwz v; then j; then i.
+// Node velocity tile of a bin, one 16-byte (FP32) record per node at
+// vidx(x, y, z) = x + 12 y + 72 z: the 8 lanes of a quarter warp (cells x 0-3,
+// y = 2m, 2m + 1 of one z layer) read 8 distinct 4-bank groups, so a warp's
+// 128-bit gathers are conflict-free.
+constexpr int kVY = 12, kVZ = 72, kVPlane = kVZ * kTile;
+__device__ __forceinline__ int vidx(int x, int y, int z) { return x + kVY * y + kVZ * z; }
+
 template <typename R>
-__device__ __forceinline__ void gather_tile(const R (*vel)[kPlane], int base, const R (&w)[3][3], const R (&dw)[3][3],
+__device__ __forceinline__ void gather_tile(const V4<R>* vel, int base, const R (&w)[3][3], const R (&dw)[3][3],
                                             R v[3], R M[3][3], R L[3][3]) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -241,10 +248,11 @@ __device__ __forceinline__ void gather_tile(const R (*vel)[kPlane], int base, co
             R Z0[3] = {0, 0, 0}, Z1[3] = {0, 0, 0}, Z2[3] = {0, 0, 0};
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                const int idx = base + i + kSY * j + kSZ * k;
+                const V4<R> node = vel[base + i + kVY * j + kVZ * k];
+                const R vn[3] = {node.x, node.y, node.z};
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    const R vv = vel[c][idx];
+                    const R vv = vn[c];
                     Z0[c] = fma(w[2][k], vv, Z0[c]);
                     if (k == 1) Z1[c] = fma(w[2][1], vv, Z1[c]);
                     if (k == 2) Z1[c] = fma(R(2) * w[2][2], vv, Z1[c]);
@@ -897,23 +905,29 @@ __device__ __noinline__ ContactOut particle_contact_sdf(const Inst<R>& P, double
 
 // ------------------------------------------------------------------ the step kernel
 
-// Particles staged per pass and scatter payload per particle:
-//   [0..2] xi (bin-local, after the move)  [3..5] Q = m (v - dx C d) + f_ext dt
-//   [6..14] R = m dx C (row-major)         [15..23] S = -dt V J sigma / dx (row-major)
+// Particles staged per pass and scatter payload per particle: xi (bin-local,
+// after the move), Q = m (v - dx C d) + f_ext dt, R = m dx C and
+// S = -dt V J sigma / dx (row-major), in six 4-vectors grouped by the half of
+// the cell's thread pair that reads them (h = 0 takes m and p_x: groups 0-2;
+// h = 1 takes p_y and p_z: groups 0 and 2-5), so each half loads whole
+// 128-bit words:
+//   0 (xi_x, xi_y, xi_z, Q_x)  1 (R_xx, R_xy, R_xz, S_xx)  2 (S_xy, S_xz, Q_y, Q_z)
+//   3 (R_yx, R_yy, R_yz, S_yx) 4 (S_yy, S_yz, R_zx, R_zy)  5 (R_zz, S_zx, S_zy, S_zz)
+// and, in the extension variant, 6 (T, -, -, -).
 // FP32 passes stage CH x 128 particles, CH in {1, 2, 4} (the launch
-// config's pass size, 256 by default: about 4 per cell at 8 per cell, half
-// the barriers and accumulation rounds of 128-particle passes); FP64 passes
-// stage 128.
+// config's pass size, 128 by default: about 2 per cell at 8 per cell; larger
+// passes halve the barriers and node-tile adds per particle but hold more
+// payload and registers, and measured slower on the current kernel); FP64
+// passes stage 128.
 #ifndef MPMB_MIN_CTAS
 #define MPMB_MIN_CTAS 4
 #endif
-constexpr int kDefaultChunk = 2;
+constexpr int kDefaultChunk = 1;
 template <typename R, int CH> struct StepCfg {
     static constexpr int kChunk = sizeof(R) == 4 ? CH * kNT : kNT;
     static constexpr int kPerThread = kChunk / kNT;
     static constexpr int kMaskWords = kChunk / 32;   // words of a cell's slot mask
 };
-constexpr int kPay = 24;
 constexpr int kOff = 27;  // stencil offsets, off = i + 3j + 9k
 
 // Staged particles of a pass are recorded per base cell as bit masks, so
@@ -957,19 +971,21 @@ template <typename R, int CH> struct SlotIter {
 };
 
 // EXT: the kernel variant with the extensions (adiabatic shear heating, heat
-// conduction), which adds the payload's absolute temperature (row kPay), the
+// conduction), which adds the payload's absolute temperature (group 6), the
 // T m node sums (nacc[4]) and the node temperature tile with its m > 1e-18
 // mask (ttile).
 template <typename R, bool EXT, int CH> struct StepSmem {
     // The TMA tile is read only by the fill at the start of a bin and the payload
     // only inside the bin's passes, with barriers between: one buffer holds both,
     // which keeps four CTAs within the 164 KB shared-memory carveout (92 KB of L1
-    // left for the register spills).
+    // left for the register spills).  (Loading the next bin's tile during the
+    // passes, into a buffer of its own, measured 3 % slower: the thread that
+    // issues it stalls on the next work item's descriptor.)
     union {
-        V4<R> raw[kTileNodes];                          // TMA destination (offset 0 of the 128-byte aligned block)
-        R pay[EXT ? kPay + 1 : kPay][StepCfg<R, CH>::kChunk];  // scatter payload of the staged particles
+        V4<R> raw[kTileNodes];                           // TMA destination (offset 0 of the 128-byte aligned block)
+        V4<R> pay[EXT ? 7 : 6][StepCfg<R, CH>::kChunk];  // scatter payload of the staged particles
     };
-    R vel[3][kPlane];                      // node velocities after the grid update
+    V4<R> vel[kVPlane];                    // node velocities after the grid update (vidx layout)
     // the bin's node sums m, p_x, p_y, p_z (, T m) (tidx layout), one copy per
     // half of the bin's cells: each warp adds only to its own copy, so the
     // adds need no atomics (the flush sums the two)
@@ -1056,9 +1072,12 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT, CH>& Sm, int ce
     for (int q = 0; q < it.n; ++q) {
         const int e = it.next(Sm.fmask[par]);
         R w[3][3], dw[3][3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) (void)bspline(Sm.pay[a][e], w[a], dw[a]);
+        const V4<R> g0 = Sm.pay[0][e], g2 = Sm.pay[2][e];
+        (void)bspline(g0.x, w[0], dw[0]);
+        (void)bspline(g0.y, w[1], dw[1]);
+        (void)bspline(g0.z, w[2], dw[2]);
         if (h == 0) {
+            const V4<R> g1 = Sm.pay[1][e];
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 const R mx = pm * w[0][i];
@@ -1069,13 +1088,11 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT, CH>& Sm, int ce
                     for (int k = 0; k < 3; ++k) a0[i + 3 * j + 9 * k] = fma(mxy, w[2][k], a0[i + 3 * j + 9 * k]);
                 }
             }
-            channel_add<R>(w, dw, Sm.pay[3][e], Sm.pay[6][e], Sm.pay[7][e], Sm.pay[8][e], Sm.pay[15][e],
-                           Sm.pay[16][e], Sm.pay[17][e], a1);
+            channel_add<R>(w, dw, g0.w, g1.x, g1.y, g1.z, g1.w, g2.x, g2.y, a1);
         } else {
-            channel_add<R>(w, dw, Sm.pay[4][e], Sm.pay[9][e], Sm.pay[10][e], Sm.pay[11][e], Sm.pay[18][e],
-                           Sm.pay[19][e], Sm.pay[20][e], a0);
-            channel_add<R>(w, dw, Sm.pay[5][e], Sm.pay[12][e], Sm.pay[13][e], Sm.pay[14][e], Sm.pay[21][e],
-                           Sm.pay[22][e], Sm.pay[23][e], a1);
+            const V4<R> g3 = Sm.pay[3][e], g4 = Sm.pay[4][e], g5 = Sm.pay[5][e];
+            channel_add<R>(w, dw, g2.z, g3.x, g3.y, g3.z, g3.w, g4.x, g4.y, a0);
+            channel_add<R>(w, dw, g2.w, g4.z, g4.w, g5.x, g5.y, g5.z, g5.w, a1);
         }
     }
     // a warp whose 32 cells staged nothing in this pass (a sparse surface
@@ -1107,9 +1124,11 @@ __device__ __forceinline__ void cell_accumulate(StepSmem<R, EXT, CH>& Sm, int ce
         for (int q = 0; q < ih.n; ++q) {
             const int e = ih.next(Sm.fmask[par]);
             R w[3][3], dw[3][3];
-#pragma unroll
-            for (int a = 0; a < 3; ++a) (void)bspline(Sm.pay[a][e], w[a], dw[a]);
-            const R mT = pm * Sm.pay[kPay][e];
+            const V4<R> g0 = Sm.pay[0][e];
+            (void)bspline(g0.x, w[0], dw[0]);
+            (void)bspline(g0.y, w[1], dw[1]);
+            (void)bspline(g0.z, w[2], dw[2]);
+            const R mT = pm * Sm.pay[EXT ? 6 : 0][e].x;
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 const R mx = mT * w[0][i];
@@ -1215,7 +1234,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                 const int lx = nidx % kTile, ly = (nidx / kTile) % kTile, lz = nidx / (kTile * kTile);
                 const NV<R> nv = node_vel_inl(P, Sm.raw[nidx], g0x + lx, g0y + ly, g0z + lz, pose[0], pose[2]);
                 const int t = tidx(lx, ly, lz);
-                Sm.vel[0][t] = nv.x; Sm.vel[1][t] = nv.y; Sm.vel[2][t] = nv.z;
+                Sm.vel[vidx(lx, ly, lz)] = mk4<R>(nv.x, nv.y, nv.z, R(0));
                 if (EXT && P.heat_on) {
                     // node temperatures after the diffusion step, for the nodes the
                     // temperature gather counts (m > 1e-18, inside the domain)
@@ -1287,7 +1306,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                             R M[3][3], L[3][3];
                             TSum<R> tsum{R(0), R(0)};
                             if (b[0] >= 0 && b[0] < kBin && b[1] >= 0 && b[1] < kBin && b[2] >= 0 && b[2] < kBin) {
-                                gather_tile<R>(Sm.vel, tidx(b[0], b[1], b[2]), w, dw, v, M, L);
+                                gather_tile<R>(Sm.vel, vidx(b[0], b[1], b[2]), w, dw, v, M, L);
                                 if (EXT && P.heat_on) {
                                     const int tb = tidx(b[0], b[1], b[2]);
 #pragma unroll
@@ -1595,12 +1614,14 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                     atomicOr(&Sm.fmask[par][slot >> 5][scell], 1u << (slot & 31));
                                     atomicOr(&Sm.hmask[par][scell], 0x80000000u);
                                 }
-                                if (EXT) Sm.pay[EXT ? kPay : 0][slot] = P.Tamb + dT;   // absolute T (heat conduction)
-                                Sm.pay[0][slot] = xi[0]; Sm.pay[1][slot] = xi[1]; Sm.pay[2][slot] = xi[2];
-#pragma unroll
-                                for (int a = 0; a < 3; ++a) Sm.pay[3 + a][slot] = Q[a];
-#pragma unroll
-                                for (int q = 0; q < 9; ++q) { Sm.pay[6 + q][slot] = Rm[q]; Sm.pay[15 + q][slot] = S[q]; }
+                                if (EXT)   // absolute T (heat conduction)
+                                    Sm.pay[EXT ? 6 : 0][slot] = mk4<R>(P.Tamb + dT, R(0), R(0), R(0));
+                                Sm.pay[0][slot] = mk4<R>(xi[0], xi[1], xi[2], Q[0]);
+                                Sm.pay[1][slot] = mk4<R>(Rm[0], Rm[1], Rm[2], S[0]);
+                                Sm.pay[2][slot] = mk4<R>(S[1], S[2], Q[1], Q[2]);
+                                Sm.pay[3][slot] = mk4<R>(Rm[3], Rm[4], Rm[5], S[3]);
+                                Sm.pay[4][slot] = mk4<R>(S[4], S[5], Rm[6], Rm[7]);
+                                Sm.pay[5][slot] = mk4<R>(Rm[8], S[6], S[7], S[8]);
                             } else {
                                 ScatterIn<R> si;
 #pragma unroll

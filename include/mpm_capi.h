@@ -511,11 +511,10 @@ typedef struct mpm_launch_config {
      * MPMWorkpieceSolver semantics (MPM_NOT_SUPPORTED at the step). */
     int32_t deterministic;
     /* FP32 particles staged per pass of the step kernel: 128, 256 or 512
-     * (0: the default, 256).  A larger pass halves the passes' barriers and
+     * (0: the default, 128).  A larger pass halves the passes' barriers and
      * node-tile adds and takes more shared memory per CTA (512: three CTAs
      * per SM).  FP64 and the kernel variant with the adiabatic shear model,
-     * heat conduction or the voxel contact stage 256 (FP64: 128) whatever
-     * this says. */
+     * heat conduction or the voxel contact stage 128 whatever this says. */
     int32_t pass_size;
 } mpm_launch_config;
 mpm_status mpm_get_launch_config(const mpm_handle *h, mpm_launch_config *out);
