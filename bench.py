@@ -568,8 +568,11 @@ def run_batched(args):
         n_live += _init(bt, c, i, rank)
     dts = [c["dt"] for c in cases]
     # autotune (real steps, untimed) then warm-up
+    if args.atomic:
+        bt.set_launch_config(deterministic=False)
     tune = bt.autotune(dts) if not args.no_tune else bt.launch_config()
-    bt.set_launch_config(tune["ctas_per_sm"], tune["sort_every"], use_graph=True, pass_size=tune["pass_size"])
+    bt.set_launch_config(tune["ctas_per_sm"], tune["sort_every"], use_graph=True, pass_size=tune["pass_size"],
+                         deterministic=not args.atomic)
     tune = bt.launch_config()
     bt.step_all(dts, args.warmup)
     torch.cuda.synchronize(dev)
@@ -592,7 +595,8 @@ def run_batched(args):
     ms = e0.elapsed_time(e1)
     launches = bt.launches() - launches0
     # kernel time of the fused launches (separate pass of the same length, not graph-replayed)
-    bt.set_launch_config(tune["ctas_per_sm"], tune["sort_every"], use_graph=False, pass_size=tune["pass_size"])
+    bt.set_launch_config(tune["ctas_per_sm"], tune["sort_every"], use_graph=False, pass_size=tune["pass_size"],
+                         deterministic=not args.atomic)
     bt.profile(True)
     bt.profile_read()
     bt.step_all(dts, min(args.steps, 50))

@@ -270,14 +270,20 @@ __device__ __forceinline__ int64_t bin_dest(const Inst<R>& P, int ii, int64_t pi
 // through L2) -- a scatter by source slot wrote every 16-, 4- and 1-byte field
 // to a permuted slot and moved about twice the bytes through DRAM.
 template <typename R>
+// perm[d] = the source slot of destination slot d, perm[np + d] = that
+// source's upload position (the order k_bin_order sorts by, read here where
+// it is coalesced).
 __global__ void k_bin_perm(const Inst<R>* insts, int n_inst, const int32_t* key, const int32_t* rank,
-                           const int32_t* offset, const int32_t* key_base, const int32_t* newbin, int32_t* perm,
-                           int64_t np) {
+                           const int32_t* offset, const int32_t* key_base, const int32_t* newbin,
+                           const int32_t* orig, int32_t* perm, int64_t np) {
     const int64_t pi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pi >= np) return;
     const int ii = find_inst(insts, n_inst, pi);
     const int64_t d = bin_dest(insts[ii], ii, pi, key, rank, offset, key_base, newbin);
-    if (d >= 0) perm[d] = (int32_t)pi;
+    if (d >= 0) {
+        perm[d] = (int32_t)pi;
+        perm[np + d] = orig[pi];
+    }
 }
 
 // The ranks of k_bin_count follow the atomics' arrival order.  One CTA per
@@ -297,8 +303,9 @@ __device__ __forceinline__ int64_t order_dest(const int32_t* cs, int c, int r, i
 }
 
 __global__ void __launch_bounds__(kCellsPerBin) k_bin_order(const int32_t* __restrict__ bin_key,
-                                                            const int32_t* __restrict__ offset,
-                                                            const int32_t* __restrict__ orig, int32_t* perm) {
+                                                            const int32_t* __restrict__ offset, int32_t* perm,
+                                                            int64_t np) {
+    const int32_t* __restrict__ okey = perm + np;   // upload position of each destination's source
     __shared__ int32_t cs[kCellsPerBin + 1];
     const int32_t fk = bin_key[blockIdx.x];
     const int c = threadIdx.x;
@@ -314,7 +321,7 @@ __global__ void __launch_bounds__(kCellsPerBin) k_bin_order(const int32_t* __res
         for (int r = 0; r < m; ++r) {
             dst[r] = order_dest(cs, c, r, b0);
             src[r] = perm[dst[r]];
-            key[r] = orig[src[r]];
+            key[r] = okey[dst[r]];
         }
         // insertion sort by orig (distinct within an instance)
         for (int r = 1; r < m; ++r) {
@@ -334,15 +341,17 @@ __global__ void __launch_bounds__(kCellsPerBin) k_bin_order(const int32_t* __res
         for (int r = 0; r < m - 1; ++r) {
             const int64_t dr = order_dest(cs, c, r, b0);
             int64_t best = dr;
-            int32_t bv = perm[dr], bk = orig[bv];
+            int32_t bv = perm[dr], bk = okey[dr];
             for (int q = r + 1; q < m; ++q) {
                 const int64_t dq = order_dest(cs, c, q, b0);
-                const int32_t v = perm[dq], k = orig[v];
+                const int32_t v = perm[dq], k = okey[dq];
                 if (k < bk) { bv = v; bk = k; best = dq; }
             }
             if (best != dr) {
                 perm[best] = perm[dr];
+                perm[np + best] = okey[dr];
                 perm[dr] = bv;
+                perm[np + dr] = bk;
             }
         }
     }
@@ -914,8 +923,8 @@ void launch_bin_scatter(const PState<R>& src, const PState<R>& dst, const Inst<R
     if (np <= 0) return;
     const int blocks = (int)((np + kT - 1) / kT);
     cudaMemsetAsync(perm, 0xff, sizeof(int32_t) * np, st);
-    k_bin_perm<R><<<blocks, kT, 0, st>>>(insts, n_inst, key, rank, offset, key_base, newbin, perm, np);
-    if (nbins_total > 0) k_bin_order<<<nbins_total, kCellsPerBin, 0, st>>>(bin_key, offset, src.orig, perm);
+    k_bin_perm<R><<<blocks, kT, 0, st>>>(insts, n_inst, key, rank, offset, key_base, newbin, src.orig, perm, np);
+    if (nbins_total > 0) k_bin_order<<<nbins_total, kCellsPerBin, 0, st>>>(bin_key, offset, perm, np);
     k_bin_gather<R><<<blocks, kT, 0, st>>>(src, dst, insts, n_inst, key, key_base, newbin, perm, initial,
                                            pos_scratch, has_K, np);
     launch_counter() += nbins_total > 0 ? 3 : 2;

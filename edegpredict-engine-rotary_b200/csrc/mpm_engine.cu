@@ -112,7 +112,7 @@ class Engine final : public EngineBase {
     int32_t *d_key_base = nullptr, *d_bin_key = nullptr, *d_bin_inst = nullptr, *d_bin_local = nullptr;
     int64_t* d_inst_pbase = nullptr;
     int32_t *d_key = nullptr, *d_rank = nullptr, *d_newbin = nullptr, *d_count = nullptr, *d_offset = nullptr;
-    int32_t* d_perm = nullptr;     // re-bin: source slot of every destination slot
+    int32_t* d_perm = nullptr;     // re-bin: source slot of every destination slot, then its upload position
     int64_t perm_alloc = 0;
     int32_t *d_flag = nullptr, *d_flag_scan = nullptr, *d_scan_tmp = nullptr;
     double* d_pos = nullptr;
@@ -463,7 +463,7 @@ class Engine final : public EngineBase {
         MS(grow(d_key, slot_alloc[0], cp));
         MS(grow(d_rank, slot_alloc[1], cp));
         MS(grow(d_newbin, slot_alloc[2], cp));
-        MS(grow(d_perm, perm_alloc, cp));
+        MS(grow(d_perm, perm_alloc, 2 * cp));
         MS(grow(d_pos, slot_alloc[3], 3 * cp));
         MS(grow(d_count, key_alloc[0], nkeys + 1));
         MS(grow(d_offset, key_alloc[1], nkeys + 1));
@@ -550,7 +550,7 @@ class Engine final : public EngineBase {
         MS(grow(d_key, slot_alloc[0], particles, false));
         MS(grow(d_rank, slot_alloc[1], particles, false));
         MS(grow(d_newbin, slot_alloc[2], particles, false));
-        MS(grow(d_perm, perm_alloc, particles, false));
+        MS(grow(d_perm, perm_alloc, 2 * particles, false));
         MS(grow(d_pos, slot_alloc[3], 3 * particles, false));
         MS(grow(d_count, key_alloc[0], keys + 1, false));
         MS(grow(d_offset, key_alloc[1], keys + 1, false));

@@ -93,6 +93,7 @@ void launch_bin_scatter(const PState<R>& src, const PState<R>& dst, const Inst<R
                         const int32_t* key, const int32_t* rank, const int32_t* offset, const int32_t* key_base,
                         const int32_t* newbin, bool initial, const double* pos_scratch, bool has_K, int64_t np,
                         int32_t* perm, const int32_t* bin_key, int nbins_total, cudaStream_t st);
+// (perm holds 2 np int32: the permutation, then its sources' upload positions)
 
 template <typename R>
 void launch_pad_counts(const Inst<R>* insts, int n_inst, const int32_t* key_base, int32_t* count, cudaStream_t st);

@@ -395,7 +395,7 @@ def test_footprint_is_host_arithmetic():
     nodes = p["nx"] * p["ny"] * p["nz"]
     bins = ((p["nx"] + 3) // 4) * ((p["ny"] + 3) // 4) * ((p["nz"] + 3) // 4)
     particles = 16 ** 3 * 8
-    per_particle = 2 * (13 * 16 + 4 + 2 + 16) + 36 + 4   # 12 state vectors + the position low parts, permutation
+    per_particle = 2 * (13 * 16 + 4 + 2 + 16) + 36 + 8   # 12 state vectors + the position low parts, permutation
     # per node: two 16 B grids, an int32 tool mask, three FP32 heat-conduction arrays
     want = particles * per_particle + nodes * (36 + 12) + (bins * 64 + 2) * 8 + bins * 40
     assert abs(b.value - want) <= 1
