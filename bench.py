@@ -235,8 +235,9 @@ def run_ours(args):
         p.heat_conduction = 1
     cap = int(np.prod([box["c1"][i] - box["c0"][i] for i in range(3)]) * box["ppc"])
     s = Solver(p, cap, stream=stream.cuda_stream)
-    if args.atomic or args.pass_size:
-        s.set_launch_config(deterministic=not args.atomic, pass_size=args.pass_size)
+    if args.atomic or args.pass_size or args.ctas_per_sm:
+        s.set_launch_config(ctas_per_sm=args.ctas_per_sm or 4, deterministic=not args.atomic,
+                            pass_size=args.pass_size)
     launch_cfg = s.launch_config()
     n = s.init_box(box["c0"], box["c1"], box["ppc"], box["seed"] + rank, box["instance"], box["fixed_layers"],
                    T0, tool=case["tool"])
@@ -990,6 +991,8 @@ def main():
     ap.add_argument("--chunk", type=int, default=50, help="serving: steps per tick at most")
     ap.add_argument("--resident-particles", type=float, default=0,
                     help="serving: admission cap on resident particles (0: the HBM budget alone)")
+    ap.add_argument("--ctas-per-sm", type=int, default=0,
+                    help="plain configs: persistent CTAs per SM of the step kernel (0: the default, 4)")
     ap.add_argument("--pass-size", type=int, default=0, choices=[0, 128, 256, 512],
                     help="plain configs: FP32 particles per pass of the step kernel (0: the default)")
     ap.add_argument("--atomic", action="store_true",

@@ -793,8 +793,10 @@ class Engine final : public EngineBase {
         Range nvtx_range("mpm.rebin");
         CK(cudaMemsetAsync(d_count, 0, 4 * (nkeys + 1), st));
         launch_pad_counts<R>(d_inst, (int)I.size(), d_key_base, d_count, st);
+        // (the atomic mode keeps no layout: every instance is binned from its
+        // positions, and all share one re-bin phase from here)
         launch_bin_count<R>(d_inst, (int)I.size(), ps[cur], d_key_base, true, d_pos, d_key, d_rank, d_count, d_newbin,
-                            cap_total, 0, sort_every, true, st);
+                            cap_total, det ? 0 : -1, sort_every, det, st);
         exclusive_scan(d_count, d_offset, nkeys, d_scan_tmp, st);
         launch_bin_scatter<R>(ps[cur], ps[cur ^ 1], d_inst, (int)I.size(), d_key, d_rank, d_offset, d_key_base,
                               d_newbin, true, d_pos, has_K, cap_total, d_perm, d_bin_key, max_work, st);
@@ -808,7 +810,7 @@ class Engine final : public EngineBase {
         for (auto& x : I) {
             any_fresh |= (x.fresh != 0);
             any_now |= x.rebin_now;
-            if (x.fresh || x.rebin_now) x.since = 0;
+            if (x.fresh || x.rebin_now || !det) x.since = 0;
             x.fresh = 0;
             x.rebin_now = false;
         }
@@ -1299,6 +1301,10 @@ class Engine final : public EngineBase {
         // re-binned (the others keep their layout); last[i] = the call's last
         // such point of instance i
         std::vector<int> last(I.size(), -1);
+        // The atomic mode re-bins every instance whenever one is due, so the
+        // instances keep one shared phase: a batch of workpieces admitted at
+        // different steps would otherwise re-bin (and move every particle)
+        // at nearly every step.
         auto maybe_sort = [&](int k) -> mpm_status {
             bool any = false;
             for (size_t i = 0; i < I.size(); ++i) {
@@ -1308,7 +1314,9 @@ class Engine final : public EngineBase {
                     last[i] = k;
                 }
             }
-            return any ? rebin_regular(k) : MPM_OK;
+            if (any && !det)
+                for (size_t i = 0; i < I.size(); ++i) last[i] = k;
+            return any ? rebin_regular(det ? k : -1) : MPM_OK;
         };
         const int cps = ctas_per_sm;
         int xk = 0, heat = 0;
