@@ -812,12 +812,13 @@ __global__ void k_stats(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64_
     const double m = (double)P.pmass, V = (double)P.pvol;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
         const int64_t pi = pbase + s;
+        // every load before the branch on the status: one memory round trip
         const int st = ps.status[pi];
+        const V4<R> a0 = ps.A[0][pi], a3 = ps.A[3][pi], b0 = ps.B[0][pi], s0 = ps.S[0][pi], s1 = ps.S[1][pi];
         if (st == ST_INACTIVE) { acc[18] += 1.0; continue; }
         if (st == ST_ACTIVE) acc[15] += 1.0;
         else if (st == ST_CHIP) acc[16] += 1.0;
         else if (st == ST_FIXED) acc[17] += 1.0;
-        const V4<R> a0 = ps.A[0][pi], a3 = ps.A[3][pi], b0 = ps.B[0][pi], s0 = ps.S[0][pi], s1 = ps.S[1][pi];
         const double sxx = s0.x, syy = s0.y, szz = s0.z, sxy = s0.w, sxz = s1.x, syz = s1.y;
         const double tr = sxx + syy + szz;
         const double dx_ = sxx - tr / 3.0, dy_ = syy - tr / 3.0, dz_ = szz - tr / 3.0;

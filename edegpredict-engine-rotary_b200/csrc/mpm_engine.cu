@@ -240,7 +240,7 @@ class Engine final : public EngineBase {
         // then two FP64 sums (contact friction work, contact normal force)
         CK(cudaMalloc(&d_ctr, kCtrBytes));
         CK(cudaMemsetAsync(d_ctr, 0, kCtrBytes, st));
-        stat_blocks = 592;
+        stat_blocks = 148 * 8;   // 8 CTAs per SM of the metrics reduction (more loads in flight)
         CK(cudaMalloc(&d_stat_part, sizeof(double) * kStatSlots * stat_blocks));
         CK(cudaMalloc(&d_stat_out, sizeof(double) * kStatSlots));
         return relayout(std::move(nI), std::vector<int>(n, -1));
@@ -1717,8 +1717,10 @@ class Engine final : public EngineBase {
         if (s != MPM_OK) return s;
         const double mu = x.p.E / (2.0 * (1.0 + x.p.nu));
         const double K = x.p.E / (3.0 * (1.0 - 2.0 * x.p.nu));
-        launch_stats<R>(d_inst + i, ps[cur], x.pbase, x.np, mu, K, x.p.rho_phys, x.p.cp, x.p.Tamb, d_stat_part,
-                        stat_blocks, d_stat_out, st);
+        // at least 4 particles per thread (256-thread CTAs), at most stat_blocks CTAs
+        const int nb = (int)std::max<int64_t>(1, std::min<int64_t>(stat_blocks, (x.np + 4 * 256 - 1) / (4 * 256)));
+        launch_stats<R>(d_inst + i, ps[cur], x.pbase, x.np, mu, K, x.p.rho_phys, x.p.cp, x.p.Tamb, d_stat_part, nb,
+                        d_stat_out, st);
         double v[kStatSlots];
         unsigned long long ctr[4];
         double fsum[2];
