@@ -302,77 +302,19 @@ __device__ __forceinline__ int64_t order_dest(const int32_t* cs, int c, int r, i
     return b0 + column_slot(cs, c, r);
 }
 
-// Bins of up to kOrderSmem particles are staged through shared memory: the
-// bin's permutation and keys are read and the permutation written back with
-// coalesced accesses, and each cell's thread sorts its entries in between.
-constexpr int kOrderSmem = 2048;
-
 __global__ void __launch_bounds__(kCellsPerBin) k_bin_order(const int32_t* __restrict__ bin_key,
                                                             const int32_t* __restrict__ offset, int32_t* perm,
                                                             int64_t np) {
     const int32_t* __restrict__ okey = perm + np;   // upload position of each destination's source
     __shared__ int32_t cs[kCellsPerBin + 1];
-    __shared__ int32_t sp[kOrderSmem], sk[kOrderSmem];
     const int32_t fk = bin_key[blockIdx.x];
     const int c = threadIdx.x;
     cs[c] = offset[fk + c];
     if (c == 0) cs[kCellsPerBin] = offset[fk + kCellsPerBin];
     __syncthreads();
-    const int n = cs[kCellsPerBin] - cs[0];
-    if (n <= 1) return;
     const int m = cs[c + 1] - cs[c];
-    const int64_t b0 = cs[0];
-    if (n <= kOrderSmem) {
-        for (int j = c; j < n; j += kCellsPerBin) {
-            sp[j] = perm[b0 + j];
-            sk[j] = okey[b0 + j];
-        }
-        __syncthreads();
-        if (m > 1 && m <= kOrderLocal) {
-            int32_t src[kOrderLocal], key[kOrderLocal];
-            int pos[kOrderLocal];
-            for (int r = 0; r < m; ++r) {
-                pos[r] = (int)column_slot(cs, c, r);
-                src[r] = sp[pos[r]];
-                key[r] = sk[pos[r]];
-            }
-            // insertion sort by orig (distinct within an instance)
-            for (int r = 1; r < m; ++r) {
-                const int32_t v = src[r], k = key[r];
-                int q = r - 1;
-                while (q >= 0 && key[q] > k) {
-                    src[q + 1] = src[q];
-                    key[q + 1] = key[q];
-                    --q;
-                }
-                src[q + 1] = v;
-                key[q + 1] = k;
-            }
-            for (int r = 0; r < m; ++r) sp[pos[r]] = src[r];
-        } else if (m > kOrderLocal) {
-            // selection sort in shared memory: rank r takes the smallest orig among ranks r..m-1
-            for (int r = 0; r < m - 1; ++r) {
-                const int pr = (int)column_slot(cs, c, r);
-                int best = pr;
-                int32_t bv = sp[pr], bk = sk[pr];
-                for (int q = r + 1; q < m; ++q) {
-                    const int pq = (int)column_slot(cs, c, q);
-                    if (sk[pq] < bk) { bv = sp[pq]; bk = sk[pq]; best = pq; }
-                }
-                if (best != pr) {
-                    sp[best] = sp[pr];
-                    sk[best] = sk[pr];
-                    sp[pr] = bv;
-                    sk[pr] = bk;
-                }
-            }
-        }
-        __syncthreads();
-        for (int j = c; j < n; j += kCellsPerBin) perm[b0 + j] = sp[j];
-        return;
-    }
-    // a bin larger than the staging buffer: sorted in place in global memory
     if (m <= 1) return;
+    const int64_t b0 = cs[0];
     if (m <= kOrderLocal) {
         int32_t src[kOrderLocal], key[kOrderLocal];
         int64_t dst[kOrderLocal];
@@ -381,6 +323,7 @@ __global__ void __launch_bounds__(kCellsPerBin) k_bin_order(const int32_t* __res
             src[r] = perm[dst[r]];
             key[r] = okey[dst[r]];
         }
+        // insertion sort by orig (distinct within an instance)
         for (int r = 1; r < m; ++r) {
             const int32_t v = src[r], k = key[r];
             int q = r - 1;
@@ -394,6 +337,7 @@ __global__ void __launch_bounds__(kCellsPerBin) k_bin_order(const int32_t* __res
         }
         for (int r = 0; r < m; ++r) perm[dst[r]] = src[r];
     } else {
+        // selection sort in place: rank r takes the smallest orig among ranks r..m-1
         for (int r = 0; r < m - 1; ++r) {
             const int64_t dr = order_dest(cs, c, r, b0);
             int64_t best = dr;
