@@ -521,7 +521,7 @@ template <typename R> struct JCFlow {
 };
 
 template <typename R>
-__device__ __noinline__ JCFlow<R> jc_flow(const Inst<R>& P, JCFlow<R> f, R* bsx, R* sres_p, const Inst<R>* insts) {
+__device__ __noinline__ JCFlow<R> jc_flow(const Inst<R>& P, JCFlow<R> f, R* bsx, R* sres_p, int inst_tag) {
     R(&Hp)[9] = f.Hp;
     R(&sig)[6] = f.sig;
     R(&sl)[3] = f.sl;
@@ -547,7 +547,7 @@ __device__ __noinline__ JCFlow<R> jc_flow(const Inst<R>& P, JCFlow<R> f, R* bsx,
                                (double)tt, P.newton_tol, P.newton_maxit, &dg)) {
                 // the failing instance (tag = index + 1, from the record's address) in
                 // a register; a second instance failing on this thread makes it -1
-                const int tag = (int)(&P - insts) + 1;
+                const int tag = inst_tag;
                 errf = (errf == 0 || errf == tag) ? tag : -1;
             }
             dE = (R)dg;
@@ -627,7 +627,7 @@ __device__ __noinline__ JCFlow<R> jc_flow(const Inst<R>& P, JCFlow<R> f, R* bsx,
 template <typename R>
 __device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[9], R& eps, R& dT, R& D, R edot,
                                            R sig[6], R sl[3], R& J, R* sres_p, R* bsx, int& errf,
-                                           const Inst<R>* insts) {
+                                           int inst_tag) {
     JCOut o{true, false, false};
     // inverse of G = I + Hp (identity when |det G| < 1e-12, inv3x3 :50-57);
     // a particle that never yielded has Hp = 0 exactly and F_e = F
@@ -714,7 +714,7 @@ __device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[
     f.sl[0] = sl[0]; f.sl[1] = sl[1]; f.sl[2] = sl[2];
     f.e[0] = ex; f.e[1] = ey; f.e[2] = ez; f.e[3] = exy; f.e[4] = exz; f.e[5] = eyz;
     f.eps = eps; f.dT = dT; f.D = D; f.q = q; f.p3 = p3; f.Ts = Ts; f.edot = edot; f.errf = errf;
-    f = jc_flow<R>(P, f, bsx, sres_p, insts);
+    f = jc_flow<R>(P, f, bsx, sres_p, inst_tag);
 #pragma unroll
     for (int k = 0; k < 9; ++k) Hp[k] = f.Hp[k];
 #pragma unroll
@@ -1000,6 +1000,9 @@ template <typename R, bool EXT, int CH> struct StepSmem {
     // read where used (volatile), so that no thread holds them in registers
     // across the particle loop
     double pose[6];
+    // the work item's instance record (the particle loop reads its constants
+    // from here rather than holding them in registers)
+    Inst<R> inst;
     uint64_t mbar;
     int fail;
 };
@@ -1181,10 +1184,20 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
     __syncthreads();
     int par = 0;  // parity of the staging pass (counts double-buffered across passes)
     int last_inst = -1;
+    int cur_inst = -1;
 
     for (int wi = blockIdx.x; wi < nw; wi += gridDim.x) {
         const Work wk = work[wi];
-        const Inst<R>& P = insts[wk.inst];
+        if (wk.inst != cur_inst) {
+            // all threads are past the previous item (the barrier that ends it)
+            const uint4* __restrict__ src = reinterpret_cast<const uint4*>(&insts[wk.inst]);
+            uint4* dst = reinterpret_cast<uint4*>(&Sm.inst);
+            for (int q = tid; q < (int)(sizeof(Inst<R>) / 16); q += kNT) dst[q] = src[q];
+            cur_inst = wk.inst;
+            __syncthreads();
+        }
+        const Inst<R>& P = Sm.inst;
+        const Inst<R>& Pg = insts[wk.inst];   // the tensor maps are read from global memory
         const int bx = wk.bin % P.nbx, by = (wk.bin / P.nbx) % P.nby, bz = wk.bin / (P.nbx * P.nby);
         const int g0x = bx * kBin, g0y = by * kBin, g0z = bz * kBin;
         // (uniform across the CTA: a skipped work item skips for every thread)
@@ -1207,10 +1220,10 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
 
         if (G2P) {
             if (tid == 0) {
-                if (wk.inst != last_inst) tmap_acquire(&P.tmap[rbuf]);
+                if (wk.inst != last_inst) tmap_acquire(&Pg.tmap[rbuf]);
                 fence_async_smem();
                 mbar_expect_tx(&Sm.mbar, (uint32_t)(kTileNodes * sizeof(V4<R>)));
-                tma_load_4d(Sm.raw, &P.tmap[rbuf], &Sm.mbar, 0, g0x, g0y, g0z);
+                tma_load_4d(Sm.raw, &Pg.tmap[rbuf], &Sm.mbar, 0, g0x, g0y, g0z);
                 if (!mbar_wait_bounded(&Sm.mbar, phase, 2000000000ull)) {
                     // give the copy in flight a second bounded chance, then stop
                     mbar_wait_bounded(&Sm.mbar, phase, 2000000000ull);
@@ -1525,7 +1538,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                     bsp = bsv;
                                 }
                                 JCOut jo = jc_update<R>(P, H, Hp, eps, dT, Dm, edot, sig, sl, Jv, &ps.sres[pi], bsp,
-                                                        errf, insts);
+                                                        errf, wk.inst + 1);
                                 if (jo.yielded) {
                                     yielded = true;
                                     dirtyA = true;
