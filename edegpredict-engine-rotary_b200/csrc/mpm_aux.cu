@@ -547,8 +547,33 @@ __global__ void k_import(DevSoA in, int64_t n, double ox, double oy, double oz, 
 // ------------------------------------------------------------------ generator
 
 // Seeded box workpiece: candidate (cell, k) gets Philox4x32-10 uniforms keyed
-// by (seed_lo, seed_hi) with counter (cell index in the box, k, instance, 0).
+// by (seed_lo, seed_hi) with counter (cell index in the box, k, instance, 0),
+// and sits at a jittered point of its own stratum of the cell (the reference
+// fills the box on a regular lattice, src/MPMSolver.cu:1311-1315; the jitter
+// is the seeded part).  For ppc <= 8 the strata are the cell's octants, in
+// the fixed order kOctant, whose prefixes of even length take each half of
+// every axis equally often; with the same octants in every cell, each
+// interior cell's stencil base (the node below x - 1/2, which collects the
+// upper octants of its cell and the lower ones of the next) holds exactly ppc
+// particles.  For ppc > 8 the strata are sub-cells of an n^3 grid, n the
+// smallest even number with n^3 >= ppc (even, so that the same holds),
+// candidate k taking sub-cell s = 37 k mod n^3 (spread over the cell).
+// Offsets in cells: octant o, axis a: 0.5 bit_a(o) + 0.5 u_a (exact);
+// sub-cell s: (s_a + u_a) / n.
 // keep = not inside the tool at t=0 (phi > 0 when a tool is given).
+__constant__ int kOctant[8] = {0, 7, 3, 4, 5, 2, 6, 1};
+__device__ __forceinline__ void gen_offset(int k, int ppc, const float u[4], double off[3]) {
+    if (ppc <= 8) {
+        const int o = kOctant[k & 7];
+        for (int a = 0; a < 3; ++a) off[a] = 0.5 * (double)((o >> a) & 1) + 0.5 * (double)u[a];
+    } else {
+        int n = 4;
+        while (n * n * n < ppc) n += 2;
+        const int q = (int)((37ll * k) % (n * n * n));
+        const int sa[3] = {q % n, (q / n) % n, q / (n * n)};
+        for (int a = 0; a < 3; ++a) off[a] = ((double)sa[a] + (double)u[a]) / (double)n;
+    }
+}
 template <typename R>
 __global__ void k_gen_flags(Inst<R> P, int c0x, int c0y, int c0z, int wx, int wy, int wz, int ppc, uint32_t s0,
                             uint32_t s1, uint32_t inst, int tool_check, int32_t* flag, int64_t ncand) {
@@ -561,8 +586,10 @@ __global__ void k_gen_flags(Inst<R> P, int c0x, int c0y, int c0z, int wx, int wy
         const int ix = (int)(cell % wx), iy = (int)((cell / wx) % wy), iz = (int)(cell / ((int64_t)wx * wy));
         float u[4];
         philox_u4(s0, s1, (uint32_t)cell, (uint32_t)k, inst, 0u, u);
-        const double x = P.ox + ((double)(c0x + ix) + (double)u[0]) * P.dx;
-        const double z = P.oz + ((double)(c0z + iz) + (double)u[2]) * P.dx;
+        double off[3];
+        gen_offset(k, ppc, u, off);
+        const double x = P.ox + ((double)(c0x + ix) + off[0]) * P.dx;
+        const double z = P.oz + ((double)(c0z + iz) + off[2]) * P.dx;
         (void)iy;
         double nrm[3];
         if (tool_sdf(P, x, z, P.tool_p0[0], P.tool_p0[2], nrm) <= 0.0) keep = 0;
@@ -581,11 +608,13 @@ __global__ void k_gen_write(Inst<R> P, int c0x, int c0y, int c0z, int wx, int wy
     const int ix = (int)(cell % wx), iy = (int)((cell / wx) % wy), iz = (int)(cell / ((int64_t)wx * wy));
     float u[4];
     philox_u4(s0, s1, (uint32_t)cell, (uint32_t)k, inst, 0u, u);
+    double off[3];
+    gen_offset(k, ppc, u, off);
     const int64_t i = idx[c];
     const int64_t d = pbase + i;
-    pos_scratch[3 * d + 0] = (double)(c0x + ix) + (double)u[0];
-    pos_scratch[3 * d + 1] = (double)(c0y + iy) + (double)u[1];
-    pos_scratch[3 * d + 2] = (double)(c0z + iz) + (double)u[2];
+    pos_scratch[3 * d + 0] = (double)(c0x + ix) + off[0];
+    pos_scratch[3 * d + 1] = (double)(c0y + iy) + off[1];
+    pos_scratch[3 * d + 2] = (double)(c0z + iz) + off[2];
     ps.A[0][d] = mk4<R>(R(0), R(0), R(0), R(0));
     ps.A[1][d] = mk4<R>(R(0), R(0), R(0), R(0));
     ps.A[2][d] = mk4<R>(R(0), R(0), R(0), R(0));

@@ -515,7 +515,7 @@ struct JCOut {
 // so that the common elastic path keeps fewer registers.
 template <typename R> struct JCFlow {
     R Hp[9], sig[6], sl[3], sd[6], bs[6], e[6];
-    R eps, dT, D, q, p3, Ts, edot;
+    R eps, dT, D, q, p3, Ts, edot, tt;
     int errf;
     bool yielded, to_chip;
 };
@@ -531,13 +531,11 @@ __device__ __noinline__ JCFlow<R> jc_flow(const Inst<R>& P, JCFlow<R> f, R* bsx,
     R& dT = f.dT;
     R& D = f.D;
     int& errf = f.errf;
-    const R q = f.q, p3 = f.p3, Ts = f.Ts, edot = f.edot;
+    const R q = f.q, p3 = f.p3, Ts = f.Ts, edot = f.edot, tt = f.tt;
     const R ex = f.e[0], ey = f.e[1], ez = f.e[2], exy = f.e[3], exz = f.e[4], eyz = f.e[5];
     JCOut o{true, false, false};
     const R es = fmax(edot / P.edot0, R(1e-5));
     const R rt = R(1) + P.C * log(es);
-    // pow(0, y) is +0 for y > 0: skipped for the common unheated, unyielded particle
-    const R tt = R(1) - ((Ts > R(0) || !(P.m > R(0))) ? pow(Ts, P.m) : R(0));
     const R Y = (P.A + P.B * ((eps > R(0) || !(P.n > R(0))) ? pow(eps, P.n) : R(0))) * rt * tt;
     if (q > Y && q > R(1e-12)) {
         R dE, Yr = Y;
@@ -703,9 +701,13 @@ __device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[
 #pragma unroll
     for (int q2 = 0; q2 < 6; ++q2) sig[q2] = s[q2];
     sl[0] = s[3]; sl[1] = s[4]; sl[2] = s[5];
-    // an unheated particle with q below the smallest flow stress the step can
-    // have (ylo) cannot yield: the flow stress itself is not needed
-    if (Ts == R(0) && q < P.ylo) return o;
+    // thermal factor of the flow stress (pow(0, y) is +0 for y > 0: skipped
+    // for the common unheated particle)
+    const R tt = R(1) - ((Ts > R(0) || !(P.m > R(0))) ? pow(Ts, P.m) : R(0));
+    // a particle with q below the smallest flow stress the step can have
+    // (ylo tt, heated or not: ylo bounds (A + B eps^n)(1 + C ln es) from
+    // below) cannot yield: the flow stress itself is not needed
+    if (q < P.ylo * tt) return o;
     JCFlow<R> f;
 #pragma unroll
     for (int k = 0; k < 9; ++k) f.Hp[k] = Hp[k];
@@ -713,7 +715,7 @@ __device__ __forceinline__ JCOut jc_update(const Inst<R>& P, const R H[9], R Hp[
     for (int k = 0; k < 6; ++k) { f.sig[k] = sig[k]; f.sd[k] = sd[k]; f.bs[k] = bs[k]; }
     f.sl[0] = sl[0]; f.sl[1] = sl[1]; f.sl[2] = sl[2];
     f.e[0] = ex; f.e[1] = ey; f.e[2] = ez; f.e[3] = exy; f.e[4] = exz; f.e[5] = eyz;
-    f.eps = eps; f.dT = dT; f.D = D; f.q = q; f.p3 = p3; f.Ts = Ts; f.edot = edot; f.errf = errf;
+    f.eps = eps; f.dT = dT; f.D = D; f.q = q; f.p3 = p3; f.Ts = Ts; f.edot = edot; f.tt = tt; f.errf = errf;
     f = jc_flow<R>(P, f, bsx, sres_p, inst_tag);
 #pragma unroll
     for (int k = 0; k < 9; ++k) Hp[k] = f.Hp[k];

@@ -197,6 +197,28 @@ def tool_sdf(tool: dict, x: np.ndarray, z: np.ndarray, pr0: float, pr2: float) -
     return core - tool["radius"]
 
 
+# Strata of a cell's candidates for ppc <= 8: its octants in this fixed order
+# (mpm_aux.cu, gen_offset).
+OCTANT_ORDER = (0, 7, 3, 4, 5, 2, 6, 1)
+
+
+def gen_offset(k: np.ndarray, ppc: int, u) -> list:
+    """Offsets in cells of candidates k of a cell (host mirror of gen_offset,
+    mpm_aux.cu): a jittered point of the candidate's stratum, an octant of the
+    cell for ppc <= 8 (0.5 bit + 0.5 u, exact), else sub-cell 37 k mod n^3
+    of the n^3 grid, n the smallest even number with n^3 >= ppc
+    ((s + u) / n)."""
+    if ppc <= 8:
+        o = np.asarray(OCTANT_ORDER, dtype=np.int64)[k & 7]
+        return [0.5 * ((o >> a) & 1).astype(np.float64) + 0.5 * u[a].astype(np.float64) for a in range(3)]
+    n = 4
+    while n ** 3 < ppc:
+        n += 2
+    q = (37 * k) % (n ** 3)
+    sa = (q % n, (q // n) % n, q // (n * n))
+    return [(sa[a].astype(np.float64) + u[a].astype(np.float64)) / float(n) for a in range(3)]
+
+
 def generate_box(case: dict) -> Dict[str, np.ndarray]:
     """Host mirror of mpm_init_box: returns particle arrays in upload order."""
     p, box, tool = case["params"], case["box"], case["tool"]
@@ -209,8 +231,8 @@ def generate_box(case: dict) -> Dict[str, np.ndarray]:
     seed = int(box["seed"])
     u = philox4x32_10(seed & 0xFFFFFFFF, seed >> 32, cell, k, np.full_like(cell, box["instance"]),
                       np.zeros_like(cell))
-    xi = np.stack([(c0[0] + ix) + u[0].astype(np.float64), (c0[1] + iy) + u[1].astype(np.float64),
-                   (c0[2] + iz) + u[2].astype(np.float64)], axis=1)
+    off = gen_offset(k, ppc, u)
+    xi = np.stack([(c0[0] + ix) + off[0], (c0[1] + iy) + off[1], (c0[2] + iz) + off[2]], axis=1)
     dx = p["dx"]
     org = p["origin"]
     x = org[0] + xi[:, 0] * dx
@@ -313,9 +335,10 @@ def _generate_box_offset(case: dict, cell_offset: int) -> Dict[str, np.ndarray]:
     u = philox4x32_10(seed & 0xFFFFFFFF, seed >> 32, cell + cell_offset, k, np.full_like(cell, box["instance"]),
                       np.zeros_like(cell))
     dx, org = p["dx"], p["origin"]
-    x = org[0] + ((c0[0] + ix) + u[0].astype(np.float64)) * dx
-    y = org[1] + ((c0[1] + iy) + u[1].astype(np.float64)) * dx
-    z = org[2] + ((c0[2] + iz) + u[2].astype(np.float64)) * dx
+    off = gen_offset(k, ppc, u)
+    x = org[0] + ((c0[0] + ix) + off[0]) * dx
+    y = org[1] + ((c0[1] + iy) + off[1]) * dx
+    z = org[2] + ((c0[2] + iz) + off[2]) * dx
     keep = np.ones(len(cand), dtype=bool)
     if tool and tool.get("mode", A.TOOL_NONE) != A.TOOL_NONE:
         keep = tool_sdf(tool, x, z, tool["position"][0], tool["position"][2]) > 0.0

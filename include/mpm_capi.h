@@ -202,10 +202,13 @@ mpm_status mpm_destroy(mpm_handle *h);
 
 /* Replaces MPMSolver::initializeParticleBox (src/MPMSolver.cu:1297-1336) with a
  * seeded, jittered box: cells [c0, c1) (cell units from the grid origin),
- * ppc particles per cell at Philox4x32-10 uniform positions keyed by
- * (seed, instance, cell, k); cells whose lowest `fixed_layers` z-layers are
- * FIXED_BOUNDARY; particles inside the tool at t=0 are not kept.  Generated on
- * the device. */
+ * ppc particles per cell, candidate k of a cell at a Philox4x32-10 uniform
+ * point (keyed by seed, instance, cell, k) of its own stratum of the cell --
+ * for ppc <= 8 one octant per candidate in a fixed order, for larger ppc one
+ * sub-cell of the n^3 grid (n even) -- so that, as on the reference's regular
+ * lattice, every interior stencil-base cell holds exactly ppc particles;
+ * cells whose lowest `fixed_layers` z-layers are FIXED_BOUNDARY; particles
+ * inside the tool at t=0 are not kept.  Generated on the device. */
 mpm_status mpm_init_box(mpm_handle *h, const int32_t c0[3], const int32_t c1[3], int32_t ppc, uint64_t seed,
                         uint32_t instance, int32_t fixed_layers, double T0, const mpm_tool_desc *tool_at_t0);
 
