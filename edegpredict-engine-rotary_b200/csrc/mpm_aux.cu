@@ -841,9 +841,12 @@ __global__ void k_stats(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64_
     const double m = (double)P.pmass, V = (double)P.pvol;
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
         const int64_t pi = pbase + s;
-        // every load before the branch on the status: one memory round trip
+        // every load before the branch on the status (the position's bin and
+        // low parts included): one memory round trip
         const int st = ps.status[pi];
         const V4<R> a0 = ps.A[0][pi], a3 = ps.A[3][pi], b0 = ps.B[0][pi], s0 = ps.S[0][pi], s1 = ps.S[1][pi];
+        const int bin = ps.bin[pi];
+        const V4<R> xl = ps.X ? ps.X[pi] : mk4<R>(0, 0, 0, 0);
         if (st == ST_INACTIVE) { acc[18] += 1.0; continue; }
         if (st == ST_ACTIVE) acc[15] += 1.0;
         else if (st == ST_CHIP) acc[16] += 1.0;
@@ -870,8 +873,10 @@ __global__ void k_stats(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64_
             acc[12] = fmax(acc[12], Tamb + dT);
             acc[13] += 0.5 * m * v2;
             acc[14] += (vm * vm * m) / (6.0 * 80e9) + V * eps * vm;
-            double xw[3];
-            world_pos(P, ps, pi, a0, xw);
+            const int bx = bin % P.nbx, by = (bin / P.nbx) % P.nby, bz = bin / (P.nbx * P.nby);
+            const double xw[3] = {P.ox + ((double)(bx * kBin) + ((double)a0.x + (double)xl.x)) * P.dx,
+                                  P.oy + ((double)(by * kBin) + ((double)a0.y + (double)xl.y)) * P.dx,
+                                  P.oz + ((double)(bz * kBin) + ((double)a0.z + (double)xl.z)) * P.dx};
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
                 acc[19 + q] = fmin(acc[19 + q], xw[q]);
@@ -902,17 +907,29 @@ __global__ void k_stats(const Inst<R>* inst, PState<R> ps, int64_t pbase, int64_
     }
 }
 
-__global__ void k_stats_final(const double* partial, int nb, double* out) {
-    const int q = threadIdx.x;
-    if (q >= kStatSlots) return;
+// One CTA per slot: thread t combines the block partials t, t + kFinalT, ...
+// in order, then a fixed tree over the threads (the same order on every run).
+constexpr int kFinalT = 256;
+__global__ void __launch_bounds__(kFinalT) k_stats_final(const double* partial, int nb, double* out) {
+    __shared__ double sh[kFinalT];
+    const int q = blockIdx.x, t = threadIdx.x;
     const bool isMin = (q >= 19 && q < 22);
     const bool isMax = (q == 7 || q == 8 || q == 9 || q == 11 || q == 12 || (q >= 22 && q < 25));
-    double v = partial[q];
-    for (int b = 1; b < nb; ++b) {
+    double v = isMin ? INFINITY : (isMax ? -INFINITY : 0.0);
+    for (int b = t; b < nb; b += kFinalT) {
         const double u = partial[(int64_t)b * kStatSlots + q];
         v = isMin ? fmin(v, u) : (isMax ? fmax(v, u) : v + u);
     }
-    out[q] = v;
+    sh[t] = v;
+    __syncthreads();
+    for (int w = kFinalT / 2; w > 0; w >>= 1) {
+        if (t < w) {
+            const double u = sh[t + w];
+            sh[t] = isMin ? fmin(sh[t], u) : (isMax ? fmax(sh[t], u) : sh[t] + u);
+        }
+        __syncthreads();
+    }
+    if (t == 0) out[q] = sh[0];
 }
 
 template <typename R>
@@ -1021,7 +1038,7 @@ template <typename R>
 void launch_stats(const Inst<R>* inst_dev, const PState<R>& ps, int64_t pbase, int64_t n, double mu, double K,
                   double rho, double cp, double Tamb, double* partial, int nblocks, double* out, cudaStream_t st) {
     k_stats<R><<<nblocks, kT, 0, st>>>(inst_dev, ps, pbase, n, mu, K, rho, cp, Tamb, partial);
-    k_stats_final<<<1, kStatSlots, 0, st>>>(partial, nblocks, out);
+    k_stats_final<<<kStatSlots, kFinalT, 0, st>>>(partial, nblocks, out);
     launch_counter() += 2;
 }
 

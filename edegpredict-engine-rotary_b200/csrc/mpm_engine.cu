@@ -536,6 +536,7 @@ class Engine final : public EngineBase {
             if (gpool[b]) cudaFree(gpool[b]);
             gpool[b] = nullptr;
             CK(cudaMalloc(&gpool[b], sizeof(V4<R>) * nodes));
+            CK(cudaMemsetAsync(gpool[b], 0, sizeof(V4<R>) * nodes, st));
         }
         for (int b = 0; b < 3; ++b) {
             if (tpool[b]) cudaFree(tpool[b]);
