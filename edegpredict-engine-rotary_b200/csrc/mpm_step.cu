@@ -63,6 +63,14 @@ __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.a
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
+// Particle state is read and written once per step: streaming loads and
+// stores (evict-first) keep L1 for the register spills and L2 for the grid
+// tiles and stored node tiles (1.7 % off the fused step on 33.5 M particles,
+// 1.5 % on the 512-workpiece batch).  FP64 keeps plain accesses.
+__device__ __forceinline__ float4 ldcs4(const float4* p) { return __ldcs(p); }
+__device__ __forceinline__ D4 ldcs4(const D4* p) { return *p; }
+__device__ __forceinline__ void stcs4(float4* p, const float4 v) { __stcs(p, v); }
+__device__ __forceinline__ void stcs4(D4* p, const D4 v) { *p = v; }
 __device__ __forceinline__ void tmap_acquire(const CUtensorMap* map) {
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
 }
@@ -1286,9 +1294,10 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                 const int64_t pi = P.pbase + wk.start + (valid ? pl : 0);
 #endif
                 const uint8_t st_ld = ps.status[pi];
-                const V4<R> a0 = ps.A[0][pi], a1 = ps.A[1][pi], a2 = ps.A[2][pi], a3 = ps.A[3][pi];
-                const V4<R> xl = (G2P && ps.X) ? ps.X[pi] : mk4<R>(0, 0, 0, 0);
-                const V4<R> b0_ld = G2P ? mk4<R>(0, 0, 0, 0) : ps.B[0][pi];
+                const V4<R> a0 = ldcs4(&ps.A[0][pi]), a1 = ldcs4(&ps.A[1][pi]), a2 = ldcs4(&ps.A[2][pi]),
+                            a3 = ldcs4(&ps.A[3][pi]);
+                const V4<R> xl = (G2P && ps.X) ? ldcs4(&ps.X[pi]) : mk4<R>(0, 0, 0, 0);
+                const V4<R> b0_ld = G2P ? mk4<R>(0, 0, 0, 0) : ldcs4(&ps.B[0][pi]);
                 uint8_t st = valid ? st_ld : (uint8_t)ST_INACTIVE;
                 if (st != ST_INACTIVE) {
                     const uint8_t st_in = st;
@@ -1426,11 +1435,11 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                 const double zw = P.oz + ((double)g0z + ((double)xi[2] + (double)lo[2])) * P.dx;
                                 if (zw < tipz && Dm > R(1e-6)) {
                                     st = ST_CHIP;
-                                    const V4<R> s0 = ps.S[0][pi];
+                                    const V4<R> s0 = ldcs4(&ps.S[0][pi]);
                                     const R rs = sqrt(s0.x * s0.x + s0.y * s0.y + s0.z * s0.z);
                                     ps.sres[pi] = fmax(ps.sres[pi], rs);
-                                    ps.S[0][pi] = mk4<R>(0, 0, 0, 0);
-                                    ps.S[1][pi] = mk4<R>(0, 0, 0, 0);
+                                    stcs4(&ps.S[0][pi], mk4<R>(0, 0, 0, 0));
+                                    stcs4(&ps.S[1][pi], mk4<R>(0, 0, 0, 0));
                                     Dm = fmax(Dm, P.Dth);
                                     dirtyA = true;
                                 }
@@ -1501,11 +1510,11 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                             st = ST_INACTIVE;
                             if (G2P) {
                                 // no later G2P writes this particle: store this step's v, strain rate and C
-                                ps.B[0][pi] = mk4<R>(v[0], v[1], v[2], edot);
+                                stcs4(&ps.B[0][pi], mk4<R>(v[0], v[1], v[2], edot));
                                 if (have_C) {
-                                    ps.B[1][pi] = mk4<R>(Cm[0], Cm[1], Cm[2], Cm[3]);
-                                    ps.B[2][pi] = mk4<R>(Cm[4], Cm[5], Cm[6], Cm[7]);
-                                    ps.B[3][pi] = mk4<R>(Cm[8], R(0), R(0), R(0));
+                                    stcs4(&ps.B[1][pi], mk4<R>(Cm[0], Cm[1], Cm[2], Cm[3]));
+                                    stcs4(&ps.B[2][pi], mk4<R>(Cm[4], Cm[5], Cm[6], Cm[7]));
+                                    stcs4(&ps.B[3][pi], mk4<R>(Cm[8], R(0), R(0), R(0)));
                                 }
                             }
                         } else {
@@ -1529,7 +1538,7 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                             if (!skip && st == ST_ACTIVE) {
                                 // F_p - I: loaded here, where the constitutive update needs
                                 // it, rather than held in registers through the gather
-                                const V4<R> a4 = ps.A[4][pi], a5 = ps.A[5][pi];
+                                const V4<R> a4 = ldcs4(&ps.A[4][pi]), a5 = ldcs4(&ps.A[5][pi]);
                                 R Hp[9] = {a4.x, a4.y, a4.z, a4.w, a5.x, a5.y, a5.z, a5.w, Hp8};
                                 R bsv[6];
                                 R* bsp = nullptr;
@@ -1545,8 +1554,8 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                     yielded = true;
                                     dirtyA = true;
                                     Hp8 = Hp[8];
-                                    ps.A[4][pi] = mk4<R>(Hp[0], Hp[1], Hp[2], Hp[3]);
-                                    ps.A[5][pi] = mk4<R>(Hp[4], Hp[5], Hp[6], Hp[7]);
+                                    stcs4(&ps.A[4][pi], mk4<R>(Hp[0], Hp[1], Hp[2], Hp[3]));
+                                    stcs4(&ps.A[5][pi], mk4<R>(Hp[4], Hp[5], Hp[6], Hp[7]));
                                     if (bsp) {
                                         ps.K[0][pi] = mk4<R>(bsv[0], bsv[1], bsv[2], bsv[3]);
                                         ps.K[1][pi] = mk4<R>(bsv[4], bsv[5], R(0), R(0));
@@ -1557,22 +1566,23 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
                                 // of every particle that passes its temperature guard
                                 if (sa.sigma_all || Dm > R(1e-6) || P.lod || near_kill ||
                                     (P.asb_on && dT > P.asb_rise)) {
-                                    ps.S[0][pi] = mk4<R>(sig[0], sig[1], sig[2], sig[3]);
-                                    ps.S[1][pi] = mk4<R>(sig[4], sig[5], R(0), R(0));
+                                    stcs4(&ps.S[0][pi], mk4<R>(sig[0], sig[1], sig[2], sig[3]));
+                                    stcs4(&ps.S[1][pi], mk4<R>(sig[4], sig[5], R(0), R(0)));
                                 }
                             }
                             // C of the particle: from this launch's gather, or the frozen value of
                             // a CHIP particle (g2pKernel keeps it)
                             if (!have_C && !fixed) {
-                                const V4<R> c1 = ps.B[1][pi], c2 = ps.B[2][pi], c3 = ps.B[3][pi];
+                                const V4<R> c1 = ldcs4(&ps.B[1][pi]), c2 = ldcs4(&ps.B[2][pi]),
+                                            c3 = ldcs4(&ps.B[3][pi]);
                                 Cm[0] = c1.x; Cm[1] = c1.y; Cm[2] = c1.z; Cm[3] = c1.w;
                                 Cm[4] = c2.x; Cm[5] = c2.y; Cm[6] = c2.z; Cm[7] = c2.w; Cm[8] = c3.x;
                             }
                             if (!fixed && have_C && st == ST_CHIP && st_in != ST_CHIP) {
                                 // turned CHIP this launch: freeze C as the reference does
-                                ps.B[1][pi] = mk4<R>(Cm[0], Cm[1], Cm[2], Cm[3]);
-                                ps.B[2][pi] = mk4<R>(Cm[4], Cm[5], Cm[6], Cm[7]);
-                                ps.B[3][pi] = mk4<R>(Cm[8], R(0), R(0), R(0));
+                                stcs4(&ps.B[1][pi], mk4<R>(Cm[0], Cm[1], Cm[2], Cm[3]));
+                                stcs4(&ps.B[2][pi], mk4<R>(Cm[4], Cm[5], Cm[6], Cm[7]));
+                                stcs4(&ps.B[3][pi], mk4<R>(Cm[8], R(0), R(0), R(0)));
                                 wrote_C = true;
                             }
                             // scatter payload: Q = m (v - dx C d) + f_ext dt, R = m dx C,
@@ -1655,23 +1665,23 @@ __global__ void __launch_bounds__(kNT, MPMB_MIN_CTAS) k_step(const Inst<R>* __re
 
                     // write back
                     if (dirtyA) {
-                        if (has_lo) ps.X[pi] = mk4<R>(lo[0], lo[1], lo[2], R(0));
-                        ps.A[0][pi] = mk4<R>(xi[0], xi[1], xi[2], eps);
-                        ps.A[1][pi] = mk4<R>(H[0], H[1], H[2], H[3]);
-                        ps.A[2][pi] = mk4<R>(H[4], H[5], H[6], H[7]);
-                        ps.A[3][pi] = mk4<R>(H[8], Hp8, dT, Dm);
+                        if (has_lo) stcs4(&ps.X[pi], mk4<R>(lo[0], lo[1], lo[2], R(0)));
+                        stcs4(&ps.A[0][pi], mk4<R>(xi[0], xi[1], xi[2], eps));
+                        stcs4(&ps.A[1][pi], mk4<R>(H[0], H[1], H[2], H[3]));
+                        stcs4(&ps.A[2][pi], mk4<R>(H[4], H[5], H[6], H[7]));
+                        stcs4(&ps.A[3][pi], mk4<R>(H[8], Hp8, dT, Dm));
                     }
                     if (st != st_in) ps.status[pi] = st;
                     if (G2P && sa.write_out && st != ST_INACTIVE) {
                         if (fixed) {
-                            const V4<R> b0 = ps.B[0][pi];
-                            ps.B[0][pi] = mk4<R>(R(0), R(0), R(0), b0.w);
+                            const V4<R> b0 = ldcs4(&ps.B[0][pi]);
+                            stcs4(&ps.B[0][pi], mk4<R>(R(0), R(0), R(0), b0.w));
                         } else {
-                            ps.B[0][pi] = mk4<R>(v[0], v[1], v[2], edot);
+                            stcs4(&ps.B[0][pi], mk4<R>(v[0], v[1], v[2], edot));
                             if (have_C && !wrote_C && st_in != ST_CHIP) {
-                                ps.B[1][pi] = mk4<R>(Cm[0], Cm[1], Cm[2], Cm[3]);
-                                ps.B[2][pi] = mk4<R>(Cm[4], Cm[5], Cm[6], Cm[7]);
-                                ps.B[3][pi] = mk4<R>(Cm[8], R(0), R(0), R(0));
+                                stcs4(&ps.B[1][pi], mk4<R>(Cm[0], Cm[1], Cm[2], Cm[3]));
+                                stcs4(&ps.B[2][pi], mk4<R>(Cm[4], Cm[5], Cm[6], Cm[7]));
+                                stcs4(&ps.B[3][pi], mk4<R>(Cm[8], R(0), R(0), R(0)));
                             }
                         }
                     }
