@@ -310,18 +310,25 @@ __device__ __noinline__ GatherOut<R> gather_global(const Inst<R>& P, const V4<R>
         o.v[c] = R(0);
         for (int b = 0; b < 3; ++b) { o.M[c][b] = R(0); o.L[c][b] = R(0); }
     }
+    // the 27 node loads first, all in flight together, then the node updates
+    V4<R> gv[27];
+    bool in[27];
+#pragma unroll
+    for (int q = 0; q < 27; ++q) {
+        const int gx = gb[0] + q / 9, gy = gb[1] + (q / 3) % 3, gz = gb[2] + q % 3;
+        const int64_t gi = gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz);
+        in[q] = gx >= 0 && gx < P.nx && gy >= 0 && gy < P.ny && gz >= 0 && gz < P.nz &&
+                MPMB_CHECK(gi >= 0 && gi < P.nn, kSiteGather, gi);
+        gv[q] = in[q] ? grid[gi] : mk4<R>(R(0), R(0), R(0), R(0));
+    }
     for (int i = 0; i < 3; ++i) {
         const int gx = gb[0] + i;
-        if (gx < 0 || gx >= P.nx) continue;
         for (int j = 0; j < 3; ++j) {
             const int gy = gb[1] + j;
-            if (gy < 0 || gy >= P.ny) continue;
             for (int k = 0; k < 3; ++k) {
                 const int gz = gb[2] + k;
-                if (gz < 0 || gz >= P.nz) continue;
-                const int64_t gi = gx + (int64_t)P.nx * (gy + (int64_t)P.ny * gz);
-                if (!MPMB_CHECK(gi >= 0 && gi < P.nn, kSiteGather, gi)) continue;
-                const NV<R> nv = node_vel(P, grid[gi], gx, gy, gz, pr0, pr2);
+                if (!in[i * 9 + j * 3 + k]) continue;
+                const NV<R> nv = node_vel(P, gv[i * 9 + j * 3 + k], gx, gy, gz, pr0, pr2);
                 const R vv[3] = {nv.x, nv.y, nv.z};
                 const R ww = w[0][i] * w[1][j] * w[2][k];
                 const R g0 = dw[0][i] * w[1][j] * w[2][k], g1 = w[0][i] * dw[1][j] * w[2][k],
